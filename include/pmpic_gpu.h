@@ -1,0 +1,196 @@
+/*
+ * pmpic_gpu.h -- C ABI of libpmpic_gpu.so, the B200 implementation of the PMPIC
+ * per-timestep hot path.
+ *
+ * The reference (EPCCed/pmpic, Fortran + MPI) runs its hot path as five MONC
+ * components whose timestep callbacks the timestepper calls rksteps (= 4) times
+ * per model step, in the integrator group order of global_config:43:
+ *   vort2vel -> vorticity_tendency -> rk4_integrator -> parcel_splitting -> parcel_mixing
+ * Each component exports `<name>_get_descriptor()` with init / timestep /
+ * finalise procedure pointers taking `type(model_state_type)`
+ * (model_core/src/components/monc_component.F90:51-107).  This header declares
+ * the C entry points that new versions of those five component modules bind
+ * through `iso_c_binding`: one entry point per timestep
+ * callback, plus context set-up, parcel/grid transfer and step information.
+ *
+ * Conventions
+ *  - Every call is synchronous from the caller's view and returns PMPIC_OK (0)
+ *    or a negative PMPIC_ERR_* code; pmpic_last_error() gives the message.  The
+ *    reference aborts (`error stop`) in the same situations; the Fortran shim
+ *    turns a non-zero return into `error stop`.
+ *  - Device memory is owned by the context.  Host pointers are borrowed for the
+ *    duration of a call.  Parcel state stays on the device between callbacks.
+ *  - A context is not thread-safe: one host thread per context (the reference
+ *    runs MPI_THREAD_SERIALIZED and calls callbacks from the master thread).
+ *  - Parcel slots are 0-based here (Fortran slot n is C slot n-1).
+ *  - Grids are exchanged dense, x fastest: physical (nz+1) x ny x nx; spectral
+ *    (nz+1) x (ny+2) x (nx+2) in the reference's four-reals-per-mode layout.
+ */
+#ifndef PMPIC_GPU_H
+#define PMPIC_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes ------------------------------------------------------- */
+#define PMPIC_OK              0
+#define PMPIC_ERR_CONFIG     -1  /* invalid configuration (sizes, origin, capacity) */
+#define PMPIC_ERR_CAPACITY   -2  /* max_parcels reached: parcel_splitting.F90:90-93, parcel_mixing.F90:196-199, haloswap.F90:705-708 */
+#define PMPIC_ERR_OUT_OF_BOX -3  /* parcel outside the grid: parcel_interpolation.F90:222-237 */
+#define PMPIC_ERR_ZERO_PIVOT -4  /* tridiagonal zero pivot: fft_ops.F90:642-645 */
+#define PMPIC_ERR_BACKFILL   -5  /* mixing backfill ran below slot 1 (reference reads keep(0)) */
+#define PMPIC_ERR_TIMEOUT    -6  /* a bounded device wait gave up */
+#define PMPIC_ERR_CUDA       -7  /* CUDA runtime error */
+#define PMPIC_ERR_ARG        -8  /* invalid argument */
+#define PMPIC_ERR_STATE      -9  /* call not valid in the current state */
+
+/* ---- precision forms ---------------------------------------------------- */
+#define PMPIC_FP64  0            /* plain FP64 throughout (the reference's DEFAULT_PRECISION) */
+
+/* ---- parcel property ids (parcels.F90:19-34) ----------------------------- */
+enum {
+  PMPIC_PROP_X = 0, PMPIC_PROP_Y, PMPIC_PROP_Z, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R,
+  PMPIC_PROP_DXDT, PMPIC_PROP_DYDT, PMPIC_PROP_DZDT, PMPIC_PROP_DPDT, PMPIC_PROP_DQDT, PMPIC_PROP_DRDT,
+  PMPIC_PROP_H, PMPIC_PROP_B, PMPIC_PROP_VOL, PMPIC_PROP_STRETCH, PMPIC_PROP_TAG, PMPIC_PROP_BTOT,
+  PMPIC_PROP_XO, PMPIC_PROP_YO, PMPIC_PROP_ZO, PMPIC_PROP_XF, PMPIC_PROP_YF, PMPIC_PROP_ZF,
+  PMPIC_PROP_PO, PMPIC_PROP_QO, PMPIC_PROP_RO, PMPIC_PROP_PF, PMPIC_PROP_QF, PMPIC_PROP_RF,
+  PMPIC_NPROP
+};
+
+/* ---- grid ids (state.F90:38-67; vorticity_tendency.F90:90-91) ----------- */
+enum {
+  PMPIC_GRID_U = 0, PMPIC_GRID_V, PMPIC_GRID_W, PMPIC_GRID_P, PMPIC_GRID_Q, PMPIC_GRID_R,
+  PMPIC_GRID_B, PMPIC_GRID_DP, PMPIC_GRID_DQ, PMPIC_GRID_DR, PMPIC_GRID_VOL, PMPIC_GRID_HG,
+  PMPIC_NGRID
+};
+enum { PMPIC_SPEC_U = 0, PMPIC_SPEC_V, PMPIC_SPEC_W, PMPIC_NSPEC };  /* u_s, v_s, w_s */
+
+typedef struct pmpic_ctx pmpic_ctx;
+
+/* Model configuration: the hot-path keys of config.mcf / global_config. */
+typedef struct pmpic_config {
+  int32_t nx, ny, nz;              /* cell counts (config keys nx, ny, nz); nz+1 z points (setup_grid.F90:51) */
+  double xmin, xmax, ymin, ymax, zmin, zmax;  /* domain; origins must be 0 */
+  double dtm, dtmax;               /* rk4_integrator.F90:38-41 */
+  double timestep_prefactor;       /* vorticity_tendency.F90:96 */
+  int64_t max_parcels;             /* parcelsetup_base max_parcels */
+  int32_t precision;               /* PMPIC_FP64 */
+  int32_t device;                  /* CUDA device ordinal */
+} pmpic_config;
+
+/* Per-step counters, copied to the host once per call of pmpic_get_step_info. */
+typedef struct pmpic_step_info {
+  int64_t n_parcels;               /* numparcels_local */
+  double dtm;                      /* state%dtm after the dt rule */
+  int32_t limiter;                 /* 0 dtmax, 1 velocity (vort2vel.F90:368), 2 vorticity (vorticity_tendency.F90:300) */
+  int64_t n_split;                 /* parcels split in the last splitting call */
+  int64_t n_removed;               /* nremove of the last mixing call */
+  int64_t n_added;                 /* nadd of the last mixing call */
+  int64_t n_migrated;              /* parcels re-slotted by the last parcel haloswap */
+  int32_t error;                   /* sticky device error word (PMPIC_ERR_*) */
+  char message[160];
+} pmpic_step_info;
+
+/* ---- context ------------------------------------------------------------ */
+/* Replaces the initialisation callbacks of the five components plus the
+ * setup_grid / parcelsetup_base allocation (setup_grid.F90:116-144,
+ * parcelsetup_base.F90:63-81, rk4_integrator.F90:33-78, vort2vel.F90:46-90,
+ * vorticity_tendency.F90:52-99, parcel_mixing.F90:46-64). */
+int  pmpic_create(const pmpic_config* cfg, pmpic_ctx** out);
+/* Replaces the finalisation callbacks (e.g. rk4_integrator.F90:321-337). */
+void pmpic_destroy(pmpic_ctx* ctx);
+const char* pmpic_last_error(const pmpic_ctx* ctx);
+
+/* ---- parcel transfer (setup, restart and dumps; not on the timestep path) -- */
+/* Sets numparcels_local = n and the 11 prognostic properties of slots 0..n-1;
+ * the RK4 arrays and tendencies of those slots are set to zero. */
+int pmpic_upload_parcels(pmpic_ctx* ctx, int64_t n,
+                         const double* x, const double* y, const double* z,
+                         const double* p, const double* q, const double* r,
+                         const double* b, const double* h, const double* vol,
+                         const double* stretch, const double* tag);
+/* Copies slots 0..n-1 (n = numparcels_local, returned in *n) of the same 11
+ * properties; any pointer may be NULL. Fails if capacity < n. */
+int pmpic_download_parcels(pmpic_ctx* ctx, int64_t capacity, int64_t* n,
+                           double* x, double* y, double* z, double* p, double* q, double* r,
+                           double* b, double* h, double* vol, double* stretch, double* tag);
+/* Generic property access over slots 0..n-1 (n <= max_parcels). */
+int pmpic_set_property(pmpic_ctx* ctx, int prop, int64_t n, const double* src);
+int pmpic_get_property(pmpic_ctx* ctx, int prop, int64_t n, double* dst);
+int pmpic_set_count(pmpic_ctx* ctx, int64_t n);
+int pmpic_get_count(pmpic_ctx* ctx, int64_t* n);
+
+/* ---- component timestep callbacks (one call each, as the timestepper does) -- */
+int pmpic_vort2vel(pmpic_ctx* ctx);              /* vort2vel.F90:98-400 */
+int pmpic_vorticity_tendency(pmpic_ctx* ctx);    /* vorticity_tendency.F90:107-334 */
+int pmpic_rk4_integrator(pmpic_ctx* ctx);        /* rk4_integrator.F90:95-319 (+ parcel_haloswap) */
+int pmpic_parcel_splitting(pmpic_ctx* ctx);      /* parcel_splitting.F90:47-168 */
+int pmpic_parcel_mixing(pmpic_ctx* ctx);         /* parcel_mixing.F90:68-431 */
+/* nsteps model steps: the integrator group run rksteps (=4) times per step
+ * (timestepper.F90:89-106 with global_config:43's group contents). */
+int pmpic_step(pmpic_ctx* ctx, int nsteps);
+int pmpic_get_step_info(pmpic_ctx* ctx, pmpic_step_info* info);
+
+/* Component iteration counters (vort2vel, vorticity_tendency, rk4 stage,
+ * splitting, mixing) -- the modules' `iteration` / `rkstep` save variables. */
+int pmpic_get_counters(pmpic_ctx* ctx, int32_t counters[5]);
+int pmpic_set_counters(pmpic_ctx* ctx, const int32_t counters[5]);
+int pmpic_set_dtm(pmpic_ctx* ctx, double dtm);
+
+/* ---- grid transfer (diagnostics, writebinary-style dumps, tests) ---------- */
+int pmpic_download_grid(pmpic_ctx* ctx, int grid, double* dst);      /* (nz+1) x ny x nx */
+int pmpic_upload_grid(pmpic_ctx* ctx, int grid, const double* src);
+int pmpic_download_spectral(pmpic_ctx* ctx, int spec, double* dst);  /* (nz+1) x (ny+2) x (nx+2) */
+
+/* ---- kernel-level entry points (the model-core routines the components call) */
+/* cache_parcel_interp_weights (parcel_interpolation.F90:186-262): writes the
+ * interior cell id ((k-1)*ny + (j-3))*nx + (i-3) of slots 0..n-1. */
+int pmpic_op_cell_ids(pmpic_ctx* ctx, int32_t* cells);
+/* par2grid (parcel_interpolation.F90:336-481) of a property into a grid. */
+int pmpic_op_par2grid(pmpic_ctx* ctx, int prop, int grid);
+/* grid2par (parcel_interpolation.F90:267-332) of a grid into a property. */
+int pmpic_op_grid2par(pmpic_ctx* ctx, int grid, int prop);
+/* perform_forward_3dfft / perform_backwards_3dfft (pencilfft.F90:151-212). */
+int pmpic_op_fft_forward(pmpic_ctx* ctx, const double* phys, double* spec);
+int pmpic_op_fft_backward(pmpic_ctx* ctx, const double* spec, double* phys);
+/* fft_ops.F90: diffx :204-302, diffy :305-401, spectral_filter :176-197,
+ * diffz :419-483 (bot/top may be NULL; else (ny+2) x (nx+2)), laplinv :505-601. */
+int pmpic_op_diffx(pmpic_ctx* ctx, const double* in, double* out);
+int pmpic_op_diffy(pmpic_ctx* ctx, const double* in, double* out);
+int pmpic_op_filter(pmpic_ctx* ctx, const double* in, double* out);
+int pmpic_op_diffz(pmpic_ctx* ctx, const double* in, double* out, const double* bot, const double* top);
+int pmpic_op_laplinv(pmpic_ctx* ctx, double* inout, int df_zero_on_boundary);
+/* parcel_haloswap (parcels/haloswap.F90:109-289), single-GPU semantics. */
+int pmpic_op_parcel_haloswap(pmpic_ctx* ctx);
+
+/* ---- parcel set-up (new set-up components; not on the graded path) -------- */
+/* Jittered thermal plume: sub^3 parcels per cell on a sub-lattice jittered by
+ * U(+-jitter) sub-spacings (Philox4x32-10 keyed by seed and parcel index),
+ * vol = cell volume / sub^3, zero vorticity, tag = parcel index.  Buoyancy
+ * b = max(0, z - z_strat) * n2 + excess * cos^2(pi r / (2 radius)) inside the
+ * thermal; humidity h = h_in inside, h_env0 * (1 - z / Lz) outside.
+ * Parcels are ordered cell by cell (x outer, then y, then z) and, inside a
+ * cell, sub-lattice point by point (x outer, z inner), the order of
+ * basic_parcelsetup.F90:90-118. */
+typedef struct pmpic_thermal_params {
+  int32_t nx, ny, nz;
+  double lx, ly, lz;
+  int32_t sub;            /* parcels per cell per direction (2) */
+  double jitter;          /* jitter amplitude in sub-spacings (0.25) */
+  uint64_t seed;
+  double xc, yc, zc, radius, excess;
+  double h_in, h_env0;
+  double z_strat, n2;
+} pmpic_thermal_params;
+int64_t pmpic_setup_count(const pmpic_thermal_params* prm);
+int pmpic_setup_thermal(const pmpic_thermal_params* prm, int64_t n,
+                        double* x, double* y, double* z, double* p, double* q, double* r,
+                        double* b, double* h, double* vol, double* stretch, double* tag);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PMPIC_GPU_H */

@@ -1,0 +1,325 @@
+"""pmpic_b200 -- B200 implementation of the PMPIC per-timestep hot path.
+
+A ctypes binding of ``libpmpic_gpu.so`` (the C ABI in ``include/pmpic_gpu.h``).
+The library is built in-tree by ``pmpic_b200/Makefile`` (nvcc, sm_100a).  There
+is no CPU fallback: if the library or a CUDA device is missing, creating a
+``Context`` raises.
+
+The context mirrors the reference's component interface: one method per
+timestep callback of the integrator group (``vort2vel``,
+``vorticity_tendency``, ``rk4_integrator``, ``parcel_splitting``,
+``parcel_mixing``), each advancing the component's own iteration counter
+exactly like the Fortran modules' ``iteration`` / ``rkstep`` variables, and
+``step(n)`` for whole model steps (the RK group run four times per step).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpmpic_gpu.so")
+
+PROPS = ["x", "y", "z", "p", "q", "r", "dxdt", "dydt", "dzdt", "dpdt", "dqdt", "drdt",
+         "h", "b", "vol", "stretch", "tag", "btot",
+         "xo", "yo", "zo", "xf", "yf", "zf", "po", "qo", "ro", "pf", "qf", "rf"]
+PROP = {n: i for i, n in enumerate(PROPS)}
+GRIDS = ["u", "v", "w", "p", "q", "r", "b", "dp", "dq", "dr", "vol", "hg"]
+GRID = {n: i for i, n in enumerate(GRIDS)}
+SPECS = ["u_s", "v_s", "w_s"]
+SPEC = {n: i for i, n in enumerate(SPECS)}
+IO_PROPS = ["x", "y", "z", "p", "q", "r", "b", "h", "vol", "stretch", "tag"]
+
+ERRORS = {0: "ok", -1: "config", -2: "capacity", -3: "out of box", -4: "zero pivot",
+          -5: "backfill", -6: "timeout", -7: "cuda", -8: "argument", -9: "state"}
+
+
+class Config(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+                ("xmin", C.c_double), ("xmax", C.c_double), ("ymin", C.c_double),
+                ("ymax", C.c_double), ("zmin", C.c_double), ("zmax", C.c_double),
+                ("dtm", C.c_double), ("dtmax", C.c_double), ("timestep_prefactor", C.c_double),
+                ("max_parcels", C.c_int64), ("precision", C.c_int32), ("device", C.c_int32)]
+
+
+class StepInfo(C.Structure):
+    _fields_ = [("n_parcels", C.c_int64), ("dtm", C.c_double), ("limiter", C.c_int32),
+                ("n_split", C.c_int64), ("n_removed", C.c_int64), ("n_added", C.c_int64),
+                ("n_migrated", C.c_int64), ("error", C.c_int32), ("message", C.c_char * 160)]
+
+
+class ThermalParams(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+                ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double),
+                ("sub", C.c_int32), ("jitter", C.c_double), ("seed", C.c_uint64),
+                ("xc", C.c_double), ("yc", C.c_double), ("zc", C.c_double),
+                ("radius", C.c_double), ("excess", C.c_double),
+                ("h_in", C.c_double), ("h_env0", C.c_double),
+                ("z_strat", C.c_double), ("n2", C.c_double)]
+
+
+class PmpicError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"pmpic error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+def build() -> None:
+    """Compile libpmpic_gpu.so in-tree for sm_100a."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run pmpic_b200.build() (no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        P, D, I64 = C.c_void_p, C.POINTER(C.c_double), C.c_int64
+        L.pmpic_create.argtypes = [C.POINTER(Config), C.POINTER(P)]
+        L.pmpic_destroy.argtypes = [P]
+        L.pmpic_last_error.restype = C.c_char_p
+        L.pmpic_last_error.argtypes = [P]
+        L.pmpic_upload_parcels.argtypes = [P, I64] + [D] * 11
+        L.pmpic_download_parcels.argtypes = [P, I64, C.POINTER(I64)] + [D] * 11
+        L.pmpic_set_property.argtypes = [P, C.c_int, I64, D]
+        L.pmpic_get_property.argtypes = [P, C.c_int, I64, D]
+        L.pmpic_set_count.argtypes = [P, I64]
+        L.pmpic_get_count.argtypes = [P, C.POINTER(I64)]
+        for n in ["pmpic_vort2vel", "pmpic_vorticity_tendency", "pmpic_rk4_integrator",
+                  "pmpic_parcel_splitting", "pmpic_parcel_mixing", "pmpic_op_parcel_haloswap"]:
+            getattr(L, n).argtypes = [P]
+        L.pmpic_step.argtypes = [P, C.c_int]
+        L.pmpic_get_step_info.argtypes = [P, C.POINTER(StepInfo)]
+        L.pmpic_get_counters.argtypes = [P, C.POINTER(C.c_int32)]
+        L.pmpic_set_counters.argtypes = [P, C.POINTER(C.c_int32)]
+        L.pmpic_set_dtm.argtypes = [P, C.c_double]
+        L.pmpic_download_grid.argtypes = [P, C.c_int, D]
+        L.pmpic_upload_grid.argtypes = [P, C.c_int, D]
+        L.pmpic_download_spectral.argtypes = [P, C.c_int, D]
+        L.pmpic_op_cell_ids.argtypes = [P, C.POINTER(C.c_int32)]
+        L.pmpic_op_par2grid.argtypes = [P, C.c_int, C.c_int]
+        L.pmpic_op_grid2par.argtypes = [P, C.c_int, C.c_int]
+        L.pmpic_op_fft_forward.argtypes = [P, D, D]
+        L.pmpic_op_fft_backward.argtypes = [P, D, D]
+        L.pmpic_op_diffx.argtypes = [P, D, D]
+        L.pmpic_op_diffy.argtypes = [P, D, D]
+        L.pmpic_op_filter.argtypes = [P, D, D]
+        L.pmpic_op_diffz.argtypes = [P, D, D, D, D]
+        L.pmpic_op_laplinv.argtypes = [P, D, C.c_int]
+        L.pmpic_setup_count.restype = I64
+        L.pmpic_setup_count.argtypes = [C.POINTER(ThermalParams)]
+        L.pmpic_setup_thermal.argtypes = [C.POINTER(ThermalParams), I64] + [D] * 11
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def thermal_parcels(nx, ny, nz, lx=2 * np.pi, ly=2 * np.pi, lz=np.pi, sub=2, jitter=0.25, seed=1,
+                    xc=np.pi, yc=np.pi, zc=0.6, radius=0.4, excess=1.0, h_in=0.95, h_env0=0.3,
+                    z_strat=1.2, n2=1.0) -> dict:
+    """Jittered-lattice thermal plume initial condition (host, Philox4x32-10)."""
+    prm = ThermalParams(nx, ny, nz, lx, ly, lz, sub, jitter, seed, xc, yc, zc, radius, excess,
+                        h_in, h_env0, z_strat, n2)
+    n = lib().pmpic_setup_count(C.byref(prm))
+    out = {k: np.empty(n, np.float64) for k in IO_PROPS}
+    rc = lib().pmpic_setup_thermal(C.byref(prm), n, *[_dp(out[k]) for k in IO_PROPS])
+    if rc:
+        raise PmpicError(rc, "pmpic_setup_thermal")
+    return out
+
+
+class Context:
+    """One device-resident model state (the reference's model_state_type)."""
+
+    def __init__(self, nx, ny, nz, lx, ly, lz, dtm=0.01, dtmax=0.01, prefactor=0.5,
+                 max_parcels=1 << 20, device=0):
+        L = lib()
+        self.nx, self.ny, self.nz = nx, ny, nz
+        cfg = Config(nx, ny, nz, 0.0, lx, 0.0, ly, 0.0, lz, dtm, dtmax, prefactor,
+                     int(max_parcels), 0, device)
+        h = C.c_void_p()
+        rc = L.pmpic_create(C.byref(cfg), C.byref(h))
+        if rc:
+            raise PmpicError(rc, "pmpic_create failed")
+        self._h = h
+        self.max_parcels = int(max_parcels)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pmpic_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc:
+            raise PmpicError(rc, lib().pmpic_last_error(self._h).decode())
+
+    # -- parcels -----------------------------------------------------------------
+    @property
+    def n(self) -> int:
+        v = C.c_int64()
+        self._check(lib().pmpic_get_count(self._h, C.byref(v)))
+        return int(v.value)
+
+    def upload(self, **arrays):
+        n = len(arrays["x"])
+        ptrs = []
+        keep = []
+        for k in IO_PROPS:
+            a = arrays.get(k)
+            if a is not None:
+                a = np.ascontiguousarray(a, np.float64)
+                assert len(a) == n
+                keep.append(a)
+            ptrs.append(_dp(a))
+        self._check(lib().pmpic_upload_parcels(self._h, n, *ptrs))
+
+    def download(self) -> dict:
+        n = self.n
+        out = {k: np.empty(n, np.float64) for k in IO_PROPS}
+        cnt = C.c_int64()
+        self._check(lib().pmpic_download_parcels(self._h, n, C.byref(cnt),
+                                                 *[_dp(out[k]) for k in IO_PROPS]))
+        return out
+
+    def set(self, name, arr, n=None):
+        a = np.ascontiguousarray(arr, np.float64)
+        self._check(lib().pmpic_set_property(self._h, PROP[name], len(a) if n is None else n, _dp(a)))
+
+    def get(self, name, n=None) -> np.ndarray:
+        n = self.n if n is None else n
+        out = np.empty(n, np.float64)
+        self._check(lib().pmpic_get_property(self._h, PROP[name], n, _dp(out)))
+        return out
+
+    def set_count(self, n):
+        self._check(lib().pmpic_set_count(self._h, int(n)))
+
+    def grid(self, name) -> np.ndarray:
+        out = np.empty((self.nz + 1, self.ny, self.nx), np.float64)
+        self._check(lib().pmpic_download_grid(self._h, GRID[name], _dp(out)))
+        return out
+
+    def set_grid(self, name, g):
+        g = np.ascontiguousarray(g, np.float64)
+        assert g.shape == (self.nz + 1, self.ny, self.nx)
+        self._check(lib().pmpic_upload_grid(self._h, GRID[name], _dp(g)))
+
+    def spec(self, name) -> np.ndarray:
+        out = np.empty((self.nz + 1, self.ny + 2, self.nx + 2), np.float64)
+        self._check(lib().pmpic_download_spectral(self._h, SPEC[name], _dp(out)))
+        return out
+
+    def info(self) -> StepInfo:
+        s = StepInfo()
+        self._check(lib().pmpic_get_step_info(self._h, C.byref(s)))
+        return s
+
+    def counters(self):
+        a = (C.c_int32 * 5)()
+        self._check(lib().pmpic_get_counters(self._h, a))
+        return list(a)
+
+    def set_counters(self, v):
+        a = (C.c_int32 * 5)(*v)
+        self._check(lib().pmpic_set_counters(self._h, a))
+
+    def set_dtm(self, dtm):
+        self._check(lib().pmpic_set_dtm(self._h, float(dtm)))
+
+    # -- components -----------------------------------------------------------------
+    def vort2vel(self):
+        self._check(lib().pmpic_vort2vel(self._h))
+
+    def vorticity_tendency(self):
+        self._check(lib().pmpic_vorticity_tendency(self._h))
+
+    def rk4_integrator(self):
+        self._check(lib().pmpic_rk4_integrator(self._h))
+
+    def parcel_splitting(self):
+        self._check(lib().pmpic_parcel_splitting(self._h))
+
+    def parcel_mixing(self):
+        self._check(lib().pmpic_parcel_mixing(self._h))
+
+    def step(self, nsteps=1):
+        self._check(lib().pmpic_step(self._h, int(nsteps)))
+
+    # -- model-core routines --------------------------------------------------------
+    def cell_ids(self) -> np.ndarray:
+        out = np.empty(self.n, np.int32)
+        self._check(lib().pmpic_op_cell_ids(self._h, out.ctypes.data_as(C.POINTER(C.c_int32))))
+        return out
+
+    def par2grid(self, prop, grid):
+        self._check(lib().pmpic_op_par2grid(self._h, PROP[prop], GRID[grid]))
+
+    def grid2par(self, grid, prop):
+        self._check(lib().pmpic_op_grid2par(self._h, GRID[grid], PROP[prop]))
+
+    def parcel_haloswap(self):
+        self._check(lib().pmpic_op_parcel_haloswap(self._h))
+
+    def _sshape(self):
+        return (self.nz + 1, self.ny + 2, self.nx + 2)
+
+    def fft_forward(self, phys):
+        phys = np.ascontiguousarray(phys, np.float64)
+        out = np.empty(self._sshape())
+        self._check(lib().pmpic_op_fft_forward(self._h, _dp(phys), _dp(out)))
+        return out
+
+    def fft_backward(self, spec):
+        spec = np.ascontiguousarray(spec, np.float64)
+        out = np.empty((self.nz + 1, self.ny, self.nx))
+        self._check(lib().pmpic_op_fft_backward(self._h, _dp(spec), _dp(out)))
+        return out
+
+    def _unary(self, fn, a):
+        a = np.ascontiguousarray(a, np.float64)
+        out = np.empty_like(a)
+        self._check(fn(self._h, _dp(a), _dp(out)))
+        return out
+
+    def diffx(self, a):
+        return self._unary(lib().pmpic_op_diffx, a)
+
+    def diffy(self, a):
+        return self._unary(lib().pmpic_op_diffy, a)
+
+    def filter(self, a):
+        return self._unary(lib().pmpic_op_filter, a)
+
+    def diffz(self, a, bot=None, top=None):
+        a = np.ascontiguousarray(a, np.float64)
+        out = np.empty_like(a)
+        if bot is None:
+            self._check(lib().pmpic_op_diffz(self._h, _dp(a), _dp(out), None, None))
+        else:
+            bot = np.ascontiguousarray(bot, np.float64)
+            top = np.ascontiguousarray(top, np.float64)
+            self._check(lib().pmpic_op_diffz(self._h, _dp(a), _dp(out), _dp(bot), _dp(top)))
+        return out
+
+    def laplinv(self, a, df_zero_on_boundary: bool):
+        a = np.array(a, np.float64, copy=True, order="C")
+        self._check(lib().pmpic_op_laplinv(self._h, _dp(a), 1 if df_zero_on_boundary else 0))
+        return a

@@ -1,0 +1,181 @@
+// common.cuh -- shared definitions of the B200 PMPIC library (libpmpic_gpu.so).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/pmpic_gpu.h"
+
+#define PMPIC_CUDA(call)                                                     \
+  do {                                                                       \
+    cudaError_t e_ = (call);                                                 \
+    if (e_ != cudaSuccess) return pmpic::cuda_fail(ctx, e_, #call, __LINE__); \
+  } while (0)
+
+namespace pmpic {
+
+// Fortran single-precision literals promoted to double (fft_ops.F90:427-429,
+// :512-513, parcel_splitting.F90:71,79, vort2vel.F90:237-238).
+// f4div(1.f, 6.f) is the REAL(4) quotient 1./6. widened to REAL(8).
+__host__ __device__ constexpr double f4div(float a, float b) { return (double)(a / b); }
+__host__ __device__ constexpr double f4(float a) { return (double)a; }
+
+// Device error word values (sticky until read by pmpic_get_step_info).
+enum { DEV_OK = 0 };
+
+// Stockham FFT plan for one transform length (radix 4, 2, 3, 5 stages).
+constexpr int FFT_MAX_STAGES = 16;
+struct FftPlan {
+  int n;
+  int nst;
+  int radix[FFT_MAX_STAGES];
+  int tw_off[FFT_MAX_STAGES];  // offset (in double2) of each stage's twiddle table
+};
+
+// Geometry of one rank covering the whole domain (setup_grid.F90:45-104,
+// parcel_interpolation.F90:76-136, haloswap.F90:296-318, :531-552).
+struct Geom {
+  int Nx, Ny, Nz, nzp;          // cells, and Nz+1 z points
+  int sx, sy;                   // spectral extents Nx+2, Ny+2
+  int64_t ncell;                // Nx*Ny*Nz
+  int64_t nphys;                // (Nz+1)*Ny*Nx
+  int64_t nspec;                // (Nz+1)*(Ny+2)*(Nx+2)
+  double dx, dy, dz;
+  double pxmin, pymin, pzmin;   // first halo point coordinate (-2dx, -2dy, 0)
+  double pzmax;                 // Nz*dz (z reflection limit)
+  double hxmin, hxmax, hymin, hymax;  // x_coords(3), x_coords(Nx+3), y likewise
+  double xshift_e, xshift_w, yshift_n, yshift_s;
+  double xc0, yc0, zc0;         // x_coords(1), y_coords(1), z_coords(1)
+  double vmin;                  // dx*dy*dz/6/6/6 (parcel_mixing.F90:54)
+};
+
+// Interior cell id of a parcel and its fractional offsets, restating
+// cache_parcel_interp_weights (parcel_interpolation.F90:214-237) bit for bit:
+// i = floor((x-xmin)/dx)+1 and delx = ((x-xmin)-(i-1)dx)/dx with the halo
+// origin xmin = -2dx; the interior cell is i-3 (x), j-3 (y), k-1 (z).
+// Returns false for parcels outside the interior (the reference aborts, or for
+// the halo column i = Nx+3, loses the contribution).
+__device__ __forceinline__ bool bin_parcel(const Geom& g, double xp, double yp, double zp, int& ci, int& cj,
+                                           int& ck, double& delx, double& dely, double& delz) {
+  double fi = floor(__ddiv_rn(__dsub_rn(xp, g.pxmin), g.dx));
+  double fj = floor(__ddiv_rn(__dsub_rn(yp, g.pymin), g.dy));
+  double fk = floor(__ddiv_rn(__dsub_rn(zp, g.pzmin), g.dz));
+  if (!(fi >= 2.0 && fi < 2.0 + g.Nx && fj >= 2.0 && fj < 2.0 + g.Ny && fk >= 0.0 && fk < (double)g.Nz))
+    return false;
+  int i = (int)fi + 1, j = (int)fj + 1, k = (int)fk + 1;
+  delx = __ddiv_rn(__dsub_rn(__dsub_rn(xp, g.pxmin), __dmul_rn((double)(i - 1), g.dx)), g.dx);
+  dely = __ddiv_rn(__dsub_rn(__dsub_rn(yp, g.pymin), __dmul_rn((double)(j - 1), g.dy)), g.dy);
+  delz = __ddiv_rn(__dsub_rn(__dsub_rn(zp, g.pzmin), __dmul_rn((double)(k - 1), g.dz)), g.dz);
+  if (delx > 1.0 || delx < 0.0 || dely > 1.0 || dely < 0.0 || delz > 1.0 || delz < 0.0) return false;
+  ci = i - 3;
+  cj = j - 3;
+  ck = k - 1;
+  return true;
+}
+
+// Device-side step counters and error word.
+struct DevInfo {
+  int error;
+  int pad;
+  long long n_parcels;     // current numparcels (device copy)
+  long long n_split;
+  long long n_removed;
+  long long n_added;
+  long long n_migrated;
+  long long n_zero;        // mixing: number of keep==0 slots
+  long long n_kept;        // mixing: number of keep==1 slots
+  double dtm;
+  double umax2, vmax2, wmax2, omax2;  // squared maxima (order-free reductions)
+  int limiter;
+  int pad2;
+};
+
+}  // namespace pmpic
+
+// ---------------------------------------------------------------------------
+// Context (host struct; device pointers inside)
+// ---------------------------------------------------------------------------
+struct pmpic_ctx {
+  pmpic_config cfg;
+  pmpic::Geom g;
+  int device;
+  cudaStream_t stream;
+  std::string err;
+  // parcels: NPROP arrays of capacity cap
+  int64_t cap;
+  int64_t n;                 // numparcels (host mirror, valid between calls)
+  double* parcels;           // NPROP * cap
+  int32_t* cell;             // cap: interior cell id per slot
+  bool sorted_valid;         // cell lists match the current positions
+  int32_t* sorted;           // cap: slot indices sorted by cell
+  int32_t* cell_count;       // ncell + 1
+  int32_t* cell_start;       // ncell + 1
+  int32_t* cell_fill;        // ncell
+  int32_t* keep;             // cap (mixing)
+  int32_t* aux;              // cap (scans / migration lists)
+  int32_t* aux2;             // 2*nbmax + cap (compaction block counts, offsets, lists)
+  int64_t nbmax;             // max compaction blocks: ceil(max(cap, ncell)/1024) + 8
+  int8_t* dir;               // cap (haloswap direction)
+  double* swapbuf;           // staging for migrating parcels (29 doubles each)
+  int64_t swapcap;
+  void* scan_tmp;            // block sums for scans
+  // physical grids (dense (Nz+1) x Ny x Nx)
+  double* grid[PMPIC_NGRID];
+  double* gwork[5];          // dudx, dwdx, dvdy, dwdy, ap
+  double* mixres[6];         // residual grids vres..rres
+  int32_t* npercell;         // ncell
+  int32_t* newslot;          // ncell: slot of the new parcel of a cell or -1
+  double* newportion;        // ncell: portion of the new parcel of a cell
+  // spectral arrays
+  double* spec[PMPIC_NSPEC]; // u_s, v_s, w_s
+  double* sa, *sb, *sc, *sd, *se, *sf, *sas, *sbs, *sscratch;
+  double* fftmid;            // (Nz+1) x (Ny+2) x Nx
+  double* ftw;               // twiddle tables (x plan first, then y plan)
+  int ftw_off_x, ftw_off_y;
+  pmpic::FftPlan plan_x, plan_y;
+  // small per-column data
+  double* kx, *ky, *k2, *filt;  // (Ny+2) x (Nx+2)
+  double* bt;                // atop, abot, btop, bbot: 4 x (Ny+2)(Nx+2)
+  double* zmode;             // ubar, vbar: 2 x (Nz+1)
+  // info
+  pmpic::DevInfo* dinfo;     // device
+  pmpic::DevInfo* hinfo;     // pinned host
+  int counters[5];           // it_v2v, it_vt, rkstep, it_split, it_mix
+  double dtm;
+  pmpic_step_info info;
+};
+
+namespace pmpic {
+int cuda_fail(pmpic_ctx* ctx, cudaError_t e, const char* what, int line);
+int set_error(pmpic_ctx* ctx, int code, const std::string& msg);
+inline double* prop(pmpic_ctx* ctx, int p) { return ctx->parcels + (size_t)p * (size_t)ctx->cap; }
+
+// kernels / launchers (interp.cu)
+int bin_and_sort(pmpic_ctx* ctx);
+int par2grid_multi(pmpic_ctx* ctx, const double* const* fields, int nf, double* const* out, bool btot_from_bhz);
+int grid2par_multi(pmpic_ctx* ctx, const double* const* grids, int ng, double* const* out);
+int cell_ids(pmpic_ctx* ctx, int32_t* dcells);
+// fft.cu
+int fft_init(pmpic_ctx* ctx);
+int fft_forward(pmpic_ctx* ctx, const double* phys, double* spec);
+int fft_backward(pmpic_ctx* ctx, const double* spec, double* phys);
+// spectral.cu
+int spec_diffx(pmpic_ctx* ctx, const double* in, double* out);
+int spec_diffy(pmpic_ctx* ctx, const double* in, double* out);
+int spec_filter(pmpic_ctx* ctx, const double* in, double* out);
+int spec_diffz(pmpic_ctx* ctx, const double* in, double* out, const double* bot, const double* top);
+int spec_laplinv(pmpic_ctx* ctx, double* inout, bool df0);
+int vort2vel_spectral(pmpic_ctx* ctx);
+int vorticity_tendency_grids(pmpic_ctx* ctx);
+int field_max(pmpic_ctx* ctx, bool first_substep_v2v, bool first_substep_vt);
+// parcels.cu
+int rk4_stage(pmpic_ctx* ctx, int stage);
+int parcel_haloswap(pmpic_ctx* ctx);
+int splitting(pmpic_ctx* ctx);
+int mixing(pmpic_ctx* ctx);
+int compute_btot(pmpic_ctx* ctx);
+int sync_info(pmpic_ctx* ctx);
+}  // namespace pmpic

@@ -1,0 +1,590 @@
+// ctx.cu -- the C ABI of libpmpic_gpu.so (include/pmpic_gpu.h): context
+// set-up, transfers, and the five component timestep callbacks of the
+// reference's integrator group.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+
+namespace pmpic {
+
+int spectral_init(pmpic_ctx* ctx);
+int scan_excl(pmpic_ctx* ctx, const int32_t* in, int64_t n, int32_t* out);
+
+int cuda_fail(pmpic_ctx* ctx, cudaError_t e, const char* what, int line) {
+  char buf[256];
+  std::snprintf(buf, sizeof(buf), "CUDA error %s at ctx.cu/%d: %s", cudaGetErrorString(e), line, what);
+  if (ctx) ctx->err = buf;
+  return PMPIC_ERR_CUDA;
+}
+
+int set_error(pmpic_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+static const char* err_text(int code) {
+  switch (code) {
+    case PMPIC_ERR_CAPACITY: return "maximum parcel count reached";
+    case PMPIC_ERR_OUT_OF_BOX: return "parcel out of box";
+    case PMPIC_ERR_ZERO_PIVOT: return "zero pivot in tridiagonal solver";
+    case PMPIC_ERR_BACKFILL: return "mixing backfill ran out of kept parcels";
+    case PMPIC_ERR_TIMEOUT: return "device wait timed out";
+    default: return "device error";
+  }
+}
+
+// Copy the device info block to the host; report a sticky device error.
+int sync_info(pmpic_ctx* ctx) {
+  PMPIC_CUDA(cudaMemcpyAsync(ctx->hinfo, ctx->dinfo, sizeof(DevInfo), cudaMemcpyDeviceToHost, ctx->stream));
+  PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
+  const DevInfo& h = *ctx->hinfo;
+  ctx->dtm = h.dtm;
+  ctx->info.dtm = h.dtm;
+  ctx->info.limiter = h.limiter;
+  ctx->info.n_migrated = h.n_migrated;
+  ctx->info.n_parcels = ctx->n;
+  if (h.error != 0) {
+    ctx->info.error = h.error;
+    return set_error(ctx, h.error, err_text(h.error));
+  }
+  return 0;
+}
+
+}  // namespace pmpic
+
+using namespace pmpic;
+
+namespace {
+
+template <class T>
+int dalloc(pmpic_ctx* ctx, T** p, size_t count) {
+  cudaError_t e = cudaMalloc((void**)p, sizeof(T) * std::max<size_t>(count, 1));
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc", __LINE__);
+  return 0;
+}
+
+void free_all(pmpic_ctx* c) {
+  void* ptrs[] = {c->parcels, c->cell,     c->sorted,    c->cell_count, c->cell_start, c->cell_fill, c->keep,
+                  c->aux,     c->aux2,     c->dir,       c->swapbuf,    c->scan_tmp,   c->npercell,  c->newslot,
+                  c->newportion, c->sa,    c->sb,        c->sc,         c->sd,         c->se,        c->sf,
+                  c->sas,     c->sbs,      c->sscratch,  c->fftmid,     c->ftw,        c->kx,        c->ky,
+                  c->k2,      c->filt,     c->bt,        c->zmode,      c->dinfo};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  for (int i = 0; i < PMPIC_NGRID; ++i)
+    if (c->grid[i]) cudaFree(c->grid[i]);
+  for (int i = 0; i < 5; ++i)
+    if (c->gwork[i]) cudaFree(c->gwork[i]);
+  for (int i = 0; i < 6; ++i)
+    if (c->mixres[i]) cudaFree(c->mixres[i]);
+  for (int i = 0; i < PMPIC_NSPEC; ++i)
+    if (c->spec[i]) cudaFree(c->spec[i]);
+  if (c->hinfo) cudaFreeHost(c->hinfo);
+  if (c->stream) cudaStreamDestroy(c->stream);
+}
+
+bool smooth235(int n) {
+  if (n <= 0) return false;
+  while (n % 2 == 0) n /= 2;
+  while (n % 3 == 0) n /= 3;
+  while (n % 5 == 0) n /= 5;
+  return n == 1;
+}
+
+// wavenumbers and filter (fft_ops.F90:111-140) with the reference's arithmetic
+void wavenumbers(const pmpic_config& cfg, const Geom& g, std::vector<double>& kx, std::vector<double>& ky,
+                 std::vector<double>& k2, std::vector<double>& filt) {
+  const int sx = g.sx, sy = g.sy;
+  double lx = g.dx * (double)g.Nx, ly = g.dy * (double)g.Ny;
+  const double kxm = (double)((float)g.Nx / 2.0f) / lx, kym = (double)((float)g.Ny / 2.0f) / ly;
+  double ksqmax = kxm * kxm + kym * kym;
+  ksqmax = ksqmax * 2.0 / 9.0;
+  const double twopi = 8.0 * std::atan(1.0);
+  kx.resize((size_t)sx * sy); ky.resize(kx.size()); k2.resize(kx.size()); filt.resize(kx.size());
+  for (int jp = 0; jp < sy; ++jp)
+    for (int ip = 0; ip < sx; ++ip) {
+      double xval = (double)(ip / 2) / lx;
+      double yval = (double)(jp / 2) / ly;
+      size_t o = (size_t)jp * sx + ip;
+      double kk = xval * xval + yval * yval;
+      filt[o] = (kk > ksqmax) ? 0.0 : 1.0;
+      kx[o] = xval * twopi;
+      ky[o] = yval * twopi;
+      k2[o] = kk * twopi * twopi;
+    }
+  (void)cfg;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
+  if (!cfg || !out) return PMPIC_ERR_ARG;
+  *out = nullptr;
+  if (cfg->nx < 4 || cfg->ny < 4 || cfg->nz < 3 || (cfg->nx & 1) || (cfg->ny & 1) || !smooth235(cfg->nx) ||
+      !smooth235(cfg->ny) || cfg->max_parcels <= 0 || cfg->max_parcels >= (int64_t)0x7fffffff ||
+      cfg->precision != PMPIC_FP64)
+    return PMPIC_ERR_CONFIG;
+  if (cfg->xmin != 0.0 || cfg->ymin != 0.0 || cfg->zmin != 0.0 || !(cfg->xmax > 0) || !(cfg->ymax > 0) ||
+      !(cfg->zmax > 0))
+    return PMPIC_ERR_CONFIG;
+  pmpic_ctx* ctx = new pmpic_ctx();
+  std::memset((void*)&ctx->g, 0, sizeof(ctx->g));
+  ctx->cfg = *cfg;
+  ctx->device = cfg->device;
+  ctx->parcels = nullptr;
+  cudaError_t e = cudaSetDevice(cfg->device);
+  if (e != cudaSuccess) {
+    delete ctx;
+    return PMPIC_ERR_CUDA;
+  }
+  // geometry (setup_grid.F90:73-95; parcel_interpolation.F90:104-136)
+  Geom& g = ctx->g;
+  g.Nx = cfg->nx; g.Ny = cfg->ny; g.Nz = cfg->nz; g.nzp = cfg->nz + 1;
+  g.sx = g.Nx + 2; g.sy = g.Ny + 2;
+  g.ncell = (int64_t)g.Nx * g.Ny * g.Nz;
+  g.nphys = (int64_t)g.nzp * g.Ny * g.Nx;
+  g.nspec = (int64_t)g.nzp * g.sy * g.sx;
+  g.dx = (cfg->xmax - cfg->xmin) / (double)g.Nx;
+  g.dy = (cfg->ymax - cfg->ymin) / (double)g.Ny;
+  g.dz = (cfg->zmax - cfg->zmin) / (double)(g.nzp - 1);
+  g.pxmin = (double)(-2) * g.dx + cfg->xmin;
+  g.pymin = (double)(-2) * g.dy + cfg->ymin;
+  g.pzmin = 0.0 * g.dz + cfg->zmin;
+  g.pzmax = (double)(g.nzp - 1) * g.dz;
+  g.xc0 = g.pxmin; g.yc0 = g.pymin; g.zc0 = g.pzmin;
+  g.hxmin = g.pxmin + 2.0 * g.dx;                   // x_coords(hx+1)
+  g.hxmax = g.pxmin + (double)(g.Nx + 2) * g.dx;    // x_coords(nx-hx+1)
+  g.hymin = g.pymin + 2.0 * g.dy;
+  g.hymax = g.pymin + (double)(g.Ny + 2) * g.dy;
+  const double topx = cfg->xmax - g.dx, topy = cfg->ymax - g.dy;  // setup_grid.F90:92-93
+  g.xshift_e = cfg->xmin - topx - g.dx;             // haloswap.F90:531-535
+  g.xshift_w = topx - cfg->xmin + g.dx;             // :536-540
+  g.yshift_n = cfg->ymin - topy - g.dy;             // :542-546
+  g.yshift_s = topy - cfg->ymin + g.dy;             // :547-551
+  g.vmin = g.dx * g.dy * g.dz / 6. / 6. / 6.;       // parcel_mixing.F90:54
+  ctx->cap = cfg->max_parcels;
+  ctx->n = 0;
+  ctx->sorted_valid = false;
+  ctx->nbmax = (std::max<int64_t>(ctx->cap, g.ncell) + 1023) / 1024 + 8;
+  int64_t sc = 2LL * (g.Nx + g.Ny) * (int64_t)g.nzp * 32;
+  ctx->swapcap = std::min<int64_t>(ctx->cap, std::max<int64_t>(1 << 20, sc));
+  int rc = 0;
+  e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) rc = cuda_fail(ctx, e, "stream", __LINE__);
+  const size_t cap = (size_t)ctx->cap;
+  if (!rc) rc = dalloc(ctx, &ctx->parcels, (size_t)PMPIC_NPROP * cap);
+  if (!rc) rc = dalloc(ctx, &ctx->cell, cap);
+  if (!rc) rc = dalloc(ctx, &ctx->sorted, cap);
+  if (!rc) rc = dalloc(ctx, &ctx->keep, cap);
+  if (!rc) rc = dalloc(ctx, &ctx->aux, cap);
+  if (!rc) rc = dalloc(ctx, &ctx->aux2, 2 * (size_t)ctx->nbmax + cap);
+  if (!rc) rc = dalloc(ctx, &ctx->dir, cap);
+  if (!rc) rc = dalloc(ctx, &ctx->cell_count, (size_t)g.ncell + 1);
+  if (!rc) rc = dalloc(ctx, &ctx->cell_start, (size_t)g.ncell + 1);
+  if (!rc) rc = dalloc(ctx, &ctx->cell_fill, (size_t)g.ncell);
+  if (!rc) rc = dalloc(ctx, &ctx->swapbuf, (size_t)ctx->swapcap * 29);
+  if (!rc) rc = dalloc(ctx, (int32_t**)&ctx->scan_tmp, (size_t)(std::max<int64_t>(std::max<int64_t>(g.ncell, ctx->cap), ctx->nbmax) / 4096 + 64));
+  for (int i = 0; i < PMPIC_NGRID && !rc; ++i) rc = dalloc(ctx, &ctx->grid[i], (size_t)g.nphys);
+  for (int i = 0; i < 5 && !rc; ++i) rc = dalloc(ctx, &ctx->gwork[i], (size_t)g.nphys);
+  for (int i = 0; i < 6 && !rc; ++i) rc = dalloc(ctx, &ctx->mixres[i], (size_t)g.nphys);
+  if (!rc) rc = dalloc(ctx, &ctx->npercell, (size_t)g.ncell);
+  if (!rc) rc = dalloc(ctx, &ctx->newslot, (size_t)g.ncell);
+  if (!rc) rc = dalloc(ctx, &ctx->newportion, (size_t)g.ncell);
+  for (int i = 0; i < PMPIC_NSPEC && !rc; ++i) rc = dalloc(ctx, &ctx->spec[i], (size_t)g.nspec);
+  double** sp[] = {&ctx->sa, &ctx->sb, &ctx->sc, &ctx->sd, &ctx->se, &ctx->sf, &ctx->sas, &ctx->sbs};
+  for (double** p : sp)
+    if (!rc) rc = dalloc(ctx, p, (size_t)g.nspec);
+  if (!rc) rc = dalloc(ctx, &ctx->sscratch, (size_t)g.nspec + 6 * (size_t)g.nzp);
+  if (!rc) rc = dalloc(ctx, &ctx->fftmid, (size_t)g.nzp * g.sy * g.Nx);
+  const size_t cols = (size_t)g.sx * g.sy;
+  if (!rc) rc = dalloc(ctx, &ctx->kx, cols);
+  if (!rc) rc = dalloc(ctx, &ctx->ky, cols);
+  if (!rc) rc = dalloc(ctx, &ctx->k2, cols);
+  if (!rc) rc = dalloc(ctx, &ctx->filt, cols);
+  if (!rc) rc = dalloc(ctx, &ctx->bt, 4 * cols);
+  if (!rc) rc = dalloc(ctx, &ctx->zmode, 2 * (size_t)g.nzp);
+  if (!rc) rc = dalloc(ctx, (char**)&ctx->dinfo, sizeof(DevInfo) + 64 * sizeof(int32_t));
+  if (!rc) {
+    e = cudaMallocHost((void**)&ctx->hinfo, sizeof(DevInfo));
+    if (e != cudaSuccess) rc = cuda_fail(ctx, e, "cudaMallocHost", __LINE__);
+  }
+  if (!rc) {
+    // zero-initialised state: every slot of every property starts at 0
+    e = cudaMemset(ctx->parcels, 0, sizeof(double) * (size_t)PMPIC_NPROP * cap);
+    if (e == cudaSuccess) e = cudaMemset(ctx->dinfo, 0, sizeof(DevInfo) + 64 * sizeof(int32_t));
+    for (int i = 0; i < PMPIC_NGRID && e == cudaSuccess; ++i) e = cudaMemset(ctx->grid[i], 0, sizeof(double) * g.nphys);
+    for (int i = 0; i < PMPIC_NSPEC && e == cudaSuccess; ++i) e = cudaMemset(ctx->spec[i], 0, sizeof(double) * g.nspec);
+    if (e != cudaSuccess) rc = cuda_fail(ctx, e, "cudaMemset", __LINE__);
+  }
+  if (!rc) {
+    std::vector<double> kx, ky, k2, filt;
+    wavenumbers(*cfg, g, kx, ky, k2, filt);
+    cudaMemcpy(ctx->kx, kx.data(), sizeof(double) * cols, cudaMemcpyHostToDevice);
+    cudaMemcpy(ctx->ky, ky.data(), sizeof(double) * cols, cudaMemcpyHostToDevice);
+    cudaMemcpy(ctx->k2, k2.data(), sizeof(double) * cols, cudaMemcpyHostToDevice);
+    e = cudaMemcpy(ctx->filt, filt.data(), sizeof(double) * cols, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) rc = cuda_fail(ctx, e, "wavenumbers", __LINE__);
+  }
+  if (!rc) rc = fft_init(ctx);
+  if (!rc) rc = spectral_init(ctx);
+  if (!rc) {
+    DevInfo h{};
+    h.dtm = cfg->dtm;  // rk4_integrator.F90:38-41
+    e = cudaMemcpy(ctx->dinfo, &h, sizeof(DevInfo), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) rc = cuda_fail(ctx, e, "dinfo", __LINE__);
+  }
+  ctx->dtm = cfg->dtm;
+  ctx->counters[0] = 0; ctx->counters[1] = 0; ctx->counters[2] = 1; ctx->counters[3] = 0; ctx->counters[4] = 0;
+  std::memset(&ctx->info, 0, sizeof(ctx->info));
+  ctx->info.dtm = cfg->dtm;
+  if (rc) {
+    free_all(ctx);
+    delete ctx;
+    return rc;
+  }
+  *out = ctx;
+  return PMPIC_OK;
+}
+
+void pmpic_destroy(pmpic_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  free_all(ctx);
+  delete ctx;
+}
+
+const char* pmpic_last_error(const pmpic_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int pmpic_set_count(pmpic_ctx* ctx, int64_t n) {
+  if (!ctx) return PMPIC_ERR_ARG;
+  if (n < 0 || n > ctx->cap) return set_error(ctx, PMPIC_ERR_CAPACITY, "parcel count exceeds max_parcels");
+  ctx->n = n;
+  ctx->info.n_parcels = n;
+  ctx->sorted_valid = false;
+  return PMPIC_OK;
+}
+int pmpic_get_count(pmpic_ctx* ctx, int64_t* n) {
+  if (!ctx || !n) return PMPIC_ERR_ARG;
+  *n = ctx->n;
+  return PMPIC_OK;
+}
+
+int pmpic_set_property(pmpic_ctx* ctx, int p, int64_t n, const double* src) {
+  if (!ctx || p < 0 || p >= PMPIC_NPROP || n < 0 || n > ctx->cap || (!src && n > 0)) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  PMPIC_CUDA(cudaMemcpyAsync(prop(ctx, p), src, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+  PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->sorted_valid = false;
+  return PMPIC_OK;
+}
+int pmpic_get_property(pmpic_ctx* ctx, int p, int64_t n, double* dst) {
+  if (!ctx || p < 0 || p >= PMPIC_NPROP || n < 0 || n > ctx->cap || (!dst && n > 0)) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  PMPIC_CUDA(cudaMemcpyAsync(dst, prop(ctx, p), sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
+  return PMPIC_OK;
+}
+
+static const int kIO[11] = {PMPIC_PROP_X, PMPIC_PROP_Y, PMPIC_PROP_Z, PMPIC_PROP_P,       PMPIC_PROP_Q,  PMPIC_PROP_R,
+                            PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_VOL, PMPIC_PROP_STRETCH, PMPIC_PROP_TAG};
+
+int pmpic_upload_parcels(pmpic_ctx* ctx, int64_t n, const double* x, const double* y, const double* z,
+                         const double* p, const double* q, const double* r, const double* b, const double* h,
+                         const double* vol, const double* stretch, const double* tag) {
+  if (!ctx) return PMPIC_ERR_ARG;
+  if (n < 0 || n > ctx->cap) return set_error(ctx, PMPIC_ERR_CAPACITY, "parcel count exceeds max_parcels");
+  const double* src[11] = {x, y, z, p, q, r, b, h, vol, stretch, tag};
+  cudaSetDevice(ctx->device);
+  for (int i = 0; i < 11; ++i) {
+    if (src[i])
+      PMPIC_CUDA(cudaMemcpyAsync(prop(ctx, kIO[i]), src[i], sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    else
+      PMPIC_CUDA(cudaMemsetAsync(prop(ctx, kIO[i]), 0, sizeof(double) * n, ctx->stream));
+  }
+  const int zero[] = {PMPIC_PROP_DXDT, PMPIC_PROP_DYDT, PMPIC_PROP_DZDT, PMPIC_PROP_DPDT, PMPIC_PROP_DQDT,
+                      PMPIC_PROP_DRDT, PMPIC_PROP_BTOT, PMPIC_PROP_XO,   PMPIC_PROP_YO,   PMPIC_PROP_ZO,
+                      PMPIC_PROP_XF,   PMPIC_PROP_YF,   PMPIC_PROP_ZF,   PMPIC_PROP_PO,   PMPIC_PROP_QO,
+                      PMPIC_PROP_RO,   PMPIC_PROP_PF,   PMPIC_PROP_QF,   PMPIC_PROP_RF};
+  for (int pid : zero) PMPIC_CUDA(cudaMemsetAsync(prop(ctx, pid), 0, sizeof(double) * n, ctx->stream));
+  PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->n = n;
+  ctx->info.n_parcels = n;
+  ctx->sorted_valid = false;
+  return PMPIC_OK;
+}
+
+int pmpic_download_parcels(pmpic_ctx* ctx, int64_t capacity, int64_t* n, double* x, double* y, double* z, double* p,
+                           double* q, double* r, double* b, double* h, double* vol, double* stretch, double* tag) {
+  if (!ctx) return PMPIC_ERR_ARG;
+  if (n) *n = ctx->n;
+  if (capacity < ctx->n) return set_error(ctx, PMPIC_ERR_ARG, "download capacity below parcel count");
+  double* dst[11] = {x, y, z, p, q, r, b, h, vol, stretch, tag};
+  cudaSetDevice(ctx->device);
+  for (int i = 0; i < 11; ++i)
+    if (dst[i])
+      PMPIC_CUDA(cudaMemcpyAsync(dst[i], prop(ctx, kIO[i]), sizeof(double) * ctx->n, cudaMemcpyDeviceToHost, ctx->stream));
+  PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
+  return PMPIC_OK;
+}
+
+int pmpic_download_grid(pmpic_ctx* ctx, int grid, double* dst) {
+  if (!ctx || grid < 0 || grid >= PMPIC_NGRID || !dst) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  PMPIC_CUDA(cudaMemcpyAsync(dst, ctx->grid[grid], sizeof(double) * ctx->g.nphys, cudaMemcpyDeviceToHost, ctx->stream));
+  PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
+  return PMPIC_OK;
+}
+int pmpic_upload_grid(pmpic_ctx* ctx, int grid, const double* src) {
+  if (!ctx || grid < 0 || grid >= PMPIC_NGRID || !src) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  PMPIC_CUDA(cudaMemcpyAsync(ctx->grid[grid], src, sizeof(double) * ctx->g.nphys, cudaMemcpyHostToDevice, ctx->stream));
+  PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
+  return PMPIC_OK;
+}
+int pmpic_download_spectral(pmpic_ctx* ctx, int spec, double* dst) {
+  if (!ctx || spec < 0 || spec >= PMPIC_NSPEC || !dst) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  PMPIC_CUDA(cudaMemcpyAsync(dst, ctx->spec[spec], sizeof(double) * ctx->g.nspec, cudaMemcpyDeviceToHost, ctx->stream));
+  PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
+  return PMPIC_OK;
+}
+
+int pmpic_get_counters(pmpic_ctx* ctx, int32_t c[5]) {
+  if (!ctx || !c) return PMPIC_ERR_ARG;
+  for (int i = 0; i < 5; ++i) c[i] = ctx->counters[i];
+  return PMPIC_OK;
+}
+int pmpic_set_counters(pmpic_ctx* ctx, const int32_t c[5]) {
+  if (!ctx || !c || c[2] < 1 || c[2] > 4) return PMPIC_ERR_ARG;
+  for (int i = 0; i < 5; ++i) ctx->counters[i] = c[i];
+  return PMPIC_OK;
+}
+int pmpic_set_dtm(pmpic_ctx* ctx, double dtm) {
+  if (!ctx) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  PMPIC_CUDA(cudaMemcpyAsync(&ctx->dinfo->dtm, &dtm, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->dtm = dtm;
+  ctx->info.dtm = dtm;
+  return PMPIC_OK;
+}
+
+int pmpic_get_step_info(pmpic_ctx* ctx, pmpic_step_info* info) {
+  if (!ctx || !info) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  int rc = sync_info(ctx);
+  *info = ctx->info;
+  info->n_parcels = ctx->n;
+  info->error = rc ? rc : 0;
+  std::snprintf(info->message, sizeof(info->message), "%s", ctx->err.c_str());
+  return rc;
+}
+
+// ---- component callbacks --------------------------------------------------------
+// Internal forms without the trailing error check; the public entry points
+// check the sticky device error word once per call.
+
+static int do_vort2vel(pmpic_ctx* ctx) {
+  int rc;
+  // vort2vel.F90:117-121: binning and par2grid of p, q, r with one set of weights
+  if ((rc = bin_and_sort(ctx))) return rc;
+  const double* f[3] = {prop(ctx, PMPIC_PROP_P), prop(ctx, PMPIC_PROP_Q), prop(ctx, PMPIC_PROP_R)};
+  double* o[3] = {ctx->grid[PMPIC_GRID_P], ctx->grid[PMPIC_GRID_Q], ctx->grid[PMPIC_GRID_R]};
+  if ((rc = par2grid_multi(ctx, f, 3, o, false))) return rc;
+  if ((rc = vort2vel_spectral(ctx))) return rc;
+  // :325-327
+  const double* gr[3] = {ctx->grid[PMPIC_GRID_U], ctx->grid[PMPIC_GRID_V], ctx->grid[PMPIC_GRID_W]};
+  double* out[3] = {prop(ctx, PMPIC_PROP_DXDT), prop(ctx, PMPIC_PROP_DYDT), prop(ctx, PMPIC_PROP_DZDT)};
+  if ((rc = grid2par_multi(ctx, gr, 3, out))) return rc;
+  if (ctx->counters[0] % 4 == 0)
+    if ((rc = field_max(ctx, true, false))) return rc;  // :329-372
+  ctx->counters[0]++;
+  return 0;
+}
+
+static int do_vorticity_tendency(pmpic_ctx* ctx) {
+  int rc;
+  if ((rc = compute_btot(ctx))) return rc;  // :121-126
+  // par2grid(btot) (:129) with the cell lists of this substep (positions
+  // are unchanged since vort2vel binned them)
+  if (!ctx->sorted_valid)
+    if ((rc = bin_and_sort(ctx))) return rc;
+  const double* f[1] = {prop(ctx, PMPIC_PROP_BTOT)};
+  double* o[1] = {ctx->grid[PMPIC_GRID_B]};
+  if ((rc = par2grid_multi(ctx, f, 1, o, false))) return rc;
+  if ((rc = vorticity_tendency_grids(ctx))) return rc;
+  const double* gr[3] = {ctx->grid[PMPIC_GRID_DP], ctx->grid[PMPIC_GRID_DQ], ctx->grid[PMPIC_GRID_DR]};
+  double* out[3] = {prop(ctx, PMPIC_PROP_DPDT), prop(ctx, PMPIC_PROP_DQDT), prop(ctx, PMPIC_PROP_DRDT)};
+  if ((rc = grid2par_multi(ctx, gr, 3, out))) return rc;  // :273-275
+  if (ctx->counters[1] % 4 == 0)
+    if ((rc = field_max(ctx, false, true))) return rc;  // :277-313
+  ctx->counters[1]++;
+  return 0;
+}
+
+static int do_rk4(pmpic_ctx* ctx) {
+  int rc;
+  if ((rc = rk4_stage(ctx, ctx->counters[2]))) return rc;
+  ctx->counters[2] = ctx->counters[2] < 4 ? ctx->counters[2] + 1 : 1;  // rk4_integrator.F90:311-315
+  return parcel_haloswap(ctx);                                          // :317
+}
+
+static int do_split(pmpic_ctx* ctx) {
+  int rc = 0;
+  if (ctx->counters[3] % 4 == 3) rc = splitting(ctx);  // parcel_splitting.F90:59
+  ctx->counters[3]++;
+  return rc;
+}
+
+static int do_mix(pmpic_ctx* ctx) {
+  int rc = 0;
+  if (ctx->counters[4] % 4 == 3) rc = mixing(ctx);  // parcel_mixing.F90:77
+  ctx->counters[4]++;
+  return rc;
+}
+
+#define PMPIC_ENTRY(body)                 \
+  if (!ctx) return PMPIC_ERR_ARG;         \
+  cudaSetDevice(ctx->device);             \
+  int rc_ = (body);                       \
+  if (rc_) return rc_;                    \
+  return sync_info(ctx);
+
+int pmpic_vort2vel(pmpic_ctx* ctx) { PMPIC_ENTRY(do_vort2vel(ctx)) }
+int pmpic_vorticity_tendency(pmpic_ctx* ctx) { PMPIC_ENTRY(do_vorticity_tendency(ctx)) }
+int pmpic_rk4_integrator(pmpic_ctx* ctx) { PMPIC_ENTRY(do_rk4(ctx)) }
+int pmpic_parcel_splitting(pmpic_ctx* ctx) { PMPIC_ENTRY(do_split(ctx)) }
+int pmpic_parcel_mixing(pmpic_ctx* ctx) { PMPIC_ENTRY(do_mix(ctx)) }
+
+int pmpic_step(pmpic_ctx* ctx, int nsteps) {
+  if (!ctx || nsteps < 0) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  for (int s = 0; s < nsteps; ++s) {
+    for (int sub = 0; sub < 4; ++sub) {
+      int rc;
+      if ((rc = do_vort2vel(ctx))) return rc;
+      if ((rc = do_vorticity_tendency(ctx))) return rc;
+      if ((rc = do_rk4(ctx))) return rc;
+      if ((rc = do_split(ctx))) return rc;
+      if ((rc = do_mix(ctx))) return rc;
+    }
+    int rc = sync_info(ctx);
+    if (rc) return rc;
+  }
+  return PMPIC_OK;
+}
+
+// ---- kernel-level entry points ----------------------------------------------------
+int pmpic_op_cell_ids(pmpic_ctx* ctx, int32_t* cells) {
+  if (!ctx || !cells) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  int rc = cell_ids(ctx, ctx->cell);
+  if (rc) return rc;
+  PMPIC_CUDA(cudaMemcpyAsync(cells, ctx->cell, sizeof(int32_t) * ctx->n, cudaMemcpyDeviceToHost, ctx->stream));
+  return sync_info(ctx);
+}
+
+int pmpic_op_par2grid(pmpic_ctx* ctx, int p, int grid) {
+  if (!ctx || p < 0 || p >= PMPIC_NPROP || grid < 0 || grid >= PMPIC_NGRID) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  int rc = bin_and_sort(ctx);
+  if (rc) return rc;
+  const double* f[1] = {prop(ctx, p)};
+  double* o[1] = {ctx->grid[grid]};
+  if ((rc = par2grid_multi(ctx, f, 1, o, false))) return rc;
+  return sync_info(ctx);
+}
+
+int pmpic_op_grid2par(pmpic_ctx* ctx, int grid, int p) {
+  if (!ctx || p < 0 || p >= PMPIC_NPROP || grid < 0 || grid >= PMPIC_NGRID) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  const double* gr[1] = {ctx->grid[grid]};
+  double* out[1] = {prop(ctx, p)};
+  int rc = grid2par_multi(ctx, gr, 1, out);
+  if (rc) return rc;
+  return sync_info(ctx);
+}
+
+// host <-> device helpers for the spectral test entry points
+static int h2d(pmpic_ctx* ctx, double* d, const double* h, size_t n) {
+  PMPIC_CUDA(cudaMemcpyAsync(d, h, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+  return 0;
+}
+static int d2h(pmpic_ctx* ctx, double* h, const double* d, size_t n) {
+  PMPIC_CUDA(cudaMemcpyAsync(h, d, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int pmpic_op_fft_forward(pmpic_ctx* ctx, const double* phys, double* spec) {
+  if (!ctx || !phys || !spec) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  int rc;
+  if ((rc = h2d(ctx, ctx->gwork[0], phys, ctx->g.nphys))) return rc;
+  if ((rc = fft_forward(ctx, ctx->gwork[0], ctx->sa))) return rc;
+  return d2h(ctx, spec, ctx->sa, ctx->g.nspec);
+}
+int pmpic_op_fft_backward(pmpic_ctx* ctx, const double* spec, double* phys) {
+  if (!ctx || !phys || !spec) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  int rc;
+  if ((rc = h2d(ctx, ctx->sa, spec, ctx->g.nspec))) return rc;
+  if ((rc = fft_backward(ctx, ctx->sa, ctx->gwork[0]))) return rc;
+  return d2h(ctx, phys, ctx->gwork[0], ctx->g.nphys);
+}
+
+typedef int (*spec_op)(pmpic_ctx*, const double*, double*);
+static int spec_unary(pmpic_ctx* ctx, const double* in, double* out, spec_op op) {
+  if (!ctx || !in || !out) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  int rc;
+  if ((rc = h2d(ctx, ctx->sa, in, ctx->g.nspec))) return rc;
+  if ((rc = op(ctx, ctx->sa, ctx->sb))) return rc;
+  return d2h(ctx, out, ctx->sb, ctx->g.nspec);
+}
+int pmpic_op_diffx(pmpic_ctx* ctx, const double* in, double* out) { return spec_unary(ctx, in, out, spec_diffx); }
+int pmpic_op_diffy(pmpic_ctx* ctx, const double* in, double* out) { return spec_unary(ctx, in, out, spec_diffy); }
+int pmpic_op_filter(pmpic_ctx* ctx, const double* in, double* out) { return spec_unary(ctx, in, out, spec_filter); }
+int pmpic_op_diffz(pmpic_ctx* ctx, const double* in, double* out, const double* bot, const double* top) {
+  if (!ctx || !in || !out || ((bot == nullptr) != (top == nullptr))) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  int rc;
+  const size_t cols = (size_t)ctx->g.sx * ctx->g.sy;
+  if ((rc = h2d(ctx, ctx->sa, in, ctx->g.nspec))) return rc;
+  const double *db = nullptr, *dt = nullptr;
+  if (bot) {
+    if ((rc = h2d(ctx, ctx->bt, bot, cols))) return rc;
+    if ((rc = h2d(ctx, ctx->bt + cols, top, cols))) return rc;
+    db = ctx->bt;
+    dt = ctx->bt + cols;
+  }
+  if ((rc = spec_diffz(ctx, ctx->sa, ctx->sb, db, dt))) return rc;
+  return d2h(ctx, out, ctx->sb, ctx->g.nspec);
+}
+int pmpic_op_laplinv(pmpic_ctx* ctx, double* inout, int df0) {
+  if (!ctx || !inout) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  int rc;
+  if ((rc = h2d(ctx, ctx->sa, inout, ctx->g.nspec))) return rc;
+  if ((rc = spec_laplinv(ctx, ctx->sa, df0 != 0))) return rc;
+  if ((rc = d2h(ctx, inout, ctx->sa, ctx->g.nspec))) return rc;
+  return sync_info(ctx);
+}
+int pmpic_op_parcel_haloswap(pmpic_ctx* ctx) {
+  if (!ctx) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  int rc = parcel_haloswap(ctx);
+  if (rc) return rc;
+  return sync_info(ctx);
+}
+
+}  // extern "C"

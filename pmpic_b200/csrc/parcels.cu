@@ -1,0 +1,641 @@
+// parcels.cu -- parcel-side components on the B200: the RK4 stage update, the
+// single-GPU parcel haloswap, parcel splitting and residual-grid mixing.
+//
+// The integer bookkeeping of the reference's serial loops (migration re-slot
+// order, split child slots, mixing keep / npercell / new-parcel slots /
+// backfill order) is reproduced exactly with deterministic stream compaction:
+// per-block counts, an exclusive scan, and block-local ranks, so every list is
+// built in ascending slot (or reference loop) order.
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace pmpic {
+
+int scan_excl(pmpic_ctx* ctx, const int32_t* in, int64_t n, int32_t* out);
+int launch_mix_grids(pmpic_ctx* ctx);
+
+namespace {
+
+inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
+constexpr int CB = 1024;  // compaction block
+
+// ---- deterministic compaction ------------------------------------------------------
+// Pred(i) -> bool over i in [0, n); list[] receives the true indices ascending.
+template <class Pred>
+__global__ void k_count(Pred pr, int64_t n, int32_t* __restrict__ blockcnt) {
+  int64_t i = (int64_t)blockIdx.x * CB + threadIdx.x;
+  int f = (i < n) && pr(i);
+  int c = __syncthreads_count(f);
+  if (threadIdx.x == 0) blockcnt[blockIdx.x] = c;
+}
+template <class Pred>
+__global__ void k_write(Pred pr, int64_t n, const int32_t* __restrict__ blockoff, int32_t* __restrict__ list) {
+  __shared__ int wsum[32];
+  int64_t i = (int64_t)blockIdx.x * CB + threadIdx.x;
+  int f = (i < n) && pr(i);
+  unsigned bal = __ballot_sync(0xffffffffu, f);
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) wsum[w] = __popc(bal);
+  __syncthreads();
+  if (w == 0) {
+    int v = wsum[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += y;
+    }
+    wsum[lane] = v;  // inclusive
+  }
+  __syncthreads();
+  if (f) {
+    int r = (w > 0 ? wsum[w - 1] : 0) + __popc(bal & ((1u << lane) - 1));
+    list[blockoff[blockIdx.x] + r] = (int32_t)i;
+  }
+}
+
+struct PredKeepEq {
+  const int32_t* keep;
+  int v;
+  __device__ bool operator()(int64_t i) const { return keep[i] == v; }
+};
+struct PredDirNZ {
+  const int8_t* dir;
+  __device__ bool operator()(int64_t i) const { return dir[i] != 0; }
+};
+struct PredFlag {
+  const int32_t* f;
+  __device__ bool operator()(int64_t i) const { return f[i] != 0; }
+};
+// cell in the reference's loop order o = (i*Ny + j)*Nz + k (parcel_mixing.F90:160-162)
+struct PredNewCell {
+  const int32_t* npc;
+  int Nx, Ny, Nz;
+  __device__ bool operator()(int64_t o) const {
+    int k = (int)(o % Nz);
+    int j = (int)((o / Nz) % Ny);
+    int i = (int)(o / ((int64_t)Nz * Ny));
+    return npc[((int64_t)k * Ny + j) * Nx + i] < 3;
+  }
+};
+
+// ---- RK4 stage (rk4_integrator.F90:95-319) -----------------------------------------
+struct RkPtrs {
+  double* s[6];
+  double* o[6];
+  double* f[6];
+  const double* d[6];
+};
+__global__ void k_rk4(int64_t n, RkPtrs P, int stage, const double* __restrict__ dtp) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const double dt = *dtp;  // state%dtm (rk4_integrator.F90:102)
+  const double dt6 = dt / 6, dt2 = dt / 2, dt3 = dt / 3;
+#pragma unroll
+  for (int v = 0; v < 6; ++v) {
+    double d = P.d[v][t];
+    if (stage == 1) {
+      double o = P.s[v][t];
+      P.o[v][t] = o;
+      P.f[v][t] = o + dt6 * d;
+      P.s[v][t] = o + dt2 * d;
+    } else if (stage == 2) {
+      P.f[v][t] = P.f[v][t] + dt3 * d;
+      P.s[v][t] = P.o[v][t] + dt2 * d;
+    } else if (stage == 3) {
+      P.f[v][t] = P.f[v][t] + dt3 * d;
+      P.s[v][t] = P.o[v][t] + dt * d;
+    } else {
+      double f = P.f[v][t] + dt6 * d;
+      P.f[v][t] = f;
+      P.s[v][t] = f;
+    }
+  }
+}
+
+// ---- parcel haloswap (parcels/haloswap.F90:109-289, one rank) -------------------------
+// Reflect z at the walls (:440-456), then classify into N,NE,E,SE,S,SW,W,NW
+// = 1..8 (:296-437) with the limits x_coords(3), x_coords(Nx+3) (:314-318).
+__global__ void k_reflect_classify(Geom g, int64_t n, const double* __restrict__ X, const double* __restrict__ Y,
+                                   double* __restrict__ Z, int8_t* __restrict__ dir) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double z = Z[i];
+  if (z < g.pzmin) Z[i] = g.pzmin + (g.pzmin - z);
+  else if (z > g.pzmax) Z[i] = g.pzmax - (z - g.pzmax);
+  double x = X[i], y = Y[i];
+  const double xmin = g.hxmin, xmax = g.hxmax, ymin = g.hymin, ymax = g.hymax;
+  int d = 0;
+  if (y >= ymax && x >= xmin && x < xmax) d = 1;        // N
+  else if (y < ymin && x >= xmin && x < xmax) d = 5;    // S
+  else if (x >= xmax && y >= ymin && y < ymax) d = 3;   // E
+  else if (x < xmin && y >= ymin && y < ymax) d = 7;    // W
+  else if (x >= xmax && y >= ymax) d = 2;               // NE
+  else if (x < xmin && y >= ymax) d = 8;                // NW
+  else if (x >= xmax && y < ymin) d = 4;                // SE
+  else if (x < xmin && y < ymin) d = 6;                 // SW
+  dir[i] = (int8_t)d;
+}
+
+// Stable partition of the ascending moved list V by direction 1..8 (single
+// CTA; the moved list is short): M = the order in which the reference sends,
+// receives and unpacks the parcels (dir 1..8, ascending index within a dir).
+__global__ void k_partition_dirs(const int32_t* __restrict__ V, const int32_t* __restrict__ nmov,
+                                 const int8_t* __restrict__ dir, int32_t* __restrict__ M) {
+  __shared__ int base[9];
+  __shared__ int cnt[9];
+  __shared__ int wcnt[32][9];
+  const int nm = *nmov;
+  if (threadIdx.x < 9) cnt[threadIdx.x] = 0;
+  __syncthreads();
+  for (int t = threadIdx.x; t < nm; t += blockDim.x) atomicAdd(&cnt[dir[V[t]]], 1);  // integer: order-free
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int s = 0;
+    for (int d = 1; d <= 8; ++d) {
+      base[d] = s;
+      s += cnt[d];
+    }
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int c0 = 0; c0 < nm; c0 += blockDim.x) {
+    int t = c0 + threadIdx.x;
+    int d = (t < nm) ? dir[V[t]] : 0;
+    // per-warp, per-direction counts and ranks
+    int myrank = 0;
+    for (int dd = 1; dd <= 8; ++dd) {
+      unsigned b = __ballot_sync(0xffffffffu, d == dd);
+      if (d == dd) myrank = __popc(b & ((1u << lane) - 1));
+      if (lane == 0) wcnt[w][dd] = __popc(b);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int dd = 1; dd <= 8; ++dd) {
+        int s = base[dd];
+        for (int q = 0; q < nw; ++q) {
+          int v = wcnt[q][dd];
+          wcnt[q][dd] = s;
+          s += v;
+        }
+        base[dd] = s;
+      }
+    }
+    __syncthreads();
+    if (t < nm && d > 0) M[wcnt[w][d] + myrank] = V[t];
+    __syncthreads();
+  }
+}
+
+// The 29 properties carried by the haloswap buffers (haloswap.F90:35-52, :585-600).
+__constant__ int c_swap_props[29] = {PMPIC_PROP_X,    PMPIC_PROP_Y,    PMPIC_PROP_Z,    PMPIC_PROP_P,
+                                     PMPIC_PROP_Q,    PMPIC_PROP_R,    PMPIC_PROP_DXDT, PMPIC_PROP_DYDT,
+                                     PMPIC_PROP_DZDT, PMPIC_PROP_DPDT, PMPIC_PROP_DQDT, PMPIC_PROP_DRDT,
+                                     PMPIC_PROP_H,    PMPIC_PROP_B,    PMPIC_PROP_VOL,  PMPIC_PROP_STRETCH,
+                                     PMPIC_PROP_TAG,  PMPIC_PROP_XO,   PMPIC_PROP_YO,   PMPIC_PROP_ZO,
+                                     PMPIC_PROP_XF,   PMPIC_PROP_YF,   PMPIC_PROP_ZF,   PMPIC_PROP_PO,
+                                     PMPIC_PROP_QO,   PMPIC_PROP_RO,   PMPIC_PROP_PF,   PMPIC_PROP_QF,
+                                     PMPIC_PROP_RF};
+
+// gather moved parcels (with the periodic shift of their direction,
+// haloswap.F90:531-559, :587-591) into the staging buffer
+__global__ void k_swap_gather(Geom g, const int32_t* __restrict__ nmov, const int32_t* __restrict__ M,
+                              const int8_t* __restrict__ dir, const double* __restrict__ parcels, int64_t cap,
+                              double* __restrict__ buf) {
+  const int nm = *nmov;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)nm * 29;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    int t = (int)(e / 29), q = (int)(e - (int64_t)t * 29);
+    int src = M[t];
+    int pid = c_swap_props[q];
+    double v = parcels[(size_t)pid * cap + src];
+    int d = dir[src];
+    double xs = 0.0, ys = 0.0;
+    if (d == 3 || d == 2 || d == 4) xs = g.xshift_e;
+    else if (d == 7 || d == 8 || d == 6) xs = g.xshift_w;
+    if (d == 1 || d == 2 || d == 8) ys = g.yshift_n;
+    else if (d == 5 || d == 6 || d == 4) ys = g.yshift_s;
+    if (pid == PMPIC_PROP_X || pid == PMPIC_PROP_XO || pid == PMPIC_PROP_XF) v = v + xs;
+    if (pid == PMPIC_PROP_Y || pid == PMPIC_PROP_YO || pid == PMPIC_PROP_YF) v = v + ys;
+    buf[e] = v;
+  }
+}
+// unpack into the vacated slots in ascending order (haloswap.F90:695-716)
+__global__ void k_swap_scatter(const int32_t* __restrict__ nmov, const int32_t* __restrict__ V,
+                               const double* __restrict__ buf, double* __restrict__ parcels, int64_t cap) {
+  const int nm = *nmov;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)nm * 29;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    int t = (int)(e / 29), q = (int)(e - (int64_t)t * 29);
+    parcels[(size_t)c_swap_props[q] * cap + V[t]] = buf[e];
+  }
+}
+__global__ void k_check_swapcap(const int32_t* nmov, int32_t* nclamped, int64_t swapcap, DevInfo* info) {
+  int nm = *nmov;
+  if (nm > swapcap) {
+    atomicCAS(&info->error, 0, PMPIC_ERR_CAPACITY);
+    nm = 0;  // nothing is moved; the call reports the capacity error
+  }
+  *nclamped = nm;
+  info->n_migrated = *nmov;
+}
+
+// ---- parcel splitting (parcel_splitting.F90:64-133) -----------------------------------
+__global__ void k_split_flag(int64_t n, double* __restrict__ parcels, int64_t cap, const double* __restrict__ dtp,
+                             int32_t* __restrict__ flag) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double dt = *dtp;
+  const double* P = parcels + (size_t)PMPIC_PROP_P * cap;
+  const double* Q = parcels + (size_t)PMPIC_PROP_Q * cap;
+  const double* R = parcels + (size_t)PMPIC_PROP_R * cap;
+  const double* DP = parcels + (size_t)PMPIC_PROP_DPDT * cap;
+  const double* DQ = parcels + (size_t)PMPIC_PROP_DQDT * cap;
+  const double* DR = parcels + (size_t)PMPIC_PROP_DRDT * cap;
+  double* S = parcels + (size_t)PMPIC_PROP_STRETCH * cap;
+  double ds = P[i] * DP[i] + Q[i] * DQ[i] + R[i] * DR[i];  // :68-70
+  ds = pow(fabs(ds), f4div(1.f, 3.f));                      // :71
+  double s = S[i] + ds * dt;                                // :73
+  S[i] = s;
+  flag[i] = s > 4. ? 1 : 0;                                  // :76 (stretchmax = 4)
+}
+__global__ void k_split_apply(int64_t n, const int32_t* __restrict__ list, const int32_t* __restrict__ nsplit,
+                              double* __restrict__ parcels, int64_t cap, DevInfo* info) {
+  const int ns = *nsplit;
+  const double pi = 4. * atan(1.0);
+  const double third = f4div(1.f, 3.f);
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ns; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t i = list[t];
+    int64_t c = n + t;  // child slot: appended in index order (:94)
+    if (c >= cap) {
+      atomicCAS(&info->error, 0, PMPIC_ERR_CAPACITY);
+      continue;
+    }
+    double* p = parcels;
+    auto A = [&](int pid) -> double* { return p + (size_t)pid * cap; };
+    double r = A(PMPIC_PROP_VOL)[i] / 4. / pi;  // :78-79
+    r = pow(r, third);
+    double pp = A(PMPIC_PROP_P)[i], qq = A(PMPIC_PROP_Q)[i], rr = A(PMPIC_PROP_R)[i];
+    double absw = pp * pp + qq * qq + rr * rr;  // :83-84
+    absw = sqrt(absw);
+    double x = A(PMPIC_PROP_X)[i], y = A(PMPIC_PROP_Y)[i], z = A(PMPIC_PROP_Z)[i];
+    A(PMPIC_PROP_X)[c] = x + r * pp / absw;  // :95-118
+    A(PMPIC_PROP_Y)[c] = y + r * qq / absw;
+    A(PMPIC_PROP_Z)[c] = z + r * rr / absw;
+    A(PMPIC_PROP_P)[c] = pp;
+    A(PMPIC_PROP_Q)[c] = qq;
+    A(PMPIC_PROP_R)[c] = rr;
+    A(PMPIC_PROP_DXDT)[c] = A(PMPIC_PROP_DXDT)[i];
+    A(PMPIC_PROP_DYDT)[c] = A(PMPIC_PROP_DYDT)[i];
+    A(PMPIC_PROP_DZDT)[c] = A(PMPIC_PROP_DZDT)[i];
+    A(PMPIC_PROP_DPDT)[c] = A(PMPIC_PROP_DPDT)[i];
+    A(PMPIC_PROP_DQDT)[c] = A(PMPIC_PROP_DQDT)[i];
+    A(PMPIC_PROP_DRDT)[c] = A(PMPIC_PROP_DRDT)[i];
+    A(PMPIC_PROP_H)[c] = A(PMPIC_PROP_H)[i];
+    A(PMPIC_PROP_B)[c] = A(PMPIC_PROP_B)[i];
+    double vol = A(PMPIC_PROP_VOL)[i];
+    A(PMPIC_PROP_VOL)[c] = vol / 2;
+    A(PMPIC_PROP_STRETCH)[c] = 0.;
+    A(PMPIC_PROP_TAG)[c] = A(PMPIC_PROP_TAG)[i];
+    A(PMPIC_PROP_X)[i] = x - r * pp / absw;  // :121-127
+    A(PMPIC_PROP_Y)[i] = y - r * qq / absw;
+    A(PMPIC_PROP_Z)[i] = z - r * rr / absw;
+    A(PMPIC_PROP_VOL)[i] = vol / 2;
+    A(PMPIC_PROP_STRETCH)[i] = 0.;
+  }
+}
+
+// ---- btot (vorticity_tendency.F90:121-126) ------------------------------------------------
+__global__ void k_btot(int64_t n, const double* __restrict__ B, const double* __restrict__ H,
+                       const double* __restrict__ Z, double* __restrict__ BT) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  BT[i] = B[i] + 12.5 * fmax(0.0, H[i] - exp(-Z[i]));
+}
+
+// ---- mixing (parcel_mixing.F90:68-431) --------------------------------------------------
+__global__ void k_keep(int64_t n, const double* __restrict__ VOL, double vmin, int32_t* __restrict__ keep) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  keep[i] = VOL[i] < vmin ? 0 : 1;  // :488, :555
+}
+
+// New parcels (:160-212): the a-th under-populated cell in loop order takes the
+// a-th removed slot, or is appended after norig; keep = 2 only for slots below
+// the last one (:191-193, strict <).
+__global__ void k_new_parcels(Geom g, const int32_t* __restrict__ olist, const int32_t* __restrict__ nnew,
+                              const int32_t* __restrict__ zlist, const int32_t* __restrict__ nzero, int64_t norig,
+                              int64_t cap, int32_t* __restrict__ keep, double* __restrict__ parcels,
+                              const double* __restrict__ KV, const double* __restrict__ KB,
+                              const double* __restrict__ KH, const double* __restrict__ KP,
+                              const double* __restrict__ KQ, const double* __restrict__ KR,
+                              int32_t* __restrict__ newslot, double* __restrict__ portion, DevInfo* info) {
+  const int na = *nnew, nz0 = *nzero;
+  for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < na; a += (int64_t)gridDim.x * blockDim.x) {
+    int64_t o = olist[a];
+    int k = (int)(o % g.Nz);
+    int j = (int)((o / g.Nz) % g.Ny);
+    int i = (int)(o / ((int64_t)g.Nz * g.Ny));
+    int64_t slot = a < nz0 ? (int64_t)zlist[a] : norig + (a - nz0);
+    if (slot + 2 > cap) {  // :194-199: n+1 > maxparcels after placing at n
+      atomicCAS(&info->error, 0, PMPIC_ERR_CAPACITY);
+      continue;
+    }
+    int i1 = i + 1 == g.Nx ? 0 : i + 1, j1 = j + 1 == g.Ny ? 0 : j + 1;
+    // Fortran sum over the (2,2,2) section: k fastest, then j, then i
+    size_t q[8] = {((size_t)k * g.Ny + j) * g.Nx + i,        ((size_t)(k + 1) * g.Ny + j) * g.Nx + i,
+                   ((size_t)k * g.Ny + j1) * g.Nx + i,       ((size_t)(k + 1) * g.Ny + j1) * g.Nx + i,
+                   ((size_t)k * g.Ny + j) * g.Nx + i1,       ((size_t)(k + 1) * g.Ny + j) * g.Nx + i1,
+                   ((size_t)k * g.Ny + j1) * g.Nx + i1,      ((size_t)(k + 1) * g.Ny + j1) * g.Nx + i1};
+    auto box = [&](const double* G) {
+      double s = 0.0;
+#pragma unroll
+      for (int u = 0; u < 8; ++u) s = s + G[q[u]];
+      return s;
+    };
+    double v = box(KV);
+    double por = 2 * g.vmin / v;
+    auto A = [&](int pid) -> double* { return parcels + (size_t)pid * cap; };
+    // x_coords(I) with I = i+3 (halo-inclusive, parcel_interpolation.F90:126-136)
+    double xc = g.pxmin + (double)(i + 2) * g.dx, xc1 = g.pxmin + (double)(i + 3) * g.dx;
+    double yc = g.pymin + (double)(j + 2) * g.dy, yc1 = g.pymin + (double)(j + 3) * g.dy;
+    double zc = g.pzmin + (double)k * g.dz, zc1 = g.pzmin + (double)(k + 1) * g.dz;
+    A(PMPIC_PROP_X)[slot] = 0.5 * (xc + xc1);
+    A(PMPIC_PROP_Y)[slot] = 0.5 * (yc + yc1);
+    A(PMPIC_PROP_Z)[slot] = 0.5 * (zc + zc1);
+    A(PMPIC_PROP_VOL)[slot] = 2 * g.vmin;
+    A(PMPIC_PROP_STRETCH)[slot] = 0;
+    A(PMPIC_PROP_B)[slot] = box(KB) / v;
+    A(PMPIC_PROP_H)[slot] = box(KH) / v;
+    A(PMPIC_PROP_P)[slot] = box(KP) / v;
+    A(PMPIC_PROP_Q)[slot] = box(KQ) / v;
+    A(PMPIC_PROP_R)[slot] = box(KR) / v;
+    if (slot + 1 < norig) keep[slot] = 2;
+    int64_t cell = ((int64_t)k * g.Ny + j) * g.Nx + i;
+    newslot[cell] = (int32_t)slot;
+    portion[cell] = por;
+  }
+}
+
+// residual grids minus the new parcels' portions, then doubled at the walls
+// (:202-207, :221-240)
+struct ResPtrs {
+  double* r[6];
+  const double* k[6];
+};
+__global__ void k_residual_update(Geom g, ResPtrs RP, const int32_t* __restrict__ newslot,
+                                  const double* __restrict__ portion) {
+  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= g.nphys) return;
+  int i = (int)(e % g.Nx);
+  int j = (int)((e / g.Nx) % g.Ny);
+  int k = (int)(e / ((int64_t)g.Nx * g.Ny));
+  int im = i == 0 ? g.Nx - 1 : i - 1, jm = j == 0 ? g.Ny - 1 : j - 1;
+  double por[8];
+  int np = 0;
+  const int cis[2] = {im, i}, cjs[2] = {jm, j};
+  for (int a = 0; a < 2; ++a)
+    for (int b = 0; b < 2; ++b)
+      for (int c = 0; c < 2; ++c) {
+        int ck = k - 1 + c;
+        if (ck < 0 || ck >= g.Nz) continue;
+        int64_t cell = ((int64_t)ck * g.Ny + cjs[b]) * g.Nx + cis[a];
+        if (newslot[cell] >= 0) por[np++] = portion[cell];
+      }
+  const bool wall = (k == 0 || k == g.Nz);
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    double r = RP.r[q][e];
+    double kv = RP.k[q][e];
+    for (int u = 0; u < np; ++u) r = r - por[u] * kv;
+    if (wall) r = r * 2;
+    RP.r[q][e] = r;
+  }
+}
+
+// residuals onto the kept original parcels (:245-342)
+__global__ void k_redistribute(Geom g, int64_t norig, const int32_t* __restrict__ keep, double* __restrict__ parcels,
+                               int64_t cap, ResPtrs RP, DevInfo* info) {
+  int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= norig || keep[m] != 1) return;
+  auto A = [&](int pid) -> double* { return parcels + (size_t)pid * cap; };
+  int ci, cj, ck;
+  double delx, dely, delz;
+  if (!bin_parcel(g, A(PMPIC_PROP_X)[m], A(PMPIC_PROP_Y)[m], A(PMPIC_PROP_Z)[m], ci, cj, ck, delx, dely, delz)) {
+    atomicCAS(&info->error, 0, PMPIC_ERR_OUT_OF_BOX);
+    return;
+  }
+  int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
+  size_t c[8] = {((size_t)ck * g.Ny + cj) * g.Nx + ci,        ((size_t)ck * g.Ny + cj) * g.Nx + ci1,
+                 ((size_t)ck * g.Ny + cj1) * g.Nx + ci,       ((size_t)ck * g.Ny + cj1) * g.Nx + ci1,
+                 ((size_t)(ck + 1) * g.Ny + cj) * g.Nx + ci,  ((size_t)(ck + 1) * g.Ny + cj) * g.Nx + ci1,
+                 ((size_t)(ck + 1) * g.Ny + cj1) * g.Nx + ci, ((size_t)(ck + 1) * g.Ny + cj1) * g.Nx + ci1};
+  double v = A(PMPIC_PROP_VOL)[m];
+  double w[8];
+  w[0] = (1 - delz) * (1 - dely) * (1 - delx) * v;
+  w[1] = (1 - delz) * (1 - dely) * (delx) * v;
+  w[2] = (1 - delz) * (dely) * (1 - delx) * v;
+  w[3] = (1 - delz) * (dely) * (delx) * v;
+  w[4] = (delz) * (1 - dely) * (1 - delx) * v;
+  w[5] = (delz) * (1 - dely) * (delx) * v;
+  w[6] = (delz) * (dely) * (1 - delx) * v;
+  w[7] = (delz) * (dely) * (delx) * v;
+  const double* V = RP.k[0];
+  const double* vres = RP.r[0];
+  double nv = v;
+#pragma unroll
+  for (int u = 0; u < 8; ++u) nv = nv + w[u] * vres[c[u]] / V[c[u]];  // :268-276
+  A(PMPIC_PROP_VOL)[m] = nv;
+  const int pids[5] = {PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    const double* res = RP.r[q + 1];
+    double s = A(pids[q])[m] * v;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) s = s + w[u] / V[c[u]] * res[c[u]];  // :279-336
+    A(pids[q])[m] = s / nv;
+  }
+}
+
+// backfill (:347-389): the t-th removed slot (ascending) receives the t-th kept
+// parcel counted from the top; 11 properties are copied.
+__global__ void k_backfill(const int32_t* __restrict__ zlist, const int32_t* __restrict__ nz,
+                           const int32_t* __restrict__ olist, const int32_t* __restrict__ no,
+                           double* __restrict__ parcels, int64_t cap, DevInfo* info) {
+  const int nzero = *nz, nones = *no;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && nzero > nones) atomicCAS(&info->error, 0, PMPIC_ERR_BACKFILL);
+  const int pids[11] = {PMPIC_PROP_X, PMPIC_PROP_Y, PMPIC_PROP_Z, PMPIC_PROP_P,   PMPIC_PROP_Q,      PMPIC_PROP_R,
+                        PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_VOL, PMPIC_PROP_TAG, PMPIC_PROP_STRETCH};
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)nzero * 11;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    int t = (int)(e / 11), q = (int)(e - (int64_t)t * 11);
+    if (t >= nones) continue;
+    int dst = zlist[t], src = olist[nones - 1 - t];
+    parcels[(size_t)pids[q] * cap + dst] = parcels[(size_t)pids[q] * cap + src];
+  }
+}
+
+}  // namespace
+
+// list of i in [0,n) with pred(i), ascending; count written to *dcount (device)
+template <class Pred>
+static int compact(pmpic_ctx* ctx, Pred pr, int64_t n, int32_t* list, int32_t* dcount) {
+  int64_t nb = (n + CB - 1) / CB;
+  if (nb == 0) {
+    PMPIC_CUDA(cudaMemsetAsync(dcount, 0, sizeof(int32_t), ctx->stream));
+    return 0;
+  }
+  int32_t* cnt = ctx->aux2;            // nb + 1 (nb + 1 <= nbmax)
+  int32_t* off = ctx->aux2 + ctx->nbmax;
+  k_count<<<(unsigned)nb, CB, 0, ctx->stream>>>(pr, n, cnt);
+  int rc = scan_excl(ctx, cnt, nb, off);
+  if (rc) return rc;
+  k_write<<<(unsigned)nb, CB, 0, ctx->stream>>>(pr, n, off, list);
+  PMPIC_CUDA(cudaMemcpyAsync(dcount, off + nb, sizeof(int32_t), cudaMemcpyDeviceToDevice, ctx->stream));
+  PMPIC_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// small device counters live after the DevInfo block
+static int32_t* dcounter(pmpic_ctx* ctx, int i) { return (int32_t*)(ctx->dinfo + 1) + i; }
+
+int compute_btot(pmpic_ctx* ctx) {
+  if (ctx->n == 0) return 0;
+  k_btot<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->n, prop(ctx, PMPIC_PROP_B), prop(ctx, PMPIC_PROP_H),
+                                                     prop(ctx, PMPIC_PROP_Z), prop(ctx, PMPIC_PROP_BTOT));
+  PMPIC_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int rk4_stage(pmpic_ctx* ctx, int stage) {
+  if (ctx->n == 0) return 0;
+  RkPtrs P;
+  const int S[6] = {PMPIC_PROP_X, PMPIC_PROP_Y, PMPIC_PROP_Z, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
+  const int O[6] = {PMPIC_PROP_XO, PMPIC_PROP_YO, PMPIC_PROP_ZO, PMPIC_PROP_PO, PMPIC_PROP_QO, PMPIC_PROP_RO};
+  const int F[6] = {PMPIC_PROP_XF, PMPIC_PROP_YF, PMPIC_PROP_ZF, PMPIC_PROP_PF, PMPIC_PROP_QF, PMPIC_PROP_RF};
+  const int D[6] = {PMPIC_PROP_DXDT, PMPIC_PROP_DYDT, PMPIC_PROP_DZDT, PMPIC_PROP_DPDT, PMPIC_PROP_DQDT, PMPIC_PROP_DRDT};
+  for (int v = 0; v < 6; ++v) {
+    P.s[v] = prop(ctx, S[v]);
+    P.o[v] = prop(ctx, O[v]);
+    P.f[v] = prop(ctx, F[v]);
+    P.d[v] = prop(ctx, D[v]);
+  }
+  k_rk4<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->n, P, stage, &ctx->dinfo->dtm);
+  ctx->sorted_valid = false;
+  PMPIC_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int parcel_haloswap(pmpic_ctx* ctx) {
+  const int64_t n = ctx->n;
+  ctx->sorted_valid = false;
+  if (n == 0) return 0;
+  k_reflect_classify<<<nblk(n, 256), 256, 0, ctx->stream>>>(ctx->g, n, prop(ctx, PMPIC_PROP_X),
+                                                            prop(ctx, PMPIC_PROP_Y), prop(ctx, PMPIC_PROP_Z),
+                                                            ctx->dir);
+  int32_t* V = ctx->aux;                 // vacated slots, ascending
+  int32_t* M = ctx->keep;                // moved parcels in send order (keep is free outside mixing)
+  int32_t* nm = dcounter(ctx, 0);
+  int rc = compact(ctx, PredDirNZ{ctx->dir}, n, V, nm);
+  if (rc) return rc;
+  k_partition_dirs<<<1, 1024, 0, ctx->stream>>>(V, nm, ctx->dir, M);
+  // the staging buffer is bounded: on overflow nothing moves and the call
+  // reports PMPIC_ERR_CAPACITY
+  int32_t* nmc = dcounter(ctx, 1);
+  k_check_swapcap<<<1, 1, 0, ctx->stream>>>(nm, nmc, ctx->swapcap, ctx->dinfo);
+  k_swap_gather<<<592, 256, 0, ctx->stream>>>(ctx->g, nmc, M, ctx->dir, ctx->parcels, ctx->cap, ctx->swapbuf);
+  k_swap_scatter<<<592, 256, 0, ctx->stream>>>(nmc, V, ctx->swapbuf, ctx->parcels, ctx->cap);
+  PMPIC_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int splitting(pmpic_ctx* ctx) {
+  const int64_t n = ctx->n;
+  int32_t* flag = ctx->aux;
+  int32_t* list = ctx->keep;
+  int32_t* ns = dcounter(ctx, 2);
+  if (n > 0) {
+    k_split_flag<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, ctx->parcels, ctx->cap, &ctx->dinfo->dtm, flag);
+    int rc = compact(ctx, PredFlag{flag}, n, list, ns);
+    if (rc) return rc;
+    k_split_apply<<<592, 256, 0, ctx->stream>>>(n, list, ns, ctx->parcels, ctx->cap, ctx->dinfo);
+  } else {
+    PMPIC_CUDA(cudaMemsetAsync(ns, 0, sizeof(int32_t), ctx->stream));
+  }
+  int32_t hns = 0;
+  PMPIC_CUDA(cudaMemcpyAsync(&hns, ns, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
+  int64_t nn = n + hns;
+  if (nn > ctx->cap) return set_error(ctx, PMPIC_ERR_CAPACITY, "maxparcels reached (parcel splitting)");
+  ctx->n = nn;
+  ctx->info.n_split = hns;
+  return parcel_haloswap(ctx);
+}
+
+int mixing(pmpic_ctx* ctx) {
+  const Geom& g = ctx->g;
+  const int64_t norig = ctx->n;
+  int rc;
+  // keep flags (:488) and the kept / residual grids (construct_grids :440-624)
+  if (norig > 0)
+    k_keep<<<nblk(norig, 256), 256, 0, ctx->stream>>>(norig, prop(ctx, PMPIC_PROP_VOL), g.vmin, ctx->keep);
+  if ((rc = bin_and_sort(ctx))) return rc;
+  if ((rc = launch_mix_grids(ctx))) return rc;
+  // removed slots Z (ascending) and under-populated cells in loop order
+  int32_t* zlist = ctx->aux;
+  int32_t* nz0 = dcounter(ctx, 3);
+  if ((rc = compact(ctx, PredKeepEq{ctx->keep, 0}, norig, zlist, nz0))) return rc;
+  int32_t* olist = ctx->cell_fill;  // ncell entries; free after bin_and_sort
+  int32_t* nnew = dcounter(ctx, 4);
+  if ((rc = compact(ctx, PredNewCell{ctx->npercell, g.Nx, g.Ny, g.Nz}, g.ncell, olist, nnew))) return rc;
+  PMPIC_CUDA(cudaMemsetAsync(ctx->newslot, 0xff, sizeof(int32_t) * g.ncell, ctx->stream));
+  double* K[6] = {ctx->grid[PMPIC_GRID_VOL], ctx->grid[PMPIC_GRID_B], ctx->grid[PMPIC_GRID_HG],
+                  ctx->grid[PMPIC_GRID_P],   ctx->grid[PMPIC_GRID_Q], ctx->grid[PMPIC_GRID_R]};
+  k_new_parcels<<<592, 256, 0, ctx->stream>>>(g, olist, nnew, zlist, nz0, norig, ctx->cap, ctx->keep, ctx->parcels,
+                                              K[0], K[1], K[2], K[3], K[4], K[5], ctx->newslot, ctx->newportion,
+                                              ctx->dinfo);
+  ResPtrs RP;
+  for (int q = 0; q < 6; ++q) {
+    RP.r[q] = ctx->mixres[q];
+    RP.k[q] = K[q];
+  }
+  k_residual_update<<<nblk(g.nphys, 256), 256, 0, ctx->stream>>>(g, RP, ctx->newslot, ctx->newportion);
+  if (norig > 0)
+    k_redistribute<<<nblk(norig, 256), 256, 0, ctx->stream>>>(g, norig, ctx->keep, ctx->parcels, ctx->cap, RP,
+                                                              ctx->dinfo);
+  // counts to the host: removed, new cells
+  int32_t h[2];
+  PMPIC_CUDA(cudaMemcpyAsync(&h[0], nz0, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  PMPIC_CUDA(cudaMemcpyAsync(&h[1], nnew, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
+  const int64_t nremove = h[0], nadd = h[1];
+  // count = max(n-1, numparcels_local) (:217)
+  int64_t count = norig;
+  if (nadd > nremove) count = norig + (nadd - nremove);
+  if (nadd > 0 && nadd <= nremove) {
+    // the last new parcel sits in a removed slot: count stays norig
+    count = norig;
+  }
+  if (count == norig) {
+    // backfill: keep==0 slots now exclude the ones that received new parcels
+    // (keep = 2), except the last slot (:191-193)
+    int32_t* z2 = ctx->aux;
+    int32_t* nz2 = dcounter(ctx, 5);
+    int32_t* ones = ctx->aux2 + 2 * ctx->nbmax;
+    int32_t* no = dcounter(ctx, 6);
+    if ((rc = compact(ctx, PredKeepEq{ctx->keep, 0}, norig, z2, nz2))) return rc;
+    if ((rc = compact(ctx, PredKeepEq{ctx->keep, 1}, norig, ones, no))) return rc;
+    k_backfill<<<592, 256, 0, ctx->stream>>>(z2, nz2, ones, no, ctx->parcels, ctx->cap, ctx->dinfo);
+    int32_t hz = 0;
+    PMPIC_CUDA(cudaMemcpyAsync(&hz, nz2, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
+    count = norig - hz;
+  }
+  ctx->n = count;
+  ctx->sorted_valid = false;
+  ctx->info.n_removed = nremove;
+  ctx->info.n_added = nadd;
+  PMPIC_CUDA(cudaGetLastError());
+  return 0;
+}
+
+}  // namespace pmpic
