@@ -1,0 +1,342 @@
+#!/usr/bin/env python
+"""Benchmark of the PMPIC hot path on B200: parcel-RK4-steps/s of the 256^3
+thermal plume (one model step = four RK4 substeps of vort2vel,
+vorticity_tendency, rk4_integrator, parcel_splitting, parcel_mixing).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One process per GPU (torchrun for N > 1); every rank runs an independent
+replica of the plume (the path does not shard), value = all ranks' parcel
+steps / the max over ranks of the device time.  ``--impl reference`` times the
+CPU restatement of the reference on the host cores instead (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "parcel-RK4-steps/s at 256³: mixed-prec vs FP64 GPU, ≤1e-4 rel err vs FP64"
+UNIT = "parcel-RK4-steps/s"
+PEAKS_FILE = os.path.join(HERE, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0
+
+# the 256^3 plume (thermal of radius 0.4 at (pi, pi, 0.6) in [0,2pi]^2 x [0,pi])
+PLUME = dict(lx=2 * np.pi, ly=2 * np.pi, lz=np.pi, sub=2, jitter=0.25, seed=1, xc=np.pi, yc=np.pi,
+             zc=0.6, radius=0.4, excess=1.0, h_in=0.95, h_env0=0.3, z_strat=1.2, n2=1.0)
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_FILE) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def combine(t_dev, work, pg, device):
+    """Max of the device time and sum of the work over ranks (replicas)."""
+    if pg is None:
+        return float(t_dev), float(work)
+    import torch
+    t = torch.tensor([float(t_dev)], device=device, dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    w = torch.tensor([float(work)], device=device, dtype=torch.float64)
+    pg.all_reduce(w, op=pg.ReduceOp.SUM)
+    return float(t.item()), float(w.item())
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def cpu_reference(grid, steps, warmup, threads):
+    """The CPU restatement of the reference (oracle), timed on the host cores."""
+    import pmpic_b200 as pm
+    from oracle import Oracle
+    ic = pm.thermal_parcels(grid, grid, grid, **PLUME)
+    n0 = len(ic["x"])
+    o = Oracle(grid, grid, grid, PLUME["lx"], PLUME["ly"], PLUME["lz"], dtm=0.0025, dtmax=0.0025,
+               max_parcels=int(1.25 * n0), threads=threads)
+    o.set_parcels(**ic)
+    for _ in range(warmup):
+        o.step()
+    work = 0
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        work += o.n
+        o.step()
+    dt = time.perf_counter() - t0
+    return work / dt, n0, dt
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    grid = args.ref_grid
+    value, n0, dt = cpu_reference(grid, args.steps, args.warmup, threads)
+    sample = (f"{grid}^3 plume ({n0} parcels, same thermal and environment), {args.steps} timed steps "
+              f"after {args.warmup} warm-up; C++ restatement of the reference Fortran (no Fortran "
+              f"compiler or MPI here to build the reference itself)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"thermal plume {grid}^3 sample of the 256^3 plume, FP64, 8 parcels/cell",
+                       "grid": grid, "parcels": n0, "dt": 0.0025},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(args):
+    rank, world, local = dist_env()
+    import torch  # device selection and the multi-rank plumbing only
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    import pmpic_b200 as pm
+
+    grid = args.grid
+    ic = pm.thermal_parcels(grid, grid, grid, **PLUME)
+    n0 = len(ic["x"])
+    cap = int(args.capacity * n0)
+    ctx = pm.Context(grid, grid, grid, PLUME["lx"], PLUME["ly"], PLUME["lz"], dtm=0.0025, dtmax=0.0025,
+                     max_parcels=cap, device=local)
+    ctx.upload(**ic)
+    L = pm.lib()
+    h = ctx._h
+
+    def barrier():
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        ctx.step(1)
+    barrier()
+    # timed region: device-resident state, CUDA events on the library's stream
+    L.pmpic_timing(h, 1)
+    l0 = C.c_int64()
+    L.pmpic_launch_count(h, C.byref(l0))
+    work = 0
+    with ClockSampler(local) as clk:
+        L.pmpic_event_record(h, 0)
+        for _ in range(args.steps):
+            work += ctx.n
+            ctx.step(1)
+        L.pmpic_event_record(h, 1)
+        ms = C.c_float()
+        L.pmpic_event_elapsed(h, 0, 1, C.byref(ms))
+    l1 = C.c_int64()
+    L.pmpic_launch_count(h, C.byref(l1))
+    t_dev = ms.value / 1e3
+    timers = {}
+    for i in range(L.pmpic_timer_count()):
+        tot, calls = C.c_double(), C.c_int64()
+        L.pmpic_timer_read(h, i, C.byref(tot), C.byref(calls))
+        timers[L.pmpic_timer_name(i).decode()] = (tot.value, calls.value)
+    L.pmpic_timing(h, 0)
+    barrier()
+    t_max, work_all = combine(t_dev, work, pg, "cuda")
+    value = work_all / t_max
+
+    # roofline of the dominant kernel family (by share of the timed region)
+    peak, peak_kind = hbm_peak()
+    nz1 = grid + 1
+    nphys = nz1 * grid * grid
+    nspec = nz1 * (grid + 2) * (grid + 2)
+    n_avg = work / max(args.steps, 1)
+    # algorithmic bytes per launch (minimal traffic of one call):
+    #  par2grid: x,y,z,vol + NQ fields per parcel, NQ grids out (vort2vel NQ=3,
+    #            btot NQ=1, the two mixing classes NQ=6: averaged over launches)
+    #  grid2par: x,y,z per parcel + 3 outputs, 3 grids read
+    #  fft:      read + write of both passes over a spectral field
+    fam = {
+        "par2grid": None, "grid2par": 8.0 * n_avg * 6 + 8.0 * 3 * nphys,
+        "fft_inv_tot": 8.0 * 2 * (nspec + nphys), "fft_fwd_tot": 8.0 * 2 * (nspec + nphys),
+    }
+    # par2grid launches per step: 4 x (NQ=3) + 4 x (NQ=1) + 2 x (NQ=6, mixing)
+    p2g_bytes_step = 4 * (8.0 * n_avg * 7 + 8.0 * 3 * nphys) + 4 * (8.0 * n_avg * 5 + 8.0 * nphys) \
+        + 2 * (8.0 * n_avg * 9 + 8.0 * 6 * nphys)
+    fam["par2grid"] = p2g_bytes_step / 10.0
+    step_ms = timers.get("step", (t_dev * 1e3, args.steps))[0]
+    best = max(fam, key=lambda k: timers.get(k, (0.0, 0))[0])
+    tot, calls = timers.get(best, (0.0, 0))
+    avg_s = (tot / calls) / 1e3 if calls else float("nan")
+    achieved = fam[best] / avg_s / 1e9 if calls else None
+    roofline = {"bound": "hbm", "kernel": best, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": None,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+                "share_of_step": tot / step_ms if step_ms else None, "launches": calls,
+                "avg_launch_ms": tot / calls if calls else None,
+                "algorithmic_bytes_per_launch": fam[best]}
+
+    # end to end: the host owns the state; each step uploads it from pinned
+    # host memory, runs the step through the C ABI and downloads the result
+    e2e = None
+    if args.e2e_steps > 0:
+        nb = ctx.n
+        cap_h = int(nb * 1.02) + 1024
+        host = {}
+        for k in pm.IO_PROPS:
+            a = np.empty(cap_h, np.float64)
+            host[k] = a
+            L.pmpic_pin_host(C.c_void_p(a.ctypes.data), C.c_size_t(a.nbytes))
+        cur = ctx.download()
+        for k in pm.IO_PROPS:
+            host[k][:len(cur[k])] = cur[k]
+        nh = len(cur["x"])
+        del cur
+        barrier()
+        e2e_work, h2d, d2h, done = 0, 0, 0, 0
+        cnt = C.c_int64()
+        L.pmpic_event_record(h, 2)
+        for _ in range(args.e2e_steps):
+            ptrs = [host[k].ctypes.data_as(C.POINTER(C.c_double)) for k in pm.IO_PROPS]
+            rc = L.pmpic_upload_parcels(h, nh, *ptrs)
+            if rc:
+                break
+            e2e_work += nh
+            h2d += 8 * 11 * nh
+            L.pmpic_step(h, 1)
+            if ctx.n > cap_h:
+                break
+            rc = L.pmpic_download_parcels(h, cap_h, C.byref(cnt), *ptrs)
+            nh = int(cnt.value)
+            d2h += 8 * 11 * nh
+            done += 1
+        L.pmpic_event_record(h, 3)
+        ms2 = C.c_float()
+        L.pmpic_event_elapsed(h, 2, 3, C.byref(ms2))
+        for k in pm.IO_PROPS:
+            L.pmpic_unpin_host(C.c_void_p(host[k].ctypes.data))
+        t_e2e, e2e_all = combine(ms2.value / 1e3, e2e_work, pg, "cuda")
+        if done:
+            e2e = {"value": e2e_all / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d // done,
+                   "d2h_bytes_per_step": d2h // done, "steps": done,
+                   "path": "pmpic_upload_parcels (pinned host) -> pmpic_step -> pmpic_download_parcels"}
+
+    cpu = None
+    if rank == 0 and world == 1 and args.cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, n_s, dt = cpu_reference(args.ref_grid, 1, 0, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{args.ref_grid}^3 plume ({n_s} parcels), 1 step, C++ restatement of the reference"}
+
+    if pg:
+        pg.barrier()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded jittered-lattice thermal plume, 8 parcels/cell)",
+                "config": {"workload": f"thermal plume {grid}^3, FP64 GPU path, 4 RK4 substeps + splitting + mixing per step",
+                           "grid": grid, "parcels_initial": n0, "max_parcels": cap, "dt": 0.0025,
+                           "precision": "fp64", "parallelism": f"replicas x{world}",
+                           "l2": "inputs larger than L2 (parcel state ~{:.0f} GB)".format(n0 * 30 * 8 / 1e9)},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": int(l1.value - l0.value),
+                "clocks": clk.summary(),
+                "timers_ms": {k: round(v[0], 3) for k, v in timers.items() if v[1]}}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--grid", type=int, default=256)
+    ap.add_argument("--capacity", type=float, default=2.25, help="max_parcels / initial parcels")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--ref-grid", type=int, default=128)
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

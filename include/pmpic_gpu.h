@@ -10,7 +10,7 @@
  * finalise procedure pointers taking `type(model_state_type)`
  * (model_core/src/components/monc_component.F90:51-107).  This header declares
  * the C entry points that new versions of those five component modules bind
- * through `iso_c_binding` (see INTEGRATION.md): one entry point per timestep
+ * through `iso_c_binding`: one entry point per timestep
  * callback, plus context set-up, parcel/grid transfer and step information.
  *
  * Conventions
@@ -29,6 +29,7 @@
 #ifndef PMPIC_GPU_H
 #define PMPIC_GPU_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -73,7 +74,7 @@ typedef struct pmpic_ctx pmpic_ctx;
 /* Model configuration: the hot-path keys of config.mcf / global_config. */
 typedef struct pmpic_config {
   int32_t nx, ny, nz;              /* cell counts (config keys nx, ny, nz); nz+1 z points (setup_grid.F90:51) */
-  double xmin, xmax, ymin, ymax, zmin, zmax;  /* domain; origins must be 0 */
+  double xmin, xmax, ymin, ymax, zmin, zmax;  /* domain; the origins must be 0 (the reference adds a non-zero origin twice) */
   double dtm, dtmax;               /* rk4_integrator.F90:38-41 */
   double timestep_prefactor;       /* vorticity_tendency.F90:96 */
   int64_t max_parcels;             /* parcelsetup_base max_parcels */
@@ -106,7 +107,8 @@ const char* pmpic_last_error(const pmpic_ctx* ctx);
 
 /* ---- parcel transfer (setup, restart and dumps; not on the timestep path) -- */
 /* Sets numparcels_local = n and the 11 prognostic properties of slots 0..n-1;
- * the RK4 arrays and tendencies of those slots are set to zero. */
+ * the RK4 arrays and tendencies of those slots are set to zero and a sticky
+ * device error from an earlier call is cleared. */
 int pmpic_upload_parcels(pmpic_ctx* ctx, int64_t n,
                          const double* x, const double* y, const double* z,
                          const double* p, const double* q, const double* r,
@@ -165,6 +167,26 @@ int pmpic_op_diffz(pmpic_ctx* ctx, const double* in, double* out, const double* 
 int pmpic_op_laplinv(pmpic_ctx* ctx, double* inout, int df_zero_on_boundary);
 /* parcel_haloswap (parcels/haloswap.F90:109-289), single-GPU semantics. */
 int pmpic_op_parcel_haloswap(pmpic_ctx* ctx);
+
+/* ---- instrumentation ------------------------------------------------------ */
+/* Named timers after the reference's timer_mod (register_routine_for_timing /
+ * timer_start / timer_stop, model_core/src/utils/timer.F90:110-245), backed by
+ * CUDA events on the context's stream: cache_weights, par2grid, grid2par,
+ * fft_fwd_tot, fft_inv_tot, diffz, laplinv, vort2vel, vort_tend,
+ * RK4_all_steps, Par_HSWP_entire, splitting, mixing, step.  Enabling resets. */
+int pmpic_timing(pmpic_ctx* ctx, int enable);
+int pmpic_timer_count(void);
+const char* pmpic_timer_name(int id);
+int pmpic_timer_read(pmpic_ctx* ctx, int id, double* total_ms, int64_t* calls);
+/* Number of kernels this context has launched since creation. */
+int pmpic_launch_count(pmpic_ctx* ctx, int64_t* n);
+/* CUDA events recorded on the context's stream (slots 0..7), for timing a
+ * region of calls on the device; elapsed time in milliseconds. */
+int pmpic_event_record(pmpic_ctx* ctx, int slot);
+int pmpic_event_elapsed(pmpic_ctx* ctx, int slot_a, int slot_b, float* ms);
+/* Page-lock (pin) an existing host buffer for fast transfers, and release it. */
+int pmpic_pin_host(void* ptr, size_t bytes);
+int pmpic_unpin_host(void* ptr);
 
 /* ---- parcel set-up (new set-up components; not on the graded path) -------- */
 /* Jittered thermal plume: sub^3 parcels per cell on a sub-lattice jittered by

@@ -495,9 +495,12 @@ extern "C" int orc_cache_weights(orc_ctx* c, int32_t* cells) {
   if (rc) return rc;
   if (cells) {
     // cell id in the interior numbering used by the GPU library:
-    // ((k-1)*Ny + (j-3))*Nx + (i-3)  with periodic interior cells i in 3..Nx+2
-    for (int64_t n = 0; n < c->numparcels; ++n)
-      cells[n] = (int32_t)(((int64_t)(c->ks[n] - 1) * c->Ny + (c->js[n] - 1 - c->hy)) * c->Nx + (c->is[n] - 1 - c->hx));
+    // ((k-1)*Ny + (j-3))*Nx + (i-3), with the halo cell i = Nx+3 (j = Ny+3)
+    // identified with its periodic image, interior cell i = 3 (j = 3)
+    for (int64_t n = 0; n < c->numparcels; ++n) {
+      int ii = (c->is[n] - 1 - c->hx) % c->Nx, jj = (c->js[n] - 1 - c->hy) % c->Ny;
+      cells[n] = (int32_t)(((int64_t)(c->ks[n] - 1) * c->Ny + jj) * c->Nx + ii);
+    }
   }
   return 0;
 }

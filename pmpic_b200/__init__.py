@@ -113,6 +113,16 @@ def lib() -> C.CDLL:
         L.pmpic_op_filter.argtypes = [P, D, D]
         L.pmpic_op_diffz.argtypes = [P, D, D, D, D]
         L.pmpic_op_laplinv.argtypes = [P, D, C.c_int]
+        L.pmpic_timing.argtypes = [P, C.c_int]
+        L.pmpic_timer_count.argtypes = []
+        L.pmpic_timer_name.restype = C.c_char_p
+        L.pmpic_timer_name.argtypes = [C.c_int]
+        L.pmpic_timer_read.argtypes = [P, C.c_int, C.POINTER(C.c_double), C.POINTER(I64)]
+        L.pmpic_launch_count.argtypes = [P, C.POINTER(I64)]
+        L.pmpic_event_record.argtypes = [P, C.c_int]
+        L.pmpic_event_elapsed.argtypes = [P, C.c_int, C.c_int, C.POINTER(C.c_float)]
+        L.pmpic_pin_host.argtypes = [C.c_void_p, C.c_size_t]
+        L.pmpic_unpin_host.argtypes = [C.c_void_p]
         L.pmpic_setup_count.restype = I64
         L.pmpic_setup_count.argtypes = [C.POINTER(ThermalParams)]
         L.pmpic_setup_thermal.argtypes = [C.POINTER(ThermalParams), I64] + [D] * 11

@@ -56,14 +56,17 @@ struct Geom {
 // cache_parcel_interp_weights (parcel_interpolation.F90:214-237) bit for bit:
 // i = floor((x-xmin)/dx)+1 and delx = ((x-xmin)-(i-1)dx)/dx with the halo
 // origin xmin = -2dx; the interior cell is i-3 (x), j-3 (y), k-1 (z).
-// Returns false for parcels outside the interior (the reference aborts, or for
-// the halo column i = Nx+3, loses the contribution).
+// A parcel one ulp below x = Lx is not wrapped by the parcel haloswap
+// (x < x_coords(Nx+3)) yet bins to the halo cell i = Nx+3 with delx = 0; the
+// reference then puts its weight on the halo point that par2grid_haloswap
+// folds onto x = 0, which is interior cell 0 here.  Anything else outside the
+// interior is an error (the reference aborts).
 __device__ __forceinline__ bool bin_parcel(const Geom& g, double xp, double yp, double zp, int& ci, int& cj,
                                            int& ck, double& delx, double& dely, double& delz) {
   double fi = floor(__ddiv_rn(__dsub_rn(xp, g.pxmin), g.dx));
   double fj = floor(__ddiv_rn(__dsub_rn(yp, g.pymin), g.dy));
   double fk = floor(__ddiv_rn(__dsub_rn(zp, g.pzmin), g.dz));
-  if (!(fi >= 2.0 && fi < 2.0 + g.Nx && fj >= 2.0 && fj < 2.0 + g.Ny && fk >= 0.0 && fk < (double)g.Nz))
+  if (!(fi >= 2.0 && fi <= 2.0 + g.Nx && fj >= 2.0 && fj <= 2.0 + g.Ny && fk >= 0.0 && fk < (double)g.Nz))
     return false;
   int i = (int)fi + 1, j = (int)fj + 1, k = (int)fk + 1;
   delx = __ddiv_rn(__dsub_rn(__dsub_rn(xp, g.pxmin), __dmul_rn((double)(i - 1), g.dx)), g.dx);
@@ -73,6 +76,8 @@ __device__ __forceinline__ bool bin_parcel(const Geom& g, double xp, double yp, 
   ci = i - 3;
   cj = j - 3;
   ck = k - 1;
+  if (ci == g.Nx) ci = 0;
+  if (cj == g.Ny) cj = 0;
   return true;
 }
 
@@ -93,6 +98,25 @@ struct DevInfo {
   int pad2;
 };
 
+// Named timers, after the reference's timer_mod handles (e.g.
+// parcel_interpolation.F90:144-148, pencilfft.F90:104-108, fft_ops.F90:157-160,
+// rk4_integrator.F90:71-75), backed by CUDA events on the context's stream.
+enum TimerId {
+  T_CACHE = 0, T_P2G, T_G2P, T_FFTF, T_FFTI, T_DIFFZ, T_LAPLINV, T_V2V, T_VT, T_RK4, T_HSWP, T_SPLIT,
+  T_MIX, T_STEP, T_NT
+};
+
+}  // namespace pmpic
+
+struct pmpic_ctx;
+namespace pmpic {
+struct TimerScope {
+  pmpic_ctx* c;
+  int id;
+  int e0;
+  TimerScope(pmpic_ctx* ctx, int id);
+  ~TimerScope();
+};
 }  // namespace pmpic
 
 // ---------------------------------------------------------------------------
@@ -146,6 +170,15 @@ struct pmpic_ctx {
   int counters[5];           // it_v2v, it_vt, rkstep, it_split, it_mix
   double dtm;
   pmpic_step_info info;
+  // instrumentation
+  int64_t nlaunch;           // kernels launched by this context
+  bool timing;               // named timers enabled
+  std::vector<cudaEvent_t> evpool;
+  std::vector<int> evfree;
+  std::vector<std::pair<int, int>> pending[pmpic::T_NT];
+  double tms[pmpic::T_NT];
+  int64_t tcalls[pmpic::T_NT];
+  cudaEvent_t marks[8];      // pmpic_event_record slots
 };
 
 namespace pmpic {

@@ -56,6 +56,51 @@ int sync_info(pmpic_ctx* ctx) {
   return 0;
 }
 
+static const char* kTimerNames[T_NT] = {"cache_weights", "par2grid", "grid2par", "fft_fwd_tot",
+                                        "fft_inv_tot",   "diffz",    "laplinv",  "vort2vel",
+                                        "vort_tend",     "RK4_all_steps", "Par_HSWP_entire", "splitting",
+                                        "mixing",        "step"};
+
+static int take_event(pmpic_ctx* c) {
+  if (c->evfree.empty()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return -1;
+    c->evpool.push_back(e);
+    return (int)c->evpool.size() - 1;
+  }
+  int i = c->evfree.back();
+  c->evfree.pop_back();
+  return i;
+}
+
+TimerScope::TimerScope(pmpic_ctx* ctx, int tid) : c(ctx), id(tid), e0(-1) {
+  if (!c->timing) return;
+  e0 = take_event(c);
+  if (e0 >= 0) cudaEventRecord(c->evpool[e0], c->stream);
+}
+TimerScope::~TimerScope() {
+  if (e0 < 0) return;
+  int e1 = take_event(c);
+  if (e1 < 0) return;
+  cudaEventRecord(c->evpool[e1], c->stream);
+  c->pending[id].push_back({e0, e1});
+}
+
+// fold recorded event pairs into the accumulated times
+static void drain_timers(pmpic_ctx* c) {
+  cudaStreamSynchronize(c->stream);
+  for (int t = 0; t < T_NT; ++t) {
+    for (auto& pr : c->pending[t]) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, c->evpool[pr.first], c->evpool[pr.second]) == cudaSuccess) c->tms[t] += ms;
+      c->tcalls[t] += 1;
+      c->evfree.push_back(pr.first);
+      c->evfree.push_back(pr.second);
+    }
+    c->pending[t].clear();
+  }
+}
+
 }  // namespace pmpic
 
 using namespace pmpic;
@@ -86,6 +131,9 @@ void free_all(pmpic_ctx* c) {
   for (int i = 0; i < PMPIC_NSPEC; ++i)
     if (c->spec[i]) cudaFree(c->spec[i]);
   if (c->hinfo) cudaFreeHost(c->hinfo);
+  for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
+  for (int i = 0; i < 8; ++i)
+    if (c->marks[i]) cudaEventDestroy(c->marks[i]);
   if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -241,6 +289,10 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
     e = cudaMemcpy(ctx->dinfo, &h, sizeof(DevInfo), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) rc = cuda_fail(ctx, e, "dinfo", __LINE__);
   }
+  for (int i = 0; i < 8 && !rc; ++i) {
+    e = cudaEventCreate(&ctx->marks[i]);
+    if (e != cudaSuccess) rc = cuda_fail(ctx, e, "cudaEventCreate", __LINE__);
+  }
   ctx->dtm = cfg->dtm;
   ctx->counters[0] = 0; ctx->counters[1] = 0; ctx->counters[2] = 1; ctx->counters[3] = 0; ctx->counters[4] = 0;
   std::memset(&ctx->info, 0, sizeof(ctx->info));
@@ -315,6 +367,8 @@ int pmpic_upload_parcels(pmpic_ctx* ctx, int64_t n, const double* x, const doubl
                       PMPIC_PROP_XF,   PMPIC_PROP_YF,   PMPIC_PROP_ZF,   PMPIC_PROP_PO,   PMPIC_PROP_QO,
                       PMPIC_PROP_RO,   PMPIC_PROP_PF,   PMPIC_PROP_QF,   PMPIC_PROP_RF};
   for (int pid : zero) PMPIC_CUDA(cudaMemsetAsync(prop(ctx, pid), 0, sizeof(double) * n, ctx->stream));
+  // a new state clears the sticky device error word
+  PMPIC_CUDA(cudaMemsetAsync(&ctx->dinfo->error, 0, sizeof(int), ctx->stream));
   PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
   ctx->n = n;
   ctx->info.n_parcels = n;
@@ -394,6 +448,7 @@ int pmpic_get_step_info(pmpic_ctx* ctx, pmpic_step_info* info) {
 // check the sticky device error word once per call.
 
 static int do_vort2vel(pmpic_ctx* ctx) {
+  TimerScope ts(ctx, T_V2V);
   int rc;
   // vort2vel.F90:117-121: binning and par2grid of p, q, r with one set of weights
   if ((rc = bin_and_sort(ctx))) return rc;
@@ -412,6 +467,7 @@ static int do_vort2vel(pmpic_ctx* ctx) {
 }
 
 static int do_vorticity_tendency(pmpic_ctx* ctx) {
+  TimerScope ts(ctx, T_VT);
   int rc;
   if ((rc = compute_btot(ctx))) return rc;  // :121-126
   // par2grid(btot) (:129) with the cell lists of this substep (positions
@@ -432,6 +488,7 @@ static int do_vorticity_tendency(pmpic_ctx* ctx) {
 }
 
 static int do_rk4(pmpic_ctx* ctx) {
+  TimerScope ts(ctx, T_RK4);
   int rc;
   if ((rc = rk4_stage(ctx, ctx->counters[2]))) return rc;
   ctx->counters[2] = ctx->counters[2] < 4 ? ctx->counters[2] + 1 : 1;  // rk4_integrator.F90:311-315
@@ -440,14 +497,20 @@ static int do_rk4(pmpic_ctx* ctx) {
 
 static int do_split(pmpic_ctx* ctx) {
   int rc = 0;
-  if (ctx->counters[3] % 4 == 3) rc = splitting(ctx);  // parcel_splitting.F90:59
+  if (ctx->counters[3] % 4 == 3) {  // parcel_splitting.F90:59
+    TimerScope ts(ctx, T_SPLIT);
+    rc = splitting(ctx);
+  }
   ctx->counters[3]++;
   return rc;
 }
 
 static int do_mix(pmpic_ctx* ctx) {
   int rc = 0;
-  if (ctx->counters[4] % 4 == 3) rc = mixing(ctx);  // parcel_mixing.F90:77
+  if (ctx->counters[4] % 4 == 3) {  // parcel_mixing.F90:77
+    TimerScope ts(ctx, T_MIX);
+    rc = mixing(ctx);
+  }
   ctx->counters[4]++;
   return rc;
 }
@@ -469,6 +532,7 @@ int pmpic_step(pmpic_ctx* ctx, int nsteps) {
   if (!ctx || nsteps < 0) return PMPIC_ERR_ARG;
   cudaSetDevice(ctx->device);
   for (int s = 0; s < nsteps; ++s) {
+    TimerScope ts(ctx, T_STEP);
     for (int sub = 0; sub < 4; ++sub) {
       int rc;
       if ((rc = do_vort2vel(ctx))) return rc;
@@ -585,6 +649,55 @@ int pmpic_op_parcel_haloswap(pmpic_ctx* ctx) {
   int rc = parcel_haloswap(ctx);
   if (rc) return rc;
   return sync_info(ctx);
+}
+
+// ---- instrumentation -------------------------------------------------------------
+int pmpic_timing(pmpic_ctx* ctx, int enable) {
+  if (!ctx) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  drain_timers(ctx);
+  for (int t = 0; t < T_NT; ++t) {
+    ctx->tms[t] = 0.0;
+    ctx->tcalls[t] = 0;
+  }
+  ctx->timing = enable != 0;
+  return PMPIC_OK;
+}
+int pmpic_timer_count(void) { return T_NT; }
+const char* pmpic_timer_name(int id) { return (id >= 0 && id < T_NT) ? kTimerNames[id] : ""; }
+int pmpic_timer_read(pmpic_ctx* ctx, int id, double* total_ms, int64_t* calls) {
+  if (!ctx || id < 0 || id >= T_NT) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  drain_timers(ctx);
+  if (total_ms) *total_ms = ctx->tms[id];
+  if (calls) *calls = ctx->tcalls[id];
+  return PMPIC_OK;
+}
+int pmpic_launch_count(pmpic_ctx* ctx, int64_t* n) {
+  if (!ctx || !n) return PMPIC_ERR_ARG;
+  *n = ctx->nlaunch;
+  return PMPIC_OK;
+}
+int pmpic_event_record(pmpic_ctx* ctx, int slot) {
+  if (!ctx || slot < 0 || slot >= 8) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  PMPIC_CUDA(cudaEventRecord(ctx->marks[slot], ctx->stream));
+  return PMPIC_OK;
+}
+int pmpic_event_elapsed(pmpic_ctx* ctx, int a, int b, float* ms) {
+  if (!ctx || a < 0 || a >= 8 || b < 0 || b >= 8 || !ms) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  PMPIC_CUDA(cudaEventSynchronize(ctx->marks[b]));
+  PMPIC_CUDA(cudaEventElapsedTime(ms, ctx->marks[a], ctx->marks[b]));
+  return PMPIC_OK;
+}
+int pmpic_pin_host(void* ptr, size_t bytes) {
+  if (!ptr || bytes == 0) return PMPIC_ERR_ARG;
+  return cudaHostRegister(ptr, bytes, cudaHostRegisterDefault) == cudaSuccess ? PMPIC_OK : PMPIC_ERR_CUDA;
+}
+int pmpic_unpin_host(void* ptr) {
+  if (!ptr) return PMPIC_ERR_ARG;
+  return cudaHostUnregister(ptr) == cudaSuccess ? PMPIC_OK : PMPIC_ERR_CUDA;
 }
 
 }  // extern "C"

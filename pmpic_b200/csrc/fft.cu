@@ -358,6 +358,7 @@ int fft_init(pmpic_ctx* ctx) {
 }
 
 int fft_forward(pmpic_ctx* ctx, const double* phys, double* spec) {
+  TimerScope ts(ctx, T_FFTF);
   const Geom& g = ctx->g;
   const FftPlan& px = ctx->plan_x;
   const FftPlan& py = ctx->plan_y;
@@ -365,17 +366,18 @@ int fft_forward(pmpic_ctx* ctx, const double* phys, double* spec) {
   int txf = pick_txf(g.Nx);
   size_t sm_y = sizeof(double2) * (size_t)(txf / 2) * g.Ny * 2;
   dim3 gy(g.Nx / txf, g.nzp);
-  k_fwd_y<<<gy, FFT_THREADS, sm_y, ctx->stream>>>(g, txf, py, tw + ctx->ftw_off_y, phys, ctx->fftmid);
+  k_fwd_y<<<gy, FFT_THREADS, sm_y, ctx->stream>>>(g, txf, py, tw + ctx->ftw_off_y, phys, ctx->fftmid); ++ctx->nlaunch;
   int rp = pick_rp(g.Nx);
   int64_t nrows = (int64_t)g.nzp * g.sy;
   size_t sm_x = sizeof(double2) * (size_t)rp * g.Nx * 2;
   k_fwd_x<<<(unsigned)((nrows + 2 * rp - 1) / (2 * rp)), FFT_THREADS, sm_x, ctx->stream>>>(g, rp, nrows, px, tw,
-                                                                                        ctx->fftmid, spec);
+                                                                                        ctx->fftmid, spec); ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
 
 int fft_backward(pmpic_ctx* ctx, const double* spec, double* phys) {
+  TimerScope ts(ctx, T_FFTI);
   const Geom& g = ctx->g;
   const FftPlan& px = ctx->plan_x;
   const FftPlan& py = ctx->plan_y;
@@ -384,12 +386,12 @@ int fft_backward(pmpic_ctx* ctx, const double* spec, double* phys) {
   int64_t nrows = (int64_t)g.nzp * g.sy;
   size_t sm_x = sizeof(double2) * (size_t)rp * g.Nx * 2;
   k_inv_x<<<(unsigned)((nrows + 2 * rp - 1) / (2 * rp)), FFT_THREADS, sm_x, ctx->stream>>>(g, rp, nrows, px, tw,
-                                                                                        spec, ctx->fftmid);
+                                                                                        spec, ctx->fftmid); ++ctx->nlaunch;
   int txf = pick_txf(g.Nx);
   size_t half = (size_t)g.Ny / 2 + 1;
   size_t sm_y = sizeof(double2) * std::max((size_t)(txf / 2) * g.Ny * 2, (size_t)(txf / 2) * g.Ny + txf * half);
   dim3 gy(g.Nx / txf, g.nzp);
-  k_inv_y<<<gy, FFT_THREADS, sm_y, ctx->stream>>>(g, txf, py, tw + ctx->ftw_off_y, ctx->fftmid, phys);
+  k_inv_y<<<gy, FFT_THREADS, sm_y, ctx->stream>>>(g, txf, py, tw + ctx->ftw_off_y, ctx->fftmid, phys); ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }

@@ -346,27 +346,30 @@ inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 int scan_excl(pmpic_ctx* ctx, const int32_t* in, int64_t n, int32_t* out) {
   int64_t ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
   int32_t* sums = (int32_t*)ctx->scan_tmp;
-  k_scan_tiles<<<(unsigned)ntiles, SCAN_BLOCK, 0, ctx->stream>>>(in, n, sums);
-  k_scan_sums<<<1, SCAN_BLOCK, 0, ctx->stream>>>(sums, ntiles, out + n);
-  k_scan_apply<<<(unsigned)ntiles, SCAN_BLOCK, 0, ctx->stream>>>(in, n, sums, out);
+  k_scan_tiles<<<(unsigned)ntiles, SCAN_BLOCK, 0, ctx->stream>>>(in, n, sums); ++ctx->nlaunch;
+  k_scan_sums<<<1, SCAN_BLOCK, 0, ctx->stream>>>(sums, ntiles, out + n); ++ctx->nlaunch;
+  k_scan_apply<<<(unsigned)ntiles, SCAN_BLOCK, 0, ctx->stream>>>(in, n, sums, out); ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
 
 int bin_and_sort(pmpic_ctx* ctx) {
+  TimerScope ts(ctx, T_CACHE);
   const Geom& g = ctx->g;
   const int64_t n = ctx->n;
   PMPIC_CUDA(cudaMemsetAsync(ctx->cell_count, 0, sizeof(int32_t) * (g.ncell + 1), ctx->stream));
   PMPIC_CUDA(cudaMemsetAsync(ctx->cell_fill, 0, sizeof(int32_t) * g.ncell, ctx->stream));
-  if (n > 0)
+  if (n > 0) {
     k_bin_count<<<nblk(n, 256), 256, 0, ctx->stream>>>(g, n, prop(ctx, PMPIC_PROP_X), prop(ctx, PMPIC_PROP_Y),
                                                        prop(ctx, PMPIC_PROP_Z), ctx->cell, ctx->cell_count,
-                                                       ctx->dinfo);
+                                                       ctx->dinfo); ++ctx->nlaunch;
+  }
   int rc = scan_excl(ctx, ctx->cell_count, g.ncell, ctx->cell_start);
   if (rc) return rc;
-  if (n > 0)
+  if (n > 0) {
     k_bin_scatter<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, ctx->cell, ctx->cell_start, ctx->cell_fill,
-                                                         ctx->sorted);
+                                                         ctx->sorted); ++ctx->nlaunch;
+  }
   PMPIC_CUDA(cudaGetLastError());
   ctx->sorted_valid = true;
   return 0;
@@ -374,6 +377,7 @@ int bin_and_sort(pmpic_ctx* ctx) {
 
 template <int NQ, int MODE = 0>
 static int launch_p2g(pmpic_ctx* ctx, const double* const* fields, double* const* out) {
+  TimerScope ts(ctx, T_P2G);
   const Geom& g = ctx->g;
   P2GArgs<NQ> a;
   for (int q = 0; q < NQ; ++q) {
@@ -385,7 +389,7 @@ static int launch_p2g(pmpic_ctx* ctx, const double* const* fields, double* const
   dim3 grid((g.Nx + TILE - 1) / TILE, (g.Ny + TILE - 1) / TILE, (g.nzp + ZCHUNK - 1) / ZCHUNK);
   k_par2grid<NQ, MODE><<<grid, P2G_THREADS, 0, ctx->stream>>>(g, ctx->cell_start, ctx->sorted,
                                                               prop(ctx, PMPIC_PROP_X), prop(ctx, PMPIC_PROP_Y),
-                                                              prop(ctx, PMPIC_PROP_Z), prop(ctx, PMPIC_PROP_VOL), a);
+                                                              prop(ctx, PMPIC_PROP_Z), prop(ctx, PMPIC_PROP_VOL), a); ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
@@ -416,6 +420,7 @@ int par2grid_multi(pmpic_ctx* ctx, const double* const* fields, int nf, double* 
 
 template <int NG>
 static int launch_g2p(pmpic_ctx* ctx, const double* const* grids, double* const* out) {
+  TimerScope ts(ctx, T_G2P);
   const Geom& g = ctx->g;
   if (ctx->n == 0) return 0;
   G2PArgs<NG> a;
@@ -425,7 +430,7 @@ static int launch_g2p(pmpic_ctx* ctx, const double* const* grids, double* const*
   }
   k_grid2par<NG><<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(g, ctx->n, prop(ctx, PMPIC_PROP_X),
                                                               prop(ctx, PMPIC_PROP_Y), prop(ctx, PMPIC_PROP_Z), a,
-                                                              ctx->dinfo);
+                                                              ctx->dinfo); ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
@@ -443,7 +448,7 @@ int cell_ids(pmpic_ctx* ctx, int32_t* dcells) {
   if (ctx->n == 0) return 0;
   k_cell_only<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, prop(ctx, PMPIC_PROP_X),
                                                           prop(ctx, PMPIC_PROP_Y), prop(ctx, PMPIC_PROP_Z), dcells,
-                                                          ctx->dinfo);
+                                                          ctx->dinfo); ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }

@@ -486,10 +486,10 @@ static int compact(pmpic_ctx* ctx, Pred pr, int64_t n, int32_t* list, int32_t* d
   }
   int32_t* cnt = ctx->aux2;            // nb + 1 (nb + 1 <= nbmax)
   int32_t* off = ctx->aux2 + ctx->nbmax;
-  k_count<<<(unsigned)nb, CB, 0, ctx->stream>>>(pr, n, cnt);
+  k_count<<<(unsigned)nb, CB, 0, ctx->stream>>>(pr, n, cnt); ++ctx->nlaunch;
   int rc = scan_excl(ctx, cnt, nb, off);
   if (rc) return rc;
-  k_write<<<(unsigned)nb, CB, 0, ctx->stream>>>(pr, n, off, list);
+  k_write<<<(unsigned)nb, CB, 0, ctx->stream>>>(pr, n, off, list); ++ctx->nlaunch;
   PMPIC_CUDA(cudaMemcpyAsync(dcount, off + nb, sizeof(int32_t), cudaMemcpyDeviceToDevice, ctx->stream));
   PMPIC_CUDA(cudaGetLastError());
   return 0;
@@ -501,7 +501,7 @@ static int32_t* dcounter(pmpic_ctx* ctx, int i) { return (int32_t*)(ctx->dinfo +
 int compute_btot(pmpic_ctx* ctx) {
   if (ctx->n == 0) return 0;
   k_btot<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->n, prop(ctx, PMPIC_PROP_B), prop(ctx, PMPIC_PROP_H),
-                                                     prop(ctx, PMPIC_PROP_Z), prop(ctx, PMPIC_PROP_BTOT));
+                                                     prop(ctx, PMPIC_PROP_Z), prop(ctx, PMPIC_PROP_BTOT)); ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
@@ -519,31 +519,32 @@ int rk4_stage(pmpic_ctx* ctx, int stage) {
     P.f[v] = prop(ctx, F[v]);
     P.d[v] = prop(ctx, D[v]);
   }
-  k_rk4<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->n, P, stage, &ctx->dinfo->dtm);
+  k_rk4<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->n, P, stage, &ctx->dinfo->dtm); ++ctx->nlaunch;
   ctx->sorted_valid = false;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
 
 int parcel_haloswap(pmpic_ctx* ctx) {
+  TimerScope ts(ctx, T_HSWP);
   const int64_t n = ctx->n;
   ctx->sorted_valid = false;
   if (n == 0) return 0;
   k_reflect_classify<<<nblk(n, 256), 256, 0, ctx->stream>>>(ctx->g, n, prop(ctx, PMPIC_PROP_X),
                                                             prop(ctx, PMPIC_PROP_Y), prop(ctx, PMPIC_PROP_Z),
-                                                            ctx->dir);
+                                                            ctx->dir); ++ctx->nlaunch;
   int32_t* V = ctx->aux;                 // vacated slots, ascending
   int32_t* M = ctx->keep;                // moved parcels in send order (keep is free outside mixing)
   int32_t* nm = dcounter(ctx, 0);
   int rc = compact(ctx, PredDirNZ{ctx->dir}, n, V, nm);
   if (rc) return rc;
-  k_partition_dirs<<<1, 1024, 0, ctx->stream>>>(V, nm, ctx->dir, M);
+  k_partition_dirs<<<1, 1024, 0, ctx->stream>>>(V, nm, ctx->dir, M); ++ctx->nlaunch;
   // the staging buffer is bounded: on overflow nothing moves and the call
   // reports PMPIC_ERR_CAPACITY
   int32_t* nmc = dcounter(ctx, 1);
-  k_check_swapcap<<<1, 1, 0, ctx->stream>>>(nm, nmc, ctx->swapcap, ctx->dinfo);
-  k_swap_gather<<<592, 256, 0, ctx->stream>>>(ctx->g, nmc, M, ctx->dir, ctx->parcels, ctx->cap, ctx->swapbuf);
-  k_swap_scatter<<<592, 256, 0, ctx->stream>>>(nmc, V, ctx->swapbuf, ctx->parcels, ctx->cap);
+  k_check_swapcap<<<1, 1, 0, ctx->stream>>>(nm, nmc, ctx->swapcap, ctx->dinfo); ++ctx->nlaunch;
+  k_swap_gather<<<592, 256, 0, ctx->stream>>>(ctx->g, nmc, M, ctx->dir, ctx->parcels, ctx->cap, ctx->swapbuf); ++ctx->nlaunch;
+  k_swap_scatter<<<592, 256, 0, ctx->stream>>>(nmc, V, ctx->swapbuf, ctx->parcels, ctx->cap); ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
@@ -554,10 +555,10 @@ int splitting(pmpic_ctx* ctx) {
   int32_t* list = ctx->keep;
   int32_t* ns = dcounter(ctx, 2);
   if (n > 0) {
-    k_split_flag<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, ctx->parcels, ctx->cap, &ctx->dinfo->dtm, flag);
+    k_split_flag<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, ctx->parcels, ctx->cap, &ctx->dinfo->dtm, flag); ++ctx->nlaunch;
     int rc = compact(ctx, PredFlag{flag}, n, list, ns);
     if (rc) return rc;
-    k_split_apply<<<592, 256, 0, ctx->stream>>>(n, list, ns, ctx->parcels, ctx->cap, ctx->dinfo);
+    k_split_apply<<<592, 256, 0, ctx->stream>>>(n, list, ns, ctx->parcels, ctx->cap, ctx->dinfo); ++ctx->nlaunch;
   } else {
     PMPIC_CUDA(cudaMemsetAsync(ns, 0, sizeof(int32_t), ctx->stream));
   }
@@ -576,8 +577,9 @@ int mixing(pmpic_ctx* ctx) {
   const int64_t norig = ctx->n;
   int rc;
   // keep flags (:488) and the kept / residual grids (construct_grids :440-624)
-  if (norig > 0)
-    k_keep<<<nblk(norig, 256), 256, 0, ctx->stream>>>(norig, prop(ctx, PMPIC_PROP_VOL), g.vmin, ctx->keep);
+  if (norig > 0) {
+    k_keep<<<nblk(norig, 256), 256, 0, ctx->stream>>>(norig, prop(ctx, PMPIC_PROP_VOL), g.vmin, ctx->keep); ++ctx->nlaunch;
+  }
   if ((rc = bin_and_sort(ctx))) return rc;
   if ((rc = launch_mix_grids(ctx))) return rc;
   // removed slots Z (ascending) and under-populated cells in loop order
@@ -592,16 +594,17 @@ int mixing(pmpic_ctx* ctx) {
                   ctx->grid[PMPIC_GRID_P],   ctx->grid[PMPIC_GRID_Q], ctx->grid[PMPIC_GRID_R]};
   k_new_parcels<<<592, 256, 0, ctx->stream>>>(g, olist, nnew, zlist, nz0, norig, ctx->cap, ctx->keep, ctx->parcels,
                                               K[0], K[1], K[2], K[3], K[4], K[5], ctx->newslot, ctx->newportion,
-                                              ctx->dinfo);
+                                              ctx->dinfo); ++ctx->nlaunch;
   ResPtrs RP;
   for (int q = 0; q < 6; ++q) {
     RP.r[q] = ctx->mixres[q];
     RP.k[q] = K[q];
   }
-  k_residual_update<<<nblk(g.nphys, 256), 256, 0, ctx->stream>>>(g, RP, ctx->newslot, ctx->newportion);
-  if (norig > 0)
+  k_residual_update<<<nblk(g.nphys, 256), 256, 0, ctx->stream>>>(g, RP, ctx->newslot, ctx->newportion); ++ctx->nlaunch;
+  if (norig > 0) {
     k_redistribute<<<nblk(norig, 256), 256, 0, ctx->stream>>>(g, norig, ctx->keep, ctx->parcels, ctx->cap, RP,
-                                                              ctx->dinfo);
+                                                              ctx->dinfo); ++ctx->nlaunch;
+  }
   // counts to the host: removed, new cells
   int32_t h[2];
   PMPIC_CUDA(cudaMemcpyAsync(&h[0], nz0, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
@@ -624,7 +627,7 @@ int mixing(pmpic_ctx* ctx) {
     int32_t* no = dcounter(ctx, 6);
     if ((rc = compact(ctx, PredKeepEq{ctx->keep, 0}, norig, z2, nz2))) return rc;
     if ((rc = compact(ctx, PredKeepEq{ctx->keep, 1}, norig, ones, no))) return rc;
-    k_backfill<<<592, 256, 0, ctx->stream>>>(z2, nz2, ones, no, ctx->parcels, ctx->cap, ctx->dinfo);
+    k_backfill<<<592, 256, 0, ctx->stream>>>(z2, nz2, ones, no, ctx->parcels, ctx->cap, ctx->dinfo); ++ctx->nlaunch;
     int32_t hz = 0;
     PMPIC_CUDA(cudaMemcpyAsync(&hz, nz2, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
     PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));

@@ -413,11 +413,12 @@ static int diffz_coef(pmpic_ctx* ctx, bool bt, std::vector<double>& out) {
 }
 
 static int diffz_launch(pmpic_ctx* ctx, const double* in, double* out, const double* bot, const double* top) {
+  TimerScope ts(ctx, T_DIFFZ);
   const Geom& g = ctx->g;
   int which = bot ? 1 : 0;
   double* coef = ctx->sscratch + g.nspec;  // 2 x 3*nzp doubles after the cp scratch
   coef += which * 3 * g.nzp;
-  k_diffz<<<nblk((int64_t)g.sx * g.sy, 128), 128, 0, ctx->stream>>>(g, in, out, coef, bot, top, f4div(1.f, 6.f));
+  k_diffz<<<nblk((int64_t)g.sx * g.sy, 128), 128, 0, ctx->stream>>>(g, in, out, coef, bot, top, f4div(1.f, 6.f)); ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
@@ -436,17 +437,17 @@ int spectral_init(pmpic_ctx* ctx) {
 }
 
 int spec_diffx(pmpic_ctx* ctx, const double* in, double* out) {
-  k_diffx<<<nblk(ctx->g.nspec, 256), 256, 0, ctx->stream>>>(ctx->g, in, out, ctx->kx);
+  k_diffx<<<nblk(ctx->g.nspec, 256), 256, 0, ctx->stream>>>(ctx->g, in, out, ctx->kx); ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
 int spec_diffy(pmpic_ctx* ctx, const double* in, double* out) {
-  k_diffy<<<nblk(ctx->g.nspec, 256), 256, 0, ctx->stream>>>(ctx->g, in, out, ctx->ky);
+  k_diffy<<<nblk(ctx->g.nspec, 256), 256, 0, ctx->stream>>>(ctx->g, in, out, ctx->ky); ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
 int spec_filter(pmpic_ctx* ctx, const double* in, double* out) {
-  k_filter<<<nblk(ctx->g.nspec, 256), 256, 0, ctx->stream>>>(ctx->g, in, out, ctx->filt);
+  k_filter<<<nblk(ctx->g.nspec, 256), 256, 0, ctx->stream>>>(ctx->g, in, out, ctx->filt); ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
@@ -454,8 +455,9 @@ int spec_diffz(pmpic_ctx* ctx, const double* in, double* out, const double* bot,
   return diffz_launch(ctx, in, out, bot, top);
 }
 int spec_laplinv(pmpic_ctx* ctx, double* inout, bool df0) {
+  TimerScope ts(ctx, T_LAPLINV);
   const Geom& g = ctx->g;
-  k_laplinv<<<nblk((int64_t)g.sx * g.sy, 128), 128, 0, ctx->stream>>>(g, inout, ctx->sscratch, ctx->k2, df0 ? 1 : 0);
+  k_laplinv<<<nblk((int64_t)g.sx * g.sy, 128), 128, 0, ctx->stream>>>(g, inout, ctx->sscratch, ctx->k2, df0 ? 1 : 0); ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
@@ -473,18 +475,18 @@ int vort2vel_spectral(pmpic_ctx* ctx) {
   if ((rc = fft_forward(ctx, ctx->grid[PMPIC_GRID_Q], b))) return rc;
   if ((rc = fft_forward(ctx, ctx->grid[PMPIC_GRID_R], c))) return rc;
   const double hdzi = f4div(1.f, 2.f) / g.dz;
-  k_div<<<nb, 256, 0, ctx->stream>>>(g, a, b, c, f, ctx->kx, ctx->ky, hdzi);
+  k_div<<<nb, 256, 0, ctx->stream>>>(g, a, b, c, f, ctx->kx, ctx->ky, hdzi); ++ctx->nlaunch;
   if ((rc = spec_laplinv(ctx, f, true))) return rc;
-  k_filter<<<nb, 256, 0, ctx->stream>>>(g, f, f, ctx->filt);
-  k_sub_diff<<<nb, 256, 0, ctx->stream>>>(g, a, f, ctx->kx, 0);
-  k_sub_diff<<<nb, 256, 0, ctx->stream>>>(g, b, f, ctx->ky, 1);
+  k_filter<<<nb, 256, 0, ctx->stream>>>(g, f, f, ctx->filt); ++ctx->nlaunch;
+  k_sub_diff<<<nb, 256, 0, ctx->stream>>>(g, a, f, ctx->kx, 0); ++ctx->nlaunch;
+  k_sub_diff<<<nb, 256, 0, ctx->stream>>>(g, b, f, ctx->ky, 1); ++ctx->nlaunch;
   if ((rc = diffz_launch(ctx, f, d, nullptr, nullptr))) return rc;
-  k_sub_zero0<<<nb, 256, 0, ctx->stream>>>(g, c, d);
-  k_filter3_bt<<<nb, 256, 0, ctx->stream>>>(g, a, b, c, d, e, f, ctx->filt, ctx->bt);
+  k_sub_zero0<<<nb, 256, 0, ctx->stream>>>(g, c, d); ++ctx->nlaunch;
+  k_filter3_bt<<<nb, 256, 0, ctx->stream>>>(g, a, b, c, d, e, f, ctx->filt, ctx->bt); ++ctx->nlaunch;
   if ((rc = fft_backward(ctx, d, ctx->grid[PMPIC_GRID_P]))) return rc;
   if ((rc = fft_backward(ctx, e, ctx->grid[PMPIC_GRID_Q]))) return rc;
   if ((rc = fft_backward(ctx, f, ctx->grid[PMPIC_GRID_R]))) return rc;
-  k_zmode<<<1, 32, 0, ctx->stream>>>(g, d, e, ctx->zmode);
+  k_zmode<<<1, 32, 0, ctx->stream>>>(g, d, e, ctx->zmode); ++ctx->nlaunch;
   if ((rc = spec_laplinv(ctx, a, false))) return rc;
   if ((rc = spec_laplinv(ctx, b, false))) return rc;
   if ((rc = spec_laplinv(ctx, c, true))) return rc;
@@ -495,16 +497,16 @@ int vort2vel_spectral(pmpic_ctx* ctx) {
   // u = dB/dz - dC/dy
   if ((rc = diffz_launch(ctx, b, e, bbot, btop))) return rc;
   k_vel<<<nb, 256, 0, ctx->stream>>>(g, 0, e, c, a, b, f, ctx->spec[PMPIC_SPEC_U], ctx->kx, ctx->ky, ctx->filt,
-                                     ctx->zmode);
+                                     ctx->zmode); ++ctx->nlaunch;
   if ((rc = fft_backward(ctx, f, ctx->grid[PMPIC_GRID_U]))) return rc;
   // v = dC/dx - dA/dz
   if ((rc = diffz_launch(ctx, a, e, abot, atop))) return rc;
   k_vel<<<nb, 256, 0, ctx->stream>>>(g, 1, e, c, a, b, f, ctx->spec[PMPIC_SPEC_V], ctx->kx, ctx->ky, ctx->filt,
-                                     ctx->zmode + g.nzp);
+                                     ctx->zmode + g.nzp); ++ctx->nlaunch;
   if ((rc = fft_backward(ctx, f, ctx->grid[PMPIC_GRID_V]))) return rc;
   // w = dA/dy - dB/dx
   k_vel<<<nb, 256, 0, ctx->stream>>>(g, 2, e, c, a, b, f, ctx->spec[PMPIC_SPEC_W], ctx->kx, ctx->ky, ctx->filt,
-                                     ctx->zmode);
+                                     ctx->zmode); ++ctx->nlaunch;
   if ((rc = fft_backward(ctx, f, ctx->grid[PMPIC_GRID_W]))) return rc;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
@@ -526,25 +528,25 @@ int vorticity_tendency_grids(pmpic_ctx* ctx) {
   if ((rc = fft_backward(ctx, as, DP))) return rc;
   if ((rc = spec_diffx(ctx, ctx->spec[PMPIC_SPEC_U], as))) return rc;
   if ((rc = fft_backward(ctx, as, dudx))) return rc;
-  k_pw_add_mul<<<nb, 256, 0, ctx->stream>>>(n, DP, P, dudx);
+  k_pw_add_mul<<<nb, 256, 0, ctx->stream>>>(n, DP, P, dudx); ++ctx->nlaunch;
   if ((rc = spec_diffy(ctx, ctx->spec[PMPIC_SPEC_U], as))) return rc;
   if ((rc = fft_backward(ctx, as, ap))) return rc;
-  k_pw_add_mul<<<nb, 256, 0, ctx->stream>>>(n, DP, Q, ap);
+  k_pw_add_mul<<<nb, 256, 0, ctx->stream>>>(n, DP, Q, ap); ++ctx->nlaunch;
   if ((rc = spec_diffx(ctx, ctx->spec[PMPIC_SPEC_W], as))) return rc;
   if ((rc = fft_backward(ctx, as, dwdx))) return rc;
-  k_pw_add_mul_sum<<<nb, 256, 0, ctx->stream>>>(n, DP, R, Q, dwdx);
+  k_pw_add_mul_sum<<<nb, 256, 0, ctx->stream>>>(n, DP, R, Q, dwdx); ++ctx->nlaunch;
   if ((rc = spec_diffx(ctx, bs, as))) return rc;
   if ((rc = fft_backward(ctx, as, DQ))) return rc;
   if ((rc = spec_diffx(ctx, ctx->spec[PMPIC_SPEC_V], as))) return rc;
   if ((rc = fft_backward(ctx, as, ap))) return rc;
-  k_pw_neg_add_mul<<<nb, 256, 0, ctx->stream>>>(n, DQ, P, ap);
+  k_pw_neg_add_mul<<<nb, 256, 0, ctx->stream>>>(n, DQ, P, ap); ++ctx->nlaunch;
   if ((rc = spec_diffy(ctx, ctx->spec[PMPIC_SPEC_V], as))) return rc;
   if ((rc = fft_backward(ctx, as, dvdy))) return rc;
-  k_pw_add_mul<<<nb, 256, 0, ctx->stream>>>(n, DQ, Q, dvdy);
+  k_pw_add_mul<<<nb, 256, 0, ctx->stream>>>(n, DQ, Q, dvdy); ++ctx->nlaunch;
   if ((rc = spec_diffy(ctx, ctx->spec[PMPIC_SPEC_W], as))) return rc;
   if ((rc = fft_backward(ctx, as, dwdy))) return rc;
-  k_pw_add_mul_negsum<<<nb, 256, 0, ctx->stream>>>(n, DQ, R, P, dwdy);
-  k_pw_dr<<<nb, 256, 0, ctx->stream>>>(n, DR, P, Q, R, dwdx, dwdy, dudx, dvdy);
+  k_pw_add_mul_negsum<<<nb, 256, 0, ctx->stream>>>(n, DQ, R, P, dwdy); ++ctx->nlaunch;
+  k_pw_dr<<<nb, 256, 0, ctx->stream>>>(n, DR, P, Q, R, dwdx, dwdy, dudx, dvdy); ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
@@ -555,14 +557,14 @@ int field_max(pmpic_ctx* ctx, bool v2v, bool vt) {
   if (v2v) {
     PMPIC_CUDA(cudaMemsetAsync(&ctx->dinfo->umax2, 0, 3 * sizeof(double), ctx->stream));
     k_max_sq3<<<592, 256, 0, ctx->stream>>>(g.nphys, ctx->grid[PMPIC_GRID_U], ctx->grid[PMPIC_GRID_V],
-                                            ctx->grid[PMPIC_GRID_W], &ctx->dinfo->umax2);
-    k_dt_velocity<<<1, 1, 0, ctx->stream>>>(g, ctx->dinfo, ctx->cfg.dtmax);
+                                            ctx->grid[PMPIC_GRID_W], &ctx->dinfo->umax2); ++ctx->nlaunch;
+    k_dt_velocity<<<1, 1, 0, ctx->stream>>>(g, ctx->dinfo, ctx->cfg.dtmax); ++ctx->nlaunch;
   }
   if (vt) {
     PMPIC_CUDA(cudaMemsetAsync(&ctx->dinfo->omax2, 0, sizeof(double), ctx->stream));
     k_max_vort<<<592, 256, 0, ctx->stream>>>(g.nphys, ctx->grid[PMPIC_GRID_P], ctx->grid[PMPIC_GRID_Q],
-                                             ctx->grid[PMPIC_GRID_R], &ctx->dinfo->omax2);
-    k_dt_vorticity<<<1, 1, 0, ctx->stream>>>(ctx->dinfo, ctx->cfg.timestep_prefactor, ctx->cfg.dtmax);
+                                             ctx->grid[PMPIC_GRID_R], &ctx->dinfo->omax2); ++ctx->nlaunch;
+    k_dt_vorticity<<<1, 1, 0, ctx->stream>>>(ctx->dinfo, ctx->cfg.timestep_prefactor, ctx->cfg.dtmax); ++ctx->nlaunch;
   }
   PMPIC_CUDA(cudaGetLastError());
   return 0;
