@@ -33,6 +33,8 @@ struct FftPlan {
   int nst;
   int radix[FFT_MAX_STAGES];
   int tw_off[FFT_MAX_STAGES];  // offset (in double2) of each stage's twiddle table
+  int n1, n2;                  // four-step split n = n1 * n2 (0: generic Stockham path)
+  int tw4_off;                 // offset of the four-step twiddles W_n^(n2 k1), [n2 * n1 + k1]
 };
 
 // Geometry of one rank covering the whole domain (setup_grid.F90:45-104,
@@ -133,7 +135,13 @@ struct pmpic_ctx {
   int64_t n;                 // numparcels (host mirror, valid between calls)
   double* parcels;           // NPROP * cap
   int32_t* cell;             // cap: interior cell id per slot
-  bool sorted_valid;         // cell lists match the current positions
+  double* del;               // 3 x cap: cached delx, dely, delz per slot
+  bool sorted_valid;         // cell ids, offsets and cell lists match the current positions
+  bool btot_grid_ready;      // gspare holds par2grid(btot) of the current substep
+  bool pending_uvw;          // vort2vel's grid2par of u, v, w not yet applied
+  bool pending_pqr;          // vorticity_tendency's grid2par of dp, dq, dr not yet applied
+  bool dir_ready;            // dir[] and the z reflection done for the current positions
+  double* gspare;            // spare physical grid
   int32_t* sorted;           // cap: slot indices sorted by cell
   int32_t* cell_count;       // ncell + 1
   int32_t* cell_start;       // ncell + 1
@@ -210,5 +218,6 @@ int parcel_haloswap(pmpic_ctx* ctx);
 int splitting(pmpic_ctx* ctx);
 int mixing(pmpic_ctx* ctx);
 int compute_btot(pmpic_ctx* ctx);
+int flush_gathers(pmpic_ctx* ctx);
 int sync_info(pmpic_ctx* ctx);
 }  // namespace pmpic

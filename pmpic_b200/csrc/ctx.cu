@@ -115,7 +115,7 @@ int dalloc(pmpic_ctx* ctx, T** p, size_t count) {
 }
 
 void free_all(pmpic_ctx* c) {
-  void* ptrs[] = {c->parcels, c->cell,     c->sorted,    c->cell_count, c->cell_start, c->cell_fill, c->keep,
+  void* ptrs[] = {c->parcels, c->cell,     c->del,       c->gspare,     c->sorted,    c->cell_count, c->cell_start, c->cell_fill, c->keep,
                   c->aux,     c->aux2,     c->dir,       c->swapbuf,    c->scan_tmp,   c->npercell,  c->newslot,
                   c->newportion, c->sa,    c->sb,        c->sc,         c->sd,         c->se,        c->sf,
                   c->sas,     c->sbs,      c->sscratch,  c->fftmid,     c->ftw,        c->kx,        c->ky,
@@ -221,6 +221,8 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   ctx->cap = cfg->max_parcels;
   ctx->n = 0;
   ctx->sorted_valid = false;
+  ctx->btot_grid_ready = false;
+  ctx->pending_uvw = ctx->pending_pqr = ctx->dir_ready = false;
   ctx->nbmax = (std::max<int64_t>(ctx->cap, g.ncell) + 1023) / 1024 + 8;
   int64_t sc = 2LL * (g.Nx + g.Ny) * (int64_t)g.nzp * 32;
   ctx->swapcap = std::min<int64_t>(ctx->cap, std::max<int64_t>(1 << 20, sc));
@@ -230,6 +232,8 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   const size_t cap = (size_t)ctx->cap;
   if (!rc) rc = dalloc(ctx, &ctx->parcels, (size_t)PMPIC_NPROP * cap);
   if (!rc) rc = dalloc(ctx, &ctx->cell, cap);
+  if (!rc) rc = dalloc(ctx, &ctx->del, 3 * cap);
+  if (!rc) rc = dalloc(ctx, &ctx->gspare, (size_t)g.nphys);
   if (!rc) rc = dalloc(ctx, &ctx->sorted, cap);
   if (!rc) rc = dalloc(ctx, &ctx->keep, cap);
   if (!rc) rc = dalloc(ctx, &ctx->aux, cap);
@@ -319,9 +323,14 @@ const char* pmpic_last_error(const pmpic_ctx* ctx) { return ctx ? ctx->err.c_str
 int pmpic_set_count(pmpic_ctx* ctx, int64_t n) {
   if (!ctx) return PMPIC_ERR_ARG;
   if (n < 0 || n > ctx->cap) return set_error(ctx, PMPIC_ERR_CAPACITY, "parcel count exceeds max_parcels");
+  cudaSetDevice(ctx->device);
+  int frc = flush_gathers(ctx);
+  if (frc) return frc;
   ctx->n = n;
   ctx->info.n_parcels = n;
   ctx->sorted_valid = false;
+  ctx->btot_grid_ready = false;
+  ctx->dir_ready = false;
   return PMPIC_OK;
 }
 int pmpic_get_count(pmpic_ctx* ctx, int64_t* n) {
@@ -333,14 +342,20 @@ int pmpic_get_count(pmpic_ctx* ctx, int64_t* n) {
 int pmpic_set_property(pmpic_ctx* ctx, int p, int64_t n, const double* src) {
   if (!ctx || p < 0 || p >= PMPIC_NPROP || n < 0 || n > ctx->cap || (!src && n > 0)) return PMPIC_ERR_ARG;
   cudaSetDevice(ctx->device);
+  int frc = flush_gathers(ctx);
+  if (frc) return frc;
+  ctx->dir_ready = false;
   PMPIC_CUDA(cudaMemcpyAsync(prop(ctx, p), src, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
   PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
   ctx->sorted_valid = false;
+  ctx->btot_grid_ready = false;
   return PMPIC_OK;
 }
 int pmpic_get_property(pmpic_ctx* ctx, int p, int64_t n, double* dst) {
   if (!ctx || p < 0 || p >= PMPIC_NPROP || n < 0 || n > ctx->cap || (!dst && n > 0)) return PMPIC_ERR_ARG;
   cudaSetDevice(ctx->device);
+  int frc = flush_gathers(ctx);
+  if (frc) return frc;
   PMPIC_CUDA(cudaMemcpyAsync(dst, prop(ctx, p), sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
   PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
   return PMPIC_OK;
@@ -356,6 +371,8 @@ int pmpic_upload_parcels(pmpic_ctx* ctx, int64_t n, const double* x, const doubl
   if (n < 0 || n > ctx->cap) return set_error(ctx, PMPIC_ERR_CAPACITY, "parcel count exceeds max_parcels");
   const double* src[11] = {x, y, z, p, q, r, b, h, vol, stretch, tag};
   cudaSetDevice(ctx->device);
+  ctx->pending_uvw = ctx->pending_pqr = false;  // a new state
+  ctx->dir_ready = false;
   for (int i = 0; i < 11; ++i) {
     if (src[i])
       PMPIC_CUDA(cudaMemcpyAsync(prop(ctx, kIO[i]), src[i], sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
@@ -373,6 +390,7 @@ int pmpic_upload_parcels(pmpic_ctx* ctx, int64_t n, const double* x, const doubl
   ctx->n = n;
   ctx->info.n_parcels = n;
   ctx->sorted_valid = false;
+  ctx->btot_grid_ready = false;
   return PMPIC_OK;
 }
 
@@ -383,6 +401,8 @@ int pmpic_download_parcels(pmpic_ctx* ctx, int64_t capacity, int64_t* n, double*
   if (capacity < ctx->n) return set_error(ctx, PMPIC_ERR_ARG, "download capacity below parcel count");
   double* dst[11] = {x, y, z, p, q, r, b, h, vol, stretch, tag};
   cudaSetDevice(ctx->device);
+  int frc = flush_gathers(ctx);
+  if (frc) return frc;
   for (int i = 0; i < 11; ++i)
     if (dst[i])
       PMPIC_CUDA(cudaMemcpyAsync(dst[i], prop(ctx, kIO[i]), sizeof(double) * ctx->n, cudaMemcpyDeviceToHost, ctx->stream));
@@ -450,16 +470,20 @@ int pmpic_get_step_info(pmpic_ctx* ctx, pmpic_step_info* info) {
 static int do_vort2vel(pmpic_ctx* ctx) {
   TimerScope ts(ctx, T_V2V);
   int rc;
-  // vort2vel.F90:117-121: binning and par2grid of p, q, r with one set of weights
+  if ((rc = flush_gathers(ctx))) return rc;
+  // vort2vel.F90:117-121: binning and par2grid of p, q, r with one set of
+  // weights.  The par2grid(btot) of vorticity_tendency.F90:121-129 uses the
+  // same weights and parcel state, so it runs in the same pass into a spare
+  // grid that the vorticity_tendency callback adopts.
   if ((rc = bin_and_sort(ctx))) return rc;
-  const double* f[3] = {prop(ctx, PMPIC_PROP_P), prop(ctx, PMPIC_PROP_Q), prop(ctx, PMPIC_PROP_R)};
-  double* o[3] = {ctx->grid[PMPIC_GRID_P], ctx->grid[PMPIC_GRID_Q], ctx->grid[PMPIC_GRID_R]};
-  if ((rc = par2grid_multi(ctx, f, 3, o, false))) return rc;
+  const double* f[4] = {prop(ctx, PMPIC_PROP_P), prop(ctx, PMPIC_PROP_Q), prop(ctx, PMPIC_PROP_R), nullptr};
+  double* o[4] = {ctx->grid[PMPIC_GRID_P], ctx->grid[PMPIC_GRID_Q], ctx->grid[PMPIC_GRID_R], ctx->gspare};
+  if ((rc = par2grid_multi(ctx, f, 4, o, true))) return rc;
+  ctx->btot_grid_ready = true;
   if ((rc = vort2vel_spectral(ctx))) return rc;
-  // :325-327
-  const double* gr[3] = {ctx->grid[PMPIC_GRID_U], ctx->grid[PMPIC_GRID_V], ctx->grid[PMPIC_GRID_W]};
-  double* out[3] = {prop(ctx, PMPIC_PROP_DXDT), prop(ctx, PMPIC_PROP_DYDT), prop(ctx, PMPIC_PROP_DZDT)};
-  if ((rc = grid2par_multi(ctx, gr, 3, out))) return rc;
+  // :325-327: the grid2par of u, v, w is deferred into the rk4 pass (or to
+  // the next call that observes the tendencies)
+  ctx->pending_uvw = true;
   if (ctx->counters[0] % 4 == 0)
     if ((rc = field_max(ctx, true, false))) return rc;  // :329-372
   ctx->counters[0]++;
@@ -469,18 +493,27 @@ static int do_vort2vel(pmpic_ctx* ctx) {
 static int do_vorticity_tendency(pmpic_ctx* ctx) {
   TimerScope ts(ctx, T_VT);
   int rc;
-  if ((rc = compute_btot(ctx))) return rc;  // :121-126
-  // par2grid(btot) (:129) with the cell lists of this substep (positions
-  // are unchanged since vort2vel binned them)
-  if (!ctx->sorted_valid)
-    if ((rc = bin_and_sort(ctx))) return rc;
-  const double* f[1] = {prop(ctx, PMPIC_PROP_BTOT)};
-  double* o[1] = {ctx->grid[PMPIC_GRID_B]};
-  if ((rc = par2grid_multi(ctx, f, 1, o, false))) return rc;
+  if (ctx->pending_pqr) {  // a second call without rk4 in between: apply the first
+    bool u = ctx->pending_uvw;  // u, v, w stay pending
+    ctx->pending_uvw = false;
+    if ((rc = flush_gathers(ctx))) return rc;
+    ctx->pending_uvw = u;
+  }
+  if ((rc = compute_btot(ctx))) return rc;  // :121-126 (the btot property)
+  // par2grid(btot) (:129): computed by vort2vel's pass when the state is unchanged
+  if (ctx->btot_grid_ready && ctx->sorted_valid) {
+    std::swap(ctx->grid[PMPIC_GRID_B], ctx->gspare);
+  } else {
+    if (!ctx->sorted_valid)
+      if ((rc = bin_and_sort(ctx))) return rc;
+    const double* f[1] = {nullptr};
+    double* o[1] = {ctx->grid[PMPIC_GRID_B]};
+    if ((rc = par2grid_multi(ctx, f, 1, o, true))) return rc;
+  }
+  ctx->btot_grid_ready = false;
   if ((rc = vorticity_tendency_grids(ctx))) return rc;
-  const double* gr[3] = {ctx->grid[PMPIC_GRID_DP], ctx->grid[PMPIC_GRID_DQ], ctx->grid[PMPIC_GRID_DR]};
-  double* out[3] = {prop(ctx, PMPIC_PROP_DPDT), prop(ctx, PMPIC_PROP_DQDT), prop(ctx, PMPIC_PROP_DRDT)};
-  if ((rc = grid2par_multi(ctx, gr, 3, out))) return rc;  // :273-275
+  // :273-275: the grid2par of dp, dq, dr is deferred like vort2vel's
+  ctx->pending_pqr = true;
   if (ctx->counters[1] % 4 == 0)
     if ((rc = field_max(ctx, false, true))) return rc;  // :277-313
   ctx->counters[1]++;
@@ -489,6 +522,7 @@ static int do_vorticity_tendency(pmpic_ctx* ctx) {
 
 static int do_rk4(pmpic_ctx* ctx) {
   TimerScope ts(ctx, T_RK4);
+  ctx->btot_grid_ready = false;
   int rc;
   if ((rc = rk4_stage(ctx, ctx->counters[2]))) return rc;
   ctx->counters[2] = ctx->counters[2] < 4 ? ctx->counters[2] + 1 : 1;  // rk4_integrator.F90:311-315
@@ -551,7 +585,11 @@ int pmpic_step(pmpic_ctx* ctx, int nsteps) {
 int pmpic_op_cell_ids(pmpic_ctx* ctx, int32_t* cells) {
   if (!ctx || !cells) return PMPIC_ERR_ARG;
   cudaSetDevice(ctx->device);
-  int rc = cell_ids(ctx, ctx->cell);
+  {
+    int frc = flush_gathers(ctx);
+    if (frc) return frc;
+  }
+  int rc = cell_ids(ctx, nullptr);
   if (rc) return rc;
   PMPIC_CUDA(cudaMemcpyAsync(cells, ctx->cell, sizeof(int32_t) * ctx->n, cudaMemcpyDeviceToHost, ctx->stream));
   return sync_info(ctx);
@@ -560,6 +598,10 @@ int pmpic_op_cell_ids(pmpic_ctx* ctx, int32_t* cells) {
 int pmpic_op_par2grid(pmpic_ctx* ctx, int p, int grid) {
   if (!ctx || p < 0 || p >= PMPIC_NPROP || grid < 0 || grid >= PMPIC_NGRID) return PMPIC_ERR_ARG;
   cudaSetDevice(ctx->device);
+  {
+    int frc = flush_gathers(ctx);
+    if (frc) return frc;
+  }
   int rc = bin_and_sort(ctx);
   if (rc) return rc;
   const double* f[1] = {prop(ctx, p)};
@@ -571,6 +613,10 @@ int pmpic_op_par2grid(pmpic_ctx* ctx, int p, int grid) {
 int pmpic_op_grid2par(pmpic_ctx* ctx, int grid, int p) {
   if (!ctx || p < 0 || p >= PMPIC_NPROP || grid < 0 || grid >= PMPIC_NGRID) return PMPIC_ERR_ARG;
   cudaSetDevice(ctx->device);
+  {
+    int frc = flush_gathers(ctx);
+    if (frc) return frc;
+  }
   const double* gr[1] = {ctx->grid[grid]};
   double* out[1] = {prop(ctx, p)};
   int rc = grid2par_multi(ctx, gr, 1, out);
@@ -646,6 +692,10 @@ int pmpic_op_laplinv(pmpic_ctx* ctx, double* inout, int df0) {
 int pmpic_op_parcel_haloswap(pmpic_ctx* ctx) {
   if (!ctx) return PMPIC_ERR_ARG;
   cudaSetDevice(ctx->device);
+  {
+    int frc = flush_gathers(ctx);
+    if (frc) return frc;
+  }
   int rc = parcel_haloswap(ctx);
   if (rc) return rc;
   return sync_info(ctx);

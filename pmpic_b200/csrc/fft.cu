@@ -18,6 +18,7 @@
 // arithmetic of the reference's zero-imaginary complex transforms.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -296,6 +297,331 @@ __global__ void __launch_bounds__(FFT_THREADS) k_inv_y(Geom g, int TXF, FftPlan 
   }
 }
 
+// ---- four-step register FFT for n = n1 * n2, n1, n2 in {4, 8, 16} --------------------
+// x[n2 + N2 n1] -> X[k1 + N1 k2]:  n1-point DFTs over n1 (one thread per n2),
+// twiddle W_n^(n2 k1), transpose through shared memory, n2-point DFTs over n2
+// (one thread per k1).  The small DFTs run in registers; loads and stores touch
+// global memory once each.
+
+// W_16^m = exp(-2 pi i m / 16), m known at compile time after unrolling
+__device__ __forceinline__ double2 w16(int m) {
+  constexpr double C1 = 0.92387953251128675613;  // cos(pi/8)
+  constexpr double C2 = 0.70710678118654752440;  // cos(pi/4)
+  constexpr double C3 = 0.38268343236508977173;  // cos(3pi/8)
+  switch (m & 15) {
+    case 0: return make_double2(1.0, 0.0);
+    case 1: return make_double2(C1, -C3);
+    case 2: return make_double2(C2, -C2);
+    case 3: return make_double2(C3, -C1);
+    case 4: return make_double2(0.0, -1.0);
+    case 5: return make_double2(-C3, -C1);
+    case 6: return make_double2(-C2, -C2);
+    case 7: return make_double2(-C1, -C3);
+    case 8: return make_double2(-1.0, 0.0);
+    case 9: return make_double2(-C1, C3);
+    case 10: return make_double2(-C2, C2);
+    case 11: return make_double2(-C3, C1);
+    case 12: return make_double2(0.0, 1.0);
+    case 13: return make_double2(C3, C1);
+    case 14: return make_double2(C2, C2);
+    default: return make_double2(C1, C3);
+  }
+}
+
+// forward DFT of size R in registers, natural order in and out
+template <int R>
+__device__ __forceinline__ void dft(double2* a) {
+  if constexpr (R <= 5) {
+    small_dft<R>(a);
+  } else {
+    constexpr int M1 = 4, M2 = R / 4;  // R = 8: 4 x 2, R = 16: 4 x 4
+    double2 y[R];
+#pragma unroll
+    for (int n2 = 0; n2 < M2; ++n2) {
+      double2 b[M1];
+#pragma unroll
+      for (int n1 = 0; n1 < M1; ++n1) b[n1] = a[M2 * n1 + n2];
+      small_dft<M1>(b);
+#pragma unroll
+      for (int k1 = 0; k1 < M1; ++k1) y[k1 * M2 + n2] = (n2 * k1 == 0) ? b[k1] : cmul(b[k1], w16(n2 * k1 * (16 / R)));
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < M1; ++k1) {
+      double2 c[M2];
+#pragma unroll
+      for (int n2 = 0; n2 < M2; ++n2) c[n2] = y[k1 * M2 + n2];
+      small_dft<M2>(c);
+#pragma unroll
+      for (int k2 = 0; k2 < M2; ++k2) a[k1 + M1 * k2] = c[k2];
+    }
+  }
+}
+
+constexpr int FS_THREADS = 128;
+
+// step 1 of one row: a[n1] = x[n2 + N2 n1] on entry; Y row [k1][n2] (padded)
+template <int N1, int N2>
+__device__ __forceinline__ void fs_step1(double2* a, int n2, double2* Yrow, const double2* __restrict__ tw4) {
+  dft<N1>(a);
+#pragma unroll
+  for (int k1 = 0; k1 < N1; ++k1) Yrow[k1 * (N2 + 1) + n2] = (k1 == 0 || n2 == 0) ? a[k1] : cmul(a[k1], tw4[n2 * N1 + k1]);
+}
+// step 3 of one row: a[k2] = X[k1 + N1 k2] on return
+template <int N1, int N2>
+__device__ __forceinline__ void fs_step3(double2* a, int k1, const double2* Yrow) {
+#pragma unroll
+  for (int n2 = 0; n2 < N2; ++n2) a[n2] = Yrow[k1 * (N2 + 1) + n2];
+  dft<N2>(a);
+}
+
+// forward x pass (mid -> spec): RP complex rows (pairs of real rows) per CTA
+template <int N1, int N2>
+__global__ void __launch_bounds__(FS_THREADS) k4_fwd_x(Geom g, int64_t nrows_total, const double2* __restrict__ tw4,
+                                                       const double* __restrict__ mid, double* __restrict__ spec) {
+  constexpr int N = N1 * N2, RP = FS_THREADS / (N1 > N2 ? N1 : N2), YS = N1 * (N2 + 1);
+  __shared__ double2 Y[RP * YS];
+  double2* X = Y;  // [RP][N], reuses Y after step 3 has read it
+  const int t = threadIdx.x;
+  const int64_t row0 = (int64_t)blockIdx.x * RP * 2;
+  if (t < RP * N2) {
+    const int r = t / N2, n2 = t % N2;
+    const int64_t ra = row0 + 2 * r, rb = ra + 1;
+    double2 a[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+      const int i = n2 + N2 * n1;
+      a[n1] = make_double2(ra < nrows_total ? mid[(size_t)ra * N + i] : 0.0,
+                           rb < nrows_total ? mid[(size_t)rb * N + i] : 0.0);
+    }
+    fs_step1<N1, N2>(a, n2, Y + r * YS, tw4);
+  }
+  __syncthreads();
+  {  // every thread reaches the barrier; RP * N1 <= FS_THREADS
+    const bool act = t < RP * N1;
+    const int r = t / N1, k1 = t % N1;
+    double2 a[N2];
+    if (act) fs_step3<N1, N2>(a, k1, Y + r * YS);
+    __syncthreads();
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2)
+      if (act) X[r * N + k1 + N1 * k2] = a[k2];
+  }
+  __syncthreads();
+  // separate the two real rows: A = (Z_b + conj Z_{N-b}) / 2, B = (Z_b - conj Z_{N-b}) / (2i)
+  constexpr int HALF = N / 2 + 1;
+  for (int e = t; e < RP * 2 * HALF; e += FS_THREADS) {
+    const int rr = e / HALF, b = e - rr * HALF;
+    const int64_t row = row0 + rr;
+    if (row >= nrows_total) continue;
+    const int r = rr >> 1;
+    const double2 z1 = X[r * N + b];
+    const double2 z2 = X[r * N + (b == 0 ? 0 : N - b)];
+    double re, im;
+    if ((rr & 1) == 0) {
+      re = 0.5 * (z1.x + z2.x);
+      im = 0.5 * (z1.y - z2.y);
+    } else {
+      re = 0.5 * (z1.y + z2.y);
+      im = -0.5 * (z1.x - z2.x);
+    }
+    spec[(size_t)row * g.sx + 2 * b] = re;
+    spec[(size_t)row * g.sx + 2 * b + 1] = im;
+  }
+}
+
+// inverse x pass (spec -> mid)
+template <int N1, int N2>
+__global__ void __launch_bounds__(FS_THREADS) k4_inv_x(Geom g, int64_t nrows_total, const double2* __restrict__ tw4,
+                                                       const double* __restrict__ spec, double* __restrict__ mid) {
+  constexpr int N = N1 * N2, RP = FS_THREADS / (N1 > N2 ? N1 : N2), YS = N1 * (N2 + 1);
+  __shared__ double2 Y[RP * YS];
+  const int t = threadIdx.x;
+  const int64_t row0 = (int64_t)blockIdx.x * RP * 2;
+  if (t < RP * N2) {
+    const int r = t / N2, n2 = t % N2;
+    const int64_t ra = row0 + 2 * r, rb = ra + 1;
+    double2 a[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+      const int k = n2 + N2 * n1;
+      const int km = (2 * k <= N) ? k : N - k;
+      double2 A = make_double2(0.0, 0.0), B = make_double2(0.0, 0.0);
+      if (ra < nrows_total) A = make_double2(spec[(size_t)ra * g.sx + 2 * km], spec[(size_t)ra * g.sx + 2 * km + 1]);
+      if (rb < nrows_total) B = make_double2(spec[(size_t)rb * g.sx + 2 * km], spec[(size_t)rb * g.sx + 2 * km + 1]);
+      a[n1] = c2r_pack(A, B, k, N);
+    }
+    fs_step1<N1, N2>(a, n2, Y + r * YS, tw4);
+  }
+  __syncthreads();
+  const double dn = 1.0 / (double)N;
+  if (t < RP * N1) {
+    const int r = t / N1, k1 = t % N1;
+    double2 a[N2];
+    fs_step3<N1, N2>(a, k1, Y + r * YS);
+    const int64_t ra = row0 + 2 * r, rb = ra + 1;
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) {
+      const int i = k1 + N1 * k2;  // conj(z) * dn: real part -> row A, imaginary part -> row B
+      if (ra < nrows_total) mid[(size_t)ra * N + i] = a[k2].x * dn;
+      if (rb < nrows_total) mid[(size_t)rb * N + i] = -a[k2].y * dn;
+    }
+  }
+}
+
+// forward y pass (phys -> mid): one z level, 16 consecutive x columns
+// (8 complex columns) per CTA; thread order puts consecutive x on consecutive threads
+template <int N1, int N2>
+__global__ void __launch_bounds__(FS_THREADS) k4_fwd_y(Geom g, const double2* __restrict__ tw4,
+                                                       const double* __restrict__ phys, double* __restrict__ mid) {
+  // rows of Y and X are padded so the 8 column pairs of a warp access fall in
+  // distinct shared-memory banks
+  constexpr int N = N1 * N2, RP = 8, YS = N1 * (N2 + 1) + 1, XS = N + 1;
+  __shared__ double2 Y[RP * YS];
+  double2* X = Y;  // [RP][XS], reuses Y after step 3 has read it
+  const int t = threadIdx.x, Nx = g.Nx;
+  const int x0 = blockIdx.x * 2 * RP, k = blockIdx.y;
+  const double* P = phys + (size_t)k * N * Nx;
+  if (t < RP * N2) {
+    const int r = t % RP, n2 = t / RP;
+    double2 a[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+      const int j = n2 + N2 * n1;
+      a[n1] = *(const double2*)&P[(size_t)j * Nx + x0 + 2 * r];  // columns x0+2r (re), x0+2r+1 (im)
+    }
+    fs_step1<N1, N2>(a, n2, Y + r * YS, tw4);
+  }
+  __syncthreads();
+  {  // every thread reaches the barrier; RP * N1 <= FS_THREADS
+    const bool act = t < RP * N1;
+    const int r = t % RP, k1 = t / RP;
+    double2 a[N2];
+    if (act) fs_step3<N1, N2>(a, k1, Y + r * YS);
+    __syncthreads();
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2)
+      if (act) X[r * XS + k1 + N1 * k2] = a[k2];
+  }
+  __syncthreads();
+  constexpr int HALF = N / 2 + 1;
+  double* M = mid + (size_t)k * g.sy * Nx;
+  for (int e = t; e < HALF * 2 * RP; e += FS_THREADS) {
+    const int a = e / (2 * RP), x = e - a * (2 * RP);
+    const int r = x >> 1;
+    const double2 z1 = X[r * XS + a];
+    const double2 z2 = X[r * XS + (a == 0 ? 0 : N - a)];
+    double re, im;
+    if ((x & 1) == 0) {
+      re = 0.5 * (z1.x + z2.x);
+      im = 0.5 * (z1.y - z2.y);
+    } else {
+      re = 0.5 * (z1.y + z2.y);
+      im = -0.5 * (z1.x - z2.x);
+    }
+    M[(size_t)(2 * a) * Nx + x0 + x] = re;
+    M[(size_t)(2 * a + 1) * Nx + x0 + x] = im;
+  }
+}
+
+// inverse y pass (mid -> phys)
+template <int N1, int N2>
+__global__ void __launch_bounds__(FS_THREADS) k4_inv_y(Geom g, const double2* __restrict__ tw4,
+                                                       const double* __restrict__ mid, double* __restrict__ phys) {
+  // rows of Y and X are padded so the 8 column pairs of a warp access fall in
+  // distinct shared-memory banks
+  constexpr int N = N1 * N2, RP = 8, YS = N1 * (N2 + 1) + 1, XS = N + 1;
+  __shared__ double2 Y[RP * YS];
+  const int t = threadIdx.x, Nx = g.Nx;
+  const int x0 = blockIdx.x * 2 * RP, k = blockIdx.y;
+  const double* M = mid + (size_t)k * g.sy * Nx;
+  if (t < RP * N2) {
+    const int r = t % RP, n2 = t / RP;
+    double2 a[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+      const int kk = n2 + N2 * n1;
+      const int km = (2 * kk <= N) ? kk : N - kk;
+      const double2 re = *(const double2*)&M[(size_t)(2 * km) * Nx + x0 + 2 * r];      // (A.re, B.re)
+      const double2 im = *(const double2*)&M[(size_t)(2 * km + 1) * Nx + x0 + 2 * r];  // (A.im, B.im)
+      a[n1] = c2r_pack(make_double2(re.x, im.x), make_double2(re.y, im.y), kk, N);
+    }
+    fs_step1<N1, N2>(a, n2, Y + r * YS, tw4);
+  }
+  __syncthreads();
+  const double dn = 1.0 / (double)N;
+  if (t < RP * N1) {
+    const int r = t % RP, k1 = t / RP;
+    double2 a[N2];
+    fs_step3<N1, N2>(a, k1, Y + r * YS);
+    double* P = phys + (size_t)k * N * Nx;
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) {
+      const int j = k1 + N1 * k2;
+      *(double2*)&P[(size_t)j * Nx + x0 + 2 * r] = make_double2(a[k2].x * dn, -a[k2].y * dn);
+    }
+  }
+}
+
+// the four-step split used for a row length (0: none)
+void fs_split(int n, int& n1, int& n2) {
+  n1 = n2 = 0;
+  switch (n) {
+    case 16: n1 = 4; n2 = 4; break;
+    case 32: n1 = 8; n2 = 4; break;
+    case 64: n1 = 8; n2 = 8; break;
+    case 128: n1 = 16; n2 = 8; break;
+    case 256: n1 = 16; n2 = 16; break;
+    default: break;
+  }
+}
+
+// launchers by split; return false if the split has no instantiation
+#define PMPIC_FS_CASES(CALL) \
+  if (n1 == 4 && n2 == 4) { CALL(4, 4); return true; } \
+  if (n1 == 8 && n2 == 4) { CALL(8, 4); return true; } \
+  if (n1 == 8 && n2 == 8) { CALL(8, 8); return true; } \
+  if (n1 == 16 && n2 == 8) { CALL(16, 8); return true; } \
+  if (n1 == 16 && n2 == 16) { CALL(16, 16); return true; } \
+  return false;
+
+bool fs_fwd_x(int n1, int n2, unsigned nb, cudaStream_t st, const Geom& g, int64_t nrows, const double2* tw4,
+              const double* mid, double* spec) {
+#define CALL(A, B) k4_fwd_x<A, B><<<nb, FS_THREADS, 0, st>>>(g, nrows, tw4, mid, spec)
+  PMPIC_FS_CASES(CALL)
+#undef CALL
+}
+bool fs_inv_x(int n1, int n2, unsigned nb, cudaStream_t st, const Geom& g, int64_t nrows, const double2* tw4,
+              const double* spec, double* mid) {
+#define CALL(A, B) k4_inv_x<A, B><<<nb, FS_THREADS, 0, st>>>(g, nrows, tw4, spec, mid)
+  PMPIC_FS_CASES(CALL)
+#undef CALL
+}
+bool fs_fwd_y(int n1, int n2, dim3 gr, cudaStream_t st, const Geom& g, const double2* tw4, const double* phys,
+              double* mid) {
+#define CALL(A, B) k4_fwd_y<A, B><<<gr, FS_THREADS, 0, st>>>(g, tw4, phys, mid)
+  PMPIC_FS_CASES(CALL)
+#undef CALL
+}
+bool fs_inv_y(int n1, int n2, dim3 gr, cudaStream_t st, const Geom& g, const double2* tw4, const double* mid,
+              double* phys) {
+#define CALL(A, B) k4_inv_y<A, B><<<gr, FS_THREADS, 0, st>>>(g, tw4, mid, phys)
+  PMPIC_FS_CASES(CALL)
+#undef CALL
+}
+#undef PMPIC_FS_CASES
+
+// four-step twiddles W_n^(n2 k1), [n2 * n1 + k1], long double accuracy
+void fs_twiddles(FftPlan& p, std::vector<double2>& tw) {
+  fs_split(p.n, p.n1, p.n2);
+  p.tw4_off = (int)tw.size();
+  if (!p.n1) return;
+  for (int n2 = 0; n2 < p.n2; ++n2)
+    for (int k1 = 0; k1 < p.n1; ++k1) {
+      long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)(n2 * k1) / (long double)p.n;
+      tw.push_back(make_double2((double)cosl(ang), (double)sinl(ang)));
+    }
+}
+
 FftPlan make_plan(int n, std::vector<double2>& tw) {
   // twiddles w^(q r) = exp(-2 pi i q r / len) of each Stockham stage, long double accuracy
   FftPlan p{};
@@ -341,10 +667,15 @@ int fft_init(pmpic_ctx* ctx) {
     return set_error(ctx, PMPIC_ERR_CONFIG, "nx and ny must have only the prime factors 2, 3 and 5");
   std::vector<double2> tw;
   FftPlan px = make_plan(ctx->g.Nx, tw);
+  fs_twiddles(px, tw);
   ctx->ftw_off_y = (int)tw.size();
   ctx->ftw_off_x = 0;
   FftPlan py = make_plan(ctx->g.Ny, tw);
+  fs_twiddles(py, tw);
   for (int s = 0; s < py.nst; ++s) py.tw_off[s] -= ctx->ftw_off_y;
+  py.tw4_off -= ctx->ftw_off_y;
+  // the y passes of the four-step path take 16 columns per CTA
+  if (ctx->g.Nx % 16 != 0) py.n1 = py.n2 = 0;
   PMPIC_CUDA(cudaMalloc(&ctx->ftw, sizeof(double2) * tw.size()));
   PMPIC_CUDA(cudaMemcpy(ctx->ftw, tw.data(), sizeof(double2) * tw.size(), cudaMemcpyHostToDevice));
   ctx->plan_x = px;
@@ -363,15 +694,28 @@ int fft_forward(pmpic_ctx* ctx, const double* phys, double* spec) {
   const FftPlan& px = ctx->plan_x;
   const FftPlan& py = ctx->plan_y;
   const double2* tw = (const double2*)ctx->ftw;
-  int txf = pick_txf(g.Nx);
-  size_t sm_y = sizeof(double2) * (size_t)(txf / 2) * g.Ny * 2;
-  dim3 gy(g.Nx / txf, g.nzp);
-  k_fwd_y<<<gy, FFT_THREADS, sm_y, ctx->stream>>>(g, txf, py, tw + ctx->ftw_off_y, phys, ctx->fftmid); ++ctx->nlaunch;
-  int rp = pick_rp(g.Nx);
+  const double2* twy = tw + ctx->ftw_off_y;
+  if (py.n1) {
+    fs_fwd_y(py.n1, py.n2, dim3(g.Nx / 16, g.nzp), ctx->stream, g, twy + py.tw4_off, phys, ctx->fftmid);
+  } else {
+    int txf = pick_txf(g.Nx);
+    size_t sm_y = sizeof(double2) * (size_t)(txf / 2) * g.Ny * 2;
+    dim3 gy(g.Nx / txf, g.nzp);
+    k_fwd_y<<<gy, FFT_THREADS, sm_y, ctx->stream>>>(g, txf, py, twy, phys, ctx->fftmid);
+  }
+  ++ctx->nlaunch;
   int64_t nrows = (int64_t)g.nzp * g.sy;
-  size_t sm_x = sizeof(double2) * (size_t)rp * g.Nx * 2;
-  k_fwd_x<<<(unsigned)((nrows + 2 * rp - 1) / (2 * rp)), FFT_THREADS, sm_x, ctx->stream>>>(g, rp, nrows, px, tw,
-                                                                                        ctx->fftmid, spec); ++ctx->nlaunch;
+  if (px.n1) {
+    const int rp = FS_THREADS / std::max(px.n1, px.n2);
+    fs_fwd_x(px.n1, px.n2, (unsigned)((nrows + 2 * rp - 1) / (2 * rp)), ctx->stream, g, nrows, tw + px.tw4_off,
+             ctx->fftmid, spec);
+  } else {
+    int rp = pick_rp(g.Nx);
+    size_t sm_x = sizeof(double2) * (size_t)rp * g.Nx * 2;
+    k_fwd_x<<<(unsigned)((nrows + 2 * rp - 1) / (2 * rp)), FFT_THREADS, sm_x, ctx->stream>>>(g, rp, nrows, px, tw,
+                                                                                          ctx->fftmid, spec);
+  }
+  ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
@@ -382,16 +726,29 @@ int fft_backward(pmpic_ctx* ctx, const double* spec, double* phys) {
   const FftPlan& px = ctx->plan_x;
   const FftPlan& py = ctx->plan_y;
   const double2* tw = (const double2*)ctx->ftw;
-  int rp = pick_rp(g.Nx);
   int64_t nrows = (int64_t)g.nzp * g.sy;
-  size_t sm_x = sizeof(double2) * (size_t)rp * g.Nx * 2;
-  k_inv_x<<<(unsigned)((nrows + 2 * rp - 1) / (2 * rp)), FFT_THREADS, sm_x, ctx->stream>>>(g, rp, nrows, px, tw,
-                                                                                        spec, ctx->fftmid); ++ctx->nlaunch;
-  int txf = pick_txf(g.Nx);
-  size_t half = (size_t)g.Ny / 2 + 1;
-  size_t sm_y = sizeof(double2) * std::max((size_t)(txf / 2) * g.Ny * 2, (size_t)(txf / 2) * g.Ny + txf * half);
-  dim3 gy(g.Nx / txf, g.nzp);
-  k_inv_y<<<gy, FFT_THREADS, sm_y, ctx->stream>>>(g, txf, py, tw + ctx->ftw_off_y, ctx->fftmid, phys); ++ctx->nlaunch;
+  if (px.n1) {
+    const int rp = FS_THREADS / std::max(px.n1, px.n2);
+    fs_inv_x(px.n1, px.n2, (unsigned)((nrows + 2 * rp - 1) / (2 * rp)), ctx->stream, g, nrows, tw + px.tw4_off,
+             spec, ctx->fftmid);
+  } else {
+    int rp = pick_rp(g.Nx);
+    size_t sm_x = sizeof(double2) * (size_t)rp * g.Nx * 2;
+    k_inv_x<<<(unsigned)((nrows + 2 * rp - 1) / (2 * rp)), FFT_THREADS, sm_x, ctx->stream>>>(g, rp, nrows, px, tw,
+                                                                                          spec, ctx->fftmid);
+  }
+  ++ctx->nlaunch;
+  const double2* twy = tw + ctx->ftw_off_y;
+  if (py.n1) {
+    fs_inv_y(py.n1, py.n2, dim3(g.Nx / 16, g.nzp), ctx->stream, g, twy + py.tw4_off, ctx->fftmid, phys);
+  } else {
+    int txf = pick_txf(g.Nx);
+    size_t half = (size_t)g.Ny / 2 + 1;
+    size_t sm_y = sizeof(double2) * std::max((size_t)(txf / 2) * g.Ny * 2, (size_t)(txf / 2) * g.Ny + txf * half);
+    dim3 gy(g.Nx / txf, g.nzp);
+    k_inv_y<<<gy, FFT_THREADS, sm_y, ctx->stream>>>(g, txf, py, twy, ctx->fftmid, phys);
+  }
+  ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }

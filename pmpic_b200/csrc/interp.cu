@@ -5,19 +5,25 @@
 // halo exchanges of MPIC_Haloswap.F90 (:95-290), which on one GPU become
 // periodic index arithmetic in x and y.
 //
+// Binning is cached exactly like the reference's cache_parcel_interp_weights:
+// per parcel the interior cell id and delx, dely, delz, computed once per
+// substep with the reference's arithmetic (bit-exact) and reused by par2grid,
+// grid2par and the mixing redistribution.
+//
 // par2grid is deterministic and uses no floating-point atomics:
-//   1. bin:   each parcel's interior cell id (bit-exact restatement of the
-//             reference binning) and an integer histogram of parcels per cell;
-//   2. scan:  exclusive scan of the histogram -> CSR offsets per cell;
-//   3. scatter the slot indices into cell order (integer atomics only decide
-//             positions inside a cell; the reduction below re-sorts each cell
-//             segment by slot index, so the summation order is fixed);
-//   4. reduce: one CTA per 16x16 column tile and a chunk of z levels walks the
-//             cell layers upwards, each thread accumulating the eight corner
-//             weights of one cell's parcels in slot order, then adding them into
-//             shared-memory level accumulators in four parity phases (cells of
-//             one parity class touch disjoint grid points), so every grid point
-//             sums its contributions in one fixed order.
+//   1. bin:     cell ids + cached offsets + an integer histogram per cell;
+//   2. scan:    exclusive scan of the histogram -> CSR offsets per cell;
+//   3. scatter: slot indices into cell order, then each cell segment sorted
+//               by slot index, so every later sum runs in slot order;
+//   4. reduce:  one CTA per 16x8 column tile and 16 grid levels walks the
+//               cell layers upwards.  For each layer the tile's parcels (17x9
+//               cells incl. the low periodic halo) are streamed into shared
+//               memory with cp.async gathers in double-buffered rank slices,
+//               then one thread per cell accumulates its parcels' eight corner
+//               weights from shared memory in slot order and adds them into
+//               the level accumulators in four parity phases (cells of one
+//               parity class touch disjoint grid points), so every grid point
+//               sums its contributions in one fixed order.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -26,15 +32,34 @@ namespace pmpic {
 
 namespace {
 
-constexpr int TILE = 16;          // owned grid points per tile edge
-constexpr int TC = TILE + 1;      // cells per tile edge incl. the low halo cell
-constexpr int P2G_THREADS = 320;  // >= TC*TC = 289
-constexpr int ZCHUNK = 16;        // grid levels per CTA
-constexpr int MAXSEG = 32;        // cell segments sorted in registers/local memory
+constexpr int TX = 16;                // owned grid points per tile in x
+constexpr int TY = 8;                 // ... in y
+constexpr int CX = TX + 1;            // cells per tile row incl. the low halo cell
+constexpr int CY = TY + 1;
+constexpr int NCELLT = CX * CY;       // 153 cells per tile layer
+constexpr int P2G_THREADS = 320;      // >= 2 * NCELLT, two threads per cell
+constexpr int P2G_WARPS = P2G_THREADS / 32;
+constexpr int ZCHUNK = 16;            // grid levels per CTA
+constexpr int RANKS = 4;              // in-cell ranks per staged slice
+constexpr int PPT = (NCELLT * RANKS + P2G_THREADS - 1) / P2G_THREADS;  // (cell, rank) pairs per thread
+// Staging position of cell c's rank ul: the cell index rotated by a per-rank
+// offset.  A warp's cp.async copies cover 8 consecutive cells x 4 ranks; with
+// rank rows 153 doubles apart the offsets 0, 15, 14, 13 put ranks 0/1 and 2/3
+// in complementary halves of the 32 banks (two wavefronts per copy), while
+// the reduction, one thread per cell, still reads consecutive addresses.
+__device__ __forceinline__ int stage_pos(int c, int ul) {
+  const int r = ul == 0 ? 0 : 16 - ul;
+  const int p = c + r;
+  return p >= NCELLT ? p - NCELLT : p;
+}
+constexpr int MAXSEG = 32;            // cell segments sorted in registers
 
+inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
+
+// ---- binning (cache_parcel_interp_weights, parcel_interpolation.F90:186-262) ----
 __global__ void k_bin_count(Geom g, int64_t n, const double* __restrict__ X, const double* __restrict__ Y,
-                            const double* __restrict__ Z, int32_t* __restrict__ cell, int32_t* __restrict__ count,
-                            DevInfo* info) {
+                            const double* __restrict__ Z, int32_t* __restrict__ cell, double* __restrict__ del,
+                            int64_t cap, int32_t* __restrict__ count, DevInfo* info) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   int ci, cj, ck;
@@ -46,6 +71,9 @@ __global__ void k_bin_count(Geom g, int64_t n, const double* __restrict__ X, con
   }
   int32_t id = (int32_t)(((int64_t)ck * g.Ny + cj) * g.Nx + ci);
   cell[t] = id;
+  del[t] = dx;
+  del[cap + t] = dy;
+  del[2 * cap + t] = dz;
   atomicAdd(&count[id], 1);
 }
 
@@ -57,6 +85,39 @@ __global__ void k_bin_scatter(int64_t n, const int32_t* __restrict__ cell, const
   if (id < 0) return;
   int32_t pos = start[id] + atomicAdd(&fill[id], 1);
   sorted[pos] = (int32_t)t;
+}
+
+// each cell's segment sorted by slot index (integer atomics above only decide
+// the order inside a cell)
+__global__ void k_sort_segments(int64_t ncell, const int32_t* __restrict__ start, int32_t* __restrict__ sorted) {
+  int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  int s0 = start[c], len = start[c + 1] - s0;
+  if (len < 2) return;
+  int32_t* s = sorted + s0;
+  if (len <= MAXSEG) {
+    int loc[MAXSEG];
+    for (int u = 0; u < len; ++u) {
+      int v = s[u];
+      int w = u - 1;
+      while (w >= 0 && loc[w] > v) {
+        loc[w + 1] = loc[w];
+        --w;
+      }
+      loc[w + 1] = v;
+    }
+    for (int u = 0; u < len; ++u) s[u] = loc[u];
+  } else {  // rare long segment: insertion sort in place
+    for (int u = 1; u < len; ++u) {
+      int v = s[u];
+      int w = u - 1;
+      while (w >= 0 && s[w] > v) {
+        s[w + 1] = s[w];
+        --w;
+      }
+      s[w + 1] = v;
+    }
+  }
 }
 
 // ---- exclusive scan of int32 counts (three-phase) ----------------------------
@@ -138,150 +199,296 @@ __global__ void k_scan_apply(const int32_t* __restrict__ in, int64_t n, const in
 
 // ---- par2grid reduction ----------------------------------------------------------
 // MODE 0: par2grid of NQ fields (plus the weights), normalised (:463-469).
+//         With BT, field NQ-1 is btot = b + 12.5 max(0, h - exp(-z)) computed
+//         per parcel (vorticity_tendency.F90:121-126).
 // MODE 1: parcel_mixing construct_grids for the kept class (vol >= vmin):
 //         NQ = 6 unnormalised sums of (1, b, h, p, q, r) * w, doubled at the
 //         walls (parcel_mixing.F90:141-152), plus npercell.
 // MODE 2: the same sums for the removed class (vol < vmin), not doubled.
 template <int NQ>
 struct P2GArgs {
-  const double* f[NQ > 0 ? NQ : 1];
-  double* out[NQ > 0 ? NQ : 1];
+  const double* f[NQ];  // per-parcel fields (MODE 1/2: f[0] unused)
+  double* out[NQ];
+  const double* bh[3];  // b, h, z for btot
   int32_t* npercell;
   double vmin;
 };
 
-template <int NQ, int MODE>
-__global__ void __launch_bounds__(P2G_THREADS) k_par2grid(Geom g, const int32_t* __restrict__ start,
-                                                          const int32_t* __restrict__ sorted,
-                                                          const double* __restrict__ X, const double* __restrict__ Y,
-                                                          const double* __restrict__ Z, const double* __restrict__ VOL,
-                                                          P2GArgs<NQ> a) {
-  constexpr int NA = MODE == 0 ? NQ + 1 : NQ;  // data fields (+ weights)
-  __shared__ double acc[2][TC * TC][NA];
-  const int t = threadIdx.x;
-  const int x0 = blockIdx.x * TILE, y0 = blockIdx.y * TILE;
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <int NQ, int MODE, bool BT>
+struct P2GLayout {
+  static constexpr int NA = MODE == 0 ? NQ + 1 : NQ;        // accumulated quantities
+  static constexpr int NF = MODE == 0 ? (BT ? NQ + 2 : NQ)  // staged per-parcel values
+                                      : NQ - 1;             //   (MODE 1/2: b,h,p,q,r)
+  static constexpr int NS = 4 + NF;                         // + delx, dely, delz, vol
+  static constexpr int FS = RANKS * NCELLT;                 // stride between staged fields
+  static constexpr size_t stage_elems = (size_t)NS * FS;    // one staging buffer
+  static constexpr size_t stage_bytes = sizeof(double) * 2 * stage_elems;
+  static constexpr size_t acc_bytes = sizeof(double) * 2 * NCELLT * NA;  // two grid levels
+  static constexpr size_t tab_bytes = sizeof(int) * (8 * NCELLT + 4 * P2G_WARPS);
+  static constexpr size_t smem = stage_bytes + acc_bytes + tab_bytes;
+};
+
+// One CTA per TX x TY column tile and ZCHUNK grid levels walks the cell layers
+// upwards.  Per layer the CTA reads each cell's CSR segment (start, length),
+// then streams the layer's parcels through shared memory in rank slices: slice
+// s holds, for every cell of the tile, its parcels of in-cell rank 4s..4s+3
+// (segments are sorted by slot, so rank order is slot order).  The gathers are
+// cp.async copies issued with consecutive threads on consecutive parcels of a
+// cell; the next slice (or the next layer's first slice) is in flight while the
+// current one is reduced.  Two adjacent threads own a cell: thread h keeps the
+// four corners of level ck+h in registers.  The corners are then added into two
+// level accumulators in four parity phases, so each grid point sums its
+// contributions in one fixed order independent of timing.
+template <int NQ, int MODE, bool BT>
+__global__ void __launch_bounds__(P2G_THREADS, 2)
+    k_par2grid(Geom g, const int32_t* __restrict__ start, const int32_t* __restrict__ sorted,
+               const double* __restrict__ del, int64_t cap, const double* __restrict__ VOL, P2GArgs<NQ> a) {
+  using Lay = P2GLayout<NQ, MODE, BT>;
+  constexpr int NA = Lay::NA, FS = Lay::FS;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double* stage = (double*)smraw;                          // [2][NS][RANKS][NCELLT]
+  double* acc = stage + 2 * Lay::stage_elems;              // [2 levels][NA][NCELLT points]
+  int* tab_s0 = (int*)(acc + 2 * NCELLT * NA);             // [4 layers][NCELLT]
+  int* tab_len = tab_s0 + 4 * NCELLT;                      // [4 layers][NCELLT]
+  int* wmax = tab_len + 4 * NCELLT;                        // [4 layers][P2G_WARPS]
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int c = t >> 1, h = t & 1;  // this thread's cell and level half
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   const int L0 = blockIdx.z * ZCHUNK;
-  const int L1 = min(L0 + ZCHUNK, g.nzp);
-  for (int e = t; e < 2 * TC * TC * NA; e += blockDim.x) (&acc[0][0][0])[e] = 0.0;
-  // this thread's cell column in the tile
-  const int tx = t % TC, ty = t / TC;
-  bool has_col = t < TC * TC;
+  const int LAST = min(L0 + ZCHUNK, g.nzp) - 1;  // last cell layer walked
+  for (int e = t; e < 2 * NCELLT * NA; e += P2G_THREADS) acc[e] = 0.0;
+  // this thread's cell column (c < NCELLT): local (tx, ty), global (ci, cj)
+  const int tx = c % CX, ty = c / CX;
+  bool has_col = c < NCELLT;
   int ci = x0 - 1 + tx, cj = y0 - 1 + ty;
   if (has_col) {
     if (tx > 0 && ci >= g.Nx) has_col = false;
     if (ty > 0 && cj >= g.Ny) has_col = false;
-    if (ci < 0) ci += g.Nx;
+    if (ci < 0) ci += g.Nx;  // low halo cell: periodic wrap (MPIC_Haloswap.F90)
     if (cj < 0) cj += g.Ny;
   }
   const int parity = (tx & 1) | ((ty & 1) << 1);
-  int cur = 0;
-  __syncthreads();
-  for (int ck = L0 - 1; ck <= L1 - 1; ++ck) {
-    double P[8][NA];
+  const double* DX = del;
+  const double* DY = del + cap;
+  const double* DZ = del + 2 * cap;
+
+  // Layer tables live in a ring of four (layers ck-1 .. ck+2 around the layer
+  // being reduced): each cell's CSR segment and the per-warp longest segment.
+  // A table's start values are loaded into registers one layer before they are
+  // stored, so no thread waits on them.
+  auto tb = [](int ck) { return (ck + 1) & 3; };
+  auto fetch = [&](int ck, int& s0, int& len) {
+    s0 = 0;
+    len = 0;
+    if (h == 0 && has_col && ck >= 0 && ck < g.Nz) {
+      const int64_t cid = ((int64_t)ck * g.Ny + cj) * g.Nx + ci;
+      s0 = start[cid];
+      len = start[cid + 1] - s0;
+    }
+  };
+  auto store_table = [&](int ck, int s0, int len) {
+    const int pb = tb(ck);
+    if (h == 0 && c < NCELLT) {
+      tab_s0[pb * NCELLT + c] = s0;
+      tab_len[pb * NCELLT + c] = len;
+    }
+    const int m = __reduce_max_sync(0xffffffffu, len);
+    if (lane == 0) wmax[pb * P2G_WARPS + warp] = m;
+  };
+  // slices of a layer; an empty layer still takes one (empty) slice
+  auto nslices = [&](int ck) {
+    const int pb = tb(ck);
+    int m = 0;
 #pragma unroll
-    for (int c = 0; c < 8; ++c)
+    for (int w = 0; w < P2G_WARPS; ++w) m = max(m, wmax[pb * P2G_WARPS + w]);
+    return max(1, (m + RANKS - 1) / RANKS);
+  };
+  // The chunk sequence is (layer, slice) in order.  Slot indices of a chunk
+  // are loaded into registers one chunk before its gathers are issued, so the
+  // dependent index load never waits in front of a cp.async.
+  int nid[PPT];
+  auto load_idx = [&](int ck, int s) {
+    const int pb = tb(ck);
 #pragma unroll
-      for (int q = 0; q < NA; ++q) P[c][q] = 0.0;
-    if (has_col && ck >= 0 && ck < g.Nz) {
-      int64_t cid = ((int64_t)ck * g.Ny + cj) * g.Nx + ci;
-      int s0 = start[cid], len = start[cid + 1] - s0;
-      int loc[MAXSEG];
-      int nl = len <= MAXSEG ? len : 0;
-      for (int u = 0; u < nl; ++u) {
-        int v = sorted[s0 + u];
-        int w = u - 1;
-        while (w >= 0 && loc[w] > v) {
-          loc[w + 1] = loc[w];
-          --w;
-        }
-        loc[w + 1] = v;
+    for (int i = 0; i < PPT; ++i) {
+      const int pr = t + i * P2G_THREADS;
+      nid[i] = -1;
+      if (pr < NCELLT * RANKS) {
+        const int cc = pr / RANKS, u = s * RANKS + pr % RANKS;
+        if (u < tab_len[pb * NCELLT + cc]) nid[i] = sorted[tab_s0[pb * NCELLT + cc] + u];
       }
-      int last = -1;
-      int nkept = 0;
-      for (int u = 0; u < len; ++u) {
-        int n;
-        if (len <= MAXSEG) {
-          n = loc[u];
-        } else {  // long segment: select the next larger slot index
-          n = 0x7fffffff;
-          for (int m = 0; m < len; ++m) {
-            int v = sorted[s0 + m];
-            if (v > last && v < n) n = v;
-          }
-          last = n;
+    }
+  };
+  auto issue = [&](int b) {
+    double* S = stage + (size_t)b * Lay::stage_elems;
+#pragma unroll
+    for (int i = 0; i < PPT; ++i) {
+      const int n = nid[i];
+      if (n < 0) continue;
+      const int pr = t + i * P2G_THREADS;
+      double* D = S + (pr % RANKS) * NCELLT + stage_pos(pr / RANKS, pr % RANKS);
+      cp_async8(D, DX + n);
+      cp_async8(D + FS, DY + n);
+      cp_async8(D + 2 * FS, DZ + n);
+      cp_async8(D + 3 * FS, VOL + n);
+      if (MODE == 0) {
+#pragma unroll
+        for (int qq = 0; qq < (BT ? NQ - 1 : NQ); ++qq) cp_async8(D + (4 + qq) * FS, a.f[qq] + n);
+        if (BT) {
+#pragma unroll
+          for (int qq = 0; qq < 3; ++qq) cp_async8(D + (4 + NQ - 1 + qq) * FS, a.bh[qq] + n);
         }
-        int bi, bj, bk;
-        double delx, dely, delz;
-        bin_parcel(g, X[n], Y[n], Z[n], bi, bj, bk, delx, dely, delz);
-        double v = VOL[n];
-        if (MODE == 1 && v < a.vmin) continue;   // parcel_mixing.F90:488
-        if (MODE == 2 && !(v < a.vmin)) continue;
+      } else {
+#pragma unroll
+        for (int qq = 1; qq < NQ; ++qq) cp_async8(D + (4 + qq - 1) * FS, a.f[qq] + n);
+      }
+    }
+  };
+
+  int cur = 0;  // level accumulator of the current layer's bottom corners
+  int ib = 0;   // staging buffer of the next issue
+  int ns0, nlen;  // start values of the next table to store (layer ck+3)
+  {
+    int s0a, la, s0b, lb, s0c, lc;
+    fetch(L0 - 1, s0a, la);
+    fetch(L0, s0b, lb);
+    fetch(L0 + 1, s0c, lc);
+    fetch(L0 + 2, ns0, nlen);
+    store_table(L0 - 1, s0a, la);
+    if (L0 <= LAST) store_table(L0, s0b, lb);
+    if (L0 + 1 <= LAST) store_table(L0 + 1, s0c, lc);
+  }
+  __syncthreads();
+  int il = L0 - 1, is = 0;  // the chunk whose indices are in nid
+  load_idx(il, is);
+  issue(ib);
+  ib ^= 1;
+  cp_async_commit();
+  if (is + 1 < nslices(il)) ++is;
+  else { ++il; is = 0; }
+  if (il <= LAST) load_idx(il, is);
+  for (int ck = L0 - 1; ck <= LAST; ++ck) {
+    const int pb = tb(ck);
+    const int ns = nslices(ck);
+    double P[4][NA];  // corners (dx, dy) of level ck + h
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc)
+#pragma unroll
+      for (int qq = 0; qq < NA; ++qq) P[cc][qq] = 0.0;
+    int nkept = 0;
+    const int mylen = c < NCELLT ? tab_len[pb * NCELLT + c] : 0;
+    for (int s = 0; s < ns; ++s) {
+      const int cb = ib ^ 1;  // buffer of slice s (the latest issue)
+      if (il <= LAST) {       // gathers of the next chunk, then its successor's indices
+        issue(ib);
+        ib ^= 1;
+      }
+      cp_async_commit();
+      if (il <= LAST) {
+        if (is + 1 < nslices(il)) ++is;
+        else { ++il; is = 0; }
+        if (il <= LAST) load_idx(il, is);
+      }
+      cp_async_wait<1>();
+      __syncthreads();
+      const int nu = min(RANKS, mylen - s * RANKS);
+      const double* S0 = stage + (size_t)cb * Lay::stage_elems;
+#pragma unroll
+      for (int ul = 0; ul < RANKS; ++ul) {
+        if (ul >= nu) break;
+        const double* S = S0 + ul * NCELLT + stage_pos(c, ul);
+        const double delx = S[0], dely = S[FS], delz = S[2 * FS], vv = S[3 * FS];
+        if (MODE == 1 && vv < a.vmin) continue;    // parcel_mixing.F90:488
+        if (MODE == 2 && !(vv < a.vmin)) continue;
         if (MODE == 1) ++nkept;
         // parcel_interpolation.F90:390-434: w = (1-delz)(1-dely)(1-delx) v etc.
-        double ez = 1 - delz, ey = 1 - dely, ex = 1 - delx;
-        double w[8];
-        w[0] = ez * ey * ex * v;
-        w[1] = ez * ey * delx * v;
-        w[2] = ez * dely * ex * v;
-        w[3] = ez * dely * delx * v;
-        w[4] = delz * ey * ex * v;
-        w[5] = delz * ey * delx * v;
-        w[6] = delz * dely * ex * v;
-        w[7] = delz * dely * delx * v;
-        double fv[NQ > 0 ? NQ : 1];
+        const double wz = h ? delz : 1 - delz, ey = 1 - dely, ex = 1 - delx;
+        double w[4];
+        w[0] = wz * ey * ex * vv;
+        w[1] = wz * ey * delx * vv;
+        w[2] = wz * dely * ex * vv;
+        w[3] = wz * dely * delx * vv;
+        double fv[NQ];
+        if (MODE == 0) {
 #pragma unroll
-        for (int q = 0; q < NQ; ++q) fv[q] = (MODE != 0 && q == 0) ? 1.0 : a.f[q][n];
+          for (int qq = 0; qq < (BT ? NQ - 1 : NQ); ++qq) fv[qq] = S[(4 + qq) * FS];
+          if (BT) {
+            const double bb = S[(4 + NQ - 1) * FS], hh = S[(4 + NQ) * FS], zz = S[(4 + NQ + 1) * FS];
+            fv[NQ - 1] = bb + 12.5 * fmax(0.0, hh - exp(-zz));  // vorticity_tendency.F90:123-124
+          }
+        } else {
+          fv[0] = 1.0;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
+          for (int qq = 1; qq < NQ; ++qq) fv[qq] = S[(4 + qq - 1) * FS];
+        }
 #pragma unroll
-          for (int q = 0; q < NQ; ++q) P[c][q] += (MODE != 0 && q == 0) ? w[c] : w[c] * fv[q];
-          if (MODE == 0) P[c][NA - 1] += w[c];
+        for (int cc = 0; cc < 4; ++cc) {
+#pragma unroll
+          for (int qq = 0; qq < NQ; ++qq) P[cc][qq] += (MODE != 0 && qq == 0) ? w[cc] : w[cc] * fv[qq];
+          if (MODE == 0) P[cc][NA - 1] += w[cc];
         }
       }
-      if (MODE == 1 && ck >= L0 && tx > 0 && ty > 0) a.npercell[cid] = nkept;
+      if (s + 1 < ns) __syncthreads();  // the buffer is refilled by the issue after next
     }
-    // add corners into the level accumulators, one parity class at a time
-    // corner c: dz = c>>2, dy = (c>>1)&1, dx = c&1
+    if (MODE == 1 && h == 0 && has_col && ck >= L0 && ck < g.Nz && tx > 0 && ty > 0)
+      a.npercell[((int64_t)ck * g.Ny + cj) * g.Nx + ci] = nkept;
+    // corners into the level accumulators, one parity class at a time;
+    // corner cc: dy = cc>>1, dx = cc&1; level ck + h
     for (int ph = 0; ph < 4; ++ph) {
+      if (ph) __syncthreads();
       if (has_col && parity == ph) {
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          int px = tx + (c & 1), py = ty + ((c >> 1) & 1);
-          if (px < TC && py < TC) {
-            double* A = acc[cur ^ (c >> 2)][py * TC + px];
+        for (int cc = 0; cc < 4; ++cc) {
+          const int px = tx + (cc & 1), py = ty + (cc >> 1);
+          if (px < CX && py < CY) {
+            double* A = acc + (size_t)(cur ^ h) * NA * NCELLT + py * CX + px;
 #pragma unroll
-            for (int q = 0; q < NA; ++q) A[q] += P[c][q];
-          }
-        }
-      }
-      __syncthreads();
-    }
-    // level ck is complete: normalise and store owned points
-    if (ck >= L0) {
-      for (int e = t; e < TILE * TILE; e += blockDim.x) {
-        int lx = e % TILE, ly = e / TILE;
-        int gx = x0 + lx, gy = y0 + ly;
-        if (gx < g.Nx && gy < g.Ny) {
-          const double* A = acc[cur][(ly + 1) * TC + (lx + 1)];
-          size_t o = ((size_t)ck * g.Ny + gy) * g.Nx + gx;
-          if (MODE == 0) {
-            double wv = A[NA - 1];
-            if (wv == 0.) wv = 1.;  // parcel_interpolation.F90:466
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) a.out[q][o] = A[q] / wv;  // :467
-          } else {
-            const bool wall = (MODE == 1) && (ck == 0 || ck == g.Nz);
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) a.out[q][o] = wall ? A[q] * 2. : A[q];
+            for (int qq = 0; qq < NA; ++qq) A[qq * NCELLT] += P[cc][qq];
           }
         }
       }
     }
     __syncthreads();
-    for (int e = t; e < TC * TC * NA; e += blockDim.x) (&acc[cur][0][0])[e] = 0.0;
+    // level ck is complete: normalise and store the owned points, clear the level
+    for (int e = t; e < NCELLT; e += P2G_THREADS) {
+      double* A = acc + (size_t)cur * NA * NCELLT + e;
+      const int px = e % CX, py = e / CX;
+      const int gx = x0 + px - 1, gy = y0 + py - 1;
+      if (ck >= L0 && px > 0 && py > 0 && gx < g.Nx && gy < g.Ny) {
+        const size_t o = ((size_t)ck * g.Ny + gy) * g.Nx + gx;
+        if (MODE == 0) {
+          double wv = A[(NA - 1) * NCELLT];
+          if (wv == 0.) wv = 1.;  // parcel_interpolation.F90:466
+#pragma unroll
+          for (int qq = 0; qq < NQ; ++qq) a.out[qq][o] = A[qq * NCELLT] / wv;  // :467
+        } else {
+          const bool wall = (MODE == 1) && (ck == 0 || ck == g.Nz);
+#pragma unroll
+          for (int qq = 0; qq < NQ; ++qq) a.out[qq][o] = wall ? A[qq * NCELLT] * 2. : A[qq * NCELLT];
+        }
+      }
+#pragma unroll
+      for (int qq = 0; qq < NA; ++qq) A[qq * NCELLT] = 0.0;
+    }
+    // the table of layer ck+3 (its start values arrived during this layer)
+    if (ck + 3 <= LAST) {
+      store_table(ck + 3, ns0, nlen);
+      fetch(ck + 4, ns0, nlen);
+    }
     cur ^= 1;
     __syncthreads();
   }
+  cp_async_wait<0>();
 }
 
 // ---- grid2par --------------------------------------------------------------------
@@ -292,16 +499,16 @@ struct G2PArgs {
 };
 
 template <int NG>
-__global__ void k_grid2par(Geom g, int64_t n, const double* __restrict__ X, const double* __restrict__ Y,
-                           const double* __restrict__ Z, G2PArgs<NG> a, DevInfo* info) {
+__global__ void k_grid2par(Geom g, int64_t n, const int32_t* __restrict__ cell, const double* __restrict__ del,
+                           int64_t cap, G2PArgs<NG> a) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  int ci, cj, ck;
-  double delx, dely, delz;
-  if (!bin_parcel(g, X[t], Y[t], Z[t], ci, cj, ck, delx, dely, delz)) {
-    atomicCAS(&info->error, 0, PMPIC_ERR_OUT_OF_BOX);
-    return;
-  }
+  const int32_t id = cell[t];
+  if (id < 0) return;  // binning reported the error
+  const double delx = del[t], dely = del[cap + t], delz = del[2 * cap + t];
+  const int ci = id % g.Nx;
+  const int cj = (id / g.Nx) % g.Ny;
+  const int ck = id / (g.Nx * g.Ny);
   int ci1 = ci + 1 == g.Nx ? 0 : ci + 1;  // grid2par_haloswap: periodic copy
   int cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
   size_t r00 = ((size_t)ck * g.Ny + cj) * g.Nx, r01 = ((size_t)ck * g.Ny + cj1) * g.Nx;
@@ -324,35 +531,24 @@ __global__ void k_grid2par(Geom g, int64_t n, const double* __restrict__ X, cons
   }
 }
 
-__global__ void k_cell_only(Geom g, int64_t n, const double* __restrict__ X, const double* __restrict__ Y,
-                            const double* __restrict__ Z, int32_t* __restrict__ cell, DevInfo* info) {
-  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  int ci, cj, ck;
-  double dx, dy, dz;
-  if (!bin_parcel(g, X[t], Y[t], Z[t], ci, cj, ck, dx, dy, dz)) {
-    cell[t] = -1;
-    atomicCAS(&info->error, 0, PMPIC_ERR_OUT_OF_BOX);
-    return;
-  }
-  cell[t] = (int32_t)(((int64_t)ck * g.Ny + cj) * g.Nx + ci);
-}
-
-inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
-
 }  // namespace
 
 // exclusive scan of n int32 values; out[n] receives the total
 int scan_excl(pmpic_ctx* ctx, const int32_t* in, int64_t n, int32_t* out) {
   int64_t ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
   int32_t* sums = (int32_t*)ctx->scan_tmp;
-  k_scan_tiles<<<(unsigned)ntiles, SCAN_BLOCK, 0, ctx->stream>>>(in, n, sums); ++ctx->nlaunch;
+  if (ntiles > 0) {
+    k_scan_tiles<<<(unsigned)ntiles, SCAN_BLOCK, 0, ctx->stream>>>(in, n, sums); ++ctx->nlaunch;
+  }
   k_scan_sums<<<1, SCAN_BLOCK, 0, ctx->stream>>>(sums, ntiles, out + n); ++ctx->nlaunch;
-  k_scan_apply<<<(unsigned)ntiles, SCAN_BLOCK, 0, ctx->stream>>>(in, n, sums, out); ++ctx->nlaunch;
+  if (ntiles > 0) {
+    k_scan_apply<<<(unsigned)ntiles, SCAN_BLOCK, 0, ctx->stream>>>(in, n, sums, out); ++ctx->nlaunch;
+  }
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
 
+// cache_parcel_interp_weights + the cell-ordered index: valid until positions change
 int bin_and_sort(pmpic_ctx* ctx) {
   TimerScope ts(ctx, T_CACHE);
   const Geom& g = ctx->g;
@@ -361,35 +557,45 @@ int bin_and_sort(pmpic_ctx* ctx) {
   PMPIC_CUDA(cudaMemsetAsync(ctx->cell_fill, 0, sizeof(int32_t) * g.ncell, ctx->stream));
   if (n > 0) {
     k_bin_count<<<nblk(n, 256), 256, 0, ctx->stream>>>(g, n, prop(ctx, PMPIC_PROP_X), prop(ctx, PMPIC_PROP_Y),
-                                                       prop(ctx, PMPIC_PROP_Z), ctx->cell, ctx->cell_count,
-                                                       ctx->dinfo); ++ctx->nlaunch;
+                                                       prop(ctx, PMPIC_PROP_Z), ctx->cell, ctx->del, ctx->cap,
+                                                       ctx->cell_count, ctx->dinfo); ++ctx->nlaunch;
   }
   int rc = scan_excl(ctx, ctx->cell_count, g.ncell, ctx->cell_start);
   if (rc) return rc;
   if (n > 0) {
     k_bin_scatter<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, ctx->cell, ctx->cell_start, ctx->cell_fill,
                                                          ctx->sorted); ++ctx->nlaunch;
+    k_sort_segments<<<nblk(g.ncell, 256), 256, 0, ctx->stream>>>(g.ncell, ctx->cell_start, ctx->sorted);
+    ++ctx->nlaunch;
   }
   PMPIC_CUDA(cudaGetLastError());
   ctx->sorted_valid = true;
   return 0;
 }
 
-template <int NQ, int MODE = 0>
+template <int NQ, int MODE, bool BT>
 static int launch_p2g(pmpic_ctx* ctx, const double* const* fields, double* const* out) {
   TimerScope ts(ctx, T_P2G);
   const Geom& g = ctx->g;
+  using Lay = P2GLayout<NQ, MODE, BT>;
+  static_assert(Lay::smem <= 227 * 1024, "par2grid shared memory");
   P2GArgs<NQ> a;
   for (int q = 0; q < NQ; ++q) {
     a.f[q] = fields[q];
     a.out[q] = out[q];
   }
+  a.bh[0] = prop(ctx, PMPIC_PROP_B);
+  a.bh[1] = prop(ctx, PMPIC_PROP_H);
+  a.bh[2] = prop(ctx, PMPIC_PROP_Z);
   a.npercell = ctx->npercell;
   a.vmin = g.vmin;
-  dim3 grid((g.Nx + TILE - 1) / TILE, (g.Ny + TILE - 1) / TILE, (g.nzp + ZCHUNK - 1) / ZCHUNK);
-  k_par2grid<NQ, MODE><<<grid, P2G_THREADS, 0, ctx->stream>>>(g, ctx->cell_start, ctx->sorted,
-                                                              prop(ctx, PMPIC_PROP_X), prop(ctx, PMPIC_PROP_Y),
-                                                              prop(ctx, PMPIC_PROP_Z), prop(ctx, PMPIC_PROP_VOL), a); ++ctx->nlaunch;
+  auto kern = k_par2grid<NQ, MODE, BT>;
+  PMPIC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::smem));
+  PMPIC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  (int)cudaSharedmemCarveoutMaxShared));
+  dim3 grid((g.Nx + TX - 1) / TX, (g.Ny + TY - 1) / TY, (g.nzp + ZCHUNK - 1) / ZCHUNK);
+  kern<<<grid, P2G_THREADS, Lay::smem, ctx->stream>>>(g, ctx->cell_start, ctx->sorted, ctx->del, ctx->cap,
+                                                      prop(ctx, PMPIC_PROP_VOL), a); ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
@@ -402,19 +608,25 @@ int launch_mix_grids(pmpic_ctx* ctx) {
                         prop(ctx, PMPIC_PROP_P), prop(ctx, PMPIC_PROP_Q), prop(ctx, PMPIC_PROP_R)};
   double* kept[6] = {ctx->grid[PMPIC_GRID_VOL], ctx->grid[PMPIC_GRID_B], ctx->grid[PMPIC_GRID_HG],
                      ctx->grid[PMPIC_GRID_P],   ctx->grid[PMPIC_GRID_Q], ctx->grid[PMPIC_GRID_R]};
-  int rc = launch_p2g<6, 1>(ctx, f, kept);
+  int rc = launch_p2g<6, 1, false>(ctx, f, kept);
   if (rc) return rc;
-  return launch_p2g<6, 2>(ctx, f, ctx->mixres);
+  return launch_p2g<6, 2, false>(ctx, f, ctx->mixres);
 }
 
-// par2grid of nf fields (1..4) with the same weights; requires bin_and_sort.
-int par2grid_multi(pmpic_ctx* ctx, const double* const* fields, int nf, double* const* out, bool) {
+// par2grid of nf fields with the same weights; with btot the last field is
+// btot computed from b, h, z.  Requires bin_and_sort.
+int par2grid_multi(pmpic_ctx* ctx, const double* const* fields, int nf, double* const* out, bool btot) {
+  if (btot) {
+    switch (nf) {
+      case 1: return launch_p2g<1, 0, true>(ctx, fields, out);
+      case 4: return launch_p2g<4, 0, true>(ctx, fields, out);
+      default: return set_error(ctx, PMPIC_ERR_ARG, "par2grid_multi: btot with 1 or 4 fields");
+    }
+  }
   switch (nf) {
-    case 1: return launch_p2g<1>(ctx, fields, out);
-    case 2: return launch_p2g<2>(ctx, fields, out);
-    case 3: return launch_p2g<3>(ctx, fields, out);
-    case 4: return launch_p2g<4>(ctx, fields, out);
-    default: return set_error(ctx, PMPIC_ERR_ARG, "par2grid_multi: 1..4 fields");
+    case 1: return launch_p2g<1, 0, false>(ctx, fields, out);
+    case 3: return launch_p2g<3, 0, false>(ctx, fields, out);
+    default: return set_error(ctx, PMPIC_ERR_ARG, "par2grid_multi: 1 or 3 fields");
   }
 }
 
@@ -428,14 +640,18 @@ static int launch_g2p(pmpic_ctx* ctx, const double* const* grids, double* const*
     a.grid[q] = grids[q];
     a.out[q] = out[q];
   }
-  k_grid2par<NG><<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(g, ctx->n, prop(ctx, PMPIC_PROP_X),
-                                                              prop(ctx, PMPIC_PROP_Y), prop(ctx, PMPIC_PROP_Z), a,
-                                                              ctx->dinfo); ++ctx->nlaunch;
+  k_grid2par<NG><<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(g, ctx->n, ctx->cell, ctx->del, ctx->cap, a);
+  ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
 
+// grid2par of ng grids; requires the cached binning of the current positions
 int grid2par_multi(pmpic_ctx* ctx, const double* const* grids, int ng, double* const* out) {
+  if (!ctx->sorted_valid) {
+    int rc = bin_and_sort(ctx);
+    if (rc) return rc;
+  }
   switch (ng) {
     case 1: return launch_g2p<1>(ctx, grids, out);
     case 3: return launch_g2p<3>(ctx, grids, out);
@@ -444,13 +660,11 @@ int grid2par_multi(pmpic_ctx* ctx, const double* const* grids, int ng, double* c
   }
 }
 
+// cached cell ids of the current positions (ctx->cell)
 int cell_ids(pmpic_ctx* ctx, int32_t* dcells) {
-  if (ctx->n == 0) return 0;
-  k_cell_only<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, prop(ctx, PMPIC_PROP_X),
-                                                          prop(ctx, PMPIC_PROP_Y), prop(ctx, PMPIC_PROP_Z), dcells,
-                                                          ctx->dinfo); ++ctx->nlaunch;
-  PMPIC_CUDA(cudaGetLastError());
-  return 0;
+  (void)dcells;
+  return bin_and_sort(ctx);
 }
 
 }  // namespace pmpic
+

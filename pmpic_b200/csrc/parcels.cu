@@ -79,37 +79,109 @@ struct PredNewCell {
 };
 
 // ---- RK4 stage (rk4_integrator.F90:95-319) -----------------------------------------
+// One pass per stage: the deferred grid2par gathers of vort2vel (u, v, w ->
+// dxdt, dydt, dzdt, vort2vel.F90:325-327) and of vorticity_tendency (dp, dq,
+// dr -> dpdt, dqdt, drdt, vorticity_tendency.F90:273-275) when pending, the
+// stage update, and the first step of the following parcel haloswap: the z
+// reflection (haloswap.F90:440-456) and the direction classification
+// (:296-437).
 struct RkPtrs {
   double* s[6];
   double* o[6];
   double* f[6];
-  const double* d[6];
+  double* d[6];
+  const double* grid[6];  // u, v, w, dp, dq, dr
 };
-__global__ void k_rk4(int64_t n, RkPtrs P, int stage, const double* __restrict__ dtp) {
+
+__device__ __forceinline__ int classify_dir(const Geom& g, double x, double y) {
+  const double xmin = g.hxmin, xmax = g.hxmax, ymin = g.hymin, ymax = g.hymax;
+  int d = 0;
+  if (y >= ymax && x >= xmin && x < xmax) d = 1;        // N
+  else if (y < ymin && x >= xmin && x < xmax) d = 5;    // S
+  else if (x >= xmax && y >= ymin && y < ymax) d = 3;   // E
+  else if (x < xmin && y >= ymin && y < ymax) d = 7;    // W
+  else if (x >= xmax && y >= ymax) d = 2;               // NE
+  else if (x < xmin && y >= ymax) d = 8;                // NW
+  else if (x >= xmax && y < ymin) d = 4;                // SE
+  else if (x < xmin && y < ymin) d = 6;                 // SW
+  return d;
+}
+
+template <bool GU, bool GP>
+__global__ void k_rk4(Geom g, int64_t n, RkPtrs P, int stage, const double* __restrict__ dtp,
+                      const int32_t* __restrict__ cell, const double* __restrict__ del, int64_t cap,
+                      int8_t* __restrict__ dir) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const double dt = *dtp;  // state%dtm (rk4_integrator.F90:102)
   const double dt6 = dt / 6, dt2 = dt / 2, dt3 = dt / 3;
+  // every load of this parcel is issued before the first store, so none of
+  // them waits behind another
+  double sv[6], ov[6], fv[6], d[6];
 #pragma unroll
   for (int v = 0; v < 6; ++v) {
-    double d = P.d[v][t];
+    if (stage == 1) sv[v] = P.s[v][t];
+    if (stage == 2 || stage == 3) ov[v] = P.o[v][t];
+    if (stage >= 2) fv[v] = P.f[v][t];
+    if ((v < 3 && !GU) || (v >= 3 && !GP)) d[v] = P.d[v][t];
+  }
+  const int32_t id = (GU || GP) ? cell[t] : -1;
+  bool gathered = false;
+  if ((GU || GP) && id >= 0) {  // id < 0: binning failed and reported the error
+    gathered = true;
+    const double delx = del[t], dely = del[cap + t], delz = del[2 * cap + t];
+    const int ci = id % g.Nx, cj = (id / g.Nx) % g.Ny, ck = id / (g.Nx * g.Ny);
+    const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
+    const size_t r00 = ((size_t)ck * g.Ny + cj) * g.Nx, r01 = ((size_t)ck * g.Ny + cj1) * g.Nx;
+    const size_t r10 = ((size_t)(ck + 1) * g.Ny + cj) * g.Nx, r11 = ((size_t)(ck + 1) * g.Ny + cj1) * g.Nx;
+#pragma unroll
+    for (int v = 0; v < 6; ++v) {
+      if ((v < 3 && !GU) || (v >= 3 && !GP)) continue;
+      const double* G = P.grid[v];
+      // grid2par, parcel_interpolation.F90:299-321
+      double c00 = G[r00 + ci] * (1 - delz) + G[r10 + ci] * delz;
+      double c01 = G[r00 + ci1] * (1 - delz) + G[r10 + ci1] * delz;
+      double c10 = G[r01 + ci] * (1 - delz) + G[r11 + ci] * delz;
+      double c11 = G[r01 + ci1] * (1 - delz) + G[r11 + ci1] * delz;
+      double c0 = c00 * (1 - dely) + c10 * dely;
+      double c1 = c01 * (1 - dely) + c11 * dely;
+      d[v] = c0 * (1 - delx) + c1 * delx;
+    }
+  } else if (GU || GP) {
+#pragma unroll
+    for (int v = 0; v < 6; ++v) d[v] = P.d[v][t];
+  }
+  double snew[6];
+#pragma unroll
+  for (int v = 0; v < 6; ++v) {
     if (stage == 1) {
-      double o = P.s[v][t];
-      P.o[v][t] = o;
-      P.f[v][t] = o + dt6 * d;
-      P.s[v][t] = o + dt2 * d;
+      ov[v] = sv[v];
+      fv[v] = sv[v] + dt6 * d[v];
+      snew[v] = sv[v] + dt2 * d[v];
     } else if (stage == 2) {
-      P.f[v][t] = P.f[v][t] + dt3 * d;
-      P.s[v][t] = P.o[v][t] + dt2 * d;
+      fv[v] = fv[v] + dt3 * d[v];
+      snew[v] = ov[v] + dt2 * d[v];
     } else if (stage == 3) {
-      P.f[v][t] = P.f[v][t] + dt3 * d;
-      P.s[v][t] = P.o[v][t] + dt * d;
+      fv[v] = fv[v] + dt3 * d[v];
+      snew[v] = ov[v] + dt * d[v];
     } else {
-      double f = P.f[v][t] + dt6 * d;
-      P.f[v][t] = f;
-      P.s[v][t] = f;
+      fv[v] = fv[v] + dt6 * d[v];
+      snew[v] = fv[v];
     }
   }
+  // parcel haloswap, first part: reflect z at the walls, classify
+  double z = snew[2];
+  if (z < g.pzmin) z = g.pzmin + (g.pzmin - z);
+  else if (z > g.pzmax) z = g.pzmax - (z - g.pzmax);
+  snew[2] = z;
+#pragma unroll
+  for (int v = 0; v < 6; ++v) {
+    if (gathered && ((v < 3 && GU) || (v >= 3 && GP))) P.d[v][t] = d[v];
+    if (stage == 1) P.o[v][t] = ov[v];
+    P.f[v][t] = fv[v];
+    P.s[v][t] = snew[v];
+  }
+  dir[t] = (int8_t)classify_dir(g, snew[0], snew[1]);
 }
 
 // ---- parcel haloswap (parcels/haloswap.F90:109-289, one rank) -------------------------
@@ -122,18 +194,7 @@ __global__ void k_reflect_classify(Geom g, int64_t n, const double* __restrict__
   double z = Z[i];
   if (z < g.pzmin) Z[i] = g.pzmin + (g.pzmin - z);
   else if (z > g.pzmax) Z[i] = g.pzmax - (z - g.pzmax);
-  double x = X[i], y = Y[i];
-  const double xmin = g.hxmin, xmax = g.hxmax, ymin = g.hymin, ymax = g.hymax;
-  int d = 0;
-  if (y >= ymax && x >= xmin && x < xmax) d = 1;        // N
-  else if (y < ymin && x >= xmin && x < xmax) d = 5;    // S
-  else if (x >= xmax && y >= ymin && y < ymax) d = 3;   // E
-  else if (x < xmin && y >= ymin && y < ymax) d = 7;    // W
-  else if (x >= xmax && y >= ymax) d = 2;               // NE
-  else if (x < xmin && y >= ymax) d = 8;                // NW
-  else if (x >= xmax && y < ymin) d = 4;                // SE
-  else if (x < xmin && y < ymin) d = 6;                 // SW
-  dir[i] = (int8_t)d;
+  dir[i] = (int8_t)classify_dir(g, X[i], Y[i]);
 }
 
 // Stable partition of the ascending moved list V by direction 1..8 (single
@@ -412,24 +473,24 @@ __global__ void k_residual_update(Geom g, ResPtrs RP, const int32_t* __restrict_
   }
 }
 
-// residuals onto the kept original parcels (:245-342)
+// residuals onto the kept original parcels (:245-342), with the binning
+// cached at the start of mixing (:80; kept parcels have not moved)
 __global__ void k_redistribute(Geom g, int64_t norig, const int32_t* __restrict__ keep, double* __restrict__ parcels,
-                               int64_t cap, ResPtrs RP, DevInfo* info) {
+                               int64_t cap, const int32_t* __restrict__ cell, const double* __restrict__ del,
+                               ResPtrs RP) {
   int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= norig || keep[m] != 1) return;
   auto A = [&](int pid) -> double* { return parcels + (size_t)pid * cap; };
-  int ci, cj, ck;
-  double delx, dely, delz;
-  if (!bin_parcel(g, A(PMPIC_PROP_X)[m], A(PMPIC_PROP_Y)[m], A(PMPIC_PROP_Z)[m], ci, cj, ck, delx, dely, delz)) {
-    atomicCAS(&info->error, 0, PMPIC_ERR_OUT_OF_BOX);
-    return;
-  }
+  const int32_t id = cell[m];
+  if (id < 0) return;
+  const double delx = del[m], dely = del[cap + m], delz = del[2 * cap + m];
+  const int ci = id % g.Nx, cj = (id / g.Nx) % g.Ny, ck = id / (g.Nx * g.Ny);
   int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
   size_t c[8] = {((size_t)ck * g.Ny + cj) * g.Nx + ci,        ((size_t)ck * g.Ny + cj) * g.Nx + ci1,
                  ((size_t)ck * g.Ny + cj1) * g.Nx + ci,       ((size_t)ck * g.Ny + cj1) * g.Nx + ci1,
                  ((size_t)(ck + 1) * g.Ny + cj) * g.Nx + ci,  ((size_t)(ck + 1) * g.Ny + cj) * g.Nx + ci1,
                  ((size_t)(ck + 1) * g.Ny + cj1) * g.Nx + ci, ((size_t)(ck + 1) * g.Ny + cj1) * g.Nx + ci1};
-  double v = A(PMPIC_PROP_VOL)[m];
+  const double v = A(PMPIC_PROP_VOL)[m];
   double w[8];
   w[0] = (1 - delz) * (1 - dely) * (1 - delx) * v;
   w[1] = (1 - delz) * (1 - dely) * (delx) * v;
@@ -441,19 +502,30 @@ __global__ void k_redistribute(Geom g, int64_t norig, const int32_t* __restrict_
   w[7] = (delz) * (dely) * (delx) * v;
   const double* V = RP.k[0];
   const double* vres = RP.r[0];
+  double vg[8], wv[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    vg[u] = V[c[u]];
+    wv[u] = w[u] / vg[u];  // the w/vol_g factor shared by b, h, p, q, r (:280-335)
+  }
   double nv = v;
 #pragma unroll
-  for (int u = 0; u < 8; ++u) nv = nv + w[u] * vres[c[u]] / V[c[u]];  // :268-276
-  A(PMPIC_PROP_VOL)[m] = nv;
+  for (int u = 0; u < 8; ++u) nv = nv + w[u] * vres[c[u]] / vg[u];  // :268-276
   const int pids[5] = {PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
+  double fo[5];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) fo[q] = A(pids[q])[m];
 #pragma unroll
   for (int q = 0; q < 5; ++q) {
     const double* res = RP.r[q + 1];
-    double s = A(pids[q])[m] * v;
+    double s = fo[q] * v;
 #pragma unroll
-    for (int u = 0; u < 8; ++u) s = s + w[u] / V[c[u]] * res[c[u]];  // :279-336
-    A(pids[q])[m] = s / nv;
+    for (int u = 0; u < 8; ++u) s = s + wv[u] * res[c[u]];  // :279-336
+    fo[q] = s / nv;
   }
+  A(PMPIC_PROP_VOL)[m] = nv;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) A(pids[q])[m] = fo[q];
 }
 
 // backfill (:347-389): the t-th removed slot (ascending) receives the t-th kept
@@ -498,6 +570,26 @@ static int compact(pmpic_ctx* ctx, Pred pr, int64_t n, int32_t* list, int32_t* d
 // small device counters live after the DevInfo block
 static int32_t* dcounter(pmpic_ctx* ctx, int i) { return (int32_t*)(ctx->dinfo + 1) + i; }
 
+// Apply deferred grid2par gathers (vort2vel.F90:325-327,
+// vorticity_tendency.F90:273-275) before anything observes or changes the
+// tendencies; the cached binning is valid while they are pending.
+int flush_gathers(pmpic_ctx* ctx) {
+  int rc = 0;
+  if (ctx->pending_uvw) {
+    ctx->pending_uvw = false;
+    const double* gr[3] = {ctx->grid[PMPIC_GRID_U], ctx->grid[PMPIC_GRID_V], ctx->grid[PMPIC_GRID_W]};
+    double* out[3] = {prop(ctx, PMPIC_PROP_DXDT), prop(ctx, PMPIC_PROP_DYDT), prop(ctx, PMPIC_PROP_DZDT)};
+    if ((rc = grid2par_multi(ctx, gr, 3, out))) return rc;
+  }
+  if (ctx->pending_pqr) {
+    ctx->pending_pqr = false;
+    const double* gr[3] = {ctx->grid[PMPIC_GRID_DP], ctx->grid[PMPIC_GRID_DQ], ctx->grid[PMPIC_GRID_DR]};
+    double* out[3] = {prop(ctx, PMPIC_PROP_DPDT), prop(ctx, PMPIC_PROP_DQDT), prop(ctx, PMPIC_PROP_DRDT)};
+    if ((rc = grid2par_multi(ctx, gr, 3, out))) return rc;
+  }
+  return 0;
+}
+
 int compute_btot(pmpic_ctx* ctx) {
   if (ctx->n == 0) return 0;
   k_btot<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->n, prop(ctx, PMPIC_PROP_B), prop(ctx, PMPIC_PROP_H),
@@ -507,32 +599,53 @@ int compute_btot(pmpic_ctx* ctx) {
 }
 
 int rk4_stage(pmpic_ctx* ctx, int stage) {
-  if (ctx->n == 0) return 0;
+  if (ctx->n == 0) {
+    ctx->pending_uvw = ctx->pending_pqr = false;
+    return 0;
+  }
   RkPtrs P;
   const int S[6] = {PMPIC_PROP_X, PMPIC_PROP_Y, PMPIC_PROP_Z, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
   const int O[6] = {PMPIC_PROP_XO, PMPIC_PROP_YO, PMPIC_PROP_ZO, PMPIC_PROP_PO, PMPIC_PROP_QO, PMPIC_PROP_RO};
   const int F[6] = {PMPIC_PROP_XF, PMPIC_PROP_YF, PMPIC_PROP_ZF, PMPIC_PROP_PF, PMPIC_PROP_QF, PMPIC_PROP_RF};
   const int D[6] = {PMPIC_PROP_DXDT, PMPIC_PROP_DYDT, PMPIC_PROP_DZDT, PMPIC_PROP_DPDT, PMPIC_PROP_DQDT, PMPIC_PROP_DRDT};
+  const int G[6] = {PMPIC_GRID_U, PMPIC_GRID_V, PMPIC_GRID_W, PMPIC_GRID_DP, PMPIC_GRID_DQ, PMPIC_GRID_DR};
   for (int v = 0; v < 6; ++v) {
     P.s[v] = prop(ctx, S[v]);
     P.o[v] = prop(ctx, O[v]);
     P.f[v] = prop(ctx, F[v]);
     P.d[v] = prop(ctx, D[v]);
+    P.grid[v] = ctx->grid[G[v]];
   }
-  k_rk4<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->n, P, stage, &ctx->dinfo->dtm); ++ctx->nlaunch;
+  const bool gu = ctx->pending_uvw, gp = ctx->pending_pqr;
+  if ((gu || gp) && !ctx->sorted_valid) return set_error(ctx, PMPIC_ERR_STATE, "deferred gather without binning");
+  auto kern = gu ? (gp ? k_rk4<true, true> : k_rk4<true, false>) : (gp ? k_rk4<false, true> : k_rk4<false, false>);
+  kern<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, P, stage, &ctx->dinfo->dtm, ctx->cell, ctx->del,
+                                                   ctx->cap, ctx->dir); ++ctx->nlaunch;
+  ctx->pending_uvw = ctx->pending_pqr = false;
+  ctx->dir_ready = true;  // z reflected and directions classified
   ctx->sorted_valid = false;
+  ctx->btot_grid_ready = false;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
 
 int parcel_haloswap(pmpic_ctx* ctx) {
   TimerScope ts(ctx, T_HSWP);
+  if (!ctx->dir_ready) {
+    int frc = flush_gathers(ctx);
+    if (frc) return frc;
+  }
   const int64_t n = ctx->n;
   ctx->sorted_valid = false;
+  ctx->btot_grid_ready = false;
+  const bool ready = ctx->dir_ready;
+  ctx->dir_ready = false;
   if (n == 0) return 0;
-  k_reflect_classify<<<nblk(n, 256), 256, 0, ctx->stream>>>(ctx->g, n, prop(ctx, PMPIC_PROP_X),
-                                                            prop(ctx, PMPIC_PROP_Y), prop(ctx, PMPIC_PROP_Z),
-                                                            ctx->dir); ++ctx->nlaunch;
+  if (!ready) {
+    k_reflect_classify<<<nblk(n, 256), 256, 0, ctx->stream>>>(ctx->g, n, prop(ctx, PMPIC_PROP_X),
+                                                              prop(ctx, PMPIC_PROP_Y), prop(ctx, PMPIC_PROP_Z),
+                                                              ctx->dir); ++ctx->nlaunch;
+  }
   int32_t* V = ctx->aux;                 // vacated slots, ascending
   int32_t* M = ctx->keep;                // moved parcels in send order (keep is free outside mixing)
   int32_t* nm = dcounter(ctx, 0);
@@ -550,6 +663,8 @@ int parcel_haloswap(pmpic_ctx* ctx) {
 }
 
 int splitting(pmpic_ctx* ctx) {
+  int frc = flush_gathers(ctx);
+  if (frc) return frc;
   const int64_t n = ctx->n;
   int32_t* flag = ctx->aux;
   int32_t* list = ctx->keep;
@@ -573,6 +688,8 @@ int splitting(pmpic_ctx* ctx) {
 }
 
 int mixing(pmpic_ctx* ctx) {
+  int frc = flush_gathers(ctx);
+  if (frc) return frc;
   const Geom& g = ctx->g;
   const int64_t norig = ctx->n;
   int rc;
@@ -602,8 +719,8 @@ int mixing(pmpic_ctx* ctx) {
   }
   k_residual_update<<<nblk(g.nphys, 256), 256, 0, ctx->stream>>>(g, RP, ctx->newslot, ctx->newportion); ++ctx->nlaunch;
   if (norig > 0) {
-    k_redistribute<<<nblk(norig, 256), 256, 0, ctx->stream>>>(g, norig, ctx->keep, ctx->parcels, ctx->cap, RP,
-                                                              ctx->dinfo); ++ctx->nlaunch;
+    k_redistribute<<<nblk(norig, 256), 256, 0, ctx->stream>>>(g, norig, ctx->keep, ctx->parcels, ctx->cap,
+                                                              ctx->cell, ctx->del, RP); ++ctx->nlaunch;
   }
   // counts to the host: removed, new cells
   int32_t h[2];
@@ -635,6 +752,7 @@ int mixing(pmpic_ctx* ctx) {
   }
   ctx->n = count;
   ctx->sorted_valid = false;
+  ctx->btot_grid_ready = false;
   ctx->info.n_removed = nremove;
   ctx->info.n_added = nadd;
   PMPIC_CUDA(cudaGetLastError());

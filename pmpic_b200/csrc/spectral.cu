@@ -159,28 +159,41 @@ __global__ void k_vel(Geom g, int mode, const double* __restrict__ e, const doub
 // to every element before the sum).
 __global__ void k_zmode(Geom g, const double* __restrict__ d, const double* __restrict__ e,
                         double* __restrict__ zb) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  extern __shared__ double zs[];  // e(:,1,1), d(:,1,1), then ubar, vbar
   const int nz = g.nzp;
   const int64_t cs = (int64_t)g.sx * g.sy;
+  double* es = zs;
+  double* ds = zs + nz;
+  for (int k = threadIdx.x; k < nz; k += blockDim.x) {  // stage the zero-mode columns
+    es[k] = e[k * cs];
+    ds[k] = d[k * cs];
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
   double* ubar = zb;
   double* vbar = zb + nz;
   const double dz = g.dz;
-  ubar[0] = 0;
-  vbar[0] = 0;
+  double u = 0, v = 0;
+  double* us = zs + 2 * nz;
+  double* vs = zs + 3 * nz;
+  us[0] = 0;
+  vs[0] = 0;
   for (int k = 0; k < nz - 1; ++k) {
-    ubar[k + 1] = ubar[k] + dz / 2. * (e[k * cs] + e[(k + 1) * cs]);
-    vbar[k + 1] = vbar[k] - dz / 2. * (d[k * cs] + d[(k + 1) * cs]);
+    u = u + dz / 2. * (es[k] + es[k + 1]);
+    v = v - dz / 2. * (ds[k] + ds[k + 1]);
+    us[k + 1] = u;
+    vs[k + 1] = v;
   }
   const double inz = (double)(1.0f / (float)nz);
   double su = 0.0, sv = 0.0;
   for (int k = 0; k < nz - 1; ++k) {
-    su = su + (ubar[k] + f4(0.5f) * ubar[nz - 1]);
-    sv = sv + (vbar[k] + f4(0.5f) * vbar[nz - 1]);
+    su = su + (us[k] + f4(0.5f) * us[nz - 1]);
+    sv = sv + (vs[k] + f4(0.5f) * vs[nz - 1]);
   }
   double uavg = inz * su, vavg = inz * sv;
   for (int k = 0; k < nz; ++k) {
-    ubar[k] = ubar[k] - uavg;
-    vbar[k] = vbar[k] - vavg;
+    ubar[k] = us[k] - uavg;
+    vbar[k] = vs[k] - vavg;
   }
 }
 
@@ -486,7 +499,7 @@ int vort2vel_spectral(pmpic_ctx* ctx) {
   if ((rc = fft_backward(ctx, d, ctx->grid[PMPIC_GRID_P]))) return rc;
   if ((rc = fft_backward(ctx, e, ctx->grid[PMPIC_GRID_Q]))) return rc;
   if ((rc = fft_backward(ctx, f, ctx->grid[PMPIC_GRID_R]))) return rc;
-  k_zmode<<<1, 32, 0, ctx->stream>>>(g, d, e, ctx->zmode); ++ctx->nlaunch;
+  k_zmode<<<1, 256, sizeof(double) * 4 * g.nzp, ctx->stream>>>(g, d, e, ctx->zmode); ++ctx->nlaunch;
   if ((rc = spec_laplinv(ctx, a, false))) return rc;
   if ((rc = spec_laplinv(ctx, b, false))) return rc;
   if ((rc = spec_laplinv(ctx, c, true))) return rc;

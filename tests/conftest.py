@@ -22,7 +22,8 @@ def pytest_configure(config):
 @pytest.fixture(scope="session", autouse=True)
 def built_libraries():
     """Build the oracle and the GPU library in-tree if they are missing."""
-    for sub, lib in [("oracle", "liboracle.so"), ("pmpic_b200", "libpmpic_gpu.so")]:
+    for sub, lib in [("oracle", "liboracle.so"), ("pmpic_b200", "libpmpic_gpu.so"),
+                     ("pmpic_b200", "pmpic_monc")]:
         if not os.path.exists(os.path.join(ROOT, sub, lib)):
             subprocess.run(["make", "-s", "-C", os.path.join(ROOT, sub)], check=True)
     yield
