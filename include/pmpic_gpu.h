@@ -47,6 +47,7 @@ extern "C" {
 #define PMPIC_ERR_CUDA       -7  /* CUDA runtime error */
 #define PMPIC_ERR_ARG        -8  /* invalid argument */
 #define PMPIC_ERR_STATE      -9  /* call not valid in the current state */
+#define PMPIC_ERR_TOO_LARGE -10  /* size beyond a fixed static maximum (pmpic_par2grid_static) */
 
 /* ---- precision forms ---------------------------------------------------- */
 #define PMPIC_FP64  0            /* plain FP64 throughout (the reference's DEFAULT_PRECISION) */
@@ -167,6 +168,26 @@ int pmpic_op_diffz(pmpic_ctx* ctx, const double* in, double* out, const double* 
 int pmpic_op_laplinv(pmpic_ctx* ctx, double* inout, int df_zero_on_boundary);
 /* parcel_haloswap (parcels/haloswap.F90:109-289), single-GPU semantics. */
 int pmpic_op_parcel_haloswap(pmpic_ctx* ctx);
+
+/* par2grid without a context and without allocation.  No counterpart in the
+ * reference: an addition for callers that cannot allocate device memory at call
+ * time.  Same arithmetic and result as pmpic_op_par2grid (binning
+ * parcel_interpolation.F90:186-262, par2grid :336-481) of one field with volume
+ * weights over an nx x ny x nz box [0,lx) x [0,ly) x [0,lz].  x, y, z, vol,
+ * field are n device doubles; out receives the dense (nz+1) x ny x nx grid on
+ * the device.  Scratch is one fixed static device array (about 4.5 MB per
+ * device): n <= 131072 and nx*ny*nz <= 32768, else PMPIC_ERR_TOO_LARGE with
+ * nothing launched.  The call clears its own counters, runs on `stream`
+ * (a cudaStream_t; NULL = the legacy default stream) and synchronizes it before
+ * returning; PMPIC_ERR_OUT_OF_BOX if a parcel is outside the box.
+ *  - Calls that overlap on one device share the scratch and race: serialize
+ *    them (one stream, or synchronize between calls).
+ *  - The first call on a device, with that device current, looks up the
+ *    scratch address (cudaGetSymbolAddress); make it before capturing the
+ *    stream into a graph. */
+int pmpic_par2grid_static(int32_t nx, int32_t ny, int32_t nz, double lx, double ly, double lz,
+                          int64_t n, const double* x, const double* y, const double* z,
+                          const double* vol, const double* field, double* out, void* stream);
 
 /* ---- instrumentation ------------------------------------------------------ */
 /* Named timers after the reference's timer_mod (register_routine_for_timing /

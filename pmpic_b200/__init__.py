@@ -123,6 +123,8 @@ def lib() -> C.CDLL:
         L.pmpic_event_elapsed.argtypes = [P, C.c_int, C.c_int, C.POINTER(C.c_float)]
         L.pmpic_pin_host.argtypes = [C.c_void_p, C.c_size_t]
         L.pmpic_unpin_host.argtypes = [C.c_void_p]
+        # device pointers as plain integers (e.g. torch data_ptr()), stream as a handle
+        L.pmpic_par2grid_static.argtypes = [C.c_int32] * 3 + [C.c_double] * 3 + [I64] + [C.c_void_p] * 7
         L.pmpic_setup_count.restype = I64
         L.pmpic_setup_count.argtypes = [C.POINTER(ThermalParams)]
         L.pmpic_setup_thermal.argtypes = [C.POINTER(ThermalParams), I64] + [D] * 11

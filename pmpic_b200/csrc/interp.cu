@@ -26,6 +26,8 @@
 //               sums its contributions in one fixed order.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "common.cuh"
 
 namespace pmpic {
@@ -668,3 +670,114 @@ int cell_ids(pmpic_ctx* ctx, int32_t* dcells) {
 
 }  // namespace pmpic
 
+// ---- par2grid without allocation -------------------------------------------------------
+// pmpic_par2grid_static: the same binning, CSR sort and par2grid reduction as
+// pmpic_op_par2grid, for callers that hold no context and may not allocate
+// device memory when they call: a host whose device memory is handed in full
+// to its own pool allocator, or a component callback that must keep the
+// device footprint fixed between steps.  Its scratch lives in one file-scope
+// device array of fixed size, so a call allocates nothing; the per-device
+// address of that array is looked up once, on the first call made with that
+// device current.
+namespace pmpic {
+namespace {
+
+constexpr int64_t SP_MAX_PARCELS = 131072;  // parcels per call
+constexpr int64_t SP_MAX_CELLS = 32768;     // nx*ny*nz per call
+constexpr int64_t SP_MAX_TILES = (SP_MAX_CELLS + SCAN_TILE - 1) / SCAN_TILE + 1;
+constexpr size_t sp_round(size_t b) { return (b + 255) / 256 * 256; }
+// scratch layout (byte offsets)
+constexpr size_t SP_DEL = 0;                                                         // double[3][MAX_PARCELS]
+constexpr size_t SP_SORTED = SP_DEL + sp_round(sizeof(double) * 3 * SP_MAX_PARCELS);  // int32[MAX_PARCELS]
+constexpr size_t SP_CELL = SP_SORTED + sp_round(sizeof(int32_t) * SP_MAX_PARCELS);    // int32[MAX_PARCELS]
+constexpr size_t SP_COUNT = SP_CELL + sp_round(sizeof(int32_t) * SP_MAX_PARCELS);     // int32[MAX_CELLS+1]
+constexpr size_t SP_START = SP_COUNT + sp_round(sizeof(int32_t) * (SP_MAX_CELLS + 1));  // int32[MAX_CELLS+1]
+constexpr size_t SP_FILL = SP_START + sp_round(sizeof(int32_t) * (SP_MAX_CELLS + 1));   // int32[MAX_CELLS]
+constexpr size_t SP_TILES = SP_FILL + sp_round(sizeof(int32_t) * SP_MAX_CELLS);         // int32[MAX_TILES]
+constexpr size_t SP_INFO = SP_TILES + sp_round(sizeof(int32_t) * SP_MAX_TILES);         // DevInfo
+constexpr size_t SP_BYTES = SP_INFO + sp_round(sizeof(DevInfo));                        // about 4.5 MB
+
+__device__ __align__(256) unsigned char g_p2g_scratch[SP_BYTES];
+
+constexpr int SP_MAX_DEVICES = 64;
+std::mutex sp_mutex;
+void* sp_addr[SP_MAX_DEVICES] = {};
+
+}  // namespace
+}  // namespace pmpic
+
+extern "C" int pmpic_par2grid_static(int32_t nx, int32_t ny, int32_t nz, double lx, double ly, double lz,
+                                     int64_t n, const double* x, const double* y, const double* z,
+                                     const double* vol, const double* field, double* out, void* stream) {
+  using namespace pmpic;
+  if (nx < 1 || ny < 1 || nz < 1 || !(lx > 0) || !(ly > 0) || !(lz > 0) || n < 0 || !out) return PMPIC_ERR_ARG;
+  if (n > 0 && (!x || !y || !z || !vol || !field)) return PMPIC_ERR_ARG;
+  const int64_t ncell = (int64_t)nx * ny * nz;
+  if (n > SP_MAX_PARCELS || ncell > SP_MAX_CELLS) return PMPIC_ERR_TOO_LARGE;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= SP_MAX_DEVICES) return PMPIC_ERR_CUDA;
+  unsigned char* base;
+  {
+    std::lock_guard<std::mutex> lk(sp_mutex);
+    if (!sp_addr[dev]) {  // set-up, once per device: the array's address on this device
+      void* p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_p2g_scratch) != cudaSuccess || !p) return PMPIC_ERR_CUDA;
+      sp_addr[dev] = p;
+    }
+    base = (unsigned char*)sp_addr[dev];
+  }
+  double* del = (double*)(base + SP_DEL);
+  int32_t* sorted = (int32_t*)(base + SP_SORTED);
+  int32_t* cell = (int32_t*)(base + SP_CELL);
+  int32_t* count = (int32_t*)(base + SP_COUNT);
+  int32_t* cstart = (int32_t*)(base + SP_START);
+  int32_t* fill = (int32_t*)(base + SP_FILL);
+  int32_t* tiles = (int32_t*)(base + SP_TILES);
+  DevInfo* info = (DevInfo*)(base + SP_INFO);
+  cudaStream_t st = (cudaStream_t)stream;
+
+  // geometry: the binning and par2grid subset of pmpic_create's (origin 0)
+  Geom g{};
+  g.Nx = nx; g.Ny = ny; g.Nz = nz; g.nzp = nz + 1;
+  g.sx = nx + 2; g.sy = ny + 2;
+  g.ncell = ncell;
+  g.nphys = (int64_t)g.nzp * ny * nx;
+  g.nspec = (int64_t)g.nzp * g.sy * g.sx;
+  g.dx = lx / (double)nx;
+  g.dy = ly / (double)ny;
+  g.dz = lz / (double)nz;
+  g.pxmin = (double)(-2) * g.dx;
+  g.pymin = (double)(-2) * g.dy;
+  g.pzmin = 0.0;
+  g.pzmax = (double)nz * g.dz;
+
+  // the counters and the error word must start at zero: cleared on every call
+  if (cudaMemsetAsync(count, 0, sizeof(int32_t) * (ncell + 1), st) != cudaSuccess) return PMPIC_ERR_CUDA;
+  if (cudaMemsetAsync(fill, 0, sizeof(int32_t) * ncell, st) != cudaSuccess) return PMPIC_ERR_CUDA;
+  if (cudaMemsetAsync(info, 0, sizeof(DevInfo), st) != cudaSuccess) return PMPIC_ERR_CUDA;
+  if (n > 0)
+    k_bin_count<<<nblk(n, 256), 256, 0, st>>>(g, n, x, y, z, cell, del, SP_MAX_PARCELS, count, info);
+  const int64_t ntiles = (ncell + SCAN_TILE - 1) / SCAN_TILE;
+  k_scan_tiles<<<(unsigned)ntiles, SCAN_BLOCK, 0, st>>>(count, ncell, tiles);
+  k_scan_sums<<<1, SCAN_BLOCK, 0, st>>>(tiles, ntiles, cstart + ncell);
+  k_scan_apply<<<(unsigned)ntiles, SCAN_BLOCK, 0, st>>>(count, ncell, tiles, cstart);
+  if (n > 0) {
+    k_bin_scatter<<<nblk(n, 256), 256, 0, st>>>(n, cell, cstart, fill, sorted);
+    k_sort_segments<<<nblk(ncell, 256), 256, 0, st>>>(ncell, cstart, sorted);
+  }
+  using Lay = P2GLayout<1, 0, false>;
+  auto kern = k_par2grid<1, 0, false>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::smem) != cudaSuccess)
+    return PMPIC_ERR_CUDA;
+  P2GArgs<1> a{};
+  a.f[0] = field;
+  a.out[0] = out;
+  dim3 grid((nx + TX - 1) / TX, (ny + TY - 1) / TY, (g.nzp + ZCHUNK - 1) / ZCHUNK);
+  kern<<<grid, P2G_THREADS, Lay::smem, st>>>(g, cstart, sorted, del, SP_MAX_PARCELS, vol, a);
+  if (cudaGetLastError() != cudaSuccess) return PMPIC_ERR_CUDA;
+  int err = 0;
+  if (cudaMemcpyAsync(&err, &info->error, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return PMPIC_ERR_CUDA;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return PMPIC_ERR_CUDA;
+  return err;
+}
