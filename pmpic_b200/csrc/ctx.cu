@@ -180,6 +180,8 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
       !smooth235(cfg->ny) || cfg->max_parcels <= 0 || cfg->max_parcels >= (int64_t)0x7fffffff ||
       cfg->precision != PMPIC_FP64)
     return PMPIC_ERR_CONFIG;
+  // cell ids and grid offsets are 32-bit: the largest grid, the spectral one, must fit
+  if ((int64_t)(cfg->nz + 1) * (cfg->ny + 2) * (cfg->nx + 2) >= (int64_t)0x7fffffff) return PMPIC_ERR_CONFIG;
   if (cfg->xmin != 0.0 || cfg->ymin != 0.0 || cfg->zmin != 0.0 || !(cfg->xmax > 0) || !(cfg->ymax > 0) ||
       !(cfg->zmax > 0))
     return PMPIC_ERR_CONFIG;

@@ -44,16 +44,6 @@ constexpr int P2G_WARPS = P2G_THREADS / 32;
 constexpr int ZCHUNK = 16;            // grid levels per CTA
 constexpr int RANKS = 4;              // in-cell ranks per staged slice
 constexpr int PPT = (NCELLT * RANKS + P2G_THREADS - 1) / P2G_THREADS;  // (cell, rank) pairs per thread
-// Staging position of cell c's rank ul: the cell index rotated by a per-rank
-// offset.  A warp's cp.async copies cover 8 consecutive cells x 4 ranks; with
-// rank rows 153 doubles apart the offsets 0, 15, 14, 13 put ranks 0/1 and 2/3
-// in complementary halves of the 32 banks (two wavefronts per copy), while
-// the reduction, one thread per cell, still reads consecutive addresses.
-__device__ __forceinline__ int stage_pos(int c, int ul) {
-  const int r = ul == 0 ? 0 : 16 - ul;
-  const int p = c + r;
-  return p >= NCELLT ? p - NCELLT : p;
-}
 constexpr int MAXSEG = 32;            // cell segments sorted in registers
 
 inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
@@ -76,7 +66,10 @@ __global__ void k_bin_count(Geom g, int64_t n, const double* __restrict__ X, con
   del[t] = dx;
   del[cap + t] = dy;
   del[2 * cap + t] = dz;
-  atomicAdd(&count[id], 1);
+  // neighbouring slots mostly share a cell: one atomic per distinct cell of the warp
+  const unsigned act = __activemask();
+  const unsigned same = __match_any_sync(act, id);
+  if ((threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&count[id], __popc(same));
 }
 
 __global__ void k_bin_scatter(int64_t n, const int32_t* __restrict__ cell, const int32_t* __restrict__ start,
@@ -85,7 +78,16 @@ __global__ void k_bin_scatter(int64_t n, const int32_t* __restrict__ cell, const
   if (t >= n) return;
   int32_t id = cell[t];
   if (id < 0) return;
-  int32_t pos = start[id] + atomicAdd(&fill[id], 1);
+  // one atomic per distinct cell of the warp; lanes take consecutive places in
+  // lane order (the segment is sorted by slot afterwards in any case)
+  const unsigned act = __activemask();
+  const unsigned same = __match_any_sync(act, id);
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(same) - 1;
+  int32_t base = 0;
+  if (lane == leader) base = atomicAdd(&fill[id], __popc(same));
+  base = __shfl_sync(same, base, leader);
+  const int32_t pos = start[id] + base + __popc(same & ((1u << lane) - 1));
   sorted[pos] = (int32_t)t;
 }
 
@@ -338,7 +340,7 @@ __global__ void __launch_bounds__(P2G_THREADS, 2)
       const int n = nid[i];
       if (n < 0) continue;
       const int pr = t + i * P2G_THREADS;
-      double* D = S + (pr % RANKS) * NCELLT + stage_pos(pr / RANKS, pr % RANKS);
+      double* D = S + (pr % RANKS) * NCELLT + pr / RANKS;
       cp_async8(D, DX + n);
       cp_async8(D + FS, DY + n);
       cp_async8(D + 2 * FS, DZ + n);
@@ -408,7 +410,7 @@ __global__ void __launch_bounds__(P2G_THREADS, 2)
 #pragma unroll
       for (int ul = 0; ul < RANKS; ++ul) {
         if (ul >= nu) break;
-        const double* S = S0 + ul * NCELLT + stage_pos(c, ul);
+        const double* S = S0 + ul * NCELLT + c;
         const double delx = S[0], dely = S[FS], delz = S[2 * FS], vv = S[3 * FS];
         if (MODE == 1 && vv < a.vmin) continue;    // parcel_mixing.F90:488
         if (MODE == 2 && !(vv < a.vmin)) continue;
@@ -605,14 +607,19 @@ static int launch_p2g(pmpic_ctx* ctx, const double* const* fields, double* const
 // parcel_mixing construct_grids (:440-624) + mixing_haloswap + wall doubling:
 // kept grids into VOL, B, HG, P, Q, R (as the reference reuses state%vol,
 // state%b, state%hg, state%p, ...), residual grids into mixres, npercell.
-int launch_mix_grids(pmpic_ctx* ctx) {
+// With no parcel in the removed class (any_removed false) its sums are all
+// +0.0, which a memset gives without a pass over the parcels.
+int launch_mix_grids(pmpic_ctx* ctx, bool any_removed) {
   const double* f[6] = {nullptr, prop(ctx, PMPIC_PROP_B), prop(ctx, PMPIC_PROP_H),
                         prop(ctx, PMPIC_PROP_P), prop(ctx, PMPIC_PROP_Q), prop(ctx, PMPIC_PROP_R)};
   double* kept[6] = {ctx->grid[PMPIC_GRID_VOL], ctx->grid[PMPIC_GRID_B], ctx->grid[PMPIC_GRID_HG],
                      ctx->grid[PMPIC_GRID_P],   ctx->grid[PMPIC_GRID_Q], ctx->grid[PMPIC_GRID_R]};
   int rc = launch_p2g<6, 1, false>(ctx, f, kept);
   if (rc) return rc;
-  return launch_p2g<6, 2, false>(ctx, f, ctx->mixres);
+  if (any_removed) return launch_p2g<6, 2, false>(ctx, f, ctx->mixres);
+  for (int q = 0; q < 6; ++q)
+    PMPIC_CUDA(cudaMemsetAsync(ctx->mixres[q], 0, sizeof(double) * ctx->g.nphys, ctx->stream));
+  return 0;
 }
 
 // par2grid of nf fields with the same weights; with btot the last field is

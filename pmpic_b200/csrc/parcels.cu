@@ -13,7 +13,7 @@
 namespace pmpic {
 
 int scan_excl(pmpic_ctx* ctx, const int32_t* in, int64_t n, int32_t* out);
-int launch_mix_grids(pmpic_ctx* ctx);
+int launch_mix_grids(pmpic_ctx* ctx, bool any_removed);
 
 namespace {
 
@@ -475,7 +475,7 @@ __global__ void k_residual_update(Geom g, ResPtrs RP, const int32_t* __restrict_
 
 // residuals onto the kept original parcels (:245-342), with the binning
 // cached at the start of mixing (:80; kept parcels have not moved)
-__global__ void k_redistribute(Geom g, int64_t norig, const int32_t* __restrict__ keep, double* __restrict__ parcels,
+__global__ void __launch_bounds__(256, 3) k_redistribute(Geom g, int64_t norig, const int32_t* __restrict__ keep, double* __restrict__ parcels,
                                int64_t cap, const int32_t* __restrict__ cell, const double* __restrict__ del,
                                ResPtrs RP) {
   int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -486,10 +486,10 @@ __global__ void k_redistribute(Geom g, int64_t norig, const int32_t* __restrict_
   const double delx = del[m], dely = del[cap + m], delz = del[2 * cap + m];
   const int ci = id % g.Nx, cj = (id / g.Nx) % g.Ny, ck = id / (g.Nx * g.Ny);
   int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
-  size_t c[8] = {((size_t)ck * g.Ny + cj) * g.Nx + ci,        ((size_t)ck * g.Ny + cj) * g.Nx + ci1,
-                 ((size_t)ck * g.Ny + cj1) * g.Nx + ci,       ((size_t)ck * g.Ny + cj1) * g.Nx + ci1,
-                 ((size_t)(ck + 1) * g.Ny + cj) * g.Nx + ci,  ((size_t)(ck + 1) * g.Ny + cj) * g.Nx + ci1,
-                 ((size_t)(ck + 1) * g.Ny + cj1) * g.Nx + ci, ((size_t)(ck + 1) * g.Ny + cj1) * g.Nx + ci1};
+  // grid offsets fit in 32 bits (pmpic_create limits (nz+1)*ny*nx)
+  const int r0 = (ck * g.Ny + cj) * g.Nx, r1 = (ck * g.Ny + cj1) * g.Nx;
+  const int r2 = ((ck + 1) * g.Ny + cj) * g.Nx, r3 = ((ck + 1) * g.Ny + cj1) * g.Nx;
+  const int c[8] = {r0 + ci, r0 + ci1, r1 + ci, r1 + ci1, r2 + ci, r2 + ci1, r3 + ci, r3 + ci1};
   const double v = A(PMPIC_PROP_VOL)[m];
   double w[8];
   w[0] = (1 - delz) * (1 - dely) * (1 - delx) * v;
@@ -698,11 +698,16 @@ int mixing(pmpic_ctx* ctx) {
     k_keep<<<nblk(norig, 256), 256, 0, ctx->stream>>>(norig, prop(ctx, PMPIC_PROP_VOL), g.vmin, ctx->keep); ++ctx->nlaunch;
   }
   if ((rc = bin_and_sort(ctx))) return rc;
-  if ((rc = launch_mix_grids(ctx))) return rc;
-  // removed slots Z (ascending) and under-populated cells in loop order
+  // removed slots Z (ascending), counted first: the removed-class grids need a
+  // pass over the parcels only when the class is not empty
   int32_t* zlist = ctx->aux;
   int32_t* nz0 = dcounter(ctx, 3);
   if ((rc = compact(ctx, PredKeepEq{ctx->keep, 0}, norig, zlist, nz0))) return rc;
+  int32_t hz0 = 0;
+  PMPIC_CUDA(cudaMemcpyAsync(&hz0, nz0, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
+  if ((rc = launch_mix_grids(ctx, hz0 > 0))) return rc;
+  // under-populated cells in loop order
   int32_t* olist = ctx->cell_fill;  // ncell entries; free after bin_and_sort
   int32_t* nnew = dcounter(ctx, 4);
   if ((rc = compact(ctx, PredNewCell{ctx->npercell, g.Nx, g.Ny, g.Nz}, g.ncell, olist, nnew))) return rc;
