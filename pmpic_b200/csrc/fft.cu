@@ -529,7 +529,7 @@ __global__ void __launch_bounds__(FS_THREADS) k4_inv_y(Geom g, const double2* __
                                                        const double* __restrict__ mid, double* __restrict__ phys) {
   // rows of Y and X are padded so the 8 column pairs of a warp access fall in
   // distinct shared-memory banks
-  constexpr int N = N1 * N2, RP = 8, YS = N1 * (N2 + 1) + 1, XS = N + 1;
+  constexpr int N = N1 * N2, RP = 8, YS = N1 * (N2 + 1) + 1;
   __shared__ double2 Y[RP * YS];
   const int t = threadIdx.x, Nx = g.Nx;
   const int x0 = blockIdx.x * 2 * RP, k = blockIdx.y;

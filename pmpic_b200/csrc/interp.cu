@@ -16,14 +16,14 @@
 //   3. scatter: slot indices into cell order, then each cell segment sorted
 //               by slot index, so every later sum runs in slot order;
 //   4. reduce:  one CTA per 16x8 column tile and 16 grid levels walks the
-//               cell layers upwards.  For each layer the tile's parcels (17x9
-//               cells incl. the low periodic halo) are streamed into shared
-//               memory with cp.async gathers in double-buffered rank slices,
-//               then one thread per cell accumulates its parcels' eight corner
-//               weights from shared memory in slot order and adds them into
-//               the level accumulators in four parity phases (cells of one
-//               parity class touch disjoint grid points), so every grid point
-//               sums its contributions in one fixed order.
+//               cell layers upwards.  A producer warp streams each layer's
+//               parcels (17x9 cells incl. the low periodic halo) into a ring of
+//               shared-memory buffers with cp.async gathers, handing them over
+//               through mbarriers; one consumer thread per cell accumulates its
+//               parcels' eight corner weights in slot order, and the cells add
+//               them into the level accumulators in four parity phases (cells
+//               of one parity class touch disjoint grid points), so every grid
+//               point sums its contributions in one fixed order.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -39,11 +39,12 @@ constexpr int TY = 8;                 // ... in y
 constexpr int CX = TX + 1;            // cells per tile row incl. the low halo cell
 constexpr int CY = TY + 1;
 constexpr int NCELLT = CX * CY;       // 153 cells per tile layer
-constexpr int P2G_THREADS = 320;      // >= 2 * NCELLT, two threads per cell
-constexpr int P2G_WARPS = P2G_THREADS / 32;
+constexpr int P2G_CONS = 160;         // consumer threads (>= NCELLT), one per cell
+constexpr int P2G_THREADS = P2G_CONS + 32;  // + one producer warp
 constexpr int ZCHUNK = 16;            // grid levels per CTA
-constexpr int RANKS = 4;              // in-cell ranks per staged slice
-constexpr int PPT = (NCELLT * RANKS + P2G_THREADS - 1) / P2G_THREADS;  // (cell, rank) pairs per thread
+constexpr int RANKS = 2;              // in-cell ranks per staged slice
+constexpr int NBUF = 4;               // staging buffers in the ring
+constexpr int NTAB = 4;               // layer tables in the ring
 constexpr int MAXSEG = 32;            // cell segments sorted in registers
 
 inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
@@ -222,11 +223,6 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
 
 template <int NQ, int MODE, bool BT>
 struct P2GLayout {
@@ -236,192 +232,279 @@ struct P2GLayout {
   static constexpr int NS = 4 + NF;                         // + delx, dely, delz, vol
   static constexpr int FS = RANKS * NCELLT;                 // stride between staged fields
   static constexpr size_t stage_elems = (size_t)NS * FS;    // one staging buffer
-  static constexpr size_t stage_bytes = sizeof(double) * 2 * stage_elems;
+  static constexpr size_t stage_bytes = sizeof(double) * NBUF * stage_elems;
   static constexpr size_t acc_bytes = sizeof(double) * 2 * NCELLT * NA;  // two grid levels
-  static constexpr size_t tab_bytes = sizeof(int) * (8 * NCELLT + 4 * P2G_WARPS);
-  static constexpr size_t smem = stage_bytes + acc_bytes + tab_bytes;
+  static constexpr size_t tab_bytes = sizeof(int) * (2 * NTAB * NCELLT + NTAB);
+  static constexpr size_t bar_bytes = sizeof(uint64_t) * (2 * NBUF + NTAB) + 16;
+  static constexpr size_t smem = stage_bytes + acc_bytes + tab_bytes + bar_bytes;
 };
 
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* b, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+// arrives on b once every cp.async this thread issued before has landed
+__device__ __forceinline__ void mbar_arrive_on_copies(uint64_t* b) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+constexpr unsigned long long WAIT_LIMIT_NS = 4000000000ull;  // 4 s: a chunk lands in microseconds
+// Wait for the phase of parity `parity` of b to complete.  Gives up after
+// WAIT_LIMIT_NS, or at once when *abort is set; returns false then, with *abort set.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, int parity, volatile int* abort) {
+  const uint32_t a = smem_u32(b);
+  unsigned long long t0 = 0;
+  for (int it = 0;; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if ((it & 31) == 31) {
+      if (*abort) return false;
+      const unsigned long long now = global_ns();
+      if (t0 == 0) t0 = now;
+      else if (now - t0 > WAIT_LIMIT_NS) {
+        *abort = 1;
+        return false;
+      }
+    }
+  }
+}
+__device__ __forceinline__ void cons_sync() {  // the consumer warps only
+  asm volatile("bar.sync 1, %0;" ::"n"(P2G_CONS) : "memory");
+}
+// consumer barrier that also returns the OR of `pred` over the consumer threads
+__device__ __forceinline__ bool cons_sync_or(bool pred) {
+  uint32_t r;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, 1, %2, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+      : "=r"(r)
+      : "r"((uint32_t)pred), "n"(P2G_CONS)
+      : "memory");
+  return r != 0;
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // One CTA per TX x TY column tile and ZCHUNK grid levels walks the cell layers
-// upwards.  Per layer the CTA reads each cell's CSR segment (start, length),
-// then streams the layer's parcels through shared memory in rank slices: slice
-// s holds, for every cell of the tile, its parcels of in-cell rank 4s..4s+3
-// (segments are sorted by slot, so rank order is slot order).  The gathers are
-// cp.async copies issued with consecutive threads on consecutive parcels of a
-// cell; the next slice (or the next layer's first slice) is in flight while the
-// current one is reduced.  Two adjacent threads own a cell: thread h keeps the
-// four corners of level ck+h in registers.  The corners are then added into two
-// level accumulators in four parity phases, so each grid point sums its
-// contributions in one fixed order independent of timing.
+// upwards.  One producer warp streams the tile's parcels into a ring of NBUF
+// shared-memory buffers; five consumer warps reduce them, one thread per cell.
+//  - The chunk sequence is (layer, slice) in order: slice s of a layer holds,
+//    for every cell of the tile, its parcels of in-cell rank 2s, 2s+1
+//    (segments are sorted by slot, so rank order is slot order).  An empty
+//    layer still takes one (empty) slice.
+//  - Producer: per layer it loads the cells' CSR segments (start values one
+//    layer ahead, in registers) into a ring of NTAB tables and releases each
+//    table through an mbarrier; per chunk it waits until the consumers have
+//    freed the buffer, issues 8-byte cp.async gathers (slot indices loaded one
+//    chunk ahead, in registers) and arms the buffer's mbarrier to complete
+//    when its copies have landed.  It runs up to NBUF-1 chunks ahead.
+//  - Consumers: each thread accumulates its cell's eight corner weights in
+//    slot order in registers; after a layer's last chunk the cells add their
+//    corners into two shared level accumulators in four parity phases (cells
+//    of one parity class touch disjoint points), so each grid point sums its
+//    contributions in one fixed order independent of timing.
+//  Every mbarrier wait is bounded: a wait that runs out sets PMPIC_ERR_TIMEOUT
+//  and the CTA stops after its copies in flight have landed.
 template <int NQ, int MODE, bool BT>
 __global__ void __launch_bounds__(P2G_THREADS, 2)
     k_par2grid(Geom g, const int32_t* __restrict__ start, const int32_t* __restrict__ sorted,
-               const double* __restrict__ del, int64_t cap, const double* __restrict__ VOL, P2GArgs<NQ> a) {
+               const double* __restrict__ del, int64_t cap, const double* __restrict__ VOL, P2GArgs<NQ> a,
+               DevInfo* info) {
   using Lay = P2GLayout<NQ, MODE, BT>;
   constexpr int NA = Lay::NA, FS = Lay::FS;
   extern __shared__ __align__(16) unsigned char smraw[];
-  double* stage = (double*)smraw;                          // [2][NS][RANKS][NCELLT]
-  double* acc = stage + 2 * Lay::stage_elems;              // [2 levels][NA][NCELLT points]
-  int* tab_s0 = (int*)(acc + 2 * NCELLT * NA);             // [4 layers][NCELLT]
-  int* tab_len = tab_s0 + 4 * NCELLT;                      // [4 layers][NCELLT]
-  int* wmax = tab_len + 4 * NCELLT;                        // [4 layers][P2G_WARPS]
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const int c = t >> 1, h = t & 1;  // this thread's cell and level half
+  double* stage = (double*)smraw;                              // [NBUF][NS][RANKS][NCELLT]
+  double* acc = stage + NBUF * Lay::stage_elems;               // [2 levels][NA][NCELLT points]
+  int* tab_s0 = (int*)(acc + 2 * NCELLT * NA);                 // [NTAB][NCELLT]
+  int* tab_len = tab_s0 + NTAB * NCELLT;                       // [NTAB][NCELLT]
+  int* tab_ns = tab_len + NTAB * NCELLT;                       // [NTAB] slices of the layer
+  uint64_t* bars = (uint64_t*)(((uintptr_t)(tab_ns + NTAB) + 7) & ~(uintptr_t)7);
+  uint64_t* full = bars;                                       // [NBUF] copies landed
+  uint64_t* empty = bars + NBUF;                               // [NBUF] consumers done
+  uint64_t* tabfull = bars + 2 * NBUF;                         // [NTAB] table written
+  volatile int* abort = (volatile int*)(bars + 2 * NBUF + NTAB);
+  const int t = threadIdx.x;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   const int L0 = blockIdx.z * ZCHUNK;
   const int LAST = min(L0 + ZCHUNK, g.nzp) - 1;  // last cell layer walked
   for (int e = t; e < 2 * NCELLT * NA; e += P2G_THREADS) acc[e] = 0.0;
-  // this thread's cell column (c < NCELLT): local (tx, ty), global (ci, cj)
+  if (t == 0) {
+    for (int b = 0; b < NBUF; ++b) {
+      mbar_init(&full[b], 32);
+      mbar_init(&empty[b], P2G_CONS);
+    }
+    for (int s = 0; s < NTAB; ++s) mbar_init(&tabfull[s], 32);
+    *abort = 0;
+  }
+  __syncthreads();
+
+  if (t >= P2G_CONS) {
+    // ================================ producer warp ================================
+    const int lane = t - P2G_CONS;
+    const double* DX = del;
+    const double* DY = del + cap;
+    const double* DZ = del + 2 * cap;
+    constexpr int CPL = (NCELLT + 31) / 32;  // table cells per lane
+    auto fetch = [&](int ck, int* s0, int* len) {
+#pragma unroll
+      for (int i = 0; i < CPL; ++i) {
+        const int c = lane + 32 * i;
+        s0[i] = 0;
+        len[i] = 0;
+        if (c < NCELLT && ck >= 0 && ck < g.Nz) {
+          const int tx = c % CX, ty = c / CX;
+          int ci = x0 - 1 + tx, cj = y0 - 1 + ty;
+          if ((tx > 0 && ci >= g.Nx) || (ty > 0 && cj >= g.Ny)) continue;
+          if (ci < 0) ci += g.Nx;  // low halo cell: periodic wrap (MPIC_Haloswap.F90)
+          if (cj < 0) cj += g.Ny;
+          const int64_t cid = ((int64_t)ck * g.Ny + cj) * g.Nx + ci;
+          s0[i] = start[cid];
+          len[i] = start[cid + 1] - s0[i];
+        }
+      }
+    };
+    int ns0[CPL], nlen[CPL];  // segments of the next layer, in flight
+    fetch(L0 - 1, ns0, nlen);
+    constexpr int PPL = (NCELLT * RANKS + 31) / 32;  // (cell, rank) pairs per lane
+    int nid[PPL];
+    auto load_idx = [&](int slot, int s) {
+#pragma unroll
+      for (int i = 0; i < PPL; ++i) {
+        const int pr = lane + 32 * i;
+        nid[i] = -1;
+        if (pr < NCELLT * RANKS) {
+          const int c = pr / RANKS, u = s * RANKS + pr % RANKS;
+          if (u < tab_len[slot * NCELLT + c]) nid[i] = sorted[tab_s0[slot * NCELLT + c] + u];
+        }
+      }
+    };
+    int k = 0;  // chunk counter
+    bool ok = true;
+    for (int ck = L0 - 1; ck <= LAST && ok; ++ck) {
+      const int li = ck - (L0 - 1), slot = li % NTAB;
+      int ns = 1;
+      for (int s = 0; s < ns && ok; ++s, ++k) {
+        const int b = k % NBUF;
+        if (k >= NBUF && !mbar_wait(&empty[b], ((k / NBUF) - 1) & 1, abort)) {
+          ok = false;
+          break;
+        }
+        if (s == 0) {
+          // this layer's table: its slot was last read for layer ck - NTAB, whose
+          // chunks the consumers finished before freeing buffer b
+          int m = 0;
+#pragma unroll
+          for (int i = 0; i < CPL; ++i) {
+            const int c = lane + 32 * i;
+            if (c < NCELLT) {
+              tab_s0[slot * NCELLT + c] = ns0[i];
+              tab_len[slot * NCELLT + c] = nlen[i];
+            }
+            m = max(m, nlen[i]);
+          }
+          m = __reduce_max_sync(0xffffffffu, m);
+          ns = max(1, (m + RANKS - 1) / RANKS);
+          if (lane == 0) tab_ns[slot] = ns;
+          __syncwarp();
+          mbar_arrive(&tabfull[slot]);
+          if (ck + 1 <= LAST) fetch(ck + 1, ns0, nlen);
+          load_idx(slot, 0);
+        }
+        double* S = stage + (size_t)b * Lay::stage_elems;
+#pragma unroll
+        for (int i = 0; i < PPL; ++i) {
+          const int n = nid[i];
+          if (n < 0) continue;
+          const int pr = lane + 32 * i;
+          double* D = S + (pr % RANKS) * NCELLT + pr / RANKS;
+          cp_async8(D, DX + n);
+          cp_async8(D + FS, DY + n);
+          cp_async8(D + 2 * FS, DZ + n);
+          cp_async8(D + 3 * FS, VOL + n);
+          if (MODE == 0) {
+#pragma unroll
+            for (int qq = 0; qq < (BT ? NQ - 1 : NQ); ++qq) cp_async8(D + (4 + qq) * FS, a.f[qq] + n);
+            if (BT) {
+#pragma unroll
+              for (int qq = 0; qq < 3; ++qq) cp_async8(D + (4 + NQ - 1 + qq) * FS, a.bh[qq] + n);
+            }
+          } else {
+#pragma unroll
+            for (int qq = 1; qq < NQ; ++qq) cp_async8(D + (4 + qq - 1) * FS, a.f[qq] + n);
+          }
+        }
+        mbar_arrive_on_copies(&full[b]);
+        if (s + 1 < ns) load_idx(slot, s + 1);  // the next chunk's indices, one chunk ahead
+      }
+    }
+    if (!ok) atomicCAS(&info->error, 0, PMPIC_ERR_TIMEOUT);
+    cp_async_wait_all();  // every copy has landed before the warp leaves
+    return;
+  }
+
+  // ================================ consumer warps ================================
+  const int c = t;  // this thread's cell (c < NCELLT)
   const int tx = c % CX, ty = c / CX;
   bool has_col = c < NCELLT;
   int ci = x0 - 1 + tx, cj = y0 - 1 + ty;
   if (has_col) {
     if (tx > 0 && ci >= g.Nx) has_col = false;
     if (ty > 0 && cj >= g.Ny) has_col = false;
-    if (ci < 0) ci += g.Nx;  // low halo cell: periodic wrap (MPIC_Haloswap.F90)
+    if (ci < 0) ci += g.Nx;
     if (cj < 0) cj += g.Ny;
   }
   const int parity = (tx & 1) | ((ty & 1) << 1);
-  const double* DX = del;
-  const double* DY = del + cap;
-  const double* DZ = del + 2 * cap;
-
-  // Layer tables live in a ring of four (layers ck-1 .. ck+2 around the layer
-  // being reduced): each cell's CSR segment and the per-warp longest segment.
-  // A table's start values are loaded into registers one layer before they are
-  // stored, so no thread waits on them.
-  auto tb = [](int ck) { return (ck + 1) & 3; };
-  auto fetch = [&](int ck, int& s0, int& len) {
-    s0 = 0;
-    len = 0;
-    if (h == 0 && has_col && ck >= 0 && ck < g.Nz) {
-      const int64_t cid = ((int64_t)ck * g.Ny + cj) * g.Nx + ci;
-      s0 = start[cid];
-      len = start[cid + 1] - s0;
-    }
-  };
-  auto store_table = [&](int ck, int s0, int len) {
-    const int pb = tb(ck);
-    if (h == 0 && c < NCELLT) {
-      tab_s0[pb * NCELLT + c] = s0;
-      tab_len[pb * NCELLT + c] = len;
-    }
-    const int m = __reduce_max_sync(0xffffffffu, len);
-    if (lane == 0) wmax[pb * P2G_WARPS + warp] = m;
-  };
-  // slices of a layer; an empty layer still takes one (empty) slice
-  auto nslices = [&](int ck) {
-    const int pb = tb(ck);
-    int m = 0;
-#pragma unroll
-    for (int w = 0; w < P2G_WARPS; ++w) m = max(m, wmax[pb * P2G_WARPS + w]);
-    return max(1, (m + RANKS - 1) / RANKS);
-  };
-  // The chunk sequence is (layer, slice) in order.  Slot indices of a chunk
-  // are loaded into registers one chunk before its gathers are issued, so the
-  // dependent index load never waits in front of a cp.async.
-  int nid[PPT];
-  auto load_idx = [&](int ck, int s) {
-    const int pb = tb(ck);
-#pragma unroll
-    for (int i = 0; i < PPT; ++i) {
-      const int pr = t + i * P2G_THREADS;
-      nid[i] = -1;
-      if (pr < NCELLT * RANKS) {
-        const int cc = pr / RANKS, u = s * RANKS + pr % RANKS;
-        if (u < tab_len[pb * NCELLT + cc]) nid[i] = sorted[tab_s0[pb * NCELLT + cc] + u];
-      }
-    }
-  };
-  auto issue = [&](int b) {
-    double* S = stage + (size_t)b * Lay::stage_elems;
-#pragma unroll
-    for (int i = 0; i < PPT; ++i) {
-      const int n = nid[i];
-      if (n < 0) continue;
-      const int pr = t + i * P2G_THREADS;
-      double* D = S + (pr % RANKS) * NCELLT + pr / RANKS;
-      cp_async8(D, DX + n);
-      cp_async8(D + FS, DY + n);
-      cp_async8(D + 2 * FS, DZ + n);
-      cp_async8(D + 3 * FS, VOL + n);
-      if (MODE == 0) {
-#pragma unroll
-        for (int qq = 0; qq < (BT ? NQ - 1 : NQ); ++qq) cp_async8(D + (4 + qq) * FS, a.f[qq] + n);
-        if (BT) {
-#pragma unroll
-          for (int qq = 0; qq < 3; ++qq) cp_async8(D + (4 + NQ - 1 + qq) * FS, a.bh[qq] + n);
-        }
-      } else {
-#pragma unroll
-        for (int qq = 1; qq < NQ; ++qq) cp_async8(D + (4 + qq - 1) * FS, a.f[qq] + n);
-      }
-    }
-  };
-
   int cur = 0;  // level accumulator of the current layer's bottom corners
-  int ib = 0;   // staging buffer of the next issue
-  int ns0, nlen;  // start values of the next table to store (layer ck+3)
-  {
-    int s0a, la, s0b, lb, s0c, lc;
-    fetch(L0 - 1, s0a, la);
-    fetch(L0, s0b, lb);
-    fetch(L0 + 1, s0c, lc);
-    fetch(L0 + 2, ns0, nlen);
-    store_table(L0 - 1, s0a, la);
-    if (L0 <= LAST) store_table(L0, s0b, lb);
-    if (L0 + 1 <= LAST) store_table(L0 + 1, s0c, lc);
-  }
-  __syncthreads();
-  int il = L0 - 1, is = 0;  // the chunk whose indices are in nid
-  load_idx(il, is);
-  issue(ib);
-  ib ^= 1;
-  cp_async_commit();
-  if (is + 1 < nslices(il)) ++is;
-  else { ++il; is = 0; }
-  if (il <= LAST) load_idx(il, is);
+  int k = 0;
+  bool ok = true;
   for (int ck = L0 - 1; ck <= LAST; ++ck) {
-    const int pb = tb(ck);
-    const int ns = nslices(ck);
-    double P[4][NA];  // corners (dx, dy) of level ck + h
+    const int li = ck - (L0 - 1), slot = li % NTAB;
+    ok = ok && mbar_wait(&tabfull[slot], (li / NTAB) & 1, abort);
+    const int ns = ok ? tab_ns[slot] : 0;
+    const int mylen = (ok && c < NCELLT) ? tab_len[slot * NCELLT + c] : 0;
+    double P[8][NA];
 #pragma unroll
-    for (int cc = 0; cc < 4; ++cc)
+    for (int cc = 0; cc < 8; ++cc)
 #pragma unroll
       for (int qq = 0; qq < NA; ++qq) P[cc][qq] = 0.0;
     int nkept = 0;
-    const int mylen = c < NCELLT ? tab_len[pb * NCELLT + c] : 0;
-    for (int s = 0; s < ns; ++s) {
-      const int cb = ib ^ 1;  // buffer of slice s (the latest issue)
-      if (il <= LAST) {       // gathers of the next chunk, then its successor's indices
-        issue(ib);
-        ib ^= 1;
+    for (int s = 0; s < ns && ok; ++s, ++k) {
+      const int b = k % NBUF;
+      if (!mbar_wait(&full[b], (k / NBUF) & 1, abort)) {
+        ok = false;
+        break;
       }
-      cp_async_commit();
-      if (il <= LAST) {
-        if (is + 1 < nslices(il)) ++is;
-        else { ++il; is = 0; }
-        if (il <= LAST) load_idx(il, is);
-      }
-      cp_async_wait<1>();
-      __syncthreads();
       const int nu = min(RANKS, mylen - s * RANKS);
-      const double* S0 = stage + (size_t)cb * Lay::stage_elems;
+      const double* S0 = stage + (size_t)b * Lay::stage_elems + c;
 #pragma unroll
       for (int ul = 0; ul < RANKS; ++ul) {
         if (ul >= nu) break;
-        const double* S = S0 + ul * NCELLT + c;
+        const double* S = S0 + ul * NCELLT;
         const double delx = S[0], dely = S[FS], delz = S[2 * FS], vv = S[3 * FS];
         if (MODE == 1 && vv < a.vmin) continue;    // parcel_mixing.F90:488
         if (MODE == 2 && !(vv < a.vmin)) continue;
         if (MODE == 1) ++nkept;
         // parcel_interpolation.F90:390-434: w = (1-delz)(1-dely)(1-delx) v etc.
-        const double wz = h ? delz : 1 - delz, ey = 1 - dely, ex = 1 - delx;
-        double w[4];
-        w[0] = wz * ey * ex * vv;
-        w[1] = wz * ey * delx * vv;
-        w[2] = wz * dely * ex * vv;
-        w[3] = wz * dely * delx * vv;
+        const double ez = 1 - delz, ey = 1 - dely, ex = 1 - delx;
+        double w[8];
+        w[0] = ez * ey * ex * vv;
+        w[1] = ez * ey * delx * vv;
+        w[2] = ez * dely * ex * vv;
+        w[3] = ez * dely * delx * vv;
+        w[4] = delz * ey * ex * vv;
+        w[5] = delz * ey * delx * vv;
+        w[6] = delz * dely * ex * vv;
+        w[7] = delz * dely * delx * vv;
         double fv[NQ];
         if (MODE == 0) {
 #pragma unroll
@@ -436,35 +519,37 @@ __global__ void __launch_bounds__(P2G_THREADS, 2)
           for (int qq = 1; qq < NQ; ++qq) fv[qq] = S[(4 + qq - 1) * FS];
         }
 #pragma unroll
-        for (int cc = 0; cc < 4; ++cc) {
+        for (int cc = 0; cc < 8; ++cc) {
 #pragma unroll
           for (int qq = 0; qq < NQ; ++qq) P[cc][qq] += (MODE != 0 && qq == 0) ? w[cc] : w[cc] * fv[qq];
           if (MODE == 0) P[cc][NA - 1] += w[cc];
         }
       }
-      if (s + 1 < ns) __syncthreads();  // the buffer is refilled by the issue after next
+      mbar_arrive(&empty[b]);  // this thread's reads of buffer b are done
     }
-    if (MODE == 1 && h == 0 && has_col && ck >= L0 && ck < g.Nz && tx > 0 && ty > 0)
+    // uniform stop: the OR over all consumers of "a wait gave up"
+    if (cons_sync_or(!ok || *abort)) break;
+    if (MODE == 1 && has_col && ck >= L0 && ck < g.Nz && tx > 0 && ty > 0)
       a.npercell[((int64_t)ck * g.Ny + cj) * g.Nx + ci] = nkept;
     // corners into the level accumulators, one parity class at a time;
-    // corner cc: dy = cc>>1, dx = cc&1; level ck + h
+    // corner cc: dz = cc>>2, dy = (cc>>1)&1, dx = cc&1
     for (int ph = 0; ph < 4; ++ph) {
-      if (ph) __syncthreads();
+      if (ph) cons_sync();
       if (has_col && parity == ph) {
 #pragma unroll
-        for (int cc = 0; cc < 4; ++cc) {
-          const int px = tx + (cc & 1), py = ty + (cc >> 1);
+        for (int cc = 0; cc < 8; ++cc) {
+          const int px = tx + (cc & 1), py = ty + ((cc >> 1) & 1);
           if (px < CX && py < CY) {
-            double* A = acc + (size_t)(cur ^ h) * NA * NCELLT + py * CX + px;
+            double* A = acc + (size_t)(cur ^ (cc >> 2)) * NA * NCELLT + py * CX + px;
 #pragma unroll
             for (int qq = 0; qq < NA; ++qq) A[qq * NCELLT] += P[cc][qq];
           }
         }
       }
     }
-    __syncthreads();
+    cons_sync();
     // level ck is complete: normalise and store the owned points, clear the level
-    for (int e = t; e < NCELLT; e += P2G_THREADS) {
+    for (int e = t; e < NCELLT; e += P2G_CONS) {
       double* A = acc + (size_t)cur * NA * NCELLT + e;
       const int px = e % CX, py = e / CX;
       const int gx = x0 + px - 1, gy = y0 + py - 1;
@@ -484,15 +569,10 @@ __global__ void __launch_bounds__(P2G_THREADS, 2)
 #pragma unroll
       for (int qq = 0; qq < NA; ++qq) A[qq * NCELLT] = 0.0;
     }
-    // the table of layer ck+3 (its start values arrived during this layer)
-    if (ck + 3 <= LAST) {
-      store_table(ck + 3, ns0, nlen);
-      fetch(ck + 4, ns0, nlen);
-    }
     cur ^= 1;
-    __syncthreads();
+    cons_sync();
   }
-  cp_async_wait<0>();
+  if (t == 0 && *abort) atomicCAS(&info->error, 0, PMPIC_ERR_TIMEOUT);
 }
 
 // ---- grid2par --------------------------------------------------------------------
@@ -599,7 +679,7 @@ static int launch_p2g(pmpic_ctx* ctx, const double* const* fields, double* const
                                   (int)cudaSharedmemCarveoutMaxShared));
   dim3 grid((g.Nx + TX - 1) / TX, (g.Ny + TY - 1) / TY, (g.nzp + ZCHUNK - 1) / ZCHUNK);
   kern<<<grid, P2G_THREADS, Lay::smem, ctx->stream>>>(g, ctx->cell_start, ctx->sorted, ctx->del, ctx->cap,
-                                                      prop(ctx, PMPIC_PROP_VOL), a); ++ctx->nlaunch;
+                                                      prop(ctx, PMPIC_PROP_VOL), a, ctx->dinfo); ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
@@ -780,7 +860,7 @@ extern "C" int pmpic_par2grid_static(int32_t nx, int32_t ny, int32_t nz, double 
   a.f[0] = field;
   a.out[0] = out;
   dim3 grid((nx + TX - 1) / TX, (ny + TY - 1) / TY, (g.nzp + ZCHUNK - 1) / ZCHUNK);
-  kern<<<grid, P2G_THREADS, Lay::smem, st>>>(g, cstart, sorted, del, SP_MAX_PARCELS, vol, a);
+  kern<<<grid, P2G_THREADS, Lay::smem, st>>>(g, cstart, sorted, del, SP_MAX_PARCELS, vol, a, info);
   if (cudaGetLastError() != cudaSuccess) return PMPIC_ERR_CUDA;
   int err = 0;
   if (cudaMemcpyAsync(&err, &info->error, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)
