@@ -134,7 +134,7 @@ struct pmpic_ctx {
   int64_t cap;
   int64_t n;                 // numparcels (host mirror, valid between calls)
   double* parcels;           // NPROP * cap
-  int32_t* cell;             // cap: interior cell id per slot
+  int32_t* cell;             // cap: interior cell id per slot, z fastest: (i*Ny + j)*Nz + k
   double* del;               // 3 x cap: cached delx, dely, delz per slot
   bool sorted_valid;         // cell ids, offsets and cell lists match the current positions
   bool btot_grid_ready;      // gspare holds par2grid(btot) of the current substep
@@ -143,6 +143,7 @@ struct pmpic_ctx {
   bool dir_ready;            // dir[] and the z reflection done for the current positions
   double* gspare;            // spare physical grid
   int32_t* sorted;           // cap: slot indices sorted by cell
+  double* rowpart;           // par2grid row partials (rowpart_bytes)
   int32_t* cell_count;       // ncell + 1
   int32_t* cell_start;       // ncell + 1
   int32_t* cell_fill;        // ncell
@@ -199,6 +200,7 @@ int bin_and_sort(pmpic_ctx* ctx);
 int par2grid_multi(pmpic_ctx* ctx, const double* const* fields, int nf, double* const* out, bool btot_from_bhz);
 int grid2par_multi(pmpic_ctx* ctx, const double* const* grids, int ng, double* const* out);
 int cell_ids(pmpic_ctx* ctx, int32_t* dcells);
+size_t rowpart_bytes(const Geom& g);
 // fft.cu
 int fft_init(pmpic_ctx* ctx);
 int fft_forward(pmpic_ctx* ctx, const double* phys, double* spec);

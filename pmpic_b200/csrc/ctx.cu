@@ -115,7 +115,7 @@ int dalloc(pmpic_ctx* ctx, T** p, size_t count) {
 }
 
 void free_all(pmpic_ctx* c) {
-  void* ptrs[] = {c->parcels, c->cell,     c->del,       c->gspare,     c->sorted,    c->cell_count, c->cell_start, c->cell_fill, c->keep,
+  void* ptrs[] = {c->parcels, c->rowpart,  c->cell,     c->del,       c->gspare,     c->sorted,    c->cell_count, c->cell_start, c->cell_fill, c->keep,
                   c->aux,     c->aux2,     c->dir,       c->swapbuf,    c->scan_tmp,   c->npercell,  c->newslot,
                   c->newportion, c->sa,    c->sb,        c->sc,         c->sd,         c->se,        c->sf,
                   c->sas,     c->sbs,      c->sscratch,  c->fftmid,     c->ftw,        c->kx,        c->ky,
@@ -237,6 +237,7 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   if (!rc) rc = dalloc(ctx, &ctx->del, 3 * cap);
   if (!rc) rc = dalloc(ctx, &ctx->gspare, (size_t)g.nphys);
   if (!rc) rc = dalloc(ctx, &ctx->sorted, cap);
+  if (!rc) rc = dalloc(ctx, (char**)&ctx->rowpart, rowpart_bytes(g));
   if (!rc) rc = dalloc(ctx, &ctx->keep, cap);
   if (!rc) rc = dalloc(ctx, &ctx->aux, cap);
   if (!rc) rc = dalloc(ctx, &ctx->aux2, 2 * (size_t)ctx->nbmax + cap);
@@ -591,9 +592,9 @@ int pmpic_op_cell_ids(pmpic_ctx* ctx, int32_t* cells) {
     int frc = flush_gathers(ctx);
     if (frc) return frc;
   }
-  int rc = cell_ids(ctx, nullptr);
+  int rc = cell_ids(ctx, ctx->aux);
   if (rc) return rc;
-  PMPIC_CUDA(cudaMemcpyAsync(cells, ctx->cell, sizeof(int32_t) * ctx->n, cudaMemcpyDeviceToHost, ctx->stream));
+  PMPIC_CUDA(cudaMemcpyAsync(cells, ctx->aux, sizeof(int32_t) * ctx->n, cudaMemcpyDeviceToHost, ctx->stream));
   return sync_info(ctx);
 }
 

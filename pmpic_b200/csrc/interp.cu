@@ -8,22 +8,18 @@
 // Binning is cached exactly like the reference's cache_parcel_interp_weights:
 // per parcel the interior cell id and delx, dely, delz, computed once per
 // substep with the reference's arithmetic (bit-exact) and reused by par2grid,
-// grid2par and the mixing redistribution.
+// grid2par and the mixing redistribution.  Cell ids here are z fastest,
+// id = (i*Ny + j)*Nz + k, the order in which the set-up stores parcels
+// (basic_parcelsetup.F90:90-118: x outer, z inner), so that the parcels of a
+// column of cells are one contiguous run of the cell-sorted index.
 //
 // par2grid is deterministic and uses no floating-point atomics:
 //   1. bin:     cell ids + cached offsets + an integer histogram per cell;
 //   2. scan:    exclusive scan of the histogram -> CSR offsets per cell;
 //   3. scatter: slot indices into cell order, then each cell segment sorted
 //               by slot index, so every later sum runs in slot order;
-//   4. reduce:  one CTA per 16x8 column tile and 16 grid levels walks the
-//               cell layers upwards.  A producer warp streams each layer's
-//               parcels (17x9 cells incl. the low periodic halo) into a ring of
-//               shared-memory buffers with cp.async gathers, handing them over
-//               through mbarriers; one consumer thread per cell accumulates its
-//               parcels' eight corner weights in slot order, and the cells add
-//               them into the level accumulators in four parity phases (cells
-//               of one parity class touch disjoint grid points), so every grid
-//               point sums its contributions in one fixed order.
+//   4. reduce:  row pass + combine pass (see k_p2g_rows), each grid point
+//               summing its contributions in one fixed order.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -34,17 +30,6 @@ namespace pmpic {
 
 namespace {
 
-constexpr int TX = 16;                // owned grid points per tile in x
-constexpr int TY = 8;                 // ... in y
-constexpr int CX = TX + 1;            // cells per tile row incl. the low halo cell
-constexpr int CY = TY + 1;
-constexpr int NCELLT = CX * CY;       // 153 cells per tile layer
-constexpr int P2G_CONS = 160;         // consumer threads (>= NCELLT), one per cell
-constexpr int P2G_THREADS = P2G_CONS + 32;  // + one producer warp
-constexpr int ZCHUNK = 16;            // grid levels per CTA
-constexpr int RANKS = 2;              // in-cell ranks per staged slice
-constexpr int NBUF = 4;               // staging buffers in the ring
-constexpr int NTAB = 4;               // layer tables in the ring
 constexpr int MAXSEG = 32;            // cell segments sorted in registers
 
 inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
@@ -62,7 +47,7 @@ __global__ void k_bin_count(Geom g, int64_t n, const double* __restrict__ X, con
     atomicCAS(&info->error, 0, PMPIC_ERR_OUT_OF_BOX);
     return;
   }
-  int32_t id = (int32_t)(((int64_t)ck * g.Ny + cj) * g.Nx + ci);
+  int32_t id = (int32_t)(((int64_t)ci * g.Ny + cj) * g.Nz + ck);
   cell[t] = id;
   del[t] = dx;
   del[cap + t] = dy;
@@ -210,6 +195,25 @@ __global__ void k_scan_apply(const int32_t* __restrict__ in, int64_t n, const in
 //         NQ = 6 unnormalised sums of (1, b, h, p, q, r) * w, doubled at the
 //         walls (parcel_mixing.F90:141-152), plus npercell.
 // MODE 2: the same sums for the removed class (vol < vmin), not doubled.
+//
+// Two passes, no atomics; every grid point sums its contributions in one fixed
+// order that does not depend on timing:
+//  1. k_p2g_rows: one warp per (x segment, row of cells y = cy, chunk of ZC
+//     cell layers) walks the segment's columns in x order.  Cell ids are z
+//     fastest, so a column chunk's parcels are one contiguous range of the
+//     cell-sorted index, and with parcels stored in cell order (as the set-up
+//     writes them) one contiguous range of slots: the gathers are coalesced.
+//     Two lanes per cell layer (bottom and top z corner) accumulate the four
+//     xy corners of their z corner over the cell's parcels in slot order.  A
+//     shuffle adds the top corners of layer k-1 to the bottom corners of layer
+//     k (grid level k), and a register carry adds the x-high corners of column
+//     x-1 to the x-low corners of column x (grid point x).  The result, per
+//     grid point and level, is the sum over the point's four cells of this
+//     row, separately for the row below (y-high corners) and above (y-low
+//     corners): the row partials.
+//  2. k_p2g_combine: per grid point, row y-1's y-high part plus row y's y-low
+//     part (and, on the bottom level of a chunk, the chunk below's top level
+//     first), then the normalisation or wall doubling.
 template <int NQ>
 struct P2GArgs {
   const double* f[NQ];  // per-parcel fields (MODE 1/2: f[0] unused)
@@ -219,360 +223,256 @@ struct P2GArgs {
   double vmin;
 };
 
+constexpr int ZC = 16;                    // cell layers per z chunk: two lanes per layer
+constexpr int NLV = ZC + 1;               // grid levels a chunk contributes to
+constexpr int BATCH = 128;                // sorted positions staged per batch
+constexpr int SPAD = BATCH + BATCH / 16;  // staged field stride: position p sits at p + p/16
+constexpr int RW = 4;                     // warps per CTA of the row pass
+constexpr int XSEG = 64;                  // columns per x segment of a warp
+constexpr int PXB = 16;                   // grid points in x per CTA of the combine pass
+
+template <int NQ, int MODE, bool BT>
+struct P2GLayout {
+  static constexpr int NA = MODE == 0 ? NQ + 1 : NQ;  // accumulated quantities per corner
+  static constexpr int NF = MODE == 0 ? NQ : NQ - 1;  // per-parcel fields staged (btot counts as one)
+  static constexpr int NS = 4 + NF + (BT ? 2 : 0);    // + delx, dely, delz, vol (+ h, z for btot)
+  static constexpr int RPS = 2 * NA * NLV;            // doubles of row partials per (chunk, row, column)
+};
+
+// largest row-partial record of any instantiation: MODE 1/2 with NQ = 6
+constexpr int RPS_MAX = 2 * 6 * NLV;
+
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
-
-template <int NQ, int MODE, bool BT>
-struct P2GLayout {
-  static constexpr int NA = MODE == 0 ? NQ + 1 : NQ;        // accumulated quantities
-  static constexpr int NF = MODE == 0 ? (BT ? NQ + 2 : NQ)  // staged per-parcel values
-                                      : NQ - 1;             //   (MODE 1/2: b,h,p,q,r)
-  static constexpr int NS = 4 + NF;                         // + delx, dely, delz, vol
-  static constexpr int FS = RANKS * NCELLT;                 // stride between staged fields
-  static constexpr size_t stage_elems = (size_t)NS * FS;    // one staging buffer
-  static constexpr size_t stage_bytes = sizeof(double) * NBUF * stage_elems;
-  static constexpr size_t acc_bytes = sizeof(double) * 2 * NCELLT * NA;  // two grid levels
-  static constexpr size_t tab_bytes = sizeof(int) * (2 * NTAB * NCELLT + NTAB);
-  static constexpr size_t bar_bytes = sizeof(uint64_t) * (2 * NBUF + NTAB) + 16;
-  static constexpr size_t smem = stage_bytes + acc_bytes + tab_bytes + bar_bytes;
-};
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(uint64_t* b, int count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
-}
-// arrives on b once every cp.async this thread issued before has landed
-__device__ __forceinline__ void mbar_arrive_on_copies(uint64_t* b) {
-  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(b)) : "memory");
-}
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-constexpr unsigned long long WAIT_LIMIT_NS = 4000000000ull;  // 4 s: a chunk lands in microseconds
-// Wait for the phase of parity `parity` of b to complete.  Gives up after
-// WAIT_LIMIT_NS, or at once when *abort is set; returns false then, with *abort set.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, int parity, volatile int* abort) {
-  const uint32_t a = smem_u32(b);
-  unsigned long long t0 = 0;
-  for (int it = 0;; ++it) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (ok) return true;
-    if ((it & 31) == 31) {
-      if (*abort) return false;
-      const unsigned long long now = global_ns();
-      if (t0 == 0) t0 = now;
-      else if (now - t0 > WAIT_LIMIT_NS) {
-        *abort = 1;
-        return false;
-      }
-    }
-  }
-}
-__device__ __forceinline__ void cons_sync() {  // the consumer warps only
-  asm volatile("bar.sync 1, %0;" ::"n"(P2G_CONS) : "memory");
-}
-// consumer barrier that also returns the OR of `pred` over the consumer threads
-__device__ __forceinline__ bool cons_sync_or(bool pred) {
-  uint32_t r;
-  asm volatile(
-      "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, 1, %2, p;\n selp.u32 %0, 1, 0, q;\n}\n"
-      : "=r"(r)
-      : "r"((uint32_t)pred), "n"(P2G_CONS)
-      : "memory");
-  return r != 0;
-}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// One CTA per TX x TY column tile and ZCHUNK grid levels walks the cell layers
-// upwards.  One producer warp streams the tile's parcels into a ring of NBUF
-// shared-memory buffers; five consumer warps reduce them, one thread per cell.
-//  - The chunk sequence is (layer, slice) in order: slice s of a layer holds,
-//    for every cell of the tile, its parcels of in-cell rank 2s, 2s+1
-//    (segments are sorted by slot, so rank order is slot order).  An empty
-//    layer still takes one (empty) slice.
-//  - Producer: per layer it loads the cells' CSR segments (start values one
-//    layer ahead, in registers) into a ring of NTAB tables and releases each
-//    table through an mbarrier; per chunk it waits until the consumers have
-//    freed the buffer, issues 8-byte cp.async gathers (slot indices loaded one
-//    chunk ahead, in registers) and arms the buffer's mbarrier to complete
-//    when its copies have landed.  It runs up to NBUF-1 chunks ahead.
-//  - Consumers: each thread accumulates its cell's eight corner weights in
-//    slot order in registers; after a layer's last chunk the cells add their
-//    corners into two shared level accumulators in four parity phases (cells
-//    of one parity class touch disjoint points), so each grid point sums its
-//    contributions in one fixed order independent of timing.
-//  Every mbarrier wait is bounded: a wait that runs out sets PMPIC_ERR_TIMEOUT
-//  and the CTA stops after its copies in flight have landed.
 template <int NQ, int MODE, bool BT>
-__global__ void __launch_bounds__(P2G_THREADS, 2)
-    k_par2grid(Geom g, const int32_t* __restrict__ start, const int32_t* __restrict__ sorted,
-               const double* __restrict__ del, int64_t cap, const double* __restrict__ VOL, P2GArgs<NQ> a,
-               DevInfo* info) {
+__global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, const int32_t* __restrict__ start,
+                                                     const int32_t* __restrict__ sorted, const double* __restrict__ del,
+                                                     int64_t cap, const double* __restrict__ VOL, P2GArgs<NQ> a,
+                                                     double* __restrict__ rowpart) {
   using Lay = P2GLayout<NQ, MODE, BT>;
-  constexpr int NA = Lay::NA, FS = Lay::FS;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  double* stage = (double*)smraw;                              // [NBUF][NS][RANKS][NCELLT]
-  double* acc = stage + NBUF * Lay::stage_elems;               // [2 levels][NA][NCELLT points]
-  int* tab_s0 = (int*)(acc + 2 * NCELLT * NA);                 // [NTAB][NCELLT]
-  int* tab_len = tab_s0 + NTAB * NCELLT;                       // [NTAB][NCELLT]
-  int* tab_ns = tab_len + NTAB * NCELLT;                       // [NTAB] slices of the layer
-  uint64_t* bars = (uint64_t*)(((uintptr_t)(tab_ns + NTAB) + 7) & ~(uintptr_t)7);
-  uint64_t* full = bars;                                       // [NBUF] copies landed
-  uint64_t* empty = bars + NBUF;                               // [NBUF] consumers done
-  uint64_t* tabfull = bars + 2 * NBUF;                         // [NTAB] table written
-  volatile int* abort = (volatile int*)(bars + 2 * NBUF + NTAB);
-  const int t = threadIdx.x;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-  const int L0 = blockIdx.z * ZCHUNK;
-  const int LAST = min(L0 + ZCHUNK, g.nzp) - 1;  // last cell layer walked
-  for (int e = t; e < 2 * NCELLT * NA; e += P2G_THREADS) acc[e] = 0.0;
-  if (t == 0) {
-    for (int b = 0; b < NBUF; ++b) {
-      mbar_init(&full[b], 32);
-      mbar_init(&empty[b], P2G_CONS);
+  constexpr int NA = Lay::NA, NS = Lay::NS;
+  constexpr unsigned FULL = 0xffffffffu;
+  __shared__ __align__(16) double smem[RW][NS * SPAD];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t wid = (int64_t)blockIdx.x * RW + warp;
+  if (wid >= (int64_t)nxs * g.Ny * nzc) return;  // the whole warp leaves together
+  const int xs = (int)(wid % nxs);
+  const int cy = (int)((wid / nxs) % g.Ny);
+  const int zc = (int)(wid / ((int64_t)nxs * g.Ny));
+  const int x_lo = xs * XSEG, x_hi = min(g.Nx, x_lo + XSEG);
+  const int k0 = zc * ZC, nk = min(ZC, g.Nz - k0);
+  const int kk = lane >> 1, cz = lane & 1;
+  const bool has_cell = kk < nk;
+  // after the z combination lane 0 holds level 0 (bottom corners of layer 0)
+  // and odd lane 2m+1 level m+1 (top corners of layer m + bottom corners of m+1)
+  const int lev = lane == 0 ? 0 : (lane >> 1) + 1;
+  const bool owner = (lane == 0 || (lane & 1)) && lev <= nk;
+  double* S = smem[warp];
+  const double* DX = del;
+  const double* DY = del + cap;
+  const double* DZ = del + 2 * cap;
+  double* out_row = rowpart + ((size_t)zc * g.Ny + cy) * (size_t)g.Nx * Lay::RPS;
+  double C[2][NA];  // x-high corners of the previous column, per y corner
+  // the column before the segment (periodic) only seeds the carry
+  for (int it = -1; it < x_hi - x_lo; ++it) {
+    int cx = x_lo + it;
+    if (cx < 0) cx += g.Nx;
+    const int64_t cb = ((int64_t)cx * g.Ny + cy) * g.Nz + k0;
+    int s_me = 0, e_me = 0;
+    if (has_cell) {
+      s_me = start[cb + kk];
+      e_me = start[cb + kk + 1];
     }
-    for (int s = 0; s < NTAB; ++s) mbar_init(&tabfull[s], 32);
-    *abort = 0;
-  }
-  __syncthreads();
-
-  if (t >= P2G_CONS) {
-    // ================================ producer warp ================================
-    const int lane = t - P2G_CONS;
-    const double* DX = del;
-    const double* DY = del + cap;
-    const double* DZ = del + 2 * cap;
-    constexpr int CPL = (NCELLT + 31) / 32;  // table cells per lane
-    auto fetch = [&](int ck, int* s0, int* len) {
+    const int q0 = __shfl_sync(FULL, s_me, 0);
+    const int q1 = __shfl_sync(FULL, e_me, 2 * nk - 2);
+    double acc[4][NA];  // [y corner * 2 + x corner][quantity] of this lane's z corner
 #pragma unroll
-      for (int i = 0; i < CPL; ++i) {
-        const int c = lane + 32 * i;
-        s0[i] = 0;
-        len[i] = 0;
-        if (c < NCELLT && ck >= 0 && ck < g.Nz) {
-          const int tx = c % CX, ty = c / CX;
-          int ci = x0 - 1 + tx, cj = y0 - 1 + ty;
-          if ((tx > 0 && ci >= g.Nx) || (ty > 0 && cj >= g.Ny)) continue;
-          if (ci < 0) ci += g.Nx;  // low halo cell: periodic wrap (MPIC_Haloswap.F90)
-          if (cj < 0) cj += g.Ny;
-          const int64_t cid = ((int64_t)ck * g.Ny + cj) * g.Nx + ci;
-          s0[i] = start[cid];
-          len[i] = start[cid + 1] - s0[i];
-        }
-      }
-    };
-    int ns0[CPL], nlen[CPL];  // segments of the next layer, in flight
-    fetch(L0 - 1, ns0, nlen);
-    constexpr int PPL = (NCELLT * RANKS + 31) / 32;  // (cell, rank) pairs per lane
-    int nid[PPL];
-    auto load_idx = [&](int slot, int s) {
+    for (int ab = 0; ab < 4; ++ab)
 #pragma unroll
-      for (int i = 0; i < PPL; ++i) {
-        const int pr = lane + 32 * i;
-        nid[i] = -1;
-        if (pr < NCELLT * RANKS) {
-          const int c = pr / RANKS, u = s * RANKS + pr % RANKS;
-          if (u < tab_len[slot * NCELLT + c]) nid[i] = sorted[tab_s0[slot * NCELLT + c] + u];
-        }
-      }
-    };
-    int k = 0;  // chunk counter
-    bool ok = true;
-    for (int ck = L0 - 1; ck <= LAST && ok; ++ck) {
-      const int li = ck - (L0 - 1), slot = li % NTAB;
-      int ns = 1;
-      for (int s = 0; s < ns && ok; ++s, ++k) {
-        const int b = k % NBUF;
-        if (k >= NBUF && !mbar_wait(&empty[b], ((k / NBUF) - 1) & 1, abort)) {
-          ok = false;
-          break;
-        }
-        if (s == 0) {
-          // this layer's table: its slot was last read for layer ck - NTAB, whose
-          // chunks the consumers finished before freeing buffer b
-          int m = 0;
-#pragma unroll
-          for (int i = 0; i < CPL; ++i) {
-            const int c = lane + 32 * i;
-            if (c < NCELLT) {
-              tab_s0[slot * NCELLT + c] = ns0[i];
-              tab_len[slot * NCELLT + c] = nlen[i];
-            }
-            m = max(m, nlen[i]);
-          }
-          m = __reduce_max_sync(0xffffffffu, m);
-          ns = max(1, (m + RANKS - 1) / RANKS);
-          if (lane == 0) tab_ns[slot] = ns;
-          __syncwarp();
-          mbar_arrive(&tabfull[slot]);
-          if (ck + 1 <= LAST) fetch(ck + 1, ns0, nlen);
-          load_idx(slot, 0);
-        }
-        double* S = stage + (size_t)b * Lay::stage_elems;
-#pragma unroll
-        for (int i = 0; i < PPL; ++i) {
-          const int n = nid[i];
-          if (n < 0) continue;
-          const int pr = lane + 32 * i;
-          double* D = S + (pr % RANKS) * NCELLT + pr / RANKS;
-          cp_async8(D, DX + n);
-          cp_async8(D + FS, DY + n);
-          cp_async8(D + 2 * FS, DZ + n);
-          cp_async8(D + 3 * FS, VOL + n);
-          if (MODE == 0) {
-#pragma unroll
-            for (int qq = 0; qq < (BT ? NQ - 1 : NQ); ++qq) cp_async8(D + (4 + qq) * FS, a.f[qq] + n);
-            if (BT) {
-#pragma unroll
-              for (int qq = 0; qq < 3; ++qq) cp_async8(D + (4 + NQ - 1 + qq) * FS, a.bh[qq] + n);
-            }
-          } else {
-#pragma unroll
-            for (int qq = 1; qq < NQ; ++qq) cp_async8(D + (4 + qq - 1) * FS, a.f[qq] + n);
-          }
-        }
-        mbar_arrive_on_copies(&full[b]);
-        if (s + 1 < ns) load_idx(slot, s + 1);  // the next chunk's indices, one chunk ahead
-      }
-    }
-    if (!ok) atomicCAS(&info->error, 0, PMPIC_ERR_TIMEOUT);
-    cp_async_wait_all();  // every copy has landed before the warp leaves
-    return;
-  }
-
-  // ================================ consumer warps ================================
-  const int c = t;  // this thread's cell (c < NCELLT)
-  const int tx = c % CX, ty = c / CX;
-  bool has_col = c < NCELLT;
-  int ci = x0 - 1 + tx, cj = y0 - 1 + ty;
-  if (has_col) {
-    if (tx > 0 && ci >= g.Nx) has_col = false;
-    if (ty > 0 && cj >= g.Ny) has_col = false;
-    if (ci < 0) ci += g.Nx;
-    if (cj < 0) cj += g.Ny;
-  }
-  const int parity = (tx & 1) | ((ty & 1) << 1);
-  int cur = 0;  // level accumulator of the current layer's bottom corners
-  int k = 0;
-  bool ok = true;
-  for (int ck = L0 - 1; ck <= LAST; ++ck) {
-    const int li = ck - (L0 - 1), slot = li % NTAB;
-    ok = ok && mbar_wait(&tabfull[slot], (li / NTAB) & 1, abort);
-    const int ns = ok ? tab_ns[slot] : 0;
-    const int mylen = (ok && c < NCELLT) ? tab_len[slot * NCELLT + c] : 0;
-    double P[8][NA];
-#pragma unroll
-    for (int cc = 0; cc < 8; ++cc)
-#pragma unroll
-      for (int qq = 0; qq < NA; ++qq) P[cc][qq] = 0.0;
+      for (int q = 0; q < NA; ++q) acc[ab][q] = 0.0;
     int nkept = 0;
-    for (int s = 0; s < ns && ok; ++s, ++k) {
-      const int b = k % NBUF;
-      if (!mbar_wait(&full[b], (k / NBUF) & 1, abort)) {
-        ok = false;
-        break;
-      }
-      const int nu = min(RANKS, mylen - s * RANKS);
-      const double* S0 = stage + (size_t)b * Lay::stage_elems + c;
+    for (int b0 = q0; b0 < q1; b0 += BATCH) {
+      const int nb = min(BATCH, q1 - b0);
+      __syncwarp();  // the previous batch has been read
+      int slot[BATCH / 32];
 #pragma unroll
-      for (int ul = 0; ul < RANKS; ++ul) {
-        if (ul >= nu) break;
-        const double* S = S0 + ul * NCELLT;
-        const double delx = S[0], dely = S[FS], delz = S[2 * FS], vv = S[3 * FS];
-        if (MODE == 1 && vv < a.vmin) continue;    // parcel_mixing.F90:488
+      for (int j = 0; j < BATCH / 32; ++j) {
+        const int p = lane + 32 * j;
+        slot[j] = p < nb ? sorted[b0 + p] : -1;
+      }
+#pragma unroll
+      for (int j = 0; j < BATCH / 32; ++j) {
+        const int n = slot[j];
+        if (n < 0) continue;
+        const int p = lane + 32 * j;
+        double* D = S + p + (p >> 4);
+        cp_async8(D, DX + n);
+        cp_async8(D + SPAD, DY + n);
+        cp_async8(D + 2 * SPAD, DZ + n);
+        cp_async8(D + 3 * SPAD, VOL + n);
+        if (MODE == 0) {
+#pragma unroll
+          for (int f = 0; f < (BT ? NQ - 1 : NQ); ++f) cp_async8(D + (4 + f) * SPAD, a.f[f] + n);
+          if (BT) {
+#pragma unroll
+            for (int f = 0; f < 3; ++f) cp_async8(D + (4 + NQ - 1 + f) * SPAD, a.bh[f] + n);
+          }
+        } else {
+#pragma unroll
+          for (int f = 1; f < NQ; ++f) cp_async8(D + (4 + f - 1) * SPAD, a.f[f] + n);
+        }
+      }
+      cp_async_wait_all();
+      __syncwarp();
+      if (BT) {  // btot per parcel, once (vorticity_tendency.F90:123-124)
+#pragma unroll
+        for (int j = 0; j < BATCH / 32; ++j) {
+          const int p = lane + 32 * j;
+          if (p >= nb) continue;
+          double* D = S + p + (p >> 4) + (4 + NQ - 1) * SPAD;
+          const double bb = D[0], hh = D[SPAD], zz = D[2 * SPAD];
+          D[0] = bb + 12.5 * fmax(0.0, hh - exp(-zz));
+        }
+        __syncwarp();
+      }
+      const int lo = max(s_me, b0) - b0, hi = min(e_me, b0 + nb) - b0;
+      for (int p = lo; p < hi; ++p) {
+        const double* D = S + p + (p >> 4);
+        const double delx = D[0], dely = D[SPAD], delz = D[2 * SPAD], vv = D[3 * SPAD];
+        if (MODE == 1 && vv < a.vmin) continue;  // parcel_mixing.F90:488
         if (MODE == 2 && !(vv < a.vmin)) continue;
         if (MODE == 1) ++nkept;
-        // parcel_interpolation.F90:390-434: w = (1-delz)(1-dely)(1-delx) v etc.
-        const double ez = 1 - delz, ey = 1 - dely, ex = 1 - delx;
-        double w[8];
-        w[0] = ez * ey * ex * vv;
-        w[1] = ez * ey * delx * vv;
-        w[2] = ez * dely * ex * vv;
-        w[3] = ez * dely * delx * vv;
-        w[4] = delz * ey * ex * vv;
-        w[5] = delz * ey * delx * vv;
-        w[6] = delz * dely * ex * vv;
-        w[7] = delz * dely * delx * vv;
-        double fv[NQ];
+        // parcel_interpolation.F90:390-434: w = (1-delz)(1-dely)(1-delx) v etc.,
+        // evaluated left to right as there
+        const double ez = cz ? delz : 1 - delz;
+        const double zy0 = ez * (1 - dely), zy1 = ez * dely;
+        double w[4];
+        w[0] = zy0 * (1 - delx) * vv;
+        w[1] = zy0 * delx * vv;
+        w[2] = zy1 * (1 - delx) * vv;
+        w[3] = zy1 * delx * vv;
+        double fv[NA];
         if (MODE == 0) {
 #pragma unroll
-          for (int qq = 0; qq < (BT ? NQ - 1 : NQ); ++qq) fv[qq] = S[(4 + qq) * FS];
-          if (BT) {
-            const double bb = S[(4 + NQ - 1) * FS], hh = S[(4 + NQ) * FS], zz = S[(4 + NQ + 1) * FS];
-            fv[NQ - 1] = bb + 12.5 * fmax(0.0, hh - exp(-zz));  // vorticity_tendency.F90:123-124
-          }
+          for (int q = 0; q < NQ; ++q) fv[q] = D[(4 + q) * SPAD];
         } else {
-          fv[0] = 1.0;
 #pragma unroll
-          for (int qq = 1; qq < NQ; ++qq) fv[qq] = S[(4 + qq - 1) * FS];
+          for (int q = 1; q < NQ; ++q) fv[q] = D[(4 + q - 1) * SPAD];
         }
 #pragma unroll
-        for (int cc = 0; cc < 8; ++cc) {
+        for (int ab = 0; ab < 4; ++ab) {
+          if (MODE == 0) {
 #pragma unroll
-          for (int qq = 0; qq < NQ; ++qq) P[cc][qq] += (MODE != 0 && qq == 0) ? w[cc] : w[cc] * fv[qq];
-          if (MODE == 0) P[cc][NA - 1] += w[cc];
-        }
-      }
-      mbar_arrive(&empty[b]);  // this thread's reads of buffer b are done
-    }
-    // uniform stop: the OR over all consumers of "a wait gave up"
-    if (cons_sync_or(!ok || *abort)) break;
-    if (MODE == 1 && has_col && ck >= L0 && ck < g.Nz && tx > 0 && ty > 0)
-      a.npercell[((int64_t)ck * g.Ny + cj) * g.Nx + ci] = nkept;
-    // corners into the level accumulators, one parity class at a time;
-    // corner cc: dz = cc>>2, dy = (cc>>1)&1, dx = cc&1
-    for (int ph = 0; ph < 4; ++ph) {
-      if (ph) cons_sync();
-      if (has_col && parity == ph) {
+            for (int q = 0; q < NQ; ++q) acc[ab][q] += w[ab] * fv[q];
+            acc[ab][NQ] += w[ab];
+          } else {
+            acc[ab][0] += w[ab];
 #pragma unroll
-        for (int cc = 0; cc < 8; ++cc) {
-          const int px = tx + (cc & 1), py = ty + ((cc >> 1) & 1);
-          if (px < CX && py < CY) {
-            double* A = acc + (size_t)(cur ^ (cc >> 2)) * NA * NCELLT + py * CX + px;
-#pragma unroll
-            for (int qq = 0; qq < NA; ++qq) A[qq * NCELLT] += P[cc][qq];
+            for (int q = 1; q < NQ; ++q) acc[ab][q] += w[ab] * fv[q];
           }
         }
       }
     }
-    cons_sync();
-    // level ck is complete: normalise and store the owned points, clear the level
-    for (int e = t; e < NCELLT; e += P2G_CONS) {
-      double* A = acc + (size_t)cur * NA * NCELLT + e;
-      const int px = e % CX, py = e / CX;
-      const int gx = x0 + px - 1, gy = y0 + py - 1;
-      if (ck >= L0 && px > 0 && py > 0 && gx < g.Nx && gy < g.Ny) {
-        const size_t o = ((size_t)ck * g.Ny + gy) * g.Nx + gx;
-        if (MODE == 0) {
-          double wv = A[(NA - 1) * NCELLT];
-          if (wv == 0.) wv = 1.;  // parcel_interpolation.F90:466
+    // level m+1 = top corners of layer m (odd lane 2m+1) + bottom corners of layer m+1 (lane 2m+2)
 #pragma unroll
-          for (int qq = 0; qq < NQ; ++qq) a.out[qq][o] = A[qq * NCELLT] / wv;  // :467
-        } else {
-          const bool wall = (MODE == 1) && (ck == 0 || ck == g.Nz);
+    for (int ab = 0; ab < 4; ++ab)
 #pragma unroll
-          for (int qq = 0; qq < NQ; ++qq) a.out[qq][o] = wall ? A[qq * NCELLT] * 2. : A[qq * NCELLT];
-        }
+      for (int q = 0; q < NA; ++q) {
+        const double o = __shfl_down_sync(FULL, acc[ab][q], 1);
+        if ((lane & 1) && kk + 1 < nk) acc[ab][q] = acc[ab][q] + o;
       }
+    if (it >= 0) {
+      // grid point x = cx: x-high corners of column cx-1, then x-low corners of column cx
+      if (owner) {
+        double* dst = out_row + (size_t)cx * Lay::RPS + lev;
 #pragma unroll
-      for (int qq = 0; qq < NA; ++qq) A[qq * NCELLT] = 0.0;
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+          for (int q = 0; q < NA; ++q) dst[(b * NA + q) * NLV] = C[b][q] + acc[2 * b][q];
+      }
+      if (MODE == 1 && cz == 0 && has_cell) a.npercell[((int64_t)(k0 + kk) * g.Ny + cy) * g.Nx + cx] = nkept;
     }
-    cur ^= 1;
-    cons_sync();
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int q = 0; q < NA; ++q) C[b][q] = acc[2 * b + 1][q];
   }
-  if (t == 0 && *abort) atomicCAS(&info->error, 0, PMPIC_ERR_TIMEOUT);
+}
+
+// per grid point: the y-high part of row y-1 plus the y-low part of row y; on
+// the bottom level of a chunk the chunk below's top level comes first
+template <int NQ, int MODE>
+__global__ void __launch_bounds__(256) k_p2g_combine(Geom g, int nzc, const double* __restrict__ rowpart,
+                                                    P2GArgs<NQ> a) {
+  constexpr int NA = MODE == 0 ? NQ + 1 : NQ;
+  constexpr int RPS = 2 * NA * NLV;
+  constexpr int TS = NA * NLV + 1;  // odd stride: conflict-free reads by consecutive points
+  __shared__ double T[2][PXB * TS];      // [0]: row y (y-low part), [1]: row y-1 (y-high part)
+  __shared__ double Bz[2][PXB * NA];     // the chunk below's top level, same rows
+  const int px0 = blockIdx.x * PXB, py = blockIdx.y, zc = blockIdx.z;
+  const int pym = py == 0 ? g.Ny - 1 : py - 1;
+  const int npx = min(PXB, g.Nx - px0);
+  const int k0 = zc * ZC, nk = min(ZC, g.Nz - k0);
+  const int seg = NA * NLV;
+  for (int e = threadIdx.x; e < 2 * npx * seg; e += blockDim.x) {
+    const int r = e / (npx * seg);
+    const int rem = e - r * npx * seg;
+    const int pxl = rem / seg, o = rem - pxl * seg;
+    const int row = r == 0 ? py : pym;
+    T[r][pxl * TS + o] = rowpart[(((size_t)zc * g.Ny + row) * g.Nx + px0 + pxl) * RPS + r * seg + o];
+  }
+  if (zc > 0) {
+    for (int e = threadIdx.x; e < 2 * npx * NA; e += blockDim.x) {
+      const int r = e / (npx * NA);
+      const int rem = e - r * npx * NA;
+      const int pxl = rem / NA, q = rem - pxl * NA;
+      const int row = r == 0 ? py : pym;
+      Bz[r][pxl * NA + q] =
+          rowpart[(((size_t)(zc - 1) * g.Ny + row) * g.Nx + px0 + pxl) * RPS + r * seg + q * NLV + ZC];
+    }
+  }
+  __syncthreads();
+  // levels this chunk completes: its bottom nk, and the top level on the last chunk
+  const int nlev = k0 + nk == g.Nz ? nk + 1 : nk;
+  for (int e = threadIdx.x; e < nlev * npx; e += blockDim.x) {
+    const int L = e / npx, pxl = e - L * npx;
+    double v[NA];
+#pragma unroll
+    for (int q = 0; q < NA; ++q) v[q] = T[1][pxl * TS + q * NLV + L] + T[0][pxl * TS + q * NLV + L];
+    if (L == 0 && zc > 0) {
+#pragma unroll
+      for (int q = 0; q < NA; ++q) v[q] = (Bz[1][pxl * NA + q] + Bz[0][pxl * NA + q]) + v[q];
+    }
+    const int gl = k0 + L;
+    const size_t o = ((size_t)gl * g.Ny + py) * g.Nx + px0 + pxl;
+    if (MODE == 0) {
+      double wv = v[NQ];
+      if (wv == 0.) wv = 1.;  // parcel_interpolation.F90:466
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) a.out[q][o] = v[q] / wv;  // :467
+    } else {
+      const bool wall = (MODE == 1) && (gl == 0 || gl == g.Nz);
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) a.out[q][o] = wall ? v[q] * 2. : v[q];
+    }
+  }
+}
+
+// z-fastest cell id -> x-fastest id ((k*Ny + j)*Nx + i); -1 stays -1
+__global__ void k_cell_xfast(Geom g, int64_t n, const int32_t* __restrict__ cell, int32_t* __restrict__ out) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int32_t id = cell[t];
+  if (id < 0) {
+    out[t] = -1;
+    return;
+  }
+  const int ck = id % g.Nz, cj = (id / g.Nz) % g.Ny, ci = id / (g.Nz * g.Ny);
+  out[t] = (int32_t)(((int64_t)ck * g.Ny + cj) * g.Nx + ci);
 }
 
 // ---- grid2par --------------------------------------------------------------------
@@ -590,9 +490,9 @@ __global__ void k_grid2par(Geom g, int64_t n, const int32_t* __restrict__ cell, 
   const int32_t id = cell[t];
   if (id < 0) return;  // binning reported the error
   const double delx = del[t], dely = del[cap + t], delz = del[2 * cap + t];
-  const int ci = id % g.Nx;
-  const int cj = (id / g.Nx) % g.Ny;
-  const int ck = id / (g.Nx * g.Ny);
+  const int ck = id % g.Nz;
+  const int cj = (id / g.Nz) % g.Ny;
+  const int ci = id / (g.Nz * g.Ny);
   int ci1 = ci + 1 == g.Nx ? 0 : ci + 1;  // grid2par_haloswap: periodic copy
   int cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
   size_t r00 = ((size_t)ck * g.Ny + cj) * g.Nx, r01 = ((size_t)ck * g.Ny + cj1) * g.Nx;
@@ -657,12 +557,28 @@ int bin_and_sort(pmpic_ctx* ctx) {
   return 0;
 }
 
+// the two passes of par2grid on `st`; rowpart holds nzc * Ny * Nx records of
+// P2GLayout::RPS doubles
+template <int NQ, int MODE, bool BT>
+static cudaError_t run_p2g(const Geom& g, const int32_t* start, const int32_t* sorted, const double* del,
+                           int64_t cap, const double* vol, const P2GArgs<NQ>& a, double* rowpart, cudaStream_t st) {
+  const int nzc = (g.Nz + ZC - 1) / ZC;
+  const int nxs = (g.Nx + XSEG - 1) / XSEG;
+  const int64_t nw = (int64_t)nxs * g.Ny * nzc;
+  auto rows = k_p2g_rows<NQ, MODE, BT>;
+  cudaError_t e = cudaFuncSetAttribute(rows, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
+  rows<<<nblk(nw, RW), 32 * RW, 0, st>>>(g, nzc, nxs, start, sorted, del, cap, vol, a, rowpart);
+  dim3 gb((g.Nx + PXB - 1) / PXB, g.Ny, nzc);
+  k_p2g_combine<NQ, MODE><<<gb, 256, 0, st>>>(g, nzc, rowpart, a);
+  return cudaGetLastError();
+}
+
 template <int NQ, int MODE, bool BT>
 static int launch_p2g(pmpic_ctx* ctx, const double* const* fields, double* const* out) {
   TimerScope ts(ctx, T_P2G);
   const Geom& g = ctx->g;
-  using Lay = P2GLayout<NQ, MODE, BT>;
-  static_assert(Lay::smem <= 227 * 1024, "par2grid shared memory");
   P2GArgs<NQ> a;
   for (int q = 0; q < NQ; ++q) {
     a.f[q] = fields[q];
@@ -673,15 +589,16 @@ static int launch_p2g(pmpic_ctx* ctx, const double* const* fields, double* const
   a.bh[2] = prop(ctx, PMPIC_PROP_Z);
   a.npercell = ctx->npercell;
   a.vmin = g.vmin;
-  auto kern = k_par2grid<NQ, MODE, BT>;
-  PMPIC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::smem));
-  PMPIC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                  (int)cudaSharedmemCarveoutMaxShared));
-  dim3 grid((g.Nx + TX - 1) / TX, (g.Ny + TY - 1) / TY, (g.nzp + ZCHUNK - 1) / ZCHUNK);
-  kern<<<grid, P2G_THREADS, Lay::smem, ctx->stream>>>(g, ctx->cell_start, ctx->sorted, ctx->del, ctx->cap,
-                                                      prop(ctx, PMPIC_PROP_VOL), a, ctx->dinfo); ++ctx->nlaunch;
-  PMPIC_CUDA(cudaGetLastError());
+  PMPIC_CUDA((run_p2g<NQ, MODE, BT>(g, ctx->cell_start, ctx->sorted, ctx->del, ctx->cap, prop(ctx, PMPIC_PROP_VOL),
+                                    a, ctx->rowpart, ctx->stream)));
+  ctx->nlaunch += 2;
   return 0;
+}
+
+// bytes of the row-partial buffer of a context
+size_t rowpart_bytes(const Geom& g) {
+  const size_t nzc = (size_t)(g.Nz + ZC - 1) / ZC;
+  return sizeof(double) * nzc * (size_t)g.Ny * (size_t)g.Nx * RPS_MAX;
 }
 
 // parcel_mixing construct_grids (:440-624) + mixing_haloswap + wall doubling:
@@ -749,10 +666,16 @@ int grid2par_multi(pmpic_ctx* ctx, const double* const* grids, int ng, double* c
   }
 }
 
-// cached cell ids of the current positions (ctx->cell)
+// cell ids of the current positions in the x-fastest form of the C ABI,
+// ((k-1)*ny + (j-3))*nx + (i-3), into dcells (device, n entries)
 int cell_ids(pmpic_ctx* ctx, int32_t* dcells) {
-  (void)dcells;
-  return bin_and_sort(ctx);
+  int rc = bin_and_sort(ctx);
+  if (rc) return rc;
+  if (ctx->n > 0) {
+    k_cell_xfast<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, ctx->cell, dcells); ++ctx->nlaunch;
+  }
+  PMPIC_CUDA(cudaGetLastError());
+  return 0;
 }
 
 }  // namespace pmpic
@@ -771,6 +694,7 @@ namespace {
 
 constexpr int64_t SP_MAX_PARCELS = 131072;  // parcels per call
 constexpr int64_t SP_MAX_CELLS = 32768;     // nx*ny*nz per call
+constexpr int64_t SP_MAX_COLCHUNKS = 4096;  // ceil(nz/16)*nx*ny per call (row partials of par2grid)
 constexpr int64_t SP_MAX_TILES = (SP_MAX_CELLS + SCAN_TILE - 1) / SCAN_TILE + 1;
 constexpr size_t sp_round(size_t b) { return (b + 255) / 256 * 256; }
 // scratch layout (byte offsets)
@@ -782,7 +706,9 @@ constexpr size_t SP_START = SP_COUNT + sp_round(sizeof(int32_t) * (SP_MAX_CELLS 
 constexpr size_t SP_FILL = SP_START + sp_round(sizeof(int32_t) * (SP_MAX_CELLS + 1));   // int32[MAX_CELLS]
 constexpr size_t SP_TILES = SP_FILL + sp_round(sizeof(int32_t) * SP_MAX_CELLS);         // int32[MAX_TILES]
 constexpr size_t SP_INFO = SP_TILES + sp_round(sizeof(int32_t) * SP_MAX_TILES);         // DevInfo
-constexpr size_t SP_BYTES = SP_INFO + sp_round(sizeof(DevInfo));                        // about 4.5 MB
+constexpr size_t SP_ROWS = SP_INFO + sp_round(sizeof(DevInfo));                         // double[MAX_COLCHUNKS][RPS]
+constexpr size_t SP_BYTES = SP_ROWS + sp_round(sizeof(double) * SP_MAX_COLCHUNKS * P2GLayout<1, 0, false>::RPS);
+static_assert(SP_BYTES < 8u << 20, "static par2grid scratch stays below 8 MB");
 
 __device__ __align__(256) unsigned char g_p2g_scratch[SP_BYTES];
 
@@ -801,6 +727,7 @@ extern "C" int pmpic_par2grid_static(int32_t nx, int32_t ny, int32_t nz, double 
   if (n > 0 && (!x || !y || !z || !vol || !field)) return PMPIC_ERR_ARG;
   const int64_t ncell = (int64_t)nx * ny * nz;
   if (n > SP_MAX_PARCELS || ncell > SP_MAX_CELLS) return PMPIC_ERR_TOO_LARGE;
+  if ((int64_t)((nz + ZC - 1) / ZC) * nx * ny > SP_MAX_COLCHUNKS) return PMPIC_ERR_TOO_LARGE;
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= SP_MAX_DEVICES) return PMPIC_ERR_CUDA;
   unsigned char* base;
@@ -821,6 +748,7 @@ extern "C" int pmpic_par2grid_static(int32_t nx, int32_t ny, int32_t nz, double 
   int32_t* fill = (int32_t*)(base + SP_FILL);
   int32_t* tiles = (int32_t*)(base + SP_TILES);
   DevInfo* info = (DevInfo*)(base + SP_INFO);
+  double* rows = (double*)(base + SP_ROWS);
   cudaStream_t st = (cudaStream_t)stream;
 
   // geometry: the binning and par2grid subset of pmpic_create's (origin 0)
@@ -852,16 +780,11 @@ extern "C" int pmpic_par2grid_static(int32_t nx, int32_t ny, int32_t nz, double 
     k_bin_scatter<<<nblk(n, 256), 256, 0, st>>>(n, cell, cstart, fill, sorted);
     k_sort_segments<<<nblk(ncell, 256), 256, 0, st>>>(ncell, cstart, sorted);
   }
-  using Lay = P2GLayout<1, 0, false>;
-  auto kern = k_par2grid<1, 0, false>;
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::smem) != cudaSuccess)
-    return PMPIC_ERR_CUDA;
   P2GArgs<1> a{};
   a.f[0] = field;
   a.out[0] = out;
-  dim3 grid((nx + TX - 1) / TX, (ny + TY - 1) / TY, (g.nzp + ZCHUNK - 1) / ZCHUNK);
-  kern<<<grid, P2G_THREADS, Lay::smem, st>>>(g, cstart, sorted, del, SP_MAX_PARCELS, vol, a, info);
-  if (cudaGetLastError() != cudaSuccess) return PMPIC_ERR_CUDA;
+  if (run_p2g<1, 0, false>(g, cstart, sorted, del, SP_MAX_PARCELS, vol, a, rows, st) != cudaSuccess)
+    return PMPIC_ERR_CUDA;
   int err = 0;
   if (cudaMemcpyAsync(&err, &info->error, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)
     return PMPIC_ERR_CUDA;

@@ -130,7 +130,7 @@ __global__ void k_rk4(Geom g, int64_t n, RkPtrs P, int stage, const double* __re
   if ((GU || GP) && id >= 0) {  // id < 0: binning failed and reported the error
     gathered = true;
     const double delx = del[t], dely = del[cap + t], delz = del[2 * cap + t];
-    const int ci = id % g.Nx, cj = (id / g.Nx) % g.Ny, ck = id / (g.Nx * g.Ny);
+    const int ck = id % g.Nz, cj = (id / g.Nz) % g.Ny, ci = id / (g.Nz * g.Ny);
     const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
     const size_t r00 = ((size_t)ck * g.Ny + cj) * g.Nx, r01 = ((size_t)ck * g.Ny + cj1) * g.Nx;
     const size_t r10 = ((size_t)(ck + 1) * g.Ny + cj) * g.Nx, r11 = ((size_t)(ck + 1) * g.Ny + cj1) * g.Nx;
@@ -484,7 +484,7 @@ __global__ void __launch_bounds__(256, 3) k_redistribute(Geom g, int64_t norig, 
   const int32_t id = cell[m];
   if (id < 0) return;
   const double delx = del[m], dely = del[cap + m], delz = del[2 * cap + m];
-  const int ci = id % g.Nx, cj = (id / g.Nx) % g.Ny, ck = id / (g.Nx * g.Ny);
+  const int ck = id % g.Nz, cj = (id / g.Nz) % g.Ny, ci = id / (g.Nz * g.Ny);
   int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
   // grid offsets fit in 32 bits (pmpic_create limits (nz+1)*ny*nx)
   const int r0 = (ck * g.Ny + cj) * g.Nx, r1 = (ck * g.Ny + cj1) * g.Nx;
