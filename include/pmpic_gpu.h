@@ -175,8 +175,9 @@ int pmpic_op_parcel_haloswap(pmpic_ctx* ctx);
  * parcel_interpolation.F90:186-262, par2grid :336-481) of one field with volume
  * weights over an nx x ny x nz box [0,lx) x [0,ly) x [0,lz].  x, y, z, vol,
  * field are n device doubles; out receives the dense (nz+1) x ny x nx grid on
- * the device.  Scratch is one fixed static device array (about 4.5 MB per
- * device): n <= 131072 and nx*ny*nz <= 32768, else PMPIC_ERR_TOO_LARGE with
+ * the device.  Scratch is one fixed static device array (about 7 MB per
+ * device): n <= 131072, nx*ny*nz <= 32768 and ceil(nz/16)*nx*ny <= 4096,
+ * else PMPIC_ERR_TOO_LARGE with
  * nothing launched.  The call clears its own counters, runs on `stream`
  * (a cudaStream_t; NULL = the legacy default stream) and synchronizes it before
  * returning; PMPIC_ERR_OUT_OF_BOX if a parcel is outside the box.
