@@ -177,7 +177,7 @@ def run_b200(args):
     n0 = len(ic["x"])
     cap = int(args.capacity * n0)
     ctx = pm.Context(grid, grid, grid, PLUME["lx"], PLUME["ly"], PLUME["lz"], dtm=0.0025, dtmax=0.0025,
-                     max_parcels=cap, device=local)
+                     max_parcels=cap, device=local, precision=args.precision)
     ctx.upload(**ic)
     L = pm.lib()
     h = ctx._h
@@ -332,6 +332,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--ref-grid", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -51,6 +51,8 @@ extern "C" {
 
 /* ---- precision forms ---------------------------------------------------- */
 #define PMPIC_FP64  0            /* plain FP64 throughout (the reference's DEFAULT_PRECISION) */
+#define PMPIC_MIXED 1            /* FP32 fields, grids, transforms and RK4; positions as integer cell
+                                    index + FP32 offset; FP64 zero mode and conserved sums */
 
 /* ---- parcel property ids (parcels.F90:19-34) ----------------------------- */
 enum {
@@ -79,7 +81,7 @@ typedef struct pmpic_config {
   double dtm, dtmax;               /* rk4_integrator.F90:38-41 */
   double timestep_prefactor;       /* vorticity_tendency.F90:96 */
   int64_t max_parcels;             /* parcelsetup_base max_parcels */
-  int32_t precision;               /* PMPIC_FP64 */
+  int32_t precision;               /* PMPIC_FP64 or PMPIC_MIXED */
   int32_t device;                  /* CUDA device ordinal */
 } pmpic_config;
 

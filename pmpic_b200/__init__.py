@@ -32,9 +32,10 @@ GRID = {n: i for i, n in enumerate(GRIDS)}
 SPECS = ["u_s", "v_s", "w_s"]
 SPEC = {n: i for i, n in enumerate(SPECS)}
 IO_PROPS = ["x", "y", "z", "p", "q", "r", "b", "h", "vol", "stretch", "tag"]
+PRECISIONS = {"fp64": 0, "mixed": 1}
 
 ERRORS = {0: "ok", -1: "config", -2: "capacity", -3: "out of box", -4: "zero pivot",
-          -5: "backfill", -6: "timeout", -7: "cuda", -8: "argument", -9: "state"}
+          -5: "backfill", -6: "timeout", -7: "cuda", -8: "argument", -9: "state", -10: "too large"}
 
 
 class Config(C.Structure):
@@ -156,11 +157,17 @@ class Context:
     """One device-resident model state (the reference's model_state_type)."""
 
     def __init__(self, nx, ny, nz, lx, ly, lz, dtm=0.01, dtmax=0.01, prefactor=0.5,
-                 max_parcels=1 << 20, device=0):
+                 max_parcels=1 << 20, device=0, precision="fp64"):
+        """precision: "fp64" (the plain path) or "mixed" (FP32 fields, grids,
+        transforms and RK4; positions as integer cell index + FP32 offset; FP64
+        zero mode).  Transfers are FP64 on the host either way."""
         L = lib()
         self.nx, self.ny, self.nz = nx, ny, nz
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+        self.precision = precision
         cfg = Config(nx, ny, nz, 0.0, lx, 0.0, ly, 0.0, lz, dtm, dtmax, prefactor,
-                     int(max_parcels), 0, device)
+                     int(max_parcels), PRECISIONS[precision], device)
         h = C.c_void_p()
         rc = L.pmpic_create(C.byref(cfg), C.byref(h))
         if rc:

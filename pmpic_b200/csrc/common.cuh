@@ -83,6 +83,58 @@ __device__ __forceinline__ bool bin_parcel(const Geom& g, double xp, double yp, 
   return true;
 }
 
+// ---- mixed-precision form --------------------------------------------------
+// A position component of the mixed form: the integer cell index along the axis
+// and the FP32 offset inside the cell in cell units, so x = (i + f) * dx.  It
+// fills the 8-byte slot an FP64 position takes on the plain path.  f lies in
+// [0, 1); the one exception is f = 1 in cell Nz-1, a parcel exactly on the top
+// wall (the reference bins z = zmax with delz = 1 in the last cell).
+struct __align__(8) CellOff {
+  int32_t i;
+  float f;
+};
+// a + d cell units, renormalised so that f is in [0, 1)
+__device__ __forceinline__ CellOff co_add(CellOff a, float d) {
+  const float t = a.f + d;
+  const float fl = floorf(t);
+  CellOff r;
+  r.i = a.i + (int)fl;
+  r.f = t - fl;
+  if (r.f >= 1.0f) {  // t just below an integer, rounded up by the subtraction
+    r.f -= 1.0f;
+    r.i += 1;
+  }
+  return r;
+}
+// mirror of a z component at the walls z = 0 and z = nz (haloswap.F90:440-456)
+__device__ __forceinline__ CellOff co_reflect(CellOff a, int nz) {
+  if (a.i < 0) {  // -(i + f) = (-i - 1) + (1 - f)
+    a.i = -a.i - 1;
+    a.f = 1.0f - a.f;
+  } else if (a.i > nz || (a.i == nz && a.f > 0.0f)) {  // 2 nz - (i + f)
+    a.i = 2 * nz - a.i - 1;
+    a.f = 1.0f - a.f;
+  }
+  if (a.f >= 1.0f) {
+    a.f -= 1.0f;
+    a.i += 1;
+  }
+  if (a.i == nz && a.f == 0.0f) {  // on the top wall: last cell, offset 1
+    a.i = nz - 1;
+    a.f = 1.0f;
+  }
+  return a;
+}
+// element size of a property on the mixed form: positions and tag 8 bytes, the rest FP32
+__host__ __device__ __forceinline__ bool mixed_is_pos(int pid) {
+  return pid == PMPIC_PROP_X || pid == PMPIC_PROP_Y || pid == PMPIC_PROP_Z || pid == PMPIC_PROP_XO ||
+         pid == PMPIC_PROP_YO || pid == PMPIC_PROP_ZO || pid == PMPIC_PROP_XF || pid == PMPIC_PROP_YF ||
+         pid == PMPIC_PROP_ZF;
+}
+__host__ __device__ __forceinline__ int mixed_elem_bytes(int pid) {
+  return (mixed_is_pos(pid) || pid == PMPIC_PROP_TAG) ? 8 : 4;
+}
+
 // Device-side step counters and error word.
 struct DevInfo {
   int error;
@@ -126,6 +178,7 @@ struct TimerScope {
 // ---------------------------------------------------------------------------
 struct pmpic_ctx {
   pmpic_config cfg;
+  bool mixed;                // PMPIC_MIXED: FP32 bulk, int cell + FP32 offset positions
   pmpic::Geom g;
   int device;
   cudaStream_t stream;
@@ -166,7 +219,12 @@ struct pmpic_ctx {
   double* spec[PMPIC_NSPEC]; // u_s, v_s, w_s
   double* sa, *sb, *sc, *sd, *se, *sf, *sas, *sbs, *sscratch;
   double* fftmid;            // (Nz+1) x (Ny+2) x Nx
-  double* ftw;               // twiddle tables (x plan first, then y plan)
+  double* ftw;               // twiddle tables (x plan first, then y plan), double2
+  float* ftw32;              // the same twiddles as float2 (mixed-precision form)
+  float* wn32;               // FP32 kx, ky, k2, filter tables and diffz factors
+  double* hsum;              // FP64 horizontal sums of p and q per level (mixed form's zero mode)
+  double* stage64;           // mixed form: FP64 staging of host transfers (stage_n values)
+  int64_t stage_n;
   int ftw_off_x, ftw_off_y;
   pmpic::FftPlan plan_x, plan_y;
   // small per-column data
@@ -194,17 +252,23 @@ namespace pmpic {
 int cuda_fail(pmpic_ctx* ctx, cudaError_t e, const char* what, int line);
 int set_error(pmpic_ctx* ctx, int code, const std::string& msg);
 inline double* prop(pmpic_ctx* ctx, int p) { return ctx->parcels + (size_t)p * (size_t)ctx->cap; }
+// the mixed form's views of the same property arrays
+inline float* propf(pmpic_ctx* ctx, int p) { return (float*)prop(ctx, p); }
+inline CellOff* propc(pmpic_ctx* ctx, int p) { return (CellOff*)prop(ctx, p); }
 
 // kernels / launchers (interp.cu)
 int bin_and_sort(pmpic_ctx* ctx);
 int par2grid_multi(pmpic_ctx* ctx, const double* const* fields, int nf, double* const* out, bool btot_from_bhz);
 int grid2par_multi(pmpic_ctx* ctx, const double* const* grids, int ng, double* const* out);
+int par2grid_multi_m(pmpic_ctx* ctx, const float* const* fields, int nf, float* const* out);
 int cell_ids(pmpic_ctx* ctx, int32_t* dcells);
 size_t rowpart_bytes(const Geom& g);
 // fft.cu
 int fft_init(pmpic_ctx* ctx);
 int fft_forward(pmpic_ctx* ctx, const double* phys, double* spec);
 int fft_backward(pmpic_ctx* ctx, const double* spec, double* phys);
+int fft_forward(pmpic_ctx* ctx, const float* phys, float* spec);
+int fft_backward(pmpic_ctx* ctx, const float* spec, float* phys);
 // spectral.cu
 int spec_diffx(pmpic_ctx* ctx, const double* in, double* out);
 int spec_diffy(pmpic_ctx* ctx, const double* in, double* out);

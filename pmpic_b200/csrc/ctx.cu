@@ -118,7 +118,7 @@ void free_all(pmpic_ctx* c) {
   void* ptrs[] = {c->parcels, c->rowpart,  c->cell,     c->del,       c->gspare,     c->sorted,    c->cell_count, c->cell_start, c->cell_fill, c->keep,
                   c->aux,     c->aux2,     c->dir,       c->swapbuf,    c->scan_tmp,   c->npercell,  c->newslot,
                   c->newportion, c->sa,    c->sb,        c->sc,         c->sd,         c->se,        c->sf,
-                  c->sas,     c->sbs,      c->sscratch,  c->fftmid,     c->ftw,        c->kx,        c->ky,
+                  c->sas,     c->sbs,      c->sscratch,  c->fftmid,     c->ftw,        c->ftw32,      c->wn32,       c->hsum,       c->stage64,        c->kx,        c->ky,
                   c->k2,      c->filt,     c->bt,        c->zmode,      c->dinfo};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -178,7 +178,7 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   *out = nullptr;
   if (cfg->nx < 4 || cfg->ny < 4 || cfg->nz < 3 || (cfg->nx & 1) || (cfg->ny & 1) || !smooth235(cfg->nx) ||
       !smooth235(cfg->ny) || cfg->max_parcels <= 0 || cfg->max_parcels >= (int64_t)0x7fffffff ||
-      cfg->precision != PMPIC_FP64)
+      (cfg->precision != PMPIC_FP64 && cfg->precision != PMPIC_MIXED))
     return PMPIC_ERR_CONFIG;
   // cell ids and grid offsets are 32-bit: the largest grid, the spectral one, must fit
   if ((int64_t)(cfg->nz + 1) * (cfg->ny + 2) * (cfg->nx + 2) >= (int64_t)0x7fffffff) return PMPIC_ERR_CONFIG;
@@ -188,6 +188,7 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   pmpic_ctx* ctx = new pmpic_ctx();
   std::memset((void*)&ctx->g, 0, sizeof(ctx->g));
   ctx->cfg = *cfg;
+  ctx->mixed = cfg->precision == PMPIC_MIXED;
   ctx->device = cfg->device;
   ctx->parcels = nullptr;
   cudaError_t e = cudaSetDevice(cfg->device);
@@ -234,10 +235,12 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   const size_t cap = (size_t)ctx->cap;
   if (!rc) rc = dalloc(ctx, &ctx->parcels, (size_t)PMPIC_NPROP * cap);
   if (!rc) rc = dalloc(ctx, &ctx->cell, cap);
-  if (!rc) rc = dalloc(ctx, &ctx->del, 3 * cap);
+  if (!rc && !ctx->mixed) rc = dalloc(ctx, &ctx->del, 3 * cap);  // the mixed form's offsets live in its positions
   if (!rc) rc = dalloc(ctx, &ctx->gspare, (size_t)g.nphys);
   if (!rc) rc = dalloc(ctx, &ctx->sorted, cap);
   if (!rc) rc = dalloc(ctx, (char**)&ctx->rowpart, rowpart_bytes(g));
+  ctx->stage_n = std::min<int64_t>(ctx->cap, (int64_t)1 << 24);
+  if (!rc && ctx->mixed) rc = dalloc(ctx, &ctx->stage64, (size_t)ctx->stage_n);
   if (!rc) rc = dalloc(ctx, &ctx->keep, cap);
   if (!rc) rc = dalloc(ctx, &ctx->aux, cap);
   if (!rc) rc = dalloc(ctx, &ctx->aux2, 2 * (size_t)ctx->nbmax + cap);
@@ -323,6 +326,121 @@ void pmpic_destroy(pmpic_ctx* ctx) {
 
 const char* pmpic_last_error(const pmpic_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
+// ---- the mixed form's property and grid conversions ---------------------------------
+namespace {
+// kind 0: FP32 value, 1: position component with cell size d (nz: the wall index
+// for z, else 0), 2: FP64 value (tag)
+__global__ void k_conv_in(int64_t n, const double* __restrict__ src, void* __restrict__ dst, int kind, double d,
+                          int period, int nz) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const double v = src ? src[t] : 0.0;
+  if (kind == 0) {
+    ((float*)dst)[t] = (float)v;
+  } else if (kind == 2) {
+    ((double*)dst)[t] = v;
+  } else {
+    const double u = v / d;
+    const double fl = floor(u);
+    CellOff c;
+    c.i = (int)fl;
+    c.f = (float)(u - fl);
+    if (c.f >= 1.0f) {
+      c.f = 0.0f;
+      c.i += 1;
+    }
+    if (period > 0) {  // x, y: periodic
+      if (c.i >= period) c.i -= period;
+      if (c.i < 0) c.i += period;
+    }
+    if (nz > 0 && c.i == nz && c.f == 0.0f) {  // z on the top wall
+      c.i = nz - 1;
+      c.f = 1.0f;
+    }
+    ((CellOff*)dst)[t] = c;
+  }
+}
+__global__ void k_conv_out(int64_t n, const void* __restrict__ src, double* __restrict__ dst, int kind, double d) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  if (kind == 0) dst[t] = (double)((const float*)src)[t];
+  else if (kind == 2) dst[t] = ((const double*)src)[t];
+  else {
+    const CellOff c = ((const CellOff*)src)[t];
+    dst[t] = ((double)c.i + (double)c.f) * d;
+  }
+}
+__global__ void k_f2d(int64_t n, const float* __restrict__ src, double* __restrict__ dst) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) dst[t] = (double)src[t];
+}
+__global__ void k_d2f(int64_t n, const double* __restrict__ src, float* __restrict__ dst) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) dst[t] = (float)src[t];
+}
+unsigned cblk(int64_t n) { return (unsigned)((n + 255) / 256); }
+}  // namespace
+
+static void conv_kind(pmpic_ctx* ctx, int pid, int& kind, double& d, int& period, int& nz) {
+  const Geom& g = ctx->g;
+  kind = pid == PMPIC_PROP_TAG ? 2 : (mixed_is_pos(pid) ? 1 : 0);
+  d = 1.0;
+  period = 0;
+  nz = 0;
+  if (pid == PMPIC_PROP_X || pid == PMPIC_PROP_XO || pid == PMPIC_PROP_XF) { d = g.dx; period = g.Nx; }
+  if (pid == PMPIC_PROP_Y || pid == PMPIC_PROP_YO || pid == PMPIC_PROP_YF) { d = g.dy; period = g.Ny; }
+  if (pid == PMPIC_PROP_Z || pid == PMPIC_PROP_ZO || pid == PMPIC_PROP_ZF) { d = g.dz; nz = g.Nz; }
+}
+
+// host FP64 values (NULL: zeros) into property pid of slots 0..n-1, in the
+// context's precision; stream-ordered
+static int put_prop(pmpic_ctx* ctx, int pid, int64_t n, const double* src) {
+  if (n <= 0) return 0;
+  if (!ctx->mixed) {
+    if (src) PMPIC_CUDA(cudaMemcpyAsync(prop(ctx, pid), src, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    else PMPIC_CUDA(cudaMemsetAsync(prop(ctx, pid), 0, sizeof(double) * n, ctx->stream));
+    return 0;
+  }
+  if (!src) {
+    PMPIC_CUDA(cudaMemsetAsync(prop(ctx, pid), 0, (size_t)mixed_elem_bytes(pid) * n, ctx->stream));
+    return 0;
+  }
+  int kind, period, nz;
+  double d;
+  conv_kind(ctx, pid, kind, d, period, nz);
+  char* base = (char*)prop(ctx, pid);
+  const size_t es = (size_t)mixed_elem_bytes(pid);
+  for (int64_t c0 = 0; c0 < n; c0 += ctx->stage_n) {
+    const int64_t len = std::min<int64_t>(ctx->stage_n, n - c0);
+    PMPIC_CUDA(cudaMemcpyAsync(ctx->stage64, src + c0, sizeof(double) * len, cudaMemcpyHostToDevice, ctx->stream));
+    k_conv_in<<<cblk(len), 256, 0, ctx->stream>>>(len, ctx->stage64, base + es * c0, kind, d, period, nz);
+    ++ctx->nlaunch;
+  }
+  PMPIC_CUDA(cudaGetLastError());
+  return 0;
+}
+// property pid of slots 0..n-1 into host FP64 values; stream-ordered
+static int get_prop(pmpic_ctx* ctx, int pid, int64_t n, double* dst) {
+  if (n <= 0) return 0;
+  if (!ctx->mixed) {
+    PMPIC_CUDA(cudaMemcpyAsync(dst, prop(ctx, pid), sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    return 0;
+  }
+  int kind, period, nz;
+  double d;
+  conv_kind(ctx, pid, kind, d, period, nz);
+  const char* base = (const char*)prop(ctx, pid);
+  const size_t es = (size_t)mixed_elem_bytes(pid);
+  for (int64_t c0 = 0; c0 < n; c0 += ctx->stage_n) {
+    const int64_t len = std::min<int64_t>(ctx->stage_n, n - c0);
+    k_conv_out<<<cblk(len), 256, 0, ctx->stream>>>(len, base + es * c0, ctx->stage64, kind, d);
+    ++ctx->nlaunch;
+    PMPIC_CUDA(cudaMemcpyAsync(dst + c0, ctx->stage64, sizeof(double) * len, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  PMPIC_CUDA(cudaGetLastError());
+  return 0;
+}
+
 int pmpic_set_count(pmpic_ctx* ctx, int64_t n) {
   if (!ctx) return PMPIC_ERR_ARG;
   if (n < 0 || n > ctx->cap) return set_error(ctx, PMPIC_ERR_CAPACITY, "parcel count exceeds max_parcels");
@@ -348,7 +466,8 @@ int pmpic_set_property(pmpic_ctx* ctx, int p, int64_t n, const double* src) {
   int frc = flush_gathers(ctx);
   if (frc) return frc;
   ctx->dir_ready = false;
-  PMPIC_CUDA(cudaMemcpyAsync(prop(ctx, p), src, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+  int rc = put_prop(ctx, p, n, src);
+  if (rc) return rc;
   PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
   ctx->sorted_valid = false;
   ctx->btot_grid_ready = false;
@@ -359,7 +478,8 @@ int pmpic_get_property(pmpic_ctx* ctx, int p, int64_t n, double* dst) {
   cudaSetDevice(ctx->device);
   int frc = flush_gathers(ctx);
   if (frc) return frc;
-  PMPIC_CUDA(cudaMemcpyAsync(dst, prop(ctx, p), sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  int rc = get_prop(ctx, p, n, dst);
+  if (rc) return rc;
   PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
   return PMPIC_OK;
 }
@@ -377,16 +497,17 @@ int pmpic_upload_parcels(pmpic_ctx* ctx, int64_t n, const double* x, const doubl
   ctx->pending_uvw = ctx->pending_pqr = false;  // a new state
   ctx->dir_ready = false;
   for (int i = 0; i < 11; ++i) {
-    if (src[i])
-      PMPIC_CUDA(cudaMemcpyAsync(prop(ctx, kIO[i]), src[i], sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
-    else
-      PMPIC_CUDA(cudaMemsetAsync(prop(ctx, kIO[i]), 0, sizeof(double) * n, ctx->stream));
+    int rc = put_prop(ctx, kIO[i], n, src[i]);
+    if (rc) return rc;
   }
   const int zero[] = {PMPIC_PROP_DXDT, PMPIC_PROP_DYDT, PMPIC_PROP_DZDT, PMPIC_PROP_DPDT, PMPIC_PROP_DQDT,
                       PMPIC_PROP_DRDT, PMPIC_PROP_BTOT, PMPIC_PROP_XO,   PMPIC_PROP_YO,   PMPIC_PROP_ZO,
                       PMPIC_PROP_XF,   PMPIC_PROP_YF,   PMPIC_PROP_ZF,   PMPIC_PROP_PO,   PMPIC_PROP_QO,
                       PMPIC_PROP_RO,   PMPIC_PROP_PF,   PMPIC_PROP_QF,   PMPIC_PROP_RF};
-  for (int pid : zero) PMPIC_CUDA(cudaMemsetAsync(prop(ctx, pid), 0, sizeof(double) * n, ctx->stream));
+  for (int pid : zero) {
+    int rc = put_prop(ctx, pid, n, nullptr);
+    if (rc) return rc;
+  }
   // a new state clears the sticky device error word
   PMPIC_CUDA(cudaMemsetAsync(&ctx->dinfo->error, 0, sizeof(int), ctx->stream));
   PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -407,8 +528,10 @@ int pmpic_download_parcels(pmpic_ctx* ctx, int64_t capacity, int64_t* n, double*
   int frc = flush_gathers(ctx);
   if (frc) return frc;
   for (int i = 0; i < 11; ++i)
-    if (dst[i])
-      PMPIC_CUDA(cudaMemcpyAsync(dst[i], prop(ctx, kIO[i]), sizeof(double) * ctx->n, cudaMemcpyDeviceToHost, ctx->stream));
+    if (dst[i]) {
+      int rc = get_prop(ctx, kIO[i], ctx->n, dst[i]);
+      if (rc) return rc;
+    }
   PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
   return PMPIC_OK;
 }
@@ -416,21 +539,41 @@ int pmpic_download_parcels(pmpic_ctx* ctx, int64_t capacity, int64_t* n, double*
 int pmpic_download_grid(pmpic_ctx* ctx, int grid, double* dst) {
   if (!ctx || grid < 0 || grid >= PMPIC_NGRID || !dst) return PMPIC_ERR_ARG;
   cudaSetDevice(ctx->device);
-  PMPIC_CUDA(cudaMemcpyAsync(dst, ctx->grid[grid], sizeof(double) * ctx->g.nphys, cudaMemcpyDeviceToHost, ctx->stream));
+  if (ctx->mixed) {  // FP32 grid widened into the spare grid first
+    k_f2d<<<cblk(ctx->g.nphys), 256, 0, ctx->stream>>>(ctx->g.nphys, (const float*)ctx->grid[grid], ctx->gspare);
+    ++ctx->nlaunch;
+    ctx->btot_grid_ready = false;  // gspare is overwritten
+    PMPIC_CUDA(cudaMemcpyAsync(dst, ctx->gspare, sizeof(double) * ctx->g.nphys, cudaMemcpyDeviceToHost, ctx->stream));
+  } else {
+    PMPIC_CUDA(cudaMemcpyAsync(dst, ctx->grid[grid], sizeof(double) * ctx->g.nphys, cudaMemcpyDeviceToHost, ctx->stream));
+  }
   PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
   return PMPIC_OK;
 }
 int pmpic_upload_grid(pmpic_ctx* ctx, int grid, const double* src) {
   if (!ctx || grid < 0 || grid >= PMPIC_NGRID || !src) return PMPIC_ERR_ARG;
   cudaSetDevice(ctx->device);
-  PMPIC_CUDA(cudaMemcpyAsync(ctx->grid[grid], src, sizeof(double) * ctx->g.nphys, cudaMemcpyHostToDevice, ctx->stream));
+  if (ctx->mixed) {
+    PMPIC_CUDA(cudaMemcpyAsync(ctx->gspare, src, sizeof(double) * ctx->g.nphys, cudaMemcpyHostToDevice, ctx->stream));
+    k_d2f<<<cblk(ctx->g.nphys), 256, 0, ctx->stream>>>(ctx->g.nphys, ctx->gspare, (float*)ctx->grid[grid]);
+    ++ctx->nlaunch;
+    ctx->btot_grid_ready = false;
+  } else {
+    PMPIC_CUDA(cudaMemcpyAsync(ctx->grid[grid], src, sizeof(double) * ctx->g.nphys, cudaMemcpyHostToDevice, ctx->stream));
+  }
   PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
   return PMPIC_OK;
 }
 int pmpic_download_spectral(pmpic_ctx* ctx, int spec, double* dst) {
   if (!ctx || spec < 0 || spec >= PMPIC_NSPEC || !dst) return PMPIC_ERR_ARG;
   cudaSetDevice(ctx->device);
-  PMPIC_CUDA(cudaMemcpyAsync(dst, ctx->spec[spec], sizeof(double) * ctx->g.nspec, cudaMemcpyDeviceToHost, ctx->stream));
+  if (ctx->mixed) {
+    k_f2d<<<cblk(ctx->g.nspec), 256, 0, ctx->stream>>>(ctx->g.nspec, (const float*)ctx->spec[spec], ctx->sscratch);
+    ++ctx->nlaunch;
+    PMPIC_CUDA(cudaMemcpyAsync(dst, ctx->sscratch, sizeof(double) * ctx->g.nspec, cudaMemcpyDeviceToHost, ctx->stream));
+  } else {
+    PMPIC_CUDA(cudaMemcpyAsync(dst, ctx->spec[spec], sizeof(double) * ctx->g.nspec, cudaMemcpyDeviceToHost, ctx->stream));
+  }
   PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
   return PMPIC_OK;
 }
@@ -479,9 +622,20 @@ static int do_vort2vel(pmpic_ctx* ctx) {
   // same weights and parcel state, so it runs in the same pass into a spare
   // grid that the vorticity_tendency callback adopts.
   if ((rc = bin_and_sort(ctx))) return rc;
-  const double* f[4] = {prop(ctx, PMPIC_PROP_P), prop(ctx, PMPIC_PROP_Q), prop(ctx, PMPIC_PROP_R), nullptr};
-  double* o[4] = {ctx->grid[PMPIC_GRID_P], ctx->grid[PMPIC_GRID_Q], ctx->grid[PMPIC_GRID_R], ctx->gspare};
-  if ((rc = par2grid_multi(ctx, f, 4, o, true))) return rc;
+  if (ctx->mixed) {
+    // the mixed form computes the btot property first (vorticity_tendency.F90:121-126)
+    // and grids it in the same FP32 pass as p, q, r
+    if ((rc = compute_btot(ctx))) return rc;
+    const float* f[4] = {propf(ctx, PMPIC_PROP_P), propf(ctx, PMPIC_PROP_Q), propf(ctx, PMPIC_PROP_R),
+                         propf(ctx, PMPIC_PROP_BTOT)};
+    float* o[4] = {(float*)ctx->grid[PMPIC_GRID_P], (float*)ctx->grid[PMPIC_GRID_Q], (float*)ctx->grid[PMPIC_GRID_R],
+                   (float*)ctx->gspare};
+    if ((rc = par2grid_multi_m(ctx, f, 4, o))) return rc;
+  } else {
+    const double* f[4] = {prop(ctx, PMPIC_PROP_P), prop(ctx, PMPIC_PROP_Q), prop(ctx, PMPIC_PROP_R), nullptr};
+    double* o[4] = {ctx->grid[PMPIC_GRID_P], ctx->grid[PMPIC_GRID_Q], ctx->grid[PMPIC_GRID_R], ctx->gspare};
+    if ((rc = par2grid_multi(ctx, f, 4, o, true))) return rc;
+  }
   ctx->btot_grid_ready = true;
   if ((rc = vort2vel_spectral(ctx))) return rc;
   // :325-327: the grid2par of u, v, w is deferred into the rk4 pass (or to
@@ -502,16 +656,24 @@ static int do_vorticity_tendency(pmpic_ctx* ctx) {
     if ((rc = flush_gathers(ctx))) return rc;
     ctx->pending_uvw = u;
   }
-  if ((rc = compute_btot(ctx))) return rc;  // :121-126 (the btot property)
   // par2grid(btot) (:129): computed by vort2vel's pass when the state is unchanged
   if (ctx->btot_grid_ready && ctx->sorted_valid) {
+    // :121-126, the btot property (the mixed form wrote it in that pass)
+    if (!ctx->mixed && (rc = compute_btot(ctx))) return rc;
     std::swap(ctx->grid[PMPIC_GRID_B], ctx->gspare);
   } else {
+    if ((rc = compute_btot(ctx))) return rc;
     if (!ctx->sorted_valid)
       if ((rc = bin_and_sort(ctx))) return rc;
-    const double* f[1] = {nullptr};
-    double* o[1] = {ctx->grid[PMPIC_GRID_B]};
-    if ((rc = par2grid_multi(ctx, f, 1, o, true))) return rc;
+    if (ctx->mixed) {
+      const float* f[1] = {propf(ctx, PMPIC_PROP_BTOT)};
+      float* o[1] = {(float*)ctx->grid[PMPIC_GRID_B]};
+      if ((rc = par2grid_multi_m(ctx, f, 1, o))) return rc;
+    } else {
+      const double* f[1] = {nullptr};
+      double* o[1] = {ctx->grid[PMPIC_GRID_B]};
+      if ((rc = par2grid_multi(ctx, f, 1, o, true))) return rc;
+    }
   }
   ctx->btot_grid_ready = false;
   if ((rc = vorticity_tendency_grids(ctx))) return rc;
@@ -600,6 +762,7 @@ int pmpic_op_cell_ids(pmpic_ctx* ctx, int32_t* cells) {
 
 int pmpic_op_par2grid(pmpic_ctx* ctx, int p, int grid) {
   if (!ctx || p < 0 || p >= PMPIC_NPROP || grid < 0 || grid >= PMPIC_NGRID) return PMPIC_ERR_ARG;
+  if (ctx->mixed) return set_error(ctx, PMPIC_ERR_STATE, "kernel-level FP64 operator on a mixed-precision context");
   cudaSetDevice(ctx->device);
   {
     int frc = flush_gathers(ctx);
@@ -615,6 +778,7 @@ int pmpic_op_par2grid(pmpic_ctx* ctx, int p, int grid) {
 
 int pmpic_op_grid2par(pmpic_ctx* ctx, int grid, int p) {
   if (!ctx || p < 0 || p >= PMPIC_NPROP || grid < 0 || grid >= PMPIC_NGRID) return PMPIC_ERR_ARG;
+  if (ctx->mixed) return set_error(ctx, PMPIC_ERR_STATE, "kernel-level FP64 operator on a mixed-precision context");
   cudaSetDevice(ctx->device);
   {
     int frc = flush_gathers(ctx);
@@ -640,6 +804,7 @@ static int d2h(pmpic_ctx* ctx, double* h, const double* d, size_t n) {
 
 int pmpic_op_fft_forward(pmpic_ctx* ctx, const double* phys, double* spec) {
   if (!ctx || !phys || !spec) return PMPIC_ERR_ARG;
+  if (ctx->mixed) return set_error(ctx, PMPIC_ERR_STATE, "kernel-level FP64 operator on a mixed-precision context");
   cudaSetDevice(ctx->device);
   int rc;
   if ((rc = h2d(ctx, ctx->gwork[0], phys, ctx->g.nphys))) return rc;
@@ -648,6 +813,7 @@ int pmpic_op_fft_forward(pmpic_ctx* ctx, const double* phys, double* spec) {
 }
 int pmpic_op_fft_backward(pmpic_ctx* ctx, const double* spec, double* phys) {
   if (!ctx || !phys || !spec) return PMPIC_ERR_ARG;
+  if (ctx->mixed) return set_error(ctx, PMPIC_ERR_STATE, "kernel-level FP64 operator on a mixed-precision context");
   cudaSetDevice(ctx->device);
   int rc;
   if ((rc = h2d(ctx, ctx->sa, spec, ctx->g.nspec))) return rc;
@@ -658,6 +824,7 @@ int pmpic_op_fft_backward(pmpic_ctx* ctx, const double* spec, double* phys) {
 typedef int (*spec_op)(pmpic_ctx*, const double*, double*);
 static int spec_unary(pmpic_ctx* ctx, const double* in, double* out, spec_op op) {
   if (!ctx || !in || !out) return PMPIC_ERR_ARG;
+  if (ctx->mixed) return set_error(ctx, PMPIC_ERR_STATE, "kernel-level FP64 operator on a mixed-precision context");
   cudaSetDevice(ctx->device);
   int rc;
   if ((rc = h2d(ctx, ctx->sa, in, ctx->g.nspec))) return rc;
@@ -669,6 +836,7 @@ int pmpic_op_diffy(pmpic_ctx* ctx, const double* in, double* out) { return spec_
 int pmpic_op_filter(pmpic_ctx* ctx, const double* in, double* out) { return spec_unary(ctx, in, out, spec_filter); }
 int pmpic_op_diffz(pmpic_ctx* ctx, const double* in, double* out, const double* bot, const double* top) {
   if (!ctx || !in || !out || ((bot == nullptr) != (top == nullptr))) return PMPIC_ERR_ARG;
+  if (ctx->mixed) return set_error(ctx, PMPIC_ERR_STATE, "kernel-level FP64 operator on a mixed-precision context");
   cudaSetDevice(ctx->device);
   int rc;
   const size_t cols = (size_t)ctx->g.sx * ctx->g.sy;
@@ -685,6 +853,7 @@ int pmpic_op_diffz(pmpic_ctx* ctx, const double* in, double* out, const double* 
 }
 int pmpic_op_laplinv(pmpic_ctx* ctx, double* inout, int df0) {
   if (!ctx || !inout) return PMPIC_ERR_ARG;
+  if (ctx->mixed) return set_error(ctx, PMPIC_ERR_STATE, "kernel-level FP64 operator on a mixed-precision context");
   cudaSetDevice(ctx->device);
   int rc;
   if ((rc = h2d(ctx, ctx->sa, inout, ctx->g.nspec))) return rc;

@@ -29,6 +29,7 @@ namespace pmpic {
 namespace {
 
 constexpr int FFT_THREADS = 256;
+constexpr int FS_THREADS = 128;
 
 bool factor(int n, std::vector<int>& out) {
   out.clear();
@@ -38,528 +39,6 @@ bool factor(int n, std::vector<int>& out) {
   while (m % 3 == 0) { out.push_back(3); m /= 3; }
   while (m % 5 == 0) { out.push_back(5); m /= 5; }
   return m == 1;
-}
-
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-
-// forward DFT of size R in registers (exp(-2 pi i rt/R))
-template <int R>
-__device__ __forceinline__ void small_dft(double2* a) {
-  if (R == 2) {
-    double2 t0 = cadd(a[0], a[1]), t1 = csub(a[0], a[1]);
-    a[0] = t0; a[1] = t1;
-  } else if (R == 4) {
-    double2 t0 = cadd(a[0], a[2]), t1 = csub(a[0], a[2]);
-    double2 t2 = cadd(a[1], a[3]), t3 = csub(a[1], a[3]);
-    double2 mt3 = make_double2(t3.y, -t3.x);  // -i * t3
-    a[0] = cadd(t0, t2);
-    a[2] = csub(t0, t2);
-    a[1] = cadd(t1, mt3);
-    a[3] = csub(t1, mt3);
-  } else if (R == 3) {
-    const double s3 = 0.86602540378443864676;  // sin(2pi/3)
-    double2 s = cadd(a[1], a[2]), d = csub(a[1], a[2]);
-    double2 b0 = cadd(a[0], s);
-    double2 m = make_double2(a[0].x - 0.5 * s.x, a[0].y - 0.5 * s.y);
-    double2 r = make_double2(s3 * d.y, -s3 * d.x);  // -i sin(2pi/3) d
-    a[0] = b0;
-    a[1] = cadd(m, r);
-    a[2] = csub(m, r);
-  } else if (R == 5) {
-    const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
-    const double s1 = 0.95105651629515357212, s2 = 0.58778525229247312917;
-    double2 t1 = cadd(a[1], a[4]), t2 = cadd(a[2], a[3]);
-    double2 t3 = csub(a[1], a[4]), t4 = csub(a[2], a[3]);
-    double2 b0 = cadd(a[0], cadd(t1, t2));
-    double2 m1 = make_double2(a[0].x + c1 * t1.x + c2 * t2.x, a[0].y + c1 * t1.y + c2 * t2.y);
-    double2 m2 = make_double2(a[0].x + c2 * t1.x + c1 * t2.x, a[0].y + c2 * t1.y + c1 * t2.y);
-    // -i (s1 t3 + s2 t4) and -i (s2 t3 - s1 t4)
-    double2 n1 = make_double2(s1 * t3.y + s2 * t4.y, -(s1 * t3.x + s2 * t4.x));
-    double2 n2 = make_double2(s2 * t3.y - s1 * t4.y, -(s2 * t3.x - s1 * t4.x));
-    a[0] = b0;
-    a[1] = cadd(m1, n1);
-    a[4] = csub(m1, n1);
-    a[2] = cadd(m2, n2);
-    a[3] = csub(m2, n2);
-  }
-}
-
-template <int R>
-__device__ __forceinline__ void stage(const double2* __restrict__ src, double2* __restrict__ dst, int n, int len,
-                                      int nrows, int stride_row, const double2* __restrict__ tw) {
-  const int m = len / R, s = n / len;
-  const int nb = m * s;  // butterflies per row
-  for (int e = threadIdx.x; e < nb * nrows; e += blockDim.x) {
-    int row = e / nb, b = e - row * nb;
-    int p = b / s, q = b - p * s;
-    const double2* S = src + (size_t)row * stride_row;
-    double2* D = dst + (size_t)row * stride_row;
-    double2 a[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) a[r] = S[q + s * (p + r * m)];
-    small_dft<R>(a);
-    D[q + s * (R * p)] = a[0];
-#pragma unroll
-    for (int t = 1; t < R; ++t) D[q + s * (R * p + t)] = cmul(a[t], tw[p * R + t]);
-  }
-}
-
-// Forward complex FFT of nrows rows held in buf0 (stride_row); buf1 is the
-// ping-pong workspace.  Returns the buffer holding the result.
-__device__ double2* fft_rows(double2* buf0, double2* buf1, int nrows, int stride_row, const FftPlan& pl,
-                             const double2* __restrict__ twbase) {
-  double2* src = buf0;
-  double2* dst = buf1;
-  int len = pl.n;
-  for (int st = 0; st < pl.nst; ++st) {
-    const double2* tw = twbase + pl.tw_off[st];
-    switch (pl.radix[st]) {
-      case 4: stage<4>(src, dst, pl.n, len, nrows, stride_row, tw); break;
-      case 2: stage<2>(src, dst, pl.n, len, nrows, stride_row, tw); break;
-      case 3: stage<3>(src, dst, pl.n, len, nrows, stride_row, tw); break;
-      case 5: stage<5>(src, dst, pl.n, len, nrows, stride_row, tw); break;
-    }
-    __syncthreads();
-    len /= pl.radix[st];
-    double2* t = src;
-    src = dst;
-    dst = t;
-  }
-  return src;
-}
-
-// ---- forward y pass: phys -> mid ------------------------------------------------
-// CTA: one z level, TXF consecutive x columns (TXF/2 complex rows of length Ny).
-__global__ void __launch_bounds__(FFT_THREADS) k_fwd_y(Geom g, int TXF, FftPlan pl, const double2* __restrict__ tw,
-                                                       const double* __restrict__ phys, double* __restrict__ mid) {
-  extern __shared__ double2 sm[];
-  const int Ny = g.Ny, Nx = g.Nx;
-  const int nr = TXF / 2;
-  double2* b0 = sm;
-  double2* b1 = sm + (size_t)nr * Ny;
-  const int x0 = blockIdx.x * TXF, k = blockIdx.y;
-  const double* P = phys + (size_t)k * Ny * Nx;
-  for (int e = threadIdx.x; e < Ny * TXF; e += blockDim.x) {
-    int j = e / TXF, x = e - j * TXF;
-    double v = P[(size_t)j * Nx + x0 + x];
-    double* c = (double*)&b0[(x >> 1) * Ny + j];
-    c[x & 1] = v;
-  }
-  __syncthreads();
-  double2* res = fft_rows(b0, b1, nr, Ny, pl, tw);
-  double* M = mid + (size_t)k * g.sy * Nx;
-  const int half = Ny / 2 + 1;
-  for (int e = threadIdx.x; e < half * TXF; e += blockDim.x) {
-    int a = e / TXF, x = e - a * TXF;
-    int r = x >> 1;
-    double2 z1 = res[r * Ny + a];
-    double2 z2 = res[r * Ny + (a == 0 ? 0 : Ny - a)];
-    double re, im;
-    if ((x & 1) == 0) {  // A = (Z_a + conj Z_{N-a}) / 2
-      re = 0.5 * (z1.x + z2.x);
-      im = 0.5 * (z1.y - z2.y);
-    } else {             // B = (Z_a - conj Z_{N-a}) / (2i)
-      re = 0.5 * (z1.y + z2.y);
-      im = -0.5 * (z1.x - z2.x);
-    }
-    M[(size_t)(2 * a) * Nx + x0 + x] = re;
-    M[(size_t)(2 * a + 1) * Nx + x0 + x] = im;
-  }
-}
-
-// ---- forward x pass: mid -> spec ------------------------------------------------
-// CTA: RP pairs of consecutive rows (row = (k, j') flattened), rows of length Nx.
-__global__ void __launch_bounds__(FFT_THREADS) k_fwd_x(Geom g, int RP, int64_t nrows_total, FftPlan pl,
-                                                       const double2* __restrict__ tw, const double* __restrict__ mid,
-                                                       double* __restrict__ spec) {
-  extern __shared__ double2 sm[];
-  const int Nx = g.Nx;
-  double2* b0 = sm;
-  double2* b1 = sm + (size_t)RP * Nx;
-  const int64_t row0 = (int64_t)blockIdx.x * RP * 2;
-  for (int e = threadIdx.x; e < RP * 2 * Nx; e += blockDim.x) {
-    int rr = e / Nx, i = e - rr * Nx;
-    int64_t row = row0 + rr;
-    double v = row < nrows_total ? mid[(size_t)row * Nx + i] : 0.0;
-    double* c = (double*)&b0[(rr >> 1) * Nx + i];
-    c[rr & 1] = v;
-  }
-  __syncthreads();
-  double2* res = fft_rows(b0, b1, RP, Nx, pl, tw);
-  const int half = Nx / 2 + 1;
-  for (int e = threadIdx.x; e < RP * 2 * half; e += blockDim.x) {
-    int rr = e / half, b = e - rr * half;
-    int64_t row = row0 + rr;
-    if (row >= nrows_total) continue;
-    int r = rr >> 1;
-    double2 z1 = res[r * Nx + b];
-    double2 z2 = res[r * Nx + (b == 0 ? 0 : Nx - b)];
-    double re, im;
-    if ((rr & 1) == 0) {
-      re = 0.5 * (z1.x + z2.x);
-      im = 0.5 * (z1.y - z2.y);
-    } else {
-      re = 0.5 * (z1.y + z2.y);
-      im = -0.5 * (z1.x - z2.x);
-    }
-    spec[(size_t)row * g.sx + 2 * b] = re;
-    spec[(size_t)row * g.sx + 2 * b + 1] = im;
-  }
-}
-
-// Build Z_k = A_k + i B_k over the full circle from two half spectra, applying
-// ffte_c2r's conjugate-symmetric fill (ffte_mod.F90:108-113): for k > N/2,
-// A_k = conj(A_{N-k}); the imaginary parts of modes 0 and N/2 never reach the
-// real output, so they are dropped.  Stored conjugated (FFTE computes the
-// inverse as conj(FFT(conj(Z)))/N, vzfft1d.f:41-46, 63-68).
-__device__ __forceinline__ double2 c2r_pack(double2 A, double2 B, int k, int n) {
-  // A, B are the half-spectrum values at min(k, n-k); mirrored if k > n/2
-  if (k == 0 || 2 * k == n) {
-    A.y = 0.0;
-    B.y = 0.0;
-  }
-  double2 z;
-  if (2 * k <= n) {
-    z = make_double2(A.x - B.y, A.y + B.x);  // A + iB
-  } else {
-    // conj(A) + i conj(B) = (A.x + B.y) + i(-A.y + B.x)
-    z = make_double2(A.x + B.y, -A.y + B.x);
-  }
-  return make_double2(z.x, -z.y);  // conj for the forward-transform inverse
-}
-
-// ---- inverse x pass: spec -> mid ------------------------------------------------
-__global__ void __launch_bounds__(FFT_THREADS) k_inv_x(Geom g, int RP, int64_t nrows_total, FftPlan pl,
-                                                       const double2* __restrict__ tw, const double* __restrict__ spec,
-                                                       double* __restrict__ mid) {
-  extern __shared__ double2 sm[];
-  const int Nx = g.Nx;
-  double2* b0 = sm;
-  double2* b1 = sm + (size_t)RP * Nx;
-  const int64_t row0 = (int64_t)blockIdx.x * RP * 2;
-  for (int e = threadIdx.x; e < RP * Nx; e += blockDim.x) {
-    int r = e / Nx, k = e - r * Nx;
-    int km = (2 * k <= Nx) ? k : Nx - k;
-    int64_t ra = row0 + 2 * r, rb = ra + 1;
-    double2 A = make_double2(0.0, 0.0), B = make_double2(0.0, 0.0);
-    if (ra < nrows_total) A = make_double2(spec[(size_t)ra * g.sx + 2 * km], spec[(size_t)ra * g.sx + 2 * km + 1]);
-    if (rb < nrows_total) B = make_double2(spec[(size_t)rb * g.sx + 2 * km], spec[(size_t)rb * g.sx + 2 * km + 1]);
-    b0[r * Nx + k] = c2r_pack(A, B, k, Nx);
-  }
-  __syncthreads();
-  double2* res = fft_rows(b0, b1, RP, Nx, pl, tw);
-  const double dn = 1.0 / (double)Nx;
-  for (int e = threadIdx.x; e < RP * 2 * Nx; e += blockDim.x) {
-    int rr = e / Nx, i = e - rr * Nx;
-    int64_t row = row0 + rr;
-    if (row >= nrows_total) continue;
-    double2 z = res[(rr >> 1) * Nx + i];
-    // conj(z) * dn: real part -> row A, imaginary part -> row B
-    mid[(size_t)row * Nx + i] = (rr & 1) == 0 ? z.x * dn : -z.y * dn;
-  }
-}
-
-// ---- inverse y pass: mid -> phys ------------------------------------------------
-__global__ void __launch_bounds__(FFT_THREADS) k_inv_y(Geom g, int TXF, FftPlan pl, const double2* __restrict__ tw,
-                                                       const double* __restrict__ mid, double* __restrict__ phys) {
-  extern __shared__ double2 sm[];
-  const int Ny = g.Ny, Nx = g.Nx;
-  const int nr = TXF / 2;
-  double2* b0 = sm;
-  double2* b1 = sm + (size_t)nr * Ny;
-  const int x0 = blockIdx.x * TXF, k = blockIdx.y;
-  const double* M = mid + (size_t)k * g.sy * Nx;
-  // stage the half spectra (Ny/2+1 modes x TXF columns) into b1 first
-  const int half = Ny / 2 + 1;
-  for (int e = threadIdx.x; e < half * TXF; e += blockDim.x) {
-    int a = e / TXF, x = e - a * TXF;
-    b1[x * half + a] = make_double2(M[(size_t)(2 * a) * Nx + x0 + x], M[(size_t)(2 * a + 1) * Nx + x0 + x]);
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < nr * Ny; e += blockDim.x) {
-    int r = e / Ny, kk = e - r * Ny;
-    int km = (2 * kk <= Ny) ? kk : Ny - kk;
-    double2 A = b1[(2 * r) * half + km], B = b1[(2 * r + 1) * half + km];
-    b0[r * Ny + kk] = c2r_pack(A, B, kk, Ny);
-  }
-  __syncthreads();
-  double2* res = fft_rows(b0, b1, nr, Ny, pl, tw);
-  const double dn = 1.0 / (double)Ny;
-  double* P = phys + (size_t)k * Ny * Nx;
-  for (int e = threadIdx.x; e < Ny * TXF; e += blockDim.x) {
-    int j = e / TXF, x = e - j * TXF;
-    double2 z = res[(x >> 1) * Ny + j];
-    P[(size_t)j * Nx + x0 + x] = (x & 1) == 0 ? z.x * dn : -z.y * dn;
-  }
-}
-
-// ---- four-step register FFT for n = n1 * n2, n1, n2 in {4, 8, 16} --------------------
-// x[n2 + N2 n1] -> X[k1 + N1 k2]:  n1-point DFTs over n1 (one thread per n2),
-// twiddle W_n^(n2 k1), transpose through shared memory, n2-point DFTs over n2
-// (one thread per k1).  The small DFTs run in registers; loads and stores touch
-// global memory once each.
-
-// W_16^m = exp(-2 pi i m / 16), m known at compile time after unrolling
-__device__ __forceinline__ double2 w16(int m) {
-  constexpr double C1 = 0.92387953251128675613;  // cos(pi/8)
-  constexpr double C2 = 0.70710678118654752440;  // cos(pi/4)
-  constexpr double C3 = 0.38268343236508977173;  // cos(3pi/8)
-  switch (m & 15) {
-    case 0: return make_double2(1.0, 0.0);
-    case 1: return make_double2(C1, -C3);
-    case 2: return make_double2(C2, -C2);
-    case 3: return make_double2(C3, -C1);
-    case 4: return make_double2(0.0, -1.0);
-    case 5: return make_double2(-C3, -C1);
-    case 6: return make_double2(-C2, -C2);
-    case 7: return make_double2(-C1, -C3);
-    case 8: return make_double2(-1.0, 0.0);
-    case 9: return make_double2(-C1, C3);
-    case 10: return make_double2(-C2, C2);
-    case 11: return make_double2(-C3, C1);
-    case 12: return make_double2(0.0, 1.0);
-    case 13: return make_double2(C3, C1);
-    case 14: return make_double2(C2, C2);
-    default: return make_double2(C1, C3);
-  }
-}
-
-// forward DFT of size R in registers, natural order in and out
-template <int R>
-__device__ __forceinline__ void dft(double2* a) {
-  if constexpr (R <= 5) {
-    small_dft<R>(a);
-  } else {
-    constexpr int M1 = 4, M2 = R / 4;  // R = 8: 4 x 2, R = 16: 4 x 4
-    double2 y[R];
-#pragma unroll
-    for (int n2 = 0; n2 < M2; ++n2) {
-      double2 b[M1];
-#pragma unroll
-      for (int n1 = 0; n1 < M1; ++n1) b[n1] = a[M2 * n1 + n2];
-      small_dft<M1>(b);
-#pragma unroll
-      for (int k1 = 0; k1 < M1; ++k1) y[k1 * M2 + n2] = (n2 * k1 == 0) ? b[k1] : cmul(b[k1], w16(n2 * k1 * (16 / R)));
-    }
-#pragma unroll
-    for (int k1 = 0; k1 < M1; ++k1) {
-      double2 c[M2];
-#pragma unroll
-      for (int n2 = 0; n2 < M2; ++n2) c[n2] = y[k1 * M2 + n2];
-      small_dft<M2>(c);
-#pragma unroll
-      for (int k2 = 0; k2 < M2; ++k2) a[k1 + M1 * k2] = c[k2];
-    }
-  }
-}
-
-constexpr int FS_THREADS = 128;
-
-// step 1 of one row: a[n1] = x[n2 + N2 n1] on entry; Y row [k1][n2] (padded)
-template <int N1, int N2>
-__device__ __forceinline__ void fs_step1(double2* a, int n2, double2* Yrow, const double2* __restrict__ tw4) {
-  dft<N1>(a);
-#pragma unroll
-  for (int k1 = 0; k1 < N1; ++k1) Yrow[k1 * (N2 + 1) + n2] = (k1 == 0 || n2 == 0) ? a[k1] : cmul(a[k1], tw4[n2 * N1 + k1]);
-}
-// step 3 of one row: a[k2] = X[k1 + N1 k2] on return
-template <int N1, int N2>
-__device__ __forceinline__ void fs_step3(double2* a, int k1, const double2* Yrow) {
-#pragma unroll
-  for (int n2 = 0; n2 < N2; ++n2) a[n2] = Yrow[k1 * (N2 + 1) + n2];
-  dft<N2>(a);
-}
-
-// forward x pass (mid -> spec): RP complex rows (pairs of real rows) per CTA
-template <int N1, int N2>
-__global__ void __launch_bounds__(FS_THREADS) k4_fwd_x(Geom g, int64_t nrows_total, const double2* __restrict__ tw4,
-                                                       const double* __restrict__ mid, double* __restrict__ spec) {
-  constexpr int N = N1 * N2, RP = FS_THREADS / (N1 > N2 ? N1 : N2), YS = N1 * (N2 + 1);
-  __shared__ double2 Y[RP * YS];
-  double2* X = Y;  // [RP][N], reuses Y after step 3 has read it
-  const int t = threadIdx.x;
-  const int64_t row0 = (int64_t)blockIdx.x * RP * 2;
-  if (t < RP * N2) {
-    const int r = t / N2, n2 = t % N2;
-    const int64_t ra = row0 + 2 * r, rb = ra + 1;
-    double2 a[N1];
-#pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1) {
-      const int i = n2 + N2 * n1;
-      a[n1] = make_double2(ra < nrows_total ? mid[(size_t)ra * N + i] : 0.0,
-                           rb < nrows_total ? mid[(size_t)rb * N + i] : 0.0);
-    }
-    fs_step1<N1, N2>(a, n2, Y + r * YS, tw4);
-  }
-  __syncthreads();
-  {  // every thread reaches the barrier; RP * N1 <= FS_THREADS
-    const bool act = t < RP * N1;
-    const int r = t / N1, k1 = t % N1;
-    double2 a[N2];
-    if (act) fs_step3<N1, N2>(a, k1, Y + r * YS);
-    __syncthreads();
-#pragma unroll
-    for (int k2 = 0; k2 < N2; ++k2)
-      if (act) X[r * N + k1 + N1 * k2] = a[k2];
-  }
-  __syncthreads();
-  // separate the two real rows: A = (Z_b + conj Z_{N-b}) / 2, B = (Z_b - conj Z_{N-b}) / (2i)
-  constexpr int HALF = N / 2 + 1;
-  for (int e = t; e < RP * 2 * HALF; e += FS_THREADS) {
-    const int rr = e / HALF, b = e - rr * HALF;
-    const int64_t row = row0 + rr;
-    if (row >= nrows_total) continue;
-    const int r = rr >> 1;
-    const double2 z1 = X[r * N + b];
-    const double2 z2 = X[r * N + (b == 0 ? 0 : N - b)];
-    double re, im;
-    if ((rr & 1) == 0) {
-      re = 0.5 * (z1.x + z2.x);
-      im = 0.5 * (z1.y - z2.y);
-    } else {
-      re = 0.5 * (z1.y + z2.y);
-      im = -0.5 * (z1.x - z2.x);
-    }
-    spec[(size_t)row * g.sx + 2 * b] = re;
-    spec[(size_t)row * g.sx + 2 * b + 1] = im;
-  }
-}
-
-// inverse x pass (spec -> mid)
-template <int N1, int N2>
-__global__ void __launch_bounds__(FS_THREADS) k4_inv_x(Geom g, int64_t nrows_total, const double2* __restrict__ tw4,
-                                                       const double* __restrict__ spec, double* __restrict__ mid) {
-  constexpr int N = N1 * N2, RP = FS_THREADS / (N1 > N2 ? N1 : N2), YS = N1 * (N2 + 1);
-  __shared__ double2 Y[RP * YS];
-  const int t = threadIdx.x;
-  const int64_t row0 = (int64_t)blockIdx.x * RP * 2;
-  if (t < RP * N2) {
-    const int r = t / N2, n2 = t % N2;
-    const int64_t ra = row0 + 2 * r, rb = ra + 1;
-    double2 a[N1];
-#pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1) {
-      const int k = n2 + N2 * n1;
-      const int km = (2 * k <= N) ? k : N - k;
-      double2 A = make_double2(0.0, 0.0), B = make_double2(0.0, 0.0);
-      if (ra < nrows_total) A = make_double2(spec[(size_t)ra * g.sx + 2 * km], spec[(size_t)ra * g.sx + 2 * km + 1]);
-      if (rb < nrows_total) B = make_double2(spec[(size_t)rb * g.sx + 2 * km], spec[(size_t)rb * g.sx + 2 * km + 1]);
-      a[n1] = c2r_pack(A, B, k, N);
-    }
-    fs_step1<N1, N2>(a, n2, Y + r * YS, tw4);
-  }
-  __syncthreads();
-  const double dn = 1.0 / (double)N;
-  if (t < RP * N1) {
-    const int r = t / N1, k1 = t % N1;
-    double2 a[N2];
-    fs_step3<N1, N2>(a, k1, Y + r * YS);
-    const int64_t ra = row0 + 2 * r, rb = ra + 1;
-#pragma unroll
-    for (int k2 = 0; k2 < N2; ++k2) {
-      const int i = k1 + N1 * k2;  // conj(z) * dn: real part -> row A, imaginary part -> row B
-      if (ra < nrows_total) mid[(size_t)ra * N + i] = a[k2].x * dn;
-      if (rb < nrows_total) mid[(size_t)rb * N + i] = -a[k2].y * dn;
-    }
-  }
-}
-
-// forward y pass (phys -> mid): one z level, 16 consecutive x columns
-// (8 complex columns) per CTA; thread order puts consecutive x on consecutive threads
-template <int N1, int N2>
-__global__ void __launch_bounds__(FS_THREADS) k4_fwd_y(Geom g, const double2* __restrict__ tw4,
-                                                       const double* __restrict__ phys, double* __restrict__ mid) {
-  // rows of Y and X are padded so the 8 column pairs of a warp access fall in
-  // distinct shared-memory banks
-  constexpr int N = N1 * N2, RP = 8, YS = N1 * (N2 + 1) + 1, XS = N + 1;
-  __shared__ double2 Y[RP * YS];
-  double2* X = Y;  // [RP][XS], reuses Y after step 3 has read it
-  const int t = threadIdx.x, Nx = g.Nx;
-  const int x0 = blockIdx.x * 2 * RP, k = blockIdx.y;
-  const double* P = phys + (size_t)k * N * Nx;
-  if (t < RP * N2) {
-    const int r = t % RP, n2 = t / RP;
-    double2 a[N1];
-#pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1) {
-      const int j = n2 + N2 * n1;
-      a[n1] = *(const double2*)&P[(size_t)j * Nx + x0 + 2 * r];  // columns x0+2r (re), x0+2r+1 (im)
-    }
-    fs_step1<N1, N2>(a, n2, Y + r * YS, tw4);
-  }
-  __syncthreads();
-  {  // every thread reaches the barrier; RP * N1 <= FS_THREADS
-    const bool act = t < RP * N1;
-    const int r = t % RP, k1 = t / RP;
-    double2 a[N2];
-    if (act) fs_step3<N1, N2>(a, k1, Y + r * YS);
-    __syncthreads();
-#pragma unroll
-    for (int k2 = 0; k2 < N2; ++k2)
-      if (act) X[r * XS + k1 + N1 * k2] = a[k2];
-  }
-  __syncthreads();
-  constexpr int HALF = N / 2 + 1;
-  double* M = mid + (size_t)k * g.sy * Nx;
-  for (int e = t; e < HALF * 2 * RP; e += FS_THREADS) {
-    const int a = e / (2 * RP), x = e - a * (2 * RP);
-    const int r = x >> 1;
-    const double2 z1 = X[r * XS + a];
-    const double2 z2 = X[r * XS + (a == 0 ? 0 : N - a)];
-    double re, im;
-    if ((x & 1) == 0) {
-      re = 0.5 * (z1.x + z2.x);
-      im = 0.5 * (z1.y - z2.y);
-    } else {
-      re = 0.5 * (z1.y + z2.y);
-      im = -0.5 * (z1.x - z2.x);
-    }
-    M[(size_t)(2 * a) * Nx + x0 + x] = re;
-    M[(size_t)(2 * a + 1) * Nx + x0 + x] = im;
-  }
-}
-
-// inverse y pass (mid -> phys)
-template <int N1, int N2>
-__global__ void __launch_bounds__(FS_THREADS) k4_inv_y(Geom g, const double2* __restrict__ tw4,
-                                                       const double* __restrict__ mid, double* __restrict__ phys) {
-  // rows of Y and X are padded so the 8 column pairs of a warp access fall in
-  // distinct shared-memory banks
-  constexpr int N = N1 * N2, RP = 8, YS = N1 * (N2 + 1) + 1;
-  __shared__ double2 Y[RP * YS];
-  const int t = threadIdx.x, Nx = g.Nx;
-  const int x0 = blockIdx.x * 2 * RP, k = blockIdx.y;
-  const double* M = mid + (size_t)k * g.sy * Nx;
-  if (t < RP * N2) {
-    const int r = t % RP, n2 = t / RP;
-    double2 a[N1];
-#pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1) {
-      const int kk = n2 + N2 * n1;
-      const int km = (2 * kk <= N) ? kk : N - kk;
-      const double2 re = *(const double2*)&M[(size_t)(2 * km) * Nx + x0 + 2 * r];      // (A.re, B.re)
-      const double2 im = *(const double2*)&M[(size_t)(2 * km + 1) * Nx + x0 + 2 * r];  // (A.im, B.im)
-      a[n1] = c2r_pack(make_double2(re.x, im.x), make_double2(re.y, im.y), kk, N);
-    }
-    fs_step1<N1, N2>(a, n2, Y + r * YS, tw4);
-  }
-  __syncthreads();
-  const double dn = 1.0 / (double)N;
-  if (t < RP * N1) {
-    const int r = t % RP, k1 = t / RP;
-    double2 a[N2];
-    fs_step3<N1, N2>(a, k1, Y + r * YS);
-    double* P = phys + (size_t)k * N * Nx;
-#pragma unroll
-    for (int k2 = 0; k2 < N2; ++k2) {
-      const int j = k1 + N1 * k2;
-      *(double2*)&P[(size_t)j * Nx + x0 + 2 * r] = make_double2(a[k2].x * dn, -a[k2].y * dn);
-    }
-  }
 }
 
 // the four-step split used for a row length (0: none)
@@ -574,41 +53,6 @@ void fs_split(int n, int& n1, int& n2) {
     default: break;
   }
 }
-
-// launchers by split; return false if the split has no instantiation
-#define PMPIC_FS_CASES(CALL) \
-  if (n1 == 4 && n2 == 4) { CALL(4, 4); return true; } \
-  if (n1 == 8 && n2 == 4) { CALL(8, 4); return true; } \
-  if (n1 == 8 && n2 == 8) { CALL(8, 8); return true; } \
-  if (n1 == 16 && n2 == 8) { CALL(16, 8); return true; } \
-  if (n1 == 16 && n2 == 16) { CALL(16, 16); return true; } \
-  return false;
-
-bool fs_fwd_x(int n1, int n2, unsigned nb, cudaStream_t st, const Geom& g, int64_t nrows, const double2* tw4,
-              const double* mid, double* spec) {
-#define CALL(A, B) k4_fwd_x<A, B><<<nb, FS_THREADS, 0, st>>>(g, nrows, tw4, mid, spec)
-  PMPIC_FS_CASES(CALL)
-#undef CALL
-}
-bool fs_inv_x(int n1, int n2, unsigned nb, cudaStream_t st, const Geom& g, int64_t nrows, const double2* tw4,
-              const double* spec, double* mid) {
-#define CALL(A, B) k4_inv_x<A, B><<<nb, FS_THREADS, 0, st>>>(g, nrows, tw4, spec, mid)
-  PMPIC_FS_CASES(CALL)
-#undef CALL
-}
-bool fs_fwd_y(int n1, int n2, dim3 gr, cudaStream_t st, const Geom& g, const double2* tw4, const double* phys,
-              double* mid) {
-#define CALL(A, B) k4_fwd_y<A, B><<<gr, FS_THREADS, 0, st>>>(g, tw4, phys, mid)
-  PMPIC_FS_CASES(CALL)
-#undef CALL
-}
-bool fs_inv_y(int n1, int n2, dim3 gr, cudaStream_t st, const Geom& g, const double2* tw4, const double* mid,
-              double* phys) {
-#define CALL(A, B) k4_inv_y<A, B><<<gr, FS_THREADS, 0, st>>>(g, tw4, mid, phys)
-  PMPIC_FS_CASES(CALL)
-#undef CALL
-}
-#undef PMPIC_FS_CASES
 
 // four-step twiddles W_n^(n2 k1), [n2 * n1 + k1], long double accuracy
 void fs_twiddles(FftPlan& p, std::vector<double2>& tw) {
@@ -661,6 +105,20 @@ int pick_rp(int n) {  // complex rows per CTA for the x passes
 
 }  // namespace
 
+// the transform kernels, once per precision
+namespace f64 {
+using real = double;
+using real2 = double2;
+__host__ __device__ __forceinline__ double2 mk2(double a, double b) { return make_double2(a, b); }
+#include "fft_impl.cuh"
+}  // namespace f64
+namespace f32 {
+using real = float;
+using real2 = float2;
+__host__ __device__ __forceinline__ float2 mk2(float a, float b) { return make_float2(a, b); }
+#include "fft_impl.cuh"
+}  // namespace f32
+
 int fft_init(pmpic_ctx* ctx) {
   std::vector<int> tmp;
   if (!factor(ctx->g.Nx, tmp) || !factor(ctx->g.Ny, tmp))
@@ -678,79 +136,30 @@ int fft_init(pmpic_ctx* ctx) {
   if (ctx->g.Nx % 16 != 0) py.n1 = py.n2 = 0;
   PMPIC_CUDA(cudaMalloc(&ctx->ftw, sizeof(double2) * tw.size()));
   PMPIC_CUDA(cudaMemcpy(ctx->ftw, tw.data(), sizeof(double2) * tw.size(), cudaMemcpyHostToDevice));
+  // the FP32 table: the same twiddles rounded once to single precision
+  std::vector<float2> tw32(tw.size());
+  for (size_t i = 0; i < tw.size(); ++i) tw32[i] = make_float2((float)tw[i].x, (float)tw[i].y);
+  PMPIC_CUDA(cudaMalloc(&ctx->ftw32, sizeof(float2) * tw32.size()));
+  PMPIC_CUDA(cudaMemcpy(ctx->ftw32, tw32.data(), sizeof(float2) * tw32.size(), cudaMemcpyHostToDevice));
   ctx->plan_x = px;
   ctx->plan_y = py;
   // per device (the attribute is a property of the function on the current device)
-  PMPIC_CUDA(cudaFuncSetAttribute(k_fwd_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-  PMPIC_CUDA(cudaFuncSetAttribute(k_inv_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-  PMPIC_CUDA(cudaFuncSetAttribute(k_fwd_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-  PMPIC_CUDA(cudaFuncSetAttribute(k_inv_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  PMPIC_CUDA(f64::fft_attributes());
+  PMPIC_CUDA(f32::fft_attributes());
   return 0;
 }
 
 int fft_forward(pmpic_ctx* ctx, const double* phys, double* spec) {
-  TimerScope ts(ctx, T_FFTF);
-  const Geom& g = ctx->g;
-  const FftPlan& px = ctx->plan_x;
-  const FftPlan& py = ctx->plan_y;
-  const double2* tw = (const double2*)ctx->ftw;
-  const double2* twy = tw + ctx->ftw_off_y;
-  if (py.n1) {
-    fs_fwd_y(py.n1, py.n2, dim3(g.Nx / 16, g.nzp), ctx->stream, g, twy + py.tw4_off, phys, ctx->fftmid);
-  } else {
-    int txf = pick_txf(g.Nx);
-    size_t sm_y = sizeof(double2) * (size_t)(txf / 2) * g.Ny * 2;
-    dim3 gy(g.Nx / txf, g.nzp);
-    k_fwd_y<<<gy, FFT_THREADS, sm_y, ctx->stream>>>(g, txf, py, twy, phys, ctx->fftmid);
-  }
-  ++ctx->nlaunch;
-  int64_t nrows = (int64_t)g.nzp * g.sy;
-  if (px.n1) {
-    const int rp = FS_THREADS / std::max(px.n1, px.n2);
-    fs_fwd_x(px.n1, px.n2, (unsigned)((nrows + 2 * rp - 1) / (2 * rp)), ctx->stream, g, nrows, tw + px.tw4_off,
-             ctx->fftmid, spec);
-  } else {
-    int rp = pick_rp(g.Nx);
-    size_t sm_x = sizeof(double2) * (size_t)rp * g.Nx * 2;
-    k_fwd_x<<<(unsigned)((nrows + 2 * rp - 1) / (2 * rp)), FFT_THREADS, sm_x, ctx->stream>>>(g, rp, nrows, px, tw,
-                                                                                          ctx->fftmid, spec);
-  }
-  ++ctx->nlaunch;
-  PMPIC_CUDA(cudaGetLastError());
-  return 0;
+  return f64::fft_forward_impl(ctx, phys, spec, ctx->fftmid, (const double2*)ctx->ftw);
 }
-
 int fft_backward(pmpic_ctx* ctx, const double* spec, double* phys) {
-  TimerScope ts(ctx, T_FFTI);
-  const Geom& g = ctx->g;
-  const FftPlan& px = ctx->plan_x;
-  const FftPlan& py = ctx->plan_y;
-  const double2* tw = (const double2*)ctx->ftw;
-  int64_t nrows = (int64_t)g.nzp * g.sy;
-  if (px.n1) {
-    const int rp = FS_THREADS / std::max(px.n1, px.n2);
-    fs_inv_x(px.n1, px.n2, (unsigned)((nrows + 2 * rp - 1) / (2 * rp)), ctx->stream, g, nrows, tw + px.tw4_off,
-             spec, ctx->fftmid);
-  } else {
-    int rp = pick_rp(g.Nx);
-    size_t sm_x = sizeof(double2) * (size_t)rp * g.Nx * 2;
-    k_inv_x<<<(unsigned)((nrows + 2 * rp - 1) / (2 * rp)), FFT_THREADS, sm_x, ctx->stream>>>(g, rp, nrows, px, tw,
-                                                                                          spec, ctx->fftmid);
-  }
-  ++ctx->nlaunch;
-  const double2* twy = tw + ctx->ftw_off_y;
-  if (py.n1) {
-    fs_inv_y(py.n1, py.n2, dim3(g.Nx / 16, g.nzp), ctx->stream, g, twy + py.tw4_off, ctx->fftmid, phys);
-  } else {
-    int txf = pick_txf(g.Nx);
-    size_t half = (size_t)g.Ny / 2 + 1;
-    size_t sm_y = sizeof(double2) * std::max((size_t)(txf / 2) * g.Ny * 2, (size_t)(txf / 2) * g.Ny + txf * half);
-    dim3 gy(g.Nx / txf, g.nzp);
-    k_inv_y<<<gy, FFT_THREADS, sm_y, ctx->stream>>>(g, txf, py, twy, ctx->fftmid, phys);
-  }
-  ++ctx->nlaunch;
-  PMPIC_CUDA(cudaGetLastError());
-  return 0;
+  return f64::fft_backward_impl(ctx, spec, phys, ctx->fftmid, (const double2*)ctx->ftw);
+}
+int fft_forward(pmpic_ctx* ctx, const float* phys, float* spec) {
+  return f32::fft_forward_impl(ctx, phys, spec, (float*)ctx->fftmid, (const float2*)ctx->ftw32);
+}
+int fft_backward(pmpic_ctx* ctx, const float* spec, float* phys) {
+  return f32::fft_backward_impl(ctx, spec, phys, (float*)ctx->fftmid, (const float2*)ctx->ftw32);
 }
 
 }  // namespace pmpic

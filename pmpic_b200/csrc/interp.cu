@@ -58,6 +58,26 @@ __global__ void k_bin_count(Geom g, int64_t n, const double* __restrict__ X, con
   if ((threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&count[id], __popc(same));
 }
 
+// the mixed form's binning: the cell is the integer part of the position
+__global__ void k_bin_count_m(Geom g, int64_t n, const CellOff* __restrict__ X, const CellOff* __restrict__ Y,
+                              const CellOff* __restrict__ Z, int32_t* __restrict__ cell, int32_t* __restrict__ count,
+                              DevInfo* info) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const CellOff x = X[t], y = Y[t], z = Z[t];
+  if (x.i < 0 || x.i >= g.Nx || y.i < 0 || y.i >= g.Ny || z.i < 0 || z.i >= g.Nz || !(x.f >= 0.f && x.f <= 1.f) ||
+      !(y.f >= 0.f && y.f <= 1.f) || !(z.f >= 0.f && z.f <= 1.f)) {
+    cell[t] = -1;
+    atomicCAS(&info->error, 0, PMPIC_ERR_OUT_OF_BOX);
+    return;
+  }
+  const int32_t id = (int32_t)(((int64_t)x.i * g.Ny + y.i) * g.Nz + z.i);
+  cell[t] = id;
+  const unsigned act = __activemask();
+  const unsigned same = __match_any_sync(act, id);
+  if ((threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&count[id], __popc(same));
+}
+
 __global__ void k_bin_scatter(int64_t n, const int32_t* __restrict__ cell, const int32_t* __restrict__ start,
                               int32_t* __restrict__ fill, int32_t* __restrict__ sorted) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -214,11 +234,11 @@ __global__ void k_scan_apply(const int32_t* __restrict__ in, int64_t n, const in
 //  2. k_p2g_combine: per grid point, row y-1's y-high part plus row y's y-low
 //     part (and, on the bottom level of a chunk, the chunk below's top level
 //     first), then the normalisation or wall doubling.
-template <int NQ>
+template <int NQ, class R = double>
 struct P2GArgs {
-  const double* f[NQ];  // per-parcel fields (MODE 1/2: f[0] unused)
-  double* out[NQ];
-  const double* bh[3];  // b, h, z for btot
+  const R* f[NQ];       // per-parcel fields (MODE 1/2: f[0] unused)
+  R* out[NQ];
+  const R* bh[3];       // b, h, z for btot (plain FP64 path only)
   int32_t* npercell;
   double vmin;
 };
@@ -246,17 +266,33 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+// one staged value of type R
+template <class R>
+__device__ __forceinline__ void cp_async_r(R* smem, const R* gmem) {
+  if constexpr (sizeof(R) == 8) cp_async8(smem, gmem);
+  else cp_async4(smem, gmem);
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-template <int NQ, int MODE, bool BT>
+// R: the arithmetic type (double: plain path, float: mixed-precision form).
+// The cell offsets delx, dely, delz of parcel n are DX[ds * n], DY[ds * n],
+// DZ[ds * n]: the cached binning (ds = 1) or the offset half of the mixed
+// form's {cell index, offset} positions (ds = 2).
+template <int NQ, int MODE, bool BT, class R = double>
 __global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, const int32_t* __restrict__ start,
-                                                     const int32_t* __restrict__ sorted, const double* __restrict__ del,
-                                                     int64_t cap, const double* __restrict__ VOL, P2GArgs<NQ> a,
-                                                     double* __restrict__ rowpart) {
+                                                     const int32_t* __restrict__ sorted, const R* __restrict__ DX,
+                                                     const R* __restrict__ DY, const R* __restrict__ DZ, int ds,
+                                                     const R* __restrict__ VOL, P2GArgs<NQ, R> a,
+                                                     R* __restrict__ rowpart) {
   using Lay = P2GLayout<NQ, MODE, BT>;
   constexpr int NA = Lay::NA, NS = Lay::NS;
   constexpr unsigned FULL = 0xffffffffu;
-  __shared__ __align__(16) double smem[RW][NS * SPAD];
+  static_assert(!BT || sizeof(R) == 8, "btot from b, h, z only on the FP64 path");
+  __shared__ __align__(16) R smem[RW][NS * SPAD];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t wid = (int64_t)blockIdx.x * RW + warp;
   if (wid >= (int64_t)nxs * g.Ny * nzc) return;  // the whole warp leaves together
@@ -271,12 +307,9 @@ __global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, 
   // and odd lane 2m+1 level m+1 (top corners of layer m + bottom corners of m+1)
   const int lev = lane == 0 ? 0 : (lane >> 1) + 1;
   const bool owner = (lane == 0 || (lane & 1)) && lev <= nk;
-  double* S = smem[warp];
-  const double* DX = del;
-  const double* DY = del + cap;
-  const double* DZ = del + 2 * cap;
-  double* out_row = rowpart + ((size_t)zc * g.Ny + cy) * (size_t)g.Nx * Lay::RPS;
-  double C[2][NA];  // x-high corners of the previous column, per y corner
+  R* S = smem[warp];
+  R* out_row = rowpart + ((size_t)zc * g.Ny + cy) * (size_t)g.Nx * Lay::RPS;
+  R C[2][NA];  // x-high corners of the previous column, per y corner
   // the column before the segment (periodic) only seeds the carry
   for (int it = -1; it < x_hi - x_lo; ++it) {
     int cx = x_lo + it;
@@ -289,11 +322,11 @@ __global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, 
     }
     const int q0 = __shfl_sync(FULL, s_me, 0);
     const int q1 = __shfl_sync(FULL, e_me, 2 * nk - 2);
-    double acc[4][NA];  // [y corner * 2 + x corner][quantity] of this lane's z corner
+    R acc[4][NA];  // [y corner * 2 + x corner][quantity] of this lane's z corner
 #pragma unroll
     for (int ab = 0; ab < 4; ++ab)
 #pragma unroll
-      for (int q = 0; q < NA; ++q) acc[ab][q] = 0.0;
+      for (int q = 0; q < NA; ++q) acc[ab][q] = R(0);
     int nkept = 0;
     for (int b0 = q0; b0 < q1; b0 += BATCH) {
       const int nb = min(BATCH, q1 - b0);
@@ -309,53 +342,54 @@ __global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, 
         const int n = slot[j];
         if (n < 0) continue;
         const int p = lane + 32 * j;
-        double* D = S + p + (p >> 4);
-        cp_async8(D, DX + n);
-        cp_async8(D + SPAD, DY + n);
-        cp_async8(D + 2 * SPAD, DZ + n);
-        cp_async8(D + 3 * SPAD, VOL + n);
+        R* D = S + p + (p >> 4);
+        const size_t nd = (size_t)ds * n;
+        cp_async_r(D, DX + nd);
+        cp_async_r(D + SPAD, DY + nd);
+        cp_async_r(D + 2 * SPAD, DZ + nd);
+        cp_async_r(D + 3 * SPAD, VOL + n);
         if (MODE == 0) {
 #pragma unroll
-          for (int f = 0; f < (BT ? NQ - 1 : NQ); ++f) cp_async8(D + (4 + f) * SPAD, a.f[f] + n);
+          for (int f = 0; f < (BT ? NQ - 1 : NQ); ++f) cp_async_r(D + (4 + f) * SPAD, a.f[f] + n);
           if (BT) {
 #pragma unroll
-            for (int f = 0; f < 3; ++f) cp_async8(D + (4 + NQ - 1 + f) * SPAD, a.bh[f] + n);
+            for (int f = 0; f < 3; ++f) cp_async_r(D + (4 + NQ - 1 + f) * SPAD, a.bh[f] + n);
           }
         } else {
 #pragma unroll
-          for (int f = 1; f < NQ; ++f) cp_async8(D + (4 + f - 1) * SPAD, a.f[f] + n);
+          for (int f = 1; f < NQ; ++f) cp_async_r(D + (4 + f - 1) * SPAD, a.f[f] + n);
         }
       }
       cp_async_wait_all();
       __syncwarp();
-      if (BT) {  // btot per parcel, once (vorticity_tendency.F90:123-124)
+      if constexpr (BT) {  // btot per parcel, once (vorticity_tendency.F90:123-124)
 #pragma unroll
         for (int j = 0; j < BATCH / 32; ++j) {
           const int p = lane + 32 * j;
           if (p >= nb) continue;
-          double* D = S + p + (p >> 4) + (4 + NQ - 1) * SPAD;
-          const double bb = D[0], hh = D[SPAD], zz = D[2 * SPAD];
+          R* D = S + p + (p >> 4) + (4 + NQ - 1) * SPAD;
+          const R bb = D[0], hh = D[SPAD], zz = D[2 * SPAD];
           D[0] = bb + 12.5 * fmax(0.0, hh - exp(-zz));
         }
         __syncwarp();
       }
       const int lo = max(s_me, b0) - b0, hi = min(e_me, b0 + nb) - b0;
       for (int p = lo; p < hi; ++p) {
-        const double* D = S + p + (p >> 4);
-        const double delx = D[0], dely = D[SPAD], delz = D[2 * SPAD], vv = D[3 * SPAD];
+        const R* D = S + p + (p >> 4);
+        const R delx = D[0], dely = D[SPAD], delz = D[2 * SPAD], vv = D[3 * SPAD];
         if (MODE == 1 && vv < a.vmin) continue;  // parcel_mixing.F90:488
         if (MODE == 2 && !(vv < a.vmin)) continue;
         if (MODE == 1) ++nkept;
         // parcel_interpolation.F90:390-434: w = (1-delz)(1-dely)(1-delx) v etc.,
         // evaluated left to right as there
-        const double ez = cz ? delz : 1 - delz;
-        const double zy0 = ez * (1 - dely), zy1 = ez * dely;
-        double w[4];
-        w[0] = zy0 * (1 - delx) * vv;
+        const R ez = cz ? delz : R(1) - delz;
+        const R zy0 = ez * (R(1) - dely), zy1 = ez * dely;
+        R w[4];
+        w[0] = zy0 * (R(1) - delx) * vv;
         w[1] = zy0 * delx * vv;
-        w[2] = zy1 * (1 - delx) * vv;
+        w[2] = zy1 * (R(1) - delx) * vv;
         w[3] = zy1 * delx * vv;
-        double fv[NA];
+        R fv[NA];
         if (MODE == 0) {
 #pragma unroll
           for (int q = 0; q < NQ; ++q) fv[q] = D[(4 + q) * SPAD];
@@ -382,13 +416,13 @@ __global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, 
     for (int ab = 0; ab < 4; ++ab)
 #pragma unroll
       for (int q = 0; q < NA; ++q) {
-        const double o = __shfl_down_sync(FULL, acc[ab][q], 1);
+        const R o = __shfl_down_sync(FULL, acc[ab][q], 1);
         if ((lane & 1) && kk + 1 < nk) acc[ab][q] = acc[ab][q] + o;
       }
     if (it >= 0) {
       // grid point x = cx: x-high corners of column cx-1, then x-low corners of column cx
       if (owner) {
-        double* dst = out_row + (size_t)cx * Lay::RPS + lev;
+        R* dst = out_row + (size_t)cx * Lay::RPS + lev;
 #pragma unroll
         for (int b = 0; b < 2; ++b)
 #pragma unroll
@@ -405,14 +439,14 @@ __global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, 
 
 // per grid point: the y-high part of row y-1 plus the y-low part of row y; on
 // the bottom level of a chunk the chunk below's top level comes first
-template <int NQ, int MODE>
-__global__ void __launch_bounds__(256) k_p2g_combine(Geom g, int nzc, const double* __restrict__ rowpart,
-                                                    P2GArgs<NQ> a) {
+template <int NQ, int MODE, class R = double>
+__global__ void __launch_bounds__(256) k_p2g_combine(Geom g, int nzc, const R* __restrict__ rowpart,
+                                                    P2GArgs<NQ, R> a) {
   constexpr int NA = MODE == 0 ? NQ + 1 : NQ;
   constexpr int RPS = 2 * NA * NLV;
   constexpr int TS = NA * NLV + 1;  // odd stride: conflict-free reads by consecutive points
-  __shared__ double T[2][PXB * TS];      // [0]: row y (y-low part), [1]: row y-1 (y-high part)
-  __shared__ double Bz[2][PXB * NA];     // the chunk below's top level, same rows
+  __shared__ R T[2][PXB * TS];      // [0]: row y (y-low part), [1]: row y-1 (y-high part)
+  __shared__ R Bz[2][PXB * NA];     // the chunk below's top level, same rows
   const int px0 = blockIdx.x * PXB, py = blockIdx.y, zc = blockIdx.z;
   const int pym = py == 0 ? g.Ny - 1 : py - 1;
   const int npx = min(PXB, g.Nx - px0);
@@ -440,7 +474,7 @@ __global__ void __launch_bounds__(256) k_p2g_combine(Geom g, int nzc, const doub
   const int nlev = k0 + nk == g.Nz ? nk + 1 : nk;
   for (int e = threadIdx.x; e < nlev * npx; e += blockDim.x) {
     const int L = e / npx, pxl = e - L * npx;
-    double v[NA];
+    R v[NA];
 #pragma unroll
     for (int q = 0; q < NA; ++q) v[q] = T[1][pxl * TS + q * NLV + L] + T[0][pxl * TS + q * NLV + L];
     if (L == 0 && zc > 0) {
@@ -450,14 +484,14 @@ __global__ void __launch_bounds__(256) k_p2g_combine(Geom g, int nzc, const doub
     const int gl = k0 + L;
     const size_t o = ((size_t)gl * g.Ny + py) * g.Nx + px0 + pxl;
     if (MODE == 0) {
-      double wv = v[NQ];
-      if (wv == 0.) wv = 1.;  // parcel_interpolation.F90:466
+      R wv = v[NQ];
+      if (wv == R(0)) wv = R(1);  // parcel_interpolation.F90:466
 #pragma unroll
       for (int q = 0; q < NQ; ++q) a.out[q][o] = v[q] / wv;  // :467
     } else {
       const bool wall = (MODE == 1) && (gl == 0 || gl == g.Nz);
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) a.out[q][o] = wall ? v[q] * 2. : v[q];
+      for (int q = 0; q < NQ; ++q) a.out[q][o] = wall ? v[q] * R(2) : v[q];
     }
   }
 }
@@ -539,7 +573,11 @@ int bin_and_sort(pmpic_ctx* ctx) {
   const int64_t n = ctx->n;
   PMPIC_CUDA(cudaMemsetAsync(ctx->cell_count, 0, sizeof(int32_t) * (g.ncell + 1), ctx->stream));
   PMPIC_CUDA(cudaMemsetAsync(ctx->cell_fill, 0, sizeof(int32_t) * g.ncell, ctx->stream));
-  if (n > 0) {
+  if (n > 0 && ctx->mixed) {
+    k_bin_count_m<<<nblk(n, 256), 256, 0, ctx->stream>>>(g, n, propc(ctx, PMPIC_PROP_X), propc(ctx, PMPIC_PROP_Y),
+                                                         propc(ctx, PMPIC_PROP_Z), ctx->cell, ctx->cell_count,
+                                                         ctx->dinfo); ++ctx->nlaunch;
+  } else if (n > 0) {
     k_bin_count<<<nblk(n, 256), 256, 0, ctx->stream>>>(g, n, prop(ctx, PMPIC_PROP_X), prop(ctx, PMPIC_PROP_Y),
                                                        prop(ctx, PMPIC_PROP_Z), ctx->cell, ctx->del, ctx->cap,
                                                        ctx->cell_count, ctx->dinfo); ++ctx->nlaunch;
@@ -558,20 +596,20 @@ int bin_and_sort(pmpic_ctx* ctx) {
 }
 
 // the two passes of par2grid on `st`; rowpart holds nzc * Ny * Nx records of
-// P2GLayout::RPS doubles
-template <int NQ, int MODE, bool BT>
-static cudaError_t run_p2g(const Geom& g, const int32_t* start, const int32_t* sorted, const double* del,
-                           int64_t cap, const double* vol, const P2GArgs<NQ>& a, double* rowpart, cudaStream_t st) {
+// P2GLayout::RPS values of type R
+template <int NQ, int MODE, bool BT, class R = double>
+static cudaError_t run_p2g(const Geom& g, const int32_t* start, const int32_t* sorted, const R* dx, const R* dy,
+                           const R* dz, int ds, const R* vol, const P2GArgs<NQ, R>& a, R* rowpart, cudaStream_t st) {
   const int nzc = (g.Nz + ZC - 1) / ZC;
   const int nxs = (g.Nx + XSEG - 1) / XSEG;
   const int64_t nw = (int64_t)nxs * g.Ny * nzc;
-  auto rows = k_p2g_rows<NQ, MODE, BT>;
+  auto rows = k_p2g_rows<NQ, MODE, BT, R>;
   cudaError_t e = cudaFuncSetAttribute(rows, cudaFuncAttributePreferredSharedMemoryCarveout,
                                        (int)cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
-  rows<<<nblk(nw, RW), 32 * RW, 0, st>>>(g, nzc, nxs, start, sorted, del, cap, vol, a, rowpart);
+  rows<<<nblk(nw, RW), 32 * RW, 0, st>>>(g, nzc, nxs, start, sorted, dx, dy, dz, ds, vol, a, rowpart);
   dim3 gb((g.Nx + PXB - 1) / PXB, g.Ny, nzc);
-  k_p2g_combine<NQ, MODE><<<gb, 256, 0, st>>>(g, nzc, rowpart, a);
+  k_p2g_combine<NQ, MODE, R><<<gb, 256, 0, st>>>(g, nzc, rowpart, a);
   return cudaGetLastError();
 }
 
@@ -589,10 +627,43 @@ static int launch_p2g(pmpic_ctx* ctx, const double* const* fields, double* const
   a.bh[2] = prop(ctx, PMPIC_PROP_Z);
   a.npercell = ctx->npercell;
   a.vmin = g.vmin;
-  PMPIC_CUDA((run_p2g<NQ, MODE, BT>(g, ctx->cell_start, ctx->sorted, ctx->del, ctx->cap, prop(ctx, PMPIC_PROP_VOL),
-                                    a, ctx->rowpart, ctx->stream)));
+  const double* del = ctx->del;
+  PMPIC_CUDA((run_p2g<NQ, MODE, BT>(g, ctx->cell_start, ctx->sorted, del, del + ctx->cap, del + 2 * ctx->cap, 1,
+                                    prop(ctx, PMPIC_PROP_VOL), a, ctx->rowpart, ctx->stream)));
   ctx->nlaunch += 2;
   return 0;
+}
+
+// the mixed form's par2grid: FP32 fields and accumulation, cell offsets read
+// from the {cell index, offset} positions
+template <int NQ, int MODE>
+static int launch_p2g_m(pmpic_ctx* ctx, const float* const* fields, float* const* out) {
+  TimerScope ts(ctx, T_P2G);
+  const Geom& g = ctx->g;
+  P2GArgs<NQ, float> a{};
+  for (int q = 0; q < NQ; ++q) {
+    a.f[q] = fields[q];
+    a.out[q] = out[q];
+  }
+  a.npercell = ctx->npercell;
+  a.vmin = (double)(float)g.vmin;
+  const float* px = (const float*)prop(ctx, PMPIC_PROP_X) + 1;  // offset halves of the CellOff slots
+  const float* py = (const float*)prop(ctx, PMPIC_PROP_Y) + 1;
+  const float* pz = (const float*)prop(ctx, PMPIC_PROP_Z) + 1;
+  PMPIC_CUDA((run_p2g<NQ, MODE, false, float>(g, ctx->cell_start, ctx->sorted, px, py, pz, 2,
+                                              propf(ctx, PMPIC_PROP_VOL), a, (float*)ctx->rowpart, ctx->stream)));
+  ctx->nlaunch += 2;
+  return 0;
+}
+
+// par2grid of nf FP32 fields on the mixed form (1, 3 or 4 fields)
+int par2grid_multi_m(pmpic_ctx* ctx, const float* const* fields, int nf, float* const* out) {
+  switch (nf) {
+    case 1: return launch_p2g_m<1, 0>(ctx, fields, out);
+    case 3: return launch_p2g_m<3, 0>(ctx, fields, out);
+    case 4: return launch_p2g_m<4, 0>(ctx, fields, out);
+    default: return set_error(ctx, PMPIC_ERR_ARG, "par2grid_multi_m: 1, 3 or 4 fields");
+  }
 }
 
 // bytes of the row-partial buffer of a context
@@ -607,6 +678,21 @@ size_t rowpart_bytes(const Geom& g) {
 // With no parcel in the removed class (any_removed false) its sums are all
 // +0.0, which a memset gives without a pass over the parcels.
 int launch_mix_grids(pmpic_ctx* ctx, bool any_removed) {
+  if (ctx->mixed) {
+    const float* f[6] = {nullptr, propf(ctx, PMPIC_PROP_B), propf(ctx, PMPIC_PROP_H),
+                         propf(ctx, PMPIC_PROP_P), propf(ctx, PMPIC_PROP_Q), propf(ctx, PMPIC_PROP_R)};
+    float* kept[6] = {(float*)ctx->grid[PMPIC_GRID_VOL], (float*)ctx->grid[PMPIC_GRID_B],
+                      (float*)ctx->grid[PMPIC_GRID_HG],  (float*)ctx->grid[PMPIC_GRID_P],
+                      (float*)ctx->grid[PMPIC_GRID_Q],   (float*)ctx->grid[PMPIC_GRID_R]};
+    int rc = launch_p2g_m<6, 1>(ctx, f, kept);
+    if (rc) return rc;
+    float* res[6];
+    for (int q = 0; q < 6; ++q) res[q] = (float*)ctx->mixres[q];
+    if (any_removed) return launch_p2g_m<6, 2>(ctx, f, res);
+    for (int q = 0; q < 6; ++q)
+      PMPIC_CUDA(cudaMemsetAsync(res[q], 0, sizeof(float) * ctx->g.nphys, ctx->stream));
+    return 0;
+  }
   const double* f[6] = {nullptr, prop(ctx, PMPIC_PROP_B), prop(ctx, PMPIC_PROP_H),
                         prop(ctx, PMPIC_PROP_P), prop(ctx, PMPIC_PROP_Q), prop(ctx, PMPIC_PROP_R)};
   double* kept[6] = {ctx->grid[PMPIC_GRID_VOL], ctx->grid[PMPIC_GRID_B], ctx->grid[PMPIC_GRID_HG],
@@ -783,7 +869,8 @@ extern "C" int pmpic_par2grid_static(int32_t nx, int32_t ny, int32_t nz, double 
   P2GArgs<1> a{};
   a.f[0] = field;
   a.out[0] = out;
-  if (run_p2g<1, 0, false>(g, cstart, sorted, del, SP_MAX_PARCELS, vol, a, rows, st) != cudaSuccess)
+  if (run_p2g<1, 0, false>(g, cstart, sorted, del, del + SP_MAX_PARCELS, del + 2 * SP_MAX_PARCELS, 1, vol, a, rows,
+                           st) != cudaSuccess)
     return PMPIC_ERR_CUDA;
   int err = 0;
   if (cudaMemcpyAsync(&err, &info->error, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)

@@ -546,6 +546,418 @@ __global__ void k_backfill(const int32_t* __restrict__ zlist, const int32_t* __r
   }
 }
 
+// ==== mixed-precision form ===========================================================
+// The same components with FP32 fields and {cell index, FP32 offset} positions
+// (CellOff); the integer bookkeeping (directions, lists, slots) is shared with
+// the plain path.  Float property p of parcel n is ((float*)array_p)[n].
+struct MPtrs {
+  CellOff* s[3];
+  CellOff* o[3];
+  CellOff* f[3];
+  float* sv[3];  // p, q, r
+  float* ov[3];
+  float* fv[3];
+  float* d[6];   // dxdt, dydt, dzdt, dpdt, dqdt, drdt
+  const float* grid[6];
+};
+
+// grid2par (parcel_interpolation.F90:299-321) of one FP32 grid at cell (i, j, k), offsets (dx, dy, dz)
+__device__ __forceinline__ float g2p_f(const Geom& g, const float* __restrict__ G, int ci, int cj, int ck,
+                                       float delx, float dely, float delz) {
+  const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
+  const size_t r00 = ((size_t)ck * g.Ny + cj) * g.Nx, r01 = ((size_t)ck * g.Ny + cj1) * g.Nx;
+  const size_t r10 = ((size_t)(ck + 1) * g.Ny + cj) * g.Nx, r11 = ((size_t)(ck + 1) * g.Ny + cj1) * g.Nx;
+  const float c00 = G[r00 + ci] * (1.f - delz) + G[r10 + ci] * delz;
+  const float c01 = G[r00 + ci1] * (1.f - delz) + G[r10 + ci1] * delz;
+  const float c10 = G[r01 + ci] * (1.f - delz) + G[r11 + ci] * delz;
+  const float c11 = G[r01 + ci1] * (1.f - delz) + G[r11 + ci1] * delz;
+  const float c0 = c00 * (1.f - dely) + c10 * dely;
+  const float c1 = c01 * (1.f - dely) + c11 * dely;
+  return c0 * (1.f - delx) + c1 * delx;
+}
+
+__device__ __forceinline__ int classify_dir_m(const Geom& g, int i, int j) {
+  const bool xl = i < 0, xh = i >= g.Nx, yl = j < 0, yh = j >= g.Ny;
+  if (yh && !xl && !xh) return 1;
+  if (yl && !xl && !xh) return 5;
+  if (xh && !yl && !yh) return 3;
+  if (xl && !yl && !yh) return 7;
+  if (xh && yh) return 2;
+  if (xl && yh) return 8;
+  if (xh && yl) return 4;
+  if (xl && yl) return 6;
+  return 0;
+}
+
+// RK4 stage (rk4_integrator.F90:95-319) with the deferred gathers, the z
+// reflection and the direction classification, as k_rk4; position updates in
+// cell units (velocity * dt / cell size), renormalised into [0, 1).
+template <bool GU, bool GP>
+__global__ void k_rk4_m(Geom g, int64_t n, MPtrs P, int stage, const double* __restrict__ dtp,
+                        int8_t* __restrict__ dir) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const double dtd = *dtp;
+  const float dt = (float)dtd, dt6 = (float)(dtd / 6), dt2 = (float)(dtd / 2), dt3 = (float)(dtd / 3);
+  const float inv[3] = {(float)(1.0 / g.dx), (float)(1.0 / g.dy), (float)(1.0 / g.dz)};
+  CellOff sp[3], op[3], fp[3];
+  float sv[3], ov[3], fv[3], d[6];
+  const bool need_s = stage == 1 || GU || GP;
+#pragma unroll
+  for (int v = 0; v < 3; ++v) {
+    if (need_s) sp[v] = P.s[v][t];
+    if (stage == 1) sv[v] = P.sv[v][t];
+    if (stage == 2 || stage == 3) {
+      op[v] = P.o[v][t];
+      ov[v] = P.ov[v][t];
+    }
+    if (stage >= 2) {
+      fp[v] = P.f[v][t];
+      fv[v] = P.fv[v][t];
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < 6; ++v)
+    if ((v < 3 && !GU) || (v >= 3 && !GP)) d[v] = P.d[v][t];
+  bool gathered = false;
+  if (GU || GP) {
+    const int ci = sp[0].i, cj = sp[1].i, ck = sp[2].i;
+    // a position outside the grid was reported by the binning; it gathers nothing
+    gathered = ci >= 0 && ci < g.Nx && cj >= 0 && cj < g.Ny && ck >= 0 && ck < g.Nz;
+#pragma unroll
+    for (int v = 0; v < 6; ++v) {
+      if ((v < 3 && !GU) || (v >= 3 && !GP)) continue;
+      d[v] = gathered ? g2p_f(g, P.grid[v], ci, cj, ck, sp[0].f, sp[1].f, sp[2].f) : P.d[v][t];
+    }
+  }
+  CellOff sn[3];
+  float svn[3];
+#pragma unroll
+  for (int v = 0; v < 3; ++v) {
+    const float dc = d[v] * inv[v];  // cell units per unit time
+    const float dw = d[v + 3];
+    if (stage == 1) {
+      op[v] = sp[v];
+      ov[v] = sv[v];
+      fp[v] = co_add(sp[v], dt6 * dc);
+      fv[v] = sv[v] + dt6 * dw;
+      sn[v] = co_add(sp[v], dt2 * dc);
+      svn[v] = sv[v] + dt2 * dw;
+    } else if (stage == 2) {
+      fp[v] = co_add(fp[v], dt3 * dc);
+      fv[v] = fv[v] + dt3 * dw;
+      sn[v] = co_add(op[v], dt2 * dc);
+      svn[v] = ov[v] + dt2 * dw;
+    } else if (stage == 3) {
+      fp[v] = co_add(fp[v], dt3 * dc);
+      fv[v] = fv[v] + dt3 * dw;
+      sn[v] = co_add(op[v], dt * dc);
+      svn[v] = ov[v] + dt * dw;
+    } else {
+      fp[v] = co_add(fp[v], dt6 * dc);
+      fv[v] = fv[v] + dt6 * dw;
+      sn[v] = fp[v];
+      svn[v] = fv[v];
+    }
+  }
+  sn[2] = co_reflect(sn[2], g.Nz);
+#pragma unroll
+  for (int v = 0; v < 6; ++v)
+    if (gathered && ((v < 3 && GU) || (v >= 3 && GP))) P.d[v][t] = d[v];
+#pragma unroll
+  for (int v = 0; v < 3; ++v) {
+    if (stage == 1) {
+      P.o[v][t] = op[v];
+      P.ov[v][t] = ov[v];
+    }
+    P.f[v][t] = fp[v];
+    P.fv[v][t] = fv[v];
+    P.s[v][t] = sn[v];
+    P.sv[v][t] = svn[v];
+  }
+  dir[t] = (int8_t)classify_dir_m(g, sn[0].i, sn[1].i);
+}
+
+__global__ void k_reflect_classify_m(Geom g, int64_t n, const CellOff* __restrict__ X, const CellOff* __restrict__ Y,
+                                     CellOff* __restrict__ Z, int8_t* __restrict__ dir) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Z[i] = co_reflect(Z[i], g.Nz);
+  dir[i] = (int8_t)classify_dir_m(g, X[i].i, Y[i].i);
+}
+
+// the haloswap staging of the mixed form: each property as its 8-byte slot or
+// its 4-byte value, positions shifted by whole periods (haloswap.F90:531-559)
+__global__ void k_swap_gather_m(Geom g, const int32_t* __restrict__ nmov, const int32_t* __restrict__ M,
+                                const int8_t* __restrict__ dir, const double* __restrict__ parcels, int64_t cap,
+                                double* __restrict__ buf) {
+  const int nm = *nmov;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)nm * 29;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int t = (int)(e / 29), q = (int)(e - (int64_t)t * 29);
+    const int src = M[t];
+    const int pid = c_swap_props[q];
+    const double* A = parcels + (size_t)pid * cap;
+    if (mixed_elem_bytes(pid) == 4) {
+      buf[e] = (double)((const float*)A)[src];  // exact widening
+      continue;
+    }
+    double v = A[src];
+    const int d = dir[src];
+    int sx = 0, sy = 0;
+    if (d == 3 || d == 2 || d == 4) sx = -g.Nx;
+    else if (d == 7 || d == 8 || d == 6) sx = g.Nx;
+    if (d == 1 || d == 2 || d == 8) sy = -g.Ny;
+    else if (d == 5 || d == 6 || d == 4) sy = g.Ny;
+    if (pid == PMPIC_PROP_X || pid == PMPIC_PROP_XO || pid == PMPIC_PROP_XF || pid == PMPIC_PROP_Y ||
+        pid == PMPIC_PROP_YO || pid == PMPIC_PROP_YF) {
+      CellOff c = *(const CellOff*)&v;
+      c.i += (pid == PMPIC_PROP_X || pid == PMPIC_PROP_XO || pid == PMPIC_PROP_XF) ? sx : sy;
+      v = *(const double*)&c;
+    }
+    buf[e] = v;
+  }
+}
+__global__ void k_swap_scatter_m(const int32_t* __restrict__ nmov, const int32_t* __restrict__ V,
+                                 const double* __restrict__ buf, double* __restrict__ parcels, int64_t cap) {
+  const int nm = *nmov;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)nm * 29;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int t = (int)(e / 29), q = (int)(e - (int64_t)t * 29);
+    const int pid = c_swap_props[q];
+    double* A = parcels + (size_t)pid * cap;
+    if (mixed_elem_bytes(pid) == 4) ((float*)A)[V[t]] = (float)buf[e];
+    else A[V[t]] = buf[e];
+  }
+}
+
+// splitting (parcel_splitting.F90:64-133) in FP32
+__global__ void k_split_flag_m(int64_t n, double* __restrict__ parcels, int64_t cap, const double* __restrict__ dtp,
+                               int32_t* __restrict__ flag) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float dt = (float)*dtp;
+  auto F = [&](int pid) { return (float*)(parcels + (size_t)pid * cap); };
+  float ds = F(PMPIC_PROP_P)[i] * F(PMPIC_PROP_DPDT)[i] + F(PMPIC_PROP_Q)[i] * F(PMPIC_PROP_DQDT)[i] +
+             F(PMPIC_PROP_R)[i] * F(PMPIC_PROP_DRDT)[i];
+  ds = powf(fabsf(ds), 1.f / 3.f);
+  const float s = F(PMPIC_PROP_STRETCH)[i] + ds * dt;
+  F(PMPIC_PROP_STRETCH)[i] = s;
+  flag[i] = s > 4.f ? 1 : 0;
+}
+__global__ void k_split_apply_m(Geom g, int64_t n, const int32_t* __restrict__ list, const int32_t* __restrict__ nsplit,
+                                double* __restrict__ parcels, int64_t cap, DevInfo* info) {
+  const int ns = *nsplit;
+  const float pi = 3.14159265358979f;
+  const float inv[3] = {(float)(1.0 / g.dx), (float)(1.0 / g.dy), (float)(1.0 / g.dz)};
+  const int fprops[11] = {PMPIC_PROP_P,    PMPIC_PROP_Q,    PMPIC_PROP_R,    PMPIC_PROP_DXDT,
+                          PMPIC_PROP_DYDT, PMPIC_PROP_DZDT, PMPIC_PROP_DPDT, PMPIC_PROP_DQDT,
+                          PMPIC_PROP_DRDT, PMPIC_PROP_H,    PMPIC_PROP_B};
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ns; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = list[t];
+    const int64_t c = n + t;  // child slot: appended in index order (:94)
+    if (c >= cap) {
+      atomicCAS(&info->error, 0, PMPIC_ERR_CAPACITY);
+      continue;
+    }
+    auto F = [&](int pid) { return (float*)(parcels + (size_t)pid * cap); };
+    auto C = [&](int pid) { return (CellOff*)(parcels + (size_t)pid * cap); };
+    const float vol = F(PMPIC_PROP_VOL)[i];
+    const float r = powf(vol / 4.f / pi, 1.f / 3.f);  // :78-79
+    const float pp = F(PMPIC_PROP_P)[i], qq = F(PMPIC_PROP_Q)[i], rr = F(PMPIC_PROP_R)[i];
+    const float absw = sqrtf(pp * pp + qq * qq + rr * rr);
+    const float w[3] = {pp / absw, qq / absw, rr / absw};
+    const int pos[3] = {PMPIC_PROP_X, PMPIC_PROP_Y, PMPIC_PROP_Z};
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+      const CellOff x = C(pos[v])[i];
+      const float sh = r * w[v] * inv[v];
+      C(pos[v])[c] = co_add(x, sh);  // :95-118
+      C(pos[v])[i] = co_add(x, -sh);  // :121-127
+    }
+#pragma unroll
+    for (int q = 0; q < 11; ++q) F(fprops[q])[c] = F(fprops[q])[i];
+    F(PMPIC_PROP_VOL)[c] = vol / 2;
+    F(PMPIC_PROP_STRETCH)[c] = 0.f;
+    parcels[(size_t)PMPIC_PROP_TAG * cap + c] = parcels[(size_t)PMPIC_PROP_TAG * cap + i];
+    F(PMPIC_PROP_VOL)[i] = vol / 2;
+    F(PMPIC_PROP_STRETCH)[i] = 0.f;
+  }
+}
+
+// btot (vorticity_tendency.F90:121-126) in FP32, z from the cell position
+__global__ void k_btot_m(Geom g, int64_t n, const float* __restrict__ B, const float* __restrict__ H,
+                         const CellOff* __restrict__ Z, float* __restrict__ BT) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const CellOff z = Z[i];
+  const float zz = ((float)z.i + z.f) * (float)g.dz;
+  BT[i] = B[i] + 12.5f * fmaxf(0.f, H[i] - expf(-zz));
+}
+
+// mixing (parcel_mixing.F90:68-431) in FP32
+__global__ void k_keep_m(int64_t n, const float* __restrict__ VOL, float vmin, int32_t* __restrict__ keep) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  keep[i] = VOL[i] < vmin ? 0 : 1;
+}
+__global__ void k_new_parcels_m(Geom g, const int32_t* __restrict__ olist, const int32_t* __restrict__ nnew,
+                                const int32_t* __restrict__ zlist, const int32_t* __restrict__ nzero, int64_t norig,
+                                int64_t cap, int32_t* __restrict__ keep, double* __restrict__ parcels,
+                                const float* __restrict__ KV, const float* __restrict__ KB,
+                                const float* __restrict__ KH, const float* __restrict__ KP,
+                                const float* __restrict__ KQ, const float* __restrict__ KR,
+                                int32_t* __restrict__ newslot, float* __restrict__ portion, float vmin,
+                                DevInfo* info) {
+  const int na = *nnew, nz0 = *nzero;
+  for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < na; a += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t o = olist[a];
+    const int k = (int)(o % g.Nz);
+    const int j = (int)((o / g.Nz) % g.Ny);
+    const int i = (int)(o / ((int64_t)g.Nz * g.Ny));
+    const int64_t slot = a < nz0 ? (int64_t)zlist[a] : norig + (a - nz0);
+    if (slot + 2 > cap) {
+      atomicCAS(&info->error, 0, PMPIC_ERR_CAPACITY);
+      continue;
+    }
+    const int i1 = i + 1 == g.Nx ? 0 : i + 1, j1 = j + 1 == g.Ny ? 0 : j + 1;
+    const size_t q[8] = {((size_t)k * g.Ny + j) * g.Nx + i,   ((size_t)(k + 1) * g.Ny + j) * g.Nx + i,
+                         ((size_t)k * g.Ny + j1) * g.Nx + i,  ((size_t)(k + 1) * g.Ny + j1) * g.Nx + i,
+                         ((size_t)k * g.Ny + j) * g.Nx + i1,  ((size_t)(k + 1) * g.Ny + j) * g.Nx + i1,
+                         ((size_t)k * g.Ny + j1) * g.Nx + i1, ((size_t)(k + 1) * g.Ny + j1) * g.Nx + i1};
+    auto box = [&](const float* G) {
+      float s = 0.f;
+#pragma unroll
+      for (int u = 0; u < 8; ++u) s = s + G[q[u]];
+      return s;
+    };
+    const float v = box(KV);
+    const float por = 2.f * vmin / v;
+    auto F = [&](int pid) { return (float*)(parcels + (size_t)pid * cap); };
+    auto C = [&](int pid) { return (CellOff*)(parcels + (size_t)pid * cap); };
+    C(PMPIC_PROP_X)[slot] = CellOff{i, 0.5f};  // the cell centre
+    C(PMPIC_PROP_Y)[slot] = CellOff{j, 0.5f};
+    C(PMPIC_PROP_Z)[slot] = CellOff{k, 0.5f};
+    F(PMPIC_PROP_VOL)[slot] = 2.f * vmin;
+    F(PMPIC_PROP_STRETCH)[slot] = 0.f;
+    F(PMPIC_PROP_B)[slot] = box(KB) / v;
+    F(PMPIC_PROP_H)[slot] = box(KH) / v;
+    F(PMPIC_PROP_P)[slot] = box(KP) / v;
+    F(PMPIC_PROP_Q)[slot] = box(KQ) / v;
+    F(PMPIC_PROP_R)[slot] = box(KR) / v;
+    if (slot + 1 < norig) keep[slot] = 2;
+    const int64_t cell = ((int64_t)k * g.Ny + j) * g.Nx + i;
+    newslot[cell] = (int32_t)slot;
+    portion[cell] = por;
+  }
+}
+struct ResPtrsF {
+  float* r[6];
+  const float* k[6];
+};
+__global__ void k_residual_update_m(Geom g, ResPtrsF RP, const int32_t* __restrict__ newslot,
+                                    const float* __restrict__ portion) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= g.nphys) return;
+  const int i = (int)(e % g.Nx);
+  const int j = (int)((e / g.Nx) % g.Ny);
+  const int k = (int)(e / ((int64_t)g.Nx * g.Ny));
+  const int im = i == 0 ? g.Nx - 1 : i - 1, jm = j == 0 ? g.Ny - 1 : j - 1;
+  float por[8];
+  int np = 0;
+  const int cis[2] = {im, i}, cjs[2] = {jm, j};
+  for (int a = 0; a < 2; ++a)
+    for (int b = 0; b < 2; ++b)
+      for (int c = 0; c < 2; ++c) {
+        const int ck = k - 1 + c;
+        if (ck < 0 || ck >= g.Nz) continue;
+        const int64_t cell = ((int64_t)ck * g.Ny + cjs[b]) * g.Nx + cis[a];
+        if (newslot[cell] >= 0) por[np++] = portion[cell];
+      }
+  const bool wall = (k == 0 || k == g.Nz);
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    float r = RP.r[q][e];
+    const float kv = RP.k[q][e];
+    for (int u = 0; u < np; ++u) r = r - por[u] * kv;
+    if (wall) r = r * 2.f;
+    RP.r[q][e] = r;
+  }
+}
+__global__ void __launch_bounds__(256, 4) k_redistribute_m(Geom g, int64_t norig, const int32_t* __restrict__ keep,
+                                                          double* __restrict__ parcels, int64_t cap, ResPtrsF RP) {
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= norig || keep[m] != 1) return;
+  auto F = [&](int pid) { return (float*)(parcels + (size_t)pid * cap); };
+  auto C = [&](int pid) { return (CellOff*)(parcels + (size_t)pid * cap); };
+  const CellOff px = C(PMPIC_PROP_X)[m], py = C(PMPIC_PROP_Y)[m], pz = C(PMPIC_PROP_Z)[m];
+  const int ci = px.i, cj = py.i, ck = pz.i;
+  if (ci < 0 || ci >= g.Nx || cj < 0 || cj >= g.Ny || ck < 0 || ck >= g.Nz) return;  // reported by the binning
+  const float delx = px.f, dely = py.f, delz = pz.f;
+  const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
+  const int r0 = (ck * g.Ny + cj) * g.Nx, r1 = (ck * g.Ny + cj1) * g.Nx;
+  const int r2 = ((ck + 1) * g.Ny + cj) * g.Nx, r3 = ((ck + 1) * g.Ny + cj1) * g.Nx;
+  const int c[8] = {r0 + ci, r0 + ci1, r1 + ci, r1 + ci1, r2 + ci, r2 + ci1, r3 + ci, r3 + ci1};
+  const float v = F(PMPIC_PROP_VOL)[m];
+  float w[8];
+  w[0] = (1.f - delz) * (1.f - dely) * (1.f - delx) * v;
+  w[1] = (1.f - delz) * (1.f - dely) * (delx) * v;
+  w[2] = (1.f - delz) * (dely) * (1.f - delx) * v;
+  w[3] = (1.f - delz) * (dely) * (delx) * v;
+  w[4] = (delz) * (1.f - dely) * (1.f - delx) * v;
+  w[5] = (delz) * (1.f - dely) * (delx) * v;
+  w[6] = (delz) * (dely) * (1.f - delx) * v;
+  w[7] = (delz) * (dely) * (delx) * v;
+  float wv[8];
+  float nv = v;
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    wv[u] = w[u] / RP.k[0][c[u]];
+    nv = nv + wv[u] * RP.r[0][c[u]];  // :268-276
+  }
+  const int pids[5] = {PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
+  const float rnv = 1.f / nv;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    const float* res = RP.r[q + 1];
+    float s = F(pids[q])[m] * v;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) s = s + wv[u] * res[c[u]];  // :279-336
+    F(pids[q])[m] = s * rnv;
+  }
+  F(PMPIC_PROP_VOL)[m] = nv;
+}
+__global__ void k_backfill_m(const int32_t* __restrict__ zlist, const int32_t* __restrict__ nz,
+                             const int32_t* __restrict__ olist, const int32_t* __restrict__ no,
+                             double* __restrict__ parcels, int64_t cap, DevInfo* info) {
+  const int nzero = *nz, nones = *no;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && nzero > nones) atomicCAS(&info->error, 0, PMPIC_ERR_BACKFILL);
+  const int pids[11] = {PMPIC_PROP_X, PMPIC_PROP_Y, PMPIC_PROP_Z, PMPIC_PROP_P,   PMPIC_PROP_Q,      PMPIC_PROP_R,
+                        PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_VOL, PMPIC_PROP_TAG, PMPIC_PROP_STRETCH};
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)nzero * 11;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int t = (int)(e / 11), q = (int)(e - (int64_t)t * 11);
+    if (t >= nones) continue;
+    const int dst = zlist[t], src = olist[nones - 1 - t];
+    double* A = parcels + (size_t)pids[q] * cap;
+    if (mixed_elem_bytes(pids[q]) == 4) ((float*)A)[dst] = ((const float*)A)[src];
+    else A[dst] = A[src];
+  }
+}
+// grid2par of three FP32 grids into three float properties at the current positions
+__global__ void k_grid2par_m(Geom g, int64_t n, const CellOff* __restrict__ X, const CellOff* __restrict__ Y,
+                             const CellOff* __restrict__ Z, const float* __restrict__ G0, const float* __restrict__ G1,
+                             const float* __restrict__ G2, float* __restrict__ O0, float* __restrict__ O1,
+                             float* __restrict__ O2) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const CellOff x = X[t], y = Y[t], z = Z[t];
+  if (x.i < 0 || x.i >= g.Nx || y.i < 0 || y.i >= g.Ny || z.i < 0 || z.i >= g.Nz) return;  // reported by the binning
+  O0[t] = g2p_f(g, G0, x.i, y.i, z.i, x.f, y.f, z.f);
+  O1[t] = g2p_f(g, G1, x.i, y.i, z.i, x.f, y.f, z.f);
+  O2[t] = g2p_f(g, G2, x.i, y.i, z.i, x.f, y.f, z.f);
+}
+
 }  // namespace
 
 // list of i in [0,n) with pred(i), ascending; count written to *dcount (device)
@@ -575,6 +987,25 @@ static int32_t* dcounter(pmpic_ctx* ctx, int i) { return (int32_t*)(ctx->dinfo +
 // tendencies; the cached binning is valid while they are pending.
 int flush_gathers(pmpic_ctx* ctx) {
   int rc = 0;
+  if (ctx->mixed) {  // gathers at the current {cell, offset} positions; no binning needed
+    float* const* G = (float* const*)ctx->grid;
+    const int64_t n = ctx->n;
+    if (ctx->pending_uvw && n > 0) {
+      k_grid2par_m<<<nblk(n, 256), 256, 0, ctx->stream>>>(
+          ctx->g, n, propc(ctx, PMPIC_PROP_X), propc(ctx, PMPIC_PROP_Y), propc(ctx, PMPIC_PROP_Z), G[PMPIC_GRID_U],
+          G[PMPIC_GRID_V], G[PMPIC_GRID_W], propf(ctx, PMPIC_PROP_DXDT), propf(ctx, PMPIC_PROP_DYDT),
+          propf(ctx, PMPIC_PROP_DZDT)); ++ctx->nlaunch;
+    }
+    if (ctx->pending_pqr && n > 0) {
+      k_grid2par_m<<<nblk(n, 256), 256, 0, ctx->stream>>>(
+          ctx->g, n, propc(ctx, PMPIC_PROP_X), propc(ctx, PMPIC_PROP_Y), propc(ctx, PMPIC_PROP_Z), G[PMPIC_GRID_DP],
+          G[PMPIC_GRID_DQ], G[PMPIC_GRID_DR], propf(ctx, PMPIC_PROP_DPDT), propf(ctx, PMPIC_PROP_DQDT),
+          propf(ctx, PMPIC_PROP_DRDT)); ++ctx->nlaunch;
+    }
+    ctx->pending_uvw = ctx->pending_pqr = false;
+    PMPIC_CUDA(cudaGetLastError());
+    return 0;
+  }
   if (ctx->pending_uvw) {
     ctx->pending_uvw = false;
     const double* gr[3] = {ctx->grid[PMPIC_GRID_U], ctx->grid[PMPIC_GRID_V], ctx->grid[PMPIC_GRID_W]};
@@ -592,6 +1023,13 @@ int flush_gathers(pmpic_ctx* ctx) {
 
 int compute_btot(pmpic_ctx* ctx) {
   if (ctx->n == 0) return 0;
+  if (ctx->mixed) {
+    k_btot_m<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, propf(ctx, PMPIC_PROP_B),
+                                                         propf(ctx, PMPIC_PROP_H), propc(ctx, PMPIC_PROP_Z),
+                                                         propf(ctx, PMPIC_PROP_BTOT)); ++ctx->nlaunch;
+    PMPIC_CUDA(cudaGetLastError());
+    return 0;
+  }
   k_btot<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->n, prop(ctx, PMPIC_PROP_B), prop(ctx, PMPIC_PROP_H),
                                                      prop(ctx, PMPIC_PROP_Z), prop(ctx, PMPIC_PROP_BTOT)); ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
@@ -601,6 +1039,35 @@ int compute_btot(pmpic_ctx* ctx) {
 int rk4_stage(pmpic_ctx* ctx, int stage) {
   if (ctx->n == 0) {
     ctx->pending_uvw = ctx->pending_pqr = false;
+    return 0;
+  }
+  if (ctx->mixed) {
+    MPtrs P;
+    const int S[6] = {PMPIC_PROP_X, PMPIC_PROP_Y, PMPIC_PROP_Z, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
+    const int O[6] = {PMPIC_PROP_XO, PMPIC_PROP_YO, PMPIC_PROP_ZO, PMPIC_PROP_PO, PMPIC_PROP_QO, PMPIC_PROP_RO};
+    const int F[6] = {PMPIC_PROP_XF, PMPIC_PROP_YF, PMPIC_PROP_ZF, PMPIC_PROP_PF, PMPIC_PROP_QF, PMPIC_PROP_RF};
+    const int D[6] = {PMPIC_PROP_DXDT, PMPIC_PROP_DYDT, PMPIC_PROP_DZDT, PMPIC_PROP_DPDT, PMPIC_PROP_DQDT, PMPIC_PROP_DRDT};
+    const int G[6] = {PMPIC_GRID_U, PMPIC_GRID_V, PMPIC_GRID_W, PMPIC_GRID_DP, PMPIC_GRID_DQ, PMPIC_GRID_DR};
+    for (int v = 0; v < 3; ++v) {
+      P.s[v] = propc(ctx, S[v]);
+      P.o[v] = propc(ctx, O[v]);
+      P.f[v] = propc(ctx, F[v]);
+      P.sv[v] = propf(ctx, S[v + 3]);
+      P.ov[v] = propf(ctx, O[v + 3]);
+      P.fv[v] = propf(ctx, F[v + 3]);
+    }
+    for (int v = 0; v < 6; ++v) {
+      P.d[v] = propf(ctx, D[v]);
+      P.grid[v] = (const float*)ctx->grid[G[v]];
+    }
+    const bool gu = ctx->pending_uvw, gp = ctx->pending_pqr;
+    auto kern = gu ? (gp ? k_rk4_m<true, true> : k_rk4_m<true, false>) : (gp ? k_rk4_m<false, true> : k_rk4_m<false, false>);
+    kern<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, P, stage, &ctx->dinfo->dtm, ctx->dir); ++ctx->nlaunch;
+    ctx->pending_uvw = ctx->pending_pqr = false;
+    ctx->dir_ready = true;
+    ctx->sorted_valid = false;
+    ctx->btot_grid_ready = false;
+    PMPIC_CUDA(cudaGetLastError());
     return 0;
   }
   RkPtrs P;
@@ -641,7 +1108,11 @@ int parcel_haloswap(pmpic_ctx* ctx) {
   const bool ready = ctx->dir_ready;
   ctx->dir_ready = false;
   if (n == 0) return 0;
-  if (!ready) {
+  if (!ready && ctx->mixed) {
+    k_reflect_classify_m<<<nblk(n, 256), 256, 0, ctx->stream>>>(ctx->g, n, propc(ctx, PMPIC_PROP_X),
+                                                                propc(ctx, PMPIC_PROP_Y), propc(ctx, PMPIC_PROP_Z),
+                                                                ctx->dir); ++ctx->nlaunch;
+  } else if (!ready) {
     k_reflect_classify<<<nblk(n, 256), 256, 0, ctx->stream>>>(ctx->g, n, prop(ctx, PMPIC_PROP_X),
                                                               prop(ctx, PMPIC_PROP_Y), prop(ctx, PMPIC_PROP_Z),
                                                               ctx->dir); ++ctx->nlaunch;
@@ -656,8 +1127,13 @@ int parcel_haloswap(pmpic_ctx* ctx) {
   // reports PMPIC_ERR_CAPACITY
   int32_t* nmc = dcounter(ctx, 1);
   k_check_swapcap<<<1, 1, 0, ctx->stream>>>(nm, nmc, ctx->swapcap, ctx->dinfo); ++ctx->nlaunch;
-  k_swap_gather<<<592, 256, 0, ctx->stream>>>(ctx->g, nmc, M, ctx->dir, ctx->parcels, ctx->cap, ctx->swapbuf); ++ctx->nlaunch;
-  k_swap_scatter<<<592, 256, 0, ctx->stream>>>(nmc, V, ctx->swapbuf, ctx->parcels, ctx->cap); ++ctx->nlaunch;
+  if (ctx->mixed) {
+    k_swap_gather_m<<<592, 256, 0, ctx->stream>>>(ctx->g, nmc, M, ctx->dir, ctx->parcels, ctx->cap, ctx->swapbuf); ++ctx->nlaunch;
+    k_swap_scatter_m<<<592, 256, 0, ctx->stream>>>(nmc, V, ctx->swapbuf, ctx->parcels, ctx->cap); ++ctx->nlaunch;
+  } else {
+    k_swap_gather<<<592, 256, 0, ctx->stream>>>(ctx->g, nmc, M, ctx->dir, ctx->parcels, ctx->cap, ctx->swapbuf); ++ctx->nlaunch;
+    k_swap_scatter<<<592, 256, 0, ctx->stream>>>(nmc, V, ctx->swapbuf, ctx->parcels, ctx->cap); ++ctx->nlaunch;
+  }
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
@@ -670,10 +1146,18 @@ int splitting(pmpic_ctx* ctx) {
   int32_t* list = ctx->keep;
   int32_t* ns = dcounter(ctx, 2);
   if (n > 0) {
-    k_split_flag<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, ctx->parcels, ctx->cap, &ctx->dinfo->dtm, flag); ++ctx->nlaunch;
+    if (ctx->mixed)
+      k_split_flag_m<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, ctx->parcels, ctx->cap, &ctx->dinfo->dtm, flag);
+    else
+      k_split_flag<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, ctx->parcels, ctx->cap, &ctx->dinfo->dtm, flag);
+    ++ctx->nlaunch;
     int rc = compact(ctx, PredFlag{flag}, n, list, ns);
     if (rc) return rc;
-    k_split_apply<<<592, 256, 0, ctx->stream>>>(n, list, ns, ctx->parcels, ctx->cap, ctx->dinfo); ++ctx->nlaunch;
+    if (ctx->mixed)
+      k_split_apply_m<<<592, 256, 0, ctx->stream>>>(ctx->g, n, list, ns, ctx->parcels, ctx->cap, ctx->dinfo);
+    else
+      k_split_apply<<<592, 256, 0, ctx->stream>>>(n, list, ns, ctx->parcels, ctx->cap, ctx->dinfo);
+    ++ctx->nlaunch;
   } else {
     PMPIC_CUDA(cudaMemsetAsync(ns, 0, sizeof(int32_t), ctx->stream));
   }
@@ -694,7 +1178,9 @@ int mixing(pmpic_ctx* ctx) {
   const int64_t norig = ctx->n;
   int rc;
   // keep flags (:488) and the kept / residual grids (construct_grids :440-624)
-  if (norig > 0) {
+  if (norig > 0 && ctx->mixed) {
+    k_keep_m<<<nblk(norig, 256), 256, 0, ctx->stream>>>(norig, propf(ctx, PMPIC_PROP_VOL), (float)g.vmin, ctx->keep); ++ctx->nlaunch;
+  } else if (norig > 0) {
     k_keep<<<nblk(norig, 256), 256, 0, ctx->stream>>>(norig, prop(ctx, PMPIC_PROP_VOL), g.vmin, ctx->keep); ++ctx->nlaunch;
   }
   if ((rc = bin_and_sort(ctx))) return rc;
@@ -714,18 +1200,37 @@ int mixing(pmpic_ctx* ctx) {
   PMPIC_CUDA(cudaMemsetAsync(ctx->newslot, 0xff, sizeof(int32_t) * g.ncell, ctx->stream));
   double* K[6] = {ctx->grid[PMPIC_GRID_VOL], ctx->grid[PMPIC_GRID_B], ctx->grid[PMPIC_GRID_HG],
                   ctx->grid[PMPIC_GRID_P],   ctx->grid[PMPIC_GRID_Q], ctx->grid[PMPIC_GRID_R]};
-  k_new_parcels<<<592, 256, 0, ctx->stream>>>(g, olist, nnew, zlist, nz0, norig, ctx->cap, ctx->keep, ctx->parcels,
-                                              K[0], K[1], K[2], K[3], K[4], K[5], ctx->newslot, ctx->newportion,
-                                              ctx->dinfo); ++ctx->nlaunch;
-  ResPtrs RP;
-  for (int q = 0; q < 6; ++q) {
-    RP.r[q] = ctx->mixres[q];
-    RP.k[q] = K[q];
-  }
-  k_residual_update<<<nblk(g.nphys, 256), 256, 0, ctx->stream>>>(g, RP, ctx->newslot, ctx->newportion); ++ctx->nlaunch;
-  if (norig > 0) {
-    k_redistribute<<<nblk(norig, 256), 256, 0, ctx->stream>>>(g, norig, ctx->keep, ctx->parcels, ctx->cap,
-                                                              ctx->cell, ctx->del, RP); ++ctx->nlaunch;
+  if (ctx->mixed) {
+    const float* KF[6];
+    ResPtrsF RF;
+    for (int q = 0; q < 6; ++q) {
+      KF[q] = (const float*)K[q];
+      RF.r[q] = (float*)ctx->mixres[q];
+      RF.k[q] = KF[q];
+    }
+    float* por = (float*)ctx->newportion;
+    k_new_parcels_m<<<592, 256, 0, ctx->stream>>>(g, olist, nnew, zlist, nz0, norig, ctx->cap, ctx->keep, ctx->parcels,
+                                                  KF[0], KF[1], KF[2], KF[3], KF[4], KF[5], ctx->newslot, por,
+                                                  (float)g.vmin, ctx->dinfo); ++ctx->nlaunch;
+    k_residual_update_m<<<nblk(g.nphys, 256), 256, 0, ctx->stream>>>(g, RF, ctx->newslot, por); ++ctx->nlaunch;
+    if (norig > 0) {
+      k_redistribute_m<<<nblk(norig, 256), 256, 0, ctx->stream>>>(g, norig, ctx->keep, ctx->parcels, ctx->cap, RF);
+      ++ctx->nlaunch;
+    }
+  } else {
+    k_new_parcels<<<592, 256, 0, ctx->stream>>>(g, olist, nnew, zlist, nz0, norig, ctx->cap, ctx->keep, ctx->parcels,
+                                                K[0], K[1], K[2], K[3], K[4], K[5], ctx->newslot, ctx->newportion,
+                                                ctx->dinfo); ++ctx->nlaunch;
+    ResPtrs RP;
+    for (int q = 0; q < 6; ++q) {
+      RP.r[q] = ctx->mixres[q];
+      RP.k[q] = K[q];
+    }
+    k_residual_update<<<nblk(g.nphys, 256), 256, 0, ctx->stream>>>(g, RP, ctx->newslot, ctx->newportion); ++ctx->nlaunch;
+    if (norig > 0) {
+      k_redistribute<<<nblk(norig, 256), 256, 0, ctx->stream>>>(g, norig, ctx->keep, ctx->parcels, ctx->cap,
+                                                                ctx->cell, ctx->del, RP); ++ctx->nlaunch;
+    }
   }
   // counts to the host: removed, new cells
   int32_t h[2];
@@ -749,7 +1254,11 @@ int mixing(pmpic_ctx* ctx) {
     int32_t* no = dcounter(ctx, 6);
     if ((rc = compact(ctx, PredKeepEq{ctx->keep, 0}, norig, z2, nz2))) return rc;
     if ((rc = compact(ctx, PredKeepEq{ctx->keep, 1}, norig, ones, no))) return rc;
-    k_backfill<<<592, 256, 0, ctx->stream>>>(z2, nz2, ones, no, ctx->parcels, ctx->cap, ctx->dinfo); ++ctx->nlaunch;
+    if (ctx->mixed)
+      k_backfill_m<<<592, 256, 0, ctx->stream>>>(z2, nz2, ones, no, ctx->parcels, ctx->cap, ctx->dinfo);
+    else
+      k_backfill<<<592, 256, 0, ctx->stream>>>(z2, nz2, ones, no, ctx->parcels, ctx->cap, ctx->dinfo);
+    ++ctx->nlaunch;
     int32_t hz = 0;
     PMPIC_CUDA(cudaMemcpyAsync(&hz, nz2, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
     PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));

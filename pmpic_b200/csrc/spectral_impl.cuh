@@ -1,0 +1,463 @@
+// spectral_impl.cuh -- the semi-spectral operators and the vort2vel /
+// vorticity_tendency grid pipelines of spectral.cu, written once over the
+// scalar type `real` and included by spectral.cu into one namespace per
+// precision (FP64 plain path, FP32 mixed-precision form).  The namespace
+// provides the tables of its precision (tab_kx, tab_ky, tab_k2, tab_filt,
+// tab_diffz) and the zero-mode hooks (zero_mode_prepare, zero_mode_launch).
+// Not a standalone header.
+
+template <class P>
+inline real* RP(P* p) { return reinterpret_cast<real*>(p); }
+
+// ---- elementwise spectral operators --------------------------------------------
+// diffx (fft_ops.F90:266-295): out(i) = -in(i+1) kx, out(i+1) = in(i) kx
+__device__ __forceinline__ real dx_of(const real* in, int64_t e, int ip, const real* kx, int col) {
+  return (ip & 1) == 0 ? (real(-1) * in[e + 1]) * kx[col] : in[e - 1] * kx[col];
+}
+// diffy (fft_ops.F90:366-394)
+__device__ __forceinline__ real dy_of(const real* in, int64_t e, int jp, int sx, const real* ky, int col) {
+  return (jp & 1) == 0 ? (real(-1) * in[e + sx]) * ky[col] : in[e - sx] * ky[col];
+}
+
+struct EwIdx {
+  int64_t e;
+  int col, ip, jp, k;
+};
+__device__ __forceinline__ bool ew_index(const Geom& g, EwIdx& x) {
+  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= g.nspec) return false;
+  int cols = g.sx * g.sy;
+  x.e = e;
+  x.k = (int)(e / cols);
+  x.col = (int)(e - (int64_t)x.k * cols);
+  x.jp = x.col / g.sx;
+  x.ip = x.col - x.jp * g.sx;
+  return true;
+}
+
+__global__ void k_diffx(Geom g, const real* __restrict__ in, real* __restrict__ out, const real* __restrict__ kx) {
+  EwIdx x;
+  if (!ew_index(g, x)) return;
+  out[x.e] = dx_of(in, x.e, x.ip, kx, x.col);
+}
+__global__ void k_diffy(Geom g, const real* __restrict__ in, real* __restrict__ out, const real* __restrict__ ky) {
+  EwIdx x;
+  if (!ew_index(g, x)) return;
+  out[x.e] = dy_of(in, x.e, x.jp, g.sx, ky, x.col);
+}
+__global__ void k_filter(Geom g, const real* __restrict__ in, real* __restrict__ out,
+                         const real* __restrict__ filt) {
+  EwIdx x;
+  if (!ew_index(g, x)) return;
+  out[x.e] = in[x.e] * filt[x.col];
+}
+
+// vort2vel.F90:158-173: f = diffx(a) + diffy(b) + (dc/dz, 2nd order with
+// one-sided ends); f(:,1,1) = 0
+__global__ void k_div(Geom g, const real* __restrict__ a, const real* __restrict__ b,
+                      const real* __restrict__ c, real* __restrict__ f, const real* __restrict__ kx,
+                      const real* __restrict__ ky, real hdzi) {
+  EwIdx x;
+  if (!ew_index(g, x)) return;
+  const int64_t cs = (int64_t)g.sx * g.sy;
+  const int nz = g.nzp;
+  real d = dx_of(a, x.e, x.ip, kx, x.col);
+  real e = dy_of(b, x.e, x.jp, g.sx, ky, x.col);
+  real fz;
+  if (x.k == 0) {
+    fz = hdzi * (real(4) * c[x.e + cs] - c[x.e + 2 * cs] - real(3) * c[x.e]);
+  } else if (x.k == nz - 1) {
+    fz = hdzi * (c[x.e - 2 * cs] + real(3) * c[x.e] - real(4) * c[x.e - cs]);
+  } else {
+    fz = (c[x.e + cs] - c[x.e - cs]) * hdzi;
+  }
+  real v = d + e + fz;
+  if (x.col == 0) v = real(0);
+  f[x.e] = v;
+}
+
+// a = a - diffx(f) (vort2vel.F90:185-188) or b = b - diffy(f) (:191-194)
+__global__ void k_sub_diff(Geom g, real* __restrict__ a, const real* __restrict__ f, const real* __restrict__ kk,
+                           int ydir) {
+  EwIdx x;
+  if (!ew_index(g, x)) return;
+  real d = ydir ? dy_of(f, x.e, x.jp, g.sx, kk, x.col) : dx_of(f, x.e, x.ip, kk, x.col);
+  a[x.e] = a[x.e] - d;
+}
+
+// c = c - d; c(1,:,:) = 0 (vort2vel.F90:197-205)
+__global__ void k_sub_zero0(Geom g, real* __restrict__ c, const real* __restrict__ d) {
+  EwIdx x;
+  if (!ew_index(g, x)) return;
+  real v = c[x.e] - d[x.e];
+  if (x.k == 0) v = real(0);
+  c[x.e] = v;
+}
+
+// d,e,f = filter(a,b,c) and the top/bottom planes of a and b (vort2vel.F90:208-217)
+__global__ void k_filter3_bt(Geom g, const real* __restrict__ a, const real* __restrict__ b,
+                             const real* __restrict__ c, real* __restrict__ d, real* __restrict__ e,
+                             real* __restrict__ f, const real* __restrict__ filt, real* __restrict__ bt) {
+  EwIdx x;
+  if (!ew_index(g, x)) return;
+  real m = filt[x.col];
+  d[x.e] = a[x.e] * m;
+  e[x.e] = b[x.e] * m;
+  f[x.e] = c[x.e] * m;
+  const int cols = g.sx * g.sy;
+  if (x.k == g.nzp - 1) {
+    bt[0 * cols + x.col] = a[x.e];  // atop
+    bt[2 * cols + x.col] = b[x.e];  // btop
+  }
+  if (x.k == 0) {
+    bt[1 * cols + x.col] = a[x.e];  // abot
+    bt[3 * cols + x.col] = b[x.e];  // bbot
+  }
+}
+
+// Velocity components from the potentials (vort2vel.F90:254-315):
+//  mode 0: f = e - diffy(c), f(:,1,1) = ubar, u_s = filter(f)
+//  mode 1: f = diffx(c) - e, f(:,1,1) = vbar, v_s = filter(f)
+//  mode 2: f = diffy(a) - diffx(b),             w_s = filter(f)
+__global__ void k_vel(Geom g, int mode, const real* __restrict__ e, const real* __restrict__ c,
+                      const real* __restrict__ a, const real* __restrict__ b, real* __restrict__ f,
+                      real* __restrict__ fs, const real* __restrict__ kx, const real* __restrict__ ky,
+                      const real* __restrict__ filt, const double* __restrict__ zbar) {
+  EwIdx x;
+  if (!ew_index(g, x)) return;
+  real v;
+  if (mode == 0) {
+    v = e[x.e] - dy_of(c, x.e, x.jp, g.sx, ky, x.col);
+    if (x.col == 0) v = (real)zbar[x.k];
+  } else if (mode == 1) {
+    v = dx_of(c, x.e, x.ip, kx, x.col) - e[x.e];
+    if (x.col == 0) v = (real)zbar[x.k];
+  } else {
+    v = dy_of(a, x.e, x.jp, g.sx, ky, x.col) - dx_of(b, x.e, x.ip, kx, x.col);
+  }
+  f[x.e] = v;
+  fs[x.e] = v * filt[x.col];
+}
+
+// ---- compact z operators ----------------------------------------------------------
+// diffz (fft_ops.F90:419-483).  The tridiagonal coefficients are the same for
+// every column, so the Thomas factors (cp and the denominators) are computed
+// once on the host with the reference's arithmetic and passed in.
+__global__ void k_diffz(Geom g, const real* __restrict__ f, real* __restrict__ out,
+                        const real* __restrict__ coef /* a[nz], den[nz], cp[nz] */, const real* __restrict__ bot,
+                        const real* __restrict__ top, real a1) {
+  int col = blockIdx.x * blockDim.x + threadIdx.x;
+  const int cols = g.sx * g.sy;
+  if (col >= cols) return;
+  const int nz = g.nzp;
+  const int64_t cs = cols;
+  const real* A = coef;
+  const real* DEN = coef + nz;
+  const real* CP = coef + 2 * nz;
+  const real dz = (real)g.dz;
+  const bool bt = bot != nullptr;
+  // forward sweep: f'(1) = d(1)/den(1); f'(i) = (d(i) - a(i) f'(i-1)) / den(i)
+  real fm = f[col], f0 = f[cs + col];
+  real d1 = bt ? f0 / dz - a1 * bot[col] * dz : real(0);
+  real prev = d1 / DEN[0];
+  out[col] = prev;
+  for (int k = 1; k < nz - 1; ++k) {
+    real fp = f[(int64_t)(k + 1) * cs + col];
+    real d = (fp - fm) / real(2) / dz;
+    prev = (d - A[k] * prev) / DEN[k];
+    out[(int64_t)k * cs + col] = prev;
+    fm = f0;
+    f0 = fp;
+  }
+  {
+    int k = nz - 1;
+    real dn = bt ? -fm / dz + a1 * top[col] * dz : real(0);  // fm = f(nz-1)
+    prev = (dn - A[k] * prev) / DEN[k];
+    out[(int64_t)k * cs + col] = prev;
+  }
+  // back substitution: f(i) = f(i) - cp(i+1) f(i+1)
+  real nxt = prev;
+  for (int k = nz - 2; k >= 0; --k) {
+    real v = out[(int64_t)k * cs + col] - CP[k + 1] * nxt;
+    out[(int64_t)k * cs + col] = v;
+    nxt = v;
+  }
+}
+
+// laplinv (fft_ops.F90:505-601), in place, one thread per column; columns with
+// k2 == 0 keep their input (:567).  cp is kept in a scratch array.
+__global__ void k_laplinv(Geom g, real* __restrict__ f, real* __restrict__ cpbuf, const real* __restrict__ k2,
+                          int df0) {
+  int col = blockIdx.x * blockDim.x + threadIdx.x;
+  const int cols = g.sx * g.sy;
+  if (col >= cols) return;
+  const real kk = k2[col];
+  if (kk == 0) return;
+  const int nz = g.nzp;
+  const int64_t cs = cols;
+  const real f16 = (real)f4div(1.f, 6.f), f13 = (real)f4div(1.f, 3.f), f112 = (real)f4div(1.f, 12.f), f56 = (real)f4div(5.f, 6.f);
+  const real dz = (real)g.dz;
+  const real i2dz2 = real(2) / dz / dz;
+  const real idz2 = real(1) / dz / dz;
+  const real ai = idz2 - f112 * kk, bi = -i2dz2 - f56 * kk, ci = idz2 - f112 * kk;
+  real b1, c1, an, bn;
+  real fm, f0, fp;
+  f0 = f[col];
+  fp = f[cs + col];
+  real d;
+  if (!df0) {
+    b1 = real(1); c1 = real(0); d = real(0);
+    an = real(0); bn = real(1);
+  } else {
+    b1 = -idz2 - f13 * kk;
+    c1 = idz2 - f16 * kk;
+    d = f13 * f0 + f16 * fp;
+    an = idz2 - f16 * kk;
+    bn = -idz2 - f13 * kk;
+  }
+  // tridiagonal (fft_ops.F90:620-656)
+  real den = b1;
+  real prev = d / den;
+  f[col] = prev;
+  real cprev = c1;  // c(i-1)
+  for (int k = 1; k < nz; ++k) {
+    fm = f0;
+    f0 = fp;
+    real a, b, c;
+    if (k < nz - 1) {
+      fp = f[(int64_t)(k + 1) * cs + col];
+      a = ai; b = bi; c = ci;
+      d = f112 * fm + f56 * f0 + f112 * fp;
+    } else {
+      a = an; b = bn; c = real(0);
+      d = df0 ? f13 * f0 + f16 * fm : real(0);
+    }
+    real cp = cprev / den;
+    den = b - a * cp;
+    prev = (d - a * prev) / den;
+    f[(int64_t)k * cs + col] = prev;
+    cpbuf[(int64_t)k * cs + col] = cp;
+    cprev = c;
+  }
+  real nxt = prev;
+  for (int k = nz - 2; k >= 0; --k) {
+    real v = f[(int64_t)k * cs + col] - cpbuf[(int64_t)(k + 1) * cs + col] * nxt;
+    f[(int64_t)k * cs + col] = v;
+    nxt = v;
+  }
+}
+
+// ---- vorticity tendency pointwise combinations (vorticity_tendency.F90:169-265)
+__global__ void k_pw_add_mul(int64_t n, real* __restrict__ o, const real* __restrict__ a,
+                             const real* __restrict__ b) {  // o = o + a*b
+  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) o[e] = o[e] + a[e] * b[e];
+}
+__global__ void k_pw_add_mul_sum(int64_t n, real* __restrict__ o, const real* __restrict__ r,
+                                 const real* __restrict__ q, const real* __restrict__ w) {  // o = o + r*(q + w)
+  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) o[e] = o[e] + r[e] * (q[e] + w[e]);
+}
+__global__ void k_pw_neg_add_mul(int64_t n, real* __restrict__ o, const real* __restrict__ a,
+                                 const real* __restrict__ b) {  // o = -o + a*b
+  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) o[e] = -o[e] + a[e] * b[e];
+}
+__global__ void k_pw_add_mul_negsum(int64_t n, real* __restrict__ o, const real* __restrict__ r,
+                                    const real* __restrict__ p, const real* __restrict__ w) {  // o = o + r*(-p + w)
+  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) o[e] = o[e] + r[e] * (-p[e] + w[e]);
+}
+__global__ void k_pw_dr(int64_t n, real* __restrict__ dr, const real* __restrict__ p,
+                        const real* __restrict__ q, const real* __restrict__ r, const real* __restrict__ dwdx,
+                        const real* __restrict__ dwdy, const real* __restrict__ dudx,
+                        const real* __restrict__ dvdy) {
+  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  real v = p[e] * dwdx[e];
+  v = v + q[e] * dwdy[e];
+  v = v + r[e] * (-dudx[e]);
+  v = v + r[e] * (-dvdy[e]);
+  dr[e] = v;
+}
+
+// max of squares over the interior (vort2vel.F90:331-338,
+// vorticity_tendency.F90:279-282); non-negative doubles order like their bits
+__global__ void k_max_sq3(int64_t n, const real* __restrict__ u, const real* __restrict__ v,
+                          const real* __restrict__ w, double* __restrict__ out3) {
+  real mu = 0, mv = 0, mw = 0;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    real a = u[e], b = v[e], c = w[e];
+    mu = fmax(mu, a * a);
+    mv = fmax(mv, b * b);
+    mw = fmax(mw, c * c);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mu = fmax(mu, __shfl_down_sync(0xffffffffu, mu, o));
+    mv = fmax(mv, __shfl_down_sync(0xffffffffu, mv, o));
+    mw = fmax(mw, __shfl_down_sync(0xffffffffu, mw, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax((unsigned long long*)&out3[0], __double_as_longlong((double)mu));
+    atomicMax((unsigned long long*)&out3[1], __double_as_longlong((double)mv));
+    atomicMax((unsigned long long*)&out3[2], __double_as_longlong((double)mw));
+  }
+}
+__global__ void k_max_vort(int64_t n, const real* __restrict__ p, const real* __restrict__ q,
+                           const real* __restrict__ r, double* __restrict__ out) {
+  real m = 0;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    real a = p[e], b = q[e], c = r[e];
+    m = fmax(m, a * a + b * b + c * c);
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax((unsigned long long*)out, __double_as_longlong((double)m));
+}
+
+int diffz_launch_impl(pmpic_ctx* ctx, const real* in, real* out, const real* bot, const real* top) {
+  TimerScope ts(ctx, T_DIFFZ);
+  const Geom& g = ctx->g;
+  int which = bot ? 1 : 0;
+  const real* coef = tab_diffz(ctx, which);
+  k_diffz<<<nblk((int64_t)g.sx * g.sy, 128), 128, 0, ctx->stream>>>(g, in, out, coef, bot, top, (real)f4div(1.f, 6.f)); ++ctx->nlaunch;
+  PMPIC_CUDA(cudaGetLastError());
+  return 0;
+}
+
+
+int spec_diffx_impl(pmpic_ctx* ctx, const real* in, real* out) {
+  k_diffx<<<nblk(ctx->g.nspec, 256), 256, 0, ctx->stream>>>(ctx->g, in, out, tab_kx(ctx)); ++ctx->nlaunch;
+  PMPIC_CUDA(cudaGetLastError());
+  return 0;
+}
+int spec_diffy_impl(pmpic_ctx* ctx, const real* in, real* out) {
+  k_diffy<<<nblk(ctx->g.nspec, 256), 256, 0, ctx->stream>>>(ctx->g, in, out, tab_ky(ctx)); ++ctx->nlaunch;
+  PMPIC_CUDA(cudaGetLastError());
+  return 0;
+}
+int spec_filter_impl(pmpic_ctx* ctx, const real* in, real* out) {
+  k_filter<<<nblk(ctx->g.nspec, 256), 256, 0, ctx->stream>>>(ctx->g, in, out, tab_filt(ctx)); ++ctx->nlaunch;
+  PMPIC_CUDA(cudaGetLastError());
+  return 0;
+}
+int spec_diffz_impl(pmpic_ctx* ctx, const real* in, real* out, const real* bot, const real* top) {
+  return diffz_launch_impl(ctx, in, out, bot, top);
+}
+int spec_laplinv_impl(pmpic_ctx* ctx, real* inout, bool df0) {
+  TimerScope ts(ctx, T_LAPLINV);
+  const Geom& g = ctx->g;
+  k_laplinv<<<nblk((int64_t)g.sx * g.sy, 128), 128, 0, ctx->stream>>>(g, inout, RP(ctx->sscratch), tab_k2(ctx), df0 ? 1 : 0); ++ctx->nlaunch;
+  PMPIC_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// vort2vel.F90:139-320 after the three par2grid calls (grids P, Q, R hold the
+// gridded vorticity on entry; on exit they hold the corrected, filtered
+// vorticity, U, V, W the velocity and u_s, v_s, w_s its filtered spectra).
+int vort2vel_spectral_impl(pmpic_ctx* ctx) {
+  const Geom& g = ctx->g;
+  int rc;
+  real *a = RP(ctx->sa), *b = RP(ctx->sb), *c = RP(ctx->sc), *d = RP(ctx->sd), *e = RP(ctx->se), *f = RP(ctx->sf);
+  real* const* G = (real* const*)ctx->grid;
+  zero_mode_prepare(ctx);
+  const unsigned nb = nblk(g.nspec, 256);
+  const int cols = g.sx * g.sy;
+  if ((rc = fft_forward(ctx, G[PMPIC_GRID_P], a))) return rc;
+  if ((rc = fft_forward(ctx, G[PMPIC_GRID_Q], b))) return rc;
+  if ((rc = fft_forward(ctx, G[PMPIC_GRID_R], c))) return rc;
+  const real hdzi = (real)(f4div(1.f, 2.f) / g.dz);
+  k_div<<<nb, 256, 0, ctx->stream>>>(g, a, b, c, f, tab_kx(ctx), tab_ky(ctx), hdzi); ++ctx->nlaunch;
+  if ((rc = spec_laplinv_impl(ctx, f, true))) return rc;
+  k_filter<<<nb, 256, 0, ctx->stream>>>(g, f, f, tab_filt(ctx)); ++ctx->nlaunch;
+  k_sub_diff<<<nb, 256, 0, ctx->stream>>>(g, a, f, tab_kx(ctx), 0); ++ctx->nlaunch;
+  k_sub_diff<<<nb, 256, 0, ctx->stream>>>(g, b, f, tab_ky(ctx), 1); ++ctx->nlaunch;
+  if ((rc = diffz_launch_impl(ctx, f, d, nullptr, nullptr))) return rc;
+  k_sub_zero0<<<nb, 256, 0, ctx->stream>>>(g, c, d); ++ctx->nlaunch;
+  k_filter3_bt<<<nb, 256, 0, ctx->stream>>>(g, a, b, c, d, e, f, tab_filt(ctx), RP(ctx->bt)); ++ctx->nlaunch;
+  if ((rc = fft_backward(ctx, d, G[PMPIC_GRID_P]))) return rc;
+  if ((rc = fft_backward(ctx, e, G[PMPIC_GRID_Q]))) return rc;
+  if ((rc = fft_backward(ctx, f, G[PMPIC_GRID_R]))) return rc;
+  if ((rc = zero_mode_launch(ctx, d, e))) return rc;
+  if ((rc = spec_laplinv_impl(ctx, a, false))) return rc;
+  if ((rc = spec_laplinv_impl(ctx, b, false))) return rc;
+  if ((rc = spec_laplinv_impl(ctx, c, true))) return rc;
+  const real* atop = RP(ctx->bt);
+  const real* abot = RP(ctx->bt) + cols;
+  const real* btop = RP(ctx->bt) + 2 * cols;
+  const real* bbot = RP(ctx->bt) + 3 * cols;
+  // u = dB/dz - dC/dy
+  if ((rc = diffz_launch_impl(ctx, b, e, bbot, btop))) return rc;
+  k_vel<<<nb, 256, 0, ctx->stream>>>(g, 0, e, c, a, b, f, RP(ctx->spec[PMPIC_SPEC_U]), tab_kx(ctx), tab_ky(ctx), tab_filt(ctx),
+                                     ctx->zmode); ++ctx->nlaunch;
+  if ((rc = fft_backward(ctx, f, G[PMPIC_GRID_U]))) return rc;
+  // v = dC/dx - dA/dz
+  if ((rc = diffz_launch_impl(ctx, a, e, abot, atop))) return rc;
+  k_vel<<<nb, 256, 0, ctx->stream>>>(g, 1, e, c, a, b, f, RP(ctx->spec[PMPIC_SPEC_V]), tab_kx(ctx), tab_ky(ctx), tab_filt(ctx),
+                                     ctx->zmode + g.nzp); ++ctx->nlaunch;
+  if ((rc = fft_backward(ctx, f, G[PMPIC_GRID_V]))) return rc;
+  // w = dA/dy - dB/dx
+  k_vel<<<nb, 256, 0, ctx->stream>>>(g, 2, e, c, a, b, f, RP(ctx->spec[PMPIC_SPEC_W]), tab_kx(ctx), tab_ky(ctx), tab_filt(ctx),
+                                     ctx->zmode); ++ctx->nlaunch;
+  if ((rc = fft_backward(ctx, f, G[PMPIC_GRID_W]))) return rc;
+  PMPIC_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// vorticity_tendency.F90:147-265 (grid B holds par2grid(btot) on entry).
+int vorticity_tendency_grids_impl(pmpic_ctx* ctx) {
+  const Geom& g = ctx->g;
+  int rc;
+  real *bs = RP(ctx->sbs), *as = RP(ctx->sas);
+  real* const* G = (real* const*)ctx->grid;
+  real *DP = G[PMPIC_GRID_DP], *DQ = G[PMPIC_GRID_DQ], *DR = G[PMPIC_GRID_DR];
+  const real *P = G[PMPIC_GRID_P], *Q = G[PMPIC_GRID_Q], *R = G[PMPIC_GRID_R];
+  real *dudx = RP(ctx->gwork[0]), *dwdx = RP(ctx->gwork[1]), *dvdy = RP(ctx->gwork[2]), *dwdy = RP(ctx->gwork[3]);
+  real* ap = RP(ctx->gwork[4]);
+  const int64_t n = g.nphys;
+  const unsigned nb = nblk(n, 256);
+  if ((rc = fft_forward(ctx, G[PMPIC_GRID_B], bs))) return rc;
+  if ((rc = spec_diffy_impl(ctx, bs, as))) return rc;
+  if ((rc = fft_backward(ctx, as, DP))) return rc;
+  if ((rc = spec_diffx_impl(ctx, RP(ctx->spec[PMPIC_SPEC_U]), as))) return rc;
+  if ((rc = fft_backward(ctx, as, dudx))) return rc;
+  k_pw_add_mul<<<nb, 256, 0, ctx->stream>>>(n, DP, P, dudx); ++ctx->nlaunch;
+  if ((rc = spec_diffy_impl(ctx, RP(ctx->spec[PMPIC_SPEC_U]), as))) return rc;
+  if ((rc = fft_backward(ctx, as, ap))) return rc;
+  k_pw_add_mul<<<nb, 256, 0, ctx->stream>>>(n, DP, Q, ap); ++ctx->nlaunch;
+  if ((rc = spec_diffx_impl(ctx, RP(ctx->spec[PMPIC_SPEC_W]), as))) return rc;
+  if ((rc = fft_backward(ctx, as, dwdx))) return rc;
+  k_pw_add_mul_sum<<<nb, 256, 0, ctx->stream>>>(n, DP, R, Q, dwdx); ++ctx->nlaunch;
+  if ((rc = spec_diffx_impl(ctx, bs, as))) return rc;
+  if ((rc = fft_backward(ctx, as, DQ))) return rc;
+  if ((rc = spec_diffx_impl(ctx, RP(ctx->spec[PMPIC_SPEC_V]), as))) return rc;
+  if ((rc = fft_backward(ctx, as, ap))) return rc;
+  k_pw_neg_add_mul<<<nb, 256, 0, ctx->stream>>>(n, DQ, P, ap); ++ctx->nlaunch;
+  if ((rc = spec_diffy_impl(ctx, RP(ctx->spec[PMPIC_SPEC_V]), as))) return rc;
+  if ((rc = fft_backward(ctx, as, dvdy))) return rc;
+  k_pw_add_mul<<<nb, 256, 0, ctx->stream>>>(n, DQ, Q, dvdy); ++ctx->nlaunch;
+  if ((rc = spec_diffy_impl(ctx, RP(ctx->spec[PMPIC_SPEC_W]), as))) return rc;
+  if ((rc = fft_backward(ctx, as, dwdy))) return rc;
+  k_pw_add_mul_negsum<<<nb, 256, 0, ctx->stream>>>(n, DQ, R, P, dwdy); ++ctx->nlaunch;
+  k_pw_dr<<<nb, 256, 0, ctx->stream>>>(n, DR, P, Q, R, dwdx, dwdy, dudx, dvdy); ++ctx->nlaunch;
+  PMPIC_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// maxima for the dt rule; v2v: velocity limit, vt: vorticity limit
+int field_max_impl(pmpic_ctx* ctx, bool v2v, bool vt) {
+  real* const* G = (real* const*)ctx->grid;
+  const Geom& g = ctx->g;
+  if (v2v) {
+    PMPIC_CUDA(cudaMemsetAsync(&ctx->dinfo->umax2, 0, 3 * sizeof(double), ctx->stream));
+    k_max_sq3<<<592, 256, 0, ctx->stream>>>(g.nphys, G[PMPIC_GRID_U], G[PMPIC_GRID_V],
+                                            G[PMPIC_GRID_W], &ctx->dinfo->umax2); ++ctx->nlaunch;
+  }
+  if (vt) {
+    PMPIC_CUDA(cudaMemsetAsync(&ctx->dinfo->omax2, 0, sizeof(double), ctx->stream));
+    k_max_vort<<<592, 256, 0, ctx->stream>>>(g.nphys, G[PMPIC_GRID_P], G[PMPIC_GRID_Q],
+                                             G[PMPIC_GRID_R], &ctx->dinfo->omax2); ++ctx->nlaunch;
+  }
+  PMPIC_CUDA(cudaGetLastError());
+  return 0;
+}
+

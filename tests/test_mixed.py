@@ -1,0 +1,144 @@
+"""The mixed-precision form (PMPIC_MIXED) against the FP64 oracle and the
+plain FP64 GPU path.  Needs a CUDA device.
+
+The mixed form computes in FP32 (interpolation, transforms, tendencies, RK4),
+keeps positions as an integer cell index plus an FP32 offset, and keeps the
+zero mode (the mean flow of vort2vel.F90:230-241) in FP64.  Its results are
+not bit-identical to FP64 and are judged by error against the FP64 oracle:
+
+  * gridded velocity u, v, w after the 20 steps of the 32^3 plume (dt 0.01):
+    relative L2 error <= 1e-4;
+  * split and mixing bookkeeping (counts, slots, tags) on inputs whose
+    decisions lie far from the thresholds: identical to the oracle;
+  * transfers: FP64 -> mixed -> FP64 within one FP32 rounding of the offset;
+  * total parcel volume through a mixing step: conserved to FP32 rounding.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from helpers import rel, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TWO_PI = 2 * math.pi
+TOL_VEL = 1e-4  # relative L2 of gridded velocity vs the FP64 oracle
+
+
+@pytest.fixture(scope="module")
+def pm():
+    import pmpic_b200
+    return pmpic_b200
+
+
+def _vortical(pm, n, seed=9, amp=1.0):
+    ic = pm.thermal_parcels(n, n, n)
+    rng = np.random.default_rng(seed)
+    for q in "pqr":
+        ic[q] = amp * np.sin(ic["x"] * rng.integers(1, 3)) * np.cos(ic["y"] + ic["z"] * rng.uniform(0.5, 2))
+    return ic
+
+
+def test_mixed_transfer_round_trip(pm):
+    n = 16
+    ic = _vortical(pm, n)
+    g = pm.Context(n, n, n, TWO_PI, TWO_PI, math.pi, max_parcels=2 * len(ic["x"]), precision="mixed")
+    g.upload(**ic)
+    dx, dz = TWO_PI / n, math.pi / n
+    for q, d in [("x", dx), ("y", dx), ("z", dz)]:
+        # the offset is an FP32 fraction of a cell: error below one FP32 ulp of 1 cell
+        assert np.abs(g.get(q) - ic[q]).max() <= d * 2.0 ** -23, q
+    for q in ["p", "q", "r", "b", "h", "vol"]:
+        np.testing.assert_allclose(g.get(q), ic[q].astype(np.float32).astype(np.float64), rtol=0, atol=0)
+    np.testing.assert_array_equal(g.get("tag"), ic["tag"])
+
+
+def test_mixed_config0_twenty_steps_vs_oracle(pm):
+    """Config 0: 32^3 plume, dt = 0.01, 20 steps."""
+    from oracle import Oracle
+    n = 32
+    ic = pm.thermal_parcels(n, n, n)
+    cap = 2 * len(ic["x"])
+    g = pm.Context(n, n, n, TWO_PI, TWO_PI, math.pi, dtm=0.01, dtmax=0.01, max_parcels=cap, precision="mixed")
+    o = Oracle(n, n, n, TWO_PI, TWO_PI, math.pi, dtm=0.01, dtmax=0.01, max_parcels=cap)
+    g.upload(**ic)
+    o.set_parcels(**ic)
+    for _ in range(20):
+        g.step(1)
+        o.step()
+    errs = {name: rel_l2(g.grid(name), o.grid(name)) for name in ["u", "v", "w"]}
+    for name, e in errs.items():
+        assert e < TOL_VEL, (name, e)
+
+
+def test_mixed_split_and_mix_bookkeeping_vs_oracle(pm):
+    """Splitting and mixing active in the first step, on inputs whose decisions
+    lie far from the thresholds (stretch 3.5 or 4.5; volume 0.5 vmin or the
+    lattice volume): counts and tags identical to the oracle."""
+    from oracle import Oracle
+    n = 16
+    ic = _vortical(pm, n, amp=3.0)
+    k = len(ic["x"])
+    rng = np.random.default_rng(33)
+    ic["stretch"] = np.where(rng.uniform(size=k) < 0.1, 4.5, 3.5)
+    vmin = (TWO_PI / n) ** 2 * (math.pi / n) / 216
+    ic["vol"][rng.uniform(size=k) < 0.1] = 0.5 * vmin
+    cap = 4 * k
+    g = pm.Context(n, n, n, TWO_PI, TWO_PI, math.pi, dtm=0.02, dtmax=0.02, max_parcels=cap, precision="mixed")
+    o = Oracle(n, n, n, TWO_PI, TWO_PI, math.pi, dtm=0.02, dtmax=0.02, max_parcels=cap)
+    g.upload(**ic)
+    o.set_parcels(**ic)
+    g.step(1)
+    o.step()
+    ig, io = g.info(), o.info()
+    assert io.n_split > 0 and io.n_removed > 0
+    assert (ig.n_split, ig.n_removed, ig.n_added) == (io.n_split, io.n_removed, io.n_added)
+    assert g.n == o.n
+    np.testing.assert_array_equal(g.get("tag"), o.get("tag"))
+    for q in ["x", "y", "z"]:
+        assert rel(g.get(q), o.get(q)) < 1e-5, q
+    for name in ["u", "v", "w"]:
+        assert rel_l2(g.grid(name), o.grid(name)) < TOL_VEL, name
+
+
+def test_mixed_mixing_conserves_volume(pm):
+    """parcel_mixing moves volume between removed, new and kept parcels and
+    conserves its total (the report's check, report.tex:264); FP32 volumes
+    sum to the FP64 total within FP32 rounding."""
+    n = 16
+    ic = _vortical(pm, n)
+    k = len(ic["x"])
+    rng = np.random.default_rng(5)
+    vmin = (TWO_PI / n) ** 2 * (math.pi / n) / 216
+    ic["vol"][rng.uniform(size=k) < 0.5] = 0.5 * vmin
+    g = pm.Context(n, n, n, TWO_PI, TWO_PI, math.pi, dtm=0.01, dtmax=0.01, max_parcels=2 * k, precision="mixed")
+    g.upload(**ic)
+    v0 = np.sum(g.get("vol"))
+    g.set_counters([3, 3, 4, 3, 3])  # the next callbacks are the fourth substep's
+    g.parcel_mixing()
+    v1 = np.sum(g.get("vol"))
+    assert g.info().n_removed > 0
+    assert abs(v1 - v0) / v0 < 1e-5
+
+
+def test_mixed_deterministic(pm):
+    n = 16
+    ic = _vortical(pm, n)
+    res = []
+    for _ in range(2):
+        g = pm.Context(n, n, n, TWO_PI, TWO_PI, math.pi, max_parcels=2 * len(ic["x"]), precision="mixed")
+        g.upload(**ic)
+        g.step(2)
+        res.append({q: g.get(q) for q in ["x", "z", "p", "vol"]} | {"u": g.grid("u")})
+        g.close()
+    for q in res[0]:
+        np.testing.assert_array_equal(res[0][q], res[1][q], err_msg=q)
+
+
+def test_mixed_rejects_fp64_kernel_ops(pm):
+    g = pm.Context(8, 8, 8, 1.0, 1.0, 1.0, max_parcels=16, precision="mixed")
+    g.upload(x=np.array([0.5]), y=np.array([0.5]), z=np.array([0.5]), vol=np.ones(1))
+    with pytest.raises(pm.PmpicError) as e:
+        g.par2grid("b", "b")
+    assert e.value.code == -9  # PMPIC_ERR_STATE
