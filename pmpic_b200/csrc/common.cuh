@@ -197,6 +197,7 @@ struct pmpic_ctx {
   double* gspare;            // spare physical grid
   int32_t* sorted;           // cap: slot indices sorted by cell
   double* rowpart;           // par2grid row partials (rowpart_bytes)
+  double* gpack;             // 6 x nphys: the RK4 gather grids packed z fastest (parcels.cu)
   int32_t* cell_count;       // ncell + 1
   int32_t* cell_start;       // ncell + 1
   int32_t* cell_fill;        // ncell

@@ -78,6 +78,87 @@ struct PredNewCell {
   }
 };
 
+// ---- packed gather grids ------------------------------------------------------------
+// The RK4 pass gathers six grids (u, v, w, dp, dq, dr) at every parcel.  Parcels
+// stream in z-fastest cell order while grids are x fastest, so one stage first
+// repacks the six into G6[i][j][k][6] (z fastest, fields interleaved): a cell's
+// four xy corners then hold their two levels and six fields in 12 consecutive
+// values, and the cells of a warp (consecutive in z) share lines.
+constexpr int PK_T = 32;  // x extent of a tile
+constexpr int PK_K = 16;  // z extent of a tile
+template <class R>
+__global__ void __launch_bounds__(256) k_pack6(Geom g, const R* __restrict__ G0, const R* __restrict__ G1,
+                                               const R* __restrict__ G2, const R* __restrict__ G3,
+                                               const R* __restrict__ G4, const R* __restrict__ G5,
+                                               R* __restrict__ out) {
+  constexpr int TS = PK_K * (PK_T + 1) + 1;  // per-field tile stride, odd
+  __shared__ R tile[6 * TS];
+  const int i0 = blockIdx.x * PK_T, k0 = blockIdx.y * PK_K, j = blockIdx.z;
+  const R* G[6] = {G0, G1, G2, G3, G4, G5};
+  const int ni = min(PK_T, g.Nx - i0), nk = min(PK_K, g.nzp - k0);
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    for (int e = threadIdx.x; e < PK_K * PK_T; e += blockDim.x) {
+      const int kk = e / PK_T, ii = e - kk * PK_T;
+      if (kk < nk && ii < ni)
+        tile[f * TS + kk * (PK_T + 1) + ii] = G[f][((size_t)(k0 + kk) * g.Ny + j) * g.Nx + i0 + ii];
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < 6 * PK_K * PK_T; e += blockDim.x) {
+    const int ii = e / (6 * PK_K), r = e - ii * 6 * PK_K;
+    const int kk = r / 6, f = r - kk * 6;
+    if (kk < nk && ii < ni)
+      out[(((size_t)(i0 + ii) * g.Ny + j) * g.nzp + k0 + kk) * 6 + f] = tile[f * TS + kk * (PK_T + 1) + ii];
+  }
+}
+template <class R>
+static void pack6(pmpic_ctx* ctx, const R* const* grids, R* out) {
+  const Geom& g = ctx->g;
+  dim3 gr((g.Nx + PK_T - 1) / PK_T, (g.nzp + PK_K - 1) / PK_K, g.Ny);
+  k_pack6<R><<<gr, 256, 0, ctx->stream>>>(g, grids[0], grids[1], grids[2], grids[3], grids[4], grids[5], out);
+  ++ctx->nlaunch;
+}
+// the six fields at the two levels of xy corner (ci, cj) of a cell of level ck:
+// lo[f] at ck, hi[f] at ck+1
+__device__ __forceinline__ void corner6(const Geom& g, const double* __restrict__ G6, int ci, int cj, int ck,
+                                        double* lo, double* hi) {
+  const double2* p = (const double2*)(G6 + (((size_t)ci * g.Ny + cj) * g.nzp + ck) * 6);
+  const double2 a = p[0], b = p[1], c = p[2], d = p[3], e = p[4], f = p[5];
+  lo[0] = a.x; lo[1] = a.y; lo[2] = b.x; lo[3] = b.y; lo[4] = c.x; lo[5] = c.y;
+  hi[0] = d.x; hi[1] = d.y; hi[2] = e.x; hi[3] = e.y; hi[4] = f.x; hi[5] = f.y;
+}
+__device__ __forceinline__ void corner6(const Geom& g, const float* __restrict__ G6, int ci, int cj, int ck,
+                                        float* lo, float* hi) {
+  const float2* p = (const float2*)(G6 + (((size_t)ci * g.Ny + cj) * g.nzp + ck) * 6);
+  const float2 a = p[0], b = p[1], c = p[2], d = p[3], e = p[4], f = p[5];
+  lo[0] = a.x; lo[1] = a.y; lo[2] = b.x; lo[3] = b.y; lo[4] = c.x; lo[5] = c.y;
+  hi[0] = d.x; hi[1] = d.y; hi[2] = e.x; hi[3] = e.y; hi[4] = f.x; hi[5] = f.y;
+}
+// grid2par (parcel_interpolation.F90:299-321) of all six packed fields: z,
+// then y, then x, in the reference's operation order
+template <class R>
+__device__ __forceinline__ void g2p_packed(const Geom& g, const R* __restrict__ G6, int ci, int cj, int ck, R delx,
+                                           R dely, R delz, R* d) {
+  const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
+  const R ez = R(1) - delz, ey = R(1) - dely, ex = R(1) - delx;
+  R lo[6], hi[6], c00[6], c0[6];
+  // x corner i: c0 = c00 (1-dely) + c10 dely, with c.. = lower (1-delz) + upper delz
+  corner6(g, G6, ci, cj, ck, lo, hi);
+#pragma unroll
+  for (int f = 0; f < 6; ++f) c00[f] = lo[f] * ez + hi[f] * delz;
+  corner6(g, G6, ci, cj1, ck, lo, hi);
+#pragma unroll
+  for (int f = 0; f < 6; ++f) c0[f] = c00[f] * ey + (lo[f] * ez + hi[f] * delz) * dely;
+  // x corner i+1
+  corner6(g, G6, ci1, cj, ck, lo, hi);
+#pragma unroll
+  for (int f = 0; f < 6; ++f) c00[f] = lo[f] * ez + hi[f] * delz;
+  corner6(g, G6, ci1, cj1, ck, lo, hi);
+#pragma unroll
+  for (int f = 0; f < 6; ++f) d[f] = c0[f] * ex + (c00[f] * ey + (lo[f] * ez + hi[f] * delz) * dely) * delx;
+}
+
 // ---- RK4 stage (rk4_integrator.F90:95-319) -----------------------------------------
 // One pass per stage: the deferred grid2par gathers of vort2vel (u, v, w ->
 // dxdt, dydt, dzdt, vort2vel.F90:325-327) and of vorticity_tendency (dp, dq,
@@ -91,6 +172,7 @@ struct RkPtrs {
   double* f[6];
   double* d[6];
   const double* grid[6];  // u, v, w, dp, dq, dr
+  const double* g6;       // the six packed (k_pack6), when both gathers are pending
 };
 
 __device__ __forceinline__ int classify_dir(const Geom& g, double x, double y) {
@@ -108,7 +190,7 @@ __device__ __forceinline__ int classify_dir(const Geom& g, double x, double y) {
 }
 
 template <bool GU, bool GP>
-__global__ void k_rk4(Geom g, int64_t n, RkPtrs P, int stage, const double* __restrict__ dtp,
+__global__ void __launch_bounds__(256, 3) k_rk4(Geom g, int64_t n, RkPtrs P, int stage, const double* __restrict__ dtp,
                       const int32_t* __restrict__ cell, const double* __restrict__ del, int64_t cap,
                       int8_t* __restrict__ dir) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -134,9 +216,10 @@ __global__ void k_rk4(Geom g, int64_t n, RkPtrs P, int stage, const double* __re
     const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
     const size_t r00 = ((size_t)ck * g.Ny + cj) * g.Nx, r01 = ((size_t)ck * g.Ny + cj1) * g.Nx;
     const size_t r10 = ((size_t)(ck + 1) * g.Ny + cj) * g.Nx, r11 = ((size_t)(ck + 1) * g.Ny + cj1) * g.Nx;
+    if (GU && GP) g2p_packed<double>(g, P.g6, ci, cj, ck, delx, dely, delz, d);
 #pragma unroll
     for (int v = 0; v < 6; ++v) {
-      if ((v < 3 && !GU) || (v >= 3 && !GP)) continue;
+      if ((v < 3 && !GU) || (v >= 3 && !GP) || (GU && GP)) continue;
       const double* G = P.grid[v];
       // grid2par, parcel_interpolation.F90:299-321
       double c00 = G[r00 + ci] * (1 - delz) + G[r10 + ci] * delz;
@@ -551,6 +634,8 @@ __global__ void k_backfill(const int32_t* __restrict__ zlist, const int32_t* __r
 // (CellOff); the integer bookkeeping (directions, lists, slots) is shared with
 // the plain path.  Float property p of parcel n is ((float*)array_p)[n].
 struct MPtrs {
+  const float* g6;  // the six grids packed (k_pack6), when both gathers are pending
+  float inv[3];     // 1/dx, 1/dy, 1/dz
   CellOff* s[3];
   CellOff* o[3];
   CellOff* f[3];
@@ -593,13 +678,13 @@ __device__ __forceinline__ int classify_dir_m(const Geom& g, int i, int j) {
 // reflection and the direction classification, as k_rk4; position updates in
 // cell units (velocity * dt / cell size), renormalised into [0, 1).
 template <bool GU, bool GP>
-__global__ void k_rk4_m(Geom g, int64_t n, MPtrs P, int stage, const double* __restrict__ dtp,
+__global__ void __launch_bounds__(256, 4) k_rk4_m(Geom g, int64_t n, MPtrs P, int stage, const double* __restrict__ dtp,
                         int8_t* __restrict__ dir) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  const double dtd = *dtp;
-  const float dt = (float)dtd, dt6 = (float)(dtd / 6), dt2 = (float)(dtd / 2), dt3 = (float)(dtd / 3);
-  const float inv[3] = {(float)(1.0 / g.dx), (float)(1.0 / g.dy), (float)(1.0 / g.dz)};
+  const float dt = (float)*dtp;  // state%dtm (rk4_integrator.F90:102)
+  const float dt6 = dt * (1.f / 6.f), dt2 = dt * 0.5f, dt3 = dt * (1.f / 3.f);
+  const float* inv = P.inv;
   CellOff sp[3], op[3], fp[3];
   float sv[3], ov[3], fv[3], d[6];
   const bool need_s = stage == 1 || GU || GP;
@@ -624,10 +709,14 @@ __global__ void k_rk4_m(Geom g, int64_t n, MPtrs P, int stage, const double* __r
     const int ci = sp[0].i, cj = sp[1].i, ck = sp[2].i;
     // a position outside the grid was reported by the binning; it gathers nothing
     gathered = ci >= 0 && ci < g.Nx && cj >= 0 && cj < g.Ny && ck >= 0 && ck < g.Nz;
+    if (GU && GP && gathered) {
+      g2p_packed<float>(g, P.g6, ci, cj, ck, sp[0].f, sp[1].f, sp[2].f, d);
+    } else {
 #pragma unroll
-    for (int v = 0; v < 6; ++v) {
-      if ((v < 3 && !GU) || (v >= 3 && !GP)) continue;
-      d[v] = gathered ? g2p_f(g, P.grid[v], ci, cj, ck, sp[0].f, sp[1].f, sp[2].f) : P.d[v][t];
+      for (int v = 0; v < 6; ++v) {
+        if ((v < 3 && !GU) || (v >= 3 && !GP)) continue;
+        d[v] = gathered ? g2p_f(g, P.grid[v], ci, cj, ck, sp[0].f, sp[1].f, sp[2].f) : P.d[v][t];
+      }
     }
   }
   CellOff sn[3];
@@ -1061,6 +1150,11 @@ int rk4_stage(pmpic_ctx* ctx, int stage) {
       P.grid[v] = (const float*)ctx->grid[G[v]];
     }
     const bool gu = ctx->pending_uvw, gp = ctx->pending_pqr;
+    P.inv[0] = (float)(1.0 / ctx->g.dx);
+    P.inv[1] = (float)(1.0 / ctx->g.dy);
+    P.inv[2] = (float)(1.0 / ctx->g.dz);
+    P.g6 = (const float*)ctx->gpack;
+    if (gu && gp) pack6<float>(ctx, P.grid, (float*)ctx->gpack);
     auto kern = gu ? (gp ? k_rk4_m<true, true> : k_rk4_m<true, false>) : (gp ? k_rk4_m<false, true> : k_rk4_m<false, false>);
     kern<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, P, stage, &ctx->dinfo->dtm, ctx->dir); ++ctx->nlaunch;
     ctx->pending_uvw = ctx->pending_pqr = false;
@@ -1085,6 +1179,8 @@ int rk4_stage(pmpic_ctx* ctx, int stage) {
   }
   const bool gu = ctx->pending_uvw, gp = ctx->pending_pqr;
   if ((gu || gp) && !ctx->sorted_valid) return set_error(ctx, PMPIC_ERR_STATE, "deferred gather without binning");
+  P.g6 = ctx->gpack;
+  if (gu && gp) pack6<double>(ctx, P.grid, ctx->gpack);
   auto kern = gu ? (gp ? k_rk4<true, true> : k_rk4<true, false>) : (gp ? k_rk4<false, true> : k_rk4<false, false>);
   kern<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, P, stage, &ctx->dinfo->dtm, ctx->cell, ctx->del,
                                                    ctx->cap, ctx->dir); ++ctx->nlaunch;
