@@ -159,26 +159,52 @@ def run_reference(args):
     return 0
 
 
-def run_b200(args):
-    rank, world, local = dist_env()
-    import torch  # device selection and the multi-rank plumbing only
-    torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-        pg = dist
-    import pmpic_b200 as pm
+def algorithmic_bytes(kernel, precision, n_avg, nphys, calls, steps):
+    """Algorithmic bytes of all launches of one kernel in the timed region.
 
+    par2grid (per launch, one field set): offsets, vol and the fields of every
+      parcel, its sorted index, and the NQ grids written.  Per step: four
+      vort2vel passes (p, q, r, btot; the FP64 path stages b, h, z for btot),
+      the mixing kept class and, when any parcel is removed, the removed class
+      (6 sums over b, h, p, q, r).
+    rk4_kernel (per stage): the RK4 state it must read and write (x, y, z, p,
+      q, r and their xo/xf copies, the six tendencies, the direction byte),
+      the binning it gathers at (FP64: cell id + 3 offsets), and the six grids
+      read once.  Stage 1 reads x, writes xo, xf, x; stages 2-3 read xo, xf,
+      write xf, x; stage 4 reads xf, writes xf, x.
+    """
+    w = 8 if precision == "fp64" else 4
+    if kernel == "par2grid":
+        if precision == "fp64":
+            b0, b1 = 84.0, 76.0   # 3 del + vol + p,q,r + b,h,z (+4 index); 3 del + vol + b,h,p,q,r
+        else:
+            b0, b1 = 36.0, 40.0   # 3 offsets + vol + p,q,r,btot (+4); 3 offsets + vol + b,h,p,q,r
+        per_step = 4 * (b0 * n_avg + 4 * w * nphys) + (b1 * n_avg + 6 * w * nphys)
+        extra = max(calls - 5 * steps, 0) * (b1 * n_avg + 6 * w * nphys)
+        return per_step * steps + extra
+    if kernel == "rk4_kernel":
+        if precision == "fp64":
+            st = [76 + 193, 124 + 145, 124 + 145, 76 + 145]
+        else:  # positions: int cell + FP32 offset (8 B), the rest FP32
+            st = [36 + 133, 96 + 97, 96 + 97, 60 + 97]
+        return steps * sum(s_ * n_avg + 6 * w * nphys for s_ in st)
+    return None
+
+
+def run_form(precision, args, local, pg, headline):
+    """One context of `precision`: W warm-up steps, K timed steps (CUDA events on
+    the library's stream, clocks sampled), then untimed steps up to
+    args.error_steps, and the gridded velocity downloaded for the error check."""
+    import torch
+    import pmpic_b200 as pm
     grid = args.grid
     ic = pm.thermal_parcels(grid, grid, grid, **PLUME)
     n0 = len(ic["x"])
     cap = int(args.capacity * n0)
     ctx = pm.Context(grid, grid, grid, PLUME["lx"], PLUME["ly"], PLUME["lz"], dtm=0.0025, dtmax=0.0025,
-                     max_parcels=cap, device=local, precision=args.precision)
+                     max_parcels=cap, device=local, precision=precision)
     ctx.upload(**ic)
+    del ic
     L = pm.lib()
     h = ctx._h
 
@@ -190,7 +216,6 @@ def run_b200(args):
     for _ in range(args.warmup):
         ctx.step(1)
     barrier()
-    # timed region: device-resident state, CUDA events on the library's stream
     L.pmpic_timing(h, 1)
     l0 = C.c_int64()
     L.pmpic_launch_count(h, C.byref(l0))
@@ -205,7 +230,6 @@ def run_b200(args):
         L.pmpic_event_elapsed(h, 0, 1, C.byref(ms))
     l1 = C.c_int64()
     L.pmpic_launch_count(h, C.byref(l1))
-    t_dev = ms.value / 1e3
     timers = {}
     for i in range(L.pmpic_timer_count()):
         tot, calls = C.c_double(), C.c_int64()
@@ -213,84 +237,116 @@ def run_b200(args):
         timers[L.pmpic_timer_name(i).decode()] = (tot.value, calls.value)
     L.pmpic_timing(h, 0)
     barrier()
-    t_max, work_all = combine(t_dev, work, pg, "cuda")
-    value = work_all / t_max
+    t_max, work_all = combine(ms.value / 1e3, work, pg, "cuda")
+    res = {"value": work_all / t_max, "ms_per_step": 1e3 * t_max / args.steps, "n0": n0, "cap": cap,
+           "gpu_launches": int(l1.value - l0.value), "clocks": clk.summary(),
+           "timers_ms": {k: round(v[0], 3) for k, v in timers.items() if v[1]}}
 
-    # roofline of the dominant kernel family (by share of the timed region)
+    # roofline of the dominant kernel of the two candidates
     peak, peak_kind = hbm_peak()
-    nz1 = grid + 1
-    nphys = nz1 * grid * grid
-    nspec = nz1 * (grid + 2) * (grid + 2)
+    nphys = (grid + 1) * grid * grid
     n_avg = work / max(args.steps, 1)
-    # algorithmic bytes per launch (minimal traffic of one call):
-    #  par2grid: x,y,z,vol + NQ fields per parcel, NQ grids out (vort2vel NQ=3,
-    #            btot NQ=1, the two mixing classes NQ=6: averaged over launches)
-    #  grid2par: x,y,z per parcel + 3 outputs, 3 grids read
-    #  fft:      read + write of both passes over a spectral field
-    fam = {
-        "par2grid": None, "grid2par": 8.0 * n_avg * 6 + 8.0 * 3 * nphys,
-        "fft_inv_tot": 8.0 * 2 * (nspec + nphys), "fft_fwd_tot": 8.0 * 2 * (nspec + nphys),
-    }
-    # par2grid launches per step: 4 x (NQ=3) + 4 x (NQ=1) + 2 x (NQ=6, mixing)
-    p2g_bytes_step = 4 * (8.0 * n_avg * 7 + 8.0 * 3 * nphys) + 4 * (8.0 * n_avg * 5 + 8.0 * nphys) \
-        + 2 * (8.0 * n_avg * 9 + 8.0 * 6 * nphys)
-    fam["par2grid"] = p2g_bytes_step / 10.0
-    step_ms = timers.get("step", (t_dev * 1e3, args.steps))[0]
-    best = max(fam, key=lambda k: timers.get(k, (0.0, 0))[0])
+    best = max(["par2grid", "rk4_kernel"], key=lambda k: timers.get(k, (0.0, 0))[0])
     tot, calls = timers.get(best, (0.0, 0))
-    avg_s = (tot / calls) / 1e3 if calls else float("nan")
-    achieved = fam[best] / avg_s / 1e9 if calls else None
-    roofline = {"bound": "hbm", "kernel": best, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None, "traffic": None,
-                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
-                "share_of_step": tot / step_ms if step_ms else None, "launches": calls,
-                "avg_launch_ms": tot / calls if calls else None,
-                "algorithmic_bytes_per_launch": fam[best]}
+    step_ms = timers.get("step", (ms.value, args.steps))[0]
+    total_bytes = algorithmic_bytes(best, precision, n_avg, nphys, calls, args.steps)
+    achieved = total_bytes / (tot / 1e3) / 1e9 if calls and tot > 0 else None
+    res["roofline"] = {
+        "bound": "hbm", "kernel": best, "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": (achieved / peak) if achieved else None, "traffic": None,
+        "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+        "share_of_step": tot / step_ms if step_ms else None, "launches": calls,
+        "avg_launch_ms": tot / calls if calls else None,
+        "algorithmic_bytes_per_launch": total_bytes / calls if calls else None}
 
-    # end to end: the host owns the state; each step uploads it from pinned
-    # host memory, runs the step through the C ABI and downloads the result
-    e2e = None
-    if args.e2e_steps > 0:
-        nb = ctx.n
-        cap_h = int(nb * 1.02) + 1024
-        host = {}
-        for k in pm.IO_PROPS:
-            a = np.empty(cap_h, np.float64)
-            host[k] = a
-            L.pmpic_pin_host(C.c_void_p(a.ctypes.data), C.c_size_t(a.nbytes))
-        cur = ctx.download()
-        for k in pm.IO_PROPS:
-            host[k][:len(cur[k])] = cur[k]
-        nh = len(cur["x"])
-        del cur
-        barrier()
-        e2e_work, h2d, d2h, done = 0, 0, 0, 0
-        cnt = C.c_int64()
-        L.pmpic_event_record(h, 2)
-        for _ in range(args.e2e_steps):
-            ptrs = [host[k].ctypes.data_as(C.POINTER(C.c_double)) for k in pm.IO_PROPS]
-            rc = L.pmpic_upload_parcels(h, nh, *ptrs)
-            if rc:
-                break
-            e2e_work += nh
-            h2d += 8 * 11 * nh
-            L.pmpic_step(h, 1)
-            if ctx.n > cap_h:
-                break
-            rc = L.pmpic_download_parcels(h, cap_h, C.byref(cnt), *ptrs)
-            nh = int(cnt.value)
-            d2h += 8 * 11 * nh
-            done += 1
-        L.pmpic_event_record(h, 3)
-        ms2 = C.c_float()
-        L.pmpic_event_elapsed(h, 2, 3, C.byref(ms2))
-        for k in pm.IO_PROPS:
-            L.pmpic_unpin_host(C.c_void_p(host[k].ctypes.data))
-        t_e2e, e2e_all = combine(ms2.value / 1e3, e2e_work, pg, "cuda")
-        if done:
-            e2e = {"value": e2e_all / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d // done,
-                   "d2h_bytes_per_step": d2h // done, "steps": done,
-                   "path": "pmpic_upload_parcels (pinned host) -> pmpic_step -> pmpic_download_parcels"}
+    # untimed continuation to args.error_steps, then the gridded velocity
+    done = args.warmup + args.steps
+    while done < args.error_steps:
+        ctx.step(1)
+        done += 1
+    res["steps_total"] = done
+    res["n_final"] = ctx.n
+    res["grids"] = {q: ctx.grid(q) for q in ("u", "v", "w")} if args.error_steps > 0 else None
+
+    # end to end through the C ABI, host-owned state (headline form only; after
+    # the error check, whose step count it would otherwise change)
+    if headline and args.e2e_steps > 0:
+        res["e2e"] = e2e_run(ctx, args, pg, barrier)
+    ctx.close()
+    return res
+
+
+def e2e_run(ctx, args, pg, barrier):
+    """The same step with the state on the host: each step uploads it from pinned
+    host memory, runs through the C ABI and downloads the result."""
+    import pmpic_b200 as pm
+    L = pm.lib()
+    h = ctx._h
+    nb = ctx.n
+    cap_h = int(nb * 1.02) + 1024
+    host = {}
+    for k in pm.IO_PROPS:
+        a = np.empty(cap_h, np.float64)
+        host[k] = a
+        L.pmpic_pin_host(C.c_void_p(a.ctypes.data), C.c_size_t(a.nbytes))
+    cur = ctx.download()
+    for k in pm.IO_PROPS:
+        host[k][:len(cur[k])] = cur[k]
+    nh = len(cur["x"])
+    del cur
+    barrier()
+    e2e_work, h2d, d2h, done = 0, 0, 0, 0
+    cnt = C.c_int64()
+    L.pmpic_event_record(h, 2)
+    for _ in range(args.e2e_steps):
+        ptrs = [host[k].ctypes.data_as(C.POINTER(C.c_double)) for k in pm.IO_PROPS]
+        if L.pmpic_upload_parcels(h, nh, *ptrs):
+            break
+        e2e_work += nh
+        h2d += 8 * 11 * nh
+        L.pmpic_step(h, 1)
+        if ctx.n > cap_h:
+            break
+        L.pmpic_download_parcels(h, cap_h, C.byref(cnt), *ptrs)
+        nh = int(cnt.value)
+        d2h += 8 * 11 * nh
+        done += 1
+    L.pmpic_event_record(h, 3)
+    ms2 = C.c_float()
+    L.pmpic_event_elapsed(h, 2, 3, C.byref(ms2))
+    for k in pm.IO_PROPS:
+        L.pmpic_unpin_host(C.c_void_p(host[k].ctypes.data))
+    t_e2e, e2e_all = combine(ms2.value / 1e3, e2e_work, pg, "cuda")
+    if not done:
+        return None
+    return {"value": e2e_all / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d // done,
+            "d2h_bytes_per_step": d2h // done, "steps": done,
+            "path": "pmpic_upload_parcels (pinned host, FP64) -> pmpic_step -> pmpic_download_parcels"}
+
+
+def run_b200(args):
+    rank, world, local = dist_env()
+    import torch  # device selection and the multi-rank plumbing only
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    forms = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    headline = forms[-1]
+    res = {f: run_form(f, args, local, pg, f == headline) for f in forms}
+    hr = res[headline]
+    err = None
+    if "fp64" in res and "mixed" in res and res["mixed"]["grids"] is not None:
+        err = {"steps": res["mixed"]["steps_total"], "reference": "the plain FP64 GPU path, same plume"}
+        for q in ("u", "v", "w"):
+            a, b = res["mixed"]["grids"][q], res["fp64"]["grids"][q]
+            err[q + "_rel_l2"] = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+            err[q + "_max_abs"] = float(np.abs(a - b).max())
+        err["n_parcels"] = {"mixed": res["mixed"]["n_final"], "fp64": res["fp64"]["n_final"]}
 
     cpu = None
     if rank == 0 and world == 1 and args.cpu_baseline:
@@ -298,24 +354,31 @@ def run_b200(args):
         v, n_s, dt = cpu_reference(args.ref_grid, 1, 0, threads)
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{args.ref_grid}^3 plume ({n_s} parcels), 1 step, C++ restatement of the reference"}
-
     if pg:
         pg.barrier()
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        grid = args.grid
+        label = {"mixed": "mixed-precision form (FP32 fields/grids/RK4, int cell + FP32 offset positions, "
+                          "FP64 zero mode)", "fp64": "plain FP64 path"}
+        line = {"metric": METRIC, "value": hr["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": hr["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 (f64 zero mode)" if headline == "mixed" else "f64",
                 "data": "synthetic (seeded jittered-lattice thermal plume, 8 parcels/cell)",
-                "config": {"workload": f"thermal plume {grid}^3, FP64 GPU path, 4 RK4 substeps + splitting + mixing per step",
-                           "grid": grid, "parcels_initial": n0, "max_parcels": cap, "dt": 0.0025,
-                           "precision": "fp64", "parallelism": f"replicas x{world}",
-                           "l2": "inputs larger than L2 (parcel state ~{:.0f} GB)".format(n0 * 30 * 8 / 1e9)},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": int(l1.value - l0.value),
-                "clocks": clk.summary(),
-                "timers_ms": {k: round(v[0], 3) for k, v in timers.items() if v[1]}}
+                "config": {"workload": f"thermal plume {grid}^3, {label[headline]}; 4 RK4 substeps + "
+                                       f"splitting + mixing per step",
+                           "grid": grid, "parcels_initial": hr["n0"], "max_parcels": hr["cap"], "dt": 0.0025,
+                           "precision": headline, "parallelism": f"replicas x{world}",
+                           "l2": "inputs larger than L2 (parcel state {:.0f} GB)".format(hr["n0"] * 30 * 8 / 1e9)},
+                "roofline": hr["roofline"], "cpu_baseline": cpu, "e2e": hr.get("e2e"),
+                "gpu_launches": hr["gpu_launches"], "clocks": hr["clocks"], "timers_ms": hr["timers_ms"]}
+        if "fp64" in res and headline != "fp64":
+            f = res["fp64"]
+            line["fp64"] = {"value": f["value"], "ms_per_step": f["ms_per_step"], "roofline": f["roofline"],
+                            "gpu_launches": f["gpu_launches"], "clocks": f["clocks"], "timers_ms": f["timers_ms"]}
+            line["mixed_over_fp64"] = hr["value"] / f["value"]
+        line["error_vs_fp64"] = err
         print(json.dumps(line), flush=True)
-    ctx.close()
     if pg:
         pg.destroy_process_group()
     return 0
@@ -332,7 +395,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--ref-grid", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
+                    help="both: time FP64 then the mixed form (the headline value), and compare them")
+    ap.add_argument("--error-steps", type=int, default=100,
+                    help="total steps per form before the gridded velocities are compared (0: no check)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -197,7 +197,8 @@ int pmpic_par2grid_static(int32_t nx, int32_t ny, int32_t nz, double lx, double 
  * timer_start / timer_stop, model_core/src/utils/timer.F90:110-245), backed by
  * CUDA events on the context's stream: cache_weights, par2grid, grid2par,
  * fft_fwd_tot, fft_inv_tot, diffz, laplinv, vort2vel, vort_tend,
- * RK4_all_steps, Par_HSWP_entire, splitting, mixing, step.  Enabling resets. */
+ * RK4_all_steps, Par_HSWP_entire, splitting, mixing, step, rk4_kernel (the RK4
+ * stage kernel alone).  Enabling resets. */
 int pmpic_timing(pmpic_ctx* ctx, int enable);
 int pmpic_timer_count(void);
 const char* pmpic_timer_name(int id);

@@ -157,7 +157,7 @@ struct DevInfo {
 // rk4_integrator.F90:71-75), backed by CUDA events on the context's stream.
 enum TimerId {
   T_CACHE = 0, T_P2G, T_G2P, T_FFTF, T_FFTI, T_DIFFZ, T_LAPLINV, T_V2V, T_VT, T_RK4, T_HSWP, T_SPLIT,
-  T_MIX, T_STEP, T_NT
+  T_MIX, T_STEP, T_RK4K, T_NT
 };
 
 }  // namespace pmpic
@@ -197,7 +197,8 @@ struct pmpic_ctx {
   double* gspare;            // spare physical grid
   int32_t* sorted;           // cap: slot indices sorted by cell
   double* rowpart;           // par2grid row partials (rowpart_bytes)
-  double* gpack;             // 6 x nphys: the RK4 gather grids packed z fastest (parcels.cu)
+  double* gpack;             // 8 x nphys: gather grids packed z fastest (parcels.cu)
+  double* lapcp;             // 3 x nspec: Thomas factors of a batched laplinv
   int32_t* cell_count;       // ncell + 1
   int32_t* cell_start;       // ncell + 1
   int32_t* cell_fill;        // ncell

@@ -59,7 +59,7 @@ int sync_info(pmpic_ctx* ctx) {
 static const char* kTimerNames[T_NT] = {"cache_weights", "par2grid", "grid2par", "fft_fwd_tot",
                                         "fft_inv_tot",   "diffz",    "laplinv",  "vort2vel",
                                         "vort_tend",     "RK4_all_steps", "Par_HSWP_entire", "splitting",
-                                        "mixing",        "step"};
+                                        "mixing",        "step", "rk4_kernel"};
 
 static int take_event(pmpic_ctx* c) {
   if (c->evfree.empty()) {
@@ -115,7 +115,7 @@ int dalloc(pmpic_ctx* ctx, T** p, size_t count) {
 }
 
 void free_all(pmpic_ctx* c) {
-  void* ptrs[] = {c->parcels, c->rowpart,  c->gpack,    c->cell,     c->del,       c->gspare,     c->sorted,    c->cell_count, c->cell_start, c->cell_fill, c->keep,
+  void* ptrs[] = {c->parcels, c->rowpart,  c->gpack,    c->lapcp,    c->cell,     c->del,       c->gspare,     c->sorted,    c->cell_count, c->cell_start, c->cell_fill, c->keep,
                   c->aux,     c->aux2,     c->dir,       c->swapbuf,    c->scan_tmp,   c->npercell,  c->newslot,
                   c->newportion, c->sa,    c->sb,        c->sc,         c->sd,         c->se,        c->sf,
                   c->sas,     c->sbs,      c->sscratch,  c->fftmid,     c->ftw,        c->ftw32,      c->wn32,       c->hsum,       c->stage64,        c->kx,        c->ky,
@@ -239,7 +239,8 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   if (!rc) rc = dalloc(ctx, &ctx->gspare, (size_t)g.nphys);
   if (!rc) rc = dalloc(ctx, &ctx->sorted, cap);
   if (!rc) rc = dalloc(ctx, (char**)&ctx->rowpart, rowpart_bytes(g));
-  if (!rc) rc = dalloc(ctx, &ctx->gpack, 6 * (size_t)g.nphys);
+  if (!rc) rc = dalloc(ctx, &ctx->gpack, 8 * (size_t)g.nphys);  // six RK4 grids or eight mixing fields
+  if (!rc) rc = dalloc(ctx, &ctx->lapcp, 3 * (size_t)g.nspec);
   ctx->stage_n = std::min<int64_t>(ctx->cap, (int64_t)1 << 24);
   if (!rc && ctx->mixed) rc = dalloc(ctx, &ctx->stage64, (size_t)ctx->stage_n);
   if (!rc) rc = dalloc(ctx, &ctx->keep, cap);

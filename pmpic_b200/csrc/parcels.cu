@@ -18,38 +18,79 @@ int launch_mix_grids(pmpic_ctx* ctx, bool any_removed);
 namespace {
 
 inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
-constexpr int CB = 1024;  // compaction block
 
 // ---- deterministic compaction ------------------------------------------------------
 // Pred(i) -> bool over i in [0, n); list[] receives the true indices ascending.
+// A CTA of 256 threads covers CCH chunks of 256 consecutive items (thread t
+// takes item t of each chunk, so every load is coalesced and each thread has
+// CCH independent loads in flight).  Order inside a CTA is (chunk, warp,
+// lane), which is ascending item order.
+constexpr int CCH = 32;              // chunks per CTA
+constexpr int CITEMS = 256 * CCH;    // items per CTA
 template <class Pred>
-__global__ void k_count(Pred pr, int64_t n, int32_t* __restrict__ blockcnt) {
-  int64_t i = (int64_t)blockIdx.x * CB + threadIdx.x;
-  int f = (i < n) && pr(i);
-  int c = __syncthreads_count(f);
-  if (threadIdx.x == 0) blockcnt[blockIdx.x] = c;
+__global__ void __launch_bounds__(256) k_count(Pred pr, int64_t n, int32_t* __restrict__ blockcnt) {
+  __shared__ int ws[8];
+  const int64_t base = (int64_t)blockIdx.x * CITEMS + threadIdx.x;
+  int c = 0;
+#pragma unroll 8
+  for (int j = 0; j < CCH; ++j) {
+    const int64_t i = base + 256 * j;
+    c += (i < n && pr(i)) ? 1 : 0;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < 8; ++w) t += ws[w];
+    blockcnt[blockIdx.x] = t;
+  }
 }
 template <class Pred>
-__global__ void k_write(Pred pr, int64_t n, const int32_t* __restrict__ blockoff, int32_t* __restrict__ list) {
-  __shared__ int wsum[32];
-  int64_t i = (int64_t)blockIdx.x * CB + threadIdx.x;
-  int f = (i < n) && pr(i);
-  unsigned bal = __ballot_sync(0xffffffffu, f);
-  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (lane == 0) wsum[w] = __popc(bal);
-  __syncthreads();
-  if (w == 0) {
-    int v = wsum[lane];
-    for (int o = 1; o < 32; o <<= 1) {
-      int y = __shfl_up_sync(0xffffffffu, v, o);
-      if (lane >= o) v += y;
-    }
-    wsum[lane] = v;  // inclusive
+__global__ void __launch_bounds__(256) k_write(Pred pr, int64_t n, const int32_t* __restrict__ blockoff,
+                                               int32_t* __restrict__ list) {
+  __shared__ int wc[CCH * 8];  // per (chunk, warp): count, then exclusive offset within the CTA
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t base = (int64_t)blockIdx.x * CITEMS + threadIdx.x;
+  uint32_t mask = 0;
+#pragma unroll 8
+  for (int j = 0; j < CCH; ++j) {
+    const int64_t i = base + 256 * j;
+    const bool f = i < n && pr(i);
+    mask |= (uint32_t)f << j;
+    const unsigned b = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) wc[j * 8 + w] = __popc(b);
   }
   __syncthreads();
-  if (f) {
-    int r = (w > 0 ? wsum[w - 1] : 0) + __popc(bal & ((1u << lane) - 1));
-    list[blockoff[blockIdx.x] + r] = (int32_t)i;
+  if (w == 0) {  // exclusive scan of the CCH*8 counts in (chunk, warp) order, 8 per lane
+    int v[8], s = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      v[q] = wc[lane * 8 + q];
+      s += v[q];
+    }
+    int incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    int ex = incl - s;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      wc[lane * 8 + q] = ex;
+      ex += v[q];
+    }
+  }
+  __syncthreads();
+  const int32_t off = blockoff[blockIdx.x];
+  const unsigned lt = (1u << lane) - 1;
+#pragma unroll 8
+  for (int j = 0; j < CCH; ++j) {
+    const bool f = (mask >> j) & 1u;
+    const unsigned b = __ballot_sync(0xffffffffu, f);
+    if (f) list[off + wc[j * 8 + w] + __popc(b & lt)] = (int32_t)(base + 256 * j);
   }
 }
 
@@ -86,37 +127,48 @@ struct PredNewCell {
 // values, and the cells of a warp (consecutive in z) share lines.
 constexpr int PK_T = 32;  // x extent of a tile
 constexpr int PK_K = 16;  // z extent of a tile
-template <class R>
-__global__ void __launch_bounds__(256) k_pack6(Geom g, const R* __restrict__ G0, const R* __restrict__ G1,
-                                               const R* __restrict__ G2, const R* __restrict__ G3,
-                                               const R* __restrict__ G4, const R* __restrict__ G5,
-                                               R* __restrict__ out) {
+template <class R, int NF>
+__global__ void __launch_bounds__(256) k_pack(Geom g, const R* __restrict__ G0, const R* __restrict__ G1,
+                                              const R* __restrict__ G2, const R* __restrict__ G3,
+                                              const R* __restrict__ G4, const R* __restrict__ G5,
+                                              const R* __restrict__ G6, R* __restrict__ out) {
+  // NF = 6: fields G0..G5; NF = 8: G0..G6 and a zero pad
   constexpr int TS = PK_K * (PK_T + 1) + 1;  // per-field tile stride, odd
-  __shared__ R tile[6 * TS];
+  __shared__ R tile[NF * TS];
   const int i0 = blockIdx.x * PK_T, k0 = blockIdx.y * PK_K, j = blockIdx.z;
-  const R* G[6] = {G0, G1, G2, G3, G4, G5};
+  const R* G[7] = {G0, G1, G2, G3, G4, G5, G6};
   const int ni = min(PK_T, g.Nx - i0), nk = min(PK_K, g.nzp - k0);
 #pragma unroll
-  for (int f = 0; f < 6; ++f) {
+  for (int f = 0; f < NF; ++f) {
     for (int e = threadIdx.x; e < PK_K * PK_T; e += blockDim.x) {
       const int kk = e / PK_T, ii = e - kk * PK_T;
       if (kk < nk && ii < ni)
-        tile[f * TS + kk * (PK_T + 1) + ii] = G[f][((size_t)(k0 + kk) * g.Ny + j) * g.Nx + i0 + ii];
+        tile[f * TS + kk * (PK_T + 1) + ii] =
+            f < 7 ? G[f][((size_t)(k0 + kk) * g.Ny + j) * g.Nx + i0 + ii] : R(0);
     }
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < 6 * PK_K * PK_T; e += blockDim.x) {
-    const int ii = e / (6 * PK_K), r = e - ii * 6 * PK_K;
-    const int kk = r / 6, f = r - kk * 6;
+  for (int e = threadIdx.x; e < NF * PK_K * PK_T; e += blockDim.x) {
+    const int ii = e / (NF * PK_K), r = e - ii * NF * PK_K;
+    const int kk = r / NF, f = r - kk * NF;
     if (kk < nk && ii < ni)
-      out[(((size_t)(i0 + ii) * g.Ny + j) * g.nzp + k0 + kk) * 6 + f] = tile[f * TS + kk * (PK_T + 1) + ii];
+      out[(((size_t)(i0 + ii) * g.Ny + j) * g.nzp + k0 + kk) * NF + f] = tile[f * TS + kk * (PK_T + 1) + ii];
   }
 }
 template <class R>
 static void pack6(pmpic_ctx* ctx, const R* const* grids, R* out) {
   const Geom& g = ctx->g;
   dim3 gr((g.Nx + PK_T - 1) / PK_T, (g.nzp + PK_K - 1) / PK_K, g.Ny);
-  k_pack6<R><<<gr, 256, 0, ctx->stream>>>(g, grids[0], grids[1], grids[2], grids[3], grids[4], grids[5], out);
+  k_pack<R, 6><<<gr, 256, 0, ctx->stream>>>(g, grids[0], grids[1], grids[2], grids[3], grids[4], grids[5], nullptr,
+                                            out);
+  ++ctx->nlaunch;
+}
+template <class R>
+static void pack8(pmpic_ctx* ctx, const R* const* grids, R* out) {  // 7 grids + a pad
+  const Geom& g = ctx->g;
+  dim3 gr((g.Nx + PK_T - 1) / PK_T, (g.nzp + PK_K - 1) / PK_K, g.Ny);
+  k_pack<R, 8><<<gr, 256, 0, ctx->stream>>>(g, grids[0], grids[1], grids[2], grids[3], grids[4], grids[5], grids[6],
+                                            out);
   ++ctx->nlaunch;
 }
 // the six fields at the two levels of xy corner (ci, cj) of a cell of level ck:
@@ -172,7 +224,7 @@ struct RkPtrs {
   double* f[6];
   double* d[6];
   const double* grid[6];  // u, v, w, dp, dq, dr
-  const double* g6;       // the six packed (k_pack6), when both gathers are pending
+  const double* g6;       // the six packed (k_pack), when both gathers are pending
 };
 
 __device__ __forceinline__ int classify_dir(const Geom& g, double x, double y) {
@@ -557,10 +609,15 @@ __global__ void k_residual_update(Geom g, ResPtrs RP, const int32_t* __restrict_
 }
 
 // residuals onto the kept original parcels (:245-342), with the binning
-// cached at the start of mixing (:80; kept parcels have not moved)
-__global__ void __launch_bounds__(256, 3) k_redistribute(Geom g, int64_t norig, const int32_t* __restrict__ keep, double* __restrict__ parcels,
-                               int64_t cap, const int32_t* __restrict__ cell, const double* __restrict__ del,
-                               ResPtrs RP) {
+// cached at the start of mixing (:80; kept parcels have not moved).  The kept
+// volume grid and the six residual grids are read packed (k_pack, 8 fields per
+// level: vol, vres, bres, hres, pres, qres, rres, pad), the corners visited in
+// the reference's order u = 0..7 (x fastest, then y, then z).
+__global__ void __launch_bounds__(256) k_redistribute(Geom g, int64_t norig, const int32_t* __restrict__ keep,
+                                                         double* __restrict__ parcels, int64_t cap,
+                                                         const int32_t* __restrict__ cell,
+                                                         const double* __restrict__ del,
+                                                         const double* __restrict__ G8) {
   int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= norig || keep[m] != 1) return;
   auto A = [&](int pid) -> double* { return parcels + (size_t)pid * cap; };
@@ -568,11 +625,7 @@ __global__ void __launch_bounds__(256, 3) k_redistribute(Geom g, int64_t norig, 
   if (id < 0) return;
   const double delx = del[m], dely = del[cap + m], delz = del[2 * cap + m];
   const int ck = id % g.Nz, cj = (id / g.Nz) % g.Ny, ci = id / (g.Nz * g.Ny);
-  int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
-  // grid offsets fit in 32 bits (pmpic_create limits (nz+1)*ny*nx)
-  const int r0 = (ck * g.Ny + cj) * g.Nx, r1 = (ck * g.Ny + cj1) * g.Nx;
-  const int r2 = ((ck + 1) * g.Ny + cj) * g.Nx, r3 = ((ck + 1) * g.Ny + cj1) * g.Nx;
-  const int c[8] = {r0 + ci, r0 + ci1, r1 + ci, r1 + ci1, r2 + ci, r2 + ci1, r3 + ci, r3 + ci1};
+  const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
   const double v = A(PMPIC_PROP_VOL)[m];
   double w[8];
   w[0] = (1 - delz) * (1 - dely) * (1 - delx) * v;
@@ -583,32 +636,27 @@ __global__ void __launch_bounds__(256, 3) k_redistribute(Geom g, int64_t norig, 
   w[5] = (delz) * (1 - dely) * (delx) * v;
   w[6] = (delz) * (dely) * (1 - delx) * v;
   w[7] = (delz) * (dely) * (delx) * v;
-  const double* V = RP.k[0];
-  const double* vres = RP.r[0];
-  double vg[8], wv[8];
+  const int pids[5] = {PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
+  double s[5];
 #pragma unroll
-  for (int u = 0; u < 8; ++u) {
-    vg[u] = V[c[u]];
-    wv[u] = w[u] / vg[u];  // the w/vol_g factor shared by b, h, p, q, r (:280-335)
-  }
+  for (int q = 0; q < 5; ++q) s[q] = A(pids[q])[m] * v;
   double nv = v;
 #pragma unroll
-  for (int u = 0; u < 8; ++u) nv = nv + w[u] * vres[c[u]] / vg[u];  // :268-276
-  const int pids[5] = {PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
-  double fo[5];
-#pragma unroll
-  for (int q = 0; q < 5; ++q) fo[q] = A(pids[q])[m];
-#pragma unroll
-  for (int q = 0; q < 5; ++q) {
-    const double* res = RP.r[q + 1];
-    double s = fo[q] * v;
-#pragma unroll
-    for (int u = 0; u < 8; ++u) s = s + wv[u] * res[c[u]];  // :279-336
-    fo[q] = s / nv;
+  for (int u = 0; u < 8; ++u) {
+    const int x = (u & 1) ? ci1 : ci, y = (u & 2) ? cj1 : cj, z = ck + (u >> 2);
+    const double2* P = (const double2*)(G8 + (((size_t)x * g.Ny + y) * g.nzp + z) * 8);
+    const double2 a0 = P[0], a1 = P[1], a2 = P[2], a3 = P[3];  // (vol, vres) (b, h) (p, q) (r, pad)
+    const double wv = w[u] / a0.x;  // the w/vol_g factor shared by b, h, p, q, r (:280-335)
+    nv = nv + w[u] * a0.y / a0.x;   // :268-276
+    s[0] = s[0] + wv * a1.x;        // :279-336
+    s[1] = s[1] + wv * a1.y;
+    s[2] = s[2] + wv * a2.x;
+    s[3] = s[3] + wv * a2.y;
+    s[4] = s[4] + wv * a3.x;
   }
   A(PMPIC_PROP_VOL)[m] = nv;
 #pragma unroll
-  for (int q = 0; q < 5; ++q) A(pids[q])[m] = fo[q];
+  for (int q = 0; q < 5; ++q) A(pids[q])[m] = s[q] / nv;
 }
 
 // backfill (:347-389): the t-th removed slot (ascending) receives the t-th kept
@@ -634,7 +682,7 @@ __global__ void k_backfill(const int32_t* __restrict__ zlist, const int32_t* __r
 // (CellOff); the integer bookkeeping (directions, lists, slots) is shared with
 // the plain path.  Float property p of parcel n is ((float*)array_p)[n].
 struct MPtrs {
-  const float* g6;  // the six grids packed (k_pack6), when both gathers are pending
+  const float* g6;  // the six grids packed (k_pack), when both gathers are pending
   float inv[3];     // 1/dx, 1/dy, 1/dz
   CellOff* s[3];
   CellOff* o[3];
@@ -974,7 +1022,8 @@ __global__ void k_residual_update_m(Geom g, ResPtrsF RP, const int32_t* __restri
   }
 }
 __global__ void __launch_bounds__(256, 4) k_redistribute_m(Geom g, int64_t norig, const int32_t* __restrict__ keep,
-                                                          double* __restrict__ parcels, int64_t cap, ResPtrsF RP) {
+                                                          double* __restrict__ parcels, int64_t cap,
+                                                          const float* __restrict__ G8) {
   const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= norig || keep[m] != 1) return;
   auto F = [&](int pid) { return (float*)(parcels + (size_t)pid * cap); };
@@ -984,9 +1033,6 @@ __global__ void __launch_bounds__(256, 4) k_redistribute_m(Geom g, int64_t norig
   if (ci < 0 || ci >= g.Nx || cj < 0 || cj >= g.Ny || ck < 0 || ck >= g.Nz) return;  // reported by the binning
   const float delx = px.f, dely = py.f, delz = pz.f;
   const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
-  const int r0 = (ck * g.Ny + cj) * g.Nx, r1 = (ck * g.Ny + cj1) * g.Nx;
-  const int r2 = ((ck + 1) * g.Ny + cj) * g.Nx, r3 = ((ck + 1) * g.Ny + cj1) * g.Nx;
-  const int c[8] = {r0 + ci, r0 + ci1, r1 + ci, r1 + ci1, r2 + ci, r2 + ci1, r3 + ci, r3 + ci1};
   const float v = F(PMPIC_PROP_VOL)[m];
   float w[8];
   w[0] = (1.f - delz) * (1.f - dely) * (1.f - delx) * v;
@@ -997,23 +1043,27 @@ __global__ void __launch_bounds__(256, 4) k_redistribute_m(Geom g, int64_t norig
   w[5] = (delz) * (1.f - dely) * (delx) * v;
   w[6] = (delz) * (dely) * (1.f - delx) * v;
   w[7] = (delz) * (dely) * (delx) * v;
-  float wv[8];
+  const int pids[5] = {PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
+  float s[5];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) s[q] = F(pids[q])[m] * v;
   float nv = v;
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
-    wv[u] = w[u] / RP.k[0][c[u]];
-    nv = nv + wv[u] * RP.r[0][c[u]];  // :268-276
+    const int x = (u & 1) ? ci1 : ci, y = (u & 2) ? cj1 : cj, z = ck + (u >> 2);
+    const float4* P = (const float4*)(G8 + (((size_t)x * g.Ny + y) * g.nzp + z) * 8);
+    const float4 a0 = P[0], a1 = P[1];  // (vol, vres, b, h) (p, q, r, pad)
+    const float wv = w[u] / a0.x;
+    nv = nv + wv * a0.y;  // :268-276
+    s[0] = s[0] + wv * a0.z;
+    s[1] = s[1] + wv * a0.w;
+    s[2] = s[2] + wv * a1.x;
+    s[3] = s[3] + wv * a1.y;
+    s[4] = s[4] + wv * a1.z;
   }
-  const int pids[5] = {PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
   const float rnv = 1.f / nv;
 #pragma unroll
-  for (int q = 0; q < 5; ++q) {
-    const float* res = RP.r[q + 1];
-    float s = F(pids[q])[m] * v;
-#pragma unroll
-    for (int u = 0; u < 8; ++u) s = s + wv[u] * res[c[u]];  // :279-336
-    F(pids[q])[m] = s * rnv;
-  }
+  for (int q = 0; q < 5; ++q) F(pids[q])[m] = s[q] * rnv;
   F(PMPIC_PROP_VOL)[m] = nv;
 }
 __global__ void k_backfill_m(const int32_t* __restrict__ zlist, const int32_t* __restrict__ nz,
@@ -1052,17 +1102,17 @@ __global__ void k_grid2par_m(Geom g, int64_t n, const CellOff* __restrict__ X, c
 // list of i in [0,n) with pred(i), ascending; count written to *dcount (device)
 template <class Pred>
 static int compact(pmpic_ctx* ctx, Pred pr, int64_t n, int32_t* list, int32_t* dcount) {
-  int64_t nb = (n + CB - 1) / CB;
+  int64_t nb = (n + CITEMS - 1) / CITEMS;
   if (nb == 0) {
     PMPIC_CUDA(cudaMemsetAsync(dcount, 0, sizeof(int32_t), ctx->stream));
     return 0;
   }
   int32_t* cnt = ctx->aux2;            // nb + 1 (nb + 1 <= nbmax)
   int32_t* off = ctx->aux2 + ctx->nbmax;
-  k_count<<<(unsigned)nb, CB, 0, ctx->stream>>>(pr, n, cnt); ++ctx->nlaunch;
+  k_count<<<(unsigned)nb, 256, 0, ctx->stream>>>(pr, n, cnt); ++ctx->nlaunch;
   int rc = scan_excl(ctx, cnt, nb, off);
   if (rc) return rc;
-  k_write<<<(unsigned)nb, CB, 0, ctx->stream>>>(pr, n, off, list); ++ctx->nlaunch;
+  k_write<<<(unsigned)nb, 256, 0, ctx->stream>>>(pr, n, off, list); ++ctx->nlaunch;
   PMPIC_CUDA(cudaMemcpyAsync(dcount, off + nb, sizeof(int32_t), cudaMemcpyDeviceToDevice, ctx->stream));
   PMPIC_CUDA(cudaGetLastError());
   return 0;
@@ -1130,6 +1180,7 @@ int rk4_stage(pmpic_ctx* ctx, int stage) {
     ctx->pending_uvw = ctx->pending_pqr = false;
     return 0;
   }
+  TimerScope ts(ctx, T_RK4K);  // the stage kernel with its grid packing
   if (ctx->mixed) {
     MPtrs P;
     const int S[6] = {PMPIC_PROP_X, PMPIC_PROP_Y, PMPIC_PROP_Z, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
@@ -1310,7 +1361,10 @@ int mixing(pmpic_ctx* ctx) {
                                                   (float)g.vmin, ctx->dinfo); ++ctx->nlaunch;
     k_residual_update_m<<<nblk(g.nphys, 256), 256, 0, ctx->stream>>>(g, RF, ctx->newslot, por); ++ctx->nlaunch;
     if (norig > 0) {
-      k_redistribute_m<<<nblk(norig, 256), 256, 0, ctx->stream>>>(g, norig, ctx->keep, ctx->parcels, ctx->cap, RF);
+      const float* g7[7] = {KF[0], RF.r[0], RF.r[1], RF.r[2], RF.r[3], RF.r[4], RF.r[5]};
+      pack8<float>(ctx, g7, (float*)ctx->gpack);
+      k_redistribute_m<<<nblk(norig, 256), 256, 0, ctx->stream>>>(g, norig, ctx->keep, ctx->parcels, ctx->cap,
+                                                                  (const float*)ctx->gpack);
       ++ctx->nlaunch;
     }
   } else {
@@ -1324,8 +1378,10 @@ int mixing(pmpic_ctx* ctx) {
     }
     k_residual_update<<<nblk(g.nphys, 256), 256, 0, ctx->stream>>>(g, RP, ctx->newslot, ctx->newportion); ++ctx->nlaunch;
     if (norig > 0) {
+      const double* g7[7] = {K[0], RP.r[0], RP.r[1], RP.r[2], RP.r[3], RP.r[4], RP.r[5]};
+      pack8<double>(ctx, g7, ctx->gpack);
       k_redistribute<<<nblk(norig, 256), 256, 0, ctx->stream>>>(g, norig, ctx->keep, ctx->parcels, ctx->cap,
-                                                                ctx->cell, ctx->del, RP); ++ctx->nlaunch;
+                                                                ctx->cell, ctx->del, ctx->gpack); ++ctx->nlaunch;
     }
   }
   // counts to the host: removed, new cells

@@ -161,6 +161,7 @@ __global__ void k_diffz(Geom g, const real* __restrict__ f, real* __restrict__ o
   real d1 = bt ? f0 / dz - a1 * bot[col] * dz : real(0);
   real prev = d1 / DEN[0];
   out[col] = prev;
+#pragma unroll 8
   for (int k = 1; k < nz - 1; ++k) {
     real fp = f[(int64_t)(k + 1) * cs + col];
     real d = (fp - fm) / real(2) / dz;
@@ -177,6 +178,7 @@ __global__ void k_diffz(Geom g, const real* __restrict__ f, real* __restrict__ o
   }
   // back substitution: f(i) = f(i) - cp(i+1) f(i+1)
   real nxt = prev;
+#pragma unroll 8
   for (int k = nz - 2; k >= 0; --k) {
     real v = out[(int64_t)k * cs + col] - CP[k + 1] * nxt;
     out[(int64_t)k * cs + col] = v;
@@ -186,11 +188,19 @@ __global__ void k_diffz(Geom g, const real* __restrict__ f, real* __restrict__ o
 
 // laplinv (fft_ops.F90:505-601), in place, one thread per column; columns with
 // k2 == 0 keep their input (:567).  cp is kept in a scratch array.
-__global__ void k_laplinv(Geom g, real* __restrict__ f, real* __restrict__ cpbuf, const real* __restrict__ k2,
-                          int df0) {
+// blockIdx.y selects one of up to three arrays solved in the same launch
+struct LapBatch {
+  real* f[3];
+  int df0[3];
+};
+__global__ void k_laplinv(Geom g, LapBatch lb, real* __restrict__ cpbase, const real* __restrict__ k2) {
   int col = blockIdx.x * blockDim.x + threadIdx.x;
   const int cols = g.sx * g.sy;
   if (col >= cols) return;
+  const int q = blockIdx.y;  // selected without indexing the parameter arrays (no local copy)
+  real* __restrict__ f = q == 0 ? lb.f[0] : (q == 1 ? lb.f[1] : lb.f[2]);
+  real* __restrict__ cpbuf = cpbase + (size_t)q * g.nspec;
+  const int df0 = q == 0 ? lb.df0[0] : (q == 1 ? lb.df0[1] : lb.df0[2]);
   const real kk = k2[col];
   if (kk == 0) return;
   const int nz = g.nzp;
@@ -220,6 +230,7 @@ __global__ void k_laplinv(Geom g, real* __restrict__ f, real* __restrict__ cpbuf
   real prev = d / den;
   f[col] = prev;
   real cprev = c1;  // c(i-1)
+#pragma unroll 8
   for (int k = 1; k < nz; ++k) {
     fm = f0;
     f0 = fp;
@@ -240,6 +251,7 @@ __global__ void k_laplinv(Geom g, real* __restrict__ f, real* __restrict__ cpbuf
     cprev = c;
   }
   real nxt = prev;
+#pragma unroll 8
   for (int k = nz - 2; k >= 0; --k) {
     real v = f[(int64_t)k * cs + col] - cpbuf[(int64_t)(k + 1) * cs + col] * nxt;
     f[(int64_t)k * cs + col] = v;
@@ -343,13 +355,21 @@ int spec_filter_impl(pmpic_ctx* ctx, const real* in, real* out) {
 int spec_diffz_impl(pmpic_ctx* ctx, const real* in, real* out, const real* bot, const real* top) {
   return diffz_launch_impl(ctx, in, out, bot, top);
 }
-int spec_laplinv_impl(pmpic_ctx* ctx, real* inout, bool df0) {
+// laplinv of na (1..3) arrays in one launch; the Thomas factors of array q go
+// to the scratch at q * nspec
+int spec_laplinv_batch(pmpic_ctx* ctx, int na, real* const* fs, const bool* df0) {
   TimerScope ts(ctx, T_LAPLINV);
   const Geom& g = ctx->g;
-  k_laplinv<<<nblk((int64_t)g.sx * g.sy, 128), 128, 0, ctx->stream>>>(g, inout, RP(ctx->sscratch), tab_k2(ctx), df0 ? 1 : 0); ++ctx->nlaunch;
+  LapBatch lb{};
+  for (int q = 0; q < na; ++q) {
+    lb.f[q] = fs[q];
+    lb.df0[q] = df0[q] ? 1 : 0;
+  }
+  k_laplinv<<<dim3(nblk((int64_t)g.sx * g.sy, 128), na), 128, 0, ctx->stream>>>(g, lb, RP(ctx->lapcp), tab_k2(ctx)); ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
+int spec_laplinv_impl(pmpic_ctx* ctx, real* inout, bool df0) { return spec_laplinv_batch(ctx, 1, &inout, &df0); }
 
 // vort2vel.F90:139-320 after the three par2grid calls (grids P, Q, R hold the
 // gridded vorticity on entry; on exit they hold the corrected, filtered
@@ -378,9 +398,11 @@ int vort2vel_spectral_impl(pmpic_ctx* ctx) {
   if ((rc = fft_backward(ctx, e, G[PMPIC_GRID_Q]))) return rc;
   if ((rc = fft_backward(ctx, f, G[PMPIC_GRID_R]))) return rc;
   if ((rc = zero_mode_launch(ctx, d, e))) return rc;
-  if ((rc = spec_laplinv_impl(ctx, a, false))) return rc;
-  if ((rc = spec_laplinv_impl(ctx, b, false))) return rc;
-  if ((rc = spec_laplinv_impl(ctx, c, true))) return rc;
+  {
+    real* abc[3] = {a, b, c};
+    const bool df[3] = {false, false, true};
+    if ((rc = spec_laplinv_batch(ctx, 3, abc, df))) return rc;
+  }
   const real* atop = RP(ctx->bt);
   const real* abot = RP(ctx->bt) + cols;
   const real* btop = RP(ctx->bt) + 2 * cols;
