@@ -191,6 +191,13 @@ def algorithmic_bytes(kernel, precision, n_avg, nphys, calls, steps):
     return None
 
 
+# DRAM bytes per parcel of one launch, from ncu captures of the same kernels on
+# the 128^3 plume (16.8 M parcels; these kernels stream the parcel state once, so
+# traffic scales with parcels): RK4 stages 1-2 averaged, par2grid vort2vel pass.
+TRAFFIC_PER_PARCEL = {("rk4_kernel", "fp64"): 272.0, ("rk4_kernel", "mixed"): 181.0,
+                      ("par2grid", "fp64"): 100.0, ("par2grid", "mixed"): 56.0}
+
+
 def run_form(precision, args, local, pg, headline):
     """One context of `precision`: W warm-up steps, K timed steps (CUDA events on
     the library's stream, clocks sampled), then untimed steps up to
@@ -253,7 +260,9 @@ def run_form(precision, args, local, pg, headline):
     achieved = total_bytes / (tot / 1e3) / 1e9 if calls and tot > 0 else None
     res["roofline"] = {
         "bound": "hbm", "kernel": best, "achieved": achieved, "peak": peak, "unit": "GB/s",
-        "frac": (achieved / peak) if achieved else None, "traffic": None,
+        "frac": (achieved / peak) if achieved else None,
+        "traffic": TRAFFIC_PER_PARCEL.get((best, precision), 0.0) * n_avg or None,
+        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per parcel at 128^3, scaled by parcels",
         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
         "share_of_step": tot / step_ms if step_ms else None, "launches": calls,
         "avg_launch_ms": tot / calls if calls else None,
