@@ -171,7 +171,26 @@ int pmpic_op_laplinv(pmpic_ctx* ctx, double* inout, int df_zero_on_boundary);
 /* parcel_haloswap (parcels/haloswap.F90:109-289), single-GPU semantics. */
 int pmpic_op_parcel_haloswap(pmpic_ctx* ctx);
 
-/* par2grid without a context and without allocation.  No counterpart in the
+/* par2grid (parcel_interpolation.F90:336-481) of nf (1, 3 or 4) properties into
+ * nf grids with one set of weights, in the context's precision (the mixed form
+ * takes FP32 properties only). */
+int pmpic_op_par2grid_multi(pmpic_ctx* ctx, int nf, const int* props, const int* grids);
+/* grid2par (parcel_interpolation.F90:267-332) of ng (1, 3 or 6) grids into ng
+ * properties at the current positions. */
+int pmpic_op_grid2par_multi(pmpic_ctx* ctx, int ng, const int* grids, const int* props);
+/* The inversion of vort2vel.F90:139-320 alone, on the gridded vorticity
+ * already in grids p, q, r: velocity into u, v, w, corrected vorticity into
+ * p, q, r, filtered spectra into u_s, v_s, w_s.  Both precisions. */
+int pmpic_op_vort2vel_grids(pmpic_ctx* ctx);
+/* Renumbers parcel slots into cell order (cell id z fastest, slot order kept
+ * inside a cell), moving every property.  No counterpart in the reference,
+ * whose slot order is part of its integer bookkeeping: use it where slot
+ * numbering does not matter (e.g. after set-up, before a run) to make the
+ * parcel gathers of par2grid and the RK4 stage contiguous.  Allocates a
+ * temporary device buffer of n doubles. */
+int pmpic_sort_parcels(pmpic_ctx* ctx);
+
+/* par2grid without a context and without allocation./* par2grid without a context and without allocation.  No counterpart in the
  * reference: an addition for callers that cannot allocate device memory at call
  * time.  Same arithmetic and result as pmpic_op_par2grid (binning
  * parcel_interpolation.F90:186-262, par2grid :336-481) of one field with volume

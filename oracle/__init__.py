@@ -74,7 +74,7 @@ def lib():
         L.orc_laplinv.argtypes = [P, D, C.c_int]
         L.orc_filter.argtypes = [P, D, D]
         L.orc_kx_ky_k2.argtypes = [P, D, D, D, D]
-        for n in ["orc_parcel_haloswap", "orc_vort2vel", "orc_vorticity_tendency",
+        for n in ["orc_parcel_haloswap", "orc_vort2vel", "orc_vort2vel_grids", "orc_vorticity_tendency",
                   "orc_rk4_integrator", "orc_parcel_splitting", "orc_parcel_mixing", "orc_step"]:
             getattr(L, n).argtypes = [P]
         L.orc_get_counters.argtypes = [P, C.POINTER(C.c_int)]
@@ -245,6 +245,10 @@ class Oracle:
     # -- components -----------------------------------------------------------
     def vort2vel(self):
         self._check(lib().orc_vort2vel(self._h))
+
+    def vort2vel_grids(self):
+        """The inversion alone (vort2vel.F90:139-320) of grids p, q, r."""
+        self._check(lib().orc_vort2vel_grids(self._h))
 
     def vorticity_tendency(self):
         self._check(lib().orc_vorticity_tendency(self._h))

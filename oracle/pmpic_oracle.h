@@ -99,6 +99,8 @@ int orc_kx_ky_k2(orc_ctx*, double* kx, double* ky, double* k2, double* filt);
 
 /* Component callbacks (one call = one timestep callback of the component). */
 int orc_vort2vel(orc_ctx*);
+/* vort2vel.F90:139-320 alone: the inversion of the gridded vorticity (grids p, q, r). */
+int orc_vort2vel_grids(orc_ctx*);
 int orc_vorticity_tendency(orc_ctx*);
 int orc_rk4_integrator(orc_ctx*);
 int orc_parcel_splitting(orc_ctx*);

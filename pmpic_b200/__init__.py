@@ -114,6 +114,11 @@ def lib() -> C.CDLL:
         L.pmpic_op_filter.argtypes = [P, D, D]
         L.pmpic_op_diffz.argtypes = [P, D, D, D, D]
         L.pmpic_op_laplinv.argtypes = [P, D, C.c_int]
+        IP = C.POINTER(C.c_int)
+        L.pmpic_op_par2grid_multi.argtypes = [P, C.c_int, IP, IP]
+        L.pmpic_op_grid2par_multi.argtypes = [P, C.c_int, IP, IP]
+        L.pmpic_op_vort2vel_grids.argtypes = [P]
+        L.pmpic_sort_parcels.argtypes = [P]
         L.pmpic_timing.argtypes = [P, C.c_int]
         L.pmpic_timer_count.argtypes = []
         L.pmpic_timer_name.restype = C.c_char_p
@@ -293,6 +298,26 @@ class Context:
 
     def grid2par(self, grid, prop):
         self._check(lib().pmpic_op_grid2par(self._h, GRID[grid], PROP[prop]))
+
+    def par2grid_multi(self, props, grids):
+        """par2grid of 1, 3 or 4 properties into as many grids, one set of weights."""
+        a = (C.c_int * len(props))(*[PROP[p] for p in props])
+        b = (C.c_int * len(grids))(*[GRID[g] for g in grids])
+        self._check(lib().pmpic_op_par2grid_multi(self._h, len(props), a, b))
+
+    def grid2par_multi(self, grids, props):
+        """grid2par of 1, 3 or 6 grids into as many properties."""
+        a = (C.c_int * len(grids))(*[GRID[g] for g in grids])
+        b = (C.c_int * len(props))(*[PROP[p] for p in props])
+        self._check(lib().pmpic_op_grid2par_multi(self._h, len(grids), a, b))
+
+    def vort2vel_grids(self):
+        """vort2vel's inversion alone on the vorticity in grids p, q, r."""
+        self._check(lib().pmpic_op_vort2vel_grids(self._h))
+
+    def sort_parcels(self):
+        """Renumber slots into cell order (not a reference operation)."""
+        self._check(lib().pmpic_sort_parcels(self._h))
 
     def parcel_haloswap(self):
         self._check(lib().pmpic_op_parcel_haloswap(self._h))

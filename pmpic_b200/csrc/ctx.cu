@@ -863,6 +863,112 @@ int pmpic_op_laplinv(pmpic_ctx* ctx, double* inout, int df0) {
   if ((rc = d2h(ctx, inout, ctx->sa, ctx->g.nspec))) return rc;
   return sync_info(ctx);
 }
+int pmpic_op_vort2vel_grids(pmpic_ctx* ctx) {
+  if (!ctx) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  int rc = vort2vel_spectral(ctx);
+  if (rc) return rc;
+  return sync_info(ctx);
+}
+
+int pmpic_op_par2grid_multi(pmpic_ctx* ctx, int nf, const int* props, const int* grids) {
+  if (!ctx || !props || !grids || (nf != 1 && nf != 3 && nf != 4)) return PMPIC_ERR_ARG;
+  for (int q = 0; q < nf; ++q)
+    if (props[q] < 0 || props[q] >= PMPIC_NPROP || grids[q] < 0 || grids[q] >= PMPIC_NGRID) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  int rc = flush_gathers(ctx);
+  if (rc) return rc;
+  if ((rc = bin_and_sort(ctx))) return rc;
+  if (ctx->mixed) {
+    const float* f[4];
+    float* o[4];
+    for (int q = 0; q < nf; ++q) {
+      if (mixed_elem_bytes(props[q]) != 4) return set_error(ctx, PMPIC_ERR_ARG, "par2grid of a position or tag");
+      f[q] = propf(ctx, props[q]);
+      o[q] = (float*)ctx->grid[grids[q]];
+    }
+    rc = par2grid_multi_m(ctx, f, nf, o);
+  } else {
+    const double* f[4];
+    double* o[4];
+    for (int q = 0; q < nf; ++q) {
+      f[q] = prop(ctx, props[q]);
+      o[q] = ctx->grid[grids[q]];
+    }
+    rc = par2grid_multi(ctx, f, nf, o, false);
+  }
+  if (rc) return rc;
+  ctx->btot_grid_ready = false;
+  return sync_info(ctx);
+}
+
+int pmpic_op_grid2par_multi(pmpic_ctx* ctx, int ng, const int* grids, const int* props) {
+  if (!ctx || !props || !grids || (ng != 1 && ng != 3 && ng != 6)) return PMPIC_ERR_ARG;
+  for (int q = 0; q < ng; ++q)
+    if (props[q] < 0 || props[q] >= PMPIC_NPROP || grids[q] < 0 || grids[q] >= PMPIC_NGRID) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  int rc = flush_gathers(ctx);
+  if (rc) return rc;
+  if (ctx->mixed) {
+    const float* gr[6];
+    float* o[6];
+    for (int q = 0; q < ng; ++q) {
+      if (mixed_elem_bytes(props[q]) != 4) return set_error(ctx, PMPIC_ERR_ARG, "grid2par into a position or tag");
+      gr[q] = (const float*)ctx->grid[grids[q]];
+      o[q] = propf(ctx, props[q]);
+    }
+    if ((rc = bin_and_sort(ctx))) return rc;  // validates the positions (out-of-box error)
+    rc = grid2par_multi_m(ctx, gr, ng, o);
+  } else {
+    const double* gr[6];
+    double* o[6];
+    for (int q = 0; q < ng; ++q) {
+      gr[q] = ctx->grid[grids[q]];
+      o[q] = prop(ctx, props[q]);
+    }
+    rc = grid2par_multi(ctx, gr, ng, o);
+  }
+  if (rc) return rc;
+  return sync_info(ctx);
+}
+
+namespace {
+__global__ void k_permute(int64_t n, const int32_t* __restrict__ perm, const void* __restrict__ src,
+                          void* __restrict__ dst, int es) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  if (es == 8) ((double*)dst)[q] = ((const double*)src)[perm[q]];
+  else ((float*)dst)[q] = ((const float*)src)[perm[q]];
+}
+}  // namespace
+
+int pmpic_sort_parcels(pmpic_ctx* ctx) {
+  if (!ctx) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  int rc = flush_gathers(ctx);
+  if (rc) return rc;
+  const int64_t n = ctx->n;
+  if (n == 0) return PMPIC_OK;
+  if ((rc = bin_and_sort(ctx))) return rc;
+  if ((rc = sync_info(ctx))) return rc;  // every parcel binned (else out of box)
+  void* tmp = nullptr;
+  PMPIC_CUDA(cudaMalloc(&tmp, sizeof(double) * (size_t)n));
+  for (int p = 0; p < PMPIC_NPROP && !rc; ++p) {
+    const int es = ctx->mixed ? mixed_elem_bytes(p) : 8;
+    k_permute<<<cblk(n), 256, 0, ctx->stream>>>(n, ctx->sorted, prop(ctx, p), tmp, es);
+    ++ctx->nlaunch;
+    cudaError_t e = cudaMemcpyAsync(prop(ctx, p), tmp, (size_t)es * n, cudaMemcpyDeviceToDevice, ctx->stream);
+    if (e != cudaSuccess) rc = cuda_fail(ctx, e, "cudaMemcpyAsync", __LINE__);
+  }
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(tmp);
+  if (rc) return rc;
+  ctx->sorted_valid = false;
+  ctx->btot_grid_ready = false;
+  ctx->dir_ready = false;
+  return sync_info(ctx);
+}
+
 int pmpic_op_parcel_haloswap(pmpic_ctx* ctx) {
   if (!ctx) return PMPIC_ERR_ARG;
   cudaSetDevice(ctx->device);

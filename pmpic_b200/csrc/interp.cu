@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <mutex>
+#include <type_traits>
 
 #include "common.cuh"
 
@@ -718,7 +719,8 @@ int par2grid_multi(pmpic_ctx* ctx, const double* const* fields, int nf, double* 
   switch (nf) {
     case 1: return launch_p2g<1, 0, false>(ctx, fields, out);
     case 3: return launch_p2g<3, 0, false>(ctx, fields, out);
-    default: return set_error(ctx, PMPIC_ERR_ARG, "par2grid_multi: 1 or 3 fields");
+    case 4: return launch_p2g<4, 0, false>(ctx, fields, out);
+    default: return set_error(ctx, PMPIC_ERR_ARG, "par2grid_multi: 1, 3 or 4 fields");
   }
 }
 
@@ -734,6 +736,57 @@ static int launch_g2p(pmpic_ctx* ctx, const double* const* grids, double* const*
   }
   k_grid2par<NG><<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(g, ctx->n, ctx->cell, ctx->del, ctx->cap, a);
   ++ctx->nlaunch;
+  PMPIC_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// grid2par of NG FP32 grids at the mixed form's {cell, offset} positions
+template <int NG>
+__global__ void k_grid2par_mt(Geom g, int64_t n, const CellOff* __restrict__ X, const CellOff* __restrict__ Y,
+                              const CellOff* __restrict__ Z, G2PArgs<NG> a) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const CellOff x = X[t], y = Y[t], z = Z[t];
+  const int ci = x.i, cj = y.i, ck = z.i;
+  if (ci < 0 || ci >= g.Nx || cj < 0 || cj >= g.Ny || ck < 0 || ck >= g.Nz) return;  // reported by the binning
+  const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
+  const size_t r00 = ((size_t)ck * g.Ny + cj) * g.Nx, r01 = ((size_t)ck * g.Ny + cj1) * g.Nx;
+  const size_t r10 = ((size_t)(ck + 1) * g.Ny + cj) * g.Nx, r11 = ((size_t)(ck + 1) * g.Ny + cj1) * g.Nx;
+  const float delx = x.f, dely = y.f, delz = z.f;
+#pragma unroll
+  for (int q = 0; q < NG; ++q) {
+    const float* G = (const float*)a.grid[q];
+    const float c00 = G[r00 + ci] * (1.f - delz) + G[r10 + ci] * delz;
+    const float c01 = G[r00 + ci1] * (1.f - delz) + G[r10 + ci1] * delz;
+    const float c10 = G[r01 + ci] * (1.f - delz) + G[r11 + ci] * delz;
+    const float c11 = G[r01 + ci1] * (1.f - delz) + G[r11 + ci1] * delz;
+    const float c0 = c00 * (1.f - dely) + c10 * dely;
+    const float c1 = c01 * (1.f - dely) + c11 * dely;
+    ((float*)a.out[q])[t] = c0 * (1.f - delx) + c1 * delx;
+  }
+}
+
+// the mixed form's grid2par of ng FP32 grids into FP32 properties (1, 3 or 6)
+int grid2par_multi_m(pmpic_ctx* ctx, const float* const* grids, int ng, float* const* out) {
+  TimerScope ts(ctx, T_G2P);
+  if (ctx->n == 0) return 0;
+  auto run = [&](auto tag) {
+    constexpr int NG = decltype(tag)::value;
+    G2PArgs<NG> a;
+    for (int q = 0; q < NG; ++q) {
+      a.grid[q] = (const double*)grids[q];
+      a.out[q] = (double*)out[q];
+    }
+    k_grid2par_mt<NG><<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, propc(ctx, PMPIC_PROP_X),
+                                                                   propc(ctx, PMPIC_PROP_Y), propc(ctx, PMPIC_PROP_Z), a);
+    ++ctx->nlaunch;
+  };
+  switch (ng) {
+    case 1: run(std::integral_constant<int, 1>{}); break;
+    case 3: run(std::integral_constant<int, 3>{}); break;
+    case 6: run(std::integral_constant<int, 6>{}); break;
+    default: return set_error(ctx, PMPIC_ERR_ARG, "grid2par_multi_m: 1, 3 or 6 grids");
+  }
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
