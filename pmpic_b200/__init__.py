@@ -158,6 +158,44 @@ def thermal_parcels(nx, ny, nz, lx=2 * np.pi, ly=2 * np.pi, lz=np.pi, sub=2, jit
     return out
 
 
+def random_vorticity(nx, ny, nz, lx=2 * np.pi, ly=2 * np.pi, lz=np.pi, kmax=64, seed=4, rms=1.0):
+    """Divergence-free random vorticity on the (nz+1) x ny x nx grid (host set-up,
+    not on the hot path): omega = curl B with B_x, B_y ~ cos(kz z) and B_z ~ sin(kz z),
+    so omega_x, omega_y ~ sin(kz z) vanish at the walls z = 0, lz (free slip) and
+    omega_z ~ cos(kz z).  Mode amplitudes N(0, 1) * |k|^(-11/6) for 0 < |k| <= kmax
+    give an isotropic k^(-5/3) energy spectrum; the result is scaled to the given
+    RMS over the grid.  Returns (p, q, r) = (omega_x, omega_y, omega_z)."""
+    rng = np.random.default_rng(seed)
+    a = np.fft.rfftfreq(nx, 1.0 / nx)               # x mode numbers 0..nx/2
+    b = np.fft.fftfreq(ny, 1.0 / ny)                # y mode numbers
+    mmax = int(min(kmax * lz / np.pi, nz))
+    m = np.arange(mmax + 1)
+    kx = (2 * np.pi / lx) * a[None, None, :]
+    ky = (2 * np.pi / ly) * b[None, :, None]
+    kz = (np.pi / lz) * m[:, None, None]
+    kk = np.sqrt(kx ** 2 + ky ** 2 + kz ** 2)
+    amp = np.where((kk > 0) & (kk <= kmax), np.power(np.where(kk > 0, kk, 1.0), -11.0 / 6.0), 0.0)
+    shape = amp.shape
+
+    def coef():
+        return amp * (rng.standard_normal(shape) + 1j * rng.standard_normal(shape))
+    cx, cy, cz = coef(), coef(), coef()
+    # spectral coefficients of the vorticity per (m, ky, kx): curl of B
+    wx = 1j * ky * cz + kz * cy      # times sin(kz z)
+    wy = -kz * cx - 1j * kx * cz     # times sin(kz z)
+    wz = 1j * kx * cy - 1j * ky * cx  # times cos(kz z)
+    zk = np.arange(nz + 1) * (lz / nz)
+    sin_t = np.sin(np.outer(zk, (np.pi / lz) * m))   # (nz+1, M)
+    cos_t = np.cos(np.outer(zk, (np.pi / lz) * m))
+
+    def synth(w, basis):
+        planes = np.fft.irfft2(w, s=(ny, nx), axes=(1, 2)) * (nx * ny)  # (M, ny, nx)
+        return (basis @ planes.reshape(len(m), -1)).reshape(nz + 1, ny, nx)
+    p, q, r = synth(wx, sin_t), synth(wy, sin_t), synth(wz, cos_t)
+    scale = rms / np.sqrt((p ** 2 + q ** 2 + r ** 2).mean() / 3.0)
+    return p * scale, q * scale, r * scale
+
+
 class Context:
     """One device-resident model state (the reference's model_state_type)."""
 
