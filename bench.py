@@ -393,6 +393,178 @@ def run_b200(args):
     return 0
 
 
+def fourier_field(x, y, z, nmodes, kmax, rng, lx=2 * np.pi, ly=2 * np.pi, lz=np.pi):
+    """Sum of nmodes random Fourier modes with |k| <= kmax and N(0, 1) amplitudes:
+    periodic in x and y, cos(m pi z / lz) in z (the walls' natural condition)."""
+    out = np.zeros(np.broadcast(x, y, z).shape)
+    done = 0
+    while done < nmodes:
+        a, b, m = rng.integers(-kmax, kmax + 1), rng.integers(-kmax, kmax + 1), rng.integers(0, kmax + 1)
+        kx, ky, kz = 2 * np.pi * a / lx, 2 * np.pi * b / ly, np.pi * m / lz
+        if not (0 < kx * kx + ky * ky + kz * kz <= kmax * kmax):
+            continue
+        amp, ph = rng.standard_normal(), rng.uniform(0, 2 * np.pi)
+        out += amp * np.cos(kx * x + ky * y + ph) * np.cos(kz * z)
+        done += 1
+    return out
+
+
+def event_ms(L, h, fn, reps):
+    """Mean device time of fn() over reps calls, CUDA events on the context's stream."""
+    L.pmpic_event_record(h, 4)
+    for _ in range(reps):
+        fn()
+    L.pmpic_event_record(h, 5)
+    ms = C.c_float()
+    L.pmpic_event_elapsed(h, 4, 5, C.byref(ms))
+    return ms.value / reps
+
+
+def run_interp(args):
+    """Interpolation microbenchmark: 128^3 grid, 8 parcels per cell at seeded
+    uniform-random positions; par2grid of 4 fields and grid2par of 6 fields,
+    FP64 vs the mixed form, in the given (random) slot order and after the
+    parcels are renumbered into cell order; binning checked against the oracle."""
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    import torch
+    torch.cuda.set_device(local)
+    import pmpic_b200 as pm
+    from oracle import Oracle
+    G = args.grid if args.grid != 256 else 128
+    P = 8 * G ** 3
+    rng = np.random.default_rng(2)
+    x = rng.uniform(0, 2 * np.pi, P)
+    y = rng.uniform(0, 2 * np.pi, P)
+    z = rng.uniform(0, np.pi, P)
+    vol = np.full(P, (2 * np.pi / G) ** 2 * (np.pi / G) / 8)
+    frng = np.random.default_rng(3)
+    fields = {q: fourier_field(x, y, z, 16, 8, frng) for q in ("p", "q", "r", "b")}
+    zg, yg, xg = np.meshgrid(np.arange(G + 1) * (np.pi / G), np.arange(G) * (2 * np.pi / G),
+                             np.arange(G) * (2 * np.pi / G), indexing="ij")
+    grids = {g: fourier_field(xg, yg, zg, 16, 8, frng) for g in ("u", "v", "w", "dp", "dq", "dr")}
+    o = Oracle(G, G, G, 2 * np.pi, 2 * np.pi, np.pi, max_parcels=P, threads=os.cpu_count() or 1)
+    o.set_parcels(x=x, y=y, z=z, vol=vol)
+    ref_cells = o.cache_weights()
+    o.close()
+    p4, g6 = ["p", "q", "r", "b"], ["u", "v", "w", "dp", "dq", "dr"]
+    props6 = ["dxdt", "dydt", "dzdt", "dpdt", "dqdt", "drdt"]
+    res, outs = {}, {}
+    for prec in ("fp64", "mixed"):
+        ctx = pm.Context(G, G, G, 2 * np.pi, 2 * np.pi, np.pi, max_parcels=P, device=local, precision=prec)
+        ctx.upload(x=x, y=y, z=z, vol=vol, **fields, tag=np.arange(P, dtype=np.float64))
+        for g in g6:
+            ctx.set_grid(g, grids[g])
+        L, h = pm.lib(), ctx._h
+        mism = int(np.count_nonzero(ctx.cell_ids() != ref_cells))
+        r = {"binning_mismatches_vs_oracle": mism}
+        for order in ("random", "cell"):
+            if order == "cell":
+                ctx.sort_parcels()
+            ctx.par2grid_multi(p4, p4)
+            ctx.grid2par_multi(g6, props6)
+            t_p = event_ms(L, h, lambda: ctx.par2grid_multi(p4, p4), args.steps)
+            t_g = event_ms(L, h, lambda: ctx.grid2par_multi(g6, props6), args.steps)
+            r[order] = {"par2grid4_ms": t_p, "grid2par6_ms": t_g, "pair_parcels_per_s": P / ((t_p + t_g) / 1e3)}
+            if order == "random":
+                outs[prec] = {"grids": {q: ctx.grid(q) for q in p4}, "gath": {q: ctx.get(q) for q in props6}}
+        res[prec] = r
+        ctx.close()
+    err = {}
+    for q in p4:
+        a, b = outs["mixed"]["grids"][q], outs["fp64"]["grids"][q]
+        err["par2grid_" + q + "_rel_l2"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    for q in props6:
+        a, b = outs["mixed"]["gath"][q], outs["fp64"]["gath"][q]
+        err["grid2par_" + q + "_rel_l2"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    peak, peak_kind = hbm_peak()
+    # algorithmic bytes of the pair per parcel: par2grid reads positions (FP64 24 B; mixed: 3 int + 3 float
+    # cell slots, 24 B) + vol + 4 fields, writes the cell and (FP64) 3 offsets; grid2par reads the cell /
+    # positions and writes 6 values; plus 4 grids written and 6 read
+    bp = {"fp64": 24 + 28 + 8 + 32 + 28 + 48, "mixed": 24 + 4 + 4 + 16 + 24 + 24}
+    nph = (G + 1) * G * G
+    line = {"workload": "interp", "metric": "interpolation pairs (par2grid 4 fields + grid2par 6 fields), parcels/s",
+            "unit": "parcels/s", "higher_is_better": True, "value": res["mixed"]["cell"]["pair_parcels_per_s"],
+            "config": {"grid": G, "parcels": P, "positions": "uniform random, seed 2",
+                       "fields": "16 random Fourier modes |k|<=8, N(0,1) amplitudes, seed 3",
+                       "timing": f"CUDA events, mean of {args.steps} calls after one warm-up; par2grid includes the binning and cell sort"},
+            "fp64": res["fp64"], "mixed": res["mixed"], "mixed_vs_fp64": err,
+            "roofline": {prec: {order: {"achieved_gbs": (bp[prec] * P + (10 * nph * (8 if prec == "fp64" else 4)))
+                                        / ((res[prec][order]["par2grid4_ms"] + res[prec][order]["grid2par6_ms"]) / 1e3) / 1e9,
+                                        "peak_gbs": peak}
+                                for order in ("random", "cell")} for prec in ("fp64", "mixed")},
+            "peak_source": peak_kind}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_vort2vel(args):
+    """vort2vel's inversion alone at 256^3 on a random divergence-free vorticity
+    (k^-5/3 spectrum cut at k = 64, unit RMS, wall conditions): FP64 vs the mixed
+    form (FP32 transforms, FP64 zero mode), errors against the FP64 oracle."""
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    import torch
+    torch.cuda.set_device(local)
+    import pmpic_b200 as pm
+    from oracle import Oracle
+    G = args.grid
+    p, q, r = pm.random_vorticity(G, G, G, kmax=64, seed=4)
+    res, vel = {}, {}
+    for prec in ("fp64", "mixed"):
+        ctx = pm.Context(G, G, G, 2 * np.pi, 2 * np.pi, np.pi, max_parcels=16, device=local, precision=prec)
+        L, h = pm.lib(), ctx._h
+
+        def load():
+            ctx.set_grid("p", p)
+            ctx.set_grid("q", q)
+            ctx.set_grid("r", r)
+        load()
+        ctx.vort2vel_grids()
+        vel[prec] = {k: ctx.grid(k) for k in ("u", "v", "w")}
+        load()
+        ctx.vort2vel_grids()  # warm-up
+        res[prec] = {"ms_per_call": event_ms(L, h, ctx.vort2vel_grids, args.steps)}
+        ctx.close()
+    o = Oracle(G, G, G, 2 * np.pi, 2 * np.pi, np.pi, max_parcels=16, threads=os.cpu_count() or 1)
+    o.set_grid("p", p)
+    o.set_grid("q", q)
+    o.set_grid("r", r)
+    t0 = time.perf_counter()
+    o.vort2vel_grids()
+    t_cpu = time.perf_counter() - t0
+    ref = {k: o.grid(k) for k in ("u", "v", "w")}
+    o.close()
+    err = {}
+    for prec in ("fp64", "mixed"):
+        for k in ("u", "v", "w"):
+            d = vel[prec][k] - ref[k]
+            err[f"{prec}_{k}_rel_l2"] = float(np.linalg.norm(d) / np.linalg.norm(ref[k]))
+            err[f"{prec}_{k}_max_abs"] = float(np.abs(d).max())
+    nspec = (G + 1) * (G + 2) * (G + 2)
+    nph = (G + 1) * G * G
+    peak, peak_kind = hbm_peak()
+    roof = {}
+    for prec in ("fp64", "mixed"):
+        w = 8 if prec == "fp64" else 4
+        alg = w * 12 * nph  # 3 grids in, 9 out (corrected p, q, r; u, v, w; u_s, v_s, w_s)
+        passes = w * 9 * 4 * nspec  # 9 transforms x 2 passes x (read + write)
+        t = res[prec]["ms_per_call"] / 1e3
+        roof[prec] = {"algorithmic_gbs": alg / t / 1e9, "pass_model_gbs": passes / t / 1e9, "peak_gbs": peak}
+    line = {"workload": "vort2vel", "metric": "vort2vel inversion at 256^3, ms per call", "unit": "ms",
+            "higher_is_better": False, "value": res["mixed"]["ms_per_call"],
+            "config": {"grid": G, "vorticity": "divergence-free, k^-5/3 energy spectrum, |k|<=64, unit RMS, seed 4",
+                       "timing": f"CUDA events, mean of {args.steps} calls after one warm-up"},
+            "fp64": res["fp64"], "mixed": res["mixed"], "error_vs_oracle": err, "roofline": roof,
+            "peak_source": peak_kind,
+            "cpu_baseline": {"value": 1e3 * t_cpu, "unit": "ms", "cores": os.cpu_count() or 1, "kind": "port",
+                             "sample": "one call of the C++ restatement (oracle) at the same size"}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -408,9 +580,16 @@ def main():
                     help="both: time FP64 then the mixed form (the headline value), and compare them")
     ap.add_argument("--error-steps", type=int, default=100,
                     help="total steps per form before the gridded velocities are compared (0: no check)")
+    ap.add_argument("--workload", default="plume", choices=["plume", "interp", "vort2vel"],
+                    help="plume: the headline step; interp: the interpolation microbenchmark (128^3); "
+                         "vort2vel: the inversion alone (256^3)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "interp":
+        return run_interp(args)
+    if args.workload == "vort2vel":
+        return run_vort2vel(args)
     return run_b200(args)
 
 

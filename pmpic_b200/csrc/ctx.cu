@@ -917,8 +917,7 @@ int pmpic_op_grid2par_multi(pmpic_ctx* ctx, int ng, const int* grids, const int*
       gr[q] = (const float*)ctx->grid[grids[q]];
       o[q] = propf(ctx, props[q]);
     }
-    if ((rc = bin_and_sort(ctx))) return rc;  // validates the positions (out-of-box error)
-    rc = grid2par_multi_m(ctx, gr, ng, o);
+    rc = grid2par_multi_m(ctx, gr, ng, o);  // reports positions outside the grid
   } else {
     const double* gr[6];
     double* o[6];

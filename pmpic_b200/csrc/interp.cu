@@ -743,12 +743,15 @@ static int launch_g2p(pmpic_ctx* ctx, const double* const* grids, double* const*
 // grid2par of NG FP32 grids at the mixed form's {cell, offset} positions
 template <int NG>
 __global__ void k_grid2par_mt(Geom g, int64_t n, const CellOff* __restrict__ X, const CellOff* __restrict__ Y,
-                              const CellOff* __restrict__ Z, G2PArgs<NG> a) {
+                              const CellOff* __restrict__ Z, G2PArgs<NG> a, DevInfo* info) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const CellOff x = X[t], y = Y[t], z = Z[t];
   const int ci = x.i, cj = y.i, ck = z.i;
-  if (ci < 0 || ci >= g.Nx || cj < 0 || cj >= g.Ny || ck < 0 || ck >= g.Nz) return;  // reported by the binning
+  if (ci < 0 || ci >= g.Nx || cj < 0 || cj >= g.Ny || ck < 0 || ck >= g.Nz) {  // outside the grid: nothing read
+    atomicCAS(&info->error, 0, PMPIC_ERR_OUT_OF_BOX);
+    return;
+  }
   const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
   const size_t r00 = ((size_t)ck * g.Ny + cj) * g.Nx, r01 = ((size_t)ck * g.Ny + cj1) * g.Nx;
   const size_t r10 = ((size_t)(ck + 1) * g.Ny + cj) * g.Nx, r11 = ((size_t)(ck + 1) * g.Ny + cj1) * g.Nx;
@@ -778,7 +781,8 @@ int grid2par_multi_m(pmpic_ctx* ctx, const float* const* grids, int ng, float* c
       a.out[q] = (double*)out[q];
     }
     k_grid2par_mt<NG><<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, propc(ctx, PMPIC_PROP_X),
-                                                                   propc(ctx, PMPIC_PROP_Y), propc(ctx, PMPIC_PROP_Z), a);
+                                                                   propc(ctx, PMPIC_PROP_Y), propc(ctx, PMPIC_PROP_Z), a,
+                                                                   ctx->dinfo);
     ++ctx->nlaunch;
   };
   switch (ng) {
