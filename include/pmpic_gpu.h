@@ -211,6 +211,35 @@ int pmpic_par2grid_static(int32_t nx, int32_t ny, int32_t nz, double lx, double 
                           int64_t n, const double* x, const double* y, const double* z,
                           const double* vol, const double* field, double* out, void* stream);
 
+/* ---- ensembles (no counterpart in the reference, which runs one model per job) --
+ * A batch of independent plumes of uneven grid sizes and parcel counts on one
+ * GPU.  Every member is a full context (its own stream, its own device state):
+ * set it up with the single-context calls on pmpic_ensemble_member(e, i).
+ * pmpic_ensemble_step advances every member nsteps model steps, members running
+ * concurrently (a pool of host threads, largest members first). */
+typedef struct pmpic_ensemble pmpic_ensemble;
+/* n members with one configuration each; all on the same device. */
+int  pmpic_ensemble_create(int n, const pmpic_config* cfgs, pmpic_ensemble** out);
+void pmpic_ensemble_destroy(pmpic_ensemble* e);
+pmpic_ctx* pmpic_ensemble_member(pmpic_ensemble* e, int i);
+/* Host threads stepping members at once; 0 (the default) tunes the number
+ * online: the first steps of the next run try 2, 4, 8, 16, 32 threads, one
+ * step each, and the rest of the run uses the fastest.  1 runs the members
+ * one after another (the sequential baseline). */
+int  pmpic_ensemble_set_concurrency(pmpic_ensemble* e, int threads);
+/* Tile tuning: for each distinct grid size, the par2grid row-pass column
+ * segment (8, 16, 32 or 64 columns per warp) with the shortest time, timed on
+ * a member's own parcels; no member state changes (grids p, q, r, b are
+ * overwritten, as the next vort2vel does anyway). */
+int  pmpic_ensemble_autotune(pmpic_ensemble* e);
+/* nsteps model steps of every member; *device_ms (may be NULL) receives the
+ * device time from the first member's start to the last member's end. */
+int  pmpic_ensemble_step(pmpic_ensemble* e, int nsteps, float* device_ms);
+/* The tuning in use: host threads, and per member the par2grid segment. */
+int  pmpic_ensemble_tuning(pmpic_ensemble* e, int* threads, int32_t* xseg_per_member);
+/* Columns per x segment of the par2grid row pass of one context (default 64). */
+int  pmpic_set_p2g_segment(pmpic_ctx* ctx, int xseg);
+
 /* ---- instrumentation ------------------------------------------------------ */
 /* Named timers after the reference's timer_mod (register_routine_for_timing /
  * timer_start / timer_stop, model_core/src/utils/timer.F90:110-245), backed by

@@ -119,6 +119,15 @@ def lib() -> C.CDLL:
         L.pmpic_op_grid2par_multi.argtypes = [P, C.c_int, IP, IP]
         L.pmpic_op_vort2vel_grids.argtypes = [P]
         L.pmpic_sort_parcels.argtypes = [P]
+        L.pmpic_ensemble_create.argtypes = [C.c_int, C.POINTER(Config), C.POINTER(P)]
+        L.pmpic_ensemble_destroy.argtypes = [P]
+        L.pmpic_ensemble_member.restype = P
+        L.pmpic_ensemble_member.argtypes = [P, C.c_int]
+        L.pmpic_ensemble_set_concurrency.argtypes = [P, C.c_int]
+        L.pmpic_ensemble_autotune.argtypes = [P]
+        L.pmpic_ensemble_step.argtypes = [P, C.c_int, C.POINTER(C.c_float)]
+        L.pmpic_ensemble_tuning.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int32)]
+        L.pmpic_set_p2g_segment.argtypes = [P, C.c_int]
         L.pmpic_timing.argtypes = [P, C.c_int]
         L.pmpic_timer_count.argtypes = []
         L.pmpic_timer_name.restype = C.c_char_p
@@ -218,10 +227,21 @@ class Context:
         self._h = h
         self.max_parcels = int(max_parcels)
 
+    @classmethod
+    def _member(cls, handle, nx, ny, nz, precision, max_parcels):
+        """A view of an ensemble member's context (owned by the ensemble)."""
+        self = cls.__new__(cls)
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.precision = precision
+        self.max_parcels = int(max_parcels)
+        self._h = handle
+        self._owned = False
+        return self
+
     def close(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and getattr(self, "_owned", True):
             lib().pmpic_destroy(self._h)
-            self._h = None
+        self._h = None
 
     def __del__(self):
         try:
@@ -405,3 +425,64 @@ class Context:
         a = np.array(a, np.float64, copy=True, order="C")
         self._check(lib().pmpic_op_laplinv(self._h, _dp(a), 1 if df_zero_on_boundary else 0))
         return a
+
+
+class Ensemble:
+    """Independent plumes of uneven sizes on one GPU, stepped concurrently
+    (pmpic_ensemble_*; no counterpart in the reference).  members: a list of
+    dicts with nx, ny, nz and optionally lx, ly, lz, dtm, dtmax, max_parcels,
+    precision."""
+
+    def __init__(self, members, device=0):
+        L = lib()
+        cfgs = (Config * len(members))()
+        self._meta = []
+        for i, m in enumerate(members):
+            prec = m.get("precision", "fp64")
+            dt = m.get("dtm", 0.01)
+            cfgs[i] = Config(m["nx"], m["ny"], m["nz"], 0.0, m.get("lx", 2 * np.pi), 0.0, m.get("ly", 2 * np.pi),
+                             0.0, m.get("lz", np.pi), dt, m.get("dtmax", dt), m.get("prefactor", 0.5),
+                             int(m["max_parcels"]), PRECISIONS[prec], device)
+            self._meta.append((m["nx"], m["ny"], m["nz"], prec, m["max_parcels"]))
+        h = C.c_void_p()
+        rc = L.pmpic_ensemble_create(len(members), cfgs, C.byref(h))
+        if rc:
+            raise PmpicError(rc, "pmpic_ensemble_create failed")
+        self._h = h
+        self.members = [Context._member(L.pmpic_ensemble_member(h, i), *self._meta[i])
+                        for i in range(len(members))]
+
+    def set_concurrency(self, threads):
+        self._check(lib().pmpic_ensemble_set_concurrency(self._h, int(threads)))
+
+    def autotune(self):
+        self._check(lib().pmpic_ensemble_autotune(self._h))
+
+    def step(self, nsteps=1) -> float:
+        """Advance every member; returns the device time in ms."""
+        ms = C.c_float()
+        self._check(lib().pmpic_ensemble_step(self._h, int(nsteps), C.byref(ms)))
+        return float(ms.value)
+
+    def tuning(self):
+        t = C.c_int()
+        x = (C.c_int32 * len(self.members))()
+        self._check(lib().pmpic_ensemble_tuning(self._h, C.byref(t), x))
+        return int(t.value), list(x)
+
+    def _check(self, rc):
+        if rc:
+            raise PmpicError(rc, "ensemble call failed")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            for m in self.members:
+                m._h = None
+            lib().pmpic_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

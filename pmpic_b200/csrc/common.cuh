@@ -179,6 +179,7 @@ struct TimerScope {
 struct pmpic_ctx {
   pmpic_config cfg;
   bool mixed;                // PMPIC_MIXED: FP32 bulk, int cell + FP32 offset positions
+  int p2g_xseg;              // columns per x segment of the par2grid row pass (tunable)
   pmpic::Geom g;
   int device;
   cudaStream_t stream;

@@ -189,6 +189,7 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   std::memset((void*)&ctx->g, 0, sizeof(ctx->g));
   ctx->cfg = *cfg;
   ctx->mixed = cfg->precision == PMPIC_MIXED;
+  ctx->p2g_xseg = 64;
   ctx->device = cfg->device;
   ctx->parcels = nullptr;
   cudaError_t e = cudaSetDevice(cfg->device);

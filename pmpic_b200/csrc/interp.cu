@@ -249,7 +249,7 @@ constexpr int NLV = ZC + 1;               // grid levels a chunk contributes to
 constexpr int BATCH = 128;                // sorted positions staged per batch
 constexpr int SPAD = BATCH + BATCH / 16;  // staged field stride: position p sits at p + p/16
 constexpr int RW = 4;                     // warps per CTA of the row pass
-constexpr int XSEG = 64;                  // columns per x segment of a warp
+constexpr int XSEG = 64;                  // default columns per x segment of a warp (tunable per context)
 constexpr int PXB = 16;                   // grid points in x per CTA of the combine pass
 
 template <int NQ, int MODE, bool BT>
@@ -284,7 +284,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // DZ[ds * n]: the cached binning (ds = 1) or the offset half of the mixed
 // form's {cell index, offset} positions (ds = 2).
 template <int NQ, int MODE, bool BT, class R = double>
-__global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, const int32_t* __restrict__ start,
+__global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, int xseg, const int32_t* __restrict__ start,
                                                      const int32_t* __restrict__ sorted, const R* __restrict__ DX,
                                                      const R* __restrict__ DY, const R* __restrict__ DZ, int ds,
                                                      const R* __restrict__ VOL, P2GArgs<NQ, R> a,
@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, 
   const int xs = (int)(wid % nxs);
   const int cy = (int)((wid / nxs) % g.Ny);
   const int zc = (int)(wid / ((int64_t)nxs * g.Ny));
-  const int x_lo = xs * XSEG, x_hi = min(g.Nx, x_lo + XSEG);
+  const int x_lo = xs * xseg, x_hi = min(g.Nx, x_lo + xseg);
   const int k0 = zc * ZC, nk = min(ZC, g.Nz - k0);
   const int kk = lane >> 1, cz = lane & 1;
   const bool has_cell = kk < nk;
@@ -600,15 +600,16 @@ int bin_and_sort(pmpic_ctx* ctx) {
 // P2GLayout::RPS values of type R
 template <int NQ, int MODE, bool BT, class R = double>
 static cudaError_t run_p2g(const Geom& g, const int32_t* start, const int32_t* sorted, const R* dx, const R* dy,
-                           const R* dz, int ds, const R* vol, const P2GArgs<NQ, R>& a, R* rowpart, cudaStream_t st) {
+                           const R* dz, int ds, const R* vol, const P2GArgs<NQ, R>& a, R* rowpart, cudaStream_t st,
+                           int xseg = XSEG) {
   const int nzc = (g.Nz + ZC - 1) / ZC;
-  const int nxs = (g.Nx + XSEG - 1) / XSEG;
+  const int nxs = (g.Nx + xseg - 1) / xseg;
   const int64_t nw = (int64_t)nxs * g.Ny * nzc;
   auto rows = k_p2g_rows<NQ, MODE, BT, R>;
   cudaError_t e = cudaFuncSetAttribute(rows, cudaFuncAttributePreferredSharedMemoryCarveout,
                                        (int)cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
-  rows<<<nblk(nw, RW), 32 * RW, 0, st>>>(g, nzc, nxs, start, sorted, dx, dy, dz, ds, vol, a, rowpart);
+  rows<<<nblk(nw, RW), 32 * RW, 0, st>>>(g, nzc, nxs, xseg, start, sorted, dx, dy, dz, ds, vol, a, rowpart);
   dim3 gb((g.Nx + PXB - 1) / PXB, g.Ny, nzc);
   k_p2g_combine<NQ, MODE, R><<<gb, 256, 0, st>>>(g, nzc, rowpart, a);
   return cudaGetLastError();
@@ -630,7 +631,7 @@ static int launch_p2g(pmpic_ctx* ctx, const double* const* fields, double* const
   a.vmin = g.vmin;
   const double* del = ctx->del;
   PMPIC_CUDA((run_p2g<NQ, MODE, BT>(g, ctx->cell_start, ctx->sorted, del, del + ctx->cap, del + 2 * ctx->cap, 1,
-                                    prop(ctx, PMPIC_PROP_VOL), a, ctx->rowpart, ctx->stream)));
+                                    prop(ctx, PMPIC_PROP_VOL), a, ctx->rowpart, ctx->stream, ctx->p2g_xseg)));
   ctx->nlaunch += 2;
   return 0;
 }
@@ -652,7 +653,8 @@ static int launch_p2g_m(pmpic_ctx* ctx, const float* const* fields, float* const
   const float* py = (const float*)prop(ctx, PMPIC_PROP_Y) + 1;
   const float* pz = (const float*)prop(ctx, PMPIC_PROP_Z) + 1;
   PMPIC_CUDA((run_p2g<NQ, MODE, false, float>(g, ctx->cell_start, ctx->sorted, px, py, pz, 2,
-                                              propf(ctx, PMPIC_PROP_VOL), a, (float*)ctx->rowpart, ctx->stream)));
+                                              propf(ctx, PMPIC_PROP_VOL), a, (float*)ctx->rowpart, ctx->stream,
+                                              ctx->p2g_xseg)));
   ctx->nlaunch += 2;
   return 0;
 }
