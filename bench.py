@@ -565,6 +565,102 @@ def run_vort2vel(args):
     return 0
 
 
+def ensemble_members(n, seed=999):
+    """The config-4 ensemble: per member a grid drawn from {32, 48, 64, 96, 128}^3,
+    thermal radius U[0.25, 0.5], excess U[0.5, 1.5], humidity fraction
+    U[0.8, 1.0] of the surface saturation, own seed 1000+m, 8 parcels per cell."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for m in range(n):
+        G = int(rng.choice([32, 48, 64, 96, 128]))
+        out.append(dict(G=G, radius=float(rng.uniform(0.25, 0.5)), excess=float(rng.uniform(0.5, 1.5)),
+                        h_in=float(rng.uniform(0.8, 1.0)), seed=1000 + m, dt=0.32 / G))
+    return out
+
+
+def run_ensemble(args):
+    """Batched ensemble of independent plumes in the mixed form: the members run
+    one after another (concurrency 1, default tiles) and then batched (tuned
+    tiles, concurrent members), each from the same initial state for the same
+    number of steps; then every member against the same plume on the FP64 path."""
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    import torch
+    torch.cuda.set_device(local)
+    import pmpic_b200 as pm
+    spec = ensemble_members(args.members)
+    steps = args.ens_steps
+
+    def ic(m):
+        return pm.thermal_parcels(m["G"], m["G"], m["G"], radius=m["radius"], excess=m["excess"],
+                                  h_in=m["h_in"], seed=m["seed"])
+    counts = [8 * m["G"] ** 3 for m in spec]
+    cfgs = [dict(nx=m["G"], ny=m["G"], nz=m["G"], dtm=m["dt"], dtmax=m["dt"], max_parcels=int(1.15 * c),
+                 precision="mixed") for m, c in zip(spec, counts)]
+    ens = pm.Ensemble(cfgs, device=local)
+
+    def load():
+        for mem, m in zip(ens.members, spec):
+            mem.upload(**ic(m))
+        torch.cuda.synchronize()
+
+    def work(n_before):
+        n_after = [mem.n for mem in ens.members]
+        return sum(0.5 * (a + b) for a, b in zip(n_before, n_after)) * steps
+
+    load()
+    ens.set_concurrency(1)
+    n0 = [mem.n for mem in ens.members]
+    ms_seq = ens.step(steps)
+    w_seq = work(n0)
+    load()
+    for mem in ens.members:
+        pm.lib().pmpic_set_p2g_segment(mem._h, 64)
+    ens.autotune()
+    ens.set_concurrency(0)
+    n0 = [mem.n for mem in ens.members]
+    ms_bat = ens.step(steps)
+    w_bat = work(n0)
+    threads, xseg = ens.tuning()
+    grids = [{g: mem.grid(g) for g in ("u", "v", "w")} for mem in ens.members[:args.error_members]]
+    n_mixed = [mem.n for mem in ens.members]
+    ens.close()
+    errs = []
+    for i, m in enumerate(spec[:args.error_members]):
+        G = m["G"]
+        c = pm.Context(G, G, G, 2 * np.pi, 2 * np.pi, np.pi, dtm=m["dt"], dtmax=m["dt"],
+                       max_parcels=int(1.15 * counts[i]), device=local)
+        c.upload(**ic(m))
+        c.step(steps)
+        e = {"member": i, "grid": G, "n_mixed": n_mixed[i], "n_fp64": c.n}
+        for g in ("u", "v", "w"):
+            ref = c.grid(g)
+            e[g + "_rel_l2"] = float(np.linalg.norm(grids[i][g] - ref) / max(np.linalg.norm(ref), 1e-300))
+        errs.append(e)
+        c.close()
+    seq_v, bat_v = w_seq / (ms_seq / 1e3), w_bat / (ms_bat / 1e3)
+    sizes = {}
+    for m, s_ in zip(spec, xseg):
+        sizes.setdefault(str(m["G"]), s_)
+    line = {"workload": "ensemble", "metric": "aggregate parcel-RK4-steps/s of the batched ensemble",
+            "unit": UNIT, "higher_is_better": True, "value": bat_v,
+            "config": {"members": len(spec), "steps": steps, "precision": "mixed",
+                       "grids": {str(G): sum(1 for m in spec if m["G"] == G) for G in (32, 48, 64, 96, 128)},
+                       "parcels_initial": int(sum(counts)), "dt": "0.32 / grid size",
+                       "timing": "device time from the first member's start to the last member's end "
+                                 "(events across all member streams); the batched run includes its "
+                                 "concurrency-tuning steps"},
+            "sequential": {"value": seq_v, "ms": ms_seq, "concurrency": 1, "par2grid_segment": 64},
+            "batched": {"value": bat_v, "ms": ms_bat, "concurrency": threads, "par2grid_segment_by_grid": sizes},
+            "batched_over_sequential": bat_v / seq_v,
+            "error_vs_fp64": {"members": errs,
+                              "max_rel_l2": max((max(e["u_rel_l2"], e["v_rel_l2"], e["w_rel_l2"]) for e in errs),
+                                                default=None)}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -580,9 +676,13 @@ def main():
                     help="both: time FP64 then the mixed form (the headline value), and compare them")
     ap.add_argument("--error-steps", type=int, default=100,
                     help="total steps per form before the gridded velocities are compared (0: no check)")
-    ap.add_argument("--workload", default="plume", choices=["plume", "interp", "vort2vel"],
+    ap.add_argument("--members", type=int, default=64, help="ensemble workload: members")
+    ap.add_argument("--ens-steps", type=int, default=50, help="ensemble workload: steps per member")
+    ap.add_argument("--error-members", type=int, default=64,
+                    help="ensemble workload: members compared with the FP64 path")
+    ap.add_argument("--workload", default="plume", choices=["plume", "interp", "vort2vel", "ensemble"],
                     help="plume: the headline step; interp: the interpolation microbenchmark (128^3); "
-                         "vort2vel: the inversion alone (256^3)")
+                         "vort2vel: the inversion alone (256^3); ensemble: 64 plumes of uneven sizes")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -590,6 +690,8 @@ def main():
         return run_interp(args)
     if args.workload == "vort2vel":
         return run_vort2vel(args)
+    if args.workload == "ensemble":
+        return run_ensemble(args)
     return run_b200(args)
 
 

@@ -223,7 +223,7 @@ int  pmpic_ensemble_create(int n, const pmpic_config* cfgs, pmpic_ensemble** out
 void pmpic_ensemble_destroy(pmpic_ensemble* e);
 pmpic_ctx* pmpic_ensemble_member(pmpic_ensemble* e, int i);
 /* Host threads stepping members at once; 0 (the default) tunes the number
- * online: the first steps of the next run try 2, 4, 8, 16, 32 threads, one
+ * online: the first steps of the next run try 2, 4, 8, 16, 32, 64 threads, one
  * step each, and the rest of the run uses the fastest.  1 runs the members
  * one after another (the sequential baseline). */
 int  pmpic_ensemble_set_concurrency(pmpic_ensemble* e, int threads);

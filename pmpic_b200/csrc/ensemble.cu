@@ -186,7 +186,7 @@ int pmpic_ensemble_step(pmpic_ensemble* e, int nsteps, float* device_ms) {
   float total = 0.f;
   int done = 0;
   if (!e->tuned_threads) {
-    static const int cand[] = {2, 4, 8, 16, 32};
+    static const int cand[] = {2, 4, 8, 16, 32, 64};
     float tbest = 1e30f;
     int best = 1;
     for (int t : cand) {
@@ -202,7 +202,7 @@ int pmpic_ensemble_step(pmpic_ensemble* e, int nsteps, float* device_ms) {
         best = t;
       }
     }
-    if (done == nsteps && nsteps < 5) {
+    if (done == nsteps && nsteps < 6) {
       if (device_ms) *device_ms = total;
       return PMPIC_OK;  // not every candidate tried yet: tune again on the next run
     }
