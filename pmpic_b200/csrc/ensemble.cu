@@ -187,11 +187,13 @@ int pmpic_ensemble_step(pmpic_ensemble* e, int nsteps, float* device_ms) {
   int done = 0;
   if (!e->tuned_threads) {
     static const int cand[] = {2, 4, 8, 16, 32, 64};
+    std::vector<int> tries;  // candidates up to the member count (at least one)
+    for (int t : cand)
+      if (t <= n || tries.empty()) tries.push_back(t);
     float tbest = 1e30f;
     int best = 1;
-    for (int t : cand) {
+    for (int t : tries) {
       if (done >= nsteps) break;
-      if (t > n && t != 2) continue;
       float ms = 0.f;
       int rc = run_members(e, 1, t, &ms);
       if (rc) return rc;
@@ -202,7 +204,7 @@ int pmpic_ensemble_step(pmpic_ensemble* e, int nsteps, float* device_ms) {
         best = t;
       }
     }
-    if (done == nsteps && nsteps < 6) {
+    if (done < (int)tries.size()) {
       if (device_ms) *device_ms = total;
       return PMPIC_OK;  // not every candidate tried yet: tune again on the next run
     }
