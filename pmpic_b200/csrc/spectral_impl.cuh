@@ -156,19 +156,29 @@ __global__ void k_diffz(Geom g, const real* __restrict__ f, real* __restrict__ o
   const real* CP = coef + 2 * nz;
   const real dz = (real)g.dz;
   const bool bt = bot != nullptr;
-  // forward sweep: f'(1) = d(1)/den(1); f'(i) = (d(i) - a(i) f'(i-1)) / den(i)
+  // forward sweep: f'(1) = d(1)/den(1); f'(i) = (d(i) - a(i) f'(i-1)) / den(i).
+  // The loads of each batch of ZB levels are issued before its recurrence, so
+  // the loop waits on one memory latency per batch, not per level.
+  constexpr int ZB = 8;
   real fm = f[col], f0 = f[cs + col];
   real d1 = bt ? f0 / dz - a1 * bot[col] * dz : real(0);
   real prev = d1 / DEN[0];
   out[col] = prev;
-#pragma unroll 8
-  for (int k = 1; k < nz - 1; ++k) {
-    real fp = f[(int64_t)(k + 1) * cs + col];
-    real d = (fp - fm) / real(2) / dz;
-    prev = (d - A[k] * prev) / DEN[k];
-    out[(int64_t)k * cs + col] = prev;
-    fm = f0;
-    f0 = fp;
+  for (int kb = 1; kb < nz - 1; kb += ZB) {
+    real fb[ZB];
+#pragma unroll
+    for (int u = 0; u < ZB; ++u)
+      if (kb + u < nz - 1) fb[u] = f[(int64_t)(kb + u + 1) * cs + col];
+#pragma unroll
+    for (int u = 0; u < ZB; ++u) {
+      const int k = kb + u;
+      if (k >= nz - 1) break;
+      real d = (fb[u] - fm) / real(2) / dz;
+      prev = (d - A[k] * prev) / DEN[k];
+      out[(int64_t)k * cs + col] = prev;
+      fm = f0;
+      f0 = fb[u];
+    }
   }
   {
     int k = nz - 1;
@@ -178,11 +188,19 @@ __global__ void k_diffz(Geom g, const real* __restrict__ f, real* __restrict__ o
   }
   // back substitution: f(i) = f(i) - cp(i+1) f(i+1)
   real nxt = prev;
-#pragma unroll 8
-  for (int k = nz - 2; k >= 0; --k) {
-    real v = out[(int64_t)k * cs + col] - CP[k + 1] * nxt;
-    out[(int64_t)k * cs + col] = v;
-    nxt = v;
+  for (int kb = nz - 2; kb >= 0; kb -= ZB) {
+    real ob[ZB];
+#pragma unroll
+    for (int u = 0; u < ZB; ++u)
+      if (kb - u >= 0) ob[u] = out[(int64_t)(kb - u) * cs + col];
+#pragma unroll
+    for (int u = 0; u < ZB; ++u) {
+      const int k = kb - u;
+      if (k < 0) break;
+      real v = ob[u] - CP[k + 1] * nxt;
+      out[(int64_t)k * cs + col] = v;
+      nxt = v;
+    }
   }
 }
 
@@ -230,32 +248,54 @@ __global__ void k_laplinv(Geom g, LapBatch lb, real* __restrict__ cpbase, const 
   real prev = d / den;
   f[col] = prev;
   real cprev = c1;  // c(i-1)
-#pragma unroll 8
-  for (int k = 1; k < nz; ++k) {
-    fm = f0;
-    f0 = fp;
-    real a, b, c;
-    if (k < nz - 1) {
-      fp = f[(int64_t)(k + 1) * cs + col];
-      a = ai; b = bi; c = ci;
-      d = f112 * fm + f56 * f0 + f112 * fp;
-    } else {
-      a = an; b = bn; c = real(0);
-      d = df0 ? f13 * f0 + f16 * fm : real(0);
+  // loads of each batch of ZB levels first, then its recurrence (one memory
+  // latency per batch); the batch reads f above the levels it overwrites
+  constexpr int ZB = 8;
+  for (int kb = 1; kb < nz; kb += ZB) {
+    real fb[ZB];
+#pragma unroll
+    for (int u = 0; u < ZB; ++u)
+      if (kb + u < nz - 1) fb[u] = f[(int64_t)(kb + u + 1) * cs + col];
+#pragma unroll
+    for (int u = 0; u < ZB; ++u) {
+      const int k = kb + u;
+      if (k >= nz) break;
+      fm = f0;
+      f0 = fp;
+      real a, b, c;
+      if (k < nz - 1) {
+        fp = fb[u];
+        a = ai; b = bi; c = ci;
+        d = f112 * fm + f56 * f0 + f112 * fp;
+      } else {
+        a = an; b = bn; c = real(0);
+        d = df0 ? f13 * f0 + f16 * fm : real(0);
+      }
+      real cp = cprev / den;
+      den = b - a * cp;
+      prev = (d - a * prev) / den;
+      f[(int64_t)k * cs + col] = prev;
+      cpbuf[(int64_t)k * cs + col] = cp;
+      cprev = c;
     }
-    real cp = cprev / den;
-    den = b - a * cp;
-    prev = (d - a * prev) / den;
-    f[(int64_t)k * cs + col] = prev;
-    cpbuf[(int64_t)k * cs + col] = cp;
-    cprev = c;
   }
   real nxt = prev;
-#pragma unroll 8
-  for (int k = nz - 2; k >= 0; --k) {
-    real v = f[(int64_t)k * cs + col] - cpbuf[(int64_t)(k + 1) * cs + col] * nxt;
-    f[(int64_t)k * cs + col] = v;
-    nxt = v;
+  for (int kb = nz - 2; kb >= 0; kb -= ZB) {
+    real fb[ZB], cb[ZB];
+#pragma unroll
+    for (int u = 0; u < ZB; ++u)
+      if (kb - u >= 0) {
+        fb[u] = f[(int64_t)(kb - u) * cs + col];
+        cb[u] = cpbuf[(int64_t)(kb - u + 1) * cs + col];
+      }
+#pragma unroll
+    for (int u = 0; u < ZB; ++u) {
+      const int k = kb - u;
+      if (k < 0) break;
+      real v = fb[u] - cb[u] * nxt;
+      f[(int64_t)k * cs + col] = v;
+      nxt = v;
+    }
   }
 }
 
