@@ -211,6 +211,22 @@ int pmpic_par2grid_static(int32_t nx, int32_t ny, int32_t nz, double lx, double 
                           int64_t n, const double* x, const double* y, const double* z,
                           const double* vol, const double* field, double* out, void* stream);
 
+/* ---- dumps and restart in the reference's binary stream format ------------- */
+/* A parcel dump of writebinary.F90:149-199: time, the domain bounds, the count
+ * (int64), then x, y, z, p, q, r, dxdt, dydt, dzdt, dpdt, dqdt, drdt, h, b, vol,
+ * stretch, tag as FP64 arrays (native byte order).  The reference's reader and
+ * post-processing tools read it as one rank's file. */
+int pmpic_write_parcels(pmpic_ctx* ctx, const char* path, double time);
+/* Restart from a parcel dump (readfromfile_parcelsetup.F90:169-290): the
+ * parcels of the file inside this domain, in file order, replace the current
+ * parcels (append = 0) or follow them (append != 0, one call per file of a
+ * multi-rank dump); *time (may be NULL) receives the dump's time. */
+int pmpic_read_parcels(pmpic_ctx* ctx, const char* path, int append, double* time);
+/* A grid dump of writebinary.F90:201-299: p, q, r, b, h gridded afresh from the
+ * parcels, hgliq = max(0, hg - exp(-z)), b + 12.5 hgliq, written with u, v, w
+ * and vol as FP64, z fastest.  The model's own grids are not changed. */
+int pmpic_write_grids(pmpic_ctx* ctx, const char* path, double time);
+
 /* ---- ensembles (no counterpart in the reference, which runs one model per job) --
  * A batch of independent plumes of uneven grid sizes and parcel counts on one
  * GPU.  Every member is a full context (its own stream, its own device state):

@@ -119,6 +119,9 @@ def lib() -> C.CDLL:
         L.pmpic_op_grid2par_multi.argtypes = [P, C.c_int, IP, IP]
         L.pmpic_op_vort2vel_grids.argtypes = [P]
         L.pmpic_sort_parcels.argtypes = [P]
+        L.pmpic_write_parcels.argtypes = [P, C.c_char_p, C.c_double]
+        L.pmpic_read_parcels.argtypes = [P, C.c_char_p, C.c_int, C.POINTER(C.c_double)]
+        L.pmpic_write_grids.argtypes = [P, C.c_char_p, C.c_double]
         L.pmpic_ensemble_create.argtypes = [C.c_int, C.POINTER(Config), C.POINTER(P)]
         L.pmpic_ensemble_destroy.argtypes = [P]
         L.pmpic_ensemble_member.restype = P
@@ -373,6 +376,20 @@ class Context:
         """vort2vel's inversion alone on the vorticity in grids p, q, r."""
         self._check(lib().pmpic_op_vort2vel_grids(self._h))
 
+    def write_parcels(self, path, time=0.0):
+        """Parcel dump in the reference's binary format (writebinary.F90)."""
+        self._check(lib().pmpic_write_parcels(self._h, os.fsencode(path), float(time)))
+
+    def read_parcels(self, path, append=False) -> float:
+        """Restart from a parcel dump; returns the dump's time."""
+        t = C.c_double()
+        self._check(lib().pmpic_read_parcels(self._h, os.fsencode(path), 1 if append else 0, C.byref(t)))
+        return float(t.value)
+
+    def write_grids(self, path, time=0.0):
+        """Grid dump in the reference's binary format (writebinary.F90)."""
+        self._check(lib().pmpic_write_grids(self._h, os.fsencode(path), float(time)))
+
     def sort_parcels(self):
         """Renumber slots into cell order (not a reference operation)."""
         self._check(lib().pmpic_sort_parcels(self._h))
@@ -425,6 +442,34 @@ class Context:
         a = np.array(a, np.float64, copy=True, order="C")
         self._check(lib().pmpic_op_laplinv(self._h, _dp(a), 1 if df_zero_on_boundary else 0))
         return a
+
+
+DUMP_PROPS = ["x", "y", "z", "p", "q", "r", "dxdt", "dydt", "dzdt", "dpdt", "dqdt", "drdt",
+              "h", "b", "vol", "stretch", "tag"]
+DUMP_GRIDS = ["u", "v", "w", "p", "q", "r", "b", "hg", "hgliq", "vol"]
+
+
+def read_parcel_dump(path) -> dict:
+    """Reads a parcel dump of the reference's format (writebinary.F90:149-199)."""
+    with open(path, "rb") as f:
+        hdr = np.fromfile(f, np.float64, 7)
+        n = int(np.fromfile(f, np.int64, 1)[0])
+        data = np.fromfile(f, np.float64, 17 * n).reshape(17, n)
+    out = {k: data[i] for i, k in enumerate(DUMP_PROPS)}
+    out["time"], out["bounds"], out["n"] = float(hdr[0]), hdr[1:], n
+    return out
+
+
+def read_grid_dump(path) -> dict:
+    """Reads a grid dump of the reference's format (writebinary.F90:201-299);
+    grids are returned as (nz+1, ny, nx) arrays, x fastest."""
+    with open(path, "rb") as f:
+        hdr = np.fromfile(f, np.float64, 7)
+        nx, ny, nzp = (int(v) for v in np.fromfile(f, np.int32, 3))
+        data = np.fromfile(f, np.float64, 10 * nx * ny * nzp).reshape(10, nx, ny, nzp)
+    out = {k: np.ascontiguousarray(data[i].transpose(2, 1, 0)) for i, k in enumerate(DUMP_GRIDS)}
+    out["time"], out["bounds"], out["sizes"] = float(hdr[0]), hdr[1:], (nx, ny, nzp)
+    return out
 
 
 class Ensemble:

@@ -267,6 +267,10 @@ int par2grid_multi_m(pmpic_ctx* ctx, const float* const* fields, int nf, float* 
 int grid2par_multi_m(pmpic_ctx* ctx, const float* const* grids, int ng, float* const* out);
 int cell_ids(pmpic_ctx* ctx, int32_t* dcells);
 size_t rowpart_bytes(const Geom& g);
+// host FP64 <-> property pid of slots off..off+n-1 (NULL src: zeros), in the
+// context's precision, stream-ordered (ctx.cu)
+int prop_upload(pmpic_ctx* ctx, int pid, int64_t off, int64_t n, const double* src);
+int prop_download(pmpic_ctx* ctx, int pid, int64_t off, int64_t n, double* dst);
 // fft.cu
 int fft_init(pmpic_ctx* ctx);
 int fft_forward(pmpic_ctx* ctx, const double* phys, double* spec);

@@ -395,23 +395,26 @@ static void conv_kind(pmpic_ctx* ctx, int pid, int& kind, double& d, int& period
   if (pid == PMPIC_PROP_Z || pid == PMPIC_PROP_ZO || pid == PMPIC_PROP_ZF) { d = g.dz; nz = g.Nz; }
 }
 
-// host FP64 values (NULL: zeros) into property pid of slots 0..n-1, in the
-// context's precision; stream-ordered
-static int put_prop(pmpic_ctx* ctx, int pid, int64_t n, const double* src) {
+// host FP64 values (NULL: zeros) into property pid of slots off..off+n-1, in
+// the context's precision; stream-ordered
+}  // extern "C"
+
+int pmpic::prop_upload(pmpic_ctx* ctx, int pid, int64_t off, int64_t n, const double* src) {
   if (n <= 0) return 0;
   if (!ctx->mixed) {
-    if (src) PMPIC_CUDA(cudaMemcpyAsync(prop(ctx, pid), src, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
-    else PMPIC_CUDA(cudaMemsetAsync(prop(ctx, pid), 0, sizeof(double) * n, ctx->stream));
+    if (src) PMPIC_CUDA(cudaMemcpyAsync(prop(ctx, pid) + off, src, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    else PMPIC_CUDA(cudaMemsetAsync(prop(ctx, pid) + off, 0, sizeof(double) * n, ctx->stream));
     return 0;
   }
+  const size_t es0 = (size_t)mixed_elem_bytes(pid);
   if (!src) {
-    PMPIC_CUDA(cudaMemsetAsync(prop(ctx, pid), 0, (size_t)mixed_elem_bytes(pid) * n, ctx->stream));
+    PMPIC_CUDA(cudaMemsetAsync((char*)prop(ctx, pid) + es0 * off, 0, es0 * n, ctx->stream));
     return 0;
   }
   int kind, period, nz;
   double d;
   conv_kind(ctx, pid, kind, d, period, nz);
-  char* base = (char*)prop(ctx, pid);
+  char* base = (char*)prop(ctx, pid) + es0 * off;
   const size_t es = (size_t)mixed_elem_bytes(pid);
   for (int64_t c0 = 0; c0 < n; c0 += ctx->stage_n) {
     const int64_t len = std::min<int64_t>(ctx->stage_n, n - c0);
@@ -422,17 +425,17 @@ static int put_prop(pmpic_ctx* ctx, int pid, int64_t n, const double* src) {
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
-// property pid of slots 0..n-1 into host FP64 values; stream-ordered
-static int get_prop(pmpic_ctx* ctx, int pid, int64_t n, double* dst) {
+// property pid of slots off..off+n-1 into host FP64 values; stream-ordered
+int pmpic::prop_download(pmpic_ctx* ctx, int pid, int64_t off, int64_t n, double* dst) {
   if (n <= 0) return 0;
   if (!ctx->mixed) {
-    PMPIC_CUDA(cudaMemcpyAsync(dst, prop(ctx, pid), sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    PMPIC_CUDA(cudaMemcpyAsync(dst, prop(ctx, pid) + off, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
     return 0;
   }
   int kind, period, nz;
   double d;
   conv_kind(ctx, pid, kind, d, period, nz);
-  const char* base = (const char*)prop(ctx, pid);
+  const char* base = (const char*)prop(ctx, pid) + (size_t)mixed_elem_bytes(pid) * off;
   const size_t es = (size_t)mixed_elem_bytes(pid);
   for (int64_t c0 = 0; c0 < n; c0 += ctx->stage_n) {
     const int64_t len = std::min<int64_t>(ctx->stage_n, n - c0);
@@ -443,6 +446,13 @@ static int get_prop(pmpic_ctx* ctx, int pid, int64_t n, double* dst) {
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
+
+extern "C" {
+
+static int put_prop(pmpic_ctx* ctx, int pid, int64_t n, const double* src) {
+  return prop_upload(ctx, pid, 0, n, src);
+}
+static int get_prop(pmpic_ctx* ctx, int pid, int64_t n, double* dst) { return prop_download(ctx, pid, 0, n, dst); }
 
 int pmpic_set_count(pmpic_ctx* ctx, int64_t n) {
   if (!ctx) return PMPIC_ERR_ARG;
