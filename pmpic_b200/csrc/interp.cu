@@ -36,27 +36,17 @@ constexpr int MAXSEG = 32;            // cell segments sorted in registers
 inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
 // ---- binning (cache_parcel_interp_weights, parcel_interpolation.F90:186-262) ----
-// One integer atomic per distinct cell of the warp (neighbouring slots mostly
-// share a cell).  With rank, each parcel also gets its place among the cell's
-// parcels (leader's returned base + its rank in the warp group): the order
-// inside a cell is the order of these atomics, which the segment sort fixes.
-__device__ __forceinline__ void count_and_rank(int32_t id, int32_t* __restrict__ count, int32_t* __restrict__ rank,
-                                               int64_t t) {
+// one integer atomic per distinct cell of the warp (neighbouring slots mostly
+// share a cell)
+__device__ __forceinline__ void count_cell(int32_t id, int32_t* __restrict__ count) {
   const unsigned act = __activemask();
   const unsigned same = __match_any_sync(act, id);
-  const int lane = threadIdx.x & 31;
-  const int leader = __ffs(same) - 1;
-  int32_t base = 0;
-  if (lane == leader) base = atomicAdd(&count[id], __popc(same));
-  if (rank) {
-    base = __shfl_sync(same, base, leader);
-    rank[t] = base + __popc(same & ((1u << lane) - 1));
-  }
+  if ((threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&count[id], __popc(same));
 }
 
 __global__ void k_bin_count(Geom g, int64_t n, const double* __restrict__ X, const double* __restrict__ Y,
                             const double* __restrict__ Z, int32_t* __restrict__ cell, double* __restrict__ del,
-                            int64_t cap, int32_t* __restrict__ count, int32_t* __restrict__ rank, DevInfo* info) {
+                            int64_t cap, int32_t* __restrict__ count, DevInfo* info) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   int ci, cj, ck;
@@ -71,13 +61,13 @@ __global__ void k_bin_count(Geom g, int64_t n, const double* __restrict__ X, con
   del[t] = dx;
   del[cap + t] = dy;
   del[2 * cap + t] = dz;
-  count_and_rank(id, count, rank, t);
+  count_cell(id, count);
 }
 
 // the mixed form's binning: the cell is the integer part of the position
 __global__ void k_bin_count_m(Geom g, int64_t n, const CellOff* __restrict__ X, const CellOff* __restrict__ Y,
                               const CellOff* __restrict__ Z, int32_t* __restrict__ cell, int32_t* __restrict__ count,
-                              int32_t* __restrict__ rank, DevInfo* info) {
+                              DevInfo* info) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const CellOff x = X[t], y = Y[t], z = Z[t];
@@ -89,7 +79,7 @@ __global__ void k_bin_count_m(Geom g, int64_t n, const CellOff* __restrict__ X, 
   }
   const int32_t id = (int32_t)(((int64_t)x.i * g.Ny + y.i) * g.Nz + z.i);
   cell[t] = id;
-  count_and_rank(id, count, rank, t);
+  count_cell(id, count);
 }
 
 __global__ void k_bin_scatter(int64_t n, const int32_t* __restrict__ cell, const int32_t* __restrict__ start,
@@ -109,16 +99,6 @@ __global__ void k_bin_scatter(int64_t n, const int32_t* __restrict__ cell, const
   base = __shfl_sync(same, base, leader);
   const int32_t pos = start[id] + base + __popc(same & ((1u << lane) - 1));
   sorted[pos] = (int32_t)t;
-}
-
-// slot indices into cell order from the ranks of the count pass (no atomics)
-__global__ void k_bin_place(int64_t n, const int32_t* __restrict__ cell, const int32_t* __restrict__ rank,
-                            const int32_t* __restrict__ start, int32_t* __restrict__ sorted) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  const int32_t id = cell[t];
-  if (id < 0) return;
-  sorted[start[id] + rank[t]] = (int32_t)t;
 }
 
 // each cell's segment sorted by slot index (integer atomics above only decide
@@ -595,22 +575,22 @@ int bin_and_sort(pmpic_ctx* ctx) {
   TimerScope ts(ctx, T_CACHE);
   const Geom& g = ctx->g;
   const int64_t n = ctx->n;
-  int32_t* rank = ctx->aux;  // cap entries; free while the index is built
   PMPIC_CUDA(cudaMemsetAsync(ctx->cell_count, 0, sizeof(int32_t) * (g.ncell + 1), ctx->stream));
+  PMPIC_CUDA(cudaMemsetAsync(ctx->cell_fill, 0, sizeof(int32_t) * g.ncell, ctx->stream));
   if (n > 0 && ctx->mixed) {
     k_bin_count_m<<<nblk(n, 256), 256, 0, ctx->stream>>>(g, n, propc(ctx, PMPIC_PROP_X), propc(ctx, PMPIC_PROP_Y),
-                                                         propc(ctx, PMPIC_PROP_Z), ctx->cell, ctx->cell_count, rank,
+                                                         propc(ctx, PMPIC_PROP_Z), ctx->cell, ctx->cell_count,
                                                          ctx->dinfo); ++ctx->nlaunch;
   } else if (n > 0) {
     k_bin_count<<<nblk(n, 256), 256, 0, ctx->stream>>>(g, n, prop(ctx, PMPIC_PROP_X), prop(ctx, PMPIC_PROP_Y),
                                                        prop(ctx, PMPIC_PROP_Z), ctx->cell, ctx->del, ctx->cap,
-                                                       ctx->cell_count, rank, ctx->dinfo); ++ctx->nlaunch;
+                                                       ctx->cell_count, ctx->dinfo); ++ctx->nlaunch;
   }
   int rc = scan_excl(ctx, ctx->cell_count, g.ncell, ctx->cell_start);
   if (rc) return rc;
   if (n > 0) {
-    k_bin_place<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, ctx->cell, rank, ctx->cell_start, ctx->sorted);
-    ++ctx->nlaunch;
+    k_bin_scatter<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, ctx->cell, ctx->cell_start, ctx->cell_fill,
+                                                         ctx->sorted); ++ctx->nlaunch;
     k_sort_segments<<<nblk(g.ncell, 256), 256, 0, ctx->stream>>>(g.ncell, ctx->cell_start, ctx->sorted);
     ++ctx->nlaunch;
   }
@@ -939,7 +919,7 @@ extern "C" int pmpic_par2grid_static(int32_t nx, int32_t ny, int32_t nz, double 
   if (cudaMemsetAsync(fill, 0, sizeof(int32_t) * ncell, st) != cudaSuccess) return PMPIC_ERR_CUDA;
   if (cudaMemsetAsync(info, 0, sizeof(DevInfo), st) != cudaSuccess) return PMPIC_ERR_CUDA;
   if (n > 0)
-    k_bin_count<<<nblk(n, 256), 256, 0, st>>>(g, n, x, y, z, cell, del, SP_MAX_PARCELS, count, nullptr, info);
+    k_bin_count<<<nblk(n, 256), 256, 0, st>>>(g, n, x, y, z, cell, del, SP_MAX_PARCELS, count, info);
   const int64_t ntiles = (ncell + SCAN_TILE - 1) / SCAN_TILE;
   k_scan_tiles<<<(unsigned)ntiles, SCAN_BLOCK, 0, st>>>(count, ncell, tiles);
   k_scan_sums<<<1, SCAN_BLOCK, 0, st>>>(tiles, ntiles, cstart + ncell);
