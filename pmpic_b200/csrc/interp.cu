@@ -253,7 +253,12 @@ constexpr int BATCH = 128;                // sorted positions staged per batch
 constexpr int SPAD = BATCH + BATCH / 16;  // staged field stride: position p sits at p + p/16
 constexpr int RW = 4;                     // warps per CTA of the row pass
 constexpr int XSEG = 64;                  // default columns per x segment of a warp (tunable per context)
-constexpr int PXB = 16;                   // grid points in x per CTA of the combine pass
+// grid points in x per CTA of the combine pass (its staged rows fit the
+// 48 KB of static shared memory)
+template <class R>
+struct P2GPx {
+  static constexpr int value = sizeof(R) == 8 ? 16 : 32;
+};
 
 template <int NQ, int MODE, bool BT>
 struct P2GLayout {
@@ -449,35 +454,40 @@ __global__ void __launch_bounds__(256) k_p2g_combine(Geom g, int nzc, const R* _
   constexpr int NA = MODE == 0 ? NQ + 1 : NQ;
   constexpr int RPS = 2 * NA * NLV;
   constexpr int TS = NA * NLV + 1;  // odd stride: conflict-free reads by consecutive points
-  __shared__ R T[2][PXB * TS];      // [0]: row y (y-low part), [1]: row y-1 (y-high part)
-  __shared__ R Bz[2][PXB * NA];     // the chunk below's top level, same rows
-  const int px0 = blockIdx.x * PXB, py = blockIdx.y, zc = blockIdx.z;
+  constexpr int PX = P2GPx<R>::value;
+  constexpr int SEG = NA * NLV;
+  __shared__ R T[2][PX * TS];       // [0]: row y (y-low part), [1]: row y-1 (y-high part)
+  __shared__ R Bz[2][PX * NA];      // the chunk below's top level, same rows
+  const int px0 = blockIdx.x * PX, py = blockIdx.y, zc = blockIdx.z;
   const int pym = py == 0 ? g.Ny - 1 : py - 1;
-  const int npx = min(PXB, g.Nx - px0);
+  const int npx = min(PX, g.Nx - px0);
   const int k0 = zc * ZC, nk = min(ZC, g.Nz - k0);
-  const int seg = NA * NLV;
-  for (int e = threadIdx.x; e < 2 * npx * seg; e += blockDim.x) {
-    const int r = e / (npx * seg);
-    const int rem = e - r * npx * seg;
-    const int pxl = rem / seg, o = rem - pxl * seg;
+  // index spaces of compile-time widths: no runtime divisions per element
+  for (int e = threadIdx.x; e < 2 * PX * SEG; e += blockDim.x) {
+    const int r = e / (PX * SEG);
+    const int rem = e - r * PX * SEG;
+    const int pxl = rem / SEG, o = rem - pxl * SEG;
+    if (pxl >= npx) continue;
     const int row = r == 0 ? py : pym;
-    T[r][pxl * TS + o] = rowpart[(((size_t)zc * g.Ny + row) * g.Nx + px0 + pxl) * RPS + r * seg + o];
+    T[r][pxl * TS + o] = rowpart[(((size_t)zc * g.Ny + row) * g.Nx + px0 + pxl) * RPS + r * SEG + o];
   }
   if (zc > 0) {
-    for (int e = threadIdx.x; e < 2 * npx * NA; e += blockDim.x) {
-      const int r = e / (npx * NA);
-      const int rem = e - r * npx * NA;
+    for (int e = threadIdx.x; e < 2 * PX * NA; e += blockDim.x) {
+      const int r = e / (PX * NA);
+      const int rem = e - r * PX * NA;
       const int pxl = rem / NA, q = rem - pxl * NA;
+      if (pxl >= npx) continue;
       const int row = r == 0 ? py : pym;
       Bz[r][pxl * NA + q] =
-          rowpart[(((size_t)(zc - 1) * g.Ny + row) * g.Nx + px0 + pxl) * RPS + r * seg + q * NLV + ZC];
+          rowpart[(((size_t)(zc - 1) * g.Ny + row) * g.Nx + px0 + pxl) * RPS + r * SEG + q * NLV + ZC];
     }
   }
   __syncthreads();
   // levels this chunk completes: its bottom nk, and the top level on the last chunk
   const int nlev = k0 + nk == g.Nz ? nk + 1 : nk;
-  for (int e = threadIdx.x; e < nlev * npx; e += blockDim.x) {
-    const int L = e / npx, pxl = e - L * npx;
+  for (int e = threadIdx.x; e < nlev * PX; e += blockDim.x) {
+    const int L = e / PX, pxl = e - L * PX;
+    if (pxl >= npx) continue;
     R v[NA];
 #pragma unroll
     for (int q = 0; q < NA; ++q) v[q] = T[1][pxl * TS + q * NLV + L] + T[0][pxl * TS + q * NLV + L];
@@ -613,7 +623,7 @@ static cudaError_t run_p2g(const Geom& g, const int32_t* start, const int32_t* s
                                        (int)cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
   rows<<<nblk(nw, RW), 32 * RW, 0, st>>>(g, nzc, nxs, xseg, start, sorted, dx, dy, dz, ds, vol, a, rowpart);
-  dim3 gb((g.Nx + PXB - 1) / PXB, g.Ny, nzc);
+  dim3 gb((g.Nx + P2GPx<R>::value - 1) / P2GPx<R>::value, g.Ny, nzc);
   k_p2g_combine<NQ, MODE, R><<<gb, 256, 0, st>>>(g, nzc, rowpart, a);
   return cudaGetLastError();
 }

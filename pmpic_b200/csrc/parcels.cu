@@ -242,7 +242,7 @@ __device__ __forceinline__ int classify_dir(const Geom& g, double x, double y) {
 }
 
 template <bool GU, bool GP>
-__global__ void __launch_bounds__(256, 3) k_rk4(Geom g, int64_t n, RkPtrs P, int stage, const double* __restrict__ dtp,
+__global__ void __launch_bounds__(256, 4) k_rk4(Geom g, int64_t n, RkPtrs P, int stage, const double* __restrict__ dtp,
                       const int32_t* __restrict__ cell, const double* __restrict__ del, int64_t cap,
                       int8_t* __restrict__ dir) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -726,7 +726,7 @@ __device__ __forceinline__ int classify_dir_m(const Geom& g, int i, int j) {
 // reflection and the direction classification, as k_rk4; position updates in
 // cell units (velocity * dt / cell size), renormalised into [0, 1).
 template <bool GU, bool GP>
-__global__ void __launch_bounds__(256, 4) k_rk4_m(Geom g, int64_t n, MPtrs P, int stage, const double* __restrict__ dtp,
+__global__ void __launch_bounds__(256, 5) k_rk4_m(Geom g, int64_t n, MPtrs P, int stage, const double* __restrict__ dtp,
                         int8_t* __restrict__ dir) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
