@@ -272,11 +272,54 @@ size_t rowpart_bytes(const Geom& g);
 int prop_upload(pmpic_ctx* ctx, int pid, int64_t off, int64_t n, const double* src);
 int prop_download(pmpic_ctx* ctx, int pid, int64_t off, int64_t n, double* dst);
 // fft.cu
+// Elementwise operators fused into an inverse transform: one on its spectral
+// input, applied as the first (x) pass reads it, and one on its physical
+// output, applied as the last (y) pass writes it.  Each repeats the arithmetic
+// of the separate operator kernel it replaces (same operands, same order), so
+// fused and unfused sequences give the same bits.
+enum SpecOpKind {
+  SPEC_PLAIN = 0,
+  SPEC_DX,    // diffx (fft_ops.F90:266-295) of the input, tab = kx
+  SPEC_DY,    // diffy (fft_ops.F90:366-394) of the input, tab = ky
+  SPEC_FILT,  // the de-aliasing filter (fft_ops.F90:176-197), tab = filt
+  SPEC_VEL    // a velocity spectrum of vort2vel.F90:254-315 (see k_vel), no input array
+};
+template <class R>
+struct SpecIn {
+  int op = SPEC_PLAIN;
+  const R* tab = nullptr;
+  // SPEC_VEL: component vmode (0 u, 1 v, 2 w) from e, c (u, v) or a, b (w);
+  // its filtered copy is stored to fs; zbar is the mean flow of u or v
+  int vmode = 0;
+  const R *e = nullptr, *c = nullptr, *a = nullptr, *b = nullptr;
+  const R *kx = nullptr, *ky = nullptr, *filt = nullptr;
+  R* fs = nullptr;
+  const double* zbar = nullptr;
+};
+enum PhysOpKind {
+  PHYS_STORE = 0,
+  PHYS_ADD_MUL,      // o = o + in0 * v
+  PHYS_ADD_MUL_SUM,  // o = o + in0 * (in1 + v)
+  PHYS_NEG_ADD_MUL,  // o = -o + in0 * v
+  PHYS_DQ_DR         // o = o + in0 * (-in1 + v); o2 = in1 in3 + in2 v + in0 (-in4) + in0 (-in5)
+};
+template <class R>
+struct PhysOut {
+  int op = PHYS_STORE;
+  int store = 1;  // the transformed field itself is stored too
+  R* o = nullptr;
+  R* o2 = nullptr;
+  const R* in[6] = {};
+};
 int fft_init(pmpic_ctx* ctx);
 int fft_forward(pmpic_ctx* ctx, const double* phys, double* spec);
 int fft_backward(pmpic_ctx* ctx, const double* spec, double* phys);
 int fft_forward(pmpic_ctx* ctx, const float* phys, float* spec);
 int fft_backward(pmpic_ctx* ctx, const float* spec, float* phys);
+int fft_backward(pmpic_ctx* ctx, const double* spec, double* phys, const SpecIn<double>& si,
+                 const PhysOut<double>& po);
+int fft_backward(pmpic_ctx* ctx, const float* spec, float* phys, const SpecIn<float>& si,
+                 const PhysOut<float>& po);
 // spectral.cu
 int spec_diffx(pmpic_ctx* ctx, const double* in, double* out);
 int spec_diffy(pmpic_ctx* ctx, const double* in, double* out);

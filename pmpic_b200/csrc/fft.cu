@@ -153,13 +153,20 @@ int fft_forward(pmpic_ctx* ctx, const double* phys, double* spec) {
   return f64::fft_forward_impl(ctx, phys, spec, ctx->fftmid, (const double2*)ctx->ftw);
 }
 int fft_backward(pmpic_ctx* ctx, const double* spec, double* phys) {
-  return f64::fft_backward_impl(ctx, spec, phys, ctx->fftmid, (const double2*)ctx->ftw);
+  return fft_backward(ctx, spec, phys, SpecIn<double>{}, PhysOut<double>{});
+}
+int fft_backward(pmpic_ctx* ctx, const double* spec, double* phys, const SpecIn<double>& si,
+                 const PhysOut<double>& po) {
+  return f64::fft_backward_impl(ctx, spec, phys, ctx->fftmid, (const double2*)ctx->ftw, si, po);
 }
 int fft_forward(pmpic_ctx* ctx, const float* phys, float* spec) {
   return f32::fft_forward_impl(ctx, phys, spec, (float*)ctx->fftmid, (const float2*)ctx->ftw32);
 }
 int fft_backward(pmpic_ctx* ctx, const float* spec, float* phys) {
-  return f32::fft_backward_impl(ctx, spec, phys, (float*)ctx->fftmid, (const float2*)ctx->ftw32);
+  return fft_backward(ctx, spec, phys, SpecIn<float>{}, PhysOut<float>{});
+}
+int fft_backward(pmpic_ctx* ctx, const float* spec, float* phys, const SpecIn<float>& si, const PhysOut<float>& po) {
+  return f32::fft_backward_impl(ctx, spec, phys, (float*)ctx->fftmid, (const float2*)ctx->ftw32, si, po);
 }
 
 }  // namespace pmpic

@@ -194,10 +194,136 @@ __device__ __forceinline__ real2 c2r_pack(real2 A, real2 B, int k, int n) {
   return mk2(z.x, -z.y);  // conj for the forward-transform inverse
 }
 
+// The spectral values A (row ra) and B (row ra + 1) of x mode km as the
+// inverse x pass reads them, with the input operator applied.  ra is even and
+// Ny + 2 is even, so row ra holds the even y' index jp (the real part of a y
+// mode) and row ra + 1 the odd one of the same level lev; each value is the
+// element pair (2 km, 2 km + 1) of its row.  The operators repeat the
+// arithmetic of diffx, diffy and the filter (spectral_impl.cuh: dx_of, dy_of,
+// k_filter) and the velocity spectra of vort2vel.F90:251-320 (e - diffy(c),
+// diffx(c) - e, diffy(a) - diffx(b); the mean flow in mode (0, 0) of u and v).
+// own: this thread reads mode km unmirrored, so it stores the filtered
+// velocity spectrum of SPEC_VEL.
+__device__ __forceinline__ real2 ld2(const real* __restrict__ p, size_t i) { return *(const real2*)&p[i]; }
+__device__ __forceinline__ void st2(real* __restrict__ p, size_t i, real2 v) { *(real2*)&p[i] = v; }
+
+template <int OP>
+__device__ __forceinline__ void spec_pair(const Geom& g, const real* __restrict__ spec, const SpecIn<real>& S,
+                                          int64_t ra, int jp, int lev, int km, bool own, real2& A, real2& B) {
+  const size_t ea = (size_t)ra * g.sx + 2 * km, eb = ea + g.sx;
+  const int ca = jp * g.sx + 2 * km, cb = ca + g.sx;  // spectral columns of elements ea, eb
+  if constexpr (OP == SPEC_VEL) {
+    real2 va, vb;  // elements (ea, ea + 1), (eb, eb + 1)
+    if (S.vmode == 0) {  // f = e - diffy(c), f(:,1,1) = ubar
+      const real2 ea2 = ld2(S.e, ea), eb2 = ld2(S.e, eb), ca2 = ld2(S.c, ea), cb2 = ld2(S.c, eb);
+      const real2 ta = ld2(S.ky, ca), tb = ld2(S.ky, cb);
+      va = mk2(ea2.x - (real(-1) * cb2.x) * ta.x, ea2.y - (real(-1) * cb2.y) * ta.y);
+      vb = mk2(eb2.x - ca2.x * tb.x, eb2.y - ca2.y * tb.y);
+      if (ca == 0) va.x = (real)S.zbar[lev];
+    } else if (S.vmode == 1) {  // f = diffx(c) - e, f(:,1,1) = vbar
+      const real2 ea2 = ld2(S.e, ea), eb2 = ld2(S.e, eb), ca2 = ld2(S.c, ea), cb2 = ld2(S.c, eb);
+      const real2 ta = ld2(S.kx, ca), tb = ld2(S.kx, cb);
+      va = mk2((real(-1) * ca2.y) * ta.x - ea2.x, ca2.x * ta.y - ea2.y);
+      vb = mk2((real(-1) * cb2.y) * tb.x - eb2.x, cb2.x * tb.y - eb2.y);
+      if (ca == 0) va.x = (real)S.zbar[lev];
+    } else {  // f = diffy(a) - diffx(b)
+      const real2 aa = ld2(S.a, ea), ab = ld2(S.a, eb), ba = ld2(S.b, ea), bb = ld2(S.b, eb);
+      const real2 ya = ld2(S.ky, ca), yb = ld2(S.ky, cb), xa = ld2(S.kx, ca), xb = ld2(S.kx, cb);
+      va = mk2((real(-1) * ab.x) * ya.x - (real(-1) * ba.y) * xa.x, (real(-1) * ab.y) * ya.y - ba.x * xa.y);
+      vb = mk2(aa.x * yb.x - (real(-1) * bb.y) * xb.x, aa.y * yb.y - bb.x * xb.y);
+    }
+    if (own) {
+      const real2 fa = ld2(S.filt, ca), fb = ld2(S.filt, cb);
+      st2(S.fs, ea, mk2(va.x * fa.x, va.y * fa.y));
+      st2(S.fs, eb, mk2(vb.x * fb.x, vb.y * fb.y));
+    }
+    A = va;
+    B = vb;
+  } else {
+    const real2 a = ld2(spec, ea), b = ld2(spec, eb);
+    if constexpr (OP == SPEC_DX) {
+      const real2 ta = ld2(S.tab, ca), tb = ld2(S.tab, cb);
+      A = mk2((real(-1) * a.y) * ta.x, a.x * ta.y);
+      B = mk2((real(-1) * b.y) * tb.x, b.x * tb.y);
+    } else if constexpr (OP == SPEC_DY) {
+      const real2 ta = ld2(S.tab, ca), tb = ld2(S.tab, cb);
+      A = mk2((real(-1) * b.x) * ta.x, (real(-1) * b.y) * ta.y);
+      B = mk2(a.x * tb.x, a.y * tb.y);
+    } else if constexpr (OP == SPEC_FILT) {
+      const real2 ta = ld2(S.tab, ca), tb = ld2(S.tab, cb);
+      A = mk2(a.x * ta.x, a.y * ta.y);
+      B = mk2(b.x * tb.x, b.y * tb.y);
+    } else {
+      A = a;
+      B = b;
+    }
+  }
+}
+// the same with the operator chosen at run time (generic-length path)
+__device__ __forceinline__ void spec_pair_rt(const Geom& g, const real* __restrict__ spec, const SpecIn<real>& S,
+                                             int64_t ra, int jp, int lev, int km, bool own, real2& A, real2& B) {
+  switch (S.op) {
+    case SPEC_DX: spec_pair<SPEC_DX>(g, spec, S, ra, jp, lev, km, own, A, B); break;
+    case SPEC_DY: spec_pair<SPEC_DY>(g, spec, S, ra, jp, lev, km, own, A, B); break;
+    case SPEC_FILT: spec_pair<SPEC_FILT>(g, spec, S, ra, jp, lev, km, own, A, B); break;
+    case SPEC_VEL: spec_pair<SPEC_VEL>(g, spec, S, ra, jp, lev, km, own, A, B); break;
+    default: spec_pair<SPEC_PLAIN>(g, spec, S, ra, jp, lev, km, own, A, B); break;
+  }
+}
+
+// the output operator of an inverse transform at physical element i, v the
+// transformed value: the pointwise updates of vorticity_tendency.F90 in its
+// order of operations (dp :169-171, :180-181, :191-193; dq :213-214,
+// :224-225, :235-237; dr :250-264, with v = dw/dy)
+template <int OP>
+__device__ __forceinline__ real phys_op(const PhysOut<real>& E, size_t i, real v, real& o2) {
+  const real o = E.o[i];
+  if constexpr (OP == PHYS_ADD_MUL) return o + E.in[0][i] * v;
+  if constexpr (OP == PHYS_ADD_MUL_SUM) return o + E.in[0][i] * (E.in[1][i] + v);
+  if constexpr (OP == PHYS_NEG_ADD_MUL) return -o + E.in[0][i] * v;
+  if constexpr (OP == PHYS_DQ_DR) {
+    const real r = E.in[0][i], p = E.in[1][i];
+    real w = p * E.in[3][i];
+    w = w + E.in[2][i] * v;
+    w = w + r * (-E.in[4][i]);
+    w = w + r * (-E.in[5][i]);
+    o2 = w;
+    return o + r * (-p + v);
+  }
+  return o;
+}
+// two consecutive elements i, i + 1 (i even, rows of even length)
+template <int OP>
+__device__ __forceinline__ void phys_out2(const PhysOut<real>& E, real* __restrict__ phys, size_t i, real2 v) {
+  if (OP == PHYS_STORE || E.store) st2(phys, i, v);
+  if constexpr (OP != PHYS_STORE) {
+    real w0 = real(0), w1 = real(0);
+    const real o0 = phys_op<OP>(E, i, v.x, w0);
+    const real o1 = phys_op<OP>(E, i + 1, v.y, w1);
+    st2(E.o, i, mk2(o0, o1));
+    if constexpr (OP == PHYS_DQ_DR) st2(E.o2, i, mk2(w0, w1));
+  }
+}
+// one element, the operator chosen at run time (generic-length path)
+__device__ __forceinline__ void phys_out_rt(const PhysOut<real>& E, real* __restrict__ phys, size_t i, real v) {
+  if (E.op == PHYS_STORE || E.store) phys[i] = v;
+  real w = real(0);
+  switch (E.op) {
+    case PHYS_ADD_MUL: E.o[i] = phys_op<PHYS_ADD_MUL>(E, i, v, w); break;
+    case PHYS_ADD_MUL_SUM: E.o[i] = phys_op<PHYS_ADD_MUL_SUM>(E, i, v, w); break;
+    case PHYS_NEG_ADD_MUL: E.o[i] = phys_op<PHYS_NEG_ADD_MUL>(E, i, v, w); break;
+    case PHYS_DQ_DR:
+      E.o[i] = phys_op<PHYS_DQ_DR>(E, i, v, w);
+      E.o2[i] = w;
+      break;
+    default: break;
+  }
+}
+
 // ---- inverse x pass: spec -> mid ------------------------------------------------
 __global__ void __launch_bounds__(FFT_THREADS) k_inv_x(Geom g, int RP, int64_t nrows_total, FftPlan pl,
                                                        const real2* __restrict__ tw, const real* __restrict__ spec,
-                                                       real* __restrict__ mid) {
+                                                       real* __restrict__ mid, SpecIn<real> S) {
   extern __shared__ real2 sm[];
   const int Nx = g.Nx;
   real2* b0 = sm;
@@ -206,10 +332,12 @@ __global__ void __launch_bounds__(FFT_THREADS) k_inv_x(Geom g, int RP, int64_t n
   for (int e = threadIdx.x; e < RP * Nx; e += blockDim.x) {
     int r = e / Nx, k = e - r * Nx;
     int km = (2 * k <= Nx) ? k : Nx - k;
-    int64_t ra = row0 + 2 * r, rb = ra + 1;
+    int64_t ra = row0 + 2 * r;
     real2 A = mk2(real(0), real(0)), B = mk2(real(0), real(0));
-    if (ra < nrows_total) A = mk2(spec[(size_t)ra * g.sx + 2 * km], spec[(size_t)ra * g.sx + 2 * km + 1]);
-    if (rb < nrows_total) B = mk2(spec[(size_t)rb * g.sx + 2 * km], spec[(size_t)rb * g.sx + 2 * km + 1]);
+    if (ra < nrows_total) {
+      const int lev = (int)(ra / g.sy);
+      spec_pair_rt(g, spec, S, ra, (int)(ra - (int64_t)lev * g.sy), lev, km, 2 * k <= Nx, A, B);
+    }
     b0[r * Nx + k] = c2r_pack(A, B, k, Nx);
   }
   __syncthreads();
@@ -227,7 +355,8 @@ __global__ void __launch_bounds__(FFT_THREADS) k_inv_x(Geom g, int RP, int64_t n
 
 // ---- inverse y pass: mid -> phys ------------------------------------------------
 __global__ void __launch_bounds__(FFT_THREADS) k_inv_y(Geom g, int TXF, FftPlan pl, const real2* __restrict__ tw,
-                                                       const real* __restrict__ mid, real* __restrict__ phys) {
+                                                       const real* __restrict__ mid, real* __restrict__ phys,
+                                                       PhysOut<real> E) {
   extern __shared__ real2 sm[];
   const int Ny = g.Ny, Nx = g.Nx;
   const int nr = TXF / 2;
@@ -251,11 +380,11 @@ __global__ void __launch_bounds__(FFT_THREADS) k_inv_y(Geom g, int TXF, FftPlan 
   __syncthreads();
   real2* res = fft_rows(b0, b1, nr, Ny, pl, tw);
   const real dn = real(1) / (real)Ny;
-  real* P = phys + (size_t)k * Ny * Nx;
+  const size_t p0 = (size_t)k * Ny * Nx;
   for (int e = threadIdx.x; e < Ny * TXF; e += blockDim.x) {
     int j = e / TXF, x = e - j * TXF;
     real2 z = res[(x >> 1) * Ny + j];
-    P[(size_t)j * Nx + x0 + x] = (x & 1) == 0 ? z.x * dn : -z.y * dn;
+    phys_out_rt(E, phys, p0 + (size_t)j * Nx + x0 + x, (x & 1) == 0 ? z.x * dn : -z.y * dn);
   }
 }
 
@@ -391,24 +520,26 @@ __global__ void __launch_bounds__(FS_THREADS) k4_fwd_x(Geom g, int64_t nrows_tot
 }
 
 // inverse x pass (spec -> mid)
-template <int N1, int N2>
+template <int N1, int N2, int OP>
 __global__ void __launch_bounds__(FS_THREADS) k4_inv_x(Geom g, int64_t nrows_total, const real2* __restrict__ tw4,
-                                                       const real* __restrict__ spec, real* __restrict__ mid) {
+                                                       const real* __restrict__ spec, real* __restrict__ mid,
+                                                       SpecIn<real> S) {
   constexpr int N = N1 * N2, RP = FS_THREADS / (N1 > N2 ? N1 : N2), YS = N1 * (N2 + 1);
   __shared__ real2 Y[RP * YS];
   const int t = threadIdx.x;
   const int64_t row0 = (int64_t)blockIdx.x * RP * 2;
   if (t < RP * N2) {
     const int r = t / N2, n2 = t % N2;
-    const int64_t ra = row0 + 2 * r, rb = ra + 1;
+    const int64_t ra = row0 + 2 * r;
+    const bool valid = ra < nrows_total;  // then so is ra + 1: the row count is even
+    const int lev = (int)(ra / g.sy), jp = (int)(ra - (int64_t)lev * g.sy);
     real2 a[N1];
 #pragma unroll
     for (int n1 = 0; n1 < N1; ++n1) {
       const int k = n2 + N2 * n1;
       const int km = (2 * k <= N) ? k : N - k;
       real2 A = mk2(real(0), real(0)), B = mk2(real(0), real(0));
-      if (ra < nrows_total) A = mk2(spec[(size_t)ra * g.sx + 2 * km], spec[(size_t)ra * g.sx + 2 * km + 1]);
-      if (rb < nrows_total) B = mk2(spec[(size_t)rb * g.sx + 2 * km], spec[(size_t)rb * g.sx + 2 * km + 1]);
+      if (valid) spec_pair<OP>(g, spec, S, ra, jp, lev, km, 2 * k <= N, A, B);
       a[n1] = c2r_pack(A, B, k, N);
     }
     fs_step1<N1, N2>(a, n2, Y + r * YS, tw4);
@@ -485,9 +616,10 @@ __global__ void __launch_bounds__(FS_THREADS) k4_fwd_y(Geom g, const real2* __re
 }
 
 // inverse y pass (mid -> phys)
-template <int N1, int N2>
+template <int N1, int N2, int OP>
 __global__ void __launch_bounds__(FS_THREADS) k4_inv_y(Geom g, const real2* __restrict__ tw4,
-                                                       const real* __restrict__ mid, real* __restrict__ phys) {
+                                                       const real* __restrict__ mid, real* __restrict__ phys,
+                                                       PhysOut<real> E) {
   // rows of Y and X are padded so the 8 column pairs of a warp access fall in
   // distinct shared-memory banks
   constexpr int N = N1 * N2, RP = 8, YS = N1 * (N2 + 1) + 1;
@@ -514,12 +646,10 @@ __global__ void __launch_bounds__(FS_THREADS) k4_inv_y(Geom g, const real2* __re
     const int r = t % RP, k1 = t / RP;
     real2 a[N2];
     fs_step3<N1, N2>(a, k1, Y + r * YS);
-    real* P = phys + (size_t)k * N * Nx;
+    const size_t p0 = (size_t)k * N * Nx + x0 + 2 * r;
 #pragma unroll
-    for (int k2 = 0; k2 < N2; ++k2) {
-      const int j = k1 + N1 * k2;
-      *(real2*)&P[(size_t)j * Nx + x0 + 2 * r] = mk2(a[k2].x * dn, -a[k2].y * dn);
-    }
+    for (int k2 = 0; k2 < N2; ++k2)
+      phys_out2<OP>(E, phys, p0 + (size_t)(k1 + N1 * k2) * Nx, mk2(a[k2].x * dn, -a[k2].y * dn));
   }
 }
 
@@ -538,11 +668,22 @@ bool fs_fwd_x(int n1, int n2, unsigned nb, cudaStream_t st, const Geom& g, int64
   PMPIC_FS_CASES(CALL)
 #undef CALL
 }
-bool fs_inv_x(int n1, int n2, unsigned nb, cudaStream_t st, const Geom& g, int64_t nrows, const real2* tw4,
-              const real* spec, real* mid) {
-#define CALL(A, B) k4_inv_x<A, B><<<nb, FS_THREADS, 0, st>>>(g, nrows, tw4, spec, mid)
+template <int OP>
+bool fs_inv_x_op(int n1, int n2, unsigned nb, cudaStream_t st, const Geom& g, int64_t nrows, const real2* tw4,
+                 const real* spec, real* mid, const SpecIn<real>& S) {
+#define CALL(A, B) k4_inv_x<A, B, OP><<<nb, FS_THREADS, 0, st>>>(g, nrows, tw4, spec, mid, S)
   PMPIC_FS_CASES(CALL)
 #undef CALL
+}
+bool fs_inv_x(int n1, int n2, unsigned nb, cudaStream_t st, const Geom& g, int64_t nrows, const real2* tw4,
+              const real* spec, real* mid, const SpecIn<real>& S) {
+  switch (S.op) {
+    case SPEC_DX: return fs_inv_x_op<SPEC_DX>(n1, n2, nb, st, g, nrows, tw4, spec, mid, S);
+    case SPEC_DY: return fs_inv_x_op<SPEC_DY>(n1, n2, nb, st, g, nrows, tw4, spec, mid, S);
+    case SPEC_FILT: return fs_inv_x_op<SPEC_FILT>(n1, n2, nb, st, g, nrows, tw4, spec, mid, S);
+    case SPEC_VEL: return fs_inv_x_op<SPEC_VEL>(n1, n2, nb, st, g, nrows, tw4, spec, mid, S);
+    default: return fs_inv_x_op<SPEC_PLAIN>(n1, n2, nb, st, g, nrows, tw4, spec, mid, S);
+  }
 }
 bool fs_fwd_y(int n1, int n2, dim3 gr, cudaStream_t st, const Geom& g, const real2* tw4, const real* phys,
               real* mid) {
@@ -550,11 +691,22 @@ bool fs_fwd_y(int n1, int n2, dim3 gr, cudaStream_t st, const Geom& g, const rea
   PMPIC_FS_CASES(CALL)
 #undef CALL
 }
-bool fs_inv_y(int n1, int n2, dim3 gr, cudaStream_t st, const Geom& g, const real2* tw4, const real* mid,
-              real* phys) {
-#define CALL(A, B) k4_inv_y<A, B><<<gr, FS_THREADS, 0, st>>>(g, tw4, mid, phys)
+template <int OP>
+bool fs_inv_y_op(int n1, int n2, dim3 gr, cudaStream_t st, const Geom& g, const real2* tw4, const real* mid,
+                 real* phys, const PhysOut<real>& E) {
+#define CALL(A, B) k4_inv_y<A, B, OP><<<gr, FS_THREADS, 0, st>>>(g, tw4, mid, phys, E)
   PMPIC_FS_CASES(CALL)
 #undef CALL
+}
+bool fs_inv_y(int n1, int n2, dim3 gr, cudaStream_t st, const Geom& g, const real2* tw4, const real* mid,
+              real* phys, const PhysOut<real>& E) {
+  switch (E.op) {
+    case PHYS_ADD_MUL: return fs_inv_y_op<PHYS_ADD_MUL>(n1, n2, gr, st, g, tw4, mid, phys, E);
+    case PHYS_ADD_MUL_SUM: return fs_inv_y_op<PHYS_ADD_MUL_SUM>(n1, n2, gr, st, g, tw4, mid, phys, E);
+    case PHYS_NEG_ADD_MUL: return fs_inv_y_op<PHYS_NEG_ADD_MUL>(n1, n2, gr, st, g, tw4, mid, phys, E);
+    case PHYS_DQ_DR: return fs_inv_y_op<PHYS_DQ_DR>(n1, n2, gr, st, g, tw4, mid, phys, E);
+    default: return fs_inv_y_op<PHYS_STORE>(n1, n2, gr, st, g, tw4, mid, phys, E);
+  }
 }
 #undef PMPIC_FS_CASES
 
@@ -589,7 +741,8 @@ int fft_forward_impl(pmpic_ctx* ctx, const real* phys, real* spec, real* mid, co
   return 0;
 }
 
-int fft_backward_impl(pmpic_ctx* ctx, const real* spec, real* phys, real* mid, const real2* tw) {
+int fft_backward_impl(pmpic_ctx* ctx, const real* spec, real* phys, real* mid, const real2* tw, const SpecIn<real>& S,
+                      const PhysOut<real>& E) {
   TimerScope ts(ctx, T_FFTI);
   const Geom& g = ctx->g;
   const FftPlan& px = ctx->plan_x;
@@ -598,23 +751,23 @@ int fft_backward_impl(pmpic_ctx* ctx, const real* spec, real* phys, real* mid, c
   if (px.n1) {
     const int rp = FS_THREADS / std::max(px.n1, px.n2);
     fs_inv_x(px.n1, px.n2, (unsigned)((nrows + 2 * rp - 1) / (2 * rp)), ctx->stream, g, nrows, tw + px.tw4_off,
-             spec, mid);
+             spec, mid, S);
   } else {
     int rp = pick_rp(g.Nx);
     size_t sm_x = sizeof(real2) * (size_t)rp * g.Nx * 2;
     k_inv_x<<<(unsigned)((nrows + 2 * rp - 1) / (2 * rp)), FFT_THREADS, sm_x, ctx->stream>>>(g, rp, nrows, px, tw,
-                                                                                          spec, mid);
+                                                                                          spec, mid, S);
   }
   ++ctx->nlaunch;
   const real2* twy = tw + ctx->ftw_off_y;
   if (py.n1) {
-    fs_inv_y(py.n1, py.n2, dim3(g.Nx / 16, g.nzp), ctx->stream, g, twy + py.tw4_off, mid, phys);
+    fs_inv_y(py.n1, py.n2, dim3(g.Nx / 16, g.nzp), ctx->stream, g, twy + py.tw4_off, mid, phys, E);
   } else {
     int txf = pick_txf(g.Nx);
     size_t half = (size_t)g.Ny / 2 + 1;
     size_t sm_y = sizeof(real2) * std::max((size_t)(txf / 2) * g.Ny * 2, (size_t)(txf / 2) * g.Ny + txf * half);
     dim3 gy(g.Nx / txf, g.nzp);
-    k_inv_y<<<gy, FFT_THREADS, sm_y, ctx->stream>>>(g, txf, py, twy, mid, phys);
+    k_inv_y<<<gy, FFT_THREADS, sm_y, ctx->stream>>>(g, txf, py, twy, mid, phys, E);
   }
   ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());

@@ -27,16 +27,18 @@ inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 // mean flow of the zero mode (vort2vel.F90:230-241), one thread: the trapezoid
 // integral and the reference's average (`1./nz` in REAL(4), 0.5*ubar(nz) added
 // to every element before the sum).
-// d, e: the zero-mode values of level k at d[k * stride], e[k * stride]
+// d, e: the zero-mode values of level k at d[k * stride], e[k * stride],
+// multiplied by the filter's zero-mode factor *filt when filt is given (the
+// filtered d = filter(a), e = filter(b) of vort2vel.F90:208-209)
 __global__ void k_zmode(Geom g, const double* __restrict__ d, const double* __restrict__ e, int64_t stride,
-                        double* __restrict__ zb) {
+                        const double* __restrict__ filt, double* __restrict__ zb) {
   extern __shared__ double zs[];  // e(:,1,1), d(:,1,1), then ubar, vbar
   const int nz = g.nzp;
   double* es = zs;
   double* ds = zs + nz;
   for (int k = threadIdx.x; k < nz; k += blockDim.x) {  // stage the zero-mode columns
-    es[k] = e[k * stride];
-    ds[k] = d[k * stride];
+    es[k] = filt ? e[k * stride] * filt[0] : e[k * stride];
+    ds[k] = filt ? d[k * stride] * filt[0] : d[k * stride];
   }
   __syncthreads();
   if (threadIdx.x != 0) return;
@@ -160,10 +162,11 @@ inline const double* tab_k2(pmpic_ctx* c) { return c->k2; }
 inline const double* tab_filt(pmpic_ctx* c) { return c->filt; }
 inline const double* tab_diffz(pmpic_ctx* c, int which) { return c->sscratch + c->g.nspec + which * 3 * c->g.nzp; }
 inline void zero_mode_prepare(pmpic_ctx*) {}
-// the mean flow from the transformed columns kx = ky = 0 (vort2vel.F90:230-241)
-inline int zero_mode_launch(pmpic_ctx* ctx, const double* d, const double* e) {
+// the mean flow from the columns kx = ky = 0 of the filtered a and b
+// (vort2vel.F90:230-241); a, b are the unfiltered spectra
+inline int zero_mode_launch(pmpic_ctx* ctx, const double* a, const double* b) {
   const Geom& g = ctx->g;
-  k_zmode<<<1, 256, sizeof(double) * 4 * g.nzp, ctx->stream>>>(g, d, e, (int64_t)g.sx * g.sy, ctx->zmode); ++ctx->nlaunch;
+  k_zmode<<<1, 256, sizeof(double) * 4 * g.nzp, ctx->stream>>>(g, a, b, (int64_t)g.sx * g.sy, ctx->filt, ctx->zmode); ++ctx->nlaunch;
   return 0;
 }
 #include "spectral_impl.cuh"
@@ -185,7 +188,7 @@ inline void zero_mode_prepare(pmpic_ctx* ctx) {
 }
 inline int zero_mode_launch(pmpic_ctx* ctx, const float*, const float*) {
   const Geom& g = ctx->g;
-  k_zmode<<<1, 256, sizeof(double) * 4 * g.nzp, ctx->stream>>>(g, ctx->hsum, ctx->hsum + g.nzp, 1, ctx->zmode); ++ctx->nlaunch;
+  k_zmode<<<1, 256, sizeof(double) * 4 * g.nzp, ctx->stream>>>(g, ctx->hsum, ctx->hsum + g.nzp, 1, nullptr, ctx->zmode); ++ctx->nlaunch;
   return 0;
 }
 #include "spectral_impl.cuh"

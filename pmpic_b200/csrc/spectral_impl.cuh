@@ -94,49 +94,16 @@ __global__ void k_sub_zero0(Geom g, real* __restrict__ c, const real* __restrict
   c[x.e] = v;
 }
 
-// d,e,f = filter(a,b,c) and the top/bottom planes of a and b (vort2vel.F90:208-217)
-__global__ void k_filter3_bt(Geom g, const real* __restrict__ a, const real* __restrict__ b,
-                             const real* __restrict__ c, real* __restrict__ d, real* __restrict__ e,
-                             real* __restrict__ f, const real* __restrict__ filt, real* __restrict__ bt) {
-  EwIdx x;
-  if (!ew_index(g, x)) return;
-  real m = filt[x.col];
-  d[x.e] = a[x.e] * m;
-  e[x.e] = b[x.e] * m;
-  f[x.e] = c[x.e] * m;
+// the top and bottom planes of a and b, unfiltered (vort2vel.F90:213-218)
+__global__ void k_bt_planes(Geom g, const real* __restrict__ a, const real* __restrict__ b, real* __restrict__ bt) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
   const int cols = g.sx * g.sy;
-  if (x.k == g.nzp - 1) {
-    bt[0 * cols + x.col] = a[x.e];  // atop
-    bt[2 * cols + x.col] = b[x.e];  // btop
-  }
-  if (x.k == 0) {
-    bt[1 * cols + x.col] = a[x.e];  // abot
-    bt[3 * cols + x.col] = b[x.e];  // bbot
-  }
-}
-
-// Velocity components from the potentials (vort2vel.F90:254-315):
-//  mode 0: f = e - diffy(c), f(:,1,1) = ubar, u_s = filter(f)
-//  mode 1: f = diffx(c) - e, f(:,1,1) = vbar, v_s = filter(f)
-//  mode 2: f = diffy(a) - diffx(b),             w_s = filter(f)
-__global__ void k_vel(Geom g, int mode, const real* __restrict__ e, const real* __restrict__ c,
-                      const real* __restrict__ a, const real* __restrict__ b, real* __restrict__ f,
-                      real* __restrict__ fs, const real* __restrict__ kx, const real* __restrict__ ky,
-                      const real* __restrict__ filt, const double* __restrict__ zbar) {
-  EwIdx x;
-  if (!ew_index(g, x)) return;
-  real v;
-  if (mode == 0) {
-    v = e[x.e] - dy_of(c, x.e, x.jp, g.sx, ky, x.col);
-    if (x.col == 0) v = (real)zbar[x.k];
-  } else if (mode == 1) {
-    v = dx_of(c, x.e, x.ip, kx, x.col) - e[x.e];
-    if (x.col == 0) v = (real)zbar[x.k];
-  } else {
-    v = dy_of(a, x.e, x.jp, g.sx, ky, x.col) - dx_of(b, x.e, x.ip, kx, x.col);
-  }
-  f[x.e] = v;
-  fs[x.e] = v * filt[x.col];
+  if (col >= cols) return;
+  const size_t top = (size_t)(g.nzp - 1) * cols + col;
+  bt[0 * cols + col] = a[top];  // atop
+  bt[1 * cols + col] = a[col];  // abot
+  bt[2 * cols + col] = b[top];  // btop
+  bt[3 * cols + col] = b[col];  // bbot
 }
 
 // ---- compact z operators ----------------------------------------------------------
@@ -299,40 +266,6 @@ __global__ void k_laplinv(Geom g, LapBatch lb, real* __restrict__ cpbase, const 
   }
 }
 
-// ---- vorticity tendency pointwise combinations (vorticity_tendency.F90:169-265)
-__global__ void k_pw_add_mul(int64_t n, real* __restrict__ o, const real* __restrict__ a,
-                             const real* __restrict__ b) {  // o = o + a*b
-  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e < n) o[e] = o[e] + a[e] * b[e];
-}
-__global__ void k_pw_add_mul_sum(int64_t n, real* __restrict__ o, const real* __restrict__ r,
-                                 const real* __restrict__ q, const real* __restrict__ w) {  // o = o + r*(q + w)
-  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e < n) o[e] = o[e] + r[e] * (q[e] + w[e]);
-}
-__global__ void k_pw_neg_add_mul(int64_t n, real* __restrict__ o, const real* __restrict__ a,
-                                 const real* __restrict__ b) {  // o = -o + a*b
-  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e < n) o[e] = -o[e] + a[e] * b[e];
-}
-__global__ void k_pw_add_mul_negsum(int64_t n, real* __restrict__ o, const real* __restrict__ r,
-                                    const real* __restrict__ p, const real* __restrict__ w) {  // o = o + r*(-p + w)
-  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e < n) o[e] = o[e] + r[e] * (-p[e] + w[e]);
-}
-__global__ void k_pw_dr(int64_t n, real* __restrict__ dr, const real* __restrict__ p,
-                        const real* __restrict__ q, const real* __restrict__ r, const real* __restrict__ dwdx,
-                        const real* __restrict__ dwdy, const real* __restrict__ dudx,
-                        const real* __restrict__ dvdy) {
-  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n) return;
-  real v = p[e] * dwdx[e];
-  v = v + q[e] * dwdy[e];
-  v = v + r[e] * (-dudx[e]);
-  v = v + r[e] * (-dvdy[e]);
-  dr[e] = v;
-}
-
 // max of squares over the interior (vort2vel.F90:331-338,
 // vorticity_tendency.F90:279-282); non-negative doubles order like their bits
 __global__ void k_max_sq3(int64_t n, const real* __restrict__ u, const real* __restrict__ v,
@@ -433,11 +366,17 @@ int vort2vel_spectral_impl(pmpic_ctx* ctx) {
   k_sub_diff<<<nb, 256, 0, ctx->stream>>>(g, b, f, tab_ky(ctx), 1); ++ctx->nlaunch;
   if ((rc = diffz_launch_impl(ctx, f, d, nullptr, nullptr))) return rc;
   k_sub_zero0<<<nb, 256, 0, ctx->stream>>>(g, c, d); ++ctx->nlaunch;
-  k_filter3_bt<<<nb, 256, 0, ctx->stream>>>(g, a, b, c, d, e, f, tab_filt(ctx), RP(ctx->bt)); ++ctx->nlaunch;
-  if ((rc = fft_backward(ctx, d, G[PMPIC_GRID_P]))) return rc;
-  if ((rc = fft_backward(ctx, e, G[PMPIC_GRID_Q]))) return rc;
-  if ((rc = fft_backward(ctx, f, G[PMPIC_GRID_R]))) return rc;
-  if ((rc = zero_mode_launch(ctx, d, e))) return rc;
+  // :207-226: the top and bottom planes of a and b, then the filtered a, b, c
+  // transformed back (the filter applied as the transform reads them)
+  k_bt_planes<<<nblk(cols, 256), 256, 0, ctx->stream>>>(g, a, b, RP(ctx->bt)); ++ctx->nlaunch;
+  SpecIn<real> F;
+  F.op = SPEC_FILT;
+  F.tab = tab_filt(ctx);
+  const PhysOut<real> plain;
+  if ((rc = fft_backward(ctx, a, G[PMPIC_GRID_P], F, plain))) return rc;
+  if ((rc = fft_backward(ctx, b, G[PMPIC_GRID_Q], F, plain))) return rc;
+  if ((rc = fft_backward(ctx, c, G[PMPIC_GRID_R], F, plain))) return rc;
+  if ((rc = zero_mode_launch(ctx, a, b))) return rc;
   {
     real* abc[3] = {a, b, c};
     const bool df[3] = {false, false, true};
@@ -447,60 +386,83 @@ int vort2vel_spectral_impl(pmpic_ctx* ctx) {
   const real* abot = RP(ctx->bt) + cols;
   const real* btop = RP(ctx->bt) + 2 * cols;
   const real* bbot = RP(ctx->bt) + 3 * cols;
-  // u = dB/dz - dC/dy
+  // each velocity spectrum is formed as its inverse transform reads it, which
+  // also stores the filtered copy (u_s, v_s, w_s)
+  SpecIn<real> V;
+  V.op = SPEC_VEL;
+  V.e = e;
+  V.c = c;
+  V.a = a;
+  V.b = b;
+  V.kx = tab_kx(ctx);
+  V.ky = tab_ky(ctx);
+  V.filt = tab_filt(ctx);
+  // u = dB/dz - dC/dy (:251-276)
   if ((rc = diffz_launch_impl(ctx, b, e, bbot, btop))) return rc;
-  k_vel<<<nb, 256, 0, ctx->stream>>>(g, 0, e, c, a, b, f, RP(ctx->spec[PMPIC_SPEC_U]), tab_kx(ctx), tab_ky(ctx), tab_filt(ctx),
-                                     ctx->zmode); ++ctx->nlaunch;
-  if ((rc = fft_backward(ctx, f, G[PMPIC_GRID_U]))) return rc;
-  // v = dC/dx - dA/dz
+  V.vmode = 0;
+  V.fs = RP(ctx->spec[PMPIC_SPEC_U]);
+  V.zbar = ctx->zmode;
+  if ((rc = fft_backward(ctx, nullptr, G[PMPIC_GRID_U], V, plain))) return rc;
+  // v = dC/dx - dA/dz (:280-302)
   if ((rc = diffz_launch_impl(ctx, a, e, abot, atop))) return rc;
-  k_vel<<<nb, 256, 0, ctx->stream>>>(g, 1, e, c, a, b, f, RP(ctx->spec[PMPIC_SPEC_V]), tab_kx(ctx), tab_ky(ctx), tab_filt(ctx),
-                                     ctx->zmode + g.nzp); ++ctx->nlaunch;
-  if ((rc = fft_backward(ctx, f, G[PMPIC_GRID_V]))) return rc;
-  // w = dA/dy - dB/dx
-  k_vel<<<nb, 256, 0, ctx->stream>>>(g, 2, e, c, a, b, f, RP(ctx->spec[PMPIC_SPEC_W]), tab_kx(ctx), tab_ky(ctx), tab_filt(ctx),
-                                     ctx->zmode); ++ctx->nlaunch;
-  if ((rc = fft_backward(ctx, f, G[PMPIC_GRID_W]))) return rc;
+  V.vmode = 1;
+  V.fs = RP(ctx->spec[PMPIC_SPEC_V]);
+  V.zbar = ctx->zmode + g.nzp;
+  if ((rc = fft_backward(ctx, nullptr, G[PMPIC_GRID_V], V, plain))) return rc;
+  // w = dA/dy - dB/dx (:306-320)
+  V.vmode = 2;
+  V.fs = RP(ctx->spec[PMPIC_SPEC_W]);
+  V.zbar = nullptr;
+  if ((rc = fft_backward(ctx, nullptr, G[PMPIC_GRID_W], V, plain))) return rc;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
 
 // vorticity_tendency.F90:147-265 (grid B holds par2grid(btot) on entry).
+// Each spectral derivative is applied as its inverse transform reads it, and
+// each pointwise update of dp, dq, dr as the transform writes its result, so
+// no derivative spectrum or intermediate grid makes a round trip through HBM.
 int vorticity_tendency_grids_impl(pmpic_ctx* ctx) {
-  const Geom& g = ctx->g;
   int rc;
-  real *bs = RP(ctx->sbs), *as = RP(ctx->sas);
+  real *bs = RP(ctx->sbs);
   real* const* G = (real* const*)ctx->grid;
   real *DP = G[PMPIC_GRID_DP], *DQ = G[PMPIC_GRID_DQ], *DR = G[PMPIC_GRID_DR];
   const real *P = G[PMPIC_GRID_P], *Q = G[PMPIC_GRID_Q], *R = G[PMPIC_GRID_R];
-  real *dudx = RP(ctx->gwork[0]), *dwdx = RP(ctx->gwork[1]), *dvdy = RP(ctx->gwork[2]), *dwdy = RP(ctx->gwork[3]);
-  real* ap = RP(ctx->gwork[4]);
-  const int64_t n = g.nphys;
-  const unsigned nb = nblk(n, 256);
+  real *dudx = RP(ctx->gwork[0]), *dwdx = RP(ctx->gwork[1]), *dvdy = RP(ctx->gwork[2]);
+  const real *us = RP(ctx->spec[PMPIC_SPEC_U]), *vs = RP(ctx->spec[PMPIC_SPEC_V]), *ws = RP(ctx->spec[PMPIC_SPEC_W]);
+  SpecIn<real> DX, DY;
+  DX.op = SPEC_DX;
+  DX.tab = tab_kx(ctx);
+  DY.op = SPEC_DY;
+  DY.tab = tab_ky(ctx);
+  auto epi = [](int op, int store, real* o, const real* a, const real* b) {
+    PhysOut<real> E;
+    E.op = op;
+    E.store = store;
+    E.o = o;
+    E.in[0] = a;
+    E.in[1] = b;
+    return E;
+  };
+  const PhysOut<real> plain;
   if ((rc = fft_forward(ctx, G[PMPIC_GRID_B], bs))) return rc;
-  if ((rc = spec_diffy_impl(ctx, bs, as))) return rc;
-  if ((rc = fft_backward(ctx, as, DP))) return rc;
-  if ((rc = spec_diffx_impl(ctx, RP(ctx->spec[PMPIC_SPEC_U]), as))) return rc;
-  if ((rc = fft_backward(ctx, as, dudx))) return rc;
-  k_pw_add_mul<<<nb, 256, 0, ctx->stream>>>(n, DP, P, dudx); ++ctx->nlaunch;
-  if ((rc = spec_diffy_impl(ctx, RP(ctx->spec[PMPIC_SPEC_U]), as))) return rc;
-  if ((rc = fft_backward(ctx, as, ap))) return rc;
-  k_pw_add_mul<<<nb, 256, 0, ctx->stream>>>(n, DP, Q, ap); ++ctx->nlaunch;
-  if ((rc = spec_diffx_impl(ctx, RP(ctx->spec[PMPIC_SPEC_W]), as))) return rc;
-  if ((rc = fft_backward(ctx, as, dwdx))) return rc;
-  k_pw_add_mul_sum<<<nb, 256, 0, ctx->stream>>>(n, DP, R, Q, dwdx); ++ctx->nlaunch;
-  if ((rc = spec_diffx_impl(ctx, bs, as))) return rc;
-  if ((rc = fft_backward(ctx, as, DQ))) return rc;
-  if ((rc = spec_diffx_impl(ctx, RP(ctx->spec[PMPIC_SPEC_V]), as))) return rc;
-  if ((rc = fft_backward(ctx, as, ap))) return rc;
-  k_pw_neg_add_mul<<<nb, 256, 0, ctx->stream>>>(n, DQ, P, ap); ++ctx->nlaunch;
-  if ((rc = spec_diffy_impl(ctx, RP(ctx->spec[PMPIC_SPEC_V]), as))) return rc;
-  if ((rc = fft_backward(ctx, as, dvdy))) return rc;
-  k_pw_add_mul<<<nb, 256, 0, ctx->stream>>>(n, DQ, Q, dvdy); ++ctx->nlaunch;
-  if ((rc = spec_diffy_impl(ctx, RP(ctx->spec[PMPIC_SPEC_W]), as))) return rc;
-  if ((rc = fft_backward(ctx, as, dwdy))) return rc;
-  k_pw_add_mul_negsum<<<nb, 256, 0, ctx->stream>>>(n, DQ, R, P, dwdy); ++ctx->nlaunch;
-  k_pw_dr<<<nb, 256, 0, ctx->stream>>>(n, DR, P, Q, R, dwdx, dwdy, dudx, dvdy); ++ctx->nlaunch;
+  // dp = db/dy + p du/dx + q du/dy + r (q + dw/dx)
+  if ((rc = fft_backward(ctx, bs, DP, DY, plain))) return rc;
+  if ((rc = fft_backward(ctx, us, dudx, DX, epi(PHYS_ADD_MUL, 1, DP, P, nullptr)))) return rc;
+  if ((rc = fft_backward(ctx, us, nullptr, DY, epi(PHYS_ADD_MUL, 0, DP, Q, nullptr)))) return rc;
+  if ((rc = fft_backward(ctx, ws, dwdx, DX, epi(PHYS_ADD_MUL_SUM, 1, DP, R, Q)))) return rc;
+  // dq = -db/dx + p dv/dx + q dv/dy + r (-p + dw/dy)
+  if ((rc = fft_backward(ctx, bs, DQ, DX, plain))) return rc;
+  if ((rc = fft_backward(ctx, vs, nullptr, DX, epi(PHYS_NEG_ADD_MUL, 0, DQ, P, nullptr)))) return rc;
+  if ((rc = fft_backward(ctx, vs, dvdy, DY, epi(PHYS_ADD_MUL, 1, DQ, Q, nullptr)))) return rc;
+  // ... and, with dw/dy, dr = p dw/dx + q dw/dy - r du/dx - r dv/dy
+  PhysOut<real> last = epi(PHYS_DQ_DR, 0, DQ, R, P);
+  last.o2 = DR;
+  last.in[2] = Q;
+  last.in[3] = dwdx;
+  last.in[4] = dudx;
+  last.in[5] = dvdy;
+  if ((rc = fft_backward(ctx, ws, nullptr, DY, last))) return rc;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
