@@ -83,6 +83,14 @@ __device__ __forceinline__ bool bin_parcel(const Geom& g, double xp, double yp, 
   return true;
 }
 
+// one integer atomic per distinct cell of the warp (neighbouring slots mostly
+// share a cell): the per-cell histogram of the binning
+__device__ __forceinline__ void count_cell(int32_t id, int32_t* __restrict__ count) {
+  const unsigned act = __activemask();
+  const unsigned same = __match_any_sync(act, id);
+  if ((threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&count[id], __popc(same));
+}
+
 // ---- mixed-precision form --------------------------------------------------
 // A position component of the mixed form: the integer cell index along the axis
 // and the FP32 offset inside the cell in cell units, so x = (i + f) * dx.  It
@@ -191,6 +199,8 @@ struct pmpic_ctx {
   int32_t* cell;             // cap: interior cell id per slot, z fastest: (i*Ny + j)*Nz + k
   double* del;               // 3 x cap: cached delx, dely, delz per slot
   bool sorted_valid;         // cell ids, offsets and cell lists match the current positions
+  bool count_ready;          // mixed form: cell ids and per-cell counts were written by the
+                             // last RK4 stage and haloswap, so binning starts at the scan
   bool btot_grid_ready;      // gspare holds par2grid(btot) of the current substep
   bool pending_uvw;          // vort2vel's grid2par of u, v, w not yet applied
   bool pending_pqr;          // vorticity_tendency's grid2par of dp, dq, dr not yet applied

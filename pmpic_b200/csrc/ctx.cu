@@ -225,6 +225,7 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   ctx->cap = cfg->max_parcels;
   ctx->n = 0;
   ctx->sorted_valid = false;
+  ctx->count_ready = false;
   ctx->btot_grid_ready = false;
   ctx->pending_uvw = ctx->pending_pqr = ctx->dir_ready = false;
   ctx->nbmax = (std::max<int64_t>(ctx->cap, g.ncell) + 1023) / 1024 + 8;
@@ -463,6 +464,7 @@ int pmpic_set_count(pmpic_ctx* ctx, int64_t n) {
   ctx->n = n;
   ctx->info.n_parcels = n;
   ctx->sorted_valid = false;
+  ctx->count_ready = false;
   ctx->btot_grid_ready = false;
   ctx->dir_ready = false;
   return PMPIC_OK;
@@ -483,6 +485,7 @@ int pmpic_set_property(pmpic_ctx* ctx, int p, int64_t n, const double* src) {
   if (rc) return rc;
   PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
   ctx->sorted_valid = false;
+  ctx->count_ready = false;
   ctx->btot_grid_ready = false;
   return PMPIC_OK;
 }
@@ -527,6 +530,7 @@ int pmpic_upload_parcels(pmpic_ctx* ctx, int64_t n, const double* x, const doubl
   ctx->n = n;
   ctx->info.n_parcels = n;
   ctx->sorted_valid = false;
+  ctx->count_ready = false;
   ctx->btot_grid_ready = false;
   return PMPIC_OK;
 }
@@ -974,6 +978,7 @@ int pmpic_sort_parcels(pmpic_ctx* ctx) {
   cudaFree(tmp);
   if (rc) return rc;
   ctx->sorted_valid = false;
+  ctx->count_ready = false;
   ctx->btot_grid_ready = false;
   ctx->dir_ready = false;
   return sync_info(ctx);

@@ -207,56 +207,66 @@ __device__ __forceinline__ real2 c2r_pack(real2 A, real2 B, int k, int n) {
 __device__ __forceinline__ real2 ld2(const real* __restrict__ p, size_t i) { return *(const real2*)&p[i]; }
 __device__ __forceinline__ void st2(real* __restrict__ p, size_t i, real2 v) { *(real2*)&p[i] = v; }
 
+// The operator on the values of one spectral element pair of rows ra (xa)
+// and ra + 1 (xb); ca, cb are their spectral columns, lev their level.  For
+// SPEC_VEL x is e (u, v) or a (w) and y is c (u, v) or b (w).
+template <int OP>
+__device__ __forceinline__ void spec_op(const SpecIn<real>& S, real2 xa, real2 xb, real2 ya, real2 yb, int ca, int cb,
+                                        int lev, real2& A, real2& B) {
+  if constexpr (OP == SPEC_VEL) {
+    if (S.vmode == 0) {  // f = e - diffy(c), f(:,1,1) = ubar
+      const real2 ta = ld2(S.ky, ca), tb = ld2(S.ky, cb);
+      A = mk2(xa.x - (real(-1) * yb.x) * ta.x, xa.y - (real(-1) * yb.y) * ta.y);
+      B = mk2(xb.x - ya.x * tb.x, xb.y - ya.y * tb.y);
+      if (ca == 0) A.x = (real)S.zbar[lev];
+    } else if (S.vmode == 1) {  // f = diffx(c) - e, f(:,1,1) = vbar
+      const real2 ta = ld2(S.kx, ca), tb = ld2(S.kx, cb);
+      A = mk2((real(-1) * ya.y) * ta.x - xa.x, ya.x * ta.y - xa.y);
+      B = mk2((real(-1) * yb.y) * tb.x - xb.x, yb.x * tb.y - xb.y);
+      if (ca == 0) A.x = (real)S.zbar[lev];
+    } else {  // f = diffy(a) - diffx(b)
+      const real2 ya2 = ld2(S.ky, ca), yb2 = ld2(S.ky, cb), xa2 = ld2(S.kx, ca), xb2 = ld2(S.kx, cb);
+      A = mk2((real(-1) * xb.x) * ya2.x - (real(-1) * ya.y) * xa2.x, (real(-1) * xb.y) * ya2.y - ya.x * xa2.y);
+      B = mk2(xa.x * yb2.x - (real(-1) * yb.y) * xb2.x, xa.y * yb2.y - yb.x * xb2.y);
+    }
+  } else if constexpr (OP == SPEC_DX) {
+    const real2 ta = ld2(S.tab, ca), tb = ld2(S.tab, cb);
+    A = mk2((real(-1) * xa.y) * ta.x, xa.x * ta.y);
+    B = mk2((real(-1) * xb.y) * tb.x, xb.x * tb.y);
+  } else if constexpr (OP == SPEC_DY) {
+    const real2 ta = ld2(S.tab, ca), tb = ld2(S.tab, cb);
+    A = mk2((real(-1) * xb.x) * ta.x, (real(-1) * xb.y) * ta.y);
+    B = mk2(xa.x * tb.x, xa.y * tb.y);
+  } else if constexpr (OP == SPEC_FILT) {
+    const real2 ta = ld2(S.tab, ca), tb = ld2(S.tab, cb);
+    A = mk2(xa.x * ta.x, xa.y * ta.y);
+    B = mk2(xb.x * tb.x, xb.y * tb.y);
+  } else {
+    A = xa;
+    B = xb;
+  }
+}
+// the filtered copy of a velocity spectrum pair (SPEC_VEL), at elements ea, eb
+__device__ __forceinline__ void vel_store(const SpecIn<real>& S, size_t ea, size_t eb, int ca, int cb, real2 A,
+                                          real2 B) {
+  const real2 fa = ld2(S.filt, ca), fb = ld2(S.filt, cb);
+  st2(S.fs, ea, mk2(A.x * fa.x, A.y * fa.y));
+  st2(S.fs, eb, mk2(B.x * fb.x, B.y * fb.y));
+}
+// the operator's inputs of the element pair read from global memory
 template <int OP>
 __device__ __forceinline__ void spec_pair(const Geom& g, const real* __restrict__ spec, const SpecIn<real>& S,
                                           int64_t ra, int jp, int lev, int km, bool own, real2& A, real2& B) {
   const size_t ea = (size_t)ra * g.sx + 2 * km, eb = ea + g.sx;
   const int ca = jp * g.sx + 2 * km, cb = ca + g.sx;  // spectral columns of elements ea, eb
   if constexpr (OP == SPEC_VEL) {
-    real2 va, vb;  // elements (ea, ea + 1), (eb, eb + 1)
-    if (S.vmode == 0) {  // f = e - diffy(c), f(:,1,1) = ubar
-      const real2 ea2 = ld2(S.e, ea), eb2 = ld2(S.e, eb), ca2 = ld2(S.c, ea), cb2 = ld2(S.c, eb);
-      const real2 ta = ld2(S.ky, ca), tb = ld2(S.ky, cb);
-      va = mk2(ea2.x - (real(-1) * cb2.x) * ta.x, ea2.y - (real(-1) * cb2.y) * ta.y);
-      vb = mk2(eb2.x - ca2.x * tb.x, eb2.y - ca2.y * tb.y);
-      if (ca == 0) va.x = (real)S.zbar[lev];
-    } else if (S.vmode == 1) {  // f = diffx(c) - e, f(:,1,1) = vbar
-      const real2 ea2 = ld2(S.e, ea), eb2 = ld2(S.e, eb), ca2 = ld2(S.c, ea), cb2 = ld2(S.c, eb);
-      const real2 ta = ld2(S.kx, ca), tb = ld2(S.kx, cb);
-      va = mk2((real(-1) * ca2.y) * ta.x - ea2.x, ca2.x * ta.y - ea2.y);
-      vb = mk2((real(-1) * cb2.y) * tb.x - eb2.x, cb2.x * tb.y - eb2.y);
-      if (ca == 0) va.x = (real)S.zbar[lev];
-    } else {  // f = diffy(a) - diffx(b)
-      const real2 aa = ld2(S.a, ea), ab = ld2(S.a, eb), ba = ld2(S.b, ea), bb = ld2(S.b, eb);
-      const real2 ya = ld2(S.ky, ca), yb = ld2(S.ky, cb), xa = ld2(S.kx, ca), xb = ld2(S.kx, cb);
-      va = mk2((real(-1) * ab.x) * ya.x - (real(-1) * ba.y) * xa.x, (real(-1) * ab.y) * ya.y - ba.x * xa.y);
-      vb = mk2(aa.x * yb.x - (real(-1) * bb.y) * xb.x, aa.y * yb.y - bb.x * xb.y);
-    }
-    if (own) {
-      const real2 fa = ld2(S.filt, ca), fb = ld2(S.filt, cb);
-      st2(S.fs, ea, mk2(va.x * fa.x, va.y * fa.y));
-      st2(S.fs, eb, mk2(vb.x * fb.x, vb.y * fb.y));
-    }
-    A = va;
-    B = vb;
+    const real* x = S.vmode == 2 ? S.a : S.e;
+    const real* y = S.vmode == 2 ? S.b : S.c;
+    spec_op<OP>(S, ld2(x, ea), ld2(x, eb), ld2(y, ea), ld2(y, eb), ca, cb, lev, A, B);
+    if (own) vel_store(S, ea, eb, ca, cb, A, B);
   } else {
     const real2 a = ld2(spec, ea), b = ld2(spec, eb);
-    if constexpr (OP == SPEC_DX) {
-      const real2 ta = ld2(S.tab, ca), tb = ld2(S.tab, cb);
-      A = mk2((real(-1) * a.y) * ta.x, a.x * ta.y);
-      B = mk2((real(-1) * b.y) * tb.x, b.x * tb.y);
-    } else if constexpr (OP == SPEC_DY) {
-      const real2 ta = ld2(S.tab, ca), tb = ld2(S.tab, cb);
-      A = mk2((real(-1) * b.x) * ta.x, (real(-1) * b.y) * ta.y);
-      B = mk2(a.x * tb.x, a.y * tb.y);
-    } else if constexpr (OP == SPEC_FILT) {
-      const real2 ta = ld2(S.tab, ca), tb = ld2(S.tab, cb);
-      A = mk2(a.x * ta.x, a.y * ta.y);
-      B = mk2(b.x * tb.x, b.y * tb.y);
-    } else {
-      A = a;
-      B = b;
-    }
+    spec_op<OP>(S, a, b, a, b, ca, cb, lev, A, B);
   }
 }
 // the same with the operator chosen at run time (generic-length path)
@@ -519,45 +529,103 @@ __global__ void __launch_bounds__(FS_THREADS) k4_fwd_x(Geom g, int64_t nrows_tot
   }
 }
 
-// inverse x pass (spec -> mid)
+// inverse x pass (spec -> mid).  A CTA's 2 RP rows are contiguous in both
+// arrays: they are staged into shared memory with 16-byte loads, the input
+// operator runs over the staged block (coalesced table reads and filtered
+// velocity stores), the transform reads its modes from shared memory (no
+// mirrored global reads), and the result leaves with 16-byte stores.
+template <int N1, int N2, int OP>
+struct InvX {
+  static constexpr int N = N1 * N2, RP = FS_THREADS / (N1 > N2 ? N1 : N2), NR = 2 * RP, SX = N + 2;
+  static constexpr int YS = N1 * (N2 + 1);
+  static constexpr size_t IN = (size_t)(OP == SPEC_VEL ? 2 : 1) * NR * SX * sizeof(real);
+  static constexpr size_t YB = (size_t)RP * YS * sizeof(real2);
+  static constexpr size_t XB = (size_t)NR * N * sizeof(real);
+  static constexpr size_t SMEM = IN > YB ? (IN > XB ? IN : XB) : (YB > XB ? YB : XB);
+};
 template <int N1, int N2, int OP>
 __global__ void __launch_bounds__(FS_THREADS) k4_inv_x(Geom g, int64_t nrows_total, const real2* __restrict__ tw4,
                                                        const real* __restrict__ spec, real* __restrict__ mid,
                                                        SpecIn<real> S) {
-  constexpr int N = N1 * N2, RP = FS_THREADS / (N1 > N2 ? N1 : N2), YS = N1 * (N2 + 1);
-  __shared__ real2 Y[RP * YS];
+  using L = InvX<N1, N2, OP>;
+  constexpr int N = L::N, RP = L::RP, NR = L::NR, SX = L::SX, YS = L::YS;
+  extern __shared__ __align__(16) unsigned char fsm[];
+  real* B0 = (real*)fsm;     // staged rows (the operator's result in place)
+  real* B1 = B0 + NR * SX;   // SPEC_VEL: the second input
+  real2* Y = (real2*)fsm;    // step 1 -> step 3, over the staged rows
+  real* X = (real*)fsm;      // the result rows, over Y
   const int t = threadIdx.x;
-  const int64_t row0 = (int64_t)blockIdx.x * RP * 2;
-  if (t < RP * N2) {
-    const int r = t / N2, n2 = t % N2;
-    const int64_t ra = row0 + 2 * r;
-    const bool valid = ra < nrows_total;  // then so is ra + 1: the row count is even
-    const int lev = (int)(ra / g.sy), jp = (int)(ra - (int64_t)lev * g.sy);
-    real2 a[N1];
+  const int64_t row0 = (int64_t)blockIdx.x * NR;
+  const int nr = (int)min((int64_t)NR, nrows_total - row0);  // even: the row count is even
+  {
+    const real* in0 = OP == SPEC_VEL ? (S.vmode == 2 ? S.a : S.e) : spec;
+    const int nv = nr * SX * (int)sizeof(real) / 16;
+    const vec16* s0 = (const vec16*)(in0 + row0 * SX);
+    for (int v = t; v < nv; v += FS_THREADS) ((vec16*)B0)[v] = s0[v];
+    if constexpr (OP == SPEC_VEL) {
+      const vec16* s1 = (const vec16*)((S.vmode == 2 ? S.b : S.c) + row0 * SX);
+      for (int v = t; v < nv; v += FS_THREADS) ((vec16*)B1)[v] = s1[v];
+    }
+  }
+  __syncthreads();
+  if constexpr (OP != SPEC_PLAIN) {
+    constexpr int HM = SX / 2;  // complex elements per row
+    for (int q = t; q < (nr / 2) * HM; q += FS_THREADS) {
+      const int pr = q / HM, m = q - pr * HM;
+      const int64_t ra = row0 + 2 * pr;
+      const int lev = (int)(ra / g.sy), jp = (int)(ra - (int64_t)lev * g.sy);
+      const int ea = 2 * pr * SX + 2 * m, eb = ea + SX;
+      const int ca = jp * SX + 2 * m, cb = ca + SX;
+      const real2 xa = ld2(B0, ea), xb = ld2(B0, eb);
+      real2 A, B;
+      if constexpr (OP == SPEC_VEL) {
+        spec_op<OP>(S, xa, xb, ld2(B1, ea), ld2(B1, eb), ca, cb, lev, A, B);
+        vel_store(S, (size_t)row0 * SX + ea, (size_t)row0 * SX + eb, ca, cb, A, B);
+      } else {
+        spec_op<OP>(S, xa, xb, xa, xb, ca, cb, lev, A, B);
+      }
+      st2(B0, ea, A);
+      st2(B0, eb, B);
+    }
+    __syncthreads();
+  }
+  const bool act1 = t < RP * N2;
+  const int r1 = t / N2, n2 = t % N2;
+  real2 a[N1];
+  if (act1) {
 #pragma unroll
     for (int n1 = 0; n1 < N1; ++n1) {
       const int k = n2 + N2 * n1;
       const int km = (2 * k <= N) ? k : N - k;
       real2 A = mk2(real(0), real(0)), B = mk2(real(0), real(0));
-      if (valid) spec_pair<OP>(g, spec, S, ra, jp, lev, km, 2 * k <= N, A, B);
+      if (2 * r1 < nr) {
+        A = ld2(B0, (2 * r1) * SX + 2 * km);
+        B = ld2(B0, (2 * r1 + 1) * SX + 2 * km);
+      }
       a[n1] = c2r_pack(A, B, k, N);
     }
-    fs_step1<N1, N2>(a, n2, Y + r * YS, tw4);
   }
+  __syncthreads();  // Y overwrites the staged rows
+  if (act1) fs_step1<N1, N2>(a, n2, Y + r1 * YS, tw4);
   __syncthreads();
   const real dn = real(1) / (real)N;
-  if (t < RP * N1) {
-    const int r = t / N1, k1 = t % N1;
-    real2 a[N2];
-    fs_step3<N1, N2>(a, k1, Y + r * YS);
-    const int64_t ra = row0 + 2 * r, rb = ra + 1;
+  const bool act3 = t < RP * N1;
+  const int r3 = t / N1, k1 = t % N1;
+  real2 b[N2];
+  if (act3) fs_step3<N1, N2>(b, k1, Y + r3 * YS);
+  __syncthreads();  // X overwrites Y
+  if (act3) {
 #pragma unroll
     for (int k2 = 0; k2 < N2; ++k2) {
       const int i = k1 + N1 * k2;  // conj(z) * dn: real part -> row A, imaginary part -> row B
-      if (ra < nrows_total) mid[(size_t)ra * N + i] = a[k2].x * dn;
-      if (rb < nrows_total) mid[(size_t)rb * N + i] = -a[k2].y * dn;
+      X[(2 * r3) * N + i] = b[k2].x * dn;
+      X[(2 * r3 + 1) * N + i] = -b[k2].y * dn;
     }
   }
+  __syncthreads();
+  const int nv = nr * N * (int)sizeof(real) / 16;
+  vec16* dst = (vec16*)(mid + row0 * N);
+  for (int v = t; v < nv; v += FS_THREADS) dst[v] = ((const vec16*)X)[v];
 }
 
 // forward y pass (phys -> mid): one z level, 16 consecutive x columns
@@ -671,7 +739,7 @@ bool fs_fwd_x(int n1, int n2, unsigned nb, cudaStream_t st, const Geom& g, int64
 template <int OP>
 bool fs_inv_x_op(int n1, int n2, unsigned nb, cudaStream_t st, const Geom& g, int64_t nrows, const real2* tw4,
                  const real* spec, real* mid, const SpecIn<real>& S) {
-#define CALL(A, B) k4_inv_x<A, B, OP><<<nb, FS_THREADS, 0, st>>>(g, nrows, tw4, spec, mid, S)
+#define CALL(A, B) k4_inv_x<A, B, OP><<<nb, FS_THREADS, InvX<A, B, OP>::SMEM, st>>>(g, nrows, tw4, spec, mid, S)
   PMPIC_FS_CASES(CALL)
 #undef CALL
 }
@@ -778,7 +846,19 @@ int fft_backward_impl(pmpic_ctx* ctx, const real* spec, real* phys, real* mid, c
 // shared-memory limits of the Stockham kernels (a property of each function on
 // the current device)
 cudaError_t fft_attributes() {
-  cudaError_t e = cudaFuncSetAttribute(k_fwd_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaError_t e = cudaSuccess;
+  // the four-step inverse x pass stages its rows dynamically (SPEC_VEL on FP64: above 48 KB)
+#define PMPIC_INVX_ATTR(A, B)                                                                           \
+  if (e == cudaSuccess)                                                                                 \
+    e = cudaFuncSetAttribute(k4_inv_x<A, B, SPEC_VEL>, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
+                             (int)InvX<A, B, SPEC_VEL>::SMEM);
+  PMPIC_INVX_ATTR(4, 4)
+  PMPIC_INVX_ATTR(8, 4)
+  PMPIC_INVX_ATTR(8, 8)
+  PMPIC_INVX_ATTR(16, 8)
+  PMPIC_INVX_ATTR(16, 16)
+#undef PMPIC_INVX_ATTR
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fwd_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fwd_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);

@@ -36,14 +36,6 @@ constexpr int MAXSEG = 32;            // cell segments sorted in registers
 inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
 // ---- binning (cache_parcel_interp_weights, parcel_interpolation.F90:186-262) ----
-// one integer atomic per distinct cell of the warp (neighbouring slots mostly
-// share a cell)
-__device__ __forceinline__ void count_cell(int32_t id, int32_t* __restrict__ count) {
-  const unsigned act = __activemask();
-  const unsigned same = __match_any_sync(act, id);
-  if ((threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&count[id], __popc(same));
-}
-
 __global__ void k_bin_count(Geom g, int64_t n, const double* __restrict__ X, const double* __restrict__ Y,
                             const double* __restrict__ Z, int32_t* __restrict__ cell, double* __restrict__ del,
                             int64_t cap, int32_t* __restrict__ count, DevInfo* info) {
@@ -319,32 +311,54 @@ __global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, 
   R* S = smem[warp];
   R* out_row = rowpart + ((size_t)zc * g.Ny + cy) * (size_t)g.Nx * Lay::RPS;
   R C[2][NA];  // x-high corners of the previous column, per y corner
-  // the column before the segment (periodic) only seeds the carry
-  for (int it = -1; it < x_hi - x_lo; ++it) {
+  // Column it's bounds (this lane's cell layer) and its first batch of slots
+  // are loaded one column ahead, so a column waits on one memory latency (its
+  // staged fields), not three (bounds, slots, fields).
+  auto bounds = [&](int it, int& s, int& e) {
     int cx = x_lo + it;
     if (cx < 0) cx += g.Nx;
     const int64_t cb = ((int64_t)cx * g.Ny + cy) * g.Nz + k0;
-    int s_me = 0, e_me = 0;
+    s = e = 0;
     if (has_cell) {
-      s_me = start[cb + kk];
-      e_me = start[cb + kk + 1];
+      s = start[cb + kk];
+      e = start[cb + kk + 1];
     }
-    const int q0 = __shfl_sync(FULL, s_me, 0);
-    const int q1 = __shfl_sync(FULL, e_me, 2 * nk - 2);
+  };
+  auto slots = [&](int b0, int nb, int* sl) {
+#pragma unroll
+    for (int j = 0; j < BATCH / 32; ++j) {
+      const int p = lane + 32 * j;
+      sl[j] = p < nb ? sorted[b0 + p] : -1;
+    }
+  };
+  int s_me, e_me;
+  bounds(-1, s_me, e_me);
+  int q0 = __shfl_sync(FULL, s_me, 0);
+  int q1 = __shfl_sync(FULL, e_me, 2 * nk - 2);
+  int pre[BATCH / 32];
+  slots(q0, min(BATCH, q1 - q0), pre);
+  // the column before the segment (periodic) only seeds the carry
+  for (int it = -1; it < x_hi - x_lo; ++it) {
+    const int cx = x_lo + it;  // >= 0 where the row partials are written (it >= 0)
+    const bool more = it + 1 < x_hi - x_lo;
+    int s_nx = 0, e_nx = 0, q0n = 0, q1n = 0;
+    if (more) bounds(it + 1, s_nx, e_nx);
     R acc[4][NA];  // [y corner * 2 + x corner][quantity] of this lane's z corner
 #pragma unroll
     for (int ab = 0; ab < 4; ++ab)
 #pragma unroll
       for (int q = 0; q < NA; ++q) acc[ab][q] = R(0);
     int nkept = 0;
+    bool prefetched = false;
     for (int b0 = q0; b0 < q1; b0 += BATCH) {
       const int nb = min(BATCH, q1 - b0);
       __syncwarp();  // the previous batch has been read
       int slot[BATCH / 32];
+      if (b0 == q0) {
 #pragma unroll
-      for (int j = 0; j < BATCH / 32; ++j) {
-        const int p = lane + 32 * j;
-        slot[j] = p < nb ? sorted[b0 + p] : -1;
+        for (int j = 0; j < BATCH / 32; ++j) slot[j] = pre[j];
+      } else {
+        slots(b0, nb, slot);
       }
 #pragma unroll
       for (int j = 0; j < BATCH / 32; ++j) {
@@ -368,6 +382,12 @@ __global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, 
 #pragma unroll
           for (int f = 1; f < NQ; ++f) cp_async_r(D + (4 + f - 1) * SPAD, a.f[f] + n);
         }
+      }
+      if (more && b0 + BATCH >= q1) {  // the column's last batch: the next column's first slots
+        q0n = __shfl_sync(FULL, s_nx, 0);
+        q1n = __shfl_sync(FULL, e_nx, 2 * nk - 2);
+        slots(q0n, min(BATCH, q1n - q0n), pre);
+        prefetched = true;
       }
       cp_async_wait_all();
       __syncwarp();
@@ -420,6 +440,11 @@ __global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, 
         }
       }
     }
+    if (more && !prefetched) {  // an empty column
+      q0n = __shfl_sync(FULL, s_nx, 0);
+      q1n = __shfl_sync(FULL, e_nx, 2 * nk - 2);
+      slots(q0n, min(BATCH, q1n - q0n), pre);
+    }
     // level m+1 = top corners of layer m (odd lane 2m+1) + bottom corners of layer m+1 (lane 2m+2)
 #pragma unroll
     for (int ab = 0; ab < 4; ++ab)
@@ -443,6 +468,10 @@ __global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, 
     for (int b = 0; b < 2; ++b)
 #pragma unroll
       for (int q = 0; q < NA; ++q) C[b][q] = acc[2 * b + 1][q];
+    s_me = s_nx;
+    e_me = e_nx;
+    q0 = q0n;
+    q1 = q1n;
   }
 }
 
@@ -585,17 +614,23 @@ int bin_and_sort(pmpic_ctx* ctx) {
   TimerScope ts(ctx, T_CACHE);
   const Geom& g = ctx->g;
   const int64_t n = ctx->n;
-  PMPIC_CUDA(cudaMemsetAsync(ctx->cell_count, 0, sizeof(int32_t) * (g.ncell + 1), ctx->stream));
   PMPIC_CUDA(cudaMemsetAsync(ctx->cell_fill, 0, sizeof(int32_t) * g.ncell, ctx->stream));
-  if (n > 0 && ctx->mixed) {
-    k_bin_count_m<<<nblk(n, 256), 256, 0, ctx->stream>>>(g, n, propc(ctx, PMPIC_PROP_X), propc(ctx, PMPIC_PROP_Y),
-                                                         propc(ctx, PMPIC_PROP_Z), ctx->cell, ctx->cell_count,
-                                                         ctx->dinfo); ++ctx->nlaunch;
-  } else if (n > 0) {
-    k_bin_count<<<nblk(n, 256), 256, 0, ctx->stream>>>(g, n, prop(ctx, PMPIC_PROP_X), prop(ctx, PMPIC_PROP_Y),
-                                                       prop(ctx, PMPIC_PROP_Z), ctx->cell, ctx->del, ctx->cap,
-                                                       ctx->cell_count, ctx->dinfo); ++ctx->nlaunch;
+  // on the mixed form, after an RK4 stage and its haloswap, the cell ids and
+  // counts are written already (by the stage kernel and the haloswap's mover
+  // binning)
+  if (!ctx->count_ready) {
+    PMPIC_CUDA(cudaMemsetAsync(ctx->cell_count, 0, sizeof(int32_t) * (g.ncell + 1), ctx->stream));
+    if (n > 0 && ctx->mixed) {
+      k_bin_count_m<<<nblk(n, 256), 256, 0, ctx->stream>>>(g, n, propc(ctx, PMPIC_PROP_X), propc(ctx, PMPIC_PROP_Y),
+                                                           propc(ctx, PMPIC_PROP_Z), ctx->cell, ctx->cell_count,
+                                                           ctx->dinfo); ++ctx->nlaunch;
+    } else if (n > 0) {
+      k_bin_count<<<nblk(n, 256), 256, 0, ctx->stream>>>(g, n, prop(ctx, PMPIC_PROP_X), prop(ctx, PMPIC_PROP_Y),
+                                                         prop(ctx, PMPIC_PROP_Z), ctx->cell, ctx->del, ctx->cap,
+                                                         ctx->cell_count, ctx->dinfo); ++ctx->nlaunch;
+    }
   }
+  ctx->count_ready = false;
   int rc = scan_excl(ctx, ctx->cell_count, g.ncell, ctx->cell_start);
   if (rc) return rc;
   if (n > 0) {

@@ -613,42 +613,40 @@ __global__ void k_residual_update(Geom g, ResPtrs RP, const int32_t* __restrict_
 // volume grid and the six residual grids are read packed (k_pack, 8 fields per
 // level: vol, vres, bres, hres, pres, qres, rres, pad), the corners visited in
 // the reference's order u = 0..7 (x fastest, then y, then z).
-__global__ void __launch_bounds__(256) k_redistribute(Geom g, int64_t norig, const int32_t* __restrict__ keep,
+__global__ void __launch_bounds__(256, 3) k_redistribute(Geom g, int64_t norig, const int32_t* __restrict__ keep,
                                                          double* __restrict__ parcels, int64_t cap,
                                                          const int32_t* __restrict__ cell,
                                                          const double* __restrict__ del,
                                                          const double* __restrict__ G8) {
   int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= norig || keep[m] != 1) return;
+  if (m >= norig) return;
   auto A = [&](int pid) -> double* { return parcels + (size_t)pid * cap; };
-  const int32_t id = cell[m];
-  if (id < 0) return;
-  const double delx = del[m], dely = del[cap + m], delz = del[2 * cap + m];
-  const int ck = id % g.Nz, cj = (id / g.Nz) % g.Ny, ci = id / (g.Nz * g.Ny);
-  const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
-  const double v = A(PMPIC_PROP_VOL)[m];
-  double w[8];
-  w[0] = (1 - delz) * (1 - dely) * (1 - delx) * v;
-  w[1] = (1 - delz) * (1 - dely) * (delx) * v;
-  w[2] = (1 - delz) * (dely) * (1 - delx) * v;
-  w[3] = (1 - delz) * (dely) * (delx) * v;
-  w[4] = (delz) * (1 - dely) * (1 - delx) * v;
-  w[5] = (delz) * (1 - dely) * (delx) * v;
-  w[6] = (delz) * (dely) * (1 - delx) * v;
-  w[7] = (delz) * (dely) * (delx) * v;
   const int pids[5] = {PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
+  // the state is read before the keep flag is known: one memory round trip
+  // less per parcel (removed parcels are few)
+  const int kp = keep[m];
+  const int32_t id = cell[m];
+  const double delx = del[m], dely = del[cap + m], delz = del[2 * cap + m];
+  const double v = A(PMPIC_PROP_VOL)[m];
   double s[5];
 #pragma unroll
-  for (int q = 0; q < 5; ++q) s[q] = A(pids[q])[m] * v;
+  for (int q = 0; q < 5; ++q) s[q] = A(pids[q])[m];
+  if (kp != 1 || id < 0) return;
+  const int ck = id % g.Nz, cj = (id / g.Nz) % g.Ny, ci = id / (g.Nz * g.Ny);
+  const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) s[q] = s[q] * v;
   double nv = v;
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int x = (u & 1) ? ci1 : ci, y = (u & 2) ? cj1 : cj, z = ck + (u >> 2);
     const double2* P = (const double2*)(G8 + (((size_t)x * g.Ny + y) * g.nzp + z) * 8);
     const double2 a0 = P[0], a1 = P[1], a2 = P[2], a3 = P[3];  // (vol, vres) (b, h) (p, q) (r, pad)
-    const double wv = w[u] / a0.x;  // the w/vol_g factor shared by b, h, p, q, r (:280-335)
-    nv = nv + w[u] * a0.y / a0.x;   // :268-276
-    s[0] = s[0] + wv * a1.x;        // :279-336
+    // weight of corner u (:258-265, evaluated left to right as there)
+    const double w = ((u & 4) ? delz : 1 - delz) * ((u & 2) ? dely : 1 - dely) * ((u & 1) ? delx : 1 - delx) * v;
+    const double wv = w / a0.x;  // the w/vol_g factor shared by b, h, p, q, r (:280-335)
+    nv = nv + w * a0.y / a0.x;   // :268-276
+    s[0] = s[0] + wv * a1.x;     // :279-336
     s[1] = s[1] + wv * a1.y;
     s[2] = s[2] + wv * a2.x;
     s[3] = s[3] + wv * a2.y;
@@ -727,7 +725,8 @@ __device__ __forceinline__ int classify_dir_m(const Geom& g, int i, int j) {
 // cell units (velocity * dt / cell size), renormalised into [0, 1).
 template <bool GU, bool GP>
 __global__ void __launch_bounds__(256, 5) k_rk4_m(Geom g, int64_t n, MPtrs P, int stage, const double* __restrict__ dtp,
-                        int8_t* __restrict__ dir) {
+                        int8_t* __restrict__ dir, int32_t* __restrict__ cell, int32_t* __restrict__ count,
+                        DevInfo* info) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const float dt = (float)*dtp;  // state%dtm (rk4_integrator.F90:102)
@@ -812,7 +811,21 @@ __global__ void __launch_bounds__(256, 5) k_rk4_m(Geom g, int64_t n, MPtrs P, in
     P.s[v][t] = sn[v];
     P.sv[v][t] = svn[v];
   }
-  dir[t] = (int8_t)classify_dir_m(g, sn[0].i, sn[1].i);
+  const int dr = classify_dir_m(g, sn[0].i, sn[1].i);
+  dir[t] = (int8_t)dr;
+  // the next binning of the new position, with the per-cell count (parcels
+  // crossing a periodic boundary are binned by the haloswap once shifted)
+  int32_t nid = -1;
+  if (dr == 0) {
+    if (sn[2].i >= 0 && sn[2].i < g.Nz && sn[0].f >= 0.f && sn[0].f <= 1.f && sn[1].f >= 0.f && sn[1].f <= 1.f &&
+        sn[2].f >= 0.f && sn[2].f <= 1.f) {
+      nid = (int32_t)(((int64_t)sn[0].i * g.Ny + sn[1].i) * g.Nz + sn[2].i);
+      count_cell(nid, count);
+    } else {
+      atomicCAS(&info->error, 0, PMPIC_ERR_OUT_OF_BOX);
+    }
+  }
+  cell[t] = nid;
 }
 
 __global__ void k_reflect_classify_m(Geom g, int64_t n, const CellOff* __restrict__ X, const CellOff* __restrict__ Y,
@@ -865,6 +878,28 @@ __global__ void k_swap_scatter_m(const int32_t* __restrict__ nmov, const int32_t
     double* A = parcels + (size_t)pid * cap;
     if (mixed_elem_bytes(pid) == 4) ((float*)A)[V[t]] = (float)buf[e];
     else A[V[t]] = buf[e];
+  }
+}
+
+// binning and count of the parcels a haloswap moved, in their new slots V[t]
+// (the mixed RK4 stage kernel binned the others)
+__global__ void k_swap_bin_m(Geom g, const int32_t* __restrict__ nmov, const int32_t* __restrict__ V,
+                             const CellOff* __restrict__ X, const CellOff* __restrict__ Y,
+                             const CellOff* __restrict__ Z, int32_t* __restrict__ cell, int32_t* __restrict__ count,
+                             DevInfo* info) {
+  const int nm = *nmov;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nm; t += gridDim.x * blockDim.x) {
+    const int s = V[t];
+    const CellOff x = X[s], y = Y[s], z = Z[s];
+    int32_t id = -1;
+    if (x.i >= 0 && x.i < g.Nx && y.i >= 0 && y.i < g.Ny && z.i >= 0 && z.i < g.Nz && x.f >= 0.f && x.f <= 1.f &&
+        y.f >= 0.f && y.f <= 1.f && z.f >= 0.f && z.f <= 1.f) {
+      id = (int32_t)(((int64_t)x.i * g.Ny + y.i) * g.Nz + z.i);
+      atomicAdd(&count[id], 1);
+    } else {
+      atomicCAS(&info->error, 0, PMPIC_ERR_OUT_OF_BOX);
+    }
+    cell[s] = id;
   }
 }
 
@@ -1025,35 +1060,32 @@ __global__ void __launch_bounds__(256, 4) k_redistribute_m(Geom g, int64_t norig
                                                           double* __restrict__ parcels, int64_t cap,
                                                           const float* __restrict__ G8) {
   const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= norig || keep[m] != 1) return;
+  if (m >= norig) return;
   auto F = [&](int pid) { return (float*)(parcels + (size_t)pid * cap); };
   auto C = [&](int pid) { return (CellOff*)(parcels + (size_t)pid * cap); };
+  const int pids[5] = {PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
+  // the state is read before the keep flag is known (one round trip less)
+  const int kp = keep[m];
   const CellOff px = C(PMPIC_PROP_X)[m], py = C(PMPIC_PROP_Y)[m], pz = C(PMPIC_PROP_Z)[m];
+  const float v = F(PMPIC_PROP_VOL)[m];
+  float s[5];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) s[q] = F(pids[q])[m];
   const int ci = px.i, cj = py.i, ck = pz.i;
+  if (kp != 1) return;
   if (ci < 0 || ci >= g.Nx || cj < 0 || cj >= g.Ny || ck < 0 || ck >= g.Nz) return;  // reported by the binning
   const float delx = px.f, dely = py.f, delz = pz.f;
   const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
-  const float v = F(PMPIC_PROP_VOL)[m];
-  float w[8];
-  w[0] = (1.f - delz) * (1.f - dely) * (1.f - delx) * v;
-  w[1] = (1.f - delz) * (1.f - dely) * (delx) * v;
-  w[2] = (1.f - delz) * (dely) * (1.f - delx) * v;
-  w[3] = (1.f - delz) * (dely) * (delx) * v;
-  w[4] = (delz) * (1.f - dely) * (1.f - delx) * v;
-  w[5] = (delz) * (1.f - dely) * (delx) * v;
-  w[6] = (delz) * (dely) * (1.f - delx) * v;
-  w[7] = (delz) * (dely) * (delx) * v;
-  const int pids[5] = {PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
-  float s[5];
 #pragma unroll
-  for (int q = 0; q < 5; ++q) s[q] = F(pids[q])[m] * v;
+  for (int q = 0; q < 5; ++q) s[q] = s[q] * v;
   float nv = v;
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int x = (u & 1) ? ci1 : ci, y = (u & 2) ? cj1 : cj, z = ck + (u >> 2);
     const float4* P = (const float4*)(G8 + (((size_t)x * g.Ny + y) * g.nzp + z) * 8);
     const float4 a0 = P[0], a1 = P[1];  // (vol, vres, b, h) (p, q, r, pad)
-    const float wv = w[u] / a0.x;
+    const float w = ((u & 4) ? delz : 1.f - delz) * ((u & 2) ? dely : 1.f - dely) * ((u & 1) ? delx : 1.f - delx) * v;
+    const float wv = w / a0.x;
     nv = nv + wv * a0.y;  // :268-276
     s[0] = s[0] + wv * a0.z;
     s[1] = s[1] + wv * a0.w;
@@ -1207,10 +1239,13 @@ int rk4_stage(pmpic_ctx* ctx, int stage) {
     P.g6 = (const float*)ctx->gpack;
     if (gu && gp) pack6<float>(ctx, P.grid, (float*)ctx->gpack);
     auto kern = gu ? (gp ? k_rk4_m<true, true> : k_rk4_m<true, false>) : (gp ? k_rk4_m<false, true> : k_rk4_m<false, false>);
-    kern<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, P, stage, &ctx->dinfo->dtm, ctx->dir); ++ctx->nlaunch;
+    PMPIC_CUDA(cudaMemsetAsync(ctx->cell_count, 0, sizeof(int32_t) * (ctx->g.ncell + 1), ctx->stream));
+    kern<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, P, stage, &ctx->dinfo->dtm, ctx->dir, ctx->cell,
+                                                     ctx->cell_count, ctx->dinfo); ++ctx->nlaunch;
     ctx->pending_uvw = ctx->pending_pqr = false;
     ctx->dir_ready = true;
     ctx->sorted_valid = false;
+    ctx->count_ready = true;
     ctx->btot_grid_ready = false;
     PMPIC_CUDA(cudaGetLastError());
     return 0;
@@ -1233,11 +1268,15 @@ int rk4_stage(pmpic_ctx* ctx, int stage) {
   P.g6 = ctx->gpack;
   if (gu && gp) pack6<double>(ctx, P.grid, ctx->gpack);
   auto kern = gu ? (gp ? k_rk4<true, true> : k_rk4<true, false>) : (gp ? k_rk4<false, true> : k_rk4<false, false>);
+  // the next binning stays a separate pass on this path: its six IEEE
+  // divisions per parcel cost the HBM-bound stage kernel more than the
+  // position reads they would save
   kern<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, P, stage, &ctx->dinfo->dtm, ctx->cell, ctx->del,
                                                    ctx->cap, ctx->dir); ++ctx->nlaunch;
   ctx->pending_uvw = ctx->pending_pqr = false;
   ctx->dir_ready = true;  // z reflected and directions classified
   ctx->sorted_valid = false;
+  ctx->count_ready = false;
   ctx->btot_grid_ready = false;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
@@ -1254,6 +1293,10 @@ int parcel_haloswap(pmpic_ctx* ctx) {
   ctx->btot_grid_ready = false;
   const bool ready = ctx->dir_ready;
   ctx->dir_ready = false;
+  // after an RK4 stage the parcels that stay are binned and counted already;
+  // the movers are binned below in their new slots
+  const bool counted = ready && ctx->count_ready;
+  ctx->count_ready = counted;
   if (n == 0) return 0;
   if (!ready && ctx->mixed) {
     k_reflect_classify_m<<<nblk(n, 256), 256, 0, ctx->stream>>>(ctx->g, n, propc(ctx, PMPIC_PROP_X),
@@ -1277,6 +1320,10 @@ int parcel_haloswap(pmpic_ctx* ctx) {
   if (ctx->mixed) {
     k_swap_gather_m<<<592, 256, 0, ctx->stream>>>(ctx->g, nmc, M, ctx->dir, ctx->parcels, ctx->cap, ctx->swapbuf); ++ctx->nlaunch;
     k_swap_scatter_m<<<592, 256, 0, ctx->stream>>>(nmc, V, ctx->swapbuf, ctx->parcels, ctx->cap); ++ctx->nlaunch;
+    if (counted) {
+      k_swap_bin_m<<<148, 256, 0, ctx->stream>>>(ctx->g, nmc, V, propc(ctx, PMPIC_PROP_X), propc(ctx, PMPIC_PROP_Y),
+                                                 propc(ctx, PMPIC_PROP_Z), ctx->cell, ctx->cell_count, ctx->dinfo); ++ctx->nlaunch;
+    }
   } else {
     k_swap_gather<<<592, 256, 0, ctx->stream>>>(ctx->g, nmc, M, ctx->dir, ctx->parcels, ctx->cap, ctx->swapbuf); ++ctx->nlaunch;
     k_swap_scatter<<<592, 256, 0, ctx->stream>>>(nmc, V, ctx->swapbuf, ctx->parcels, ctx->cap); ++ctx->nlaunch;
@@ -1312,6 +1359,7 @@ int splitting(pmpic_ctx* ctx) {
   PMPIC_CUDA(cudaMemcpyAsync(&hns, ns, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
   PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
   int64_t nn = n + hns;
+  ctx->count_ready = false;  // split parents moved and children were added uncounted
   if (nn > ctx->cap) return set_error(ctx, PMPIC_ERR_CAPACITY, "maxparcels reached (parcel splitting)");
   ctx->n = nn;
   ctx->info.n_split = hns;
@@ -1418,6 +1466,7 @@ int mixing(pmpic_ctx* ctx) {
   }
   ctx->n = count;
   ctx->sorted_valid = false;
+  ctx->count_ready = false;
   ctx->btot_grid_ready = false;
   ctx->info.n_removed = nremove;
   ctx->info.n_added = nadd;
