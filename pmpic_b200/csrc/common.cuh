@@ -273,7 +273,7 @@ inline CellOff* propc(pmpic_ctx* ctx, int p) { return (CellOff*)prop(ctx, p); }
 int bin_and_sort(pmpic_ctx* ctx);
 int par2grid_multi(pmpic_ctx* ctx, const double* const* fields, int nf, double* const* out, bool btot_from_bhz);
 int grid2par_multi(pmpic_ctx* ctx, const double* const* grids, int ng, double* const* out);
-int par2grid_multi_m(pmpic_ctx* ctx, const float* const* fields, int nf, float* const* out);
+int par2grid_multi_m(pmpic_ctx* ctx, const float* const* fields, int nf, float* const* out, bool btot_from_bhz = false);
 int grid2par_multi_m(pmpic_ctx* ctx, const float* const* grids, int ng, float* const* out);
 int cell_ids(pmpic_ctx* ctx, int32_t* dcells);
 size_t rowpart_bytes(const Geom& g);

@@ -639,15 +639,13 @@ static int do_vort2vel(pmpic_ctx* ctx) {
   // same weights and parcel state, so it runs in the same pass into a spare
   // grid that the vorticity_tendency callback adopts.
   if ((rc = bin_and_sort(ctx))) return rc;
+  // The pass computes the btot property (vorticity_tendency.F90:121-126) as it
+  // stages each parcel and stores it.
   if (ctx->mixed) {
-    // the mixed form computes the btot property first (vorticity_tendency.F90:121-126)
-    // and grids it in the same FP32 pass as p, q, r
-    if ((rc = compute_btot(ctx))) return rc;
-    const float* f[4] = {propf(ctx, PMPIC_PROP_P), propf(ctx, PMPIC_PROP_Q), propf(ctx, PMPIC_PROP_R),
-                         propf(ctx, PMPIC_PROP_BTOT)};
+    const float* f[4] = {propf(ctx, PMPIC_PROP_P), propf(ctx, PMPIC_PROP_Q), propf(ctx, PMPIC_PROP_R), nullptr};
     float* o[4] = {(float*)ctx->grid[PMPIC_GRID_P], (float*)ctx->grid[PMPIC_GRID_Q], (float*)ctx->grid[PMPIC_GRID_R],
                    (float*)ctx->gspare};
-    if ((rc = par2grid_multi_m(ctx, f, 4, o))) return rc;
+    if ((rc = par2grid_multi_m(ctx, f, 4, o, true))) return rc;
   } else {
     const double* f[4] = {prop(ctx, PMPIC_PROP_P), prop(ctx, PMPIC_PROP_Q), prop(ctx, PMPIC_PROP_R), nullptr};
     double* o[4] = {ctx->grid[PMPIC_GRID_P], ctx->grid[PMPIC_GRID_Q], ctx->grid[PMPIC_GRID_R], ctx->gspare};
@@ -675,8 +673,7 @@ static int do_vorticity_tendency(pmpic_ctx* ctx) {
   }
   // par2grid(btot) (:129): computed by vort2vel's pass when the state is unchanged
   if (ctx->btot_grid_ready && ctx->sorted_valid) {
-    // :121-126, the btot property (the mixed form wrote it in that pass)
-    if (!ctx->mixed && (rc = compute_btot(ctx))) return rc;
+    // :121-126, the btot property: written by that pass
     std::swap(ctx->grid[PMPIC_GRID_B], ctx->gspare);
   } else {
     if ((rc = compute_btot(ctx))) return rc;

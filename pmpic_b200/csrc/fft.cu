@@ -109,14 +109,12 @@ int pick_rp(int n) {  // complex rows per CTA for the x passes
 namespace f64 {
 using real = double;
 using real2 = double2;
-using vec16 = double2;  // 16-byte vector of reals
 __host__ __device__ __forceinline__ double2 mk2(double a, double b) { return make_double2(a, b); }
 #include "fft_impl.cuh"
 }  // namespace f64
 namespace f32 {
 using real = float;
 using real2 = float2;
-using vec16 = float4;
 __host__ __device__ __forceinline__ float2 mk2(float a, float b) { return make_float2(a, b); }
 #include "fft_impl.cuh"
 }  // namespace f32

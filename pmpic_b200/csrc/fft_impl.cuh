@@ -529,103 +529,48 @@ __global__ void __launch_bounds__(FS_THREADS) k4_fwd_x(Geom g, int64_t nrows_tot
   }
 }
 
-// inverse x pass (spec -> mid).  A CTA's 2 RP rows are contiguous in both
-// arrays: they are staged into shared memory with 16-byte loads, the input
-// operator runs over the staged block (coalesced table reads and filtered
-// velocity stores), the transform reads its modes from shared memory (no
-// mirrored global reads), and the result leaves with 16-byte stores.
-template <int N1, int N2, int OP>
-struct InvX {
-  static constexpr int N = N1 * N2, RP = FS_THREADS / (N1 > N2 ? N1 : N2), NR = 2 * RP, SX = N + 2;
-  static constexpr int YS = N1 * (N2 + 1);
-  static constexpr size_t IN = (size_t)(OP == SPEC_VEL ? 2 : 1) * NR * SX * sizeof(real);
-  static constexpr size_t YB = (size_t)RP * YS * sizeof(real2);
-  static constexpr size_t XB = (size_t)NR * N * sizeof(real);
-  static constexpr size_t SMEM = IN > YB ? (IN > XB ? IN : XB) : (YB > XB ? YB : XB);
-};
+// inverse x pass (spec -> mid).  The modes are read straight from HBM into
+// registers (the mirrored half from L1), the input operator applied on the
+// way.  Both transform passes are bound by L1 / shared-memory throughput, not
+// HBM, so no extra staging pass through shared memory is made.
 template <int N1, int N2, int OP>
 __global__ void __launch_bounds__(FS_THREADS) k4_inv_x(Geom g, int64_t nrows_total, const real2* __restrict__ tw4,
                                                        const real* __restrict__ spec, real* __restrict__ mid,
                                                        SpecIn<real> S) {
-  using L = InvX<N1, N2, OP>;
-  constexpr int N = L::N, RP = L::RP, NR = L::NR, SX = L::SX, YS = L::YS;
-  extern __shared__ __align__(16) unsigned char fsm[];
-  real* B0 = (real*)fsm;     // staged rows (the operator's result in place)
-  real* B1 = B0 + NR * SX;   // SPEC_VEL: the second input
-  real2* Y = (real2*)fsm;    // step 1 -> step 3, over the staged rows
-  real* X = (real*)fsm;      // the result rows, over Y
+  constexpr int N = N1 * N2, RP = FS_THREADS / (N1 > N2 ? N1 : N2), YS = N1 * (N2 + 1);
+  __shared__ real2 Y[RP * YS];
   const int t = threadIdx.x;
-  const int64_t row0 = (int64_t)blockIdx.x * NR;
-  const int nr = (int)min((int64_t)NR, nrows_total - row0);  // even: the row count is even
-  {
-    const real* in0 = OP == SPEC_VEL ? (S.vmode == 2 ? S.a : S.e) : spec;
-    const int nv = nr * SX * (int)sizeof(real) / 16;
-    const vec16* s0 = (const vec16*)(in0 + row0 * SX);
-    for (int v = t; v < nv; v += FS_THREADS) ((vec16*)B0)[v] = s0[v];
-    if constexpr (OP == SPEC_VEL) {
-      const vec16* s1 = (const vec16*)((S.vmode == 2 ? S.b : S.c) + row0 * SX);
-      for (int v = t; v < nv; v += FS_THREADS) ((vec16*)B1)[v] = s1[v];
-    }
-  }
-  __syncthreads();
-  if constexpr (OP != SPEC_PLAIN) {
-    constexpr int HM = SX / 2;  // complex elements per row
-    for (int q = t; q < (nr / 2) * HM; q += FS_THREADS) {
-      const int pr = q / HM, m = q - pr * HM;
-      const int64_t ra = row0 + 2 * pr;
-      const int lev = (int)(ra / g.sy), jp = (int)(ra - (int64_t)lev * g.sy);
-      const int ea = 2 * pr * SX + 2 * m, eb = ea + SX;
-      const int ca = jp * SX + 2 * m, cb = ca + SX;
-      const real2 xa = ld2(B0, ea), xb = ld2(B0, eb);
-      real2 A, B;
-      if constexpr (OP == SPEC_VEL) {
-        spec_op<OP>(S, xa, xb, ld2(B1, ea), ld2(B1, eb), ca, cb, lev, A, B);
-        vel_store(S, (size_t)row0 * SX + ea, (size_t)row0 * SX + eb, ca, cb, A, B);
-      } else {
-        spec_op<OP>(S, xa, xb, xa, xb, ca, cb, lev, A, B);
-      }
-      st2(B0, ea, A);
-      st2(B0, eb, B);
-    }
-    __syncthreads();
-  }
-  const bool act1 = t < RP * N2;
-  const int r1 = t / N2, n2 = t % N2;
-  real2 a[N1];
-  if (act1) {
+  const int64_t row0 = (int64_t)blockIdx.x * RP * 2;
+  if (t < RP * N2) {
+    const int r = t / N2, n2 = t % N2;
+    const int64_t ra = row0 + 2 * r;
+    const bool valid = ra < nrows_total;  // then so is ra + 1: the row count is even
+    const int lev = (int)(ra / g.sy), jp = (int)(ra - (int64_t)lev * g.sy);
+    real2 a[N1];
 #pragma unroll
     for (int n1 = 0; n1 < N1; ++n1) {
       const int k = n2 + N2 * n1;
       const int km = (2 * k <= N) ? k : N - k;
       real2 A = mk2(real(0), real(0)), B = mk2(real(0), real(0));
-      if (2 * r1 < nr) {
-        A = ld2(B0, (2 * r1) * SX + 2 * km);
-        B = ld2(B0, (2 * r1 + 1) * SX + 2 * km);
-      }
+      if (valid) spec_pair<OP>(g, spec, S, ra, jp, lev, km, 2 * k <= N, A, B);
       a[n1] = c2r_pack(A, B, k, N);
     }
+    fs_step1<N1, N2>(a, n2, Y + r * YS, tw4);
   }
-  __syncthreads();  // Y overwrites the staged rows
-  if (act1) fs_step1<N1, N2>(a, n2, Y + r1 * YS, tw4);
   __syncthreads();
   const real dn = real(1) / (real)N;
-  const bool act3 = t < RP * N1;
-  const int r3 = t / N1, k1 = t % N1;
-  real2 b[N2];
-  if (act3) fs_step3<N1, N2>(b, k1, Y + r3 * YS);
-  __syncthreads();  // X overwrites Y
-  if (act3) {
+  if (t < RP * N1) {
+    const int r = t / N1, k1 = t % N1;
+    real2 a[N2];
+    fs_step3<N1, N2>(a, k1, Y + r * YS);
+    const int64_t ra = row0 + 2 * r, rb = ra + 1;
 #pragma unroll
     for (int k2 = 0; k2 < N2; ++k2) {
       const int i = k1 + N1 * k2;  // conj(z) * dn: real part -> row A, imaginary part -> row B
-      X[(2 * r3) * N + i] = b[k2].x * dn;
-      X[(2 * r3 + 1) * N + i] = -b[k2].y * dn;
+      if (ra < nrows_total) mid[(size_t)ra * N + i] = a[k2].x * dn;
+      if (rb < nrows_total) mid[(size_t)rb * N + i] = -a[k2].y * dn;
     }
   }
-  __syncthreads();
-  const int nv = nr * N * (int)sizeof(real) / 16;
-  vec16* dst = (vec16*)(mid + row0 * N);
-  for (int v = t; v < nv; v += FS_THREADS) dst[v] = ((const vec16*)X)[v];
 }
 
 // forward y pass (phys -> mid): one z level, 16 consecutive x columns
@@ -739,7 +684,7 @@ bool fs_fwd_x(int n1, int n2, unsigned nb, cudaStream_t st, const Geom& g, int64
 template <int OP>
 bool fs_inv_x_op(int n1, int n2, unsigned nb, cudaStream_t st, const Geom& g, int64_t nrows, const real2* tw4,
                  const real* spec, real* mid, const SpecIn<real>& S) {
-#define CALL(A, B) k4_inv_x<A, B, OP><<<nb, FS_THREADS, InvX<A, B, OP>::SMEM, st>>>(g, nrows, tw4, spec, mid, S)
+#define CALL(A, B) k4_inv_x<A, B, OP><<<nb, FS_THREADS, 0, st>>>(g, nrows, tw4, spec, mid, S)
   PMPIC_FS_CASES(CALL)
 #undef CALL
 }
@@ -846,19 +791,7 @@ int fft_backward_impl(pmpic_ctx* ctx, const real* spec, real* phys, real* mid, c
 // shared-memory limits of the Stockham kernels (a property of each function on
 // the current device)
 cudaError_t fft_attributes() {
-  cudaError_t e = cudaSuccess;
-  // the four-step inverse x pass stages its rows dynamically (SPEC_VEL on FP64: above 48 KB)
-#define PMPIC_INVX_ATTR(A, B)                                                                           \
-  if (e == cudaSuccess)                                                                                 \
-    e = cudaFuncSetAttribute(k4_inv_x<A, B, SPEC_VEL>, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
-                             (int)InvX<A, B, SPEC_VEL>::SMEM);
-  PMPIC_INVX_ATTR(4, 4)
-  PMPIC_INVX_ATTR(8, 4)
-  PMPIC_INVX_ATTR(8, 8)
-  PMPIC_INVX_ATTR(16, 8)
-  PMPIC_INVX_ATTR(16, 16)
-#undef PMPIC_INVX_ATTR
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fwd_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaError_t e = cudaFuncSetAttribute(k_fwd_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fwd_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);

@@ -232,11 +232,14 @@ __global__ void k_scan_apply(const int32_t* __restrict__ in, int64_t n, const in
 //     first), then the normalisation or wall doubling.
 template <int NQ, class R = double>
 struct P2GArgs {
-  const R* f[NQ];       // per-parcel fields (MODE 1/2: f[0] unused)
-  R* out[NQ];
-  const R* bh[3];       // b, h, z for btot (plain FP64 path only)
-  int32_t* npercell;
-  double vmin;
+  const R* f[NQ] = {};      // per-parcel fields (MODE 1/2: f[0] unused)
+  R* out[NQ] = {};
+  // BT: b, h and z of btot; z is FP64 (stride 1) on the plain path, the cell
+  // index half of the {cell index, offset} positions (stride 2) on the mixed form
+  const R* bh[3] = {};
+  R* btot = nullptr;        // BT: the btot property, written as staged
+  int32_t* npercell = nullptr;
+  double vmin = 0.0;
 };
 
 constexpr int ZC = 16;                    // cell layers per z chunk: two lanes per layer
@@ -292,7 +295,6 @@ __global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, 
   using Lay = P2GLayout<NQ, MODE, BT>;
   constexpr int NA = Lay::NA, NS = Lay::NS;
   constexpr unsigned FULL = 0xffffffffu;
-  static_assert(!BT || sizeof(R) == 8, "btot from b, h, z only on the FP64 path");
   __shared__ __align__(16) R smem[RW][NS * SPAD];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t wid = (int64_t)blockIdx.x * RW + warp;
@@ -375,8 +377,9 @@ __global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, 
 #pragma unroll
           for (int f = 0; f < (BT ? NQ - 1 : NQ); ++f) cp_async_r(D + (4 + f) * SPAD, a.f[f] + n);
           if (BT) {
-#pragma unroll
-            for (int f = 0; f < 3; ++f) cp_async_r(D + (4 + NQ - 1 + f) * SPAD, a.bh[f] + n);
+            cp_async_r(D + (4 + NQ - 1) * SPAD, a.bh[0] + n);
+            cp_async_r(D + (4 + NQ) * SPAD, a.bh[1] + n);
+            cp_async_r(D + (4 + NQ + 1) * SPAD, a.bh[2] + nd);
           }
         } else {
 #pragma unroll
@@ -391,14 +394,22 @@ __global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, 
       }
       cp_async_wait_all();
       __syncwarp();
-      if constexpr (BT) {  // btot per parcel, once (vorticity_tendency.F90:123-124)
+      if constexpr (BT) {  // btot per parcel (vorticity_tendency.F90:121-126), also stored as the property
 #pragma unroll
         for (int j = 0; j < BATCH / 32; ++j) {
           const int p = lane + 32 * j;
           if (p >= nb) continue;
           R* D = S + p + (p >> 4) + (4 + NQ - 1) * SPAD;
-          const R bb = D[0], hh = D[SPAD], zz = D[2 * SPAD];
-          D[0] = bb + 12.5 * fmax(0.0, hh - exp(-zz));
+          const R bb = D[0], hh = D[SPAD];
+          R bt;
+          if constexpr (sizeof(R) == 8) {
+            bt = bb + 12.5 * fmax(0.0, hh - exp(-D[2 * SPAD]));
+          } else {  // z from its cell index and offset, in FP32
+            const float zz = ((float)__float_as_int(D[2 * SPAD]) + S[p + (p >> 4) + 2 * SPAD]) * (float)g.dz;
+            bt = bb + 12.5f * fmaxf(0.f, hh - expf(-zz));
+          }
+          D[0] = bt;
+          a.btot[slot[j]] = bt;  // a seed-column parcel is staged by two warps: the same value twice
         }
         __syncwarp();
       }
@@ -675,6 +686,7 @@ static int launch_p2g(pmpic_ctx* ctx, const double* const* fields, double* const
   a.bh[0] = prop(ctx, PMPIC_PROP_B);
   a.bh[1] = prop(ctx, PMPIC_PROP_H);
   a.bh[2] = prop(ctx, PMPIC_PROP_Z);
+  a.btot = prop(ctx, PMPIC_PROP_BTOT);
   a.npercell = ctx->npercell;
   a.vmin = g.vmin;
   const double* del = ctx->del;
@@ -686,7 +698,7 @@ static int launch_p2g(pmpic_ctx* ctx, const double* const* fields, double* const
 
 // the mixed form's par2grid: FP32 fields and accumulation, cell offsets read
 // from the {cell index, offset} positions
-template <int NQ, int MODE>
+template <int NQ, int MODE, bool BT = false>
 static int launch_p2g_m(pmpic_ctx* ctx, const float* const* fields, float* const* out) {
   TimerScope ts(ctx, T_P2G);
   const Geom& g = ctx->g;
@@ -695,20 +707,32 @@ static int launch_p2g_m(pmpic_ctx* ctx, const float* const* fields, float* const
     a.f[q] = fields[q];
     a.out[q] = out[q];
   }
+  a.bh[0] = propf(ctx, PMPIC_PROP_B);
+  a.bh[1] = propf(ctx, PMPIC_PROP_H);
+  a.bh[2] = (const float*)prop(ctx, PMPIC_PROP_Z);  // the cell index halves
+  a.btot = propf(ctx, PMPIC_PROP_BTOT);
   a.npercell = ctx->npercell;
   a.vmin = (double)(float)g.vmin;
   const float* px = (const float*)prop(ctx, PMPIC_PROP_X) + 1;  // offset halves of the CellOff slots
   const float* py = (const float*)prop(ctx, PMPIC_PROP_Y) + 1;
   const float* pz = (const float*)prop(ctx, PMPIC_PROP_Z) + 1;
-  PMPIC_CUDA((run_p2g<NQ, MODE, false, float>(g, ctx->cell_start, ctx->sorted, px, py, pz, 2,
+  PMPIC_CUDA((run_p2g<NQ, MODE, BT, float>(g, ctx->cell_start, ctx->sorted, px, py, pz, 2,
                                               propf(ctx, PMPIC_PROP_VOL), a, (float*)ctx->rowpart, ctx->stream,
                                               ctx->p2g_xseg)));
   ctx->nlaunch += 2;
   return 0;
 }
 
-// par2grid of nf FP32 fields on the mixed form (1, 3 or 4 fields)
-int par2grid_multi_m(pmpic_ctx* ctx, const float* const* fields, int nf, float* const* out) {
+// par2grid of nf FP32 fields on the mixed form (1, 3 or 4 fields); with btot
+// the last field is btot computed from b, h, z (and stored as the property)
+int par2grid_multi_m(pmpic_ctx* ctx, const float* const* fields, int nf, float* const* out, bool btot) {
+  if (btot) {
+    switch (nf) {
+      case 1: return launch_p2g_m<1, 0, true>(ctx, fields, out);
+      case 4: return launch_p2g_m<4, 0, true>(ctx, fields, out);
+      default: return set_error(ctx, PMPIC_ERR_ARG, "par2grid_multi_m: btot with 1 or 4 fields");
+    }
+  }
   switch (nf) {
     case 1: return launch_p2g_m<1, 0>(ctx, fields, out);
     case 3: return launch_p2g_m<3, 0>(ctx, fields, out);
