@@ -282,12 +282,18 @@ __device__ __forceinline__ void cp_async_r(R* smem, const R* gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+
+// acc + w * f: one rounding (FMA) on the FP32 form; on the FP64 path the
+// product and the sum are rounded separately, as the reference computes them
+__device__ __forceinline__ double madd(double w, double f, double acc) { return acc + w * f; }
+__device__ __forceinline__ float madd(float w, float f, float acc) { return __fmaf_rn(w, f, acc); }
+
 // R: the arithmetic type (double: plain path, float: mixed-precision form).
 // The cell offsets delx, dely, delz of parcel n are DX[ds * n], DY[ds * n],
 // DZ[ds * n]: the cached binning (ds = 1) or the offset half of the mixed
 // form's {cell index, offset} positions (ds = 2).
 template <int NQ, int MODE, bool BT, class R = double>
-__global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, int xseg, const int32_t* __restrict__ start,
+__global__ void __launch_bounds__(32 * RW, sizeof(R) == 4 ? 6 : 1) k_p2g_rows(Geom g, int nzc, int nxs, int xseg, const int32_t* __restrict__ start,
                                                      const int32_t* __restrict__ sorted, const R* __restrict__ DX,
                                                      const R* __restrict__ DY, const R* __restrict__ DZ, int ds,
                                                      const R* __restrict__ VOL, P2GArgs<NQ, R> a,
@@ -310,13 +316,9 @@ __global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, 
   // and odd lane 2m+1 level m+1 (top corners of layer m + bottom corners of m+1)
   const int lev = lane == 0 ? 0 : (lane >> 1) + 1;
   const bool owner = (lane == 0 || (lane & 1)) && lev <= nk;
-  R* S = smem[warp];
   R* out_row = rowpart + ((size_t)zc * g.Ny + cy) * (size_t)g.Nx * Lay::RPS;
   R C[2][NA];  // x-high corners of the previous column, per y corner
-  // Column it's bounds (this lane's cell layer) and its first batch of slots
-  // are loaded one column ahead, so a column waits on one memory latency (its
-  // staged fields), not three (bounds, slots, fields).
-  auto bounds = [&](int it, int& s, int& e) {
+  auto bounds = [&](int it, int& s, int& e) {  // this lane's cell layer of column it
     int cx = x_lo + it;
     if (cx < 0) cx += g.Nx;
     const int64_t cb = ((int64_t)cx * g.Ny + cy) * g.Nz + k0;
@@ -333,129 +335,98 @@ __global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, 
       sl[j] = p < nb ? sorted[b0 + p] : -1;
     }
   };
-  int s_me, e_me;
-  bounds(-1, s_me, e_me);
-  int q0 = __shfl_sync(FULL, s_me, 0);
-  int q1 = __shfl_sync(FULL, e_me, 2 * nk - 2);
-  int pre[BATCH / 32];
-  slots(q0, min(BATCH, q1 - q0), pre);
-  // the column before the segment (periodic) only seeds the carry
-  for (int it = -1; it < x_hi - x_lo; ++it) {
-    const int cx = x_lo + it;  // >= 0 where the row partials are written (it >= 0)
-    const bool more = it + 1 < x_hi - x_lo;
-    int s_nx = 0, e_nx = 0, q0n = 0, q1n = 0;
-    if (more) bounds(it + 1, s_nx, e_nx);
-    R acc[4][NA];  // [y corner * 2 + x corner][quantity] of this lane's z corner
+  // the fields of a batch of parcels into shared memory, field-major, position
+  // p at p + p/16 (no bank conflicts for the readers)
+  auto stage = [&](R* Sb, const int* sl) {
 #pragma unroll
-    for (int ab = 0; ab < 4; ++ab)
+    for (int j = 0; j < BATCH / 32; ++j) {
+      const int n = sl[j];
+      if (n < 0) continue;
+      const int p = lane + 32 * j;
+      R* D = Sb + p + (p >> 4);
+      const size_t nd = (size_t)ds * n;
+      cp_async_r(D, DX + nd);
+      cp_async_r(D + SPAD, DY + nd);
+      cp_async_r(D + 2 * SPAD, DZ + nd);
+      cp_async_r(D + 3 * SPAD, VOL + n);
+      if (MODE == 0) {
 #pragma unroll
-      for (int q = 0; q < NA; ++q) acc[ab][q] = R(0);
-    int nkept = 0;
-    bool prefetched = false;
-    for (int b0 = q0; b0 < q1; b0 += BATCH) {
-      const int nb = min(BATCH, q1 - b0);
-      __syncwarp();  // the previous batch has been read
-      int slot[BATCH / 32];
-      if (b0 == q0) {
-#pragma unroll
-        for (int j = 0; j < BATCH / 32; ++j) slot[j] = pre[j];
+        for (int f = 0; f < (BT ? NQ - 1 : NQ); ++f) cp_async_r(D + (4 + f) * SPAD, a.f[f] + n);
+        if (BT) {
+          cp_async_r(D + (4 + NQ - 1) * SPAD, a.bh[0] + n);
+          cp_async_r(D + (4 + NQ) * SPAD, a.bh[1] + n);
+          cp_async_r(D + (4 + NQ + 1) * SPAD, a.bh[2] + nd);
+        }
       } else {
-        slots(b0, nb, slot);
+#pragma unroll
+        for (int f = 1; f < NQ; ++f) cp_async_r(D + (4 + f - 1) * SPAD, a.f[f] + n);
+      }
+    }
+  };
+  // btot per staged parcel (vorticity_tendency.F90:121-126), also stored as the property
+  auto btot_pass = [&](R* Sb, const int* sl, int nb) {
+#pragma unroll
+    for (int j = 0; j < BATCH / 32; ++j) {
+      const int p = lane + 32 * j;
+      if (p >= nb) continue;
+      R* D = Sb + p + (p >> 4) + (4 + NQ - 1) * SPAD;
+      const R bb = D[0], hh = D[SPAD];
+      R bt;
+      if constexpr (sizeof(R) == 8) {
+        bt = bb + 12.5 * fmax(0.0, hh - exp(-D[2 * SPAD]));
+      } else {  // z from its cell index and offset, in FP32
+        const float zz = ((float)__float_as_int(D[2 * SPAD]) + Sb[p + (p >> 4) + 2 * SPAD]) * (float)g.dz;
+        bt = bb + 12.5f * fmaxf(0.f, hh - expf(-zz));
+      }
+      D[0] = bt;
+      a.btot[sl[j]] = bt;  // a seed-column parcel is staged by two warps: the same value twice
+    }
+    __syncwarp();
+  };
+  // this lane's parcels (its cell layer, its z corner) among staged positions
+  // b0 .. b0+nb-1, in slot order
+  auto accumulate = [&](const R* Sb, int b0, int nb, int s_me, int e_me, R (&acc)[4][NA], int& nkept) {
+    const int lo = max(s_me, b0) - b0, hi = min(e_me, b0 + nb) - b0;
+    for (int p = lo; p < hi; ++p) {
+      const R* D = Sb + p + (p >> 4);
+      const R delx = D[0], dely = D[SPAD], delz = D[2 * SPAD], vv = D[3 * SPAD];
+      if (MODE == 1 && vv < a.vmin) continue;  // parcel_mixing.F90:488
+      if (MODE == 2 && !(vv < a.vmin)) continue;
+      if (MODE == 1) ++nkept;
+      // parcel_interpolation.F90:390-434: w = (1-delz)(1-dely)(1-delx) v etc.,
+      // evaluated left to right as there
+      const R ez = cz ? delz : R(1) - delz;
+      const R zy0 = ez * (R(1) - dely), zy1 = ez * dely;
+      R w[4];
+      w[0] = zy0 * (R(1) - delx) * vv;
+      w[1] = zy0 * delx * vv;
+      w[2] = zy1 * (R(1) - delx) * vv;
+      w[3] = zy1 * delx * vv;
+      R fv[NA];
+      if (MODE == 0) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) fv[q] = D[(4 + q) * SPAD];
+      } else {
+#pragma unroll
+        for (int q = 1; q < NQ; ++q) fv[q] = D[(4 + q - 1) * SPAD];
       }
 #pragma unroll
-      for (int j = 0; j < BATCH / 32; ++j) {
-        const int n = slot[j];
-        if (n < 0) continue;
-        const int p = lane + 32 * j;
-        R* D = S + p + (p >> 4);
-        const size_t nd = (size_t)ds * n;
-        cp_async_r(D, DX + nd);
-        cp_async_r(D + SPAD, DY + nd);
-        cp_async_r(D + 2 * SPAD, DZ + nd);
-        cp_async_r(D + 3 * SPAD, VOL + n);
+      for (int ab = 0; ab < 4; ++ab) {
         if (MODE == 0) {
 #pragma unroll
-          for (int f = 0; f < (BT ? NQ - 1 : NQ); ++f) cp_async_r(D + (4 + f) * SPAD, a.f[f] + n);
-          if (BT) {
-            cp_async_r(D + (4 + NQ - 1) * SPAD, a.bh[0] + n);
-            cp_async_r(D + (4 + NQ) * SPAD, a.bh[1] + n);
-            cp_async_r(D + (4 + NQ + 1) * SPAD, a.bh[2] + nd);
-          }
+          for (int q = 0; q < NQ; ++q) acc[ab][q] = madd(w[ab], fv[q], acc[ab][q]);
+          acc[ab][NQ] += w[ab];
         } else {
+          acc[ab][0] += w[ab];
 #pragma unroll
-          for (int f = 1; f < NQ; ++f) cp_async_r(D + (4 + f - 1) * SPAD, a.f[f] + n);
-        }
-      }
-      if (more && b0 + BATCH >= q1) {  // the column's last batch: the next column's first slots
-        q0n = __shfl_sync(FULL, s_nx, 0);
-        q1n = __shfl_sync(FULL, e_nx, 2 * nk - 2);
-        slots(q0n, min(BATCH, q1n - q0n), pre);
-        prefetched = true;
-      }
-      cp_async_wait_all();
-      __syncwarp();
-      if constexpr (BT) {  // btot per parcel (vorticity_tendency.F90:121-126), also stored as the property
-#pragma unroll
-        for (int j = 0; j < BATCH / 32; ++j) {
-          const int p = lane + 32 * j;
-          if (p >= nb) continue;
-          R* D = S + p + (p >> 4) + (4 + NQ - 1) * SPAD;
-          const R bb = D[0], hh = D[SPAD];
-          R bt;
-          if constexpr (sizeof(R) == 8) {
-            bt = bb + 12.5 * fmax(0.0, hh - exp(-D[2 * SPAD]));
-          } else {  // z from its cell index and offset, in FP32
-            const float zz = ((float)__float_as_int(D[2 * SPAD]) + S[p + (p >> 4) + 2 * SPAD]) * (float)g.dz;
-            bt = bb + 12.5f * fmaxf(0.f, hh - expf(-zz));
-          }
-          D[0] = bt;
-          a.btot[slot[j]] = bt;  // a seed-column parcel is staged by two warps: the same value twice
-        }
-        __syncwarp();
-      }
-      const int lo = max(s_me, b0) - b0, hi = min(e_me, b0 + nb) - b0;
-      for (int p = lo; p < hi; ++p) {
-        const R* D = S + p + (p >> 4);
-        const R delx = D[0], dely = D[SPAD], delz = D[2 * SPAD], vv = D[3 * SPAD];
-        if (MODE == 1 && vv < a.vmin) continue;  // parcel_mixing.F90:488
-        if (MODE == 2 && !(vv < a.vmin)) continue;
-        if (MODE == 1) ++nkept;
-        // parcel_interpolation.F90:390-434: w = (1-delz)(1-dely)(1-delx) v etc.,
-        // evaluated left to right as there
-        const R ez = cz ? delz : R(1) - delz;
-        const R zy0 = ez * (R(1) - dely), zy1 = ez * dely;
-        R w[4];
-        w[0] = zy0 * (R(1) - delx) * vv;
-        w[1] = zy0 * delx * vv;
-        w[2] = zy1 * (R(1) - delx) * vv;
-        w[3] = zy1 * delx * vv;
-        R fv[NA];
-        if (MODE == 0) {
-#pragma unroll
-          for (int q = 0; q < NQ; ++q) fv[q] = D[(4 + q) * SPAD];
-        } else {
-#pragma unroll
-          for (int q = 1; q < NQ; ++q) fv[q] = D[(4 + q - 1) * SPAD];
-        }
-#pragma unroll
-        for (int ab = 0; ab < 4; ++ab) {
-          if (MODE == 0) {
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) acc[ab][q] += w[ab] * fv[q];
-            acc[ab][NQ] += w[ab];
-          } else {
-            acc[ab][0] += w[ab];
-#pragma unroll
-            for (int q = 1; q < NQ; ++q) acc[ab][q] += w[ab] * fv[q];
-          }
+          for (int q = 1; q < NQ; ++q) acc[ab][q] = madd(w[ab], fv[q], acc[ab][q]);
         }
       }
     }
-    if (more && !prefetched) {  // an empty column
-      q0n = __shfl_sync(FULL, s_nx, 0);
-      q1n = __shfl_sync(FULL, e_nx, 2 * nk - 2);
-      slots(q0n, min(BATCH, q1n - q0n), pre);
-    }
+  };
+  // the column's z combination, its row partials (grid point x = cx: x-high
+  // corners of column cx-1, then x-low corners of column cx) and the carry
+  auto finish = [&](int it, R (&acc)[4][NA], int nkept) {
     // level m+1 = top corners of layer m (odd lane 2m+1) + bottom corners of layer m+1 (lane 2m+2)
 #pragma unroll
     for (int ab = 0; ab < 4; ++ab)
@@ -465,7 +436,7 @@ __global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, 
         if ((lane & 1) && kk + 1 < nk) acc[ab][q] = acc[ab][q] + o;
       }
     if (it >= 0) {
-      // grid point x = cx: x-high corners of column cx-1, then x-low corners of column cx
+      const int cx = x_lo + it;
       if (owner) {
         R* dst = out_row + (size_t)cx * Lay::RPS + lev;
 #pragma unroll
@@ -479,10 +450,62 @@ __global__ void __launch_bounds__(32 * RW) k_p2g_rows(Geom g, int nzc, int nxs, 
     for (int b = 0; b < 2; ++b)
 #pragma unroll
       for (int q = 0; q < NA; ++q) C[b][q] = acc[2 * b + 1][q];
-    s_me = s_nx;
-    e_me = e_nx;
-    q0 = q0n;
-    q1 = q1n;
+  };
+  const int last = x_hi - x_lo - 1;  // columns -1 .. last; -1 (periodic) only seeds the carry
+  {
+    // column it+1's bounds and first slots are loaded ahead, so a column
+    // waits on one memory latency (its staged fields), not three
+    R* S = smem[warp];
+    int s_me, e_me;
+    bounds(-1, s_me, e_me);
+    int q0 = __shfl_sync(FULL, s_me, 0);
+    int q1 = __shfl_sync(FULL, e_me, 2 * nk - 2);
+    int pre[BATCH / 32];
+    slots(q0, min(BATCH, q1 - q0), pre);
+    for (int it = -1; it <= last; ++it) {
+      const bool more = it + 1 <= last;
+      int s_nx = 0, e_nx = 0, q0n = 0, q1n = 0;
+      if (more) bounds(it + 1, s_nx, e_nx);
+      R acc[4][NA];
+#pragma unroll
+      for (int ab = 0; ab < 4; ++ab)
+#pragma unroll
+        for (int q = 0; q < NA; ++q) acc[ab][q] = R(0);
+      int nkept = 0;
+      bool prefetched = false;
+      for (int b0 = q0; b0 < q1; b0 += BATCH) {
+        const int nb = min(BATCH, q1 - b0);
+        __syncwarp();  // the previous batch has been read
+        int slot[BATCH / 32];
+        if (b0 == q0) {
+#pragma unroll
+          for (int j = 0; j < BATCH / 32; ++j) slot[j] = pre[j];
+        } else {
+          slots(b0, nb, slot);
+        }
+        stage(S, slot);
+        if (more && b0 + BATCH >= q1) {  // the column's last batch: the next column's first slots
+          q0n = __shfl_sync(FULL, s_nx, 0);
+          q1n = __shfl_sync(FULL, e_nx, 2 * nk - 2);
+          slots(q0n, min(BATCH, q1n - q0n), pre);
+          prefetched = true;
+        }
+        cp_async_wait_all();
+        __syncwarp();
+        if constexpr (BT) btot_pass(S, slot, nb);
+        accumulate(S, b0, nb, s_me, e_me, acc, nkept);
+      }
+      if (more && !prefetched) {  // an empty column
+        q0n = __shfl_sync(FULL, s_nx, 0);
+        q1n = __shfl_sync(FULL, e_nx, 2 * nk - 2);
+        slots(q0n, min(BATCH, q1n - q0n), pre);
+      }
+      finish(it, acc, nkept);
+      s_me = s_nx;
+      e_me = e_nx;
+      q0 = q0n;
+      q1 = q1n;
+    }
   }
 }
 

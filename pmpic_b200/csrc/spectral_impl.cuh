@@ -107,17 +107,38 @@ __global__ void k_bt_planes(Geom g, const real* __restrict__ a, const real* __re
 }
 
 // ---- compact z operators ----------------------------------------------------------
+// The z recurrences run one thread per spectral column, so only about 14 warps
+// per SM are resident at 256^2 columns and a level costs the latency of its
+// dependent instructions, most of them the division.  The FP64 path divides as
+// the reference does (IEEE, bit for bit); the FP32 form uses the
+// reciprocal-based quotient (within 2 ulp), well inside its tolerance.
+__device__ __forceinline__ real zdiv(real x, real y) {
+  if constexpr (sizeof(real) == 4) return __fdividef(x, y);
+  else return x / y;
+}
+
 // diffz (fft_ops.F90:419-483).  The tridiagonal coefficients are the same for
 // every column, so the Thomas factors (cp and the denominators) are computed
 // once on the host with the reference's arithmetic and passed in.
-__global__ void k_diffz(Geom g, const real* __restrict__ f, real* __restrict__ out,
-                        const real* __restrict__ coef /* a[nz], den[nz], cp[nz] */, const real* __restrict__ bot,
-                        const real* __restrict__ top, real a1) {
-  int col = blockIdx.x * blockDim.x + threadIdx.x;
+// blockIdx.y selects one of up to two independent solves in the same launch.
+struct DzBatch {
+  const real* f[2];
+  real* out[2];
+  const real* bot[2];  // both null: no boundary values (df0 form)
+  const real* top[2];
+};
+__global__ void k_diffz(Geom g, DzBatch zb, const real* __restrict__ coef /* a[nz], den[nz], cp[nz] */,
+                        real a1) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
   const int cols = g.sx * g.sy;
   if (col >= cols) return;
+  const int q = blockIdx.y;  // selected without indexing the parameter arrays (no local copy)
+  const real* __restrict__ f = q == 0 ? zb.f[0] : zb.f[1];
+  real* __restrict__ out = q == 0 ? zb.out[0] : zb.out[1];
+  const real* __restrict__ bot = q == 0 ? zb.bot[0] : zb.bot[1];
+  const real* __restrict__ top = q == 0 ? zb.top[0] : zb.top[1];
   const int nz = g.nzp;
-  const int64_t cs = cols;
+  const uint32_t cs = (uint32_t)cols;  // level offsets fit 32 bits (the spectral grid is < 2^31)
   const real* A = coef;
   const real* DEN = coef + nz;
   const real* CP = coef + 2 * nz;
@@ -129,20 +150,20 @@ __global__ void k_diffz(Geom g, const real* __restrict__ f, real* __restrict__ o
   constexpr int ZB = 8;
   real fm = f[col], f0 = f[cs + col];
   real d1 = bt ? f0 / dz - a1 * bot[col] * dz : real(0);
-  real prev = d1 / DEN[0];
+  real prev = zdiv(d1, DEN[0]);
   out[col] = prev;
   for (int kb = 1; kb < nz - 1; kb += ZB) {
     real fb[ZB];
 #pragma unroll
     for (int u = 0; u < ZB; ++u)
-      if (kb + u < nz - 1) fb[u] = f[(int64_t)(kb + u + 1) * cs + col];
+      if (kb + u < nz - 1) fb[u] = f[(uint32_t)(kb + u + 1) * cs + col];
 #pragma unroll
     for (int u = 0; u < ZB; ++u) {
       const int k = kb + u;
       if (k >= nz - 1) break;
       real d = (fb[u] - fm) / real(2) / dz;
-      prev = (d - A[k] * prev) / DEN[k];
-      out[(int64_t)k * cs + col] = prev;
+      prev = zdiv(d - A[k] * prev, DEN[k]);
+      out[(uint32_t)k * cs + col] = prev;
       fm = f0;
       f0 = fb[u];
     }
@@ -150,8 +171,8 @@ __global__ void k_diffz(Geom g, const real* __restrict__ f, real* __restrict__ o
   {
     int k = nz - 1;
     real dn = bt ? -fm / dz + a1 * top[col] * dz : real(0);  // fm = f(nz-1)
-    prev = (dn - A[k] * prev) / DEN[k];
-    out[(int64_t)k * cs + col] = prev;
+    prev = zdiv(dn - A[k] * prev, DEN[k]);
+    out[(uint32_t)k * cs + col] = prev;
   }
   // back substitution: f(i) = f(i) - cp(i+1) f(i+1)
   real nxt = prev;
@@ -159,13 +180,13 @@ __global__ void k_diffz(Geom g, const real* __restrict__ f, real* __restrict__ o
     real ob[ZB];
 #pragma unroll
     for (int u = 0; u < ZB; ++u)
-      if (kb - u >= 0) ob[u] = out[(int64_t)(kb - u) * cs + col];
+      if (kb - u >= 0) ob[u] = out[(uint32_t)(kb - u) * cs + col];
 #pragma unroll
     for (int u = 0; u < ZB; ++u) {
       const int k = kb - u;
       if (k < 0) break;
       real v = ob[u] - CP[k + 1] * nxt;
-      out[(int64_t)k * cs + col] = v;
+      out[(uint32_t)k * cs + col] = v;
       nxt = v;
     }
   }
@@ -212,7 +233,7 @@ __global__ void k_laplinv(Geom g, LapBatch lb, real* __restrict__ cpbase, const 
   }
   // tridiagonal (fft_ops.F90:620-656)
   real den = b1;
-  real prev = d / den;
+  real prev = zdiv(d, den);
   f[col] = prev;
   real cprev = c1;  // c(i-1)
   // loads of each batch of ZB levels first, then its recurrence (one memory
@@ -238,9 +259,9 @@ __global__ void k_laplinv(Geom g, LapBatch lb, real* __restrict__ cpbase, const 
         a = an; b = bn; c = real(0);
         d = df0 ? f13 * f0 + f16 * fm : real(0);
       }
-      real cp = cprev / den;
+      real cp = zdiv(cprev, den);
       den = b - a * cp;
-      prev = (d - a * prev) / den;
+      prev = zdiv(d - a * prev, den);
       f[(int64_t)k * cs + col] = prev;
       cpbuf[(int64_t)k * cs + col] = cp;
       cprev = c;
@@ -299,14 +320,26 @@ __global__ void k_max_vort(int64_t n, const real* __restrict__ p, const real* __
   if ((threadIdx.x & 31) == 0) atomicMax((unsigned long long*)out, __double_as_longlong((double)m));
 }
 
-int diffz_launch_impl(pmpic_ctx* ctx, const real* in, real* out, const real* bot, const real* top) {
+// nb (1 or 2) diffz solves of one boundary kind (all with or all without
+// boundary values) in one launch
+int diffz_batch_impl(pmpic_ctx* ctx, int nb, const real* const* in, real* const* out, const real* const* bot,
+                     const real* const* top) {
   TimerScope ts(ctx, T_DIFFZ);
   const Geom& g = ctx->g;
-  int which = bot ? 1 : 0;
-  const real* coef = tab_diffz(ctx, which);
-  k_diffz<<<nblk((int64_t)g.sx * g.sy, 128), 128, 0, ctx->stream>>>(g, in, out, coef, bot, top, (real)f4div(1.f, 6.f)); ++ctx->nlaunch;
+  DzBatch zb{};
+  for (int q = 0; q < nb; ++q) {
+    zb.f[q] = in[q];
+    zb.out[q] = out[q];
+    zb.bot[q] = bot ? bot[q] : nullptr;
+    zb.top[q] = top ? top[q] : nullptr;
+  }
+  const real* coef = tab_diffz(ctx, bot ? 1 : 0);
+  k_diffz<<<dim3(nblk((int64_t)g.sx * g.sy, 128), nb), 128, 0, ctx->stream>>>(g, zb, coef, (real)f4div(1.f, 6.f)); ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
+}
+int diffz_launch_impl(pmpic_ctx* ctx, const real* in, real* out, const real* bot, const real* top) {
+  return diffz_batch_impl(ctx, 1, &in, &out, bot ? &bot : nullptr, top ? &top : nullptr);
 }
 
 
@@ -397,14 +430,21 @@ int vort2vel_spectral_impl(pmpic_ctx* ctx) {
   V.kx = tab_kx(ctx);
   V.ky = tab_ky(ctx);
   V.filt = tab_filt(ctx);
+  // dB/dz into e and dA/dz into d (:255, :284), in one launch
+  {
+    const real* zin[2] = {b, a};
+    real* zout[2] = {e, d};
+    const real* zbot[2] = {bbot, abot};
+    const real* ztop[2] = {btop, atop};
+    if ((rc = diffz_batch_impl(ctx, 2, zin, zout, zbot, ztop))) return rc;
+  }
   // u = dB/dz - dC/dy (:251-276)
-  if ((rc = diffz_launch_impl(ctx, b, e, bbot, btop))) return rc;
   V.vmode = 0;
   V.fs = RP(ctx->spec[PMPIC_SPEC_U]);
   V.zbar = ctx->zmode;
   if ((rc = fft_backward(ctx, nullptr, G[PMPIC_GRID_U], V, plain))) return rc;
   // v = dC/dx - dA/dz (:280-302)
-  if ((rc = diffz_launch_impl(ctx, a, e, abot, atop))) return rc;
+  V.e = d;
   V.vmode = 1;
   V.fs = RP(ctx->spec[PMPIC_SPEC_V]);
   V.zbar = ctx->zmode + g.nzp;
