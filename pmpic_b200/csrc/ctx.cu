@@ -226,6 +226,7 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   ctx->n = 0;
   ctx->sorted_valid = false;
   ctx->count_ready = false;
+  ctx->in_domain = false;
   ctx->btot_grid_ready = false;
   ctx->pending_uvw = ctx->pending_pqr = ctx->dir_ready = false;
   ctx->nbmax = (std::max<int64_t>(ctx->cap, g.ncell) + 1023) / 1024 + 8;
@@ -465,6 +466,7 @@ int pmpic_set_count(pmpic_ctx* ctx, int64_t n) {
   ctx->info.n_parcels = n;
   ctx->sorted_valid = false;
   ctx->count_ready = false;
+  ctx->in_domain = false;
   ctx->btot_grid_ready = false;
   ctx->dir_ready = false;
   return PMPIC_OK;
@@ -486,6 +488,7 @@ int pmpic_set_property(pmpic_ctx* ctx, int p, int64_t n, const double* src) {
   PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
   ctx->sorted_valid = false;
   ctx->count_ready = false;
+  ctx->in_domain = false;
   ctx->btot_grid_ready = false;
   return PMPIC_OK;
 }
@@ -531,6 +534,7 @@ int pmpic_upload_parcels(pmpic_ctx* ctx, int64_t n, const double* x, const doubl
   ctx->info.n_parcels = n;
   ctx->sorted_valid = false;
   ctx->count_ready = false;
+  ctx->in_domain = false;
   ctx->btot_grid_ready = false;
   return PMPIC_OK;
 }
@@ -976,6 +980,7 @@ int pmpic_sort_parcels(pmpic_ctx* ctx) {
   if (rc) return rc;
   ctx->sorted_valid = false;
   ctx->count_ready = false;
+  ctx->in_domain = false;
   ctx->btot_grid_ready = false;
   ctx->dir_ready = false;
   return sync_info(ctx);

@@ -143,6 +143,7 @@ int pmpic_read_parcels(pmpic_ctx* ctx, const char* path, int append, double* tim
   ctx->info.n_parcels = ctx->n;
   ctx->sorted_valid = false;
   ctx->count_ready = false;
+  ctx->in_domain = false;
   ctx->btot_grid_ready = false;
   ctx->dir_ready = false;
   return PMPIC_OK;

@@ -454,8 +454,11 @@ __global__ void k_split_flag(int64_t n, double* __restrict__ parcels, int64_t ca
   S[i] = s;
   flag[i] = s > 4. ? 1 : 0;                                  // :76 (stretchmax = 4)
 }
-__global__ void k_split_apply(int64_t n, const int32_t* __restrict__ list, const int32_t* __restrict__ nsplit,
-                              double* __restrict__ parcels, int64_t cap, DevInfo* info) {
+// With dir given (every other parcel is inside the domain, its dir zero), the
+// parent and the child are reflected at the walls and classified here, as the
+// parcel haloswap that follows (:134) would do for them.
+__global__ void k_split_apply(Geom g, int64_t n, const int32_t* __restrict__ list, const int32_t* __restrict__ nsplit,
+                              double* __restrict__ parcels, int64_t cap, DevInfo* info, int8_t* __restrict__ dir) {
   const int ns = *nsplit;
   const double pi = 4. * atan(1.0);
   const double third = f4div(1.f, 3.f);
@@ -497,6 +500,17 @@ __global__ void k_split_apply(int64_t n, const int32_t* __restrict__ list, const
     A(PMPIC_PROP_Z)[i] = z - r * rr / absw;
     A(PMPIC_PROP_VOL)[i] = vol / 2;
     A(PMPIC_PROP_STRETCH)[i] = 0.;
+    if (dir) {
+      const int64_t s2[2] = {c, i};
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int64_t m = s2[u];
+        const double zz = A(PMPIC_PROP_Z)[m];
+        if (zz < g.pzmin) A(PMPIC_PROP_Z)[m] = g.pzmin + (g.pzmin - zz);
+        else if (zz > g.pzmax) A(PMPIC_PROP_Z)[m] = g.pzmax - (zz - g.pzmax);
+        dir[m] = (int8_t)classify_dir(g, A(PMPIC_PROP_X)[m], A(PMPIC_PROP_Y)[m]);
+      }
+    }
   }
 }
 
@@ -918,7 +932,7 @@ __global__ void k_split_flag_m(int64_t n, double* __restrict__ parcels, int64_t 
   flag[i] = s > 4.f ? 1 : 0;
 }
 __global__ void k_split_apply_m(Geom g, int64_t n, const int32_t* __restrict__ list, const int32_t* __restrict__ nsplit,
-                                double* __restrict__ parcels, int64_t cap, DevInfo* info) {
+                                double* __restrict__ parcels, int64_t cap, DevInfo* info, int8_t* __restrict__ dir) {
   const int ns = *nsplit;
   const float pi = 3.14159265358979f;
   const float inv[3] = {(float)(1.0 / g.dx), (float)(1.0 / g.dy), (float)(1.0 / g.dz)};
@@ -940,12 +954,24 @@ __global__ void k_split_apply_m(Geom g, int64_t n, const int32_t* __restrict__ l
     const float absw = sqrtf(pp * pp + qq * qq + rr * rr);
     const float w[3] = {pp / absw, qq / absw, rr / absw};
     const int pos[3] = {PMPIC_PROP_X, PMPIC_PROP_Y, PMPIC_PROP_Z};
+    CellOff pc[3], pi_[3];
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
       const CellOff x = C(pos[v])[i];
       const float sh = r * w[v] * inv[v];
-      C(pos[v])[c] = co_add(x, sh);  // :95-118
-      C(pos[v])[i] = co_add(x, -sh);  // :121-127
+      pc[v] = co_add(x, sh);    // :95-118
+      pi_[v] = co_add(x, -sh);  // :121-127
+    }
+    if (dir) {  // reflected and classified here (k_split_apply)
+      pc[2] = co_reflect(pc[2], g.Nz);
+      pi_[2] = co_reflect(pi_[2], g.Nz);
+      dir[c] = (int8_t)classify_dir_m(g, pc[0].i, pc[1].i);
+      dir[i] = (int8_t)classify_dir_m(g, pi_[0].i, pi_[1].i);
+    }
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+      C(pos[v])[c] = pc[v];
+      C(pos[v])[i] = pi_[v];
     }
 #pragma unroll
     for (int q = 0; q < 11; ++q) F(fprops[q])[c] = F(fprops[q])[i];
@@ -1246,6 +1272,7 @@ int rk4_stage(pmpic_ctx* ctx, int stage) {
     ctx->dir_ready = true;
     ctx->sorted_valid = false;
     ctx->count_ready = true;
+    ctx->in_domain = false;
     ctx->btot_grid_ready = false;
     PMPIC_CUDA(cudaGetLastError());
     return 0;
@@ -1277,6 +1304,7 @@ int rk4_stage(pmpic_ctx* ctx, int stage) {
   ctx->dir_ready = true;  // z reflected and directions classified
   ctx->sorted_valid = false;
   ctx->count_ready = false;
+  ctx->in_domain = false;
   ctx->btot_grid_ready = false;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
@@ -1329,6 +1357,7 @@ int parcel_haloswap(pmpic_ctx* ctx) {
     k_swap_scatter<<<592, 256, 0, ctx->stream>>>(nmc, V, ctx->swapbuf, ctx->parcels, ctx->cap); ++ctx->nlaunch;
   }
   PMPIC_CUDA(cudaGetLastError());
+  ctx->in_domain = true;  // (a staging overflow is reported as an error and ends the run)
   return 0;
 }
 
@@ -1347,11 +1376,19 @@ int splitting(pmpic_ctx* ctx) {
     ++ctx->nlaunch;
     int rc = compact(ctx, PredFlag{flag}, n, list, ns);
     if (rc) return rc;
+    // after a haloswap only the split parcels can be outside the domain: the
+    // haloswap that follows needs no pass over all parcels to find them
+    int8_t* dsplit = nullptr;
+    if (ctx->in_domain) {
+      PMPIC_CUDA(cudaMemsetAsync(ctx->dir, 0, (size_t)n, ctx->stream));
+      dsplit = ctx->dir;
+    }
     if (ctx->mixed)
-      k_split_apply_m<<<592, 256, 0, ctx->stream>>>(ctx->g, n, list, ns, ctx->parcels, ctx->cap, ctx->dinfo);
+      k_split_apply_m<<<592, 256, 0, ctx->stream>>>(ctx->g, n, list, ns, ctx->parcels, ctx->cap, ctx->dinfo, dsplit);
     else
-      k_split_apply<<<592, 256, 0, ctx->stream>>>(n, list, ns, ctx->parcels, ctx->cap, ctx->dinfo);
+      k_split_apply<<<592, 256, 0, ctx->stream>>>(ctx->g, n, list, ns, ctx->parcels, ctx->cap, ctx->dinfo, dsplit);
     ++ctx->nlaunch;
+    ctx->dir_ready = dsplit != nullptr;
   } else {
     PMPIC_CUDA(cudaMemsetAsync(ns, 0, sizeof(int32_t), ctx->stream));
   }
@@ -1467,6 +1504,7 @@ int mixing(pmpic_ctx* ctx) {
   ctx->n = count;
   ctx->sorted_valid = false;
   ctx->count_ready = false;
+  ctx->in_domain = false;
   ctx->btot_grid_ready = false;
   ctx->info.n_removed = nremove;
   ctx->info.n_added = nadd;
