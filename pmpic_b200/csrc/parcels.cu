@@ -107,6 +107,11 @@ struct PredFlag {
   const int32_t* f;
   __device__ bool operator()(int64_t i) const { return f[i] != 0; }
 };
+// the split criterion on an already advanced FP32 stretch (parcel_splitting.F90:76)
+struct PredStretchM {
+  const float* s;
+  __device__ bool operator()(int64_t i) const { return s[i] > 4.f; }
+};
 // cell in the reference's loop order o = (i*Ny + j)*Nz + k (parcel_mixing.F90:160-162)
 struct PredNewCell {
   const int32_t* npc;
@@ -740,7 +745,7 @@ __device__ __forceinline__ int classify_dir_m(const Geom& g, int i, int j) {
 template <bool GU, bool GP>
 __global__ void __launch_bounds__(256, 5) k_rk4_m(Geom g, int64_t n, MPtrs P, int stage, const double* __restrict__ dtp,
                         int8_t* __restrict__ dir, int32_t* __restrict__ cell, int32_t* __restrict__ count,
-                        DevInfo* info) {
+                        DevInfo* info, float* __restrict__ stretch) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const float dt = (float)*dtp;  // state%dtm (rk4_integrator.F90:102)
@@ -811,6 +816,11 @@ __global__ void __launch_bounds__(256, 5) k_rk4_m(Geom g, int64_t n, MPtrs P, in
     }
   }
   sn[2] = co_reflect(sn[2], g.Nz);
+  if (stretch) {  // the split's stretch update (parcel_splitting.F90:64-73) on the final p, q, r
+    float ds = svn[0] * d[3] + svn[1] * d[4] + svn[2] * d[5];
+    ds = powf(fabsf(ds), 1.f / 3.f);
+    stretch[t] = stretch[t] + ds * dt;
+  }
 #pragma unroll
   for (int v = 0; v < 6; ++v)
     if (gathered && ((v < 3 && GU) || (v >= 3 && GP))) P.d[v][t] = d[v];
@@ -931,8 +941,19 @@ __global__ void k_split_flag_m(int64_t n, double* __restrict__ parcels, int64_t 
   F(PMPIC_PROP_STRETCH)[i] = s;
   flag[i] = s > 4.f ? 1 : 0;
 }
+// With count given (the binning's cell ids and counts are current, dir
+// given too), the parent's count moves to its new cell and the child is
+// counted in its own; a parent or child that leaves the domain is binned by
+// the haloswap once shifted (k_swap_bin_m).
+__device__ __forceinline__ int32_t split_cell_m(const Geom& g, const CellOff* p, int d) {
+  if (d != 0 || p[2].i < 0 || p[2].i >= g.Nz || !(p[0].f >= 0.f && p[0].f <= 1.f) || !(p[1].f >= 0.f && p[1].f <= 1.f) ||
+      !(p[2].f >= 0.f && p[2].f <= 1.f))
+    return -1;
+  return (int32_t)(((int64_t)p[0].i * g.Ny + p[1].i) * g.Nz + p[2].i);
+}
 __global__ void k_split_apply_m(Geom g, int64_t n, const int32_t* __restrict__ list, const int32_t* __restrict__ nsplit,
-                                double* __restrict__ parcels, int64_t cap, DevInfo* info, int8_t* __restrict__ dir) {
+                                double* __restrict__ parcels, int64_t cap, DevInfo* info, int8_t* __restrict__ dir,
+                                int32_t* __restrict__ cell, int32_t* __restrict__ count) {
   const int ns = *nsplit;
   const float pi = 3.14159265358979f;
   const float inv[3] = {(float)(1.0 / g.dx), (float)(1.0 / g.dy), (float)(1.0 / g.dz)};
@@ -965,8 +986,18 @@ __global__ void k_split_apply_m(Geom g, int64_t n, const int32_t* __restrict__ l
     if (dir) {  // reflected and classified here (k_split_apply)
       pc[2] = co_reflect(pc[2], g.Nz);
       pi_[2] = co_reflect(pi_[2], g.Nz);
-      dir[c] = (int8_t)classify_dir_m(g, pc[0].i, pc[1].i);
-      dir[i] = (int8_t)classify_dir_m(g, pi_[0].i, pi_[1].i);
+      const int dc = classify_dir_m(g, pc[0].i, pc[1].i), di = classify_dir_m(g, pi_[0].i, pi_[1].i);
+      dir[c] = (int8_t)dc;
+      dir[i] = (int8_t)di;
+      if (count) {
+        const int32_t old = cell[i], ni = split_cell_m(g, pi_, di), nc = split_cell_m(g, pc, dc);
+        if (old >= 0) atomicSub(&count[old], 1);
+        if (ni >= 0) atomicAdd(&count[ni], 1);
+        if (nc >= 0) atomicAdd(&count[nc], 1);
+        if ((ni < 0 && di == 0) || (nc < 0 && dc == 0)) atomicCAS(&info->error, 0, PMPIC_ERR_OUT_OF_BOX);
+        cell[i] = ni;
+        cell[c] = nc;
+      }
     }
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
@@ -1266,8 +1297,13 @@ int rk4_stage(pmpic_ctx* ctx, int stage) {
     if (gu && gp) pack6<float>(ctx, P.grid, (float*)ctx->gpack);
     auto kern = gu ? (gp ? k_rk4_m<true, true> : k_rk4_m<true, false>) : (gp ? k_rk4_m<false, true> : k_rk4_m<false, false>);
     PMPIC_CUDA(cudaMemsetAsync(ctx->cell_count, 0, sizeof(int32_t) * (ctx->g.ncell + 1), ctx->stream));
+    // within pmpic_step the last stage also advances the stretch of the split
+    // that follows (the haloswap in between moves it with its parcel)
+    const bool adv = ctx->split_follows && stage == 4;
     kern<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, P, stage, &ctx->dinfo->dtm, ctx->dir, ctx->cell,
-                                                     ctx->cell_count, ctx->dinfo); ++ctx->nlaunch;
+                                                     ctx->cell_count, ctx->dinfo,
+                                                     adv ? propf(ctx, PMPIC_PROP_STRETCH) : nullptr); ++ctx->nlaunch;
+    ctx->stretch_advanced = adv;
     ctx->pending_uvw = ctx->pending_pqr = false;
     ctx->dir_ready = true;
     ctx->sorted_valid = false;
@@ -1368,13 +1404,21 @@ int splitting(pmpic_ctx* ctx) {
   int32_t* flag = ctx->aux;
   int32_t* list = ctx->keep;
   int32_t* ns = dcounter(ctx, 2);
+  const bool advanced = ctx->stretch_advanced;
+  ctx->stretch_advanced = false;
+  bool split_counted = false;
   if (n > 0) {
-    if (ctx->mixed)
-      k_split_flag_m<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, ctx->parcels, ctx->cap, &ctx->dinfo->dtm, flag);
-    else
-      k_split_flag<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, ctx->parcels, ctx->cap, &ctx->dinfo->dtm, flag);
-    ++ctx->nlaunch;
-    int rc = compact(ctx, PredFlag{flag}, n, list, ns);
+    int rc;
+    if (advanced) {  // the RK4 stage advanced the stretch: only the criterion is left
+      rc = compact(ctx, PredStretchM{propf(ctx, PMPIC_PROP_STRETCH)}, n, list, ns);
+    } else {
+      if (ctx->mixed)
+        k_split_flag_m<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, ctx->parcels, ctx->cap, &ctx->dinfo->dtm, flag);
+      else
+        k_split_flag<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, ctx->parcels, ctx->cap, &ctx->dinfo->dtm, flag);
+      ++ctx->nlaunch;
+      rc = compact(ctx, PredFlag{flag}, n, list, ns);
+    }
     if (rc) return rc;
     // after a haloswap only the split parcels can be outside the domain: the
     // haloswap that follows needs no pass over all parcels to find them
@@ -1383,12 +1427,17 @@ int splitting(pmpic_ctx* ctx) {
       PMPIC_CUDA(cudaMemsetAsync(ctx->dir, 0, (size_t)n, ctx->stream));
       dsplit = ctx->dir;
     }
+    // on the mixed form the binning counts stay current through the split
+    const bool keep_counts = ctx->mixed && dsplit && ctx->count_ready;
     if (ctx->mixed)
-      k_split_apply_m<<<592, 256, 0, ctx->stream>>>(ctx->g, n, list, ns, ctx->parcels, ctx->cap, ctx->dinfo, dsplit);
+      k_split_apply_m<<<592, 256, 0, ctx->stream>>>(ctx->g, n, list, ns, ctx->parcels, ctx->cap, ctx->dinfo, dsplit,
+                                                    keep_counts ? ctx->cell : nullptr,
+                                                    keep_counts ? ctx->cell_count : nullptr);
     else
       k_split_apply<<<592, 256, 0, ctx->stream>>>(ctx->g, n, list, ns, ctx->parcels, ctx->cap, ctx->dinfo, dsplit);
     ++ctx->nlaunch;
     ctx->dir_ready = dsplit != nullptr;
+    split_counted = keep_counts;
   } else {
     PMPIC_CUDA(cudaMemsetAsync(ns, 0, sizeof(int32_t), ctx->stream));
   }
@@ -1396,7 +1445,7 @@ int splitting(pmpic_ctx* ctx) {
   PMPIC_CUDA(cudaMemcpyAsync(&hns, ns, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
   PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
   int64_t nn = n + hns;
-  ctx->count_ready = false;  // split parents moved and children were added uncounted
+  ctx->count_ready = split_counted;  // else split parents moved and children were added uncounted
   if (nn > ctx->cap) return set_error(ctx, PMPIC_ERR_CAPACITY, "maxparcels reached (parcel splitting)");
   ctx->n = nn;
   ctx->info.n_split = hns;
