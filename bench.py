@@ -164,29 +164,31 @@ def algorithmic_bytes(kernel, precision, n_avg, nphys, calls, steps):
 
     par2grid (per launch, one field set): offsets, vol and the fields of every
       parcel, its sorted index, and the NQ grids written.  Per step: four
-      vort2vel passes (p, q, r, btot; the FP64 path stages b, h, z for btot),
-      the mixing kept class and, when any parcel is removed, the removed class
-      (6 sums over b, h, p, q, r).
+      vort2vel passes (p, q, r and btot from b, h, z, the btot property
+      written back), the mixing kept class and, when any parcel is removed,
+      the removed class (6 sums over b, h, p, q, r).
     rk4_kernel (per stage): the RK4 state it must read and write (x, y, z, p,
       q, r and their xo/xf copies, the six tendencies, the direction byte),
       the binning it gathers at (FP64: cell id + 3 offsets), and the six grids
       read once.  Stage 1 reads x, writes xo, xf, x; stages 2-3 read xo, xf,
-      write xf, x; stage 4 reads xf, writes xf, x.
+      write xf, x; stage 4 reads xf, writes xf, x.  The mixed form also writes
+      the next binning's cell id, and its last stage advances the stretch of
+      the split that follows (read + write).
     """
     w = 8 if precision == "fp64" else 4
     if kernel == "par2grid":
         if precision == "fp64":
-            b0, b1 = 84.0, 76.0   # 3 del + vol + p,q,r + b,h,z (+4 index); 3 del + vol + b,h,p,q,r
+            b0, b1 = 92.0, 76.0   # 3 del + vol + p,q,r + b,h,z + btot out (+4 index); 3 del + vol + b,h,p,q,r
         else:
-            b0, b1 = 36.0, 40.0   # 3 offsets + vol + p,q,r,btot (+4); 3 offsets + vol + b,h,p,q,r
+            b0, b1 = 48.0, 40.0   # 3 offsets + vol + p,q,r + b,h + z cell + btot out (+4); 3 offsets + vol + b,h,p,q,r
         per_step = 4 * (b0 * n_avg + 4 * w * nphys) + (b1 * n_avg + 6 * w * nphys)
         extra = max(calls - 5 * steps, 0) * (b1 * n_avg + 6 * w * nphys)
         return per_step * steps + extra
     if kernel == "rk4_kernel":
         if precision == "fp64":
             st = [76 + 193, 124 + 145, 124 + 145, 76 + 145]
-        else:  # positions: int cell + FP32 offset (8 B), the rest FP32
-            st = [36 + 133, 96 + 97, 96 + 97, 60 + 97]
+        else:  # positions: int cell + FP32 offset (8 B), the rest FP32; + cell id out; stage 4: stretch
+            st = [36 + 137, 96 + 101, 96 + 101, 64 + 105]
         return steps * sum(s_ * n_avg + 6 * w * nphys for s_ in st)
     return None
 
