@@ -199,6 +199,7 @@ struct pmpic_ctx {
   int32_t* cell;             // cap: interior cell id per slot, z fastest: (i*Ny + j)*Nz + k
   double* del;               // 3 x cap: cached delx, dely, delz per slot
   bool sorted_valid;         // cell ids, offsets and cell lists match the current positions
+  bool in_step;              // inside pmpic_step: no caller code runs between the callbacks
   bool split_follows;        // pmpic_step: a split that acts follows this RK4 stage
   bool stretch_advanced;     // mixed form: the last RK4 stage advanced the stretch property
                              // (parcel_splitting.F90:64-73) for the split that follows

@@ -229,7 +229,7 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   ctx->in_domain = false;
   ctx->btot_grid_ready = false;
   ctx->pending_uvw = ctx->pending_pqr = ctx->dir_ready = false;
-  ctx->split_follows = ctx->stretch_advanced = false;
+  ctx->split_follows = ctx->stretch_advanced = ctx->in_step = false;
   ctx->nbmax = (std::max<int64_t>(ctx->cap, g.ncell) + 1023) / 1024 + 8;
   int64_t sc = 2LL * (g.Nx + g.Ny) * (int64_t)g.nzp * 32;
   ctx->swapcap = std::min<int64_t>(ctx->cap, std::max<int64_t>(1 << 20, sc));
@@ -755,10 +755,14 @@ int pmpic_step(pmpic_ctx* ctx, int nsteps) {
       int rc;
       if ((rc = do_vort2vel(ctx))) return rc;
       if ((rc = do_vorticity_tendency(ctx))) return rc;
-      // the last stage of a step can advance the stretch for the split that follows
+      // the last stage of a step can advance the stretch for the split that
+      // follows; the earlier stages' tendencies are dead (store_tendencies)
       ctx->split_follows = ctx->counters[3] % 4 == 3;
+      // another stage follows within this call, with no split in between
+      ctx->in_step = ctx->counters[2] < 4 && !ctx->split_follows && !(s == nsteps - 1 && sub == 3);
       rc = do_rk4(ctx);
       ctx->split_follows = false;
+      ctx->in_step = false;
       if (rc) return rc;
       if ((rc = do_split(ctx))) return rc;
       if ((rc = do_mix(ctx))) return rc;

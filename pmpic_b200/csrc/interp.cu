@@ -293,7 +293,7 @@ __device__ __forceinline__ float madd(float w, float f, float acc) { return __fm
 // DZ[ds * n]: the cached binning (ds = 1) or the offset half of the mixed
 // form's {cell index, offset} positions (ds = 2).
 template <int NQ, int MODE, bool BT, class R = double>
-__global__ void __launch_bounds__(32 * RW, sizeof(R) == 4 ? 6 : 1) k_p2g_rows(Geom g, int nzc, int nxs, int xseg, const int32_t* __restrict__ start,
+__global__ void __launch_bounds__(32 * RW, sizeof(R) == 4 ? 6 : 4) k_p2g_rows(Geom g, int nzc, int nxs, int xseg, const int32_t* __restrict__ start,
                                                      const int32_t* __restrict__ sorted, const R* __restrict__ DX,
                                                      const R* __restrict__ DY, const R* __restrict__ DZ, int ds,
                                                      const R* __restrict__ VOL, P2GArgs<NQ, R> a,

@@ -249,7 +249,7 @@ __device__ __forceinline__ int classify_dir(const Geom& g, double x, double y) {
 template <bool GU, bool GP>
 __global__ void __launch_bounds__(256, 4) k_rk4(Geom g, int64_t n, RkPtrs P, int stage, const double* __restrict__ dtp,
                       const int32_t* __restrict__ cell, const double* __restrict__ del, int64_t cap,
-                      int8_t* __restrict__ dir) {
+                      int8_t* __restrict__ dir, int store_d) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const double dt = *dtp;  // state%dtm (rk4_integrator.F90:102)
@@ -316,7 +316,7 @@ __global__ void __launch_bounds__(256, 4) k_rk4(Geom g, int64_t n, RkPtrs P, int
   snew[2] = z;
 #pragma unroll
   for (int v = 0; v < 6; ++v) {
-    if (gathered && ((v < 3 && GU) || (v >= 3 && GP))) P.d[v][t] = d[v];
+    if (store_d && gathered && ((v < 3 && GU) || (v >= 3 && GP))) P.d[v][t] = d[v];
     if (stage == 1) P.o[v][t] = ov[v];
     P.f[v][t] = fv[v];
     P.s[v][t] = snew[v];
@@ -745,7 +745,7 @@ __device__ __forceinline__ int classify_dir_m(const Geom& g, int i, int j) {
 template <bool GU, bool GP>
 __global__ void __launch_bounds__(256, 5) k_rk4_m(Geom g, int64_t n, MPtrs P, int stage, const double* __restrict__ dtp,
                         int8_t* __restrict__ dir, int32_t* __restrict__ cell, int32_t* __restrict__ count,
-                        DevInfo* info, float* __restrict__ stretch) {
+                        DevInfo* info, float* __restrict__ stretch, int store_d) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const float dt = (float)*dtp;  // state%dtm (rk4_integrator.F90:102)
@@ -823,7 +823,7 @@ __global__ void __launch_bounds__(256, 5) k_rk4_m(Geom g, int64_t n, MPtrs P, in
   }
 #pragma unroll
   for (int v = 0; v < 6; ++v)
-    if (gathered && ((v < 3 && GU) || (v >= 3 && GP))) P.d[v][t] = d[v];
+    if (store_d && gathered && ((v < 3 && GU) || (v >= 3 && GP))) P.d[v][t] = d[v];
 #pragma unroll
   for (int v = 0; v < 3; ++v) {
     if (stage == 1) {
@@ -1264,6 +1264,14 @@ int compute_btot(pmpic_ctx* ctx) {
   return 0;
 }
 
+// Whether the stage kernel stores the gathered tendencies (dxdt .. drdt).
+// Within pmpic_step, when another stage follows in the same call with no split
+// in between, they are dead: the next stage gathers them afresh before
+// anything reads them, and no caller code runs in between.  Otherwise (the
+// last stage, a split following, components called one at a time) they are
+// stored.
+static int store_tendencies(const pmpic_ctx* ctx, int stage) { return ctx->in_step && stage < 4 ? 0 : 1; }
+
 int rk4_stage(pmpic_ctx* ctx, int stage) {
   if (ctx->n == 0) {
     ctx->pending_uvw = ctx->pending_pqr = false;
@@ -1302,7 +1310,8 @@ int rk4_stage(pmpic_ctx* ctx, int stage) {
     const bool adv = ctx->split_follows && stage == 4;
     kern<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, P, stage, &ctx->dinfo->dtm, ctx->dir, ctx->cell,
                                                      ctx->cell_count, ctx->dinfo,
-                                                     adv ? propf(ctx, PMPIC_PROP_STRETCH) : nullptr); ++ctx->nlaunch;
+                                                     adv ? propf(ctx, PMPIC_PROP_STRETCH) : nullptr,
+                                                     store_tendencies(ctx, stage)); ++ctx->nlaunch;
     ctx->stretch_advanced = adv;
     ctx->pending_uvw = ctx->pending_pqr = false;
     ctx->dir_ready = true;
@@ -1335,7 +1344,7 @@ int rk4_stage(pmpic_ctx* ctx, int stage) {
   // divisions per parcel cost the HBM-bound stage kernel more than the
   // position reads they would save
   kern<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, P, stage, &ctx->dinfo->dtm, ctx->cell, ctx->del,
-                                                   ctx->cap, ctx->dir); ++ctx->nlaunch;
+                                                   ctx->cap, ctx->dir, store_tendencies(ctx, stage)); ++ctx->nlaunch;
   ctx->pending_uvw = ctx->pending_pqr = false;
   ctx->dir_ready = true;  // z reflected and directions classified
   ctx->sorted_valid = false;
