@@ -31,8 +31,6 @@ namespace pmpic {
 
 namespace {
 
-constexpr int MAXSEG = 32;            // cell segments sorted in registers
-
 inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
 // ---- binning (cache_parcel_interp_weights, parcel_interpolation.F90:186-262) ----
@@ -74,48 +72,64 @@ __global__ void k_bin_count_m(Geom g, int64_t n, const CellOff* __restrict__ X, 
   count_cell(id, count);
 }
 
-__global__ void k_bin_scatter(int64_t n, const int32_t* __restrict__ cell, const int32_t* __restrict__ start,
-                              int32_t* __restrict__ fill, int32_t* __restrict__ sorted) {
-  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  int32_t id = cell[t];
-  if (id < 0) return;
-  // one atomic per distinct cell of the warp; lanes take consecutive places in
-  // lane order (the segment is sorted by slot afterwards in any case)
-  const unsigned act = __activemask();
-  const unsigned same = __match_any_sync(act, id);
+// Slots into their cells' ranges.  Each thread takes SC_ITEMS slots (a block's
+// slots are SC_ITEMS runs of 256) and issues all their fill atomics before it
+// uses any result, so their round trips overlap.  One atomic per distinct cell
+// of a warp; lanes take consecutive places in lane order (each segment is
+// sorted by slot afterwards in any case).
+constexpr int SC_ITEMS = 4;
+__global__ void __launch_bounds__(256) k_bin_scatter(int64_t n, const int32_t* __restrict__ cell,
+                                                     const int32_t* __restrict__ start, int32_t* __restrict__ fill,
+                                                     int32_t* __restrict__ sorted) {
+  constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  const int leader = __ffs(same) - 1;
-  int32_t base = 0;
-  if (lane == leader) base = atomicAdd(&fill[id], __popc(same));
-  base = __shfl_sync(same, base, leader);
-  const int32_t pos = start[id] + base + __popc(same & ((1u << lane) - 1));
-  sorted[pos] = (int32_t)t;
+  const int64_t t0 = (int64_t)blockIdx.x * 256 * SC_ITEMS + threadIdx.x;
+  int32_t id[SC_ITEMS], base[SC_ITEMS], st[SC_ITEMS];
+  unsigned same[SC_ITEMS];
+#pragma unroll
+  for (int k = 0; k < SC_ITEMS; ++k) {
+    const int64_t t = t0 + 256 * k;
+    id[k] = t < n ? cell[t] : -1;
+  }
+#pragma unroll
+  for (int k = 0; k < SC_ITEMS; ++k) {
+    same[k] = __match_any_sync(FULL, id[k]);
+    base[k] = 0;
+    st[k] = 0;
+    if (id[k] >= 0) {
+      if (lane == __ffs(same[k]) - 1) base[k] = atomicAdd(&fill[id[k]], __popc(same[k]));
+      st[k] = start[id[k]];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < SC_ITEMS; ++k) {
+    const int32_t b = __shfl_sync(FULL, base[k], __ffs(same[k]) - 1);
+    if (id[k] >= 0) sorted[st[k] + b + __popc(same[k] & ((1u << lane) - 1))] = (int32_t)(t0 + 256 * k);
+  }
 }
 
-// each cell's segment sorted by slot index (integer atomics above only decide
-// the order inside a cell)
-__global__ void k_sort_segments(int64_t ncell, const int32_t* __restrict__ start, int32_t* __restrict__ sorted) {
-  int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncell) return;
-  int s0 = start[c], len = start[c + 1] - s0;
-  if (len < 2) return;
-  int32_t* s = sorted + s0;
-  if (len <= MAXSEG) {
-    int loc[MAXSEG];
-    for (int u = 0; u < len; ++u) {
-      int v = s[u];
-      int w = u - 1;
-      while (w >= 0 && loc[w] > v) {
-        loc[w + 1] = loc[w];
-        --w;
-      }
-      loc[w + 1] = v;
-    }
-    for (int u = 0; u < len; ++u) s[u] = loc[u];
-  } else {  // rare long segment: insertion sort in place
+// Each cell's segment sorted by slot index (the integer atomics above only
+// decide the order inside a cell).  A CTA takes SORT_CELLS consecutive cells,
+// whose segments are one contiguous range of the index: it is read into shared
+// memory with coalesced loads, every thread insertion-sorts its cell's segment
+// there (the slots are nearly in order already), and the range is written back.
+constexpr int SORT_CELLS = 256;
+constexpr int SORT_CAP = 8192;  // index entries a CTA stages (32 KB)
+__global__ void __launch_bounds__(SORT_CELLS) k_sort_segments(int64_t ncell, const int32_t* __restrict__ start,
+                                                              int32_t* __restrict__ sorted) {
+  __shared__ int32_t buf[SORT_CAP];
+  const int64_t c0 = (int64_t)blockIdx.x * SORT_CELLS;
+  const int64_t c = c0 + threadIdx.x;
+  const int64_t c1 = min(c0 + SORT_CELLS, ncell);
+  const int base = start[c0], m = start[c1] - base;
+  int s0 = 0, len = 0;
+  if (c < ncell) {
+    s0 = start[c] - base;
+    len = start[c + 1] - base - s0;
+  }
+  auto isort = [](int32_t* s, int len) {
     for (int u = 1; u < len; ++u) {
-      int v = s[u];
+      const int32_t v = s[u];
       int w = u - 1;
       while (w >= 0 && s[w] > v) {
         s[w + 1] = s[w];
@@ -123,6 +137,15 @@ __global__ void k_sort_segments(int64_t ncell, const int32_t* __restrict__ start
       }
       s[w + 1] = v;
     }
+  };
+  if (m <= SORT_CAP) {  // uniform over the CTA
+    for (int e = threadIdx.x; e < m; e += SORT_CELLS) buf[e] = sorted[base + e];
+    __syncthreads();
+    isort(buf + s0, len);
+    __syncthreads();
+    for (int e = threadIdx.x; e < m; e += SORT_CELLS) sorted[base + e] = buf[e];
+  } else {  // cells holding more than SORT_CAP parcels together: in place in global memory
+    isort(sorted + base + s0, len);
   }
 }
 
@@ -668,9 +691,9 @@ int bin_and_sort(pmpic_ctx* ctx) {
   int rc = scan_excl(ctx, ctx->cell_count, g.ncell, ctx->cell_start);
   if (rc) return rc;
   if (n > 0) {
-    k_bin_scatter<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, ctx->cell, ctx->cell_start, ctx->cell_fill,
-                                                         ctx->sorted); ++ctx->nlaunch;
-    k_sort_segments<<<nblk(g.ncell, 256), 256, 0, ctx->stream>>>(g.ncell, ctx->cell_start, ctx->sorted);
+    k_bin_scatter<<<nblk(n, 256 * SC_ITEMS), 256, 0, ctx->stream>>>(n, ctx->cell, ctx->cell_start, ctx->cell_fill,
+                                                                    ctx->sorted); ++ctx->nlaunch;
+    k_sort_segments<<<nblk(g.ncell, SORT_CELLS), SORT_CELLS, 0, ctx->stream>>>(g.ncell, ctx->cell_start, ctx->sorted);
     ++ctx->nlaunch;
   }
   PMPIC_CUDA(cudaGetLastError());
@@ -1017,8 +1040,8 @@ extern "C" int pmpic_par2grid_static(int32_t nx, int32_t ny, int32_t nz, double 
   k_scan_sums<<<1, SCAN_BLOCK, 0, st>>>(tiles, ntiles, cstart + ncell);
   k_scan_apply<<<(unsigned)ntiles, SCAN_BLOCK, 0, st>>>(count, ncell, tiles, cstart);
   if (n > 0) {
-    k_bin_scatter<<<nblk(n, 256), 256, 0, st>>>(n, cell, cstart, fill, sorted);
-    k_sort_segments<<<nblk(ncell, 256), 256, 0, st>>>(ncell, cstart, sorted);
+    k_bin_scatter<<<nblk(n, 256 * SC_ITEMS), 256, 0, st>>>(n, cell, cstart, fill, sorted);
+    k_sort_segments<<<nblk(ncell, SORT_CELLS), SORT_CELLS, 0, st>>>(ncell, cstart, sorted);
   }
   P2GArgs<1> a{};
   a.f[0] = field;
