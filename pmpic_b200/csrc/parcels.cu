@@ -27,6 +27,13 @@ inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 // lane), which is ascending item order.
 constexpr int CCH = 32;              // chunks per CTA
 constexpr int CITEMS = 256 * CCH;    // items per CTA
+// the per-CTA counts of k_count for a direction array, accumulated by the
+// kernels that classify (one ballot per warp, an atomic only where a warp
+// holds a mover; a warp's items lie in one CTA range)
+__device__ __forceinline__ void count_mover(int64_t t, bool moves, int32_t* __restrict__ blockcnt) {
+  const unsigned b = __ballot_sync(__activemask(), moves);
+  if (b && (threadIdx.x & 31) == __ffs(__activemask()) - 1) atomicAdd(&blockcnt[t / CITEMS], __popc(b));
+}
 template <class Pred>
 __global__ void __launch_bounds__(256) k_count(Pred pr, int64_t n, int32_t* __restrict__ blockcnt) {
   __shared__ int ws[8];
@@ -51,6 +58,9 @@ template <class Pred>
 __global__ void __launch_bounds__(256) k_write(Pred pr, int64_t n, const int32_t* __restrict__ blockoff,
                                                int32_t* __restrict__ list) {
   __shared__ int wc[CCH * 8];  // per (chunk, warp): count, then exclusive offset within the CTA
+  // the lists are sparse (movers, splits, removals, under-populated cells):
+  // a CTA whose range holds none leaves at once (blockoff has nb + 1 entries)
+  if (blockoff[blockIdx.x + 1] == blockoff[blockIdx.x]) return;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t base = (int64_t)blockIdx.x * CITEMS + threadIdx.x;
   uint32_t mask = 0;
@@ -249,7 +259,7 @@ __device__ __forceinline__ int classify_dir(const Geom& g, double x, double y) {
 template <bool GU, bool GP>
 __global__ void __launch_bounds__(256, 4) k_rk4(Geom g, int64_t n, RkPtrs P, int stage, const double* __restrict__ dtp,
                       const int32_t* __restrict__ cell, const double* __restrict__ del, int64_t cap,
-                      int8_t* __restrict__ dir, int store_d) {
+                      int8_t* __restrict__ dir, int store_d, int32_t* __restrict__ dircnt) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const double dt = *dtp;  // state%dtm (rk4_integrator.F90:102)
@@ -321,7 +331,9 @@ __global__ void __launch_bounds__(256, 4) k_rk4(Geom g, int64_t n, RkPtrs P, int
     P.f[v][t] = fv[v];
     P.s[v][t] = snew[v];
   }
-  dir[t] = (int8_t)classify_dir(g, snew[0], snew[1]);
+  const int dr = classify_dir(g, snew[0], snew[1]);
+  dir[t] = (int8_t)dr;
+  count_mover(t, dr != 0, dircnt);
 }
 
 // ---- parcel haloswap (parcels/haloswap.F90:109-289, one rank) -------------------------
@@ -463,7 +475,8 @@ __global__ void k_split_flag(int64_t n, double* __restrict__ parcels, int64_t ca
 // parent and the child are reflected at the walls and classified here, as the
 // parcel haloswap that follows (:134) would do for them.
 __global__ void k_split_apply(Geom g, int64_t n, const int32_t* __restrict__ list, const int32_t* __restrict__ nsplit,
-                              double* __restrict__ parcels, int64_t cap, DevInfo* info, int8_t* __restrict__ dir) {
+                              double* __restrict__ parcels, int64_t cap, DevInfo* info, int8_t* __restrict__ dir,
+                              int32_t* __restrict__ dircnt) {
   const int ns = *nsplit;
   const double pi = 4. * atan(1.0);
   const double third = f4div(1.f, 3.f);
@@ -513,7 +526,9 @@ __global__ void k_split_apply(Geom g, int64_t n, const int32_t* __restrict__ lis
         const double zz = A(PMPIC_PROP_Z)[m];
         if (zz < g.pzmin) A(PMPIC_PROP_Z)[m] = g.pzmin + (g.pzmin - zz);
         else if (zz > g.pzmax) A(PMPIC_PROP_Z)[m] = g.pzmax - (zz - g.pzmax);
-        dir[m] = (int8_t)classify_dir(g, A(PMPIC_PROP_X)[m], A(PMPIC_PROP_Y)[m]);
+        const int dr = classify_dir(g, A(PMPIC_PROP_X)[m], A(PMPIC_PROP_Y)[m]);
+        dir[m] = (int8_t)dr;
+        if (dr) atomicAdd(&dircnt[m / CITEMS], 1);
       }
     }
   }
@@ -745,7 +760,7 @@ __device__ __forceinline__ int classify_dir_m(const Geom& g, int i, int j) {
 template <bool GU, bool GP>
 __global__ void __launch_bounds__(256, 5) k_rk4_m(Geom g, int64_t n, MPtrs P, int stage, const double* __restrict__ dtp,
                         int8_t* __restrict__ dir, int32_t* __restrict__ cell, int32_t* __restrict__ count,
-                        DevInfo* info, float* __restrict__ stretch, int store_d) {
+                        DevInfo* info, float* __restrict__ stretch, int store_d, int32_t* __restrict__ dircnt) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const float dt = (float)*dtp;  // state%dtm (rk4_integrator.F90:102)
@@ -837,6 +852,7 @@ __global__ void __launch_bounds__(256, 5) k_rk4_m(Geom g, int64_t n, MPtrs P, in
   }
   const int dr = classify_dir_m(g, sn[0].i, sn[1].i);
   dir[t] = (int8_t)dr;
+  count_mover(t, dr != 0, dircnt);
   // the next binning of the new position, with the per-cell count (parcels
   // crossing a periodic boundary are binned by the haloswap once shifted)
   int32_t nid = -1;
@@ -953,7 +969,7 @@ __device__ __forceinline__ int32_t split_cell_m(const Geom& g, const CellOff* p,
 }
 __global__ void k_split_apply_m(Geom g, int64_t n, const int32_t* __restrict__ list, const int32_t* __restrict__ nsplit,
                                 double* __restrict__ parcels, int64_t cap, DevInfo* info, int8_t* __restrict__ dir,
-                                int32_t* __restrict__ cell, int32_t* __restrict__ count) {
+                                int32_t* __restrict__ dircnt, int32_t* __restrict__ cell, int32_t* __restrict__ count) {
   const int ns = *nsplit;
   const float pi = 3.14159265358979f;
   const float inv[3] = {(float)(1.0 / g.dx), (float)(1.0 / g.dy), (float)(1.0 / g.dz)};
@@ -989,6 +1005,8 @@ __global__ void k_split_apply_m(Geom g, int64_t n, const int32_t* __restrict__ l
       const int dc = classify_dir_m(g, pc[0].i, pc[1].i), di = classify_dir_m(g, pi_[0].i, pi_[1].i);
       dir[c] = (int8_t)dc;
       dir[i] = (int8_t)di;
+      if (dc) atomicAdd(&dircnt[c / CITEMS], 1);
+      if (di) atomicAdd(&dircnt[i / CITEMS], 1);
       if (count) {
         const int32_t old = cell[i], ni = split_cell_m(g, pi_, di), nc = split_cell_m(g, pc, dc);
         if (old >= 0) atomicSub(&count[old], 1);
@@ -1207,6 +1225,25 @@ static int compact(pmpic_ctx* ctx, Pred pr, int64_t n, int32_t* list, int32_t* d
   return 0;
 }
 
+// the same with the per-CTA counts already in ctx->aux2 (written by the
+// kernel that computed the predicate's input)
+template <class Pred>
+static int compact_counted(pmpic_ctx* ctx, Pred pr, int64_t n, int32_t* list, int32_t* dcount) {
+  int64_t nb = (n + CITEMS - 1) / CITEMS;
+  if (nb == 0) {
+    PMPIC_CUDA(cudaMemsetAsync(dcount, 0, sizeof(int32_t), ctx->stream));
+    return 0;
+  }
+  int32_t* cnt = ctx->aux2;
+  int32_t* off = ctx->aux2 + ctx->nbmax;
+  int rc = scan_excl(ctx, cnt, nb, off);
+  if (rc) return rc;
+  k_write<<<(unsigned)nb, 256, 0, ctx->stream>>>(pr, n, off, list); ++ctx->nlaunch;
+  PMPIC_CUDA(cudaMemcpyAsync(dcount, off + nb, sizeof(int32_t), cudaMemcpyDeviceToDevice, ctx->stream));
+  PMPIC_CUDA(cudaGetLastError());
+  return 0;
+}
+
 // small device counters live after the DevInfo block
 static int32_t* dcounter(pmpic_ctx* ctx, int i) { return (int32_t*)(ctx->dinfo + 1) + i; }
 
@@ -1305,13 +1342,14 @@ int rk4_stage(pmpic_ctx* ctx, int stage) {
     if (gu && gp) pack6<float>(ctx, P.grid, (float*)ctx->gpack);
     auto kern = gu ? (gp ? k_rk4_m<true, true> : k_rk4_m<true, false>) : (gp ? k_rk4_m<false, true> : k_rk4_m<false, false>);
     PMPIC_CUDA(cudaMemsetAsync(ctx->cell_count, 0, sizeof(int32_t) * (ctx->g.ncell + 1), ctx->stream));
+    PMPIC_CUDA(cudaMemsetAsync(ctx->aux2, 0, sizeof(int32_t) * ctx->nbmax, ctx->stream));  // mover counts
     // within pmpic_step the last stage also advances the stretch of the split
     // that follows (the haloswap in between moves it with its parcel)
     const bool adv = ctx->split_follows && stage == 4;
     kern<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, P, stage, &ctx->dinfo->dtm, ctx->dir, ctx->cell,
                                                      ctx->cell_count, ctx->dinfo,
                                                      adv ? propf(ctx, PMPIC_PROP_STRETCH) : nullptr,
-                                                     store_tendencies(ctx, stage)); ++ctx->nlaunch;
+                                                     store_tendencies(ctx, stage), ctx->aux2); ++ctx->nlaunch;
     ctx->stretch_advanced = adv;
     ctx->pending_uvw = ctx->pending_pqr = false;
     ctx->dir_ready = true;
@@ -1343,8 +1381,9 @@ int rk4_stage(pmpic_ctx* ctx, int stage) {
   // the next binning stays a separate pass on this path: its six IEEE
   // divisions per parcel cost the HBM-bound stage kernel more than the
   // position reads they would save
+  PMPIC_CUDA(cudaMemsetAsync(ctx->aux2, 0, sizeof(int32_t) * ctx->nbmax, ctx->stream));  // mover counts
   kern<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, P, stage, &ctx->dinfo->dtm, ctx->cell, ctx->del,
-                                                   ctx->cap, ctx->dir, store_tendencies(ctx, stage)); ++ctx->nlaunch;
+                                                   ctx->cap, ctx->dir, store_tendencies(ctx, stage), ctx->aux2); ++ctx->nlaunch;
   ctx->pending_uvw = ctx->pending_pqr = false;
   ctx->dir_ready = true;  // z reflected and directions classified
   ctx->sorted_valid = false;
@@ -1383,7 +1422,8 @@ int parcel_haloswap(pmpic_ctx* ctx) {
   int32_t* V = ctx->aux;                 // vacated slots, ascending
   int32_t* M = ctx->keep;                // moved parcels in send order (keep is free outside mixing)
   int32_t* nm = dcounter(ctx, 0);
-  int rc = compact(ctx, PredDirNZ{ctx->dir}, n, V, nm);
+  // after an RK4 stage or a split, the kernel that classified counted the movers
+  int rc = ready ? compact_counted(ctx, PredDirNZ{ctx->dir}, n, V, nm) : compact(ctx, PredDirNZ{ctx->dir}, n, V, nm);
   if (rc) return rc;
   k_partition_dirs<<<1, 1024, 0, ctx->stream>>>(V, nm, ctx->dir, M); ++ctx->nlaunch;
   // the staging buffer is bounded: on overflow nothing moves and the call
@@ -1434,16 +1474,18 @@ int splitting(pmpic_ctx* ctx) {
     int8_t* dsplit = nullptr;
     if (ctx->in_domain) {
       PMPIC_CUDA(cudaMemsetAsync(ctx->dir, 0, (size_t)n, ctx->stream));
+      PMPIC_CUDA(cudaMemsetAsync(ctx->aux2, 0, sizeof(int32_t) * ctx->nbmax, ctx->stream));  // mover counts
       dsplit = ctx->dir;
     }
     // on the mixed form the binning counts stay current through the split
     const bool keep_counts = ctx->mixed && dsplit && ctx->count_ready;
     if (ctx->mixed)
       k_split_apply_m<<<592, 256, 0, ctx->stream>>>(ctx->g, n, list, ns, ctx->parcels, ctx->cap, ctx->dinfo, dsplit,
-                                                    keep_counts ? ctx->cell : nullptr,
+                                                    ctx->aux2, keep_counts ? ctx->cell : nullptr,
                                                     keep_counts ? ctx->cell_count : nullptr);
     else
-      k_split_apply<<<592, 256, 0, ctx->stream>>>(ctx->g, n, list, ns, ctx->parcels, ctx->cap, ctx->dinfo, dsplit);
+      k_split_apply<<<592, 256, 0, ctx->stream>>>(ctx->g, n, list, ns, ctx->parcels, ctx->cap, ctx->dinfo, dsplit,
+                                                  ctx->aux2);
     ++ctx->nlaunch;
     ctx->dir_ready = dsplit != nullptr;
     split_counted = keep_counts;
