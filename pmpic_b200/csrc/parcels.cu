@@ -140,7 +140,12 @@ struct PredNewCell {
 // repacks the six into G6[i][j][k][6] (z fastest, fields interleaved): a cell's
 // four xy corners then hold their two levels and six fields in 12 consecutive
 // values, and the cells of a warp (consecutive in z) share lines.
-constexpr int PK_T = 32;  // x extent of a tile
+// x extent of a tile: 64 values (256-byte row segments) on the FP32 form, 32
+// on the FP64 path (its tile would not fit the static shared memory)
+template <class R>
+struct PkT {
+  static constexpr int value = sizeof(R) == 4 ? 64 : 32;
+};
 constexpr int PK_K = 16;  // z extent of a tile
 template <class R, int NF>
 __global__ void __launch_bounds__(256) k_pack(Geom g, const R* __restrict__ G0, const R* __restrict__ G1,
@@ -148,6 +153,7 @@ __global__ void __launch_bounds__(256) k_pack(Geom g, const R* __restrict__ G0, 
                                               const R* __restrict__ G4, const R* __restrict__ G5,
                                               const R* __restrict__ G6, R* __restrict__ out) {
   // NF = 6: fields G0..G5; NF = 8: G0..G6 and a zero pad
+  constexpr int PK_T = PkT<R>::value;
   constexpr int TS = PK_K * (PK_T + 1) + 1;  // per-field tile stride, odd
   __shared__ R tile[NF * TS];
   const int i0 = blockIdx.x * PK_T, k0 = blockIdx.y * PK_K, j = blockIdx.z;
@@ -173,6 +179,7 @@ __global__ void __launch_bounds__(256) k_pack(Geom g, const R* __restrict__ G0, 
 template <class R>
 static void pack6(pmpic_ctx* ctx, const R* const* grids, R* out) {
   const Geom& g = ctx->g;
+  constexpr int PK_T = PkT<R>::value;
   dim3 gr((g.Nx + PK_T - 1) / PK_T, (g.nzp + PK_K - 1) / PK_K, g.Ny);
   k_pack<R, 6><<<gr, 256, 0, ctx->stream>>>(g, grids[0], grids[1], grids[2], grids[3], grids[4], grids[5], nullptr,
                                             out);
@@ -181,6 +188,7 @@ static void pack6(pmpic_ctx* ctx, const R* const* grids, R* out) {
 template <class R>
 static void pack8(pmpic_ctx* ctx, const R* const* grids, R* out) {  // 7 grids + a pad
   const Geom& g = ctx->g;
+  constexpr int PK_T = PkT<R>::value;
   dim3 gr((g.Nx + PK_T - 1) / PK_T, (g.nzp + PK_K - 1) / PK_K, g.Ny);
   k_pack<R, 8><<<gr, 256, 0, ctx->stream>>>(g, grids[0], grids[1], grids[2], grids[3], grids[4], grids[5], grids[6],
                                             out);
