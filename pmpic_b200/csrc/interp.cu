@@ -548,14 +548,16 @@ __global__ void __launch_bounds__(256) k_p2g_combine(Geom g, int nzc, const R* _
   const int pym = py == 0 ? g.Ny - 1 : py - 1;
   const int npx = min(PX, g.Nx - px0);
   const int k0 = zc * ZC, nk = min(ZC, g.Nz - k0);
-  // index spaces of compile-time widths: no runtime divisions per element
-  for (int e = threadIdx.x; e < 2 * PX * SEG; e += blockDim.x) {
-    const int r = e / (PX * SEG);
-    const int rem = e - r * PX * SEG;
-    const int pxl = rem / SEG, o = rem - pxl * SEG;
+  // one warp per (row, point) half-record, lanes along it: coalesced, and no
+  // index division per staged value
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int rp = warp; rp < 2 * PX; rp += blockDim.x >> 5) {
+    const int r = rp / PX, pxl = rp % PX;  // PX is a power of two
     if (pxl >= npx) continue;
     const int row = r == 0 ? py : pym;
-    T[r][pxl * TS + o] = rowpart[(((size_t)zc * g.Ny + row) * g.Nx + px0 + pxl) * RPS + r * SEG + o];
+    const R* src = rowpart + (((size_t)zc * g.Ny + row) * g.Nx + px0 + pxl) * RPS + r * SEG;
+    R* dst = &T[r][pxl * TS];
+    for (int o = lane; o < SEG; o += 32) dst[o] = src[o];
   }
   if (zc > 0) {
     for (int e = threadIdx.x; e < 2 * PX * NA; e += blockDim.x) {
