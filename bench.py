@@ -173,7 +173,8 @@ def algorithmic_bytes(kernel, precision, n_avg, nphys, calls, steps):
       read once.  Stage 1 reads x, writes xo, xf, x; stages 2-3 read xo, xf,
       write xf, x; stage 4 reads xf, writes xf, x.  The mixed form also writes
       the next binning's cell id, and its last stage advances the stretch of
-      the split that follows (read + write).
+      the split that follows (read + write).  Within pmpic_step stages 1-3
+      store no tendencies (dead until the next stage gathers them again).
     """
     w = 8 if precision == "fp64" else 4
     if kernel == "par2grid":
@@ -186,9 +187,9 @@ def algorithmic_bytes(kernel, precision, n_avg, nphys, calls, steps):
         return per_step * steps + extra
     if kernel == "rk4_kernel":
         if precision == "fp64":
-            st = [76 + 193, 124 + 145, 124 + 145, 76 + 145]
+            st = [76 + 145, 124 + 97, 124 + 97, 76 + 145]
         else:  # positions: int cell + FP32 offset (8 B), the rest FP32; + cell id out; stage 4: stretch
-            st = [36 + 137, 96 + 101, 96 + 101, 64 + 105]
+            st = [36 + 113, 96 + 77, 96 + 77, 64 + 105]
         return steps * sum(s_ * n_avg + 6 * w * nphys for s_ in st)
     return None
 
