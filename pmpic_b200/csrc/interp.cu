@@ -117,7 +117,9 @@ constexpr int SORT_CELLS = 256;
 constexpr int SORT_CAP = 8192;  // index entries a CTA stages (32 KB)
 __global__ void __launch_bounds__(SORT_CELLS) k_sort_segments(int64_t ncell, const int32_t* __restrict__ start,
                                                               int32_t* __restrict__ sorted) {
-  __shared__ int32_t buf[SORT_CAP];
+  // staged position e sits at e + e/8: segments (~8 parcels each) start in
+  // different banks for neighbouring threads
+  __shared__ int32_t buf[SORT_CAP + SORT_CAP / 8];
   const int64_t c0 = (int64_t)blockIdx.x * SORT_CELLS;
   const int64_t c = c0 + threadIdx.x;
   const int64_t c1 = min(c0 + SORT_CELLS, ncell);
@@ -127,25 +129,26 @@ __global__ void __launch_bounds__(SORT_CELLS) k_sort_segments(int64_t ncell, con
     s0 = start[c] - base;
     len = start[c + 1] - base - s0;
   }
-  auto isort = [](int32_t* s, int len) {
+  auto isort = [](int32_t* s, int s0, int len, auto at) {
     for (int u = 1; u < len; ++u) {
-      const int32_t v = s[u];
+      const int32_t v = s[at(s0 + u)];
       int w = u - 1;
-      while (w >= 0 && s[w] > v) {
-        s[w + 1] = s[w];
+      while (w >= 0 && s[at(s0 + w)] > v) {
+        s[at(s0 + w + 1)] = s[at(s0 + w)];
         --w;
       }
-      s[w + 1] = v;
+      s[at(s0 + w + 1)] = v;
     }
   };
+  auto skew = [](int e) { return e + (e >> 3); };
   if (m <= SORT_CAP) {  // uniform over the CTA
-    for (int e = threadIdx.x; e < m; e += SORT_CELLS) buf[e] = sorted[base + e];
+    for (int e = threadIdx.x; e < m; e += SORT_CELLS) buf[skew(e)] = sorted[base + e];
     __syncthreads();
-    isort(buf + s0, len);
+    isort(buf, s0, len, skew);
     __syncthreads();
-    for (int e = threadIdx.x; e < m; e += SORT_CELLS) sorted[base + e] = buf[e];
+    for (int e = threadIdx.x; e < m; e += SORT_CELLS) sorted[base + e] = buf[skew(e)];
   } else {  // cells holding more than SORT_CAP parcels together: in place in global memory
-    isort(sorted + base + s0, len);
+    isort(sorted + base, s0, len, [](int e) { return e; });
   }
 }
 

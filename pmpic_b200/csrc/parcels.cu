@@ -1139,7 +1139,7 @@ __global__ void k_residual_update_m(Geom g, ResPtrsF RP, const int32_t* __restri
     RP.r[q][e] = r;
   }
 }
-__global__ void __launch_bounds__(256, 4) k_redistribute_m(Geom g, int64_t norig, const int32_t* __restrict__ keep,
+__global__ void __launch_bounds__(256, 6) k_redistribute_m(Geom g, int64_t norig, const int32_t* __restrict__ keep,
                                                           double* __restrict__ parcels, int64_t cap,
                                                           const float* __restrict__ G8) {
   const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
