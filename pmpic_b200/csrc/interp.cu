@@ -78,9 +78,14 @@ __global__ void k_bin_count_m(Geom g, int64_t n, const CellOff* __restrict__ X, 
 // of a warp; lanes take consecutive places in lane order (each segment is
 // sorted by slot afterwards in any case).
 constexpr int SC_ITEMS = 4;
+// the total of counts kept current by other kernels against the parcel count
+// (a mismatch would leave the cell index inconsistent: reported as an error)
+__global__ void k_check_total(const int32_t* __restrict__ total, int64_t n, DevInfo* info) {
+  if (*total != n) atomicCAS(&info->error, 0, PMPIC_ERR_STATE);
+}
 __global__ void __launch_bounds__(256) k_bin_scatter(int64_t n, const int32_t* __restrict__ cell,
                                                      const int32_t* __restrict__ start, int32_t* __restrict__ fill,
-                                                     int32_t* __restrict__ sorted) {
+                                                     int32_t* __restrict__ sorted, int64_t lim) {
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int64_t t0 = (int64_t)blockIdx.x * 256 * SC_ITEMS + threadIdx.x;
@@ -104,7 +109,8 @@ __global__ void __launch_bounds__(256) k_bin_scatter(int64_t n, const int32_t* _
 #pragma unroll
   for (int k = 0; k < SC_ITEMS; ++k) {
     const int32_t b = __shfl_sync(FULL, base[k], __ffs(same[k]) - 1);
-    if (id[k] >= 0) sorted[st[k] + b + __popc(same[k] & ((1u << lane) - 1))] = (int32_t)(t0 + 256 * k);
+    const int64_t pos = (int64_t)st[k] + b + __popc(same[k] & ((1u << lane) - 1));
+    if (id[k] >= 0 && pos < lim) sorted[pos] = (int32_t)(t0 + 256 * k);  // (pos < n with exact counts)
   }
 }
 
@@ -264,6 +270,7 @@ struct P2GArgs {
   // index half of the {cell index, offset} positions (stride 2) on the mixed form
   const R* bh[3] = {};
   R* btot = nullptr;        // BT: the btot property, written as staged
+  int64_t nslot = 0;        // parcel count: staged slot indices are checked against it
   int32_t* npercell = nullptr;
   double vmin = 0.0;
 };
@@ -358,7 +365,7 @@ __global__ void __launch_bounds__(32 * RW, sizeof(R) == 4 ? 6 : 4) k_p2g_rows(Ge
 #pragma unroll
     for (int j = 0; j < BATCH / 32; ++j) {
       const int p = lane + 32 * j;
-      sl[j] = p < nb ? sorted[b0 + p] : -1;
+      sl[j] = (p < nb && b0 + p < a.nslot) ? sorted[b0 + p] : -1;  // (index positions lie below the count)
     }
   };
   // the fields of a batch of parcels into shared memory, field-major, position
@@ -367,7 +374,7 @@ __global__ void __launch_bounds__(32 * RW, sizeof(R) == 4 ? 6 : 4) k_p2g_rows(Ge
 #pragma unroll
     for (int j = 0; j < BATCH / 32; ++j) {
       const int n = sl[j];
-      if (n < 0) continue;
+      if (n < 0 || n >= a.nslot) continue;  // (an index entry is always a slot below the count)
       const int p = lane + 32 * j;
       R* D = Sb + p + (p >> 4);
       const size_t nd = (size_t)ds * n;
@@ -677,10 +684,11 @@ int bin_and_sort(pmpic_ctx* ctx) {
   const Geom& g = ctx->g;
   const int64_t n = ctx->n;
   PMPIC_CUDA(cudaMemsetAsync(ctx->cell_fill, 0, sizeof(int32_t) * g.ncell, ctx->stream));
-  // on the mixed form, after an RK4 stage and its haloswap, the cell ids and
-  // counts are written already (by the stage kernel and the haloswap's mover
-  // binning)
-  if (!ctx->count_ready) {
+  // on the mixed form, after an RK4 stage and its haloswap, a split or
+  // mixing, the cell ids and counts are current already (kept by the kernels
+  // that moved, added or removed parcels)
+  const bool counted = ctx->count_ready;
+  if (!counted) {
     PMPIC_CUDA(cudaMemsetAsync(ctx->cell_count, 0, sizeof(int32_t) * (g.ncell + 1), ctx->stream));
     if (n > 0 && ctx->mixed) {
       k_bin_count_m<<<nblk(n, 256), 256, 0, ctx->stream>>>(g, n, propc(ctx, PMPIC_PROP_X), propc(ctx, PMPIC_PROP_Y),
@@ -695,9 +703,12 @@ int bin_and_sort(pmpic_ctx* ctx) {
   ctx->count_ready = false;
   int rc = scan_excl(ctx, ctx->cell_count, g.ncell, ctx->cell_start);
   if (rc) return rc;
+  if (counted) {  // the maintained counts must add up to the parcels
+    k_check_total<<<1, 1, 0, ctx->stream>>>(ctx->cell_start + g.ncell, n, ctx->dinfo); ++ctx->nlaunch;
+  }
   if (n > 0) {
     k_bin_scatter<<<nblk(n, 256 * SC_ITEMS), 256, 0, ctx->stream>>>(n, ctx->cell, ctx->cell_start, ctx->cell_fill,
-                                                                    ctx->sorted); ++ctx->nlaunch;
+                                                                    ctx->sorted, ctx->cap); ++ctx->nlaunch;
     k_sort_segments<<<nblk(g.ncell, SORT_CELLS), SORT_CELLS, 0, ctx->stream>>>(g.ncell, ctx->cell_start, ctx->sorted);
     ++ctx->nlaunch;
   }
@@ -738,6 +749,7 @@ static int launch_p2g(pmpic_ctx* ctx, const double* const* fields, double* const
   a.bh[1] = prop(ctx, PMPIC_PROP_H);
   a.bh[2] = prop(ctx, PMPIC_PROP_Z);
   a.btot = prop(ctx, PMPIC_PROP_BTOT);
+  a.nslot = ctx->n;
   a.npercell = ctx->npercell;
   a.vmin = g.vmin;
   const double* del = ctx->del;
@@ -762,6 +774,7 @@ static int launch_p2g_m(pmpic_ctx* ctx, const float* const* fields, float* const
   a.bh[1] = propf(ctx, PMPIC_PROP_H);
   a.bh[2] = (const float*)prop(ctx, PMPIC_PROP_Z);  // the cell index halves
   a.btot = propf(ctx, PMPIC_PROP_BTOT);
+  a.nslot = ctx->n;
   a.npercell = ctx->npercell;
   a.vmin = (double)(float)g.vmin;
   const float* px = (const float*)prop(ctx, PMPIC_PROP_X) + 1;  // offset halves of the CellOff slots
@@ -1045,12 +1058,13 @@ extern "C" int pmpic_par2grid_static(int32_t nx, int32_t ny, int32_t nz, double 
   k_scan_sums<<<1, SCAN_BLOCK, 0, st>>>(tiles, ntiles, cstart + ncell);
   k_scan_apply<<<(unsigned)ntiles, SCAN_BLOCK, 0, st>>>(count, ncell, tiles, cstart);
   if (n > 0) {
-    k_bin_scatter<<<nblk(n, 256 * SC_ITEMS), 256, 0, st>>>(n, cell, cstart, fill, sorted);
+    k_bin_scatter<<<nblk(n, 256 * SC_ITEMS), 256, 0, st>>>(n, cell, cstart, fill, sorted, SP_MAX_PARCELS);
     k_sort_segments<<<nblk(ncell, SORT_CELLS), SORT_CELLS, 0, st>>>(ncell, cstart, sorted);
   }
   P2GArgs<1> a{};
   a.f[0] = field;
   a.out[0] = out;
+  a.nslot = n;
   if (run_p2g<1, 0, false>(g, cstart, sorted, del, del + SP_MAX_PARCELS, del + 2 * SP_MAX_PARCELS, 1, vol, a, rows,
                            st) != cudaSuccess)
     return PMPIC_ERR_CUDA;

@@ -1181,6 +1181,43 @@ __global__ void __launch_bounds__(256, 6) k_redistribute_m(Geom g, int64_t norig
   for (int q = 0; q < 5; ++q) F(pids[q])[m] = s[q] * rnv;
   F(PMPIC_PROP_VOL)[m] = nv;
 }
+// The binning's cell ids and counts kept current through mixing (mixed form):
+// the removed parcels leave their cells' counts first; once the final count
+// is known, every slot below it whose content changed (a new parcel, or one
+// moved there by the backfill: keep != 1) is binned from its position, and
+// every kept parcel beyond it (dropped by the backfill) leaves its count.
+__global__ void k_mix_uncount(const int32_t* __restrict__ zlist, const int32_t* __restrict__ nz,
+                              const int32_t* __restrict__ cell, int32_t* __restrict__ count) {
+  const int n = *nz;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int32_t c = cell[zlist[t]];
+    if (c >= 0) atomicSub(&count[c], 1);
+  }
+}
+__global__ void k_mix_recount(Geom g, int64_t norig, int64_t nfinal, const int32_t* __restrict__ keep,
+                              const CellOff* __restrict__ X, const CellOff* __restrict__ Y,
+                              const CellOff* __restrict__ Z, int32_t* __restrict__ cell,
+                              int32_t* __restrict__ count, DevInfo* info) {
+  const int64_t hi = norig > nfinal ? norig : nfinal;
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < hi; s += (int64_t)gridDim.x * blockDim.x) {
+    if (s < nfinal) {
+      if (s < norig && keep[s] == 1) continue;  // unchanged
+      const CellOff x = X[s], y = Y[s], z = Z[s];
+      int32_t id = -1;
+      if (x.i >= 0 && x.i < g.Nx && y.i >= 0 && y.i < g.Ny && z.i >= 0 && z.i < g.Nz && x.f >= 0.f && x.f <= 1.f &&
+          y.f >= 0.f && y.f <= 1.f && z.f >= 0.f && z.f <= 1.f) {
+        id = (int32_t)(((int64_t)x.i * g.Ny + y.i) * g.Nz + z.i);
+        atomicAdd(&count[id], 1);
+      } else {
+        atomicCAS(&info->error, 0, PMPIC_ERR_OUT_OF_BOX);
+      }
+      cell[s] = id;
+    } else if (keep[s] == 1) {  // s < norig: a kept parcel dropped beyond the final count
+      const int32_t c = cell[s];
+      if (c >= 0) atomicSub(&count[c], 1);
+    }
+  }
+}
 __global__ void k_backfill_m(const int32_t* __restrict__ zlist, const int32_t* __restrict__ nz,
                              const int32_t* __restrict__ olist, const int32_t* __restrict__ no,
                              double* __restrict__ parcels, int64_t cap, DevInfo* info) {
@@ -1529,6 +1566,9 @@ int mixing(pmpic_ctx* ctx) {
   int32_t* zlist = ctx->aux;
   int32_t* nz0 = dcounter(ctx, 3);
   if ((rc = compact(ctx, PredKeepEq{ctx->keep, 0}, norig, zlist, nz0))) return rc;
+  if (ctx->mixed) {  // the binning counts stay current through mixing
+    k_mix_uncount<<<148, 256, 0, ctx->stream>>>(zlist, nz0, ctx->cell, ctx->cell_count); ++ctx->nlaunch;
+  }
   int32_t hz0 = 0;
   PMPIC_CUDA(cudaMemcpyAsync(&hz0, nz0, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
   PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -1609,9 +1649,15 @@ int mixing(pmpic_ctx* ctx) {
     PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
     count = norig - hz;
   }
+  if (ctx->mixed && (norig > 0 || count > 0)) {
+    const int64_t hi = std::max<int64_t>(norig, count);
+    k_mix_recount<<<nblk(hi, 256), 256, 0, ctx->stream>>>(g, norig, count, ctx->keep, propc(ctx, PMPIC_PROP_X),
+                                                          propc(ctx, PMPIC_PROP_Y), propc(ctx, PMPIC_PROP_Z),
+                                                          ctx->cell, ctx->cell_count, ctx->dinfo); ++ctx->nlaunch;
+  }
   ctx->n = count;
   ctx->sorted_valid = false;
-  ctx->count_ready = false;
+  ctx->count_ready = ctx->mixed;  // the next binning starts at the scan
   ctx->in_domain = false;
   ctx->btot_grid_ready = false;
   ctx->info.n_removed = nremove;
