@@ -102,6 +102,39 @@ def test_mixed_split_and_mix_bookkeeping_vs_oracle(pm):
         assert rel_l2(g.grid(name), o.grid(name)) < TOL_VEL, name
 
 
+def test_mixed_kept_binning_counts_match_a_fresh_binning(pm):
+    """Within a step the mixed form keeps the binning's cell ids and counts
+    current through the RK4 stages, the haloswap, splitting and mixing instead
+    of recounting.  After steps with splits, removals and new parcels, a
+    par2grid through those kept counts equals, bit for bit, the par2grid of a
+    fresh context holding the same parcels (which bins from scratch; the cell
+    index orders each cell by slot either way)."""
+    n = 16
+    ic = _vortical(pm, n, amp=3.0)
+    k = len(ic["x"])
+    rng = np.random.default_rng(41)
+    ic["stretch"] = np.where(rng.uniform(size=k) < 0.1, 4.5, 3.5)
+    vmin = (TWO_PI / n) ** 2 * (math.pi / n) / 216
+    ic["vol"][rng.uniform(size=k) < 0.1] = 0.5 * vmin
+    ic["vol"][ic["x"] < 0.3] = 0.5 * vmin  # most of a column of cells emptied: new parcels there
+    cap = 4 * k
+    g = pm.Context(n, n, n, TWO_PI, TWO_PI, math.pi, dtm=0.02, dtmax=0.02, max_parcels=cap, precision="mixed")
+    g.upload(**ic)
+    g.step(1)
+    info = g.info()
+    assert info.n_split > 0 and info.n_removed > 0 and info.n_added > 0
+    g.step(1)
+    g.par2grid_multi(["p", "q", "r"], ["p", "q", "r"])  # through the kept counts
+    kept = {q: g.grid(q) for q in ["p", "q", "r"]}
+    f = pm.Context(n, n, n, TWO_PI, TWO_PI, math.pi, dtm=0.02, dtmax=0.02, max_parcels=cap, precision="mixed")
+    f.upload(**{q: g.get(q) for q in pm.DUMP_PROPS})
+    assert f.n == g.n
+    f.par2grid_multi(["p", "q", "r"], ["p", "q", "r"])  # a fresh binning
+    for q in ["p", "q", "r"]:
+        np.testing.assert_array_equal(kept[q], f.grid(q), err_msg=q)
+    np.testing.assert_array_equal(g.cell_ids(), f.cell_ids())
+
+
 def test_mixed_mixing_conserves_volume(pm):
     """parcel_mixing moves volume between removed, new and kept parcels and
     conserves its total (the report's check, report.tex:264); FP32 volumes
