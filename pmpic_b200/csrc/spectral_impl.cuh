@@ -76,22 +76,22 @@ __global__ void k_div(Geom g, const real* __restrict__ a, const real* __restrict
   f[x.e] = v;
 }
 
-// a = a - diffx(f) (vort2vel.F90:185-188) or b = b - diffy(f) (:191-194)
-__global__ void k_sub_diff(Geom g, real* __restrict__ a, const real* __restrict__ f, const real* __restrict__ kk,
-                           int ydir) {
+// The filter and both subtractions of vort2vel.F90:179-194 in one pass:
+// fo = filter(f) and a = a - diffx(fo), b = b - diffy(fo), the neighbours'
+// filtered values formed as the filter forms them (f is left unfiltered; fo
+// is a separate array, so no thread reads a value another one rewrote)
+__global__ void k_filter_sub2(Geom g, const real* __restrict__ f, real* __restrict__ fo, real* __restrict__ a,
+                              real* __restrict__ b, const real* __restrict__ kx, const real* __restrict__ ky,
+                              const real* __restrict__ filt) {
   EwIdx x;
   if (!ew_index(g, x)) return;
-  real d = ydir ? dy_of(f, x.e, x.jp, g.sx, kk, x.col) : dx_of(f, x.e, x.ip, kk, x.col);
-  a[x.e] = a[x.e] - d;
-}
-
-// c = c - d; c(1,:,:) = 0 (vort2vel.F90:197-205)
-__global__ void k_sub_zero0(Geom g, real* __restrict__ c, const real* __restrict__ d) {
-  EwIdx x;
-  if (!ew_index(g, x)) return;
-  real v = c[x.e] - d[x.e];
-  if (x.k == 0) v = real(0);
-  c[x.e] = v;
+  fo[x.e] = f[x.e] * filt[x.col];
+  const real dxf = (x.ip & 1) == 0 ? (real(-1) * (f[x.e + 1] * filt[x.col + 1])) * kx[x.col]
+                                   : (f[x.e - 1] * filt[x.col - 1]) * kx[x.col];
+  const real dyf = (x.jp & 1) == 0 ? (real(-1) * (f[x.e + g.sx] * filt[x.col + g.sx])) * ky[x.col]
+                                   : (f[x.e - g.sx] * filt[x.col - g.sx]) * ky[x.col];
+  a[x.e] = a[x.e] - dxf;
+  b[x.e] = b[x.e] - dyf;
 }
 
 // the top and bottom planes of a and b, unfiltered (vort2vel.F90:213-218)
@@ -126,6 +126,8 @@ struct DzBatch {
   real* out[2];
   const real* bot[2];  // both null: no boundary values (df0 form)
   const real* top[2];
+  real* sub;           // solve 0 only: c = c - diffz(f), c(1,:,:) = 0 (vort2vel.F90:196-205) in
+                       // place of the final values in out
 };
 __global__ void k_diffz(Geom g, DzBatch zb, const real* __restrict__ coef /* a[nz], den[nz], cp[nz] */,
                         real a1) {
@@ -168,11 +170,13 @@ __global__ void k_diffz(Geom g, DzBatch zb, const real* __restrict__ coef /* a[n
       f0 = fb[u];
     }
   }
+  real* __restrict__ sub = q == 0 ? zb.sub : nullptr;
   {
     int k = nz - 1;
     real dn = bt ? -fm / dz + a1 * top[col] * dz : real(0);  // fm = f(nz-1)
     prev = zdiv(dn - A[k] * prev, DEN[k]);
-    out[(uint32_t)k * cs + col] = prev;
+    if (sub) sub[(uint32_t)k * cs + col] = sub[(uint32_t)k * cs + col] - prev;
+    else out[(uint32_t)k * cs + col] = prev;
   }
   // back substitution: f(i) = f(i) - cp(i+1) f(i+1)
   real nxt = prev;
@@ -186,7 +190,12 @@ __global__ void k_diffz(Geom g, DzBatch zb, const real* __restrict__ coef /* a[n
       const int k = kb - u;
       if (k < 0) break;
       real v = ob[u] - CP[k + 1] * nxt;
-      out[(uint32_t)k * cs + col] = v;
+      if (sub) {
+        const uint32_t o = (uint32_t)k * cs + col;
+        sub[o] = k == 0 ? real(0) : sub[o] - v;
+      } else {
+        out[(uint32_t)k * cs + col] = v;
+      }
       nxt = v;
     }
   }
@@ -323,10 +332,11 @@ __global__ void k_max_vort(int64_t n, const real* __restrict__ p, const real* __
 // nb (1 or 2) diffz solves of one boundary kind (all with or all without
 // boundary values) in one launch
 int diffz_batch_impl(pmpic_ctx* ctx, int nb, const real* const* in, real* const* out, const real* const* bot,
-                     const real* const* top) {
+                     const real* const* top, real* sub = nullptr) {
   TimerScope ts(ctx, T_DIFFZ);
   const Geom& g = ctx->g;
   DzBatch zb{};
+  zb.sub = sub;
   for (int q = 0; q < nb; ++q) {
     zb.f[q] = in[q];
     zb.out[q] = out[q];
@@ -394,11 +404,13 @@ int vort2vel_spectral_impl(pmpic_ctx* ctx) {
   const real hdzi = (real)(f4div(1.f, 2.f) / g.dz);
   k_div<<<nb, 256, 0, ctx->stream>>>(g, a, b, c, f, tab_kx(ctx), tab_ky(ctx), hdzi); ++ctx->nlaunch;
   if ((rc = spec_laplinv_impl(ctx, f, true))) return rc;
-  k_filter<<<nb, 256, 0, ctx->stream>>>(g, f, f, tab_filt(ctx)); ++ctx->nlaunch;
-  k_sub_diff<<<nb, 256, 0, ctx->stream>>>(g, a, f, tab_kx(ctx), 0); ++ctx->nlaunch;
-  k_sub_diff<<<nb, 256, 0, ctx->stream>>>(g, b, f, tab_ky(ctx), 1); ++ctx->nlaunch;
-  if ((rc = diffz_launch_impl(ctx, f, d, nullptr, nullptr))) return rc;
-  k_sub_zero0<<<nb, 256, 0, ctx->stream>>>(g, c, d); ++ctx->nlaunch;
+  // :179-205: the filtered f (into e), a and b corrected, then c = c - diffz(filtered f)
+  k_filter_sub2<<<nb, 256, 0, ctx->stream>>>(g, f, e, a, b, tab_kx(ctx), tab_ky(ctx), tab_filt(ctx)); ++ctx->nlaunch;
+  {
+    const real* zin[1] = {e};
+    real* zout[1] = {d};
+    if ((rc = diffz_batch_impl(ctx, 1, zin, zout, nullptr, nullptr, c))) return rc;
+  }
   // :207-226: the top and bottom planes of a and b, then the filtered a, b, c
   // transformed back (the filter applied as the transform reads them)
   k_bt_planes<<<nblk(cols, 256), 256, 0, ctx->stream>>>(g, a, b, RP(ctx->bt)); ++ctx->nlaunch;
