@@ -181,18 +181,20 @@ __global__ void k_diffz(Geom g, DzBatch zb, const real* __restrict__ coef /* a[n
   // back substitution: f(i) = f(i) - cp(i+1) f(i+1)
   real nxt = prev;
   for (int kb = nz - 2; kb >= 0; kb -= ZB) {
-    real ob[ZB];
+    real ob[ZB], sb[ZB];
 #pragma unroll
     for (int u = 0; u < ZB; ++u)
-      if (kb - u >= 0) ob[u] = out[(uint32_t)(kb - u) * cs + col];
+      if (kb - u >= 0) {
+        ob[u] = out[(uint32_t)(kb - u) * cs + col];
+        if (sub) sb[u] = sub[(uint32_t)(kb - u) * cs + col];  // loaded with the batch, off the chain
+      }
 #pragma unroll
     for (int u = 0; u < ZB; ++u) {
       const int k = kb - u;
       if (k < 0) break;
       real v = ob[u] - CP[k + 1] * nxt;
       if (sub) {
-        const uint32_t o = (uint32_t)k * cs + col;
-        sub[o] = k == 0 ? real(0) : sub[o] - v;
+        sub[(uint32_t)k * cs + col] = k == 0 ? real(0) : sb[u] - v;
       } else {
         out[(uint32_t)k * cs + col] = v;
       }
