@@ -349,7 +349,12 @@ __global__ void __launch_bounds__(32 * RW, sizeof(R) == 4 ? 6 : 4) k_p2g_rows(Ge
   // and odd lane 2m+1 level m+1 (top corners of layer m + bottom corners of m+1)
   const int lev = lane == 0 ? 0 : (lane >> 1) + 1;
   const bool owner = (lane == 0 || (lane & 1)) && lev <= nk;
-  R* out_row = rowpart + ((size_t)zc * g.Ny + cy) * (size_t)g.Nx * Lay::RPS;
+  // row partials in two halves (y-low corners, then y-high corners), each
+  // nzc * Ny * Nx records of NA * NLV values: the combine pass reads each
+  // half of a row contiguously
+  constexpr int SEG = Lay::RPS / 2;  // NA * NLV
+  const size_t half = (size_t)nzc * g.Ny * g.Nx * SEG;
+  R* out_row = rowpart + ((size_t)zc * g.Ny + cy) * (size_t)g.Nx * SEG;
   R C[2][NA];  // x-high corners of the previous column, per y corner
   auto bounds = [&](int it, int& s, int& e) {  // this lane's cell layer of column it
     int cx = x_lo + it;
@@ -471,11 +476,11 @@ __global__ void __launch_bounds__(32 * RW, sizeof(R) == 4 ? 6 : 4) k_p2g_rows(Ge
     if (it >= 0) {
       const int cx = x_lo + it;
       if (owner) {
-        R* dst = out_row + (size_t)cx * Lay::RPS + lev;
+        R* dst = out_row + (size_t)cx * SEG + lev;
 #pragma unroll
         for (int b = 0; b < 2; ++b)
 #pragma unroll
-          for (int q = 0; q < NA; ++q) dst[(b * NA + q) * NLV] = C[b][q] + acc[2 * b][q];
+          for (int q = 0; q < NA; ++q) dst[b * half + q * NLV] = C[b][q] + acc[2 * b][q];
       }
       if (MODE == 1 && cz == 0 && has_cell) a.npercell[((int64_t)(k0 + kk) * g.Ny + cy) * g.Nx + cx] = nkept;
     }
@@ -548,7 +553,6 @@ template <int NQ, int MODE, class R = double>
 __global__ void __launch_bounds__(256) k_p2g_combine(Geom g, int nzc, const R* __restrict__ rowpart,
                                                     P2GArgs<NQ, R> a) {
   constexpr int NA = MODE == 0 ? NQ + 1 : NQ;
-  constexpr int RPS = 2 * NA * NLV;
   constexpr int TS = NA * NLV + 1;  // odd stride: conflict-free reads by consecutive points
   constexpr int PX = P2GPx<R>::value;
   constexpr int SEG = NA * NLV;
@@ -556,6 +560,7 @@ __global__ void __launch_bounds__(256) k_p2g_combine(Geom g, int nzc, const R* _
   __shared__ R Bz[2][PX * NA];      // the chunk below's top level, same rows
   const int px0 = blockIdx.x * PX, py = blockIdx.y, zc = blockIdx.z;
   const int pym = py == 0 ? g.Ny - 1 : py - 1;
+  const size_t half = (size_t)nzc * g.Ny * g.Nx * SEG;  // the y-high half follows the y-low one
   const int npx = min(PX, g.Nx - px0);
   const int k0 = zc * ZC, nk = min(ZC, g.Nz - k0);
   // one warp per (row, point) half-record, lanes along it: coalesced, and no
@@ -565,7 +570,7 @@ __global__ void __launch_bounds__(256) k_p2g_combine(Geom g, int nzc, const R* _
     const int r = rp / PX, pxl = rp % PX;  // PX is a power of two
     if (pxl >= npx) continue;
     const int row = r == 0 ? py : pym;
-    const R* src = rowpart + (((size_t)zc * g.Ny + row) * g.Nx + px0 + pxl) * RPS + r * SEG;
+    const R* src = rowpart + r * half + (((size_t)zc * g.Ny + row) * g.Nx + px0 + pxl) * SEG;
     R* dst = &T[r][pxl * TS];
     for (int o = lane; o < SEG; o += 32) dst[o] = src[o];
   }
@@ -576,8 +581,7 @@ __global__ void __launch_bounds__(256) k_p2g_combine(Geom g, int nzc, const R* _
       const int pxl = rem / NA, q = rem - pxl * NA;
       if (pxl >= npx) continue;
       const int row = r == 0 ? py : pym;
-      Bz[r][pxl * NA + q] =
-          rowpart[(((size_t)(zc - 1) * g.Ny + row) * g.Nx + px0 + pxl) * RPS + r * SEG + q * NLV + ZC];
+      Bz[r][pxl * NA + q] = rowpart[r * half + (((size_t)(zc - 1) * g.Ny + row) * g.Nx + px0 + pxl) * SEG + q * NLV + ZC];
     }
   }
   __syncthreads();
@@ -717,8 +721,8 @@ int bin_and_sort(pmpic_ctx* ctx) {
   return 0;
 }
 
-// the two passes of par2grid on `st`; rowpart holds nzc * Ny * Nx records of
-// P2GLayout::RPS values of type R
+// the two passes of par2grid on `st`; rowpart holds 2 * nzc * Ny * Nx records
+// of P2GLayout::RPS / 2 values of type R (the y-low half, then the y-high half)
 template <int NQ, int MODE, bool BT, class R = double>
 static cudaError_t run_p2g(const Geom& g, const int32_t* start, const int32_t* sorted, const R* dx, const R* dy,
                            const R* dz, int ds, const R* vol, const P2GArgs<NQ, R>& a, R* rowpart, cudaStream_t st,
