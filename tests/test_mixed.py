@@ -4,7 +4,7 @@ plain FP64 GPU path.  Needs a CUDA device.
 The mixed form computes in FP32 (interpolation, transforms, tendencies, RK4),
 keeps positions as an integer cell index plus an FP32 offset, and keeps the
 zero mode (the mean flow of vort2vel.F90:230-241) in FP64.  Its results are
-not bit-identical to FP64 and are judged by error against the FP64 oracle:
+not bit-identical to FP64 and are measured by their error against the FP64 oracle:
 
   * gridded velocity u, v, w after the 20 steps of the 32^3 plume (dt 0.01):
     relative L2 error <= 1e-4;
