@@ -841,7 +841,7 @@ __global__ void __launch_bounds__(256, 5) k_rk4_m(Geom g, int64_t n, MPtrs P, in
   sn[2] = co_reflect(sn[2], g.Nz);
   if (stretch) {  // the split's stretch update (parcel_splitting.F90:64-73) on the final p, q, r
     float ds = svn[0] * d[3] + svn[1] * d[4] + svn[2] * d[5];
-    ds = powf(fabsf(ds), 1.f / 3.f);
+    ds = cbrtf(fabsf(ds));  // |ds|^(1/3) (parcel_splitting.F90:71); FP32 1/3 is 1/3 to 1e-8
     stretch[t] = stretch[t] + ds * dt;
   }
 #pragma unroll
@@ -960,7 +960,7 @@ __global__ void k_split_flag_m(int64_t n, double* __restrict__ parcels, int64_t 
   auto F = [&](int pid) { return (float*)(parcels + (size_t)pid * cap); };
   float ds = F(PMPIC_PROP_P)[i] * F(PMPIC_PROP_DPDT)[i] + F(PMPIC_PROP_Q)[i] * F(PMPIC_PROP_DQDT)[i] +
              F(PMPIC_PROP_R)[i] * F(PMPIC_PROP_DRDT)[i];
-  ds = powf(fabsf(ds), 1.f / 3.f);
+  ds = cbrtf(fabsf(ds));  // |ds|^(1/3) (parcel_splitting.F90:71); FP32 1/3 is 1/3 to 1e-8
   const float s = F(PMPIC_PROP_STRETCH)[i] + ds * dt;
   F(PMPIC_PROP_STRETCH)[i] = s;
   flag[i] = s > 4.f ? 1 : 0;
