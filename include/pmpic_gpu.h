@@ -137,6 +137,24 @@ int pmpic_parcel_mixing(pmpic_ctx* ctx);         /* parcel_mixing.F90:68-431 */
 /* nsteps model steps: the integrator group run rksteps (=4) times per step
  * (timestepper.F90:89-106 with global_config:43's group contents). */
 int pmpic_step(pmpic_ctx* ctx, int nsteps);
+
+/* The reference's test components for the parcel migration path (FP64
+ * contexts; PMPIC_ERR_STATE on a mixed one):
+ * euler_integrator timestep (euler_integrator.F90:53-86): x, y, z, p, q, r
+ * += tendency * dtm, then the parcel haloswap;
+ * prescribed_parcel_velocity timestep (velocity.F90:96-255): dxdt, dydt, dzdt
+ * set from the profile (PMPIC_VELOCITY_*, the reference's velocity_profile
+ * codes) at each parcel's position, with x0, y0 the domain centre and r0 an
+ * eighth of its x extent (:66-69); and its initialisation's quadrant tags on
+ * one process (:72-84: tag = 2 [y > y0] + [x > x0]). */
+#define PMPIC_VELOCITY_SHEAR 0        /* dydt = tanh((x - x0) / r0) */
+#define PMPIC_VELOCITY_NORTH 1        /* 1..8: the compass directions N, NE, E, SE, S, SW, W, NW */
+#define PMPIC_VELOCITY_NORTH_WEST 8
+#define PMPIC_VELOCITY_CYLINDRICAL 9  /* a Gaussian vortex about (x0, y0) */
+#define PMPIC_VELOCITY_EVACUATE 10    /* flow out of (x/4, y/4) into (3x/4, 3y/4) */
+int pmpic_euler_integrator(pmpic_ctx* ctx);
+int pmpic_prescribed_velocity(pmpic_ctx* ctx, int profile);
+int pmpic_prescribed_velocity_tag(pmpic_ctx* ctx);
 int pmpic_get_step_info(pmpic_ctx* ctx, pmpic_step_info* info);
 
 /* Component iteration counters (vort2vel, vorticity_tendency, rk4 stage,

@@ -74,8 +74,10 @@ def lib():
         L.orc_laplinv.argtypes = [P, D, C.c_int]
         L.orc_filter.argtypes = [P, D, D]
         L.orc_kx_ky_k2.argtypes = [P, D, D, D, D]
+        L.orc_prescribed_velocity.argtypes = [P, C.c_int]
         for n in ["orc_parcel_haloswap", "orc_vort2vel", "orc_vort2vel_grids", "orc_vorticity_tendency",
-                  "orc_rk4_integrator", "orc_parcel_splitting", "orc_parcel_mixing", "orc_step"]:
+                  "orc_rk4_integrator", "orc_parcel_splitting", "orc_parcel_mixing", "orc_step",
+                  "orc_euler_integrator", "orc_prescribed_velocity_tag"]:
             getattr(L, n).argtypes = [P]
         L.orc_get_counters.argtypes = [P, C.POINTER(C.c_int)]
         L.orc_set_counters.argtypes = [P, C.POINTER(C.c_int)]
@@ -264,3 +266,13 @@ class Oracle:
 
     def step(self):
         self._check(lib().orc_step(self._h))
+
+    # -- test components (euler_integrator.F90, velocity.F90) ------------------
+    def euler_integrator(self):
+        self._check(lib().orc_euler_integrator(self._h))
+
+    def prescribed_velocity(self, profile):
+        self._check(lib().orc_prescribed_velocity(self._h, int(profile)))
+
+    def prescribed_velocity_tag(self):
+        self._check(lib().orc_prescribed_velocity_tag(self._h))

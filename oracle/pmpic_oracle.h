@@ -107,6 +107,12 @@ int orc_parcel_splitting(orc_ctx*);
 int orc_parcel_mixing(orc_ctx*);
 /* One full model step: the integrator group executed rksteps (=4) times. */
 int orc_step(orc_ctx*);
+/* test components: euler_integrator.F90:53-86 and prescribed_parcel_velocity
+ * (velocity.F90:59-255; profile 0 shear, 1-8 the compass directions N .. NW,
+ * 9 cylindrical, 10 evacuate) */
+int orc_euler_integrator(orc_ctx*);
+int orc_prescribed_velocity(orc_ctx*, int profile);
+int orc_prescribed_velocity_tag(orc_ctx*);
 
 /* Component iteration counters (vort2vel, vorticity_tendency, rk4 stage,
  * splitting, mixing), for re-synchronising with another implementation. */

@@ -94,9 +94,11 @@ def lib() -> C.CDLL:
         L.pmpic_set_count.argtypes = [P, I64]
         L.pmpic_get_count.argtypes = [P, C.POINTER(I64)]
         for n in ["pmpic_vort2vel", "pmpic_vorticity_tendency", "pmpic_rk4_integrator",
-                  "pmpic_parcel_splitting", "pmpic_parcel_mixing", "pmpic_op_parcel_haloswap"]:
+                  "pmpic_parcel_splitting", "pmpic_parcel_mixing", "pmpic_op_parcel_haloswap",
+                  "pmpic_euler_integrator", "pmpic_prescribed_velocity_tag"]:
             getattr(L, n).argtypes = [P]
         L.pmpic_step.argtypes = [P, C.c_int]
+        L.pmpic_prescribed_velocity.argtypes = [P, C.c_int]
         L.pmpic_get_step_info.argtypes = [P, C.POINTER(StepInfo)]
         L.pmpic_get_counters.argtypes = [P, C.POINTER(C.c_int32)]
         L.pmpic_set_counters.argtypes = [P, C.POINTER(C.c_int32)]
@@ -338,6 +340,16 @@ class Context:
 
     def rk4_integrator(self):
         self._check(lib().pmpic_rk4_integrator(self._h))
+
+    # the reference's test components for the migration path (FP64 contexts)
+    def euler_integrator(self):
+        self._check(lib().pmpic_euler_integrator(self._h))
+
+    def prescribed_velocity(self, profile):
+        self._check(lib().pmpic_prescribed_velocity(self._h, int(profile)))
+
+    def prescribed_velocity_tag(self):
+        self._check(lib().pmpic_prescribed_velocity_tag(self._h))
 
     def parcel_splitting(self):
         self._check(lib().pmpic_parcel_splitting(self._h))

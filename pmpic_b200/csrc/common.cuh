@@ -351,6 +351,8 @@ int parcel_haloswap(pmpic_ctx* ctx);
 int splitting(pmpic_ctx* ctx);
 int mixing(pmpic_ctx* ctx);
 int compute_btot(pmpic_ctx* ctx);
+int euler_step(pmpic_ctx* ctx);
+int prescribed_velocity(pmpic_ctx* ctx, int profile, bool tags);
 int flush_gathers(pmpic_ctx* ctx);
 int sync_info(pmpic_ctx* ctx);
 }  // namespace pmpic

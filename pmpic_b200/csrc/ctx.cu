@@ -740,6 +740,9 @@ static int do_mix(pmpic_ctx* ctx) {
   if (rc_) return rc_;                    \
   return sync_info(ctx);
 
+int pmpic_euler_integrator(pmpic_ctx* ctx) { PMPIC_ENTRY(euler_step(ctx)) }
+int pmpic_prescribed_velocity(pmpic_ctx* ctx, int profile) { PMPIC_ENTRY(prescribed_velocity(ctx, profile, false)) }
+int pmpic_prescribed_velocity_tag(pmpic_ctx* ctx) { PMPIC_ENTRY(prescribed_velocity(ctx, 0, true)) }
 int pmpic_vort2vel(pmpic_ctx* ctx) { PMPIC_ENTRY(do_vort2vel(ctx)) }
 int pmpic_vorticity_tendency(pmpic_ctx* ctx) { PMPIC_ENTRY(do_vorticity_tendency(ctx)) }
 int pmpic_rk4_integrator(pmpic_ctx* ctx) { PMPIC_ENTRY(do_rk4(ctx)) }

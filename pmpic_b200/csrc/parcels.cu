@@ -1249,6 +1249,64 @@ __global__ void k_grid2par_m(Geom g, int64_t n, const CellOff* __restrict__ X, c
   O2[t] = g2p_f(g, G2, x.i, y.i, z.i, x.f, y.f, z.f);
 }
 
+// ---- test components (FP64 path) ---------------------------------------------------
+// euler_integrator.F90:68-76: one explicit step of x, y, z, p, q, r
+__global__ void k_euler(int64_t n, double* __restrict__ parcels, int64_t cap, const double* __restrict__ dtp) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const double dt = *dtp;
+  const int S[6] = {PMPIC_PROP_X, PMPIC_PROP_Y, PMPIC_PROP_Z, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
+  const int D[6] = {PMPIC_PROP_DXDT, PMPIC_PROP_DYDT, PMPIC_PROP_DZDT, PMPIC_PROP_DPDT, PMPIC_PROP_DQDT,
+                    PMPIC_PROP_DRDT};
+#pragma unroll
+  for (int v = 0; v < 6; ++v) {
+    double* x = parcels + (size_t)S[v] * cap;
+    x[t] = x[t] + parcels[(size_t)D[v] * cap + t] * dt;
+  }
+}
+// prescribed_parcel_velocity (velocity.F90): x0, y0, r0 (:66-69) and the
+// centres of the evacuating profile (:233-237) from the global grid
+struct VelGeom {
+  double x0, y0, r0, xc1, yc1, xc2, yc2;
+};
+__global__ void k_prescribed_tag(int64_t n, double* __restrict__ parcels, int64_t cap, VelGeom vg) {  // :72-84
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  double tag = 0;
+  if (parcels[(size_t)PMPIC_PROP_Y * cap + t] > vg.y0) tag = tag + 2;
+  if (parcels[(size_t)PMPIC_PROP_X * cap + t] > vg.x0) tag = tag + 1;
+  parcels[(size_t)PMPIC_PROP_TAG * cap + t] = tag;
+}
+__global__ void k_prescribed_velocity(int64_t n, double* __restrict__ parcels, int64_t cap, int profile,
+                                      VelGeom vg) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const double x = parcels[(size_t)PMPIC_PROP_X * cap + t], y = parcels[(size_t)PMPIC_PROP_Y * cap + t];
+  const double x0 = vg.x0, y0 = vg.y0, r0 = vg.r0;
+  double u = 0., v = 0.;
+  if (profile == PMPIC_VELOCITY_SHEAR) {  // :103-111
+    v = tanh((x - x0) / r0);
+  } else if (profile == PMPIC_VELOCITY_CYLINDRICAL) {  // :113-129
+    const double theta = atan2(y - y0, x - x0);
+    const double r2 = ((x - x0) * (x - x0) + (y - y0) * (y - y0));
+    const double v0 = exp(-r2 / r0 / r0 / 2) / x0 * 10;
+    u = v0 * sqrt(r2) * sin(theta);
+    v = -v0 * sqrt(r2) * cos(theta);
+  } else if (profile == PMPIC_VELOCITY_EVACUATE) {  // :229-250
+    const double r1 = sqrt((x - vg.xc1) * (x - vg.xc1) + (y - vg.yc1) * (y - vg.yc1));
+    const double r2 = sqrt((x - vg.xc2) * (x - vg.xc2) + (y - vg.yc2) * (y - vg.yc2));
+    u = -(x - vg.xc1) / r1 * exp(-r1 * r1 / r0 / r0 / 4) + (x - vg.xc2) / r2 * exp(-r2 * r2 / r0 / r0 / 4);
+    v = -(y - vg.yc1) / r1 * exp(-r1 * r1 / r0 / r0 / 4) + (y - vg.yc2) / r2 * exp(-r2 * r2 / r0 / r0 / 4);
+  } else {  // the compass directions N .. NW (:131-226)
+    const int p = profile;
+    u = (p == 2 || p == 3 || p == 4) ? 1. : ((p == 6 || p == 7 || p == 8) ? -1. : 0.);
+    v = (p == 8 || p == 1 || p == 2) ? 1. : ((p == 4 || p == 5 || p == 6) ? -1. : 0.);
+  }
+  parcels[(size_t)PMPIC_PROP_DXDT * cap + t] = u;
+  parcels[(size_t)PMPIC_PROP_DYDT * cap + t] = v;
+  parcels[(size_t)PMPIC_PROP_DZDT * cap + t] = 0.;
+}
+
 }  // namespace
 
 // list of i in [0,n) with pred(i), ascending; count written to *dcount (device)
@@ -1546,6 +1604,58 @@ int splitting(pmpic_ctx* ctx) {
   ctx->n = nn;
   ctx->info.n_split = hns;
   return parcel_haloswap(ctx);
+}
+
+static VelGeom vel_geom(const pmpic_ctx* ctx) {
+  // setup_grid.F90:87-93: bottom = the domain's lower bound, top = its last grid point
+  const double bx = ctx->cfg.xmin, by = ctx->cfg.ymin;
+  const double tx = ctx->cfg.xmax - ctx->g.dx, ty = ctx->cfg.ymax - ctx->g.dy;
+  VelGeom vg;
+  vg.x0 = (tx - bx) / 2. + bx;
+  vg.y0 = (ty - by) / 2. + by;
+  vg.r0 = (tx - bx) / 8.;
+  vg.xc1 = 0.25 * (tx - bx) + bx;
+  vg.yc1 = 0.25 * (ty - by) + by;
+  vg.xc2 = 0.75 * (tx - bx) + bx;
+  vg.yc2 = 0.75 * (ty - by) + by;
+  return vg;
+}
+
+// euler_integrator.F90:53-86 (FP64 path)
+int euler_step(pmpic_ctx* ctx) {
+  if (ctx->mixed) return set_error(ctx, PMPIC_ERR_STATE, "euler_integrator: FP64 contexts only");
+  int rc = flush_gathers(ctx);
+  if (rc) return rc;
+  if (ctx->n > 0) {
+    k_euler<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->n, ctx->parcels, ctx->cap, &ctx->dinfo->dtm); ++ctx->nlaunch;
+  }
+  ctx->sorted_valid = false;
+  ctx->count_ready = false;
+  ctx->in_domain = false;
+  ctx->btot_grid_ready = false;
+  ctx->dir_ready = false;
+  PMPIC_CUDA(cudaGetLastError());
+  return parcel_haloswap(ctx);  // :82
+}
+
+// prescribed_parcel_velocity timestep (velocity.F90:96-255) and its
+// initialisation's quadrant tags (:72-84, one process); FP64 path
+int prescribed_velocity(pmpic_ctx* ctx, int profile, bool tags) {
+  if (ctx->mixed) return set_error(ctx, PMPIC_ERR_STATE, "prescribed velocity: FP64 contexts only");
+  if (!tags && (profile < 0 || profile > PMPIC_VELOCITY_EVACUATE))
+    return set_error(ctx, PMPIC_ERR_ARG, "prescribed velocity: unknown profile");
+  int rc = flush_gathers(ctx);  // the tendencies are overwritten
+  if (rc) return rc;
+  if (ctx->n > 0) {
+    if (tags)
+      k_prescribed_tag<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->n, ctx->parcels, ctx->cap, vel_geom(ctx));
+    else
+      k_prescribed_velocity<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->n, ctx->parcels, ctx->cap, profile,
+                                                                        vel_geom(ctx));
+    ++ctx->nlaunch;
+  }
+  PMPIC_CUDA(cudaGetLastError());
+  return 0;
 }
 
 int mixing(pmpic_ctx* ctx) {
