@@ -318,6 +318,31 @@ int64_t pmpic_setup_count(const pmpic_thermal_params* prm);
 int pmpic_setup_thermal(const pmpic_thermal_params* prm, int64_t n,
                         double* x, double* y, double* z, double* p, double* q, double* r,
                         double* b, double* h, double* vol, double* stretch, double* tag);
+/* The same thermal written on the device into the context's parcel state
+ * (either form), replacing it: the parcels of pmpic_setup_thermal, positions,
+ * h, vol and tag bit for bit, b within the rounding of the device cos; the
+ * count is pmpic_setup_count(prm). */
+int pmpic_setup_thermal_device(pmpic_ctx* ctx, const pmpic_thermal_params* prm);
+
+/* plume_parcelsetup initialisation (plume_parcelsetup.F90:58-334), one
+ * process, written on the device into the context's parcel state (either
+ * form), replacing it.  Plume parcels (4^3 per cell on a lattice, inside a
+ * sphere of radius r_plume * lambda resting on z = 0 at the domain centre)
+ * take the first *n_plume slots; environment parcels (2^3 per cell, outside
+ * the sphere) follow, in the reference's loop order.  Sets x, y, z, b, h and
+ * vol as the reference does; the other properties are zero.  The reference's
+ * parameter checks (:86-131) return PMPIC_ERR_ARG, and so does a plume that
+ * reaches above the domain top; too many parcels return PMPIC_ERR_CAPACITY. */
+typedef struct pmpic_plume_params {
+  double lambda;       /* scale height (config key lambda) */
+  double H;            /* relative humidity of the environment, < 1 (H) */
+  double z_c;          /* the plume's humidity is exp(-z_c) (z_c) */
+  double mu;           /* environment humidity / plume humidity, in (H, 1] (mu) */
+  double z_d, z_m;     /* the stratified layer's buoyancy gradient levels (z_d, z_m) */
+  double r_plume;      /* plume radius in scale heights (r_plume) */
+  double e_values[3];  /* buoyancy perturbation coefficients (e_values) */
+} pmpic_plume_params;
+int pmpic_setup_plume(pmpic_ctx* ctx, const pmpic_plume_params* prm, int64_t* n_plume);
 
 #ifdef __cplusplus
 }

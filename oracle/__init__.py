@@ -75,6 +75,7 @@ def lib():
         L.orc_filter.argtypes = [P, D, D]
         L.orc_kx_ky_k2.argtypes = [P, D, D, D, D]
         L.orc_prescribed_velocity.argtypes = [P, C.c_int]
+        L.orc_plume_setup.argtypes = [P, D, C.POINTER(C.c_int64)]
         for n in ["orc_parcel_haloswap", "orc_vort2vel", "orc_vort2vel_grids", "orc_vorticity_tendency",
                   "orc_rk4_integrator", "orc_parcel_splitting", "orc_parcel_mixing", "orc_step",
                   "orc_euler_integrator", "orc_prescribed_velocity_tag"]:
@@ -276,3 +277,13 @@ class Oracle:
 
     def prescribed_velocity_tag(self):
         self._check(lib().orc_prescribed_velocity_tag(self._h))
+
+    # -- plume_parcelsetup.F90:58-334 -----------------------------------------
+    def setup_plume(self, lam=1.0, H=0.8, z_c=2.5, mu=0.9, z_d=4.0, z_m=5.0, r_plume=0.8,
+                    e_values=(0.3, -0.4, 0.5)) -> int:
+        """Replace the parcels with the reference's plume initial condition;
+        returns the number of plume parcels (they take the first slots)."""
+        prm = np.ascontiguousarray([lam, H, z_c, mu, z_d, z_m, r_plume, *e_values], dtype=np.float64)
+        n_plume = C.c_int64(0)
+        self._check(lib().orc_plume_setup(self._h, _dp(prm), C.byref(n_plume)))
+        return n_plume.value

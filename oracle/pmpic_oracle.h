@@ -113,6 +113,10 @@ int orc_step(orc_ctx*);
 int orc_euler_integrator(orc_ctx*);
 int orc_prescribed_velocity(orc_ctx*, int profile);
 int orc_prescribed_velocity_tag(orc_ctx*);
+/* plume_parcelsetup initialisation (plume_parcelsetup.F90:58-334), one
+ * process: prm = {lambda, H, z_c, mu, z_d, z_m, r_plume, e_values(1:3)};
+ * replaces the parcels; *n_plume = the parcels of the plume (slots first). */
+int orc_plume_setup(orc_ctx*, const double* prm, int64_t* n_plume);
 
 /* Component iteration counters (vort2vel, vorticity_tendency, rk4 stage,
  * splitting, mixing), for re-synchronising with another implementation. */

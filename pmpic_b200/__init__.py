@@ -62,6 +62,19 @@ class ThermalParams(C.Structure):
                 ("z_strat", C.c_double), ("n2", C.c_double)]
 
 
+class PlumeParams(C.Structure):
+    _fields_ = [("lam", C.c_double), ("H", C.c_double), ("z_c", C.c_double), ("mu", C.c_double),
+                ("z_d", C.c_double), ("z_m", C.c_double), ("r_plume", C.c_double),
+                ("e_values", C.c_double * 3)]
+
+
+def thermal_params(nx, ny, nz, lx=2 * np.pi, ly=2 * np.pi, lz=np.pi, sub=2, jitter=0.25, seed=1,
+                   xc=np.pi, yc=np.pi, zc=0.6, radius=0.4, excess=1.0, h_in=0.95, h_env0=0.3,
+                   z_strat=1.2, n2=1.0) -> ThermalParams:
+    return ThermalParams(nx, ny, nz, lx, ly, lz, sub, jitter, seed, xc, yc, zc, radius, excess,
+                         h_in, h_env0, z_strat, n2)
+
+
 class PmpicError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"pmpic error {code} ({ERRORS.get(code, '?')}): {msg}")
@@ -148,6 +161,8 @@ def lib() -> C.CDLL:
         L.pmpic_setup_count.restype = I64
         L.pmpic_setup_count.argtypes = [C.POINTER(ThermalParams)]
         L.pmpic_setup_thermal.argtypes = [C.POINTER(ThermalParams), I64] + [D] * 11
+        L.pmpic_setup_thermal_device.argtypes = [P, C.POINTER(ThermalParams)]
+        L.pmpic_setup_plume.argtypes = [P, C.POINTER(PlumeParams), C.POINTER(I64)]
         _lib = L
     return _lib
 
@@ -162,8 +177,8 @@ def thermal_parcels(nx, ny, nz, lx=2 * np.pi, ly=2 * np.pi, lz=np.pi, sub=2, jit
                     xc=np.pi, yc=np.pi, zc=0.6, radius=0.4, excess=1.0, h_in=0.95, h_env0=0.3,
                     z_strat=1.2, n2=1.0) -> dict:
     """Jittered-lattice thermal plume initial condition (host, Philox4x32-10)."""
-    prm = ThermalParams(nx, ny, nz, lx, ly, lz, sub, jitter, seed, xc, yc, zc, radius, excess,
-                        h_in, h_env0, z_strat, n2)
+    prm = thermal_params(nx, ny, nz, lx, ly, lz, sub, jitter, seed, xc, yc, zc, radius, excess,
+                         h_in, h_env0, z_strat, n2)
     n = lib().pmpic_setup_count(C.byref(prm))
     out = {k: np.empty(n, np.float64) for k in IO_PROPS}
     rc = lib().pmpic_setup_thermal(C.byref(prm), n, *[_dp(out[k]) for k in IO_PROPS])
@@ -350,6 +365,21 @@ class Context:
 
     def prescribed_velocity_tag(self):
         self._check(lib().pmpic_prescribed_velocity_tag(self._h))
+
+    # -- set-up components written on the device ---------------------------------
+    def setup_plume(self, lam=1.0, H=0.8, z_c=2.5, mu=0.9, z_d=4.0, z_m=5.0, r_plume=0.8,
+                    e_values=(0.3, -0.4, 0.5)) -> int:
+        """plume_parcelsetup (the reference's defaults in its config); replaces the
+        parcels and returns the number of plume parcels (the first slots)."""
+        prm = PlumeParams(lam, H, z_c, mu, z_d, z_m, r_plume, (C.c_double * 3)(*e_values))
+        n_plume = C.c_int64(0)
+        self._check(lib().pmpic_setup_plume(self._h, C.byref(prm), C.byref(n_plume)))
+        return n_plume.value
+
+    def setup_thermal(self, **kw):
+        """The jittered thermal of thermal_parcels(**kw), written on the device."""
+        prm = thermal_params(**kw)
+        self._check(lib().pmpic_setup_thermal_device(self._h, C.byref(prm)))
 
     def parcel_splitting(self):
         self._check(lib().pmpic_parcel_splitting(self._h))

@@ -142,6 +142,29 @@ __host__ __device__ __forceinline__ bool mixed_is_pos(int pid) {
 __host__ __device__ __forceinline__ int mixed_elem_bytes(int pid) {
   return (mixed_is_pos(pid) || pid == PMPIC_PROP_TAG) ? 8 : 4;
 }
+// an FP64 coordinate v as cell index + FP32 offset for cell size d; period > 0
+// wraps the index into [0, period) (x, y); nz > 0 keeps a point on the top wall
+// z = nz d in the last cell with offset 1
+__device__ __forceinline__ CellOff co_from_double(double v, double d, int period, int nz) {
+  const double u = v / d;
+  const double fl = floor(u);
+  CellOff c;
+  c.i = (int)fl;
+  c.f = (float)(u - fl);
+  if (c.f >= 1.0f) {
+    c.f = 0.0f;
+    c.i += 1;
+  }
+  if (period > 0) {
+    if (c.i >= period) c.i -= period;
+    if (c.i < 0) c.i += period;
+  }
+  if (nz > 0 && c.i == nz && c.f == 0.0f) {
+    c.i = nz - 1;
+    c.f = 1.0f;
+  }
+  return c;
+}
 
 // Device-side step counters and error word.
 struct DevInfo {
@@ -353,6 +376,8 @@ int mixing(pmpic_ctx* ctx);
 int compute_btot(pmpic_ctx* ctx);
 int euler_step(pmpic_ctx* ctx);
 int prescribed_velocity(pmpic_ctx* ctx, int profile, bool tags);
+int setup_plume(pmpic_ctx* ctx, const pmpic_plume_params* prm, int64_t* n_plume);
+int setup_thermal_device(pmpic_ctx* ctx, const pmpic_thermal_params* prm);
 int flush_gathers(pmpic_ctx* ctx);
 int sync_info(pmpic_ctx* ctx);
 }  // namespace pmpic

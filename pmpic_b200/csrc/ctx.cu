@@ -346,24 +346,7 @@ __global__ void k_conv_in(int64_t n, const double* __restrict__ src, void* __res
   } else if (kind == 2) {
     ((double*)dst)[t] = v;
   } else {
-    const double u = v / d;
-    const double fl = floor(u);
-    CellOff c;
-    c.i = (int)fl;
-    c.f = (float)(u - fl);
-    if (c.f >= 1.0f) {
-      c.f = 0.0f;
-      c.i += 1;
-    }
-    if (period > 0) {  // x, y: periodic
-      if (c.i >= period) c.i -= period;
-      if (c.i < 0) c.i += period;
-    }
-    if (nz > 0 && c.i == nz && c.f == 0.0f) {  // z on the top wall
-      c.i = nz - 1;
-      c.f = 1.0f;
-    }
-    ((CellOff*)dst)[t] = c;
+    ((CellOff*)dst)[t] = co_from_double(v, d, period, nz);
   }
 }
 __global__ void k_conv_out(int64_t n, const void* __restrict__ src, double* __restrict__ dst, int kind, double d) {
@@ -743,6 +726,14 @@ static int do_mix(pmpic_ctx* ctx) {
 int pmpic_euler_integrator(pmpic_ctx* ctx) { PMPIC_ENTRY(euler_step(ctx)) }
 int pmpic_prescribed_velocity(pmpic_ctx* ctx, int profile) { PMPIC_ENTRY(prescribed_velocity(ctx, profile, false)) }
 int pmpic_prescribed_velocity_tag(pmpic_ctx* ctx) { PMPIC_ENTRY(prescribed_velocity(ctx, 0, true)) }
+int pmpic_setup_plume(pmpic_ctx* ctx, const pmpic_plume_params* prm, int64_t* n_plume) {
+  if (!prm) return PMPIC_ERR_ARG;
+  PMPIC_ENTRY(setup_plume(ctx, prm, n_plume))
+}
+int pmpic_setup_thermal_device(pmpic_ctx* ctx, const pmpic_thermal_params* prm) {
+  if (!prm) return PMPIC_ERR_ARG;
+  PMPIC_ENTRY(setup_thermal_device(ctx, prm))
+}
 int pmpic_vort2vel(pmpic_ctx* ctx) { PMPIC_ENTRY(do_vort2vel(ctx)) }
 int pmpic_vorticity_tendency(pmpic_ctx* ctx) { PMPIC_ENTRY(do_vorticity_tendency(ctx)) }
 int pmpic_rk4_integrator(pmpic_ctx* ctx) { PMPIC_ENTRY(do_rk4(ctx)) }
