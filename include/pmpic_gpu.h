@@ -244,6 +244,26 @@ int pmpic_read_parcels(pmpic_ctx* ctx, const char* path, int append, double* tim
  * parcels, hgliq = max(0, hg - exp(-z)), b + 12.5 hgliq, written with u, v, w
  * and vol as FP64, z fastest.  The model's own grids are not changed. */
 int pmpic_write_grids(pmpic_ctx* ctx, const char* path, double time);
+/* The NetCDF files of writenetcdf.F90 (write_ncgrid_file :225-308,
+ * write_parcels_to_file :310-439), one process, in the NetCDF classic
+ * 64-bit-offset format (the reference writes NetCDF-4; netCDF readers open
+ * both).  time is stored as given (the reference stores time + dtm); timestep
+ * is the model step number; dtm is the context's.  Grid file: dimensions
+ * time, z (nz+1), y, x; variables time, z, y, x, then u, v, w, p, q, r,
+ * b (+12.5 hgliq), hg, hgliq, vol over (time, x, y, z) gridded as in
+ * pmpic_write_grids, then timestep and dtm.  Parcel file: dimensions time and
+ * the unlimited nparcel; records parcel (1..n) and the 17 properties of
+ * pmpic_write_parcels (stretch under the reference's key "stetch"); the
+ * index bounds x_start .. z_end; timestep and dtm. */
+int pmpic_write_grids_netcdf(pmpic_ctx* ctx, const char* path, double time, int32_t timestep);
+int pmpic_write_parcels_netcdf(pmpic_ctx* ctx, const char* path, double time, int32_t timestep);
+/* The same files from host arrays: fields[10] each (nz+1)*ny*nx values, z
+ * fastest, on [0,lx) x [0,ly) x [0,lz]; props[17] each n values in the order
+ * x, y, z, p, q, r, dxdt, dydt, dzdt, dpdt, dqdt, drdt, h, b, vol, stretch, tag. */
+int pmpic_netcdf_write_grids(const char* path, int32_t nx, int32_t ny, int32_t nz, double lx, double ly, double lz,
+                             double time, int32_t timestep, double dtm, const double* const* fields);
+int pmpic_netcdf_write_parcels(const char* path, int32_t nx, int32_t ny, int32_t nz, int64_t n, double time,
+                               int32_t timestep, double dtm, const double* const* props);
 
 /* ---- ensembles (no counterpart in the reference, which runs one model per job) --
  * A batch of independent plumes of uneven grid sizes and parcel counts on one

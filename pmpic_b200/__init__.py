@@ -137,6 +137,12 @@ def lib() -> C.CDLL:
         L.pmpic_write_parcels.argtypes = [P, C.c_char_p, C.c_double]
         L.pmpic_read_parcels.argtypes = [P, C.c_char_p, C.c_int, C.POINTER(C.c_double)]
         L.pmpic_write_grids.argtypes = [P, C.c_char_p, C.c_double]
+        L.pmpic_write_grids_netcdf.argtypes = [P, C.c_char_p, C.c_double, C.c_int32]
+        L.pmpic_write_parcels_netcdf.argtypes = [P, C.c_char_p, C.c_double, C.c_int32]
+        L.pmpic_netcdf_write_grids.argtypes = [C.c_char_p] + [C.c_int32] * 3 + [C.c_double] * 4 + \
+            [C.c_int32, C.c_double, C.POINTER(D)]
+        L.pmpic_netcdf_write_parcels.argtypes = [C.c_char_p] + [C.c_int32] * 3 + [I64, C.c_double, C.c_int32,
+                                                                                 C.c_double, C.POINTER(D)]
         L.pmpic_ensemble_create.argtypes = [C.c_int, C.POINTER(Config), C.POINTER(P)]
         L.pmpic_ensemble_destroy.argtypes = [P]
         L.pmpic_ensemble_member.restype = P
@@ -185,6 +191,34 @@ def thermal_parcels(nx, ny, nz, lx=2 * np.pi, ly=2 * np.pi, lz=np.pi, sub=2, jit
     if rc:
         raise PmpicError(rc, "pmpic_setup_thermal")
     return out
+
+
+NETCDF_GRID_FIELDS = ["u", "v", "w", "p", "q", "r", "b", "hg", "hgliq", "vol"]
+NETCDF_PARCEL_PROPS = ["x", "y", "z", "p", "q", "r", "dxdt", "dydt", "dzdt", "dpdt", "dqdt", "drdt",
+                       "h", "b", "vol", "stretch", "tag"]
+
+
+def netcdf_write_grids(path, nx, ny, nz, lx, ly, lz, fields, time=0.0, timestep=0, dtm=0.0):
+    """The NetCDF grid file from host arrays: fields[name] of (nz+1)*ny*nx values, z fastest."""
+    arrs = [np.ascontiguousarray(fields[k], dtype=np.float64).ravel() for k in NETCDF_GRID_FIELDS]
+    if any(a.size != (nz + 1) * ny * nx for a in arrs):
+        raise ValueError("each field needs (nz+1)*ny*nx values")
+    ptrs = (C.POINTER(C.c_double) * 10)(*[_dp(a) for a in arrs])
+    rc = lib().pmpic_netcdf_write_grids(os.fsencode(path), nx, ny, nz, lx, ly, lz, time, timestep, dtm, ptrs)
+    if rc:
+        raise PmpicError(rc, "pmpic_netcdf_write_grids")
+
+
+def netcdf_write_parcels(path, nx, ny, nz, props, time=0.0, timestep=0, dtm=0.0):
+    """The NetCDF parcel file from host arrays: props[name] for the 17 dumped properties."""
+    arrs = [np.ascontiguousarray(props[k], dtype=np.float64) for k in NETCDF_PARCEL_PROPS]
+    n = len(arrs[0])
+    if any(len(a) != n for a in arrs):
+        raise ValueError("all properties need the same length")
+    ptrs = (C.POINTER(C.c_double) * 17)(*[_dp(a) for a in arrs])
+    rc = lib().pmpic_netcdf_write_parcels(os.fsencode(path), nx, ny, nz, n, time, timestep, dtm, ptrs)
+    if rc:
+        raise PmpicError(rc, "pmpic_netcdf_write_parcels")
 
 
 def random_vorticity(nx, ny, nz, lx=2 * np.pi, ly=2 * np.pi, lz=np.pi, kmax=64, seed=4, rms=1.0):
@@ -431,6 +465,14 @@ class Context:
     def write_grids(self, path, time=0.0):
         """Grid dump in the reference's binary format (writebinary.F90)."""
         self._check(lib().pmpic_write_grids(self._h, os.fsencode(path), float(time)))
+
+    def write_grids_netcdf(self, path, time=0.0, timestep=0):
+        """NetCDF grid file of writenetcdf.F90:225-308 (classic 64-bit-offset format)."""
+        self._check(lib().pmpic_write_grids_netcdf(self._h, os.fsencode(path), float(time), int(timestep)))
+
+    def write_parcels_netcdf(self, path, time=0.0, timestep=0):
+        """NetCDF parcel file of writenetcdf.F90:310-439 (classic 64-bit-offset format)."""
+        self._check(lib().pmpic_write_parcels_netcdf(self._h, os.fsencode(path), float(time), int(timestep)))
 
     def sort_parcels(self):
         """Renumber slots into cell order (not a reference operation)."""
