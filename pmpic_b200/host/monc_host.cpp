@@ -27,6 +27,7 @@
 #include <fstream>
 #include <functional>
 #include <map>
+#include <memory>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -127,6 +128,7 @@ struct State {
   pmpic_ctx* gpu = nullptr;
   int rksteps = 0;
   long long timestep = 0;
+  long long iterations = 0;  // steps completed (state.F90:53)
   double time = 0.0;
   double dtm = 0.0;
   bool continue_timestep = true;
@@ -168,44 +170,191 @@ static ComponentDescriptor gpu_component(const char* name, int (*fn)(pmpic_ctx*)
   return d;
 }
 
+// The device context: the grid (setup_grid.F90:45-104) and the parcel store of
+// max_parcels (parcelsetup_base.F90:49-81), created by the first component
+// that needs it (parcelsetup_base, a set-up component or an integrator).
+static int ensure_context(State& s) {
+  if (s.gpu || s.dry_run) return 0;
+  const Options& o = s.options;
+  pmpic_config cfg{};
+  cfg.nx = (int32_t)o.integer("nx");
+  cfg.ny = (int32_t)o.integer("ny");
+  cfg.nz = (int32_t)o.integer("nz");
+  cfg.xmin = o.real("xmin");
+  cfg.xmax = o.real("xmax");
+  cfg.ymin = o.real("ymin");
+  cfg.ymax = o.real("ymax");
+  cfg.zmin = o.real("zmin");
+  cfg.zmax = o.real("zmax");
+  cfg.dtm = o.real("dtm");
+  cfg.dtmax = o.real("dtmax", cfg.dtm);
+  cfg.timestep_prefactor = o.real("timestep_prefactor", 0.5);
+  cfg.max_parcels = o.integer("max_parcels");
+  cfg.precision = PMPIC_FP64;
+  cfg.device = (int32_t)o.integer("device", 0);
+  int rc = pmpic_create(&cfg, &s.gpu);
+  if (rc) {
+    std::fprintf(stderr, "pmpic_create failed: %d\n", rc);
+    return rc;
+  }
+  s.dtm = cfg.dtm;
+  return 0;
+}
+static int release_context(State& s) {
+  if (s.gpu) pmpic_destroy(s.gpu);
+  s.gpu = nullptr;
+  return 0;
+}
+
+// an integrator's initialisation: one integrator only (rk4_integrator.F90:47-51,
+// euler_integrator.F90:44-50), then the device context
+static int integrator_init(State& s, int rksteps, const char* name) {
+  if (s.rksteps != 0) {
+    std::fprintf(stderr, "Error - another integrator component is present (%s). ABORTING\n", name);
+    return (int)PMPIC_ERR_CONFIG;
+  }
+  s.rksteps = rksteps;
+  return ensure_context(s);
+}
+
+// writebinary (writebinary.F90:31-134) and writenetcdf (writenetcdf.F90:84-180):
+// <name>_mode none | step | time; files every <what>_step_write<sfx>_frequency
+// steps (by the iteration count) or every <what>_time_write<sfx>_frequency of
+// model time
+static ComponentDescriptor writer(const char* name, bool netcdf) {
+  struct Cfg {
+    std::string mode;
+    long long psteps = 0, gsteps = 0;
+    double dtp = 0, dtg = 0, tnextp = 0, tnextg = 0;
+  };
+  auto c = std::make_shared<Cfg>();
+  ComponentDescriptor d;
+  d.name = name;
+  const std::string sfx = netcdf ? "_netcdf" : "";
+  d.initialisation = [c, sfx, name](State& s) {
+    const Options& o = s.options;
+    c->mode = Options::lower(o.str(std::string(name) + "_mode", "none"));
+    if (c->mode == "time") {
+      c->dtp = o.real("parcel_time_write" + sfx + "_frequency");
+      c->dtg = o.real("grid_time_write" + sfx + "_frequency");
+    } else if (c->mode == "step") {
+      c->psteps = o.integer("parcel_step_write" + sfx + "_frequency");
+      c->gsteps = o.integer("grid_step_write" + sfx + "_frequency");
+    } else if (c->mode != "none") {
+      std::fprintf(stderr, "Error: mode '%s' not recognised. The valid options are 'none', 'time' or 'step'\n",
+                   c->mode.c_str());
+      return (int)PMPIC_ERR_CONFIG;
+    }
+    return 0;
+  };
+  d.timestep = [c, netcdf, name](State& s) {
+    if (s.dry_run) {
+      s.trace.push_back(name);
+      return 0;
+    }
+    const long long num = s.iterations;
+    bool parcels = false, grids = false;
+    if (c->mode == "step") {
+      parcels = c->psteps != 0 && num % c->psteps == 0;
+      grids = c->gsteps != 0 && num % c->gsteps == 0;
+    } else if (c->mode == "time") {
+      if (c->dtg != 0. && s.time >= c->tnextg) {
+        grids = true;
+        c->tnextg += c->dtg;
+      }
+      if (c->dtp != 0. && s.time >= c->tnextp) {
+        parcels = true;
+        c->tnextp += c->dtp;
+      }
+    }
+    char path[64];
+    int rc = 0;
+    if (grids) {  // writebinary.F90:259, writenetcdf.F90:206
+      if (netcdf) {
+        std::snprintf(path, sizeof path, "grids_%04lld.nc", num);
+        rc = check(s, pmpic_write_grids_netcdf(s.gpu, path, s.time + s.dtm, (int32_t)s.timestep), path);
+      } else {
+        std::snprintf(path, sizeof path, "grids_%05d_%05lld.dat", 0, num);
+        rc = check(s, pmpic_write_grids(s.gpu, path, s.time), path);
+      }
+    }
+    if (!rc && parcels) {  // writebinary.F90:160, writenetcdf.F90:333
+      std::snprintf(path, sizeof path, netcdf ? "parcels_%05d_%05lld.nc" : "parcels_%05d_%05lld.dat", 0, num);
+      rc = netcdf ? check(s, pmpic_write_parcels_netcdf(s.gpu, path, s.time + s.dtm, (int32_t)s.timestep), path)
+                  : check(s, pmpic_write_parcels(s.gpu, path, s.time), path);
+    }
+    return rc;
+  };
+  return d;
+}
+
 static std::vector<ComponentDescriptor> all_components() {
   std::vector<ComponentDescriptor> v;
-  // rk4_integrator also owns the device context (created once the grid and
-  // the parcel set-up options are known, rk4_integrator.F90:33-78)
+  ComponentDescriptor base;
+  base.name = "parcelsetup_base";
+  base.initialisation = ensure_context;
+  base.finalisation = release_context;
+  v.push_back(base);
   ComponentDescriptor rk4 = gpu_component("rk4_integrator", pmpic_rk4_integrator);
-  rk4.initialisation = [](State& s) {
-    s.rksteps = 4;  // rk4_integrator.F90:51
+  rk4.initialisation = [](State& s) { return integrator_init(s, 4, "rk4_integrator"); };  // rk4_integrator.F90:51
+  rk4.finalisation = release_context;
+  ComponentDescriptor euler = gpu_component("euler_integrator", pmpic_euler_integrator);
+  euler.initialisation = [](State& s) { return integrator_init(s, 1, "euler_integrator"); };  // :49
+  v.push_back(euler);
+  // prescribed_parcel_velocity (velocity.F90:58-262): quadrant tags at the
+  // start of a run, then the analytic tendencies of velocity_profile each call
+  ComponentDescriptor pv;
+  pv.name = "prescribed_parcel_velocity";
+  pv.initialisation = [](State& s) {
     if (s.dry_run) return 0;
-    const Options& o = s.options;
-    pmpic_config cfg{};
-    cfg.nx = (int32_t)o.integer("nx");
-    cfg.ny = (int32_t)o.integer("ny");
-    cfg.nz = (int32_t)o.integer("nz");
-    cfg.xmin = o.real("xmin");
-    cfg.xmax = o.real("xmax");
-    cfg.ymin = o.real("ymin");
-    cfg.ymax = o.real("ymax");
-    cfg.zmin = o.real("zmin");
-    cfg.zmax = o.real("zmax");
-    cfg.dtm = o.real("dtm");
-    cfg.dtmax = o.real("dtmax", cfg.dtm);
-    cfg.timestep_prefactor = o.real("timestep_prefactor", 0.5);
-    cfg.max_parcels = o.integer("max_parcels");
-    cfg.precision = PMPIC_FP64;
-    cfg.device = (int32_t)o.integer("device", 0);
-    int rc = pmpic_create(&cfg, &s.gpu);
-    if (rc) {
-      std::fprintf(stderr, "pmpic_create failed: %d\n", rc);
-      return rc;
+    int rc = ensure_context(s);
+    if (!rc && s.iterations == 0) rc = check(s, pmpic_prescribed_velocity_tag(s.gpu), "prescribed_velocity_tag");
+    return rc;
+  };
+  pv.timestep = [](State& s) {
+    if (s.dry_run) {
+      s.trace.push_back("prescribed_parcel_velocity");
+      return 0;
     }
-    s.dtm = cfg.dtm;
-    return 0;
+    return check(s, pmpic_prescribed_velocity(s.gpu, (int)s.options.integer("velocity_profile")),
+                 "prescribed_velocity");
   };
-  rk4.finalisation = [](State& s) {
-    if (s.gpu) pmpic_destroy(s.gpu);
-    s.gpu = nullptr;
-    return 0;
+  v.push_back(pv);
+  // plume_parcelsetup (plume_parcelsetup.F90:58-334), written on the device
+  ComponentDescriptor plume;
+  plume.name = "plume_parcelsetup";
+  plume.initialisation = [](State& s) {
+    if (s.dry_run) return 0;
+    int rc = ensure_context(s);
+    if (rc) return rc;
+    const Options& o = s.options;
+    pmpic_plume_params p{};
+    p.lambda = o.real("lambda");
+    p.H = o.real("h");
+    p.z_c = o.real("z_c");
+    p.mu = o.real("mu");
+    p.z_d = o.real("z_d");
+    p.z_m = o.real("z_m");
+    p.r_plume = o.real("r_plume");
+    const std::vector<std::string> e = o.list("e_values");
+    if (e.size() != 3) {
+      std::fprintf(stderr, "plume_parcelsetup: e_values needs 3 values\n");
+      return (int)PMPIC_ERR_CONFIG;
+    }
+    for (int i = 0; i < 3; ++i) p.e_values[i] = std::atof(e[i].c_str());
+    int64_t n_plume = 0;
+    rc = check(s, pmpic_setup_plume(s.gpu, &p, &n_plume), "plume_parcelsetup");
+    if (!rc) {
+      int64_t n = 0;
+      pmpic_get_count(s.gpu, &n);
+      std::printf("Total number of parcels= %lld background= %lld plume= %lld\n", (long long)n,
+                  (long long)(n - n_plume), (long long)n_plume);
+    }
+    return rc;
   };
+  v.push_back(plume);
+  v.push_back(writer("writebinary", false));
+  v.push_back(writer("writenetcdf", true));
   v.push_back(gpu_component("vort2vel", pmpic_vort2vel));
   v.push_back(gpu_component("vorticity_tendency", pmpic_vorticity_tendency));
   v.push_back(rk4);
@@ -216,6 +365,7 @@ static std::vector<ComponentDescriptor> all_components() {
   ic.name = "thermal_parcelsetup";
   ic.initialisation = [](State& s) {
     if (s.dry_run) return 0;
+    if (int rc = ensure_context(s)) return rc;
     const Options& o = s.options;
     pmpic_thermal_params p{};
     p.nx = (int32_t)o.integer("nx");
@@ -335,7 +485,10 @@ class Registry {
 static int run(State& s, Registry& reg) {
   for (const auto* c : reg.init_order) {
     int rc = c->initialisation(s);
-    if (rc) return rc;
+    if (rc) {
+      release_context(s);
+      return rc;
+    }
   }
   if (s.rksteps <= 0) {
     std::fprintf(stderr, "Error: number of integrator steps has not been defined.\n");  // timestepper.F90:95-98
@@ -357,9 +510,11 @@ static int run(State& s, Registry& reg) {
     if (s.continue_timestep) {
       s.timestep += 1;
       s.time += s.dtm;
+      s.iterations += 1;
     }
   }
   for (const auto* c : reg.final_order) c->finalisation(s);
+  release_context(s);
   return rc;
 }
 

@@ -90,3 +90,48 @@ def test_host_run_matches_python_binding(tmp_path):
     info = ctx.info()
     assert n_host == info.n_parcels
     assert dt_host == pytest.approx(info.dtm, rel=1e-5)
+
+
+REF_SET = ("global_configuration={g}\n"
+           "initialisation_stage_ordering=decomposition, setup_grid, parcelsetup_base, basic_parcelsetup,"
+           "plume_parcelsetup, readfromfile_parcelsetup,termination_check, model_synopsis, halo_swapper, "
+           "writebinary, writenetcdf, prescribed_parcel_velocity, euler_integrator,rk4_integrator,vort2vel,"
+           "vorticity_tendency,parcel_mixing,parcel_splitting\n"
+           "start_group_contents=writebinary,writenetcdf,termination_check, halo_swapper\n"
+           "integrator_group_contents=prescribed_parcel_velocity,euler_integrator,rk4_integrator\n"
+           "parcelsetup_base_enabled=.true.\nplume_parcelsetup_enabled=.true.\nthermal_parcelsetup_enabled=.false.\n"
+           "euler_integrator_enabled=.true.\nprescribed_parcel_velocity_enabled=.true.\nvelocity_profile=2\n"
+           "writebinary_enabled=.true.\nwritebinary_mode=step\nparcel_step_write_frequency=5\n"
+           "grid_step_write_frequency=5\nwritenetcdf_enabled=.true.\nwritenetcdf_mode=none\n"
+           "lambda=1\nH=0.8\nz_c=2.5\nmu=0.9\nz_d=4.\nz_m=5.\nr_plume=0.8\ne_values=0.3, -0.4 ,0.5\n"
+           "nx=32\nny=32\nnz=32\nxmin=0\nxmax=6.28\nymin=0\nymax=6.28\nzmin=0\nzmax=6.28\n"
+           "max_parcels=1000000\ndtm=0.1\ndtmax=0.1\n")
+
+
+def _ref_set(tmp_path, extra=""):
+    cfg = tmp_path / "ref_set.mcf"
+    cfg.write_text(REF_SET.format(g=os.path.join(DATA, "monc_global_config")) + extra)
+    return cfg
+
+
+def test_reference_component_set_order(tmp_path):
+    """The reference's set-up, test-integrator and writer components in its
+    global_config orderings: parcelsetup_base allocates, plume_parcelsetup
+    fills, the Euler integrator sets one stage per step (euler_integrator.F90:49)."""
+    out = run(f"--config={_ref_set(tmp_path)}", "--dry-run").stdout
+    init = out.split("init:")[1].split("\n")[0].split()
+    step = out.split("step:")[1].split("\n")[0].split()
+    assert init == ["parcelsetup_base", "plume_parcelsetup", "writebinary", "writenetcdf",
+                    "prescribed_parcel_velocity", "euler_integrator"]
+    assert step == ["writebinary", "writenetcdf", "termination_check", "prescribed_parcel_velocity",
+                    "euler_integrator", "model_synopsis"]
+
+
+def test_two_integrators_are_refused(tmp_path):
+    p = run(f"--config={_ref_set(tmp_path, 'rk4_integrator_enabled=.true.\n')}", "--dry-run", check=False)
+    assert p.returncode != 0 and "another integrator" in p.stderr
+
+
+def test_unknown_writer_mode_is_refused(tmp_path):
+    p = run(f"--config={_ref_set(tmp_path, 'writenetcdf_mode=sometimes\n')}", "--dry-run", check=False)
+    assert p.returncode != 0 and "not recognised" in p.stderr

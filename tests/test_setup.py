@@ -13,9 +13,8 @@ import pytest
 
 IO = ["x", "y", "z", "p", "q", "r", "b", "h", "vol", "stretch", "tag"]
 REF_CFG = dict(lam=1.0, H=0.8, z_c=2.5, mu=0.9, z_d=4.0, z_m=5.0, r_plume=0.8, e_values=(0.3, -0.4, 0.5))
-# grids: the reference's config.mcf (32 x 32 x 32 points on [0, 6.28]^3, i.e. 31 z cells) and a
-# non-cubic box
-GRIDS = [(32, 32, 31, 6.28, 6.28, 6.28), (24, 20, 12, 2 * math.pi, 5.0, math.pi)]
+# grids: the reference's config.mcf (32^3 cells on [0, 6.28]^3) and a non-cubic box
+GRIDS = [(32, 32, 32, 6.28, 6.28, 6.28), (24, 20, 12, 2 * math.pi, 5.0, math.pi)]
 
 
 def _walk(start, step, count):
@@ -144,7 +143,7 @@ def test_device_plume_errors(pm):
 @pytest.mark.gpu
 def test_device_plume_then_steps_vs_oracle(pm):
     from oracle import Oracle
-    grid = (32, 32, 31, 6.28, 6.28, 6.28)
+    grid = GRIDS[0]
     o = Oracle(*grid, dtm=0.02, dtmax=0.02, max_parcels=600000)
     g = pm.Context(*grid, dtm=0.02, dtmax=0.02, max_parcels=600000)
     o.setup_plume(**REF_CFG)
