@@ -71,7 +71,7 @@ def test_grid_file_from_host_arrays(tmp_path):
     check_grid_file(path, nx, ny, nz, lx, ly, lz, fields, 1.25, 7, 0.01)
 
 
-@pytest.mark.parametrize("n", [1, 270001])  # one record; records across the writer's 2^18-record slabs
+@pytest.mark.parametrize("n", [0, 1, 270001])  # one record; records across the writer's 2^18-record slabs
 def test_parcel_file_from_host_arrays(tmp_path, n):
     import pmpic_b200 as pm
     rng = np.random.default_rng(n)
@@ -79,6 +79,19 @@ def test_parcel_file_from_host_arrays(tmp_path, n):
     path = tmp_path / "parcels_00000_0003.nc"
     pm.netcdf_write_parcels(path, 16, 12, 8, props, time=0.5, timestep=3, dtm=0.02)
     check_parcel_file(path, 16, 12, 8, props, 0.5, 3, 0.02)
+
+
+def test_variable_beyond_the_format_limit_is_refused(tmp_path):
+    # 1025 x 1024 x 1024 FP64 values per field exceed the 4 GiB a classic
+    # 64-bit-offset variable may hold; the header check refuses the file before
+    # any field value is read, so one-value arrays stand in for the fields
+    import ctypes as C
+    import pmpic_b200 as pm
+    one = [np.zeros(1) for _ in range(10)]
+    ptrs = (C.POINTER(C.c_double) * 10)(*[a.ctypes.data_as(C.POINTER(C.c_double)) for a in one])
+    rc = pm.lib().pmpic_netcdf_write_grids(str(tmp_path / "big.nc").encode(), 1024, 1024, 1024, 1.0, 1.0, 1.0,
+                                           0.0, 0, 0.0, ptrs)
+    assert rc != 0
 
 
 @pytest.fixture(scope="module")
