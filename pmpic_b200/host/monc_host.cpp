@@ -353,6 +353,37 @@ static std::vector<ComponentDescriptor> all_components() {
     return rc;
   };
   v.push_back(plume);
+  // readfromfile_parcelsetup (readfromfile_parcelsetup.F90:26-130): restart
+  // from the parcel dumps of step restart_num, every rank's file appended in
+  // rank order; the dump's time becomes the model time
+  ComponentDescriptor restart;
+  restart.name = "readfromfile_parcelsetup";
+  restart.initialisation = [](State& s) {
+    const long long num = s.options.integer("restart_num");
+    s.iterations = num;  // :43
+    std::vector<std::string> files;
+    for (int rank = 0;; ++rank) {  // :50-68
+      char path[64];
+      std::snprintf(path, sizeof path, "parcels_%05d_%05lld.dat", rank, num);
+      std::ifstream f(path);
+      if (!f) break;
+      files.push_back(path);
+    }
+    if (files.empty()) {
+      std::fprintf(stderr, "there is no file to restart from (parcels_00000_%05lld.dat)\n", num);
+      return (int)PMPIC_ERR_CONFIG;
+    }
+    std::printf("Found %zu files\n", files.size());
+    if (s.dry_run) return 0;
+    int rc = ensure_context(s);
+    for (size_t r = 0; r < files.size() && !rc; ++r) {  // :111-117
+      double t = 0.0;
+      rc = check(s, pmpic_read_parcels(s.gpu, files[r].c_str(), r > 0 ? 1 : 0, &t), files[r].c_str());
+      if (!rc) s.time = t;  // read_file :220
+    }
+    return rc;
+  };
+  v.push_back(restart);
   v.push_back(writer("writebinary", false));
   v.push_back(writer("writenetcdf", true));
   v.push_back(gpu_component("vort2vel", pmpic_vort2vel));

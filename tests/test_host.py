@@ -135,3 +135,25 @@ def test_two_integrators_are_refused(tmp_path):
 def test_unknown_writer_mode_is_refused(tmp_path):
     p = run(f"--config={_ref_set(tmp_path, 'writenetcdf_mode=sometimes\n')}", "--dry-run", check=False)
     assert p.returncode != 0 and "not recognised" in p.stderr
+
+
+def test_restart_counts_the_rank_files(tmp_path):
+    """readfromfile_parcelsetup (readfromfile_parcelsetup.F90:50-68): the dumps of
+    step restart_num are found rank by rank until one is missing; none is an error."""
+    cfg = _ref_set(tmp_path, "plume_parcelsetup_enabled=.false.\nreadfromfile_parcelsetup_enabled=.true.\n"
+                             "restart_num=7\n")
+
+    def host():
+        return subprocess.run([MONC, f"--config={cfg}", "--dry-run"], capture_output=True, text=True,
+                              timeout=60, cwd=tmp_path)
+
+    p = host()
+    assert p.returncode != 0 and "no file to restart from" in p.stderr
+    for rank in (0, 1):
+        (tmp_path / f"parcels_{rank:05d}_00007.dat").write_bytes(b"")
+    (tmp_path / "parcels_00003_00007.dat").write_bytes(b"")  # after a gap: not part of the dump
+    p = host()
+    assert p.returncode == 0, p.stderr
+    assert "Found 2 files" in p.stdout
+    init = p.stdout.split("init:")[1].split("\n")[0].split()
+    assert init[:2] == ["parcelsetup_base", "readfromfile_parcelsetup"]
