@@ -344,6 +344,13 @@ int pmpic_setup_thermal(const pmpic_thermal_params* prm, int64_t n,
  * count is pmpic_setup_count(prm). */
 int pmpic_setup_thermal_device(pmpic_ctx* ctx, const pmpic_thermal_params* prm);
 
+/* basic_parcelsetup initialisation (basic_parcelsetup.F90:22-134), one
+ * process, written on the device into the context's parcel state (either
+ * form), replacing it: parcels_per_cell_dir^3 parcels per cell at the centres
+ * of a regular sub-lattice, cell by cell (x outer, z inner), vol = 1, the
+ * other properties zero.  PMPIC_ERR_CAPACITY if they exceed max_parcels. */
+int pmpic_setup_basic(pmpic_ctx* ctx, int32_t parcels_per_cell_dir);
+
 /* plume_parcelsetup initialisation (plume_parcelsetup.F90:58-334), one
  * process, written on the device into the context's parcel state (either
  * form), replacing it.  Plume parcels (4^3 per cell on a lattice, inside a

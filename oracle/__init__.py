@@ -76,6 +76,7 @@ def lib():
         L.orc_kx_ky_k2.argtypes = [P, D, D, D, D]
         L.orc_prescribed_velocity.argtypes = [P, C.c_int]
         L.orc_plume_setup.argtypes = [P, D, C.POINTER(C.c_int64)]
+        L.orc_basic_setup.argtypes = [P, C.c_int]
         for n in ["orc_parcel_haloswap", "orc_vort2vel", "orc_vort2vel_grids", "orc_vorticity_tendency",
                   "orc_rk4_integrator", "orc_parcel_splitting", "orc_parcel_mixing", "orc_step",
                   "orc_euler_integrator", "orc_prescribed_velocity_tag"]:
@@ -277,6 +278,11 @@ class Oracle:
 
     def prescribed_velocity_tag(self):
         self._check(lib().orc_prescribed_velocity_tag(self._h))
+
+    # -- basic_parcelsetup.F90:22-134 ----------------------------------------
+    def setup_basic(self, n_per_dir=2):
+        """Replace the parcels with the reference's regular lattice set-up."""
+        self._check(lib().orc_basic_setup(self._h, int(n_per_dir)))
 
     # -- plume_parcelsetup.F90:58-334 -----------------------------------------
     def setup_plume(self, lam=1.0, H=0.8, z_c=2.5, mu=0.9, z_d=4.0, z_m=5.0, r_plume=0.8,

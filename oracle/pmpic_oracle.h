@@ -117,6 +117,9 @@ int orc_prescribed_velocity_tag(orc_ctx*);
  * process: prm = {lambda, H, z_c, mu, z_d, z_m, r_plume, e_values(1:3)};
  * replaces the parcels; *n_plume = the parcels of the plume (slots first). */
 int orc_plume_setup(orc_ctx*, const double* prm, int64_t* n_plume);
+/* basic_parcelsetup initialisation (basic_parcelsetup.F90:22-134), one
+ * process: n_per_dir^3 parcels per cell on a regular sub-lattice, vol = 1. */
+int orc_basic_setup(orc_ctx*, int n_per_dir);
 
 /* Component iteration counters (vort2vel, vorticity_tendency, rk4 stage,
  * splitting, mixing), for re-synchronising with another implementation. */

@@ -169,6 +169,7 @@ def lib() -> C.CDLL:
         L.pmpic_setup_thermal.argtypes = [C.POINTER(ThermalParams), I64] + [D] * 11
         L.pmpic_setup_thermal_device.argtypes = [P, C.POINTER(ThermalParams)]
         L.pmpic_setup_plume.argtypes = [P, C.POINTER(PlumeParams), C.POINTER(I64)]
+        L.pmpic_setup_basic.argtypes = [P, C.c_int32]
         _lib = L
     return _lib
 
@@ -409,6 +410,11 @@ class Context:
         n_plume = C.c_int64(0)
         self._check(lib().pmpic_setup_plume(self._h, C.byref(prm), C.byref(n_plume)))
         return n_plume.value
+
+    def setup_basic(self, parcels_per_cell_dir=2):
+        """basic_parcelsetup: a regular sub-lattice of parcels_per_cell_dir^3 parcels
+        per cell, vol = 1, written on the device."""
+        self._check(lib().pmpic_setup_basic(self._h, int(parcels_per_cell_dir)))
 
     def setup_thermal(self, **kw):
         """The jittered thermal of thermal_parcels(**kw), written on the device."""

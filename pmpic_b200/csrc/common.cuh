@@ -378,6 +378,7 @@ int euler_step(pmpic_ctx* ctx);
 int prescribed_velocity(pmpic_ctx* ctx, int profile, bool tags);
 int setup_plume(pmpic_ctx* ctx, const pmpic_plume_params* prm, int64_t* n_plume);
 int setup_thermal_device(pmpic_ctx* ctx, const pmpic_thermal_params* prm);
+int setup_basic(pmpic_ctx* ctx, int n_per_dir);
 int flush_gathers(pmpic_ctx* ctx);
 int sync_info(pmpic_ctx* ctx);
 }  // namespace pmpic

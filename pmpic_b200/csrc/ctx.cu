@@ -730,6 +730,9 @@ int pmpic_setup_plume(pmpic_ctx* ctx, const pmpic_plume_params* prm, int64_t* n_
   if (!prm) return PMPIC_ERR_ARG;
   PMPIC_ENTRY(setup_plume(ctx, prm, n_plume))
 }
+int pmpic_setup_basic(pmpic_ctx* ctx, int32_t parcels_per_cell_dir) {
+  PMPIC_ENTRY(setup_basic(ctx, parcels_per_cell_dir))
+}
 int pmpic_setup_thermal_device(pmpic_ctx* ctx, const pmpic_thermal_params* prm) {
   if (!prm) return PMPIC_ERR_ARG;
   PMPIC_ENTRY(setup_thermal_device(ctx, prm))

@@ -1,8 +1,10 @@
 // setup.cu -- parcel initial conditions generated on the device.
 //
-// Two set-up components write the context's parcel state directly in HBM (FP64
+// Set-up components write the context's parcel state directly in HBM (FP64
 // or the mixed form's cell index + FP32 offset), so that a 10^8-parcel start
 // is not bound by host generation and a PCIe upload:
+//  * the reference's basic_parcelsetup (basic_parcelsetup.F90:22-134): a
+//    regular sub-lattice of n^3 parcels per cell, vol = 1;
 //  * the reference's plume_parcelsetup (plume_parcelsetup.F90:58-334): a
 //    spherical plume on a 4^3-per-cell lattice and the environment on a
 //    2^3-per-cell lattice outside it, in the reference's slot order;
@@ -157,6 +159,39 @@ __global__ void k_thermal(pmpic_thermal_params prm, ThermalGeom tg, int64_t n, P
   out.put(PMPIC_PROP_H, t, p.h);
   out.put(PMPIC_PROP_VOL, t, tg.v0);
   out.put(PMPIC_PROP_TAG, t, (double)t);
+}
+
+// basic_parcelsetup (basic_parcelsetup.F90:91-115), one thread per parcel in
+// the reference's order (cell by cell, x outer, then the sub-lattice, x
+// outer); x_coords(n) = pxmin + (n - 1) dx + bottom as in
+// parcel_interpolation.F90:126-136, interior cells from index 3 in x and y
+// (halo 2) and 1 in z
+struct BasicLattice {
+  int Nx, Ny, Nz, s;
+  double pxmin, pymin, pzmin, dx, dy, dz, bx, by, bz;
+};
+__device__ __forceinline__ double lattice_coord(double pmin, int n, double d, double b) {
+  return pmin + (double)(n - 1) * d + b;
+}
+__global__ void k_basic(BasicLattice L, int64_t n, ParcelSink out) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int64_t per_cell = (int64_t)L.s * L.s * L.s;
+  const int64_t cell = t / per_cell;
+  const int w = (int)(t - cell * per_cell);
+  const int i = (int)(cell / ((int64_t)L.Ny * L.Nz)) + 3;
+  const int j = (int)((cell / L.Nz) % L.Ny) + 3;
+  const int k = (int)(cell % L.Nz) + 1;
+  const int ii = w / (L.s * L.s), jj = (w / L.s) % L.s, kk = w % L.s;
+  const double xi = lattice_coord(L.pxmin, i, L.dx, L.bx), yj = lattice_coord(L.pymin, j, L.dy, L.by);
+  const double zk = lattice_coord(L.pzmin, k, L.dz, L.bz);
+  const double ddx = (lattice_coord(L.pxmin, i + 1, L.dx, L.bx) - xi) / L.s;
+  const double ddy = (lattice_coord(L.pymin, j + 1, L.dy, L.by) - yj) / L.s;
+  const double ddz = (lattice_coord(L.pzmin, k + 1, L.dz, L.bz) - zk) / L.s;
+  out.put(PMPIC_PROP_X, t, xi + ddx / 2 + (double)ii * ddx);
+  out.put(PMPIC_PROP_Y, t, yj + ddy / 2 + (double)jj * ddy);
+  out.put(PMPIC_PROP_Z, t, zk + ddz / 2 + (double)kk * ddz);
+  out.put(PMPIC_PROP_VOL, t, 1.0);
 }
 
 // a new state of n parcels whose properties `set` were written on the device:
@@ -327,6 +362,25 @@ int setup_plume(pmpic_ctx* ctx, const pmpic_plume_params* prm, int64_t* n_plume_
   rc = finish_state(ctx, n, {PMPIC_PROP_X, PMPIC_PROP_Y, PMPIC_PROP_Z, PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_VOL});
   if (!rc && n_plume_out) *n_plume_out = n_plume;
   return rc;
+}
+
+// basic_parcelsetup initialisation (basic_parcelsetup.F90:22-134), one process
+int setup_basic(pmpic_ctx* ctx, int n_per_dir) {
+  if (n_per_dir <= 0) return set_error(ctx, PMPIC_ERR_ARG, "basic set-up: parcels_per_cell_dir must be positive");
+  const Geom& g = ctx->g;
+  const int64_t n = (int64_t)n_per_dir * n_per_dir * n_per_dir * g.ncell;  // :53-57
+  if (n > ctx->cap)                                                      // :63-65
+    return set_error(ctx, PMPIC_ERR_CAPACITY, "Maxparcels is not big enough for the number of parcels per cell requested");
+  BasicLattice L;
+  L.Nx = g.Nx; L.Ny = g.Ny; L.Nz = g.Nz; L.s = n_per_dir;
+  L.pxmin = g.pxmin; L.pymin = g.pymin; L.pzmin = g.pzmin;
+  L.dx = g.dx; L.dy = g.dy; L.dz = g.dz;
+  L.bx = ctx->cfg.xmin; L.by = ctx->cfg.ymin; L.bz = ctx->cfg.zmin;
+  if (n > 0) {
+    k_basic<<<nblk(n, 256), 256, 0, ctx->stream>>>(L, n, sink_of(ctx)); ++ctx->nlaunch;
+    PMPIC_CUDA(cudaGetLastError());
+  }
+  return finish_state(ctx, n, {PMPIC_PROP_X, PMPIC_PROP_Y, PMPIC_PROP_Z, PMPIC_PROP_VOL});
 }
 
 // the jittered thermal of pmpic_setup_thermal, written on the device

@@ -320,6 +320,16 @@ static std::vector<ComponentDescriptor> all_components() {
                  "prescribed_velocity");
   };
   v.push_back(pv);
+  // basic_parcelsetup (basic_parcelsetup.F90:22-134), written on the device
+  ComponentDescriptor basic;
+  basic.name = "basic_parcelsetup";
+  basic.initialisation = [](State& s) {
+    if (s.dry_run) return 0;
+    int rc = ensure_context(s);
+    if (rc) return rc;
+    return check(s, pmpic_setup_basic(s.gpu, (int32_t)s.options.integer("parcels_per_cell_dir")), "basic_parcelsetup");
+  };
+  v.push_back(basic);
   // plume_parcelsetup (plume_parcelsetup.F90:58-334), written on the device
   ComponentDescriptor plume;
   plume.name = "plume_parcelsetup";

@@ -1,7 +1,8 @@
 """Initial conditions written on the device.
 
-plume_parcelsetup (plume_parcelsetup.F90:58-334): the oracle's restatement
-against an independent numpy statement of the same loops (CPU), then the
+basic_parcelsetup (basic_parcelsetup.F90:22-134) and plume_parcelsetup
+(plume_parcelsetup.F90:58-334): the oracle's restatements against independent
+numpy statements of the same loops (CPU), then the
 device set-up against the oracle, bit for bit, for both forms (GPU).  The
 jittered thermal of the benchmark workloads: the device generator against the
 host one (GPU).
@@ -154,6 +155,70 @@ def test_device_plume_then_steps_vs_oracle(pm):
     for k in ["x", "y", "z", "p", "q", "r"]:
         a, b = g.get(k), o.get(k)
         assert np.max(np.abs(a - b)) <= 1e-12 * max(1.0, np.max(np.abs(b))), k
+
+
+def numpy_basic(nx, ny, nz, lx, ly, lz, s):
+    """basic_parcelsetup.F90:91-115 on [0, lx) x [0, ly) x [0, lz] (one process),
+    parcel t decoded as cell t // s^3 (x outer, z inner) and sub-lattice point
+    t % s^3 (x outer), with x_coords(n) = -2 dx + (n - 1) dx + 0."""
+    dx, dy, dz = lx / nx, ly / ny, lz / nz
+    t = np.arange(nx * ny * nz * s ** 3)
+    cell, w = t // s ** 3, t % s ** 3
+    i, j, k = cell // (ny * nz) + 3, (cell // nz) % ny + 3, cell % nz + 1
+    ii, jj, kk = w // (s * s), (w // s) % s, w % s
+
+    def coord(pmin, n, d):
+        return pmin + (n - 1).astype(np.float64) * d + 0.0
+
+    out = {}
+    for key, pmin, d, idx, sub in [("x", -2.0 * dx, dx, i, ii), ("y", -2.0 * dy, dy, j, jj),
+                                   ("z", 0.0 * dz + 0.0, dz, k, kk)]:
+        c0 = coord(pmin, idx, d)
+        step = (coord(pmin, idx + 1, d) - c0) / s
+        out[key] = c0 + step / 2 + sub.astype(np.float64) * step
+    out["vol"] = np.ones(len(t))
+    return out
+
+
+@pytest.mark.parametrize("s", [1, 2, 3])
+def test_oracle_basic_vs_numpy(s):
+    from oracle import Oracle, OracleError
+    grid = (16, 12, 8, 2 * math.pi, 5.0, math.pi)
+    want = numpy_basic(*grid, s)
+    o = Oracle(*grid, max_parcels=len(want["x"]))
+    o.setup_basic(s)
+    assert o.n == len(want["x"])
+    for k, v in want.items():
+        np.testing.assert_array_equal(o.get(k), v, err_msg=k)
+    for k in ["p", "q", "r", "b", "h", "stretch", "tag"]:
+        assert np.all(o.get(k) == 0.0)
+    with pytest.raises(OracleError):
+        Oracle(*grid, max_parcels=len(want["x"]) - 1).setup_basic(s)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("s", [2, 3])
+def test_device_basic_vs_oracle(pm, s):
+    from oracle import Oracle
+    grid = (16, 12, 8, 2 * math.pi, 5.0, math.pi)
+    cap = 16 * 12 * 8 * s ** 3
+    o = Oracle(*grid, max_parcels=cap)
+    o.setup_basic(s)
+    g = pm.Context(*grid, max_parcels=cap)
+    g.setup_basic(s)
+    assert g.n == o.n
+    for k in IO:
+        np.testing.assert_array_equal(g.get(k), o.get(k), err_msg=k)
+    m = pm.Context(*grid, max_parcels=cap, precision="mixed")
+    u = pm.Context(*grid, max_parcels=cap, precision="mixed")
+    m.setup_basic(s)
+    u.upload(**{k: o.get(k) for k in IO})
+    for k in IO:
+        np.testing.assert_array_equal(m.get(k), u.get(k), err_msg=k)
+    with pytest.raises(pm.PmpicError):
+        pm.Context(*grid, max_parcels=cap - 1).setup_basic(s)
+    for c in (g, m, u):
+        c.close()
 
 
 THERMAL = dict(nx=24, ny=20, nz=12, lx=2 * math.pi, ly=5.0, lz=math.pi, seed=11)
