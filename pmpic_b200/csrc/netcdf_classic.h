@@ -44,12 +44,12 @@ class NcClassicWriter {
   // write the header for numrecs records; false if the file cannot be written
   // or a variable is too large for the format (vsize must fit in 32 bits)
   bool begin(const char* path, int64_t numrecs) {
-    f_ = std::fopen(path, "wb");
-    if (!f_) return false;
     numrecs_ = numrecs;
     if (numrecs < 0 || numrecs > INT32_MAX) return fail();
     for (const Var& v : vars_)
       if (v.vsize > (int64_t)UINT32_MAX - 3) return fail();
+    f_ = std::fopen(path, "wb");
+    if (!f_) return false;
     // two passes: sizes first, then the offsets are known
     std::vector<uint8_t> h;
     header(h);

@@ -270,6 +270,7 @@ int setup_plume(pmpic_ctx* ctx, const pmpic_plume_params* prm, int64_t* n_plume_
   };
   const int64_t kpl = in_box ? (int64_t)std::ceil(2. * r_plume / dzplume) : 0;
   const int64_t kbg = (int64_t)(g.nzp - 1) * n_bg;
+  if (kpl > (1 << 30)) return set_error(ctx, PMPIC_ERR_ARG, "plume set-up: lattice too large");
   std::vector<double> tab;
   size_t o_xpl = tab.size();
   walk(xmin_local + dxplume / 2., dxplume, (int64_t)g.Nx * n_pl, tab);
@@ -295,7 +296,6 @@ int setup_plume(pmpic_ctx* ctx, const pmpic_plume_params* prm, int64_t* n_plume_
       tab[o_hbg + k] = rhb * std::exp(-z / lambda);
     }
   }
-  if (kpl > (1 << 30)) return set_error(ctx, PMPIC_ERR_ARG, "plume set-up: lattice too large");
 
   PlumeLattice L;
   L.npl = in_box ? (int64_t)g.Nx * n_pl * g.Ny * n_pl : 0;

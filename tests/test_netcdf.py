@@ -92,6 +92,7 @@ def test_variable_beyond_the_format_limit_is_refused(tmp_path):
     rc = pm.lib().pmpic_netcdf_write_grids(str(tmp_path / "big.nc").encode(), 1024, 1024, 1024, 1.0, 1.0, 1.0,
                                            0.0, 0, 0.0, ptrs)
     assert rc != 0
+    assert not (tmp_path / "big.nc").exists()
 
 
 @pytest.fixture(scope="module")
