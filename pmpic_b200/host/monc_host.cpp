@@ -306,6 +306,11 @@ static std::vector<ComponentDescriptor> all_components() {
   ComponentDescriptor pv;
   pv.name = "prescribed_parcel_velocity";
   pv.initialisation = [](State& s) {
+    const long long profile = s.options.integer("velocity_profile", -1);
+    if (profile < PMPIC_VELOCITY_SHEAR || profile > PMPIC_VELOCITY_EVACUATE) {
+      std::fprintf(stderr, "prescribed_parcel_velocity: velocity_profile %lld is not one of 0..10\n", profile);
+      return (int)PMPIC_ERR_CONFIG;
+    }
     if (s.dry_run) return 0;
     int rc = ensure_context(s);
     if (!rc && s.iterations == 0) rc = check(s, pmpic_prescribed_velocity_tag(s.gpu), "prescribed_velocity_tag");
@@ -334,9 +339,6 @@ static std::vector<ComponentDescriptor> all_components() {
   ComponentDescriptor plume;
   plume.name = "plume_parcelsetup";
   plume.initialisation = [](State& s) {
-    if (s.dry_run) return 0;
-    int rc = ensure_context(s);
-    if (rc) return rc;
     const Options& o = s.options;
     pmpic_plume_params p{};
     p.lambda = o.real("lambda");
@@ -352,6 +354,9 @@ static std::vector<ComponentDescriptor> all_components() {
       return (int)PMPIC_ERR_CONFIG;
     }
     for (int i = 0; i < 3; ++i) p.e_values[i] = std::atof(e[i].c_str());
+    if (s.dry_run) return 0;
+    int rc = ensure_context(s);
+    if (rc) return rc;
     int64_t n_plume = 0;
     rc = check(s, pmpic_setup_plume(s.gpu, &p, &n_plume), "plume_parcelsetup");
     if (!rc) {

@@ -132,6 +132,13 @@ def test_two_integrators_are_refused(tmp_path):
     assert p.returncode != 0 and "another integrator" in p.stderr
 
 
+@pytest.mark.parametrize("extra,msg", [("e_values=0.3, -0.4\n", "e_values needs 3 values"),
+                                       ("velocity_profile=11\n", "not one of 0..10")])
+def test_bad_component_options_are_refused(tmp_path, extra, msg):
+    p = run(f"--config={_ref_set(tmp_path, extra)}", "--dry-run", check=False)
+    assert p.returncode != 0 and msg in p.stderr
+
+
 def test_unknown_writer_mode_is_refused(tmp_path):
     p = run(f"--config={_ref_set(tmp_path, 'writenetcdf_mode=sometimes\n')}", "--dry-run", check=False)
     assert p.returncode != 0 and "not recognised" in p.stderr
