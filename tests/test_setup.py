@@ -89,6 +89,21 @@ def test_oracle_plume_vs_numpy(grid):
     assert 0 < n_plume < n
 
 
+@pytest.mark.parametrize("cfg", [
+    dict(lam=0.8, H=0.7, z_c=2.5, mu=0.85, z_d=3.5, z_m=4.5, r_plume=0.5, e_values=(0.1, 0.2, -0.3)),
+    dict(lam=1.3, H=0.9, z_c=1.2, mu=0.95, z_d=2.0, z_m=2.6, r_plume=0.55, e_values=(-0.5, 0.0, 0.25)),
+])
+def test_oracle_plume_other_parameters_vs_numpy(cfg):
+    from oracle import Oracle
+    grid = (20, 16, 24, 5.0, 4.0, 3.5)
+    want, n_plume = numpy_plume(*grid, **cfg)
+    o = Oracle(*grid, max_parcels=len(want["x"]))
+    assert o.setup_plume(**cfg) == n_plume
+    for k, v in want.items():
+        np.testing.assert_array_equal(o.get(k), v, err_msg=k)
+    assert np.any(o.get("b")[n_plume:] > 0)  # part of the environment lies in the stratified layer
+
+
 def test_oracle_plume_parameter_checks():
     from oracle import Oracle, OracleError
     o = Oracle(16, 16, 16, 6.28, 6.28, 6.28, max_parcels=100000)
