@@ -164,3 +164,29 @@ def test_restart_counts_the_rank_files(tmp_path):
     assert "Found 2 files" in p.stdout
     init = p.stdout.split("init:")[1].split("\n")[0].split()
     assert init[:2] == ["parcelsetup_base", "readfromfile_parcelsetup"]
+
+
+CONFIGS = os.path.join(ROOT, "pmpic_b200", "host", "configs")
+
+
+def test_shipped_plume_configuration():
+    """pmpic_b200/host/configs/plume.mcf: plume set-up, the full integrator group
+    four times per step, both writers in the start group."""
+    out = run(f"--config={os.path.join(CONFIGS, 'plume.mcf')}", "--dry-run").stdout
+    init = out.split("init:")[1].split("\n")[0].split()
+    step = out.split("step:")[1].split("\n")[0].split()
+    assert init == ["parcelsetup_base", "plume_parcelsetup", "writebinary", "writenetcdf", "rk4_integrator"]
+    body = ["vort2vel", "vorticity_tendency", "rk4_integrator", "parcel_splitting", "parcel_mixing"]
+    assert step == ["writebinary", "writenetcdf", "termination_check"] + body * 4 + ["model_synopsis"]
+
+
+def test_shipped_migration_configuration():
+    """pmpic_b200/host/configs/migration.mcf: lattice set-up, prescribed velocity
+    then Euler once per step (grid2par.mcf's group order)."""
+    out = run(f"--config={os.path.join(CONFIGS, 'migration.mcf')}", "--dry-run").stdout
+    init = out.split("init:")[1].split("\n")[0].split()
+    step = out.split("step:")[1].split("\n")[0].split()
+    assert init == ["parcelsetup_base", "basic_parcelsetup", "writebinary", "writenetcdf",
+                    "prescribed_parcel_velocity", "euler_integrator"]
+    assert step == ["writebinary", "writenetcdf", "termination_check", "prescribed_parcel_velocity",
+                    "euler_integrator", "model_synopsis"]
