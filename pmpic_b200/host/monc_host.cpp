@@ -198,9 +198,20 @@ static int ensure_context(State& s) {
     return rc;
   }
   s.dtm = cfg.dtm;
+  // timer_mod (timer.F90:110-245): per-routine device times when timing_enabled
+  if (o.logical("timing_enabled", false)) return check(s, pmpic_timing(s.gpu, 1), "pmpic_timing");
   return 0;
 }
 static int release_context(State& s) {
+  if (s.gpu && s.options.logical("timing_enabled", false)) {
+    std::printf("%-20s %12s %10s\n", "routine", "total ms", "calls");
+    for (int id = 0; id < pmpic_timer_count(); ++id) {
+      double ms = 0.0;
+      int64_t calls = 0;
+      if (pmpic_timer_read(s.gpu, id, &ms, &calls) == 0 && calls > 0)
+        std::printf("%-20s %12.3f %10lld\n", pmpic_timer_name(id), ms, (long long)calls);
+    }
+  }
   if (s.gpu) pmpic_destroy(s.gpu);
   s.gpu = nullptr;
   return 0;
