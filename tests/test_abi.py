@@ -128,3 +128,76 @@ def test_bench_combine_two_ranks_gloo():
     res = sorted(q.get() for _ in range(2))
     for _, t, w in res:
         assert t == 2.0 and w == 300.0
+
+
+def _philox4x32_10(c, k0, k1):
+    """Philox4x32-10 (Salmon et al., SC'11) on numpy uint64 lanes holding 32-bit words."""
+    mask = np.uint64(0xFFFFFFFF)
+    c = [np.asarray(x, dtype=np.uint64) for x in c]
+    k0, k1 = np.uint64(k0), np.uint64(k1)
+    for _ in range(10):
+        p0 = np.uint64(0xD2511F53) * c[0]
+        p1 = np.uint64(0xCD9E8D57) * c[2]
+        c = [((p1 >> np.uint64(32)) ^ c[1] ^ k0) & mask, p1 & mask,
+             ((p0 >> np.uint64(32)) ^ c[3] ^ k1) & mask, p0 & mask]
+        k0 = (k0 + np.uint64(0x9E3779B9)) & mask
+        k1 = (k1 + np.uint64(0xBB67AE85)) & mask
+    return c
+
+
+def test_philox_known_answers():
+    """The generator's Philox4x32-10 against the known-answer vectors published
+    with the Random123 library (counter, key -> output)."""
+    cases = [([0, 0, 0, 0], (0, 0), [0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8]),
+             ([0xffffffff] * 4, (0xffffffff, 0xffffffff), [0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd]),
+             ([0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344], (0xa4093822, 0x299f31d0),
+              [0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1])]
+    for ctr, key, want in cases:
+        assert [int(x) for x in _philox4x32_10(ctr, *key)] == want
+
+
+def test_thermal_generator_vs_numpy():
+    """pmpic_setup_thermal (thermal.h) against an independent numpy statement of
+    the same stream and formula, bit for bit (glibc cos through math.cos)."""
+    import math
+    import pmpic_b200 as pm
+    nx, ny, nz, s, seed = 6, 5, 4, 2, (7 << 32) | 11
+    lx, ly, lz = 2 * np.pi, 5.0, np.pi
+    kw = dict(lx=lx, ly=ly, lz=lz, sub=s, jitter=0.25, seed=seed, xc=3.0, yc=2.4, zc=0.7, radius=0.9,
+              excess=1.5, h_in=0.9, h_env0=0.3, z_strat=1.1, n2=1.2)
+    got = pm.thermal_parcels(nx, ny, nz, **kw)
+    idx = np.arange(nx * ny * nz * s ** 3, dtype=np.uint64)
+    lo, hi = idx & np.uint64(0xFFFFFFFF), idx >> np.uint64(32)
+    k0, k1 = seed & 0xFFFFFFFF, seed >> 32
+    zero, one = np.zeros_like(idx), np.ones_like(idx)
+    c1 = _philox4x32_10([lo, hi, zero, zero], k0, k1)
+    c2 = _philox4x32_10([lo, hi, one, zero], k0, k1)
+
+    def u01(a, b):
+        v = ((a << np.uint64(21)) ^ (b >> np.uint64(11))) & np.uint64((1 << 53) - 1)
+        return v.astype(np.float64) * (1.0 / 9007199254740992.0)
+
+    jx = (2.0 * u01(c1[0], c1[1]) - 1.0) * 0.25
+    jy = (2.0 * u01(c1[2], c1[3]) - 1.0) * 0.25
+    jz = (2.0 * u01(c2[0], c2[1]) - 1.0) * 0.25
+    t = idx.astype(np.int64)
+    cell, w = t // s ** 3, t % s ** 3
+    i, j, k = cell // (ny * nz), (cell // nz) % ny, cell % nz
+    a, b, c = w // (s * s), (w // s) % s, w % s
+    dx, dy, dz = lx / nx, ly / ny, lz / nz
+    x = i * dx + (a + 0.5 + jx) * (dx / s)
+    y = j * dy + (b + 0.5 + jy) * (dy / s)
+    z = k * dz + (c + 0.5 + jz) * (dz / s)
+    rr = np.sqrt((x - 3.0) * (x - 3.0) + (y - 2.4) * (y - 2.4) + (z - 0.7) * (z - 0.7))
+    benv = np.where(z > 1.1, (z - 1.1) * 1.2, 0.0)
+    bb, hh = benv.copy(), 0.3 * (1.0 - z / lz)
+    pi = 4.0 * math.atan(1.0)
+    for e in np.nonzero(rr < 0.9)[0]:
+        cs = math.cos(pi * rr[e] / (2.0 * 0.9))
+        bb[e] = benv[e] + 1.5 * cs * cs
+        hh[e] = 0.9
+    want = {"x": x, "y": y, "z": z, "b": bb, "h": hh, "vol": np.full(len(t), dx * dy * dz / float(s ** 3)),
+            "tag": t.astype(np.float64)}
+    assert 0 < int((rr < 0.9).sum()) < len(t)
+    for key, v in want.items():
+        np.testing.assert_array_equal(got[key], v, err_msg=key)
