@@ -190,3 +190,11 @@ def test_shipped_migration_configuration():
                     "prescribed_parcel_velocity", "euler_integrator"]
     assert step == ["writebinary", "writenetcdf", "termination_check", "prescribed_parcel_velocity",
                     "euler_integrator", "model_synopsis"]
+
+
+def test_quoted_writer_modes_parse(tmp_path):
+    """The reference's config.mcf quotes string options (writebinary_mode="time")."""
+    extra = 'writebinary_mode="time"\nparcel_time_write_frequency=1.\ngrid_time_write_frequency=1.\n' \
+            'writenetcdf_mode="step"\nparcel_step_write_netcdf_frequency=10\ngrid_step_write_netcdf_frequency=5\n'
+    p = run(f"--config={_ref_set(tmp_path, extra)}", "--dry-run", check=False)
+    assert p.returncode == 0, p.stderr
