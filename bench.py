@@ -118,14 +118,17 @@ def dist_env():
 
 
 def cpu_reference(grid, steps, warmup, threads):
-    """The CPU restatement of the reference (oracle), timed on the host cores."""
-    import pmpic_b200 as pm
+    """The CPU restatement of the reference (oracle), timed on the host cores.
+    The initial condition is the oracle's own thermal generator (the same
+    parcels as the GPU path's, bit for bit), so nothing of the B200 library is
+    loaded on this leg."""
     from oracle import Oracle
-    ic = pm.thermal_parcels(grid, grid, grid, **PLUME)
-    n0 = len(ic["x"])
+    n0 = PLUME["sub"] ** 3 * grid ** 3
     o = Oracle(grid, grid, grid, PLUME["lx"], PLUME["ly"], PLUME["lz"], dtm=0.0025, dtmax=0.0025,
-               max_parcels=int(1.25 * n0), threads=threads)
-    o.set_parcels(**ic)
+               max_parcels=int(1.1 * n0), threads=threads)
+    o.setup_thermal(**{k: PLUME[k] for k in ("sub", "jitter", "seed", "xc", "yc", "zc", "radius", "excess",
+                                             "h_in", "h_env0", "z_strat", "n2")})
+    assert o.n == n0
     for _ in range(warmup):
         o.step()
     work = 0
@@ -134,6 +137,7 @@ def cpu_reference(grid, steps, warmup, threads):
         work += o.n
         o.step()
     dt = time.perf_counter() - t0
+    o.close()
     return work / dt, n0, dt
 
 
@@ -144,15 +148,16 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     grid = args.ref_grid
     value, n0, dt = cpu_reference(grid, args.steps, args.warmup, threads)
-    sample = (f"{grid}^3 plume ({n0} parcels, same thermal and environment), {args.steps} timed steps "
-              f"after {args.warmup} warm-up; C++ restatement of the reference Fortran (no Fortran "
-              f"compiler or MPI here to build the reference itself)")
+    sample = (f"{grid}^3 plume ({n0} parcels, the same thermal and environment as the GPU arm), "
+              f"{args.steps} timed steps after {args.warmup} warm-up; C++/OpenMP restatement of the "
+              f"reference Fortran (no Fortran compiler or MPI here to build the reference itself)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": f"thermal plume {grid}^3 sample of the 256^3 plume, FP64, 8 parcels/cell",
-                       "grid": grid, "parcels": n0, "dt": 0.0025},
+            "config": {"workload": f"thermal plume {grid}^3, FP64, 8 parcels/cell; 4 RK4 substeps + "
+                                   f"splitting + mixing per step",
+                       "grid": grid, "parcels_initial": n0, "dt": 0.0025, "precision": "fp64"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -271,11 +276,24 @@ def run_form(precision, args, local, pg, headline):
         "avg_launch_ms": tot / calls if calls else None,
         "algorithmic_bytes_per_launch": total_bytes / calls if calls else None}
 
-    # untimed continuation to args.error_steps, then the gridded velocity
+    # the continuation to args.error_steps, timed as a second window (the
+    # parcels have drifted from their set-up order and splitting has appended),
+    # then the gridded velocity
     done = args.warmup + args.steps
+    late_work, late_steps = 0, 0
+    L.pmpic_event_record(h, 6)
     while done < args.error_steps:
+        late_work += ctx.n
         ctx.step(1)
         done += 1
+        late_steps += 1
+    L.pmpic_event_record(h, 7)
+    if late_steps:
+        ms_late = C.c_float()
+        L.pmpic_event_elapsed(h, 6, 7, C.byref(ms_late))
+        t_late, late_all = combine(ms_late.value / 1e3, late_work, pg, "cuda")
+        res["late_run"] = {"steps": f"{args.warmup + args.steps + 1}-{done}", "value": late_all / t_late,
+                           "ms_per_step": 1e3 * t_late / late_steps, "unit": UNIT}
     res["steps_total"] = done
     res["n_final"] = ctx.n
     res["grids"] = {q: ctx.grid(q) for q in ("u", "v", "w")} if args.error_steps > 0 else None
@@ -363,9 +381,10 @@ def run_b200(args):
     cpu = None
     if rank == 0 and world == 1 and args.cpu_baseline:
         threads = os.cpu_count() or 1
-        v, n_s, dt = cpu_reference(args.ref_grid, 1, 0, threads)
+        v, n_s, dt = cpu_reference(args.ref_grid, 1, 1, threads)
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"{args.ref_grid}^3 plume ({n_s} parcels), 1 step, C++ restatement of the reference"}
+               "sample": f"{args.ref_grid}^3 plume ({n_s} parcels, the GPU arm's initial state), 1 timed "
+                         f"step after 1 warm-up step ({dt:.1f} s), C++/OpenMP restatement of the reference"}
     if pg:
         pg.barrier()
     if rank == 0:
@@ -383,11 +402,13 @@ def run_b200(args):
                            "precision": headline, "parallelism": f"replicas x{world}",
                            "l2": "inputs larger than L2 (parcel state {:.0f} GB)".format(hr["n0"] * 30 * 8 / 1e9)},
                 "roofline": hr["roofline"], "cpu_baseline": cpu, "e2e": hr.get("e2e"),
-                "gpu_launches": hr["gpu_launches"], "clocks": hr["clocks"], "timers_ms": hr["timers_ms"]}
+                "gpu_launches": hr["gpu_launches"], "clocks": hr["clocks"], "timers_ms": hr["timers_ms"],
+                "late_run": hr.get("late_run")}
         if "fp64" in res and headline != "fp64":
             f = res["fp64"]
             line["fp64"] = {"value": f["value"], "ms_per_step": f["ms_per_step"], "roofline": f["roofline"],
-                            "gpu_launches": f["gpu_launches"], "clocks": f["clocks"], "timers_ms": f["timers_ms"]}
+                            "gpu_launches": f["gpu_launches"], "clocks": f["clocks"], "timers_ms": f["timers_ms"],
+                            "late_run": f.get("late_run")}
             line["mixed_over_fp64"] = hr["value"] / f["value"]
         line["error_vs_fp64"] = err
         print(json.dumps(line), flush=True)
@@ -673,7 +694,8 @@ def main():
     ap.add_argument("--grid", type=int, default=256)
     ap.add_argument("--capacity", type=float, default=2.25, help="max_parcels / initial parcels")
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--ref-grid", type=int, default=128)
+    ap.add_argument("--ref-grid", type=int, default=256,
+                    help="grid of the CPU legs (the reference arm and cpu_baseline)")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
                     help="both: time FP64 then the mixed form (the headline value), and compare them")

@@ -52,7 +52,7 @@ extern "C" {
 /* ---- precision forms ---------------------------------------------------- */
 #define PMPIC_FP64  0            /* plain FP64 throughout (the reference's DEFAULT_PRECISION) */
 #define PMPIC_MIXED 1            /* FP32 fields, grids, transforms and RK4; positions as integer cell
-                                    index + FP32 offset; FP64 zero mode and conserved sums */
+                                    index + FP32 offset; FP64 zero mode */
 
 /* ---- parcel property ids (parcels.F90:19-34) ----------------------------- */
 enum {
@@ -208,23 +208,25 @@ int pmpic_op_vort2vel_grids(pmpic_ctx* ctx);
  * temporary device buffer of n doubles. */
 int pmpic_sort_parcels(pmpic_ctx* ctx);
 
-/* par2grid without a context and without allocation./* par2grid without a context and without allocation.  No counterpart in the
+/* par2grid without a context and without allocation.  No counterpart in the
  * reference: an addition for callers that cannot allocate device memory at call
  * time.  Same arithmetic and result as pmpic_op_par2grid (binning
  * parcel_interpolation.F90:186-262, par2grid :336-481) of one field with volume
- * weights over an nx x ny x nz box [0,lx) x [0,ly) x [0,lz].  x, y, z, vol,
- * field are n device doubles; out receives the dense (nz+1) x ny x nx grid on
- * the device.  Scratch is one fixed static device array (about 7 MB per
- * device): n <= 131072, nx*ny*nz <= 32768 and ceil(nz/16)*nx*ny <= 4096,
- * else PMPIC_ERR_TOO_LARGE with
- * nothing launched.  The call clears its own counters, runs on `stream`
- * (a cudaStream_t; NULL = the legacy default stream) and synchronizes it before
- * returning; PMPIC_ERR_OUT_OF_BOX if a parcel is outside the box.
+ * weights over an nx x ny x nz box, x in [0,lx), y in [0,ly), z in [0,lz) (the
+ * reference's binning rule k < nz rejects z = lz).  nx, ny >= 4 and nz >= 3,
+ * as pmpic_create requires, else PMPIC_ERR_ARG.  x, y, z, vol, field are n
+ * device doubles; out receives the dense (nz+1) x ny x nx grid on the device.
+ * Scratch is one fixed static device array (about 7 MB per device):
+ * n <= 131072, nx*ny*nz <= 32768 and ceil(nz/16)*nx*ny <= 4096, else
+ * PMPIC_ERR_TOO_LARGE with nothing launched.  The call clears its own counters,
+ * runs on `stream` (a cudaStream_t; NULL = the legacy default stream) and
+ * synchronizes that stream before returning; PMPIC_ERR_OUT_OF_BOX if a parcel
+ * is outside the box.
  *  - Calls that overlap on one device share the scratch and race: serialize
  *    them (one stream, or synchronize between calls).
- *  - The first call on a device, with that device current, looks up the
- *    scratch address (cudaGetSymbolAddress); make it before capturing the
- *    stream into a graph. */
+ *  - The first call on a device, made with that device current, looks up the
+ *    scratch array's device address (cudaGetSymbolAddress); make that first
+ *    call before any stream capture begins. */
 int pmpic_par2grid_static(int32_t nx, int32_t ny, int32_t nz, double lx, double ly, double lz,
                           int64_t n, const double* x, const double* y, const double* z,
                           const double* vol, const double* field, double* out, void* stream);

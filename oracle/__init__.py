@@ -77,6 +77,7 @@ def lib():
         L.orc_prescribed_velocity.argtypes = [P, C.c_int]
         L.orc_plume_setup.argtypes = [P, D, C.POINTER(C.c_int64)]
         L.orc_basic_setup.argtypes = [P, C.c_int]
+        L.orc_thermal_setup.argtypes = [P, D, C.c_uint64]
         for n in ["orc_parcel_haloswap", "orc_vort2vel", "orc_vort2vel_grids", "orc_vorticity_tendency",
                   "orc_rk4_integrator", "orc_parcel_splitting", "orc_parcel_mixing", "orc_step",
                   "orc_euler_integrator", "orc_prescribed_velocity_tag"]:
@@ -283,6 +284,15 @@ class Oracle:
     def setup_basic(self, n_per_dir=2):
         """Replace the parcels with the reference's regular lattice set-up."""
         self._check(lib().orc_basic_setup(self._h, int(n_per_dir)))
+
+    # -- the benchmark workloads' jittered thermal (no reference counterpart) --
+    def setup_thermal(self, sub=2, jitter=0.25, seed=1, xc=3.141592653589793, yc=3.141592653589793, zc=0.6,
+                      radius=0.4, excess=1.0, h_in=0.95, h_env0=0.3, z_strat=1.2, n2=1.0):
+        """Replace the parcels with the jittered thermal, generated by the
+        oracle itself (Philox4x32-10 keyed by seed and parcel index)."""
+        prm = np.ascontiguousarray([sub, jitter, xc, yc, zc, radius, excess, h_in, h_env0, z_strat, n2],
+                                   dtype=np.float64)
+        self._check(lib().orc_thermal_setup(self._h, _dp(prm), int(seed)))
 
     # -- plume_parcelsetup.F90:58-334 -----------------------------------------
     def setup_plume(self, lam=1.0, H=0.8, z_c=2.5, mu=0.9, z_d=4.0, z_m=5.0, r_plume=0.8,

@@ -120,6 +120,12 @@ int orc_plume_setup(orc_ctx*, const double* prm, int64_t* n_plume);
 /* basic_parcelsetup initialisation (basic_parcelsetup.F90:22-134), one
  * process: n_per_dir^3 parcels per cell on a regular sub-lattice, vol = 1. */
 int orc_basic_setup(orc_ctx*, int n_per_dir);
+/* The jittered thermal of the benchmark workloads (no counterpart in the
+ * reference): prm = {sub, jitter, xc, yc, zc, radius, excess, h_in, h_env0,
+ * z_strat, n2}; sub^3 parcels per cell jittered by U(+-jitter) sub-spacings
+ * (Philox4x32-10 keyed by seed and parcel index), vol = cell volume / sub^3,
+ * tag = parcel index, b and h of the thermal and its environment. */
+int orc_thermal_setup(orc_ctx*, const double* prm, uint64_t seed);
 
 /* Component iteration counters (vort2vel, vorticity_tendency, rk4 stage,
  * splitting, mixing), for re-synchronising with another implementation. */

@@ -1008,7 +1008,8 @@ extern "C" int pmpic_par2grid_static(int32_t nx, int32_t ny, int32_t nz, double 
                                      int64_t n, const double* x, const double* y, const double* z,
                                      const double* vol, const double* field, double* out, void* stream) {
   using namespace pmpic;
-  if (nx < 1 || ny < 1 || nz < 1 || !(lx > 0) || !(ly > 0) || !(lz > 0) || n < 0 || !out) return PMPIC_ERR_ARG;
+  // the smallest box pmpic_create accepts (and the oracle restates)
+  if (nx < 4 || ny < 4 || nz < 3 || !(lx > 0) || !(ly > 0) || !(lz > 0) || n < 0 || !out) return PMPIC_ERR_ARG;
   if (n > 0 && (!x || !y || !z || !vol || !field)) return PMPIC_ERR_ARG;
   const int64_t ncell = (int64_t)nx * ny * nz;
   if (n > SP_MAX_PARCELS || ncell > SP_MAX_CELLS) return PMPIC_ERR_TOO_LARGE;

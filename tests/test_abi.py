@@ -201,3 +201,24 @@ def test_thermal_generator_vs_numpy():
     assert 0 < int((rr < 0.9).sum()) < len(t)
     for key, v in want.items():
         np.testing.assert_array_equal(got[key], v, err_msg=key)
+
+
+def test_oracle_thermal_generator_matches_host_generator():
+    """The oracle's own thermal set-up (the CPU legs' initial condition) gives
+    the same parcels as the library's host generator, bit for bit, so the CPU
+    baseline and the GPU arm start from the same state without the CPU legs
+    loading the library."""
+    import pmpic_b200 as pm
+    from oracle import Oracle
+    cases = [(6, 5, 4, dict(lx=2 * np.pi, ly=5.0, lz=np.pi, sub=2, jitter=0.25, seed=(7 << 32) | 11, xc=3.0,
+                            yc=2.4, zc=0.7, radius=0.9, excess=1.5, h_in=0.9, h_env0=0.3, z_strat=1.1, n2=1.2)),
+             (16, 16, 16, dict(lx=2 * np.pi, ly=2 * np.pi, lz=np.pi)),
+             (8, 8, 6, dict(lx=2 * np.pi, ly=2 * np.pi, lz=np.pi, sub=3, seed=5))]
+    for nx, ny, nz, kw in cases:
+        got = pm.thermal_parcels(nx, ny, nz, **kw)
+        o = Oracle(nx, ny, nz, kw["lx"], kw["ly"], kw["lz"], max_parcels=len(got["x"]) + 5)
+        o.setup_thermal(**{k: v for k, v in kw.items() if k not in ("lx", "ly", "lz")})
+        assert o.n == len(got["x"])
+        for key in ("x", "y", "z", "p", "q", "r", "b", "h", "vol", "stretch", "tag"):
+            np.testing.assert_array_equal(o.get(key), got[key], err_msg=key)
+        o.close()

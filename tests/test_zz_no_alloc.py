@@ -97,6 +97,9 @@ def test_static_par2grid_rejects_sizes_beyond_its_scratch():
     # more cells than the scratch holds (64 x 32 x 32 = 65536 > 32768)
     big = torch.zeros(33 * 32 * 64, dtype=torch.float64, device="cuda")
     assert L.pmpic_par2grid_static(64, 32, 32, 1.0, 1.0, 1.0, 10, *p, big.data_ptr(), None) == -10
+    # boxes below the smallest one pmpic_create accepts (4 x 4 x 3): argument errors
+    for shape in ((1, 1, 1), (2, 3, 1), (3, 4, 3), (4, 4, 2)):
+        assert L.pmpic_par2grid_static(*shape, 1.0, 1.0, 1.0, 10, *p, out.data_ptr(), None) == -8, shape
     assert torch.count_nonzero(out).item() == 0
 
 
