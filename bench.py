@@ -176,25 +176,33 @@ def algorithmic_bytes(kernel, precision, n_avg, nphys, calls, steps):
       q, r and their xo/xf copies, the six tendencies, the direction byte),
       the binning it gathers at (FP64: cell id + 3 offsets), and the six grids
       read once.  Stage 1 reads x, writes xo, xf, x; stages 2-3 read xo, xf,
-      write xf, x; stage 4 reads xf, writes xf, x.  The mixed form also writes
-      the next binning's cell id, and its last stage advances the stretch of
-      the split that follows (read + write).  Within pmpic_step stages 1-3
-      store no tendencies (dead until the next stage gathers them again).
+      write xf, x; stage 4 reads xf, writes xf, x.  On the mixed form the
+      current position is the cell id and three offsets (also the next
+      binning), xf a displacement from xo, and every stage reads the current
+      position for its gather (stages 2-4 read xo as well); its last stage
+      advances the stretch of the split that follows (read + write).  Within
+      pmpic_step stages 1-3 store no tendencies (dead until the next stage
+      gathers them again).
     """
     w = 8 if precision == "fp64" else 4
     if kernel == "par2grid":
         if precision == "fp64":
             b0, b1 = 92.0, 76.0   # 3 del + vol + p,q,r + b,h,z + btot out (+4 index); 3 del + vol + b,h,p,q,r
         else:
-            b0, b1 = 48.0, 40.0   # 3 offsets + vol + p,q,r + b,h + z cell + btot out (+4); 3 offsets + vol + b,h,p,q,r
+            b0, b1 = 44.0, 40.0   # 3 offsets + vol + p,q,r + b,h + btot out (+4 index); 3 offsets + vol + b,h,p,q,r
         per_step = 4 * (b0 * n_avg + 4 * w * nphys) + (b1 * n_avg + 6 * w * nphys)
         extra = max(calls - 5 * steps, 0) * (b1 * n_avg + 6 * w * nphys)
         return per_step * steps + extra
     if kernel == "rk4_kernel":
         if precision == "fp64":
             st = [76 + 145, 124 + 97, 124 + 97, 76 + 145]
-        else:  # positions: int cell + FP32 offset (8 B), the rest FP32; + cell id out; stage 4: stretch
-            st = [36 + 113, 96 + 77, 96 + 77, 64 + 105]
+        else:
+            # current position: cell id + 3 FP32 offsets (16 B, read at every
+            # stage for the gather, written as the next binning); xo: 3 x
+            # {int, FP32} (written at stage 1, read after); xf: 3 FP32
+            # displacements; p, q, r and their po/pf copies FP32; the
+            # direction byte; stage 4: the stretch and the six tendencies
+            st = [28 + 89, 76 + 53, 76 + 53, 68 + 81]
         return steps * sum(s_ * n_avg + 6 * w * nphys for s_ in st)
     return None
 
@@ -222,6 +230,8 @@ def run_form(precision, args, local, pg, headline):
     del ic
     L = pm.lib()
     h = ctx._h
+    if args.p2g_segment:
+        L.pmpic_set_p2g_segment(h, args.p2g_segment)
 
     def barrier():
         if pg:
@@ -697,6 +707,8 @@ def main():
     ap.add_argument("--ref-grid", type=int, default=256,
                     help="grid of the CPU legs (the reference arm and cpu_baseline)")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--p2g-segment", type=int, default=0,
+                    help="columns per x segment of the par2grid row pass (0: the library's default)")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
                     help="both: time FP64 then the mixed form (the headline value), and compare them")
     ap.add_argument("--error-steps", type=int, default=100,

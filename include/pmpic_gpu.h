@@ -94,6 +94,10 @@ typedef struct pmpic_step_info {
   int64_t n_removed;               /* nremove of the last mixing call */
   int64_t n_added;                 /* nadd of the last mixing call */
   int64_t n_migrated;              /* parcels re-slotted by the last parcel haloswap */
+  double vol_sum, hvol_sum, bvol_sum;  /* domain totals of vol, h*vol and b*vol over the parcels by a
+                                          compensated FP64 reduction (both forms), taken after each
+                                          acting mixing call and by pmpic_conserved_sums; the reference
+                                          checks mixing by them (parcel_mixing.F90:87-103, :409-418) */
   int32_t error;                   /* sticky device error word (PMPIC_ERR_*) */
   char message[160];
 } pmpic_step_info;
@@ -156,6 +160,12 @@ int pmpic_euler_integrator(pmpic_ctx* ctx);
 int pmpic_prescribed_velocity(pmpic_ctx* ctx, int profile);
 int pmpic_prescribed_velocity_tag(pmpic_ctx* ctx);
 int pmpic_get_step_info(pmpic_ctx* ctx, pmpic_step_info* info);
+/* The domain totals of vol, h*vol and b*vol over the current parcels now
+ * (sums[0..2]; also left in pmpic_step_info): every product split exactly and
+ * summed in double-double in a fixed order, so the result is the FP64 rounding
+ * of the exact total and repeats bit for bit.  The diagnostic sums around
+ * mixing of parcel_mixing.F90:87-103 and :409-418. */
+int pmpic_conserved_sums(pmpic_ctx* ctx, double sums[3]);
 
 /* Component iteration counters (vort2vel, vorticity_tendency, rk4 stage,
  * splitting, mixing) -- the modules' `iteration` / `rkstep` save variables. */

@@ -78,6 +78,7 @@ def lib():
         L.orc_plume_setup.argtypes = [P, D, C.POINTER(C.c_int64)]
         L.orc_basic_setup.argtypes = [P, C.c_int]
         L.orc_thermal_setup.argtypes = [P, D, C.c_uint64]
+        L.orc_conserved_sums.argtypes = [P, D]
         for n in ["orc_parcel_haloswap", "orc_vort2vel", "orc_vort2vel_grids", "orc_vorticity_tendency",
                   "orc_rk4_integrator", "orc_parcel_splitting", "orc_parcel_mixing", "orc_step",
                   "orc_euler_integrator", "orc_prescribed_velocity_tag"]:
@@ -172,6 +173,12 @@ class Oracle:
         s = StepInfo()
         lib().orc_get_step_info(self._h, C.byref(s))
         return s
+
+    def conserved_sums(self):
+        """(sum vol, sum h vol, sum b vol) over the parcels, compensated FP64."""
+        out = np.zeros(3)
+        self._check(lib().orc_conserved_sums(self._h, _dp(out)))
+        return tuple(float(v) for v in out)
 
     def counters(self):
         a = (C.c_int * 5)()

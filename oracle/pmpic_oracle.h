@@ -126,6 +126,9 @@ int orc_basic_setup(orc_ctx*, int n_per_dir);
  * (Philox4x32-10 keyed by seed and parcel index), vol = cell volume / sub^3,
  * tag = parcel index, b and h of the thermal and its environment. */
 int orc_thermal_setup(orc_ctx*, const double* prm, uint64_t seed);
+/* The domain totals of vol, h*vol and b*vol over the parcels (the diagnostic
+ * sums of parcel_mixing.F90:87-103, :409-418), compensated FP64. */
+int orc_conserved_sums(const orc_ctx*, double* out3);
 
 /* Component iteration counters (vort2vel, vorticity_tendency, rk4 stage,
  * splitting, mixing), for re-synchronising with another implementation. */

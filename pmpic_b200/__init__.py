@@ -49,7 +49,8 @@ class Config(C.Structure):
 class StepInfo(C.Structure):
     _fields_ = [("n_parcels", C.c_int64), ("dtm", C.c_double), ("limiter", C.c_int32),
                 ("n_split", C.c_int64), ("n_removed", C.c_int64), ("n_added", C.c_int64),
-                ("n_migrated", C.c_int64), ("error", C.c_int32), ("message", C.c_char * 160)]
+                ("n_migrated", C.c_int64), ("vol_sum", C.c_double), ("hvol_sum", C.c_double),
+                ("bvol_sum", C.c_double), ("error", C.c_int32), ("message", C.c_char * 160)]
 
 
 class ThermalParams(C.Structure):
@@ -113,6 +114,7 @@ def lib() -> C.CDLL:
         L.pmpic_step.argtypes = [P, C.c_int]
         L.pmpic_prescribed_velocity.argtypes = [P, C.c_int]
         L.pmpic_get_step_info.argtypes = [P, C.POINTER(StepInfo)]
+        L.pmpic_conserved_sums.argtypes = [P, C.POINTER(C.c_double)]
         L.pmpic_get_counters.argtypes = [P, C.POINTER(C.c_int32)]
         L.pmpic_set_counters.argtypes = [P, C.POINTER(C.c_int32)]
         L.pmpic_set_dtm.argtypes = [P, C.c_double]
@@ -368,6 +370,12 @@ class Context:
         s = StepInfo()
         self._check(lib().pmpic_get_step_info(self._h, C.byref(s)))
         return s
+
+    def conserved_sums(self):
+        """(sum vol, sum h vol, sum b vol) over the parcels now, compensated FP64."""
+        out = (C.c_double * 3)()
+        self._check(lib().pmpic_conserved_sums(self._h, out))
+        return tuple(out)
 
     def counters(self):
         a = (C.c_int32 * 5)()

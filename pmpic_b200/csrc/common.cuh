@@ -52,7 +52,26 @@ struct Geom {
   double xshift_e, xshift_w, yshift_n, yshift_s;
   double xc0, yc0, zc0;         // x_coords(1), y_coords(1), z_coords(1)
   double vmin;                  // dx*dy*dz/6/6/6 (parcel_mixing.F90:54)
+  double rNz, rNy;              // 1/Nz, 1/Ny (cell id decoding)
 };
+
+// Cell ids are z fastest: id = (i*Ny + j)*Nz + k.  Decoding divides by Nz and
+// Ny through the reciprocals (the product's quotient is exact or one off,
+// corrected by the remainder's sign).
+__device__ __forceinline__ void cell_decode(const Geom& g, int32_t id, int& i, int& j, int& k) {
+  int t = __double2int_rz((double)id * g.rNz);
+  int r = id - t * g.Nz;
+  if (r < 0) { --t; r += g.Nz; } else if (r >= g.Nz) { ++t; r -= g.Nz; }
+  k = r;
+  int q = __double2int_rz((double)t * g.rNy);
+  int s = t - q * g.Ny;
+  if (s < 0) { --q; s += g.Ny; } else if (s >= g.Ny) { ++q; s -= g.Ny; }
+  j = s;
+  i = q;
+}
+__host__ __device__ __forceinline__ int32_t cell_encode(const Geom& g, int i, int j, int k) {
+  return (int32_t)(((int64_t)i * g.Ny + j) * g.Nz + k);
+}
 
 // Interior cell id of a parcel and its fractional offsets, restating
 // cache_parcel_interp_weights (parcel_interpolation.F90:214-237) bit for bit:
@@ -92,11 +111,21 @@ __device__ __forceinline__ void count_cell(int32_t id, int32_t* __restrict__ cou
 }
 
 // ---- mixed-precision form --------------------------------------------------
-// A position component of the mixed form: the integer cell index along the axis
-// and the FP32 offset inside the cell in cell units, so x = (i + f) * dx.  It
-// fills the 8-byte slot an FP64 position takes on the plain path.  f lies in
-// [0, 1); the one exception is f = 1 in cell Nz-1, a parcel exactly on the top
-// wall (the reference bins z = zmax with delz = 1 in the last cell).
+// Positions of the mixed form are an integer cell index plus an FP32 offset
+// inside the cell in cell units, x = (i + f) * dx, so a parcel's absolute
+// position never loses bits as it moves.  Three arrays carry them:
+//  * the current position x, y, z (the reference's parcel x, y, z): the cell
+//    id in ctx->cell (i, j, k packed z fastest; x and y wrapped into the
+//    domain, z reflected at the walls) and the three offsets as FP32 in the
+//    X, Y, Z property slots.  f lies in [0, 1); the one exception is f = 1 in
+//    cell Nz-1, a parcel exactly on the top wall (the reference bins z = zmax
+//    with delz = 1 in the last cell).  The cell id is at once the binning of
+//    par2grid: the current cell is known wherever the position is.
+//  * xo, yo, zo, the RK4 step's start (rk4_integrator.F90:125-127): a CellOff
+//    {int32 index, FP32 offset} per axis in the 8-byte XO, YO, ZO slots, the
+//    index unwrapped (the parcel haloswap shifts it by whole periods);
+//  * xf, yf, zf as the FP32 displacement from xo in cell units (bounded by the
+//    step's motion, dt |u| / dx) in the XF, YF, ZF slots.
 struct __align__(8) CellOff {
   int32_t i;
   float f;
@@ -133,19 +162,43 @@ __device__ __forceinline__ CellOff co_reflect(CellOff a, int nz) {
   }
   return a;
 }
-// element size of a property on the mixed form: positions and tag 8 bytes, the rest FP32
+// an index wrapped into [0, n) (one period at most away on the path; any
+// integer here)
+__device__ __forceinline__ int wrap_index(int i, int n) {
+  if (i >= n) i -= n;
+  else if (i < 0) i += n;
+  if ((unsigned)i >= (unsigned)n) i = ((i % n) + n) % n;
+  return i;
+}
+// the storage kinds of the properties on the mixed form
+enum MixedKind {
+  MK_F32 = 0,  // FP32 value in the first half of the allocation
+  MK_CUR = 1,  // x, y, z: FP32 offset (with the cell id in ctx->cell)
+  MK_BASE = 2, // xo, yo, zo: CellOff in the 8-byte slot
+  MK_DISP = 3, // xf, yf, zf: FP32 displacement from xo in cell units
+  MK_F64 = 4   // tag: FP64
+};
+__host__ __device__ __forceinline__ int mixed_kind(int pid) {
+  switch (pid) {
+    case PMPIC_PROP_X: case PMPIC_PROP_Y: case PMPIC_PROP_Z: return MK_CUR;
+    case PMPIC_PROP_XO: case PMPIC_PROP_YO: case PMPIC_PROP_ZO: return MK_BASE;
+    case PMPIC_PROP_XF: case PMPIC_PROP_YF: case PMPIC_PROP_ZF: return MK_DISP;
+    case PMPIC_PROP_TAG: return MK_F64;
+    default: return MK_F32;
+  }
+}
+// whether a property is a position component on the mixed form
 __host__ __device__ __forceinline__ bool mixed_is_pos(int pid) {
-  return pid == PMPIC_PROP_X || pid == PMPIC_PROP_Y || pid == PMPIC_PROP_Z || pid == PMPIC_PROP_XO ||
-         pid == PMPIC_PROP_YO || pid == PMPIC_PROP_ZO || pid == PMPIC_PROP_XF || pid == PMPIC_PROP_YF ||
-         pid == PMPIC_PROP_ZF;
+  const int k = mixed_kind(pid);
+  return k == MK_CUR || k == MK_BASE || k == MK_DISP;
 }
+// element size of a property on the mixed form
 __host__ __device__ __forceinline__ int mixed_elem_bytes(int pid) {
-  return (mixed_is_pos(pid) || pid == PMPIC_PROP_TAG) ? 8 : 4;
+  const int k = mixed_kind(pid);
+  return (k == MK_BASE || k == MK_F64) ? 8 : 4;
 }
-// an FP64 coordinate v as cell index + FP32 offset for cell size d; period > 0
-// wraps the index into [0, period) (x, y); nz > 0 keeps a point on the top wall
-// z = nz d in the last cell with offset 1
-__device__ __forceinline__ CellOff co_from_double(double v, double d, int period, int nz) {
+// an FP64 coordinate v as cell index + FP32 offset for cell size d (index not wrapped)
+__device__ __forceinline__ CellOff co_from_double(double v, double d) {
   const double u = v / d;
   const double fl = floor(u);
   CellOff c;
@@ -155,15 +208,24 @@ __device__ __forceinline__ CellOff co_from_double(double v, double d, int period
     c.f = 0.0f;
     c.i += 1;
   }
-  if (period > 0) {
-    if (c.i >= period) c.i -= period;
-    if (c.i < 0) c.i += period;
-  }
-  if (nz > 0 && c.i == nz && c.f == 0.0f) {
-    c.i = nz - 1;
-    c.f = 1.0f;
-  }
   return c;
+}
+// a current position from FP64 coordinates: x and y wrapped into the domain,
+// z reflected at the walls (what the parcel haloswap does to a parcel outside);
+// false if z lies beyond the reach of one reflection
+__device__ __forceinline__ bool cur_from_double(const Geom& g, double x, double y, double z, int32_t& id, float& fx,
+                                                float& fy, float& fz) {
+  CellOff cx = co_from_double(x, g.dx), cy = co_from_double(y, g.dy), cz = co_from_double(z, g.dz);
+  cx.i = wrap_index(cx.i, g.Nx);
+  cy.i = wrap_index(cy.i, g.Ny);
+  cz = co_reflect(cz, g.Nz);
+  const bool ok = cz.i >= 0 && cz.i < g.Nz && cz.f >= 0.f && cz.f <= 1.f;
+  if (!ok) cz = CellOff{0, 0.f};
+  id = cell_encode(g, cx.i, cy.i, cz.i);
+  fx = cx.f;
+  fy = cy.f;
+  fz = cz.f;
+  return ok;
 }
 
 // Device-side step counters and error word.
@@ -181,7 +243,10 @@ struct DevInfo {
   double umax2, vmax2, wmax2, omax2;  // squared maxima (order-free reductions)
   int limiter;
   int pad2;
+  double sums[3];          // compensated totals of vol, h*vol, b*vol (conserved.cu)
 };
+// blocks of the first pass of the conserved sums (its partials buffer holds 6 doubles each)
+constexpr int CS_BLOCKS = 148 * 4;
 
 // Named timers, after the reference's timer_mod handles (e.g.
 // parcel_interpolation.F90:144-148, pencilfft.F90:104-108, fft_ops.F90:157-160,
@@ -238,7 +303,8 @@ struct pmpic_ctx {
   int32_t* sorted;           // cap: slot indices sorted by cell
   double* rowpart;           // par2grid row partials (rowpart_bytes)
   double* gpack;             // 8 x nphys: gather grids packed z fastest (parcels.cu)
-  double* lapcp;             // 3 x nspec: Thomas factors of a batched laplinv
+  double* lapcp;             // laplinv's Thomas factor tables (spectral.cu laplinv_tables;
+                             // FP32 values on the mixed form)
   int32_t* cell_count;       // ncell + 1
   int32_t* cell_start;       // ncell + 1
   int32_t* cell_fill;        // ncell
@@ -273,6 +339,7 @@ struct pmpic_ctx {
   double* kx, *ky, *k2, *filt;  // (Ny+2) x (Nx+2)
   double* bt;                // atop, abot, btop, bbot: 4 x (Ny+2)(Nx+2)
   double* zmode;             // ubar, vbar: 2 x (Nz+1)
+  double* csum;              // 6 x CS_BLOCKS: partials of the conserved sums
   // info
   pmpic::DevInfo* dinfo;     // device
   pmpic::DevInfo* hinfo;     // pinned host
@@ -297,6 +364,8 @@ inline double* prop(pmpic_ctx* ctx, int p) { return ctx->parcels + (size_t)p * (
 // the mixed form's views of the same property arrays
 inline float* propf(pmpic_ctx* ctx, int p) { return (float*)prop(ctx, p); }
 inline CellOff* propc(pmpic_ctx* ctx, int p) { return (CellOff*)prop(ctx, p); }
+// the mixed form's current position: cell ids, and the offsets of one axis
+inline float* curoff(pmpic_ctx* ctx, int axis) { return propf(ctx, PMPIC_PROP_X + axis); }
 
 // kernels / launchers (interp.cu)
 int bin_and_sort(pmpic_ctx* ctx);
@@ -381,4 +450,6 @@ int setup_thermal_device(pmpic_ctx* ctx, const pmpic_thermal_params* prm);
 int setup_basic(pmpic_ctx* ctx, int n_per_dir);
 int flush_gathers(pmpic_ctx* ctx);
 int sync_info(pmpic_ctx* ctx);
+// conserved.cu: the compensated totals of vol, h*vol, b*vol into dinfo->sums
+int conserved_sums(pmpic_ctx* ctx);
 }  // namespace pmpic

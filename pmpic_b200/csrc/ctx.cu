@@ -48,6 +48,9 @@ int sync_info(pmpic_ctx* ctx) {
   ctx->info.dtm = h.dtm;
   ctx->info.limiter = h.limiter;
   ctx->info.n_migrated = h.n_migrated;
+  ctx->info.vol_sum = h.sums[0];
+  ctx->info.hvol_sum = h.sums[1];
+  ctx->info.bvol_sum = h.sums[2];
   ctx->info.n_parcels = ctx->n;
   if (h.error != 0) {
     ctx->info.error = h.error;
@@ -119,7 +122,7 @@ void free_all(pmpic_ctx* c) {
                   c->aux,     c->aux2,     c->dir,       c->swapbuf,    c->scan_tmp,   c->npercell,  c->newslot,
                   c->newportion, c->sa,    c->sb,        c->sc,         c->sd,         c->se,        c->sf,
                   c->sas,     c->sbs,      c->sscratch,  c->fftmid,     c->ftw,        c->ftw32,      c->wn32,       c->hsum,       c->stage64,        c->kx,        c->ky,
-                  c->k2,      c->filt,     c->bt,        c->zmode,      c->dinfo};
+                  c->k2,      c->filt,     c->bt,        c->zmode,      c->csum,       c->dinfo};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int i = 0; i < PMPIC_NGRID; ++i)
@@ -222,6 +225,8 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   g.yshift_n = cfg->ymin - topy - g.dy;             // :542-546
   g.yshift_s = topy - cfg->ymin + g.dy;             // :547-551
   g.vmin = g.dx * g.dy * g.dz / 6. / 6. / 6.;       // parcel_mixing.F90:54
+  g.rNz = 1.0 / (double)g.Nz;
+  g.rNy = 1.0 / (double)g.Ny;
   ctx->cap = cfg->max_parcels;
   ctx->n = 0;
   ctx->sorted_valid = false;
@@ -244,7 +249,6 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   if (!rc) rc = dalloc(ctx, &ctx->sorted, cap);
   if (!rc) rc = dalloc(ctx, (char**)&ctx->rowpart, rowpart_bytes(g));
   if (!rc) rc = dalloc(ctx, &ctx->gpack, 8 * (size_t)g.nphys);  // six RK4 grids or eight mixing fields
-  if (!rc) rc = dalloc(ctx, &ctx->lapcp, 3 * (size_t)g.nspec);
   ctx->stage_n = std::min<int64_t>(ctx->cap, (int64_t)1 << 24);
   if (!rc && ctx->mixed) rc = dalloc(ctx, &ctx->stage64, (size_t)ctx->stage_n);
   if (!rc) rc = dalloc(ctx, &ctx->keep, cap);
@@ -254,7 +258,7 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   if (!rc) rc = dalloc(ctx, &ctx->cell_count, (size_t)g.ncell + 1);
   if (!rc) rc = dalloc(ctx, &ctx->cell_start, (size_t)g.ncell + 1);
   if (!rc) rc = dalloc(ctx, &ctx->cell_fill, (size_t)g.ncell);
-  if (!rc) rc = dalloc(ctx, &ctx->swapbuf, (size_t)ctx->swapcap * 29);
+  if (!rc) rc = dalloc(ctx, &ctx->swapbuf, (size_t)ctx->swapcap * 30);  // 29 properties (+ the mixed form's cell id)
   if (!rc) rc = dalloc(ctx, (int32_t**)&ctx->scan_tmp, (size_t)(std::max<int64_t>(std::max<int64_t>(g.ncell, ctx->cap), ctx->nbmax) / 4096 + 64));
   for (int i = 0; i < PMPIC_NGRID && !rc; ++i) rc = dalloc(ctx, &ctx->grid[i], (size_t)g.nphys);
   for (int i = 0; i < 5 && !rc; ++i) rc = dalloc(ctx, &ctx->gwork[i], (size_t)g.nphys);
@@ -275,6 +279,7 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   if (!rc) rc = dalloc(ctx, &ctx->filt, cols);
   if (!rc) rc = dalloc(ctx, &ctx->bt, 4 * cols);
   if (!rc) rc = dalloc(ctx, &ctx->zmode, 2 * (size_t)g.nzp);
+  if (!rc) rc = dalloc(ctx, &ctx->csum, 6 * (size_t)CS_BLOCKS);
   if (!rc) rc = dalloc(ctx, (char**)&ctx->dinfo, sizeof(DevInfo) + 64 * sizeof(int32_t));
   if (!rc) {
     e = cudaMallocHost((void**)&ctx->hinfo, sizeof(DevInfo));
@@ -334,29 +339,79 @@ const char* pmpic_last_error(const pmpic_ctx* ctx) { return ctx ? ctx->err.c_str
 
 // ---- the mixed form's property and grid conversions ---------------------------------
 namespace {
-// kind 0: FP32 value, 1: position component with cell size d (nz: the wall index
-// for z, else 0), 2: FP64 value (tag)
-__global__ void k_conv_in(int64_t n, const double* __restrict__ src, void* __restrict__ dst, int kind, double d,
-                          int period, int nz) {
+// Host FP64 values into one property of the mixed form (kinds of mixed_kind):
+// FP32 values; the tag as FP64; xo as {index, offset}; xf as the displacement
+// from the slot's xo; a current position component as the offset, with the
+// axis's index written into the slot's cell id (x, y wrapped into the domain,
+// z reflected at the walls, as the parcel haloswap would; a z beyond one
+// reflection is reported out of box).
+struct ConvIn {
+  int kind, axis;
+  double d;             // cell size along the axis
+  const CellOff* base;  // MK_DISP: the axis's xo
+  int32_t* cell;        // MK_CUR: the cell ids
+  DevInfo* info;
+};
+__global__ void k_conv_in(Geom g, int64_t n, const double* __restrict__ src, void* __restrict__ dst, ConvIn c) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const double v = src ? src[t] : 0.0;
-  if (kind == 0) {
-    ((float*)dst)[t] = (float)v;
-  } else if (kind == 2) {
-    ((double*)dst)[t] = v;
-  } else {
-    ((CellOff*)dst)[t] = co_from_double(v, d, period, nz);
+  switch (c.kind) {
+    case MK_F32: ((float*)dst)[t] = (float)v; break;
+    case MK_F64: ((double*)dst)[t] = v; break;
+    case MK_BASE: ((CellOff*)dst)[t] = co_from_double(v, c.d); break;
+    case MK_DISP: {
+      const CellOff b = c.base[t];
+      ((float*)dst)[t] = (float)(v / c.d - ((double)b.i + (double)b.f));
+      break;
+    }
+    default: {  // MK_CUR
+      int ijk[3] = {0, 0, 0};
+      const int32_t id = c.cell[t];
+      if (id >= 0 && id < g.ncell) cell_decode(g, id, ijk[0], ijk[1], ijk[2]);
+      CellOff a = co_from_double(v, c.d);
+      if (c.axis == 0) a.i = wrap_index(a.i, g.Nx);
+      else if (c.axis == 1) a.i = wrap_index(a.i, g.Ny);
+      else {
+        a = co_reflect(a, g.Nz);
+        if (!(a.i >= 0 && a.i < g.Nz && a.f >= 0.f && a.f <= 1.f)) {
+          atomicCAS(&c.info->error, 0, PMPIC_ERR_OUT_OF_BOX);
+          a = CellOff{0, 0.f};
+        }
+      }
+      ijk[c.axis] = a.i;
+      c.cell[t] = cell_encode(g, ijk[0], ijk[1], ijk[2]);
+      ((float*)dst)[t] = a.f;
+    }
   }
 }
-__global__ void k_conv_out(int64_t n, const void* __restrict__ src, double* __restrict__ dst, int kind, double d) {
+struct ConvOut {
+  int kind, axis;
+  double d;
+  const CellOff* base;   // MK_DISP
+  const int32_t* cell;   // MK_CUR
+};
+__global__ void k_conv_out(Geom g, int64_t n, const void* __restrict__ src, double* __restrict__ dst, ConvOut c) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  if (kind == 0) dst[t] = (double)((const float*)src)[t];
-  else if (kind == 2) dst[t] = ((const double*)src)[t];
-  else {
-    const CellOff c = ((const CellOff*)src)[t];
-    dst[t] = ((double)c.i + (double)c.f) * d;
+  switch (c.kind) {
+    case MK_F32: dst[t] = (double)((const float*)src)[t]; break;
+    case MK_F64: dst[t] = ((const double*)src)[t]; break;
+    case MK_BASE: {
+      const CellOff b = ((const CellOff*)src)[t];
+      dst[t] = ((double)b.i + (double)b.f) * c.d;
+      break;
+    }
+    case MK_DISP: {
+      const CellOff b = c.base[t];
+      dst[t] = ((double)b.i + (double)b.f + (double)((const float*)src)[t]) * c.d;
+      break;
+    }
+    default: {  // MK_CUR
+      int ijk[3] = {0, 0, 0};
+      cell_decode(g, c.cell[t], ijk[0], ijk[1], ijk[2]);
+      dst[t] = ((double)ijk[c.axis] + (double)((const float*)src)[t]) * c.d;
+    }
   }
 }
 __global__ void k_f2d(int64_t n, const float* __restrict__ src, double* __restrict__ dst) {
@@ -368,18 +423,14 @@ __global__ void k_d2f(int64_t n, const double* __restrict__ src, float* __restri
   if (t < n) dst[t] = (float)src[t];
 }
 unsigned cblk(int64_t n) { return (unsigned)((n + 255) / 256); }
-}  // namespace
 
-static void conv_kind(pmpic_ctx* ctx, int pid, int& kind, double& d, int& period, int& nz) {
-  const Geom& g = ctx->g;
-  kind = pid == PMPIC_PROP_TAG ? 2 : (mixed_is_pos(pid) ? 1 : 0);
-  d = 1.0;
-  period = 0;
-  nz = 0;
-  if (pid == PMPIC_PROP_X || pid == PMPIC_PROP_XO || pid == PMPIC_PROP_XF) { d = g.dx; period = g.Nx; }
-  if (pid == PMPIC_PROP_Y || pid == PMPIC_PROP_YO || pid == PMPIC_PROP_YF) { d = g.dy; period = g.Ny; }
-  if (pid == PMPIC_PROP_Z || pid == PMPIC_PROP_ZO || pid == PMPIC_PROP_ZF) { d = g.dz; nz = g.Nz; }
+int axis_of(int pid) {
+  if (pid == PMPIC_PROP_X || pid == PMPIC_PROP_XO || pid == PMPIC_PROP_XF) return 0;
+  if (pid == PMPIC_PROP_Y || pid == PMPIC_PROP_YO || pid == PMPIC_PROP_YF) return 1;
+  return 2;
 }
+double cell_size(const Geom& g, int axis) { return axis == 0 ? g.dx : (axis == 1 ? g.dy : g.dz); }
+}  // namespace
 
 // host FP64 values (NULL: zeros) into property pid of slots off..off+n-1, in
 // the context's precision; stream-ordered
@@ -392,20 +443,24 @@ int pmpic::prop_upload(pmpic_ctx* ctx, int pid, int64_t off, int64_t n, const do
     else PMPIC_CUDA(cudaMemsetAsync(prop(ctx, pid) + off, 0, sizeof(double) * n, ctx->stream));
     return 0;
   }
-  const size_t es0 = (size_t)mixed_elem_bytes(pid);
-  if (!src) {
-    PMPIC_CUDA(cudaMemsetAsync((char*)prop(ctx, pid) + es0 * off, 0, es0 * n, ctx->stream));
+  const size_t es = (size_t)mixed_elem_bytes(pid);
+  const int kind = mixed_kind(pid);
+  if (!src && (kind == MK_F32 || kind == MK_F64 || kind == MK_BASE)) {
+    PMPIC_CUDA(cudaMemsetAsync((char*)prop(ctx, pid) + es * off, 0, es * n, ctx->stream));
     return 0;
   }
-  int kind, period, nz;
-  double d;
-  conv_kind(ctx, pid, kind, d, period, nz);
-  char* base = (char*)prop(ctx, pid) + es0 * off;
-  const size_t es = (size_t)mixed_elem_bytes(pid);
+  ConvIn c;
+  c.kind = kind;
+  c.axis = axis_of(pid);
+  c.d = cell_size(ctx->g, c.axis);
+  c.info = ctx->dinfo;
+  char* base = (char*)prop(ctx, pid) + es * off;
   for (int64_t c0 = 0; c0 < n; c0 += ctx->stage_n) {
     const int64_t len = std::min<int64_t>(ctx->stage_n, n - c0);
-    PMPIC_CUDA(cudaMemcpyAsync(ctx->stage64, src + c0, sizeof(double) * len, cudaMemcpyHostToDevice, ctx->stream));
-    k_conv_in<<<cblk(len), 256, 0, ctx->stream>>>(len, ctx->stage64, base + es * c0, kind, d, period, nz);
+    c.base = propc(ctx, PMPIC_PROP_XO + c.axis) + off + c0;
+    c.cell = ctx->cell + off + c0;
+    if (src) PMPIC_CUDA(cudaMemcpyAsync(ctx->stage64, src + c0, sizeof(double) * len, cudaMemcpyHostToDevice, ctx->stream));
+    k_conv_in<<<cblk(len), 256, 0, ctx->stream>>>(ctx->g, len, src ? ctx->stage64 : nullptr, base + es * c0, c);
     ++ctx->nlaunch;
   }
   PMPIC_CUDA(cudaGetLastError());
@@ -418,14 +473,17 @@ int pmpic::prop_download(pmpic_ctx* ctx, int pid, int64_t off, int64_t n, double
     PMPIC_CUDA(cudaMemcpyAsync(dst, prop(ctx, pid) + off, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
     return 0;
   }
-  int kind, period, nz;
-  double d;
-  conv_kind(ctx, pid, kind, d, period, nz);
-  const char* base = (const char*)prop(ctx, pid) + (size_t)mixed_elem_bytes(pid) * off;
   const size_t es = (size_t)mixed_elem_bytes(pid);
+  ConvOut c;
+  c.kind = mixed_kind(pid);
+  c.axis = axis_of(pid);
+  c.d = cell_size(ctx->g, c.axis);
+  const char* base = (const char*)prop(ctx, pid) + es * off;
   for (int64_t c0 = 0; c0 < n; c0 += ctx->stage_n) {
     const int64_t len = std::min<int64_t>(ctx->stage_n, n - c0);
-    k_conv_out<<<cblk(len), 256, 0, ctx->stream>>>(len, base + es * c0, ctx->stage64, kind, d);
+    c.base = propc(ctx, PMPIC_PROP_XO + c.axis) + off + c0;
+    c.cell = ctx->cell + off + c0;
+    k_conv_out<<<cblk(len), 256, 0, ctx->stream>>>(ctx->g, len, base + es * c0, ctx->stage64, c);
     ++ctx->nlaunch;
     PMPIC_CUDA(cudaMemcpyAsync(dst + c0, ctx->stage64, sizeof(double) * len, cudaMemcpyDeviceToHost, ctx->stream));
   }
@@ -614,6 +672,18 @@ int pmpic_get_step_info(pmpic_ctx* ctx, pmpic_step_info* info) {
   return rc;
 }
 
+int pmpic_conserved_sums(pmpic_ctx* ctx, double sums[3]) {
+  if (!ctx || !sums) return PMPIC_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  int rc = conserved_sums(ctx);
+  if (!rc) rc = sync_info(ctx);
+  if (rc) return rc;
+  sums[0] = ctx->info.vol_sum;
+  sums[1] = ctx->info.hvol_sum;
+  sums[2] = ctx->info.bvol_sum;
+  return PMPIC_OK;
+}
+
 // ---- component callbacks --------------------------------------------------------
 // Internal forms without the trailing error check; the public entry points
 // check the sticky device error word once per call.
@@ -711,6 +781,8 @@ static int do_mix(pmpic_ctx* ctx) {
   if (ctx->counters[4] % 4 == 3) {  // parcel_mixing.F90:77
     TimerScope ts(ctx, T_MIX);
     rc = mixing(ctx);
+    // the diagnostic totals after mixing (parcel_mixing.F90:409-418)
+    if (!rc) rc = conserved_sums(ctx);
   }
   ctx->counters[4]++;
   return rc;
@@ -974,11 +1046,14 @@ int pmpic_sort_parcels(pmpic_ctx* ctx) {
   if ((rc = sync_info(ctx))) return rc;  // every parcel binned (else out of box)
   void* tmp = nullptr;
   PMPIC_CUDA(cudaMalloc(&tmp, sizeof(double) * (size_t)n));
-  for (int p = 0; p < PMPIC_NPROP && !rc; ++p) {
-    const int es = ctx->mixed ? mixed_elem_bytes(p) : 8;
-    k_permute<<<cblk(n), 256, 0, ctx->stream>>>(n, ctx->sorted, prop(ctx, p), tmp, es);
+  // every property, and on the mixed form the cell ids (part of its positions)
+  for (int p = 0; p <= PMPIC_NPROP && !rc; ++p) {
+    if (p == PMPIC_NPROP && !ctx->mixed) break;
+    void* col = p < PMPIC_NPROP ? (void*)prop(ctx, p) : (void*)ctx->cell;
+    const int es = p == PMPIC_NPROP ? 4 : (ctx->mixed ? mixed_elem_bytes(p) : 8);
+    k_permute<<<cblk(n), 256, 0, ctx->stream>>>(n, ctx->sorted, col, tmp, es);
     ++ctx->nlaunch;
-    cudaError_t e = cudaMemcpyAsync(prop(ctx, p), tmp, (size_t)es * n, cudaMemcpyDeviceToDevice, ctx->stream);
+    cudaError_t e = cudaMemcpyAsync(col, tmp, (size_t)es * n, cudaMemcpyDeviceToDevice, ctx->stream);
     if (e != cudaSuccess) rc = cuda_fail(ctx, e, "cudaMemcpyAsync", __LINE__);
   }
   cudaStreamSynchronize(ctx->stream);

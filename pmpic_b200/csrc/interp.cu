@@ -54,21 +54,19 @@ __global__ void k_bin_count(Geom g, int64_t n, const double* __restrict__ X, con
   count_cell(id, count);
 }
 
-// the mixed form's binning: the cell is the integer part of the position
-__global__ void k_bin_count_m(Geom g, int64_t n, const CellOff* __restrict__ X, const CellOff* __restrict__ Y,
-                              const CellOff* __restrict__ Z, int32_t* __restrict__ cell, int32_t* __restrict__ count,
-                              DevInfo* info) {
+// the mixed form's binning: the cell id is part of the position already; the
+// pass only checks it and counts the cells
+__global__ void k_bin_count_m(Geom g, int64_t n, const int32_t* __restrict__ cell, const float* __restrict__ FX,
+                              const float* __restrict__ FY, const float* __restrict__ FZ,
+                              int32_t* __restrict__ count, DevInfo* info) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  const CellOff x = X[t], y = Y[t], z = Z[t];
-  if (x.i < 0 || x.i >= g.Nx || y.i < 0 || y.i >= g.Ny || z.i < 0 || z.i >= g.Nz || !(x.f >= 0.f && x.f <= 1.f) ||
-      !(y.f >= 0.f && y.f <= 1.f) || !(z.f >= 0.f && z.f <= 1.f)) {
-    cell[t] = -1;
+  const int32_t id = cell[t];
+  const float fx = FX[t], fy = FY[t], fz = FZ[t];
+  if (id < 0 || id >= g.ncell || !(fx >= 0.f && fx <= 1.f) || !(fy >= 0.f && fy <= 1.f) || !(fz >= 0.f && fz <= 1.f)) {
     atomicCAS(&info->error, 0, PMPIC_ERR_OUT_OF_BOX);
     return;
   }
-  const int32_t id = (int32_t)(((int64_t)x.i * g.Ny + y.i) * g.Nz + z.i);
-  cell[t] = id;
   count_cell(id, count);
 }
 
@@ -266,8 +264,8 @@ template <int NQ, class R = double>
 struct P2GArgs {
   const R* f[NQ] = {};      // per-parcel fields (MODE 1/2: f[0] unused)
   R* out[NQ] = {};
-  // BT: b, h and z of btot; z is FP64 (stride 1) on the plain path, the cell
-  // index half of the {cell index, offset} positions (stride 2) on the mixed form
+  // BT: b, h and z of btot; on the mixed form z is not staged (its cell layer
+  // is known from the column's layer bounds, its offset is staged as delz)
   const R* bh[3] = {};
   R* btot = nullptr;        // BT: the btot property, written as staged
   int64_t nslot = 0;        // parcel count: staged slot indices are checked against it
@@ -322,9 +320,9 @@ __device__ __forceinline__ double madd(double w, double f, double acc) { return 
 __device__ __forceinline__ float madd(float w, float f, float acc) { return __fmaf_rn(w, f, acc); }
 
 // R: the arithmetic type (double: plain path, float: mixed-precision form).
-// The cell offsets delx, dely, delz of parcel n are DX[ds * n], DY[ds * n],
-// DZ[ds * n]: the cached binning (ds = 1) or the offset half of the mixed
-// form's {cell index, offset} positions (ds = 2).
+// The cell offsets delx, dely, delz of parcel n are DX[n], DY[n], DZ[n]: the
+// cached binning on the plain path, the offsets of the current position on
+// the mixed form (ds = 1 on both; a stride ds > 1 reads interleaved offsets).
 template <int NQ, int MODE, bool BT, class R = double>
 __global__ void __launch_bounds__(32 * RW, sizeof(R) == 4 ? 6 : 4) k_p2g_rows(Geom g, int nzc, int nxs, int xseg, const int32_t* __restrict__ start,
                                                      const int32_t* __restrict__ sorted, const R* __restrict__ DX,
@@ -393,7 +391,7 @@ __global__ void __launch_bounds__(32 * RW, sizeof(R) == 4 ? 6 : 4) k_p2g_rows(Ge
         if (BT) {
           cp_async_r(D + (4 + NQ - 1) * SPAD, a.bh[0] + n);
           cp_async_r(D + (4 + NQ) * SPAD, a.bh[1] + n);
-          cp_async_r(D + (4 + NQ + 1) * SPAD, a.bh[2] + nd);
+          if constexpr (sizeof(R) == 8) cp_async_r(D + (4 + NQ + 1) * SPAD, a.bh[2] + n);
         }
       } else {
 #pragma unroll
@@ -401,8 +399,11 @@ __global__ void __launch_bounds__(32 * RW, sizeof(R) == 4 ? 6 : 4) k_p2g_rows(Ge
       }
     }
   };
-  // btot per staged parcel (vorticity_tendency.F90:121-126), also stored as the property
-  auto btot_pass = [&](R* Sb, const int* sl, int nb) {
+  // btot per staged parcel (vorticity_tendency.F90:121-126), also stored as
+  // the property.  On the mixed form z is (k + delz) dz, with k the cell layer
+  // of the parcel's index position b0 + p among the column's layer starts LS.
+  __shared__ int LS[RW][ZC + 1];
+  auto btot_pass = [&](R* Sb, const int* sl, int nb, int b0) {
 #pragma unroll
     for (int j = 0; j < BATCH / 32; ++j) {
       const int p = lane + 32 * j;
@@ -412,8 +413,13 @@ __global__ void __launch_bounds__(32 * RW, sizeof(R) == 4 ? 6 : 4) k_p2g_rows(Ge
       R bt;
       if constexpr (sizeof(R) == 8) {
         bt = bb + 12.5 * fmax(0.0, hh - exp(-D[2 * SPAD]));
-      } else {  // z from its cell index and offset, in FP32
-        const float zz = ((float)__float_as_int(D[2 * SPAD]) + Sb[p + (p >> 4) + 2 * SPAD]) * (float)g.dz;
+      } else {  // z from its cell layer and offset, in FP32
+        const int pos = b0 + p;
+        int l = 0;
+#pragma unroll 1
+        for (int step = 8; step > 0; step >>= 1)  // the last layer start at or below pos
+          if (l + step < nk && LS[warp][l + step] <= pos) l += step;
+        const float zz = ((float)(k0 + l) + Sb[p + (p >> 4) + 2 * SPAD]) * (float)g.dz;
         bt = bb + 12.5f * fmaxf(0.f, hh - expf(-zz));
       }
       D[0] = bt;
@@ -511,6 +517,11 @@ __global__ void __launch_bounds__(32 * RW, sizeof(R) == 4 ? 6 : 4) k_p2g_rows(Ge
         for (int q = 0; q < NA; ++q) acc[ab][q] = R(0);
       int nkept = 0;
       bool prefetched = false;
+      if constexpr (BT && sizeof(R) == 4) {  // this column's layer starts for btot's z
+        __syncwarp();
+        if (cz == 0 && has_cell) LS[warp][kk] = s_me;
+        __syncwarp();
+      }
       for (int b0 = q0; b0 < q1; b0 += BATCH) {
         const int nb = min(BATCH, q1 - b0);
         __syncwarp();  // the previous batch has been read
@@ -530,7 +541,7 @@ __global__ void __launch_bounds__(32 * RW, sizeof(R) == 4 ? 6 : 4) k_p2g_rows(Ge
         }
         cp_async_wait_all();
         __syncwarp();
-        if constexpr (BT) btot_pass(S, slot, nb);
+        if constexpr (BT) btot_pass(S, slot, nb, b0);
         accumulate(S, b0, nb, s_me, e_me, acc, nkept);
       }
       if (more && !prefetched) {  // an empty column
@@ -695,9 +706,9 @@ int bin_and_sort(pmpic_ctx* ctx) {
   if (!counted) {
     PMPIC_CUDA(cudaMemsetAsync(ctx->cell_count, 0, sizeof(int32_t) * (g.ncell + 1), ctx->stream));
     if (n > 0 && ctx->mixed) {
-      k_bin_count_m<<<nblk(n, 256), 256, 0, ctx->stream>>>(g, n, propc(ctx, PMPIC_PROP_X), propc(ctx, PMPIC_PROP_Y),
-                                                           propc(ctx, PMPIC_PROP_Z), ctx->cell, ctx->cell_count,
-                                                           ctx->dinfo); ++ctx->nlaunch;
+      k_bin_count_m<<<nblk(n, 256), 256, 0, ctx->stream>>>(g, n, ctx->cell, curoff(ctx, 0), curoff(ctx, 1),
+                                                           curoff(ctx, 2), ctx->cell_count, ctx->dinfo);
+      ++ctx->nlaunch;
     } else if (n > 0) {
       k_bin_count<<<nblk(n, 256), 256, 0, ctx->stream>>>(g, n, prop(ctx, PMPIC_PROP_X), prop(ctx, PMPIC_PROP_Y),
                                                          prop(ctx, PMPIC_PROP_Z), ctx->cell, ctx->del, ctx->cap,
@@ -776,15 +787,13 @@ static int launch_p2g_m(pmpic_ctx* ctx, const float* const* fields, float* const
   }
   a.bh[0] = propf(ctx, PMPIC_PROP_B);
   a.bh[1] = propf(ctx, PMPIC_PROP_H);
-  a.bh[2] = (const float*)prop(ctx, PMPIC_PROP_Z);  // the cell index halves
   a.btot = propf(ctx, PMPIC_PROP_BTOT);
   a.nslot = ctx->n;
   a.npercell = ctx->npercell;
   a.vmin = (double)(float)g.vmin;
-  const float* px = (const float*)prop(ctx, PMPIC_PROP_X) + 1;  // offset halves of the CellOff slots
-  const float* py = (const float*)prop(ctx, PMPIC_PROP_Y) + 1;
-  const float* pz = (const float*)prop(ctx, PMPIC_PROP_Z) + 1;
-  PMPIC_CUDA((run_p2g<NQ, MODE, BT, float>(g, ctx->cell_start, ctx->sorted, px, py, pz, 2,
+  // the offsets of the current positions
+  PMPIC_CUDA((run_p2g<NQ, MODE, BT, float>(g, ctx->cell_start, ctx->sorted, curoff(ctx, 0), curoff(ctx, 1),
+                                              curoff(ctx, 2), 1,
                                               propf(ctx, PMPIC_PROP_VOL), a, (float*)ctx->rowpart, ctx->stream,
                                               ctx->p2g_xseg)));
   ctx->nlaunch += 2;
@@ -882,22 +891,24 @@ static int launch_g2p(pmpic_ctx* ctx, const double* const* grids, double* const*
   return 0;
 }
 
-// grid2par of NG FP32 grids at the mixed form's {cell, offset} positions
+// grid2par of NG FP32 grids at the mixed form's current positions (cell id + offsets)
 template <int NG>
-__global__ void k_grid2par_mt(Geom g, int64_t n, const CellOff* __restrict__ X, const CellOff* __restrict__ Y,
-                              const CellOff* __restrict__ Z, G2PArgs<NG> a, DevInfo* info) {
+__global__ void k_grid2par_mt(Geom g, int64_t n, const int32_t* __restrict__ cell, const float* __restrict__ FX,
+                              const float* __restrict__ FY, const float* __restrict__ FZ, G2PArgs<NG> a,
+                              DevInfo* info) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  const CellOff x = X[t], y = Y[t], z = Z[t];
-  const int ci = x.i, cj = y.i, ck = z.i;
-  if (ci < 0 || ci >= g.Nx || cj < 0 || cj >= g.Ny || ck < 0 || ck >= g.Nz) {  // outside the grid: nothing read
+  const int32_t id = cell[t];
+  if (id < 0 || id >= g.ncell) {  // not a cell of the grid: nothing read
     atomicCAS(&info->error, 0, PMPIC_ERR_OUT_OF_BOX);
     return;
   }
+  int ci, cj, ck;
+  cell_decode(g, id, ci, cj, ck);
   const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
   const size_t r00 = ((size_t)ck * g.Ny + cj) * g.Nx, r01 = ((size_t)ck * g.Ny + cj1) * g.Nx;
   const size_t r10 = ((size_t)(ck + 1) * g.Ny + cj) * g.Nx, r11 = ((size_t)(ck + 1) * g.Ny + cj1) * g.Nx;
-  const float delx = x.f, dely = y.f, delz = z.f;
+  const float delx = FX[t], dely = FY[t], delz = FZ[t];
 #pragma unroll
   for (int q = 0; q < NG; ++q) {
     const float* G = (const float*)a.grid[q];
@@ -922,9 +933,8 @@ int grid2par_multi_m(pmpic_ctx* ctx, const float* const* grids, int ng, float* c
       a.grid[q] = (const double*)grids[q];
       a.out[q] = (double*)out[q];
     }
-    k_grid2par_mt<NG><<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, propc(ctx, PMPIC_PROP_X),
-                                                                   propc(ctx, PMPIC_PROP_Y), propc(ctx, PMPIC_PROP_Z), a,
-                                                                   ctx->dinfo);
+    k_grid2par_mt<NG><<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, ctx->cell, curoff(ctx, 0),
+                                                                   curoff(ctx, 1), curoff(ctx, 2), a, ctx->dinfo);
     ++ctx->nlaunch;
   };
   switch (ng) {

@@ -718,19 +718,22 @@ __global__ void k_backfill(const int32_t* __restrict__ zlist, const int32_t* __r
 }
 
 // ==== mixed-precision form ===========================================================
-// The same components with FP32 fields and {cell index, FP32 offset} positions
-// (CellOff); the integer bookkeeping (directions, lists, slots) is shared with
-// the plain path.  Float property p of parcel n is ((float*)array_p)[n].
+// The same components with FP32 fields and {cell, FP32 offset} positions
+// (common.cuh): the current position as the cell id and three offsets, xo as
+// a CellOff per axis, xf as the displacement from xo.  The integer bookkeeping
+// (directions, lists, slots) is shared with the plain path.  Float property p
+// of parcel n is ((float*)array_p)[n].
 struct MPtrs {
   const float* g6;  // the six grids packed (k_pack), when both gathers are pending
   float inv[3];     // 1/dx, 1/dy, 1/dz
-  CellOff* s[3];
-  CellOff* o[3];
-  CellOff* f[3];
-  float* sv[3];  // p, q, r
+  int32_t* cell;    // current cell ids
+  float* cur[3];    // current offsets
+  CellOff* o[3];    // xo, yo, zo
+  float* f[3];      // xf, yf, zf as displacements from xo (cell units)
+  float* sv[3];     // p, q, r
   float* ov[3];
   float* fv[3];
-  float* d[6];   // dxdt, dydt, dzdt, dpdt, dqdt, drdt
+  float* d[6];      // dxdt, dydt, dzdt, dpdt, dqdt, drdt
   const float* grid[6];
 };
 
@@ -762,50 +765,71 @@ __device__ __forceinline__ int classify_dir_m(const Geom& g, int i, int j) {
   return 0;
 }
 
+// A moved position p (unwrapped x, y indices; z after the wall reflection)
+// as the current position: the haloswap direction from the unwrapped indices
+// (haloswap.F90:296-437), x and y wrapped by whole periods (the shift of
+// :531-559; the haloswap then re-slots the parcel and shifts its xo), the
+// cell id.  A z outside the grid after its reflection is reported out of box.
+__device__ __forceinline__ int32_t place_m(const Geom& g, CellOff* p, int& d, DevInfo* info) {
+  d = classify_dir_m(g, p[0].i, p[1].i);
+  p[0].i = wrap_index(p[0].i, g.Nx);
+  p[1].i = wrap_index(p[1].i, g.Ny);
+  if (!(p[2].i >= 0 && p[2].i < g.Nz && p[0].f >= 0.f && p[0].f < 1.f && p[1].f >= 0.f && p[1].f < 1.f &&
+        p[2].f >= 0.f && p[2].f <= 1.f)) {
+    atomicCAS(&info->error, 0, PMPIC_ERR_OUT_OF_BOX);
+    p[0] = p[1] = p[2] = CellOff{0, 0.f};
+  }
+  return cell_encode(g, p[0].i, p[1].i, p[2].i);
+}
+
 // RK4 stage (rk4_integrator.F90:95-319) with the deferred gathers, the z
 // reflection and the direction classification, as k_rk4; position updates in
-// cell units (velocity * dt / cell size), renormalised into [0, 1).
+// cell units (velocity * dt / cell size), renormalised into [0, 1).  The
+// parcel is gathered at its current position; stage 1 takes that position as
+// xo (:125-127); the new position is xo plus the stage's displacement, and xf
+// the accumulated displacement (at stage 4 the new position is xo + xf, :303).
+// The new cell id and offsets are the next binning: every parcel is counted
+// in its new cell (movers too: they keep their cell as the haloswap re-slots
+// them).
 template <bool GU, bool GP>
 __global__ void __launch_bounds__(256, 5) k_rk4_m(Geom g, int64_t n, MPtrs P, int stage, const double* __restrict__ dtp,
-                        int8_t* __restrict__ dir, int32_t* __restrict__ cell, int32_t* __restrict__ count,
-                        DevInfo* info, float* __restrict__ stretch, int store_d, int32_t* __restrict__ dircnt) {
+                        int8_t* __restrict__ dir, int32_t* __restrict__ count, DevInfo* info,
+                        float* __restrict__ stretch, int store_d, int32_t* __restrict__ dircnt) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const float dt = (float)*dtp;  // state%dtm (rk4_integrator.F90:102)
   const float dt6 = dt * (1.f / 6.f), dt2 = dt * 0.5f, dt3 = dt * (1.f / 3.f);
   const float* inv = P.inv;
-  CellOff sp[3], op[3], fp[3];
-  float sv[3], ov[3], fv[3], d[6];
-  const bool need_s = stage == 1 || GU || GP;
+  const bool need_cur = stage == 1 || GU || GP;
+  int cx[3] = {0, 0, 0};
+  float cf[3] = {0.f, 0.f, 0.f};
+  if (need_cur) {
+    cell_decode(g, P.cell[t], cx[0], cx[1], cx[2]);
+#pragma unroll
+    for (int v = 0; v < 3; ++v) cf[v] = P.cur[v][t];
+  }
+  CellOff op[3];
+  float fd[3], sv[3], ov[3], fv[3], d[6];
 #pragma unroll
   for (int v = 0; v < 3; ++v) {
-    if (need_s) sp[v] = P.s[v][t];
     if (stage == 1) sv[v] = P.sv[v][t];
-    if (stage == 2 || stage == 3) {
-      op[v] = P.o[v][t];
-      ov[v] = P.ov[v][t];
-    }
     if (stage >= 2) {
-      fp[v] = P.f[v][t];
+      op[v] = P.o[v][t];
+      fd[v] = P.f[v][t];
       fv[v] = P.fv[v][t];
     }
+    if (stage == 2 || stage == 3) ov[v] = P.ov[v][t];
   }
 #pragma unroll
   for (int v = 0; v < 6; ++v)
     if ((v < 3 && !GU) || (v >= 3 && !GP)) d[v] = P.d[v][t];
-  bool gathered = false;
-  if (GU || GP) {
-    const int ci = sp[0].i, cj = sp[1].i, ck = sp[2].i;
-    // a position outside the grid was reported by the binning; it gathers nothing
-    gathered = ci >= 0 && ci < g.Nx && cj >= 0 && cj < g.Ny && ck >= 0 && ck < g.Nz;
-    if (GU && GP && gathered) {
-      g2p_packed<float>(g, P.g6, ci, cj, ck, sp[0].f, sp[1].f, sp[2].f, d);
-    } else {
+  if (GU && GP) {
+    g2p_packed<float>(g, P.g6, cx[0], cx[1], cx[2], cf[0], cf[1], cf[2], d);
+  } else if (GU || GP) {
 #pragma unroll
-      for (int v = 0; v < 6; ++v) {
-        if ((v < 3 && !GU) || (v >= 3 && !GP)) continue;
-        d[v] = gathered ? g2p_f(g, P.grid[v], ci, cj, ck, sp[0].f, sp[1].f, sp[2].f) : P.d[v][t];
-      }
+    for (int v = 0; v < 6; ++v) {
+      if ((v < 3 && !GU) || (v >= 3 && !GP)) continue;
+      d[v] = g2p_f(g, P.grid[v], cx[0], cx[1], cx[2], cf[0], cf[1], cf[2]);
     }
   }
   CellOff sn[3];
@@ -815,26 +839,26 @@ __global__ void __launch_bounds__(256, 5) k_rk4_m(Geom g, int64_t n, MPtrs P, in
     const float dc = d[v] * inv[v];  // cell units per unit time
     const float dw = d[v + 3];
     if (stage == 1) {
-      op[v] = sp[v];
+      op[v] = CellOff{cx[v], cf[v]};
       ov[v] = sv[v];
-      fp[v] = co_add(sp[v], dt6 * dc);
+      fd[v] = dt6 * dc;
       fv[v] = sv[v] + dt6 * dw;
-      sn[v] = co_add(sp[v], dt2 * dc);
+      sn[v] = co_add(op[v], dt2 * dc);
       svn[v] = sv[v] + dt2 * dw;
     } else if (stage == 2) {
-      fp[v] = co_add(fp[v], dt3 * dc);
+      fd[v] = fd[v] + dt3 * dc;
       fv[v] = fv[v] + dt3 * dw;
       sn[v] = co_add(op[v], dt2 * dc);
       svn[v] = ov[v] + dt2 * dw;
     } else if (stage == 3) {
-      fp[v] = co_add(fp[v], dt3 * dc);
+      fd[v] = fd[v] + dt3 * dc;
       fv[v] = fv[v] + dt3 * dw;
       sn[v] = co_add(op[v], dt * dc);
       svn[v] = ov[v] + dt * dw;
     } else {
-      fp[v] = co_add(fp[v], dt6 * dc);
+      fd[v] = fd[v] + dt6 * dc;
       fv[v] = fv[v] + dt6 * dw;
-      sn[v] = fp[v];
+      sn[v] = co_add(op[v], fd[v]);
       svn[v] = fv[v];
     }
   }
@@ -846,54 +870,44 @@ __global__ void __launch_bounds__(256, 5) k_rk4_m(Geom g, int64_t n, MPtrs P, in
   }
 #pragma unroll
   for (int v = 0; v < 6; ++v)
-    if (store_d && gathered && ((v < 3 && GU) || (v >= 3 && GP))) P.d[v][t] = d[v];
+    if (store_d && ((v < 3 && GU) || (v >= 3 && GP))) P.d[v][t] = d[v];
 #pragma unroll
   for (int v = 0; v < 3; ++v) {
     if (stage == 1) {
       P.o[v][t] = op[v];
       P.ov[v][t] = ov[v];
     }
-    P.f[v][t] = fp[v];
+    P.f[v][t] = fd[v];
     P.fv[v][t] = fv[v];
-    P.s[v][t] = sn[v];
     P.sv[v][t] = svn[v];
   }
-  const int dr = classify_dir_m(g, sn[0].i, sn[1].i);
+  int dr;
+  const int32_t nid = place_m(g, sn, dr, info);
+  P.cell[t] = nid;
+#pragma unroll
+  for (int v = 0; v < 3; ++v) P.cur[v][t] = sn[v].f;
   dir[t] = (int8_t)dr;
   count_mover(t, dr != 0, dircnt);
-  // the next binning of the new position, with the per-cell count (parcels
-  // crossing a periodic boundary are binned by the haloswap once shifted)
-  int32_t nid = -1;
-  if (dr == 0) {
-    if (sn[2].i >= 0 && sn[2].i < g.Nz && sn[0].f >= 0.f && sn[0].f <= 1.f && sn[1].f >= 0.f && sn[1].f <= 1.f &&
-        sn[2].f >= 0.f && sn[2].f <= 1.f) {
-      nid = (int32_t)(((int64_t)sn[0].i * g.Ny + sn[1].i) * g.Nz + sn[2].i);
-      count_cell(nid, count);
-    } else {
-      atomicCAS(&info->error, 0, PMPIC_ERR_OUT_OF_BOX);
-    }
-  }
-  cell[t] = nid;
-}
-
-__global__ void k_reflect_classify_m(Geom g, int64_t n, const CellOff* __restrict__ X, const CellOff* __restrict__ Y,
-                                     CellOff* __restrict__ Z, int8_t* __restrict__ dir) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  Z[i] = co_reflect(Z[i], g.Nz);
-  dir[i] = (int8_t)classify_dir_m(g, X[i].i, Y[i].i);
+  count_cell(nid, count);
 }
 
 // the haloswap staging of the mixed form: each property as its 8-byte slot or
-// its 4-byte value, positions shifted by whole periods (haloswap.F90:531-559)
+// its 4-byte value, then the cell id; xo shifted by whole periods
+// (haloswap.F90:531-559).  The current position was wrapped already by the
+// kernel that moved it, and xf is relative to xo: neither changes.
+constexpr int SWAP_M = 30;  // 29 properties + the cell id per staged parcel
 __global__ void k_swap_gather_m(Geom g, const int32_t* __restrict__ nmov, const int32_t* __restrict__ M,
                                 const int8_t* __restrict__ dir, const double* __restrict__ parcels, int64_t cap,
-                                double* __restrict__ buf) {
+                                const int32_t* __restrict__ cell, double* __restrict__ buf) {
   const int nm = *nmov;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)nm * 29;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)nm * SWAP_M;
        e += (int64_t)gridDim.x * blockDim.x) {
-    const int t = (int)(e / 29), q = (int)(e - (int64_t)t * 29);
+    const int t = (int)(e / SWAP_M), q = (int)(e - (int64_t)t * SWAP_M);
     const int src = M[t];
+    if (q == 29) {
+      buf[e] = (double)cell[src];
+      continue;
+    }
     const int pid = c_swap_props[q];
     const double* A = parcels + (size_t)pid * cap;
     if (mixed_elem_bytes(pid) == 4) {
@@ -901,53 +915,38 @@ __global__ void k_swap_gather_m(Geom g, const int32_t* __restrict__ nmov, const 
       continue;
     }
     double v = A[src];
-    const int d = dir[src];
-    int sx = 0, sy = 0;
-    if (d == 3 || d == 2 || d == 4) sx = -g.Nx;
-    else if (d == 7 || d == 8 || d == 6) sx = g.Nx;
-    if (d == 1 || d == 2 || d == 8) sy = -g.Ny;
-    else if (d == 5 || d == 6 || d == 4) sy = g.Ny;
-    if (pid == PMPIC_PROP_X || pid == PMPIC_PROP_XO || pid == PMPIC_PROP_XF || pid == PMPIC_PROP_Y ||
-        pid == PMPIC_PROP_YO || pid == PMPIC_PROP_YF) {
+    if (pid == PMPIC_PROP_XO || pid == PMPIC_PROP_YO) {
+      const int d = dir[src];
+      int sh = 0;
+      if (pid == PMPIC_PROP_XO) {
+        if (d == 3 || d == 2 || d == 4) sh = -g.Nx;
+        else if (d == 7 || d == 8 || d == 6) sh = g.Nx;
+      } else {
+        if (d == 1 || d == 2 || d == 8) sh = -g.Ny;
+        else if (d == 5 || d == 6 || d == 4) sh = g.Ny;
+      }
       CellOff c = *(const CellOff*)&v;
-      c.i += (pid == PMPIC_PROP_X || pid == PMPIC_PROP_XO || pid == PMPIC_PROP_XF) ? sx : sy;
+      c.i += sh;
       v = *(const double*)&c;
     }
     buf[e] = v;
   }
 }
 __global__ void k_swap_scatter_m(const int32_t* __restrict__ nmov, const int32_t* __restrict__ V,
-                                 const double* __restrict__ buf, double* __restrict__ parcels, int64_t cap) {
+                                 const double* __restrict__ buf, double* __restrict__ parcels, int64_t cap,
+                                 int32_t* __restrict__ cell) {
   const int nm = *nmov;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)nm * 29;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)nm * SWAP_M;
        e += (int64_t)gridDim.x * blockDim.x) {
-    const int t = (int)(e / 29), q = (int)(e - (int64_t)t * 29);
+    const int t = (int)(e / SWAP_M), q = (int)(e - (int64_t)t * SWAP_M);
+    if (q == 29) {
+      cell[V[t]] = (int32_t)buf[e];
+      continue;
+    }
     const int pid = c_swap_props[q];
     double* A = parcels + (size_t)pid * cap;
     if (mixed_elem_bytes(pid) == 4) ((float*)A)[V[t]] = (float)buf[e];
     else A[V[t]] = buf[e];
-  }
-}
-
-// binning and count of the parcels a haloswap moved, in their new slots V[t]
-// (the mixed RK4 stage kernel binned the others)
-__global__ void k_swap_bin_m(Geom g, const int32_t* __restrict__ nmov, const int32_t* __restrict__ V,
-                             const CellOff* __restrict__ X, const CellOff* __restrict__ Y,
-                             const CellOff* __restrict__ Z, int32_t* __restrict__ cell, int32_t* __restrict__ count,
-                             DevInfo* info) {
-  const int nm = *nmov;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nm; t += gridDim.x * blockDim.x) {
-    const int s = V[t];
-    const CellOff x = X[s], y = Y[s], z = Z[s];
-    int32_t id = -1;
-    if (x.i >= 0 && x.i < g.Nx && y.i >= 0 && y.i < g.Ny && z.i >= 0 && z.i < g.Nz && x.f >= 0.f && x.f <= 1.f &&
-        y.f >= 0.f && y.f <= 1.f && z.f >= 0.f && z.f <= 1.f) {
-      id = (int32_t)(((int64_t)x.i * g.Ny + y.i) * g.Nz + z.i);
-      atomicAdd(&count[id], 1);
-    } else {
-      atomicCAS(&info->error, 0, PMPIC_ERR_OUT_OF_BOX);
-    }
-    cell[s] = id;
   }
 }
 
@@ -965,16 +964,12 @@ __global__ void k_split_flag_m(int64_t n, double* __restrict__ parcels, int64_t 
   F(PMPIC_PROP_STRETCH)[i] = s;
   flag[i] = s > 4.f ? 1 : 0;
 }
-// With count given (the binning's cell ids and counts are current, dir
-// given too), the parent's count moves to its new cell and the child is
-// counted in its own; a parent or child that leaves the domain is binned by
-// the haloswap once shifted (k_swap_bin_m).
-__device__ __forceinline__ int32_t split_cell_m(const Geom& g, const CellOff* p, int d) {
-  if (d != 0 || p[2].i < 0 || p[2].i >= g.Nz || !(p[0].f >= 0.f && p[0].f <= 1.f) || !(p[1].f >= 0.f && p[1].f <= 1.f) ||
-      !(p[2].f >= 0.f && p[2].f <= 1.f))
-    return -1;
-  return (int32_t)(((int64_t)p[0].i * g.Ny + p[1].i) * g.Nz + p[2].i);
-}
+// The parent shifted by -r w / |w| and the child at +r w / |w| (:95-127) from
+// the parent's current position, reflected, classified and wrapped as an
+// RK4 stage places a parcel (place_m); their cell ids written, and with count
+// given (the cell counts are current) the parent's count moved to its new
+// cell and the child counted in its own.  dir and the per-block mover counts
+// are for the haloswap that follows (:134).
 __global__ void k_split_apply_m(Geom g, int64_t n, const int32_t* __restrict__ list, const int32_t* __restrict__ nsplit,
                                 double* __restrict__ parcels, int64_t cap, DevInfo* info, int8_t* __restrict__ dir,
                                 int32_t* __restrict__ dircnt, int32_t* __restrict__ cell, int32_t* __restrict__ count) {
@@ -992,43 +987,41 @@ __global__ void k_split_apply_m(Geom g, int64_t n, const int32_t* __restrict__ l
       continue;
     }
     auto F = [&](int pid) { return (float*)(parcels + (size_t)pid * cap); };
-    auto C = [&](int pid) { return (CellOff*)(parcels + (size_t)pid * cap); };
     const float vol = F(PMPIC_PROP_VOL)[i];
     const float r = powf(vol / 4.f / pi, 1.f / 3.f);  // :78-79
     const float pp = F(PMPIC_PROP_P)[i], qq = F(PMPIC_PROP_Q)[i], rr = F(PMPIC_PROP_R)[i];
     const float absw = sqrtf(pp * pp + qq * qq + rr * rr);
     const float w[3] = {pp / absw, qq / absw, rr / absw};
-    const int pos[3] = {PMPIC_PROP_X, PMPIC_PROP_Y, PMPIC_PROP_Z};
+    const int32_t old = cell[i];
+    int ix[3];
+    cell_decode(g, old, ix[0], ix[1], ix[2]);
     CellOff pc[3], pi_[3];
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
-      const CellOff x = C(pos[v])[i];
+      const CellOff x = CellOff{ix[v], F(PMPIC_PROP_X + v)[i]};
       const float sh = r * w[v] * inv[v];
       pc[v] = co_add(x, sh);    // :95-118
       pi_[v] = co_add(x, -sh);  // :121-127
     }
-    if (dir) {  // reflected and classified here (k_split_apply)
-      pc[2] = co_reflect(pc[2], g.Nz);
-      pi_[2] = co_reflect(pi_[2], g.Nz);
-      const int dc = classify_dir_m(g, pc[0].i, pc[1].i), di = classify_dir_m(g, pi_[0].i, pi_[1].i);
-      dir[c] = (int8_t)dc;
-      dir[i] = (int8_t)di;
-      if (dc) atomicAdd(&dircnt[c / CITEMS], 1);
-      if (di) atomicAdd(&dircnt[i / CITEMS], 1);
-      if (count) {
-        const int32_t old = cell[i], ni = split_cell_m(g, pi_, di), nc = split_cell_m(g, pc, dc);
-        if (old >= 0) atomicSub(&count[old], 1);
-        if (ni >= 0) atomicAdd(&count[ni], 1);
-        if (nc >= 0) atomicAdd(&count[nc], 1);
-        if ((ni < 0 && di == 0) || (nc < 0 && dc == 0)) atomicCAS(&info->error, 0, PMPIC_ERR_OUT_OF_BOX);
-        cell[i] = ni;
-        cell[c] = nc;
-      }
+    pc[2] = co_reflect(pc[2], g.Nz);
+    pi_[2] = co_reflect(pi_[2], g.Nz);
+    int dc, di;
+    const int32_t nc = place_m(g, pc, dc, info), ni = place_m(g, pi_, di, info);
+    dir[c] = (int8_t)dc;
+    dir[i] = (int8_t)di;
+    if (dc) atomicAdd(&dircnt[c / CITEMS], 1);
+    if (di) atomicAdd(&dircnt[i / CITEMS], 1);
+    if (count) {
+      atomicSub(&count[old], 1);
+      atomicAdd(&count[ni], 1);
+      atomicAdd(&count[nc], 1);
     }
+    cell[i] = ni;
+    cell[c] = nc;
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
-      C(pos[v])[c] = pc[v];
-      C(pos[v])[i] = pi_[v];
+      F(PMPIC_PROP_X + v)[c] = pc[v].f;
+      F(PMPIC_PROP_X + v)[i] = pi_[v].f;
     }
 #pragma unroll
     for (int q = 0; q < 11; ++q) F(fprops[q])[c] = F(fprops[q])[i];
@@ -1040,13 +1033,14 @@ __global__ void k_split_apply_m(Geom g, int64_t n, const int32_t* __restrict__ l
   }
 }
 
-// btot (vorticity_tendency.F90:121-126) in FP32, z from the cell position
+// btot (vorticity_tendency.F90:121-126) in FP32, z from the current cell layer and offset
 __global__ void k_btot_m(Geom g, int64_t n, const float* __restrict__ B, const float* __restrict__ H,
-                         const CellOff* __restrict__ Z, float* __restrict__ BT) {
+                         const int32_t* __restrict__ cell, const float* __restrict__ FZ, float* __restrict__ BT) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const CellOff z = Z[i];
-  const float zz = ((float)z.i + z.f) * (float)g.dz;
+  int ci, cj, ck;
+  cell_decode(g, cell[i], ci, cj, ck);
+  const float zz = ((float)ck + FZ[i]) * (float)g.dz;
   BT[i] = B[i] + 12.5f * fmaxf(0.f, H[i] - expf(-zz));
 }
 
@@ -1063,7 +1057,7 @@ __global__ void k_new_parcels_m(Geom g, const int32_t* __restrict__ olist, const
                                 const float* __restrict__ KH, const float* __restrict__ KP,
                                 const float* __restrict__ KQ, const float* __restrict__ KR,
                                 int32_t* __restrict__ newslot, float* __restrict__ portion, float vmin,
-                                DevInfo* info) {
+                                int32_t* __restrict__ cell, DevInfo* info) {
   const int na = *nnew, nz0 = *nzero;
   for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < na; a += (int64_t)gridDim.x * blockDim.x) {
     const int64_t o = olist[a];
@@ -1089,10 +1083,10 @@ __global__ void k_new_parcels_m(Geom g, const int32_t* __restrict__ olist, const
     const float v = box(KV);
     const float por = 2.f * vmin / v;
     auto F = [&](int pid) { return (float*)(parcels + (size_t)pid * cap); };
-    auto C = [&](int pid) { return (CellOff*)(parcels + (size_t)pid * cap); };
-    C(PMPIC_PROP_X)[slot] = CellOff{i, 0.5f};  // the cell centre
-    C(PMPIC_PROP_Y)[slot] = CellOff{j, 0.5f};
-    C(PMPIC_PROP_Z)[slot] = CellOff{k, 0.5f};
+    cell[slot] = (int32_t)o;  // the cell centre (the loop order o is the cell id)
+    F(PMPIC_PROP_X)[slot] = 0.5f;
+    F(PMPIC_PROP_Y)[slot] = 0.5f;
+    F(PMPIC_PROP_Z)[slot] = 0.5f;
     F(PMPIC_PROP_VOL)[slot] = 2.f * vmin;
     F(PMPIC_PROP_STRETCH)[slot] = 0.f;
     F(PMPIC_PROP_B)[slot] = box(KB) / v;
@@ -1141,23 +1135,24 @@ __global__ void k_residual_update_m(Geom g, ResPtrsF RP, const int32_t* __restri
 }
 __global__ void __launch_bounds__(256, 6) k_redistribute_m(Geom g, int64_t norig, const int32_t* __restrict__ keep,
                                                           double* __restrict__ parcels, int64_t cap,
+                                                          const int32_t* __restrict__ cell,
                                                           const float* __restrict__ G8) {
   const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= norig) return;
   auto F = [&](int pid) { return (float*)(parcels + (size_t)pid * cap); };
-  auto C = [&](int pid) { return (CellOff*)(parcels + (size_t)pid * cap); };
   const int pids[5] = {PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
   // the state is read before the keep flag is known (one round trip less)
   const int kp = keep[m];
-  const CellOff px = C(PMPIC_PROP_X)[m], py = C(PMPIC_PROP_Y)[m], pz = C(PMPIC_PROP_Z)[m];
+  const int32_t id = cell[m];
+  const float delx = F(PMPIC_PROP_X)[m], dely = F(PMPIC_PROP_Y)[m], delz = F(PMPIC_PROP_Z)[m];
   const float v = F(PMPIC_PROP_VOL)[m];
   float s[5];
 #pragma unroll
   for (int q = 0; q < 5; ++q) s[q] = F(pids[q])[m];
-  const int ci = px.i, cj = py.i, ck = pz.i;
   if (kp != 1) return;
-  if (ci < 0 || ci >= g.Nx || cj < 0 || cj >= g.Ny || ck < 0 || ck >= g.Nz) return;  // reported by the binning
-  const float delx = px.f, dely = py.f, delz = pz.f;
+  if (id < 0 || id >= g.ncell) return;  // reported by the binning
+  int ci, cj, ck;
+  cell_decode(g, id, ci, cj, ck);
   const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
 #pragma unroll
   for (int q = 0; q < 5; ++q) s[q] = s[q] * v;
@@ -1195,58 +1190,58 @@ __global__ void k_mix_uncount(const int32_t* __restrict__ zlist, const int32_t* 
   }
 }
 __global__ void k_mix_recount(Geom g, int64_t norig, int64_t nfinal, const int32_t* __restrict__ keep,
-                              const CellOff* __restrict__ X, const CellOff* __restrict__ Y,
-                              const CellOff* __restrict__ Z, int32_t* __restrict__ cell,
-                              int32_t* __restrict__ count, DevInfo* info) {
+                              const int32_t* __restrict__ cell, int32_t* __restrict__ count, DevInfo* info) {
   const int64_t hi = norig > nfinal ? norig : nfinal;
   for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < hi; s += (int64_t)gridDim.x * blockDim.x) {
     if (s < nfinal) {
       if (s < norig && keep[s] == 1) continue;  // unchanged
-      const CellOff x = X[s], y = Y[s], z = Z[s];
-      int32_t id = -1;
-      if (x.i >= 0 && x.i < g.Nx && y.i >= 0 && y.i < g.Ny && z.i >= 0 && z.i < g.Nz && x.f >= 0.f && x.f <= 1.f &&
-          y.f >= 0.f && y.f <= 1.f && z.f >= 0.f && z.f <= 1.f) {
-        id = (int32_t)(((int64_t)x.i * g.Ny + y.i) * g.Nz + z.i);
-        atomicAdd(&count[id], 1);
-      } else {
-        atomicCAS(&info->error, 0, PMPIC_ERR_OUT_OF_BOX);
-      }
-      cell[s] = id;
+      const int32_t id = cell[s];  // written with the slot's new position
+      if (id >= 0 && id < g.ncell) atomicAdd(&count[id], 1);
+      else atomicCAS(&info->error, 0, PMPIC_ERR_OUT_OF_BOX);
     } else if (keep[s] == 1) {  // s < norig: a kept parcel dropped beyond the final count
       const int32_t c = cell[s];
       if (c >= 0) atomicSub(&count[c], 1);
     }
   }
 }
+// backfill (:347-389) of the mixed form: the 11 properties of k_backfill and
+// the cell id, the rest of the slot's current position
 __global__ void k_backfill_m(const int32_t* __restrict__ zlist, const int32_t* __restrict__ nz,
                              const int32_t* __restrict__ olist, const int32_t* __restrict__ no,
-                             double* __restrict__ parcels, int64_t cap, DevInfo* info) {
+                             double* __restrict__ parcels, int64_t cap, int32_t* __restrict__ cell, DevInfo* info) {
   const int nzero = *nz, nones = *no;
   if (blockIdx.x == 0 && threadIdx.x == 0 && nzero > nones) atomicCAS(&info->error, 0, PMPIC_ERR_BACKFILL);
   const int pids[11] = {PMPIC_PROP_X, PMPIC_PROP_Y, PMPIC_PROP_Z, PMPIC_PROP_P,   PMPIC_PROP_Q,      PMPIC_PROP_R,
                         PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_VOL, PMPIC_PROP_TAG, PMPIC_PROP_STRETCH};
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)nzero * 11;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)nzero * 12;
        e += (int64_t)gridDim.x * blockDim.x) {
-    const int t = (int)(e / 11), q = (int)(e - (int64_t)t * 11);
+    const int t = (int)(e / 12), q = (int)(e - (int64_t)t * 12);
     if (t >= nones) continue;
     const int dst = zlist[t], src = olist[nones - 1 - t];
+    if (q == 11) {
+      cell[dst] = cell[src];
+      continue;
+    }
     double* A = parcels + (size_t)pids[q] * cap;
     if (mixed_elem_bytes(pids[q]) == 4) ((float*)A)[dst] = ((const float*)A)[src];
     else A[dst] = A[src];
   }
 }
 // grid2par of three FP32 grids into three float properties at the current positions
-__global__ void k_grid2par_m(Geom g, int64_t n, const CellOff* __restrict__ X, const CellOff* __restrict__ Y,
-                             const CellOff* __restrict__ Z, const float* __restrict__ G0, const float* __restrict__ G1,
-                             const float* __restrict__ G2, float* __restrict__ O0, float* __restrict__ O1,
-                             float* __restrict__ O2) {
+__global__ void k_grid2par_m(Geom g, int64_t n, const int32_t* __restrict__ cell, const float* __restrict__ FX,
+                             const float* __restrict__ FY, const float* __restrict__ FZ, const float* __restrict__ G0,
+                             const float* __restrict__ G1, const float* __restrict__ G2, float* __restrict__ O0,
+                             float* __restrict__ O1, float* __restrict__ O2) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  const CellOff x = X[t], y = Y[t], z = Z[t];
-  if (x.i < 0 || x.i >= g.Nx || y.i < 0 || y.i >= g.Ny || z.i < 0 || z.i >= g.Nz) return;  // reported by the binning
-  O0[t] = g2p_f(g, G0, x.i, y.i, z.i, x.f, y.f, z.f);
-  O1[t] = g2p_f(g, G1, x.i, y.i, z.i, x.f, y.f, z.f);
-  O2[t] = g2p_f(g, G2, x.i, y.i, z.i, x.f, y.f, z.f);
+  const int32_t id = cell[t];
+  if (id < 0 || id >= g.ncell) return;  // reported by the binning
+  int ci, cj, ck;
+  cell_decode(g, id, ci, cj, ck);
+  const float fx = FX[t], fy = FY[t], fz = FZ[t];
+  O0[t] = g2p_f(g, G0, ci, cj, ck, fx, fy, fz);
+  O1[t] = g2p_f(g, G1, ci, cj, ck, fx, fy, fz);
+  O2[t] = g2p_f(g, G2, ci, cj, ck, fx, fy, fz);
 }
 
 // ---- test components (FP64 path) ---------------------------------------------------
@@ -1360,15 +1355,15 @@ int flush_gathers(pmpic_ctx* ctx) {
     const int64_t n = ctx->n;
     if (ctx->pending_uvw && n > 0) {
       k_grid2par_m<<<nblk(n, 256), 256, 0, ctx->stream>>>(
-          ctx->g, n, propc(ctx, PMPIC_PROP_X), propc(ctx, PMPIC_PROP_Y), propc(ctx, PMPIC_PROP_Z), G[PMPIC_GRID_U],
-          G[PMPIC_GRID_V], G[PMPIC_GRID_W], propf(ctx, PMPIC_PROP_DXDT), propf(ctx, PMPIC_PROP_DYDT),
-          propf(ctx, PMPIC_PROP_DZDT)); ++ctx->nlaunch;
+          ctx->g, n, ctx->cell, curoff(ctx, 0), curoff(ctx, 1), curoff(ctx, 2), G[PMPIC_GRID_U], G[PMPIC_GRID_V],
+          G[PMPIC_GRID_W], propf(ctx, PMPIC_PROP_DXDT), propf(ctx, PMPIC_PROP_DYDT), propf(ctx, PMPIC_PROP_DZDT));
+      ++ctx->nlaunch;
     }
     if (ctx->pending_pqr && n > 0) {
       k_grid2par_m<<<nblk(n, 256), 256, 0, ctx->stream>>>(
-          ctx->g, n, propc(ctx, PMPIC_PROP_X), propc(ctx, PMPIC_PROP_Y), propc(ctx, PMPIC_PROP_Z), G[PMPIC_GRID_DP],
-          G[PMPIC_GRID_DQ], G[PMPIC_GRID_DR], propf(ctx, PMPIC_PROP_DPDT), propf(ctx, PMPIC_PROP_DQDT),
-          propf(ctx, PMPIC_PROP_DRDT)); ++ctx->nlaunch;
+          ctx->g, n, ctx->cell, curoff(ctx, 0), curoff(ctx, 1), curoff(ctx, 2), G[PMPIC_GRID_DP], G[PMPIC_GRID_DQ],
+          G[PMPIC_GRID_DR], propf(ctx, PMPIC_PROP_DPDT), propf(ctx, PMPIC_PROP_DQDT), propf(ctx, PMPIC_PROP_DRDT));
+      ++ctx->nlaunch;
     }
     ctx->pending_uvw = ctx->pending_pqr = false;
     PMPIC_CUDA(cudaGetLastError());
@@ -1393,7 +1388,7 @@ int compute_btot(pmpic_ctx* ctx) {
   if (ctx->n == 0) return 0;
   if (ctx->mixed) {
     k_btot_m<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, propf(ctx, PMPIC_PROP_B),
-                                                         propf(ctx, PMPIC_PROP_H), propc(ctx, PMPIC_PROP_Z),
+                                                         propf(ctx, PMPIC_PROP_H), ctx->cell, curoff(ctx, 2),
                                                          propf(ctx, PMPIC_PROP_BTOT)); ++ctx->nlaunch;
     PMPIC_CUDA(cudaGetLastError());
     return 0;
@@ -1425,10 +1420,11 @@ int rk4_stage(pmpic_ctx* ctx, int stage) {
     const int F[6] = {PMPIC_PROP_XF, PMPIC_PROP_YF, PMPIC_PROP_ZF, PMPIC_PROP_PF, PMPIC_PROP_QF, PMPIC_PROP_RF};
     const int D[6] = {PMPIC_PROP_DXDT, PMPIC_PROP_DYDT, PMPIC_PROP_DZDT, PMPIC_PROP_DPDT, PMPIC_PROP_DQDT, PMPIC_PROP_DRDT};
     const int G[6] = {PMPIC_GRID_U, PMPIC_GRID_V, PMPIC_GRID_W, PMPIC_GRID_DP, PMPIC_GRID_DQ, PMPIC_GRID_DR};
+    P.cell = ctx->cell;
     for (int v = 0; v < 3; ++v) {
-      P.s[v] = propc(ctx, S[v]);
+      P.cur[v] = curoff(ctx, v);
       P.o[v] = propc(ctx, O[v]);
-      P.f[v] = propc(ctx, F[v]);
+      P.f[v] = propf(ctx, F[v]);
       P.sv[v] = propf(ctx, S[v + 3]);
       P.ov[v] = propf(ctx, O[v + 3]);
       P.fv[v] = propf(ctx, F[v + 3]);
@@ -1449,7 +1445,7 @@ int rk4_stage(pmpic_ctx* ctx, int stage) {
     // within pmpic_step the last stage also advances the stretch of the split
     // that follows (the haloswap in between moves it with its parcel)
     const bool adv = ctx->split_follows && stage == 4;
-    kern<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, P, stage, &ctx->dinfo->dtm, ctx->dir, ctx->cell,
+    kern<<<nblk(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->n, P, stage, &ctx->dinfo->dtm, ctx->dir,
                                                      ctx->cell_count, ctx->dinfo,
                                                      adv ? propf(ctx, PMPIC_PROP_STRETCH) : nullptr,
                                                      store_tendencies(ctx, stage), ctx->aux2); ++ctx->nlaunch;
@@ -1508,15 +1504,14 @@ int parcel_haloswap(pmpic_ctx* ctx) {
   ctx->btot_grid_ready = false;
   const bool ready = ctx->dir_ready;
   ctx->dir_ready = false;
-  // after an RK4 stage the parcels that stay are binned and counted already;
-  // the movers are binned below in their new slots
-  const bool counted = ready && ctx->count_ready;
-  ctx->count_ready = counted;
+  // mixed form: every parcel keeps its cell id (part of its position) as it
+  // is re-slotted, so the cell counts stay as the kernel that moved it left them
+  if (!ctx->mixed) ctx->count_ready = false;
   if (n == 0) return 0;
   if (!ready && ctx->mixed) {
-    k_reflect_classify_m<<<nblk(n, 256), 256, 0, ctx->stream>>>(ctx->g, n, propc(ctx, PMPIC_PROP_X),
-                                                                propc(ctx, PMPIC_PROP_Y), propc(ctx, PMPIC_PROP_Z),
-                                                                ctx->dir); ++ctx->nlaunch;
+    // positions of the mixed form are kept wrapped and reflected by every
+    // kernel that moves them: none is outside the domain
+    PMPIC_CUDA(cudaMemsetAsync(ctx->dir, 0, (size_t)n, ctx->stream));
   } else if (!ready) {
     k_reflect_classify<<<nblk(n, 256), 256, 0, ctx->stream>>>(ctx->g, n, prop(ctx, PMPIC_PROP_X),
                                                               prop(ctx, PMPIC_PROP_Y), prop(ctx, PMPIC_PROP_Z),
@@ -1534,12 +1529,10 @@ int parcel_haloswap(pmpic_ctx* ctx) {
   int32_t* nmc = dcounter(ctx, 1);
   k_check_swapcap<<<1, 1, 0, ctx->stream>>>(nm, nmc, ctx->swapcap, ctx->dinfo); ++ctx->nlaunch;
   if (ctx->mixed) {
-    k_swap_gather_m<<<592, 256, 0, ctx->stream>>>(ctx->g, nmc, M, ctx->dir, ctx->parcels, ctx->cap, ctx->swapbuf); ++ctx->nlaunch;
-    k_swap_scatter_m<<<592, 256, 0, ctx->stream>>>(nmc, V, ctx->swapbuf, ctx->parcels, ctx->cap); ++ctx->nlaunch;
-    if (counted) {
-      k_swap_bin_m<<<148, 256, 0, ctx->stream>>>(ctx->g, nmc, V, propc(ctx, PMPIC_PROP_X), propc(ctx, PMPIC_PROP_Y),
-                                                 propc(ctx, PMPIC_PROP_Z), ctx->cell, ctx->cell_count, ctx->dinfo); ++ctx->nlaunch;
-    }
+    k_swap_gather_m<<<592, 256, 0, ctx->stream>>>(ctx->g, nmc, M, ctx->dir, ctx->parcels, ctx->cap, ctx->cell,
+                                                   ctx->swapbuf); ++ctx->nlaunch;
+    k_swap_scatter_m<<<592, 256, 0, ctx->stream>>>(nmc, V, ctx->swapbuf, ctx->parcels, ctx->cap, ctx->cell);
+    ++ctx->nlaunch;
   } else {
     k_swap_gather<<<592, 256, 0, ctx->stream>>>(ctx->g, nmc, M, ctx->dir, ctx->parcels, ctx->cap, ctx->swapbuf); ++ctx->nlaunch;
     k_swap_scatter<<<592, 256, 0, ctx->stream>>>(nmc, V, ctx->swapbuf, ctx->parcels, ctx->cap); ++ctx->nlaunch;
@@ -1573,19 +1566,19 @@ int splitting(pmpic_ctx* ctx) {
     }
     if (rc) return rc;
     // after a haloswap only the split parcels can be outside the domain: the
-    // haloswap that follows needs no pass over all parcels to find them
+    // haloswap that follows needs no pass over all parcels to find them.  The
+    // mixed form's positions are always inside (kept wrapped and reflected).
     int8_t* dsplit = nullptr;
-    if (ctx->in_domain) {
+    if (ctx->in_domain || ctx->mixed) {
       PMPIC_CUDA(cudaMemsetAsync(ctx->dir, 0, (size_t)n, ctx->stream));
       PMPIC_CUDA(cudaMemsetAsync(ctx->aux2, 0, sizeof(int32_t) * ctx->nbmax, ctx->stream));  // mover counts
       dsplit = ctx->dir;
     }
     // on the mixed form the binning counts stay current through the split
-    const bool keep_counts = ctx->mixed && dsplit && ctx->count_ready;
+    const bool keep_counts = ctx->mixed && ctx->count_ready;
     if (ctx->mixed)
       k_split_apply_m<<<592, 256, 0, ctx->stream>>>(ctx->g, n, list, ns, ctx->parcels, ctx->cap, ctx->dinfo, dsplit,
-                                                    ctx->aux2, keep_counts ? ctx->cell : nullptr,
-                                                    keep_counts ? ctx->cell_count : nullptr);
+                                                    ctx->aux2, ctx->cell, keep_counts ? ctx->cell_count : nullptr);
     else
       k_split_apply<<<592, 256, 0, ctx->stream>>>(ctx->g, n, list, ns, ctx->parcels, ctx->cap, ctx->dinfo, dsplit,
                                                   ctx->aux2);
@@ -1701,13 +1694,13 @@ int mixing(pmpic_ctx* ctx) {
     float* por = (float*)ctx->newportion;
     k_new_parcels_m<<<592, 256, 0, ctx->stream>>>(g, olist, nnew, zlist, nz0, norig, ctx->cap, ctx->keep, ctx->parcels,
                                                   KF[0], KF[1], KF[2], KF[3], KF[4], KF[5], ctx->newslot, por,
-                                                  (float)g.vmin, ctx->dinfo); ++ctx->nlaunch;
+                                                  (float)g.vmin, ctx->cell, ctx->dinfo); ++ctx->nlaunch;
     k_residual_update_m<<<nblk(g.nphys, 256), 256, 0, ctx->stream>>>(g, RF, ctx->newslot, por); ++ctx->nlaunch;
     if (norig > 0) {
       const float* g7[7] = {KF[0], RF.r[0], RF.r[1], RF.r[2], RF.r[3], RF.r[4], RF.r[5]};
       pack8<float>(ctx, g7, (float*)ctx->gpack);
       k_redistribute_m<<<nblk(norig, 256), 256, 0, ctx->stream>>>(g, norig, ctx->keep, ctx->parcels, ctx->cap,
-                                                                  (const float*)ctx->gpack);
+                                                                  ctx->cell, (const float*)ctx->gpack);
       ++ctx->nlaunch;
     }
   } else {
@@ -1750,7 +1743,7 @@ int mixing(pmpic_ctx* ctx) {
     if ((rc = compact(ctx, PredKeepEq{ctx->keep, 0}, norig, z2, nz2))) return rc;
     if ((rc = compact(ctx, PredKeepEq{ctx->keep, 1}, norig, ones, no))) return rc;
     if (ctx->mixed)
-      k_backfill_m<<<592, 256, 0, ctx->stream>>>(z2, nz2, ones, no, ctx->parcels, ctx->cap, ctx->dinfo);
+      k_backfill_m<<<592, 256, 0, ctx->stream>>>(z2, nz2, ones, no, ctx->parcels, ctx->cap, ctx->cell, ctx->dinfo);
     else
       k_backfill<<<592, 256, 0, ctx->stream>>>(z2, nz2, ones, no, ctx->parcels, ctx->cap, ctx->dinfo);
     ++ctx->nlaunch;
@@ -1761,9 +1754,8 @@ int mixing(pmpic_ctx* ctx) {
   }
   if (ctx->mixed && (norig > 0 || count > 0)) {
     const int64_t hi = std::max<int64_t>(norig, count);
-    k_mix_recount<<<nblk(hi, 256), 256, 0, ctx->stream>>>(g, norig, count, ctx->keep, propc(ctx, PMPIC_PROP_X),
-                                                          propc(ctx, PMPIC_PROP_Y), propc(ctx, PMPIC_PROP_Z),
-                                                          ctx->cell, ctx->cell_count, ctx->dinfo); ++ctx->nlaunch;
+    k_mix_recount<<<nblk(hi, 256), 256, 0, ctx->stream>>>(g, norig, count, ctx->keep, ctx->cell, ctx->cell_count,
+                                                          ctx->dinfo); ++ctx->nlaunch;
   }
   ctx->n = count;
   ctx->sorted_valid = false;

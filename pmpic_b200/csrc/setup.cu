@@ -24,26 +24,35 @@ namespace {
 
 inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
-// one property value into slot s, in the context's precision
+// one property value into slot s, in the context's precision; a position as
+// its three components at once (the mixed form packs them into a cell id and
+// three offsets)
 struct ParcelSink {
   double* base;  // ctx->parcels
   int64_t cap;
   bool mixed;
-  double dx, dy, dz;
-  int Nx, Ny, Nz;
+  Geom g;
+  int32_t* cell;    // the mixed form's cell ids
+  DevInfo* info;
   __device__ __forceinline__ void put(int pid, int64_t s, double v) const {
     double* col = base + (size_t)pid * (size_t)cap;
-    if (!mixed || pid == PMPIC_PROP_TAG) {
-      col[s] = v;
-    } else if (pid == PMPIC_PROP_X) {
-      ((CellOff*)col)[s] = co_from_double(v, dx, Nx, 0);
-    } else if (pid == PMPIC_PROP_Y) {
-      ((CellOff*)col)[s] = co_from_double(v, dy, Ny, 0);
-    } else if (pid == PMPIC_PROP_Z) {
-      ((CellOff*)col)[s] = co_from_double(v, dz, 0, Nz);
-    } else {
-      ((float*)col)[s] = (float)v;
+    if (!mixed || pid == PMPIC_PROP_TAG) col[s] = v;
+    else ((float*)col)[s] = (float)v;
+  }
+  __device__ __forceinline__ void put_xyz(int64_t s, double x, double y, double z) const {
+    if (!mixed) {
+      base[(size_t)PMPIC_PROP_X * cap + s] = x;
+      base[(size_t)PMPIC_PROP_Y * cap + s] = y;
+      base[(size_t)PMPIC_PROP_Z * cap + s] = z;
+      return;
     }
+    int32_t id;
+    float fx, fy, fz;
+    if (!cur_from_double(g, x, y, z, id, fx, fy, fz)) atomicCAS(&info->error, 0, PMPIC_ERR_OUT_OF_BOX);
+    cell[s] = id;
+    ((float*)(base + (size_t)PMPIC_PROP_X * cap))[s] = fx;
+    ((float*)(base + (size_t)PMPIC_PROP_Y * cap))[s] = fy;
+    ((float*)(base + (size_t)PMPIC_PROP_Z * cap))[s] = fz;
   }
 };
 
@@ -52,8 +61,9 @@ ParcelSink sink_of(pmpic_ctx* ctx) {
   k.base = ctx->parcels;
   k.cap = ctx->cap;
   k.mixed = ctx->mixed;
-  k.dx = ctx->g.dx; k.dy = ctx->g.dy; k.dz = ctx->g.dz;
-  k.Nx = ctx->g.Nx; k.Ny = ctx->g.Ny; k.Nz = ctx->g.Nz;
+  k.g = ctx->g;
+  k.cell = ctx->cell;
+  k.info = ctx->dinfo;
   return k;
 }
 
@@ -127,17 +137,13 @@ __global__ void k_plume_write(PlumeLattice L, const int64_t* __restrict__ off, P
     if (ok) {
       const int64_t s = s0 + __popc(m & ((1u << lane) - 1u));
       if (plume) {
-        out.put(PMPIC_PROP_X, s, L.xpl[col / L.jpl]);
-        out.put(PMPIC_PROP_Y, s, L.ypl[col % L.jpl]);
-        out.put(PMPIC_PROP_Z, s, L.zpl[k]);
+        out.put_xyz(s, L.xpl[col / L.jpl], L.ypl[col % L.jpl], L.zpl[k]);
         out.put(PMPIC_PROP_B, s, L.b_pl * (1. + L.e1 * xp * yp + L.e2 * xp * zp + L.e3 * yp * zp));
         out.put(PMPIC_PROP_H, s, L.h_pl);
         out.put(PMPIC_PROP_VOL, s, L.vol_pl);
       } else {
         const int64_t c = col - L.npl;
-        out.put(PMPIC_PROP_X, s, L.xbg[c / L.jbg]);
-        out.put(PMPIC_PROP_Y, s, L.ybg[c % L.jbg]);
-        out.put(PMPIC_PROP_Z, s, L.zbg[k]);
+        out.put_xyz(s, L.xbg[c / L.jbg], L.ybg[c % L.jbg], L.zbg[k]);
         out.put(PMPIC_PROP_B, s, L.bbg[k]);
         out.put(PMPIC_PROP_H, s, L.hbg[k]);
         out.put(PMPIC_PROP_VOL, s, L.vol_bg);
@@ -152,9 +158,7 @@ __global__ void k_thermal(pmpic_thermal_params prm, ThermalGeom tg, int64_t n, P
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const ThermalParcel p = thermal_parcel(prm, tg, t);
-  out.put(PMPIC_PROP_X, t, p.x);
-  out.put(PMPIC_PROP_Y, t, p.y);
-  out.put(PMPIC_PROP_Z, t, p.z);
+  out.put_xyz(t, p.x, p.y, p.z);
   out.put(PMPIC_PROP_B, t, p.b);
   out.put(PMPIC_PROP_H, t, p.h);
   out.put(PMPIC_PROP_VOL, t, tg.v0);
@@ -188,9 +192,7 @@ __global__ void k_basic(BasicLattice L, int64_t n, ParcelSink out) {
   const double ddx = (lattice_coord(L.pxmin, i + 1, L.dx, L.bx) - xi) / L.s;
   const double ddy = (lattice_coord(L.pymin, j + 1, L.dy, L.by) - yj) / L.s;
   const double ddz = (lattice_coord(L.pzmin, k + 1, L.dz, L.bz) - zk) / L.s;
-  out.put(PMPIC_PROP_X, t, xi + ddx / 2 + (double)ii * ddx);
-  out.put(PMPIC_PROP_Y, t, yj + ddy / 2 + (double)jj * ddy);
-  out.put(PMPIC_PROP_Z, t, zk + ddz / 2 + (double)kk * ddz);
+  out.put_xyz(t, xi + ddx / 2 + (double)ii * ddx, yj + ddy / 2 + (double)jj * ddy, zk + ddz / 2 + (double)kk * ddz);
   out.put(PMPIC_PROP_VOL, t, 1.0);
 }
 

@@ -154,6 +154,69 @@ int diffz_coef(pmpic_ctx* ctx, bool bt, std::vector<double>& out) {
 }
 
 
+// The Thomas factors of laplinv (fft_ops.F90:505-601, :620-656) per boundary
+// form, level and wavenumber mode (a, b), from the k2 of the mode's columns:
+// the pivots den(k) and the ratios cp(k) = c(k-1) / den(k-1) of the
+// sequential recurrence, with the coefficients and the operation order of
+// k_laplinv (FP64: the same IEEE operations, so the device's FP64 solve keeps
+// its bits; FP32 form: 1/den and cp rounded to FP32).  Layout per form:
+// den[nz][nmodes], then cp[nz][nmodes].  A zero pivot is the reference's
+// abort (:642-645).
+int laplinv_tables(pmpic_ctx* ctx, const double* k2cols) {
+  const Geom& g = ctx->g;
+  const int nz = g.nzp, mx = g.sx / 2, my = g.sy / 2, nmode = mx * my;
+  const double f16 = f4div(1.f, 6.f), f13 = f4div(1.f, 3.f), f112 = f4div(1.f, 12.f), f56 = f4div(5.f, 6.f);
+  const double dz = g.dz;
+  const double i2dz2 = 2.0 / dz / dz, idz2 = 1.0 / dz / dz;
+  const size_t per_form = 2 * (size_t)nz * nmode;
+  std::vector<double> tab(2 * per_form, 0.0);
+  for (int form = 0; form < 2; ++form) {
+    double* DEN = tab.data() + form * per_form;
+    double* CP = DEN + (size_t)nz * nmode;
+    for (int b = 0; b < my; ++b)
+      for (int a = 0; a < mx; ++a) {
+        const int m = b * mx + a;
+        const double kk = k2cols[(size_t)(2 * b) * g.sx + 2 * a];
+        const double ai = idz2 - f112 * kk, bi = -i2dz2 - f56 * kk, ci = idz2 - f112 * kk;
+        double b1, c1, an, bn;
+        if (!form) {
+          b1 = 1.0; c1 = 0.0; an = 0.0; bn = 1.0;
+        } else {
+          b1 = -idz2 - f13 * kk;
+          c1 = idz2 - f16 * kk;
+          an = idz2 - f16 * kk;
+          bn = -idz2 - f13 * kk;
+        }
+        double den = b1, cprev = c1;
+        DEN[m] = den;
+        for (int k = 1; k < nz; ++k) {
+          const double ak = k < nz - 1 ? ai : an, bk = k < nz - 1 ? bi : bn, ck = k < nz - 1 ? ci : 0.0;
+          const double cp = cprev / den;
+          den = bk - ak * cp;
+          if (den == 0 && kk != 0)
+            return set_error(ctx, PMPIC_ERR_ZERO_PIVOT, "zero pivot in tridiagonal solver (laplinv)");
+          CP[(size_t)k * nmode + m] = cp;
+          DEN[(size_t)k * nmode + m] = den;
+          cprev = ck;
+        }
+      }
+  }
+  if (!ctx->mixed) {
+    PMPIC_CUDA(cudaMalloc(&ctx->lapcp, sizeof(double) * tab.size()));
+    PMPIC_CUDA(cudaMemcpy(ctx->lapcp, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
+    return 0;
+  }
+  std::vector<float> t32(tab.size());
+  for (int form = 0; form < 2; ++form)
+    for (size_t i = 0; i < per_form; ++i) {
+      const size_t e = form * per_form + i;
+      t32[e] = i < (size_t)nz * nmode ? (float)(1.0 / tab[e]) : (float)tab[e];
+    }
+  PMPIC_CUDA(cudaMalloc(&ctx->lapcp, sizeof(float) * t32.size()));
+  PMPIC_CUDA(cudaMemcpy(ctx->lapcp, t32.data(), sizeof(float) * t32.size(), cudaMemcpyHostToDevice));
+  return 0;
+}
+
 namespace f64 {
 using real = double;
 inline const double* tab_kx(pmpic_ctx* c) { return c->kx; }
@@ -213,12 +276,17 @@ int spectral_init(pmpic_ctx* ctx) {
   PMPIC_CUDA(cudaMemcpy(tabs.data() + 3 * cols, ctx->filt, sizeof(double) * cols, cudaMemcpyDeviceToHost));
   std::vector<float> t32(4 * cols + 6 * (size_t)g.nzp);
   for (size_t i = 0; i < 4 * cols; ++i) t32[i] = (float)tabs[i];
-  for (size_t i = 0; i < c0.size(); ++i) t32[4 * cols + i] = (float)c0[i];
-  for (size_t i = 0; i < c1.size(); ++i) t32[4 * cols + 3 * g.nzp + i] = (float)c1[i];
+  // diffz factors: a, the reciprocal pivots (from the FP64 recurrence), cp
+  const int nz = g.nzp;
+  for (int v = 0; v < 2; ++v) {
+    const std::vector<double>& c = v ? c1 : c0;
+    for (int i = 0; i < 3 * nz; ++i)
+      t32[4 * cols + (size_t)v * 3 * nz + i] = (i >= nz && i < 2 * nz) ? (float)(1.0 / c[i]) : (float)c[i];
+  }
   PMPIC_CUDA(cudaMalloc(&ctx->wn32, sizeof(float) * t32.size()));
   PMPIC_CUDA(cudaMemcpy(ctx->wn32, t32.data(), sizeof(float) * t32.size(), cudaMemcpyHostToDevice));
   PMPIC_CUDA(cudaMalloc(&ctx->hsum, sizeof(double) * 2 * g.nzp));
-  return 0;
+  return laplinv_tables(ctx, tabs.data() + 2 * cols);
 }
 
 int spec_diffx(pmpic_ctx* ctx, const double* in, double* out) { return f64::spec_diffx_impl(ctx, in, out); }

@@ -109,15 +109,31 @@ __global__ void k_bt_planes(Geom g, const real* __restrict__ a, const real* __re
 // ---- compact z operators ----------------------------------------------------------
 // The z recurrences run one thread per spectral column, so only about 14 warps
 // per SM are resident at 256^2 columns and a level costs the latency of its
-// dependent instructions, most of them the division.  Both forms divide with
-// IEEE rounding: the reciprocal-based quotient (2 ulp) measured ~4x the FP32
-// form's error after the 257-level recurrences (5.1e-5 against 1.3e-5
-// relative L2 for vort2vel alone at 256^3) for under 1% of a step.
-__device__ __forceinline__ real zdiv(real x, real y) { return x / y; }
+// dependent instructions.  The Thomas factors (pivots den and ratios cp of
+// fft_ops.F90:620-656) depend only on the level and, for laplinv, on the
+// column's wavenumber: they are tables built once at set-up.  The FP64 path
+// keeps the reference's operations bit for bit (its tables repeat the
+// sequential recurrence exactly; the right-hand side is still divided by the
+// pivot); the FP32 form multiplies by the reciprocal pivot (taken from the FP64
+// recurrence and rounded once) and fuses the multiply-adds, so a level is two
+// dependent operations.
+__device__ __forceinline__ real zstep(real d, real a, real prev, real den_or_rden) {
+  if constexpr (sizeof(real) == 8) return (d - a * prev) / den_or_rden;
+  else return __fmaf_rn(-a, prev, d) * den_or_rden;
+}
+__device__ __forceinline__ real zback(real f, real cp, real nxt) {
+  if constexpr (sizeof(real) == 8) return f - cp * nxt;
+  else return __fmaf_rn(-cp, nxt, f);
+}
+__device__ __forceinline__ real zfirst(real d, real den_or_rden) {
+  if constexpr (sizeof(real) == 8) return d / den_or_rden;
+  else return d * den_or_rden;
+}
 
 // diffz (fft_ops.F90:419-483).  The tridiagonal coefficients are the same for
-// every column, so the Thomas factors (cp and the denominators) are computed
-// once on the host with the reference's arithmetic and passed in.
+// every column, so the Thomas factors (cp and the pivots; the reciprocal
+// pivots on the FP32 form) are computed once on the host with the reference's
+// arithmetic and passed in.
 // blockIdx.y selects one of up to two independent solves in the same launch.
 struct DzBatch {
   const real* f[2];
@@ -127,7 +143,7 @@ struct DzBatch {
   real* sub;           // solve 0 only: c = c - diffz(f), c(1,:,:) = 0 (vort2vel.F90:196-205) in
                        // place of the final values in out
 };
-__global__ void k_diffz(Geom g, DzBatch zb, const real* __restrict__ coef /* a[nz], den[nz], cp[nz] */,
+__global__ void k_diffz(Geom g, DzBatch zb, const real* __restrict__ coef /* a[nz], den[nz] (FP32: 1/den), cp[nz] */,
                         real a1) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   const int cols = g.sx * g.sy;
@@ -150,7 +166,7 @@ __global__ void k_diffz(Geom g, DzBatch zb, const real* __restrict__ coef /* a[n
   constexpr int ZB = 8;
   real fm = f[col], f0 = f[cs + col];
   real d1 = bt ? f0 / dz - a1 * bot[col] * dz : real(0);
-  real prev = zdiv(d1, DEN[0]);
+  real prev = zfirst(d1, DEN[0]);
   out[col] = prev;
   for (int kb = 1; kb < nz - 1; kb += ZB) {
     real fb[ZB];
@@ -162,7 +178,7 @@ __global__ void k_diffz(Geom g, DzBatch zb, const real* __restrict__ coef /* a[n
       const int k = kb + u;
       if (k >= nz - 1) break;
       real d = (fb[u] - fm) / real(2) / dz;
-      prev = zdiv(d - A[k] * prev, DEN[k]);
+      prev = zstep(d, A[k], prev, DEN[k]);
       out[(uint32_t)k * cs + col] = prev;
       fm = f0;
       f0 = fb[u];
@@ -172,7 +188,7 @@ __global__ void k_diffz(Geom g, DzBatch zb, const real* __restrict__ coef /* a[n
   {
     int k = nz - 1;
     real dn = bt ? -fm / dz + a1 * top[col] * dz : real(0);  // fm = f(nz-1)
-    prev = zdiv(dn - A[k] * prev, DEN[k]);
+    prev = zstep(dn, A[k], prev, DEN[k]);
     if (sub) sub[(uint32_t)k * cs + col] = sub[(uint32_t)k * cs + col] - prev;
     else out[(uint32_t)k * cs + col] = prev;
   }
@@ -190,7 +206,7 @@ __global__ void k_diffz(Geom g, DzBatch zb, const real* __restrict__ coef /* a[n
     for (int u = 0; u < ZB; ++u) {
       const int k = kb - u;
       if (k < 0) break;
-      real v = ob[u] - CP[k + 1] * nxt;
+      real v = zback(ob[u], CP[k + 1], nxt);
       if (sub) {
         sub[(uint32_t)k * cs + col] = k == 0 ? real(0) : sb[u] - v;
       } else {
@@ -202,78 +218,77 @@ __global__ void k_diffz(Geom g, DzBatch zb, const real* __restrict__ coef /* a[n
 }
 
 // laplinv (fft_ops.F90:505-601), in place, one thread per column; columns with
-// k2 == 0 keep their input (:567).  cp is kept in a scratch array.
+// k2 == 0 keep their input (:567).  The Thomas factors of a column depend on
+// its wavenumber only, shared by the four columns (2a-1..2a, 2b-1..2b) of one
+// mode (a, b): tab holds, per boundary form (f0, df0), the pivots (FP32: their
+// reciprocals) and then the ratios cp, each [level][mode], built at set-up
+// (laplinv_tables).
 // blockIdx.y selects one of up to three arrays solved in the same launch
 struct LapBatch {
   real* f[3];
   int df0[3];
 };
-__global__ void k_laplinv(Geom g, LapBatch lb, real* __restrict__ cpbase, const real* __restrict__ k2) {
+__global__ void k_laplinv(Geom g, LapBatch lb, const real* __restrict__ tab, const real* __restrict__ k2) {
   int col = blockIdx.x * blockDim.x + threadIdx.x;
   const int cols = g.sx * g.sy;
   if (col >= cols) return;
   const int q = blockIdx.y;  // selected without indexing the parameter arrays (no local copy)
   real* __restrict__ f = q == 0 ? lb.f[0] : (q == 1 ? lb.f[1] : lb.f[2]);
-  real* __restrict__ cpbuf = cpbase + (size_t)q * g.nspec;
   const int df0 = q == 0 ? lb.df0[0] : (q == 1 ? lb.df0[1] : lb.df0[2]);
   const real kk = k2[col];
   if (kk == 0) return;
   const int nz = g.nzp;
   const int64_t cs = cols;
+  const int nmode = (g.sx >> 1) * (g.sy >> 1);
+  const int jp = col / g.sx, ip = col - jp * g.sx;
+  const real* __restrict__ DEN = tab + (size_t)(2 * df0) * nz * nmode + (jp >> 1) * (g.sx >> 1) + (ip >> 1);
+  const real* __restrict__ CP = DEN + (size_t)nz * nmode;
   const real f16 = (real)f4div(1.f, 6.f), f13 = (real)f4div(1.f, 3.f), f112 = (real)f4div(1.f, 12.f), f56 = (real)f4div(5.f, 6.f);
   const real dz = (real)g.dz;
-  const real i2dz2 = real(2) / dz / dz;
   const real idz2 = real(1) / dz / dz;
-  const real ai = idz2 - f112 * kk, bi = -i2dz2 - f56 * kk, ci = idz2 - f112 * kk;
-  real b1, c1, an, bn;
+  const real ai = idz2 - f112 * kk;
+  real an;
   real fm, f0, fp;
   f0 = f[col];
   fp = f[cs + col];
   real d;
   if (!df0) {
-    b1 = real(1); c1 = real(0); d = real(0);
-    an = real(0); bn = real(1);
+    d = real(0);
+    an = real(0);
   } else {
-    b1 = -idz2 - f13 * kk;
-    c1 = idz2 - f16 * kk;
     d = f13 * f0 + f16 * fp;
     an = idz2 - f16 * kk;
-    bn = -idz2 - f13 * kk;
   }
-  // tridiagonal (fft_ops.F90:620-656)
-  real den = b1;
-  real prev = zdiv(d, den);
+  // tridiagonal (fft_ops.F90:620-656) with the tabulated factors
+  real prev = zfirst(d, DEN[0]);
   f[col] = prev;
-  real cprev = c1;  // c(i-1)
   // loads of each batch of ZB levels first, then its recurrence (one memory
   // latency per batch); the batch reads f above the levels it overwrites
   constexpr int ZB = 8;
   for (int kb = 1; kb < nz; kb += ZB) {
-    real fb[ZB];
+    real fb[ZB], db[ZB];
 #pragma unroll
-    for (int u = 0; u < ZB; ++u)
+    for (int u = 0; u < ZB; ++u) {
       if (kb + u < nz - 1) fb[u] = f[(int64_t)(kb + u + 1) * cs + col];
+      if (kb + u < nz) db[u] = DEN[(size_t)(kb + u) * nmode];
+    }
 #pragma unroll
     for (int u = 0; u < ZB; ++u) {
       const int k = kb + u;
       if (k >= nz) break;
       fm = f0;
       f0 = fp;
-      real a, b, c;
+      real a;
       if (k < nz - 1) {
         fp = fb[u];
-        a = ai; b = bi; c = ci;
+        a = ai;
         d = f112 * fm + f56 * f0 + f112 * fp;
       } else {
-        a = an; b = bn; c = real(0);
+        a = an;
         d = df0 ? f13 * f0 + f16 * fm : real(0);
       }
-      real cp = zdiv(cprev, den);
-      den = b - a * cp;
-      prev = zdiv(d - a * prev, den);
+      prev = zstep(d, a, prev, db[u]);
       f[(int64_t)k * cs + col] = prev;
-      cpbuf[(int64_t)k * cs + col] = cp;
-      cprev = c;
     }
   }
   real nxt = prev;
@@ -283,13 +298,13 @@ __global__ void k_laplinv(Geom g, LapBatch lb, real* __restrict__ cpbase, const 
     for (int u = 0; u < ZB; ++u)
       if (kb - u >= 0) {
         fb[u] = f[(int64_t)(kb - u) * cs + col];
-        cb[u] = cpbuf[(int64_t)(kb - u + 1) * cs + col];
+        cb[u] = CP[(size_t)(kb - u + 1) * nmode];
       }
 #pragma unroll
     for (int u = 0; u < ZB; ++u) {
       const int k = kb - u;
       if (k < 0) break;
-      real v = fb[u] - cb[u] * nxt;
+      real v = zback(fb[u], cb[u], nxt);
       f[(int64_t)k * cs + col] = v;
       nxt = v;
     }
@@ -371,8 +386,7 @@ int spec_filter_impl(pmpic_ctx* ctx, const real* in, real* out) {
 int spec_diffz_impl(pmpic_ctx* ctx, const real* in, real* out, const real* bot, const real* top) {
   return diffz_launch_impl(ctx, in, out, bot, top);
 }
-// laplinv of na (1..3) arrays in one launch; the Thomas factors of array q go
-// to the scratch at q * nspec
+// laplinv of na (1..3) arrays in one launch, the Thomas factors from the tables
 int spec_laplinv_batch(pmpic_ctx* ctx, int na, real* const* fs, const bool* df0) {
   TimerScope ts(ctx, T_LAPLINV);
   const Geom& g = ctx->g;

@@ -276,3 +276,23 @@ def test_oracle_rejects_out_of_box():
                   vol=np.ones(2))
     with pytest.raises(Exception, match="out of box"):
         o.cache_weights()
+
+
+def test_conserved_sums_are_the_rounded_exact_totals():
+    """The oracle's compensated totals of vol, h*vol and b*vol equal the FP64
+    rounding of the exact totals (rational arithmetic), on values spread over
+    many magnitudes and signs, where a plain running sum loses digits."""
+    from fractions import Fraction
+    rng = np.random.default_rng(11)
+    n = 4000
+    vol = rng.uniform(0.5, 1.5, n) * 10.0 ** rng.integers(-8, 3, n)
+    h = rng.standard_normal(n) * 10.0 ** rng.integers(-6, 6, n)
+    b = rng.standard_normal(n)
+    o = Oracle(8, 8, 8, 1.0, 1.0, 1.0, max_parcels=n)
+    o.set_parcels(x=np.full(n, 0.5), y=np.full(n, 0.5), z=np.full(n, 0.5), vol=vol, h=h, b=b)
+    got = o.conserved_sums()
+    exact = [sum(Fraction(v) for v in vol), sum(Fraction(v) * Fraction(w) for v, w in zip(vol, h)),
+             sum(Fraction(v) * Fraction(w) for v, w in zip(vol, b))]
+    for g, e in zip(got, exact):
+        assert g == float(e), (g, float(e))
+    o.close()
