@@ -210,8 +210,8 @@ def algorithmic_bytes(kernel, precision, n_avg, nphys, calls, steps):
 # DRAM bytes per parcel of one launch, from ncu captures of the same kernels on
 # the 128^3 plume (16.8 M parcels; these kernels stream the parcel state once, so
 # traffic scales with parcels): RK4 stages 1-2 averaged, par2grid vort2vel pass.
-TRAFFIC_PER_PARCEL = {("rk4_kernel", "fp64"): 235.9, ("rk4_kernel", "mixed"): 162.6,
-                      ("par2grid", "fp64"): 108.6, ("par2grid", "mixed"): 64.6}
+TRAFFIC_PER_PARCEL = {("rk4_kernel", "fp64"): 235.9, ("rk4_kernel", "mixed"): 123.9,
+                      ("par2grid", "fp64"): 108.6, ("par2grid", "mixed"): 55.7}
 
 
 def run_form(precision, args, local, pg, headline):

@@ -77,13 +77,18 @@ __global__ void __launch_bounds__(CS_THREADS) k_sums(int64_t n, const R* __restr
   }
 }
 
-// one thread per quantity, the blocks' partials in block order
+// one warp per quantity: lane l sums the partials of blocks l, l + 32, ... in
+// order, then a fixed butterfly over the lanes
 __global__ void k_sums_final(int nblocks, const double* __restrict__ part, DevInfo* info) {
-  const int q = threadIdx.x;
+  const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (q >= 3) return;
   DD s{0.0, 0.0};
-  for (int k = 0; k < nblocks; ++k) s = dd_add(s, DD{part[(size_t)k * 6 + 2 * q], part[(size_t)k * 6 + 2 * q + 1]});
-  info->sums[q] = s.hi + s.lo;
+  for (int k = lane; k < nblocks; k += 32) s = dd_add(s, DD{part[(size_t)k * 6 + 2 * q], part[(size_t)k * 6 + 2 * q + 1]});
+  for (int o = 16; o > 0; o >>= 1) {
+    const DD t{__shfl_xor_sync(0xffffffffu, s.hi, o), __shfl_xor_sync(0xffffffffu, s.lo, o)};
+    s = (lane & o) ? dd_add(t, s) : dd_add(s, t);  // the lower lane's sum first on both sides
+  }
+  if (lane == 0) info->sums[q] = s.hi + s.lo;
 }
 
 }  // namespace
@@ -98,7 +103,7 @@ int conserved_sums(pmpic_ctx* ctx) {
     k_sums<double><<<nb, CS_THREADS, 0, ctx->stream>>>(n, prop(ctx, PMPIC_PROP_VOL), prop(ctx, PMPIC_PROP_H),
                                                         prop(ctx, PMPIC_PROP_B), ctx->csum);
   }
-  k_sums_final<<<1, 32, 0, ctx->stream>>>(nb, ctx->csum, ctx->dinfo);
+  k_sums_final<<<1, 96, 0, ctx->stream>>>(nb, ctx->csum, ctx->dinfo);
   ctx->nlaunch += 2;
   PMPIC_CUDA(cudaGetLastError());
   return 0;
