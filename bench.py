@@ -291,19 +291,27 @@ def run_form(precision, args, local, pg, headline):
     # then the gridded velocity
     done = args.warmup + args.steps
     late_work, late_steps = 0, 0
+    mixing_events = {"steps_with_removals": 0, "steps_with_new_parcels": 0, "split": 0, "removed": 0, "added": 0}
     L.pmpic_event_record(h, 6)
     while done < args.error_steps:
         late_work += ctx.n
         ctx.step(1)
         done += 1
         late_steps += 1
+        inf = ctx.info()  # the step has synchronised already; this reads the counters it left
+        mixing_events["steps_with_removals"] += int(inf.n_removed > 0)
+        mixing_events["steps_with_new_parcels"] += int(inf.n_added > 0)
+        mixing_events["split"] += int(inf.n_split)
+        mixing_events["removed"] += int(inf.n_removed)
+        mixing_events["added"] += int(inf.n_added)
     L.pmpic_event_record(h, 7)
     if late_steps:
         ms_late = C.c_float()
         L.pmpic_event_elapsed(h, 6, 7, C.byref(ms_late))
         t_late, late_all = combine(ms_late.value / 1e3, late_work, pg, "cuda")
         res["late_run"] = {"steps": f"{args.warmup + args.steps + 1}-{done}", "value": late_all / t_late,
-                           "ms_per_step": 1e3 * t_late / late_steps, "unit": UNIT}
+                           "ms_per_step": 1e3 * t_late / late_steps, "unit": UNIT,
+                           "events": mixing_events}
     res["steps_total"] = done
     res["n_final"] = ctx.n
     res["grids"] = {q: ctx.grid(q) for q in ("u", "v", "w")} if args.error_steps > 0 else None
@@ -616,15 +624,24 @@ def run_ensemble(args):
     """Batched ensemble of independent plumes in the mixed form: the members run
     one after another (concurrency 1, default tiles) and then batched (tuned
     tiles, concurrent members), each from the same initial state for the same
-    number of steps; then every member against the same plume on the FP64 path."""
+    number of steps; then every member against the same plume on the FP64 path.
+    Under torchrun the members are spread over the ranks by cost
+    (pmpic_b200.assign_members; no exchange between ranks): each rank runs its
+    share both ways, and the aggregate is all work over the max device time."""
     rank, world, local = dist_env()
-    if rank != 0:
-        return 0
     import torch
     torch.cuda.set_device(local)
     import pmpic_b200 as pm
-    spec = ensemble_members(args.members)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+        pg = dist
+    spec_all = ensemble_members(args.members)
     steps = args.ens_steps
+    mine = pm.assign_members([8 * m["G"] ** 3 * steps for m in spec_all], world)[rank]
+    spec = [spec_all[i] for i in mine]
 
     def ic(m):
         return pm.thermal_parcels(m["G"], m["G"], m["G"], radius=m["radius"], excess=m["excess"],
@@ -632,66 +649,86 @@ def run_ensemble(args):
     counts = [8 * m["G"] ** 3 for m in spec]
     cfgs = [dict(nx=m["G"], ny=m["G"], nz=m["G"], dtm=m["dt"], dtmax=m["dt"], max_parcels=int(1.15 * c),
                  precision="mixed") for m, c in zip(spec, counts)]
-    ens = pm.Ensemble(cfgs, device=local)
+    ens = pm.Ensemble(cfgs, device=local) if spec else None
+    members = ens.members if ens else []
 
     def load():
-        for mem, m in zip(ens.members, spec):
+        for mem, m in zip(members, spec):
             mem.upload(**ic(m))
         torch.cuda.synchronize()
 
     def work(n_before):
-        n_after = [mem.n for mem in ens.members]
+        n_after = [mem.n for mem in members]
         return sum(0.5 * (a + b) for a, b in zip(n_before, n_after)) * steps
 
-    load()
-    ens.set_concurrency(1)
-    n0 = [mem.n for mem in ens.members]
-    ms_seq = ens.step(steps)
-    w_seq = work(n0)
-    load()
-    for mem in ens.members:
-        pm.lib().pmpic_set_p2g_segment(mem._h, 64)
-    ens.autotune()
-    ens.set_concurrency(0)
-    n0 = [mem.n for mem in ens.members]
-    ms_bat = ens.step(steps)
-    w_bat = work(n0)
-    threads, xseg = ens.tuning()
-    grids = [{g: mem.grid(g) for g in ("u", "v", "w")} for mem in ens.members[:args.error_members]]
-    n_mixed = [mem.n for mem in ens.members]
-    ens.close()
+    ms_seq = ms_bat = ms_tune = 0.0
+    w_seq = w_bat = 0.0
+    threads, xseg = 0, []
     errs = []
-    for i, m in enumerate(spec[:args.error_members]):
-        G = m["G"]
-        c = pm.Context(G, G, G, 2 * np.pi, 2 * np.pi, np.pi, dtm=m["dt"], dtmax=m["dt"],
-                       max_parcels=int(1.15 * counts[i]), device=local)
-        c.upload(**ic(m))
-        c.step(steps)
-        e = {"member": i, "grid": G, "n_mixed": n_mixed[i], "n_fp64": c.n}
-        for g in ("u", "v", "w"):
-            ref = c.grid(g)
-            e[g + "_rel_l2"] = float(np.linalg.norm(grids[i][g] - ref) / max(np.linalg.norm(ref), 1e-300))
-        errs.append(e)
-        c.close()
-    seq_v, bat_v = w_seq / (ms_seq / 1e3), w_bat / (ms_bat / 1e3)
-    sizes = {}
-    for m, s_ in zip(spec, xseg):
-        sizes.setdefault(str(m["G"]), s_)
-    line = {"workload": "ensemble", "metric": "aggregate parcel-RK4-steps/s of the batched ensemble",
-            "unit": UNIT, "higher_is_better": True, "value": bat_v,
-            "config": {"members": len(spec), "steps": steps, "precision": "mixed",
-                       "grids": {str(G): sum(1 for m in spec if m["G"] == G) for G in (32, 48, 64, 96, 128)},
-                       "parcels_initial": int(sum(counts)), "dt": "0.32 / grid size",
-                       "timing": "device time from the first member's start to the last member's end "
-                                 "(events across all member streams); the batched run includes its "
-                                 "concurrency-tuning steps"},
-            "sequential": {"value": seq_v, "ms": ms_seq, "concurrency": 1, "par2grid_segment": 64},
-            "batched": {"value": bat_v, "ms": ms_bat, "concurrency": threads, "par2grid_segment_by_grid": sizes},
-            "batched_over_sequential": bat_v / seq_v,
-            "error_vs_fp64": {"members": errs,
-                              "max_rel_l2": max((max(e["u_rel_l2"], e["v_rel_l2"], e["w_rel_l2"]) for e in errs),
-                                                default=None)}}
-    print(json.dumps(line), flush=True)
+    if ens:
+        load()
+        ens.set_concurrency(1)
+        n0 = [mem.n for mem in members]
+        ms_seq = ens.step(steps)
+        w_seq = work(n0)
+        load()
+        for mem in members:
+            pm.lib().pmpic_set_p2g_segment(mem._h, 64)
+        ens.autotune()
+        # the host concurrency is tuned online (one step per candidate); those steps
+        # run before the timed window, then the initial state is loaded again
+        ens.set_concurrency(0)
+        ms_tune = ens.step(6)
+        load()
+        n0 = [mem.n for mem in members]
+        ms_bat = ens.step(steps)
+        w_bat = work(n0)
+        threads, xseg = ens.tuning()
+        grids = [{g: mem.grid(g) for g in ("u", "v", "w")} for mem in members[:args.error_members]]
+        n_mixed = [mem.n for mem in members]
+        ens.close()
+        for i, m in enumerate(spec[:args.error_members]):
+            G = m["G"]
+            c = pm.Context(G, G, G, 2 * np.pi, 2 * np.pi, np.pi, dtm=m["dt"], dtmax=m["dt"],
+                           max_parcels=int(1.15 * counts[i]), device=local)
+            c.upload(**ic(m))
+            c.step(steps)
+            e = {"member": mine[i], "grid": G, "n_mixed": n_mixed[i], "n_fp64": c.n}
+            for g in ("u", "v", "w"):
+                ref = c.grid(g)
+                e[g + "_rel_l2"] = float(np.linalg.norm(grids[i][g] - ref) / max(np.linalg.norm(ref), 1e-300))
+            errs.append(e)
+            c.close()
+    # every rank takes the same collective steps, members or not
+    t_seq, w_seq_all = combine(ms_seq / 1e3, w_seq, pg, "cuda")
+    t_bat, w_bat_all = combine(ms_bat / 1e3, w_bat, pg, "cuda")
+    emax_local = max((max(e["u_rel_l2"], e["v_rel_l2"], e["w_rel_l2"]) for e in errs), default=0.0)
+    emax, _ = combine(emax_local, 0.0, pg, "cuda")
+    if pg:
+        pg.barrier()
+    if rank == 0:
+        seq_v, bat_v = w_seq_all / t_seq, w_bat_all / t_bat
+        sizes = {}
+        for m, s_ in zip(spec, xseg):
+            sizes.setdefault(str(m["G"]), s_)
+        line = {"workload": "ensemble", "metric": "aggregate parcel-RK4-steps/s of the batched ensemble",
+                "unit": UNIT, "higher_is_better": True, "value": bat_v, "n_gpus": world,
+                "config": {"members": len(spec_all), "steps": steps, "precision": "mixed",
+                           "grids": {str(G): sum(1 for m in spec_all if m["G"] == G) for G in (32, 48, 64, 96, 128)},
+                           "parcels_initial": int(sum(8 * m["G"] ** 3 for m in spec_all)), "dt": "0.32 / grid size",
+                           "members_per_rank": "by cost (parcels x steps), largest first to the least-loaded rank",
+                           "timing": "device time from the first member's start to the last member's end "
+                                     "(events across all member streams; max over ranks); the batched run is "
+                                     "timed after its tuning (row-pass segments per grid size, then six steps "
+                                     "trying 2-64 host threads, then the initial state loaded again)"},
+                "sequential": {"value": seq_v, "ms": 1e3 * t_seq, "concurrency": 1, "par2grid_segment": 64},
+                "batched": {"value": bat_v, "ms": 1e3 * t_bat, "concurrency": threads,
+                            "par2grid_segment_by_grid": sizes, "tuning_ms": ms_tune},
+                "batched_over_sequential": bat_v / seq_v,
+                "error_vs_fp64": {"members_rank0": errs, "max_rel_l2_all_ranks": emax}}
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.destroy_process_group()
     return 0
 
 

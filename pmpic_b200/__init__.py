@@ -570,6 +570,24 @@ def read_grid_dump(path) -> dict:
     return out
 
 
+def assign_members(costs, ranks):
+    """Spreads ensemble members over `ranks` GPUs (one process each) by their
+    estimated cost (parcels x steps): largest first, each to the least-loaded
+    rank (ties to the lower rank), so that the ranks' loads differ by at most
+    one member's cost.  Members are independent: no exchange between ranks.
+    Returns per rank the member indices, ascending."""
+    if ranks < 1:
+        raise ValueError("ranks must be positive")
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0.0] * ranks
+    out = [[] for _ in range(ranks)]
+    for i in order:
+        r = min(range(ranks), key=lambda k: (load[k], k))
+        out[r].append(i)
+        load[r] += costs[i]
+    return [sorted(o) for o in out]
+
+
 class Ensemble:
     """Independent plumes of uneven sizes on one GPU, stepped concurrently
     (pmpic_ensemble_*; no counterpart in the reference).  members: a list of

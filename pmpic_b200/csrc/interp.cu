@@ -71,10 +71,16 @@ __global__ void k_bin_count_m(Geom g, int64_t n, const int32_t* __restrict__ cel
 }
 
 // Slots into their cells' ranges.  Each thread takes SC_ITEMS slots (a block's
-// slots are SC_ITEMS runs of 256) and issues all their fill atomics before it
-// uses any result, so their round trips overlap.  One atomic per distinct cell
-// of a warp; lanes take consecutive places in lane order (each segment is
-// sorted by slot afterwards in any case).
+// slots are SC_ITEMS runs of 256, a warp's 32 consecutive slots per item).
+// A cell whose slots form one contiguous run (parcels still in set-up order, or
+// at rest) is placed without atomics: the warp holding part of the run knows
+// the run's slots before and after its window (counted back and forward
+// against the cell's count), so each slot's place is start + its rank in the
+// run, the slot order.  Every other cell's slots take places from one fill
+// atomic per distinct cell of a warp (issued for all items before any result
+// is used, so their round trips overlap), and such a cell's segment is sorted
+// by slot afterwards (its fill counter is then non-zero).  Whether a cell is
+// one run is a property of the cell, so all its slots take the same path.
 constexpr int SC_ITEMS = 4;
 // the total of counts kept current by other kernels against the parcel count
 // (a mismatch would leave the cell index inconsistent: reported as an error)
@@ -82,6 +88,7 @@ __global__ void k_check_total(const int32_t* __restrict__ total, int64_t n, DevI
   if (*total != n) atomicCAS(&info->error, 0, PMPIC_ERR_STATE);
 }
 __global__ void __launch_bounds__(256) k_bin_scatter(int64_t n, const int32_t* __restrict__ cell,
+                                                     const int32_t* __restrict__ count,
                                                      const int32_t* __restrict__ start, int32_t* __restrict__ fill,
                                                      int32_t* __restrict__ sorted, int64_t lim) {
   constexpr unsigned FULL = 0xffffffffu;
@@ -99,10 +106,27 @@ __global__ void __launch_bounds__(256) k_bin_scatter(int64_t n, const int32_t* _
     same[k] = __match_any_sync(FULL, id[k]);
     base[k] = 0;
     st[k] = 0;
-    if (id[k] >= 0) {
-      if (lane == __ffs(same[k]) - 1) base[k] = atomicAdd(&fill[id[k]], __popc(same[k]));
-      st[k] = start[id[k]];
+    const int first = __ffs(same[k]) - 1;
+    if (id[k] >= 0 && lane == first) {
+      // the run containing this window's slots of the cell: contiguous here,
+      // extended by the cell's slots just before and after the window
+      const int64_t w0 = t0 + 256 * k - lane;  // the window's first slot
+      const int last = 31 - __clz(same[k]);
+      const unsigned m = same[k] >> first;
+      const int gsize = __popc(same[k]);
+      const int cnt = count[id[k]];
+      bool run = (m & (m + 1)) == 0;
+      int before = 0, after = 0;
+      if (run && gsize < cnt) {
+        if (first == 0)
+          for (int64_t s = w0 - 1; s >= 0 && before < cnt - gsize && cell[s] == id[k]; --s) ++before;
+        if (last == 31)
+          for (int64_t s = w0 + 32; s < n && before + after < cnt - gsize && cell[s] == id[k]; ++s) ++after;
+      }
+      run = run && before + gsize + after == cnt;
+      base[k] = run ? before : atomicAdd(&fill[id[k]], gsize);
     }
+    if (id[k] >= 0) st[k] = start[id[k]];
   }
 #pragma unroll
   for (int k = 0; k < SC_ITEMS; ++k) {
@@ -113,19 +137,23 @@ __global__ void __launch_bounds__(256) k_bin_scatter(int64_t n, const int32_t* _
 }
 
 // Each cell's segment sorted by slot index (the integer atomics above only
-// decide the order inside a cell).  A CTA takes SORT_CELLS consecutive cells,
-// whose segments are one contiguous range of the index: it is read into shared
-// memory with coalesced loads, every thread insertion-sorts its cell's segment
-// there (the slots are nearly in order already), and the range is written back.
+// decide the order inside a cell that did not lie in one run of slots; such a
+// cell's fill counter is non-zero).  A CTA takes SORT_CELLS consecutive cells,
+// whose segments are one contiguous range of the index: when any of them needs
+// it, the range is read into shared memory with coalesced loads, every thread
+// insertion-sorts its cell's segment there (the slots are nearly in order
+// already), and the range is written back.
 constexpr int SORT_CELLS = 256;
 constexpr int SORT_CAP = 8192;  // index entries a CTA stages (32 KB)
 __global__ void __launch_bounds__(SORT_CELLS) k_sort_segments(int64_t ncell, const int32_t* __restrict__ start,
+                                                              const int32_t* __restrict__ fill,
                                                               int32_t* __restrict__ sorted) {
   // staged position e sits at e + e/8: segments (~8 parcels each) start in
   // different banks for neighbouring threads
   __shared__ int32_t buf[SORT_CAP + SORT_CAP / 8];
   const int64_t c0 = (int64_t)blockIdx.x * SORT_CELLS;
   const int64_t c = c0 + threadIdx.x;
+  if (!__syncthreads_or(c < ncell && fill[c] != 0)) return;  // every segment here is one run: in order
   const int64_t c1 = min(c0 + SORT_CELLS, ncell);
   const int base = start[c0], m = start[c1] - base;
   int s0 = 0, len = 0;
@@ -722,9 +750,10 @@ int bin_and_sort(pmpic_ctx* ctx) {
     k_check_total<<<1, 1, 0, ctx->stream>>>(ctx->cell_start + g.ncell, n, ctx->dinfo); ++ctx->nlaunch;
   }
   if (n > 0) {
-    k_bin_scatter<<<nblk(n, 256 * SC_ITEMS), 256, 0, ctx->stream>>>(n, ctx->cell, ctx->cell_start, ctx->cell_fill,
-                                                                    ctx->sorted, ctx->cap); ++ctx->nlaunch;
-    k_sort_segments<<<nblk(g.ncell, SORT_CELLS), SORT_CELLS, 0, ctx->stream>>>(g.ncell, ctx->cell_start, ctx->sorted);
+    k_bin_scatter<<<nblk(n, 256 * SC_ITEMS), 256, 0, ctx->stream>>>(n, ctx->cell, ctx->cell_count, ctx->cell_start,
+                                                                    ctx->cell_fill, ctx->sorted, ctx->cap); ++ctx->nlaunch;
+    k_sort_segments<<<nblk(g.ncell, SORT_CELLS), SORT_CELLS, 0, ctx->stream>>>(g.ncell, ctx->cell_start,
+                                                                               ctx->cell_fill, ctx->sorted);
     ++ctx->nlaunch;
   }
   PMPIC_CUDA(cudaGetLastError());
@@ -1073,8 +1102,8 @@ extern "C" int pmpic_par2grid_static(int32_t nx, int32_t ny, int32_t nz, double 
   k_scan_sums<<<1, SCAN_BLOCK, 0, st>>>(tiles, ntiles, cstart + ncell);
   k_scan_apply<<<(unsigned)ntiles, SCAN_BLOCK, 0, st>>>(count, ncell, tiles, cstart);
   if (n > 0) {
-    k_bin_scatter<<<nblk(n, 256 * SC_ITEMS), 256, 0, st>>>(n, cell, cstart, fill, sorted, SP_MAX_PARCELS);
-    k_sort_segments<<<nblk(ncell, SORT_CELLS), SORT_CELLS, 0, st>>>(ncell, cstart, sorted);
+    k_bin_scatter<<<nblk(n, 256 * SC_ITEMS), 256, 0, st>>>(n, cell, count, cstart, fill, sorted, SP_MAX_PARCELS);
+    k_sort_segments<<<nblk(ncell, SORT_CELLS), SORT_CELLS, 0, st>>>(ncell, cstart, fill, sorted);
   }
   P2GArgs<1> a{};
   a.f[0] = field;

@@ -211,7 +211,8 @@ __device__ __forceinline__ void corner6(const Geom& g, const float* __restrict__
   hi[0] = d.x; hi[1] = d.y; hi[2] = e.x; hi[3] = e.y; hi[4] = f.x; hi[5] = f.y;
 }
 // grid2par (parcel_interpolation.F90:299-321) of all six packed fields: z,
-// then y, then x, in the reference's operation order
+// then y, then x, in the reference's operation order (FP64 path: every product
+// and sum rounded as there; the FP32 form fuses each product into its sum)
 template <class R>
 __device__ __forceinline__ void g2p_packed(const Geom& g, const R* __restrict__ G6, int ci, int cj, int ck, R delx,
                                            R dely, R delz, R* d) {
@@ -232,6 +233,26 @@ __device__ __forceinline__ void g2p_packed(const Geom& g, const R* __restrict__ 
   corner6(g, G6, ci1, cj1, ck, lo, hi);
 #pragma unroll
   for (int f = 0; f < 6; ++f) d[f] = c0[f] * ex + (c00[f] * ey + (lo[f] * ez + hi[f] * delz) * dely) * delx;
+}
+template <>
+__device__ __forceinline__ void g2p_packed<float>(const Geom& g, const float* __restrict__ G6, int ci, int cj, int ck,
+                                                  float delx, float dely, float delz, float* d) {
+  const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
+  const float ez = 1.f - delz, ey = 1.f - dely, ex = 1.f - delx;
+  float lo[6], hi[6], c00[6], c0[6];
+  corner6(g, G6, ci, cj, ck, lo, hi);
+#pragma unroll
+  for (int f = 0; f < 6; ++f) c00[f] = __fmaf_rn(hi[f], delz, lo[f] * ez);
+  corner6(g, G6, ci, cj1, ck, lo, hi);
+#pragma unroll
+  for (int f = 0; f < 6; ++f) c0[f] = __fmaf_rn(__fmaf_rn(hi[f], delz, lo[f] * ez), dely, c00[f] * ey);
+  corner6(g, G6, ci1, cj, ck, lo, hi);
+#pragma unroll
+  for (int f = 0; f < 6; ++f) c00[f] = __fmaf_rn(hi[f], delz, lo[f] * ez);
+  corner6(g, G6, ci1, cj1, ck, lo, hi);
+#pragma unroll
+  for (int f = 0; f < 6; ++f)
+    d[f] = __fmaf_rn(__fmaf_rn(__fmaf_rn(hi[f], delz, lo[f] * ez), dely, c00[f] * ey), delx, c0[f] * ex);
 }
 
 // ---- RK4 stage (rk4_integrator.F90:95-319) -----------------------------------------
@@ -792,7 +813,7 @@ __device__ __forceinline__ int32_t place_m(const Geom& g, CellOff* p, int& d, De
 // in its new cell (movers too: they keep their cell as the haloswap re-slots
 // them).
 template <bool GU, bool GP>
-__global__ void __launch_bounds__(256, 5) k_rk4_m(Geom g, int64_t n, MPtrs P, int stage, const double* __restrict__ dtp,
+__global__ void __launch_bounds__(256, 6) k_rk4_m(Geom g, int64_t n, MPtrs P, int stage, const double* __restrict__ dtp,
                         int8_t* __restrict__ dir, int32_t* __restrict__ count, DevInfo* info,
                         float* __restrict__ stretch, int store_d, int32_t* __restrict__ dircnt) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -838,26 +859,27 @@ __global__ void __launch_bounds__(256, 5) k_rk4_m(Geom g, int64_t n, MPtrs P, in
   for (int v = 0; v < 3; ++v) {
     const float dc = d[v] * inv[v];  // cell units per unit time
     const float dw = d[v + 3];
+    // the FP32 form fuses each increment into its sum
     if (stage == 1) {
       op[v] = CellOff{cx[v], cf[v]};
       ov[v] = sv[v];
       fd[v] = dt6 * dc;
-      fv[v] = sv[v] + dt6 * dw;
+      fv[v] = __fmaf_rn(dt6, dw, sv[v]);
       sn[v] = co_add(op[v], dt2 * dc);
-      svn[v] = sv[v] + dt2 * dw;
+      svn[v] = __fmaf_rn(dt2, dw, sv[v]);
     } else if (stage == 2) {
-      fd[v] = fd[v] + dt3 * dc;
-      fv[v] = fv[v] + dt3 * dw;
+      fd[v] = __fmaf_rn(dt3, dc, fd[v]);
+      fv[v] = __fmaf_rn(dt3, dw, fv[v]);
       sn[v] = co_add(op[v], dt2 * dc);
-      svn[v] = ov[v] + dt2 * dw;
+      svn[v] = __fmaf_rn(dt2, dw, ov[v]);
     } else if (stage == 3) {
-      fd[v] = fd[v] + dt3 * dc;
-      fv[v] = fv[v] + dt3 * dw;
+      fd[v] = __fmaf_rn(dt3, dc, fd[v]);
+      fv[v] = __fmaf_rn(dt3, dw, fv[v]);
       sn[v] = co_add(op[v], dt * dc);
-      svn[v] = ov[v] + dt * dw;
+      svn[v] = __fmaf_rn(dt, dw, ov[v]);
     } else {
-      fd[v] = fd[v] + dt6 * dc;
-      fv[v] = fv[v] + dt6 * dw;
+      fd[v] = __fmaf_rn(dt6, dc, fd[v]);
+      fv[v] = __fmaf_rn(dt6, dw, fv[v]);
       sn[v] = co_add(op[v], fd[v]);
       svn[v] = fv[v];
     }
@@ -1680,6 +1702,26 @@ int mixing(pmpic_ctx* ctx) {
   int32_t* olist = ctx->cell_fill;  // ncell entries; free after bin_and_sort
   int32_t* nnew = dcounter(ctx, 4);
   if ((rc = compact(ctx, PredNewCell{ctx->npercell, g.Nx, g.Ny, g.Nz}, g.ncell, olist, nnew))) return rc;
+  int32_t hnew = 0;
+  PMPIC_CUDA(cudaMemcpyAsync(&hnew, nnew, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
+  // A call that removes no parcel and adds none leaves every residual grid at
+  // zero: the redistribution (:245-342) would only re-round the kept parcels'
+  // properties (b v / v).  The mixed form skips it then; the FP64 path runs it,
+  // as the reference does, for the bits.
+  const bool events = hz0 > 0 || hnew > 0;
+  if (ctx->mixed && !events) {
+    const int64_t count0 = norig;
+    ctx->n = count0;
+    ctx->sorted_valid = false;
+    ctx->count_ready = true;  // no slot changed: the counts stand
+    ctx->in_domain = false;
+    ctx->btot_grid_ready = false;
+    ctx->info.n_removed = 0;
+    ctx->info.n_added = 0;
+    PMPIC_CUDA(cudaGetLastError());
+    return 0;
+  }
   PMPIC_CUDA(cudaMemsetAsync(ctx->newslot, 0xff, sizeof(int32_t) * g.ncell, ctx->stream));
   double* K[6] = {ctx->grid[PMPIC_GRID_VOL], ctx->grid[PMPIC_GRID_B], ctx->grid[PMPIC_GRID_HG],
                   ctx->grid[PMPIC_GRID_P],   ctx->grid[PMPIC_GRID_Q], ctx->grid[PMPIC_GRID_R]};
@@ -1720,12 +1762,7 @@ int mixing(pmpic_ctx* ctx) {
                                                                 ctx->cell, ctx->del, ctx->gpack); ++ctx->nlaunch;
     }
   }
-  // counts to the host: removed, new cells
-  int32_t h[2];
-  PMPIC_CUDA(cudaMemcpyAsync(&h[0], nz0, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
-  PMPIC_CUDA(cudaMemcpyAsync(&h[1], nnew, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
-  PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
-  const int64_t nremove = h[0], nadd = h[1];
+  const int64_t nremove = hz0, nadd = hnew;
   // count = max(n-1, numparcels_local) (:217)
   int64_t count = norig;
   if (nadd > nremove) count = norig + (nadd - nremove);
@@ -1733,9 +1770,10 @@ int mixing(pmpic_ctx* ctx) {
     // the last new parcel sits in a removed slot: count stays norig
     count = norig;
   }
-  if (count == norig) {
+  if (count == norig && nremove > 0) {
     // backfill: keep==0 slots now exclude the ones that received new parcels
-    // (keep = 2), except the last slot (:191-193)
+    // (keep = 2), except the last slot (:191-193).  With no removed slot there
+    // is no keep==0 slot and the reference's loop (:350-389) does nothing.
     int32_t* z2 = ctx->aux;
     int32_t* nz2 = dcounter(ctx, 5);
     int32_t* ones = ctx->aux2 + 2 * ctx->nbmax;

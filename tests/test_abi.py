@@ -222,3 +222,23 @@ def test_oracle_thermal_generator_matches_host_generator():
         for key in ("x", "y", "z", "p", "q", "r", "b", "h", "vol", "stretch", "tag"):
             np.testing.assert_array_equal(o.get(key), got[key], err_msg=key)
         o.close()
+
+
+def test_ensemble_members_spread_by_cost():
+    """pmpic_b200.assign_members: every member on exactly one rank, the ranks'
+    loads within one member's cost of each other, the same answer every time,
+    and a rank without members when there are more ranks than members."""
+    import pmpic_b200 as pm
+    import bench
+    spec = bench.ensemble_members(64)
+    costs = [8 * m["G"] ** 3 * 50 for m in spec]
+    for ranks in (1, 2, 3, 4, 8):
+        parts = pm.assign_members(costs, ranks)
+        assert len(parts) == ranks
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(len(costs)))
+        loads = [sum(costs[i] for i in p) for p in parts]
+        assert max(loads) - min(loads) <= max(costs)
+        assert parts == pm.assign_members(costs, ranks)
+    parts = pm.assign_members([5.0, 3.0], 3)
+    assert parts == [[0], [1], []]

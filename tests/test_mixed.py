@@ -175,3 +175,32 @@ def test_mixed_rejects_fp64_kernel_ops(pm):
     with pytest.raises(pm.PmpicError) as e:
         g.par2grid("b", "b")
     assert e.value.code == -9  # PMPIC_ERR_STATE
+
+
+def test_mixed_mixing_without_events_keeps_parcels(pm):
+    """A mixing call that removes no parcel and adds none leaves every residual
+    grid at zero; the mixed form then skips the redistribution: the parcels are
+    unchanged bit for bit, the counts report no event, and the kept-class grids
+    (the model's vol, b, hg, p, q, r grids of construct_grids) are still built,
+    within FP32 rounding of the oracle's."""
+    from oracle import Oracle
+    n = 16
+    ic = _vortical(pm, n)
+    k = len(ic["x"])
+    g = pm.Context(n, n, n, TWO_PI, TWO_PI, math.pi, max_parcels=2 * k, precision="mixed")
+    g.upload(**ic)
+    props = ["x", "y", "z", "p", "q", "r", "b", "h", "vol", "stretch", "tag"]
+    before = {q: g.get(q) for q in props}
+    g.set_counters([3, 3, 4, 3, 3])  # the next callbacks are the fourth substep's
+    g.parcel_mixing()
+    info = g.info()
+    assert info.n_removed == 0 and info.n_added == 0 and g.n == k
+    for q in props:
+        np.testing.assert_array_equal(g.get(q), before[q], err_msg=q)
+    o = Oracle(n, n, n, TWO_PI, TWO_PI, math.pi, max_parcels=2 * k)
+    o.set_parcels(**ic)
+    o.set_counters([3, 3, 4, 3, 3])
+    o.parcel_mixing()
+    assert o.info().n_removed == 0 and o.info().n_added == 0
+    for name in ["vol", "b", "hg", "p", "q", "r"]:
+        assert rel(g.grid(name), o.grid(name)) < 1e-5, name
