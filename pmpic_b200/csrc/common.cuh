@@ -322,6 +322,8 @@ struct pmpic_ctx {
   double* mixres[6];         // residual grids vres..rres
   int32_t* npercell;         // ncell
   int32_t* newslot;          // ncell: slot of the new parcel of a cell or -1
+  uint8_t* near;             // ncell (mixed form, mixing): cell within one of a cell with a
+                             // removed or a new parcel (its corners may hold residuals)
   double* newportion;        // ncell: portion of the new parcel of a cell
   // spectral arrays
   double* spec[PMPIC_NSPEC]; // u_s, v_s, w_s

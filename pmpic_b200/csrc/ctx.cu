@@ -122,7 +122,7 @@ void free_all(pmpic_ctx* c) {
                   c->aux,     c->aux2,     c->dir,       c->swapbuf,    c->scan_tmp,   c->npercell,  c->newslot,
                   c->newportion, c->sa,    c->sb,        c->sc,         c->sd,         c->se,        c->sf,
                   c->sas,     c->sbs,      c->sscratch,  c->fftmid,     c->ftw,        c->ftw32,      c->wn32,       c->hsum,       c->stage64,        c->kx,        c->ky,
-                  c->k2,      c->filt,     c->bt,        c->zmode,      c->csum,       c->dinfo};
+                  c->k2,      c->filt,     c->bt,        c->zmode,      c->csum,       c->near,       c->dinfo};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int i = 0; i < PMPIC_NGRID; ++i)
@@ -265,6 +265,7 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   for (int i = 0; i < 6 && !rc; ++i) rc = dalloc(ctx, &ctx->mixres[i], (size_t)g.nphys);
   if (!rc) rc = dalloc(ctx, &ctx->npercell, (size_t)g.ncell);
   if (!rc) rc = dalloc(ctx, &ctx->newslot, (size_t)g.ncell);
+  if (!rc && ctx->mixed) rc = dalloc(ctx, &ctx->near, (size_t)g.ncell);
   if (!rc) rc = dalloc(ctx, &ctx->newportion, (size_t)g.ncell);
   for (int i = 0; i < PMPIC_NSPEC && !rc; ++i) rc = dalloc(ctx, &ctx->spec[i], (size_t)g.nspec);
   double** sp[] = {&ctx->sa, &ctx->sb, &ctx->sc, &ctx->sd, &ctx->se, &ctx->sf, &ctx->sas, &ctx->sbs};
@@ -695,8 +696,10 @@ static int do_vort2vel(pmpic_ctx* ctx) {
   // vort2vel.F90:117-121: binning and par2grid of p, q, r with one set of
   // weights.  The par2grid(btot) of vorticity_tendency.F90:121-129 uses the
   // same weights and parcel state, so it runs in the same pass into a spare
-  // grid that the vorticity_tendency callback adopts.
-  if ((rc = bin_and_sort(ctx))) return rc;
+  // grid that the vorticity_tendency callback adopts.  The binning of a
+  // mixing call that moved, removed and added no parcel is still current.
+  if (!ctx->sorted_valid)
+    if ((rc = bin_and_sort(ctx))) return rc;
   // The pass computes the btot property (vorticity_tendency.F90:121-126) as it
   // stages each parcel and stores it.
   if (ctx->mixed) {

@@ -1067,6 +1067,18 @@ __global__ void k_btot_m(Geom g, int64_t n, const float* __restrict__ B, const f
 }
 
 // mixing (parcel_mixing.F90:68-431) in FP32
+// the cells whose corners a residual at the corners of cell id can reach: id
+// and its neighbours (periodic in x and y), marked in near
+__device__ __forceinline__ void mark_near(const Geom& g, int32_t id, uint8_t* __restrict__ near) {
+  int i, j, k;
+  cell_decode(g, id, i, j, k);
+  for (int dk = -1; dk <= 1; ++dk) {
+    const int kk = k + dk;
+    if (kk < 0 || kk >= g.Nz) continue;
+    for (int dj = -1; dj <= 1; ++dj)
+      for (int di = -1; di <= 1; ++di) near[cell_encode(g, wrap_index(i + di, g.Nx), wrap_index(j + dj, g.Ny), kk)] = 1;
+  }
+}
 __global__ void k_keep_m(int64_t n, const float* __restrict__ VOL, float vmin, int32_t* __restrict__ keep) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -1079,7 +1091,7 @@ __global__ void k_new_parcels_m(Geom g, const int32_t* __restrict__ olist, const
                                 const float* __restrict__ KH, const float* __restrict__ KP,
                                 const float* __restrict__ KQ, const float* __restrict__ KR,
                                 int32_t* __restrict__ newslot, float* __restrict__ portion, float vmin,
-                                int32_t* __restrict__ cell, DevInfo* info) {
+                                int32_t* __restrict__ cell, uint8_t* __restrict__ near, DevInfo* info) {
   const int na = *nnew, nz0 = *nzero;
   for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < na; a += (int64_t)gridDim.x * blockDim.x) {
     const int64_t o = olist[a];
@@ -1117,9 +1129,10 @@ __global__ void k_new_parcels_m(Geom g, const int32_t* __restrict__ olist, const
     F(PMPIC_PROP_Q)[slot] = box(KQ) / v;
     F(PMPIC_PROP_R)[slot] = box(KR) / v;
     if (slot + 1 < norig) keep[slot] = 2;
-    const int64_t cell = ((int64_t)k * g.Ny + j) * g.Nx + i;
-    newslot[cell] = (int32_t)slot;
-    portion[cell] = por;
+    const int64_t gcell = ((int64_t)k * g.Ny + j) * g.Nx + i;
+    newslot[gcell] = (int32_t)slot;
+    portion[gcell] = por;
+    mark_near(g, (int32_t)o, near);  // the new parcel's portion comes off its cell's corners
   }
 }
 struct ResPtrsF {
@@ -1155,24 +1168,29 @@ __global__ void k_residual_update_m(Geom g, ResPtrsF RP, const int32_t* __restri
     RP.r[q][e] = r;
   }
 }
+// Only a kept parcel whose cell is near a mixing event can see a non-zero
+// residual at its corners; the others would only re-round their properties
+// (f v / v) and are left as they are (near, built by k_mix_uncount and
+// k_new_parcels_m).
 __global__ void __launch_bounds__(256, 6) k_redistribute_m(Geom g, int64_t norig, const int32_t* __restrict__ keep,
                                                           double* __restrict__ parcels, int64_t cap,
                                                           const int32_t* __restrict__ cell,
+                                                          const uint8_t* __restrict__ near,
                                                           const float* __restrict__ G8) {
   const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= norig) return;
   auto F = [&](int pid) { return (float*)(parcels + (size_t)pid * cap); };
   const int pids[5] = {PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
-  // the state is read before the keep flag is known (one round trip less)
   const int kp = keep[m];
   const int32_t id = cell[m];
+  if (kp != 1) return;
+  if (id < 0 || id >= g.ncell) return;  // reported by the binning
+  if (!near[id]) return;
   const float delx = F(PMPIC_PROP_X)[m], dely = F(PMPIC_PROP_Y)[m], delz = F(PMPIC_PROP_Z)[m];
   const float v = F(PMPIC_PROP_VOL)[m];
   float s[5];
 #pragma unroll
   for (int q = 0; q < 5; ++q) s[q] = F(pids[q])[m];
-  if (kp != 1) return;
-  if (id < 0 || id >= g.ncell) return;  // reported by the binning
   int ci, cj, ck;
   cell_decode(g, id, ci, cj, ck);
   const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
@@ -1203,18 +1221,24 @@ __global__ void __launch_bounds__(256, 6) k_redistribute_m(Geom g, int64_t norig
 // is known, every slot below it whose content changed (a new parcel, or one
 // moved there by the backfill: keep != 1) is binned from its position, and
 // every kept parcel beyond it (dropped by the backfill) leaves its count.
-__global__ void k_mix_uncount(const int32_t* __restrict__ zlist, const int32_t* __restrict__ nz,
-                              const int32_t* __restrict__ cell, int32_t* __restrict__ count) {
+__global__ void k_mix_uncount(Geom g, const int32_t* __restrict__ zlist, const int32_t* __restrict__ nz,
+                              const int32_t* __restrict__ cell, int32_t* __restrict__ count,
+                              uint8_t* __restrict__ near) {
   const int n = *nz;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     const int32_t c = cell[zlist[t]];
-    if (c >= 0) atomicSub(&count[c], 1);
+    if (c >= 0) {
+      atomicSub(&count[c], 1);
+      mark_near(g, c, near);  // the removed parcel's residuals land on its cell's corners
+    }
   }
 }
-__global__ void k_mix_recount(Geom g, int64_t norig, int64_t nfinal, const int32_t* __restrict__ keep,
+// s0: the first slot that can have changed (norig when no parcel was removed:
+// then only the appended slots did)
+__global__ void k_mix_recount(Geom g, int64_t s0, int64_t norig, int64_t nfinal, const int32_t* __restrict__ keep,
                               const int32_t* __restrict__ cell, int32_t* __restrict__ count, DevInfo* info) {
   const int64_t hi = norig > nfinal ? norig : nfinal;
-  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < hi; s += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t s = s0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < hi; s += (int64_t)gridDim.x * blockDim.x) {
     if (s < nfinal) {
       if (s < norig && keep[s] == 1) continue;  // unchanged
       const int32_t id = cell[s];  // written with the slot's new position
@@ -1692,7 +1716,8 @@ int mixing(pmpic_ctx* ctx) {
   int32_t* nz0 = dcounter(ctx, 3);
   if ((rc = compact(ctx, PredKeepEq{ctx->keep, 0}, norig, zlist, nz0))) return rc;
   if (ctx->mixed) {  // the binning counts stay current through mixing
-    k_mix_uncount<<<148, 256, 0, ctx->stream>>>(zlist, nz0, ctx->cell, ctx->cell_count); ++ctx->nlaunch;
+    PMPIC_CUDA(cudaMemsetAsync(ctx->near, 0, (size_t)g.ncell, ctx->stream));
+    k_mix_uncount<<<148, 256, 0, ctx->stream>>>(g, zlist, nz0, ctx->cell, ctx->cell_count, ctx->near); ++ctx->nlaunch;
   }
   int32_t hz0 = 0;
   PMPIC_CUDA(cudaMemcpyAsync(&hz0, nz0, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1713,8 +1738,8 @@ int mixing(pmpic_ctx* ctx) {
   if (ctx->mixed && !events) {
     const int64_t count0 = norig;
     ctx->n = count0;
-    ctx->sorted_valid = false;
-    ctx->count_ready = true;  // no slot changed: the counts stand
+    ctx->sorted_valid = true;  // no parcel moved or changed slot: the binning stands
+    ctx->count_ready = true;   // and so do the counts
     ctx->in_domain = false;
     ctx->btot_grid_ready = false;
     ctx->info.n_removed = 0;
@@ -1736,13 +1761,13 @@ int mixing(pmpic_ctx* ctx) {
     float* por = (float*)ctx->newportion;
     k_new_parcels_m<<<592, 256, 0, ctx->stream>>>(g, olist, nnew, zlist, nz0, norig, ctx->cap, ctx->keep, ctx->parcels,
                                                   KF[0], KF[1], KF[2], KF[3], KF[4], KF[5], ctx->newslot, por,
-                                                  (float)g.vmin, ctx->cell, ctx->dinfo); ++ctx->nlaunch;
+                                                  (float)g.vmin, ctx->cell, ctx->near, ctx->dinfo); ++ctx->nlaunch;
     k_residual_update_m<<<nblk(g.nphys, 256), 256, 0, ctx->stream>>>(g, RF, ctx->newslot, por); ++ctx->nlaunch;
     if (norig > 0) {
       const float* g7[7] = {KF[0], RF.r[0], RF.r[1], RF.r[2], RF.r[3], RF.r[4], RF.r[5]};
       pack8<float>(ctx, g7, (float*)ctx->gpack);
       k_redistribute_m<<<nblk(norig, 256), 256, 0, ctx->stream>>>(g, norig, ctx->keep, ctx->parcels, ctx->cap,
-                                                                  ctx->cell, (const float*)ctx->gpack);
+                                                                  ctx->cell, ctx->near, (const float*)ctx->gpack);
       ++ctx->nlaunch;
     }
   } else {
@@ -1791,12 +1816,19 @@ int mixing(pmpic_ctx* ctx) {
     count = norig - hz;
   }
   if (ctx->mixed && (norig > 0 || count > 0)) {
+    // with no removal every slot below norig still holds its kept parcel
+    const int64_t s0 = nremove > 0 ? 0 : norig;
     const int64_t hi = std::max<int64_t>(norig, count);
-    k_mix_recount<<<nblk(hi, 256), 256, 0, ctx->stream>>>(g, norig, count, ctx->keep, ctx->cell, ctx->cell_count,
-                                                          ctx->dinfo); ++ctx->nlaunch;
+    if (hi > s0) {
+      k_mix_recount<<<nblk(hi - s0, 256), 256, 0, ctx->stream>>>(g, s0, norig, count, ctx->keep, ctx->cell,
+                                                                 ctx->cell_count, ctx->dinfo);
+      ++ctx->nlaunch;
+    }
   }
   ctx->n = count;
-  ctx->sorted_valid = false;
+  // without an event no parcel moved or changed slot (the FP64 redistribution
+  // changes properties only): the binning made at the start still holds
+  ctx->sorted_valid = nremove == 0 && nadd == 0;
   ctx->count_ready = ctx->mixed;  // the next binning starts at the scan
   ctx->in_domain = false;
   ctx->btot_grid_ready = false;

@@ -204,3 +204,44 @@ def test_mixed_mixing_without_events_keeps_parcels(pm):
     assert o.info().n_removed == 0 and o.info().n_added == 0
     for name in ["vol", "b", "hg", "p", "q", "r"]:
         assert rel(g.grid(name), o.grid(name)) < 1e-5, name
+
+
+def test_mixed_mixing_redistributes_only_near_events(pm):
+    """A few parcels shrunk below vmin in one region: the mixed form applies the
+    residuals to the kept parcels whose cells are within one cell of a removed
+    or a new parcel's cell (only their corners can hold residuals) and leaves
+    every other parcel bit for bit as it was; parcels, counts and the volume
+    total agree with the FP64 oracle within FP32 rounding."""
+    from oracle import Oracle
+    n = 16
+    ic = _vortical(pm, n)
+    k = len(ic["x"])
+    vmin = (TWO_PI / n) ** 2 * (math.pi / n) / 216
+    dx, dz = TWO_PI / n, math.pi / n
+    region = (ic["x"] < 2 * dx) & (ic["y"] < 2 * dx) & (ic["z"] < 2 * dz)
+    shrink = np.nonzero(region)[0][::3]
+    ic["vol"][shrink] = 0.5 * vmin
+    g = pm.Context(n, n, n, TWO_PI, TWO_PI, math.pi, max_parcels=2 * k, precision="mixed")
+    g.upload(**ic)
+    before = {q: g.get(q) for q in ["b", "h", "p", "q", "r", "vol"]}
+    g.set_counters([3, 3, 4, 3, 3])
+    g.parcel_mixing()
+    o = Oracle(n, n, n, TWO_PI, TWO_PI, math.pi, max_parcels=2 * k)
+    o.set_parcels(**ic)
+    o.set_counters([3, 3, 4, 3, 3])
+    o.parcel_mixing()
+    ig, io = g.info(), o.info()
+    assert ig.n_removed == io.n_removed == len(shrink)
+    assert (ig.n_removed, ig.n_added) == (io.n_removed, io.n_added) and g.n == o.n
+    np.testing.assert_array_equal(g.get("tag"), o.get("tag"))
+    for q in ["b", "h", "p", "q", "r", "vol"]:
+        assert rel(g.get(q), o.get(q)) < 1e-5, q
+    # parcels whose cell is more than one cell away (periodically) from the region are untouched
+    tag = g.get("tag").astype(np.int64)
+    ci = np.floor(g.get("x") / dx).astype(int) % n
+    cj = np.floor(g.get("y") / dx).astype(int) % n
+    ck = np.floor(g.get("z") / dz).astype(int)
+    far = ((ci >= 3) & (ci <= n - 2)) | ((cj >= 3) & (cj <= n - 2)) | (ck >= 3)
+    assert far.sum() > k // 2
+    for q in ["b", "h", "p", "q", "r", "vol"]:
+        np.testing.assert_array_equal(g.get(q)[far], before[q][tag[far]], err_msg=q)
