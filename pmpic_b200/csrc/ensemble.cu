@@ -93,6 +93,32 @@ int pmpic_ensemble_create(int n, const pmpic_config* cfgs, pmpic_ensemble** out)
     if (!rc) e->m.push_back(c);
   }
   cudaSetDevice(e->device);
+  // Stream priorities by size: the smaller a member, the higher its stream's
+  // priority.  Small members are bound by the latency of their short kernels;
+  // with priority their blocks are dispatched as soon as an SM frees up
+  // instead of queueing behind the large members' blocks, which fill the
+  // bandwidth either way.  (Each member's stream is replaced before any work
+  // is queued on it: pmpic_create's own set-up is synchronous.)
+  if (!rc) {
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) rc = PMPIC_ERR_CUDA;
+    const int levels = least - greatest + 1;  // greatest is the numerically lowest (highest priority)
+    std::vector<int> by(n);
+    for (int i = 0; i < n; ++i) by[i] = i;
+    std::stable_sort(by.begin(), by.end(), [&](int a, int b) { return e->m[a]->cap < e->m[b]->cap; });
+    for (int r = 0; r < n && !rc && levels > 1; ++r) {
+      pmpic_ctx* c = e->m[by[r]];
+      const int prio = greatest + (int)((int64_t)r * levels / n);  // smallest members: greatest priority
+      cudaStream_t s = nullptr;
+      if (cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, prio) != cudaSuccess) {
+        rc = PMPIC_ERR_CUDA;
+        break;
+      }
+      cudaStreamSynchronize(c->stream);
+      cudaStreamDestroy(c->stream);
+      c->stream = s;
+    }
+  }
   if (!rc && cudaStreamCreateWithFlags(&e->ctl, cudaStreamNonBlocking) != cudaSuccess) rc = PMPIC_ERR_CUDA;
   if (!rc && (cudaEventCreate(&e->t0) != cudaSuccess || cudaEventCreate(&e->t1) != cudaSuccess)) rc = PMPIC_ERR_CUDA;
   e->ends.assign(n, nullptr);

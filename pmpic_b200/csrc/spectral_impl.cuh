@@ -264,7 +264,7 @@ __global__ void k_laplinv(Geom g, LapBatch lb, const real* __restrict__ tab, con
   f[col] = prev;
   // loads of each batch of ZB levels first, then its recurrence (one memory
   // latency per batch); the batch reads f above the levels it overwrites
-  constexpr int ZB = 8;
+  constexpr int ZB = sizeof(real) == 8 ? 4 : 8;  // FP64: fewer registers for the batch
   for (int kb = 1; kb < nz; kb += ZB) {
     real fb[ZB], db[ZB];
 #pragma unroll
