@@ -629,6 +629,10 @@ def run_ensemble(args):
     (pmpic_b200.assign_members; no exchange between ranks): each rank runs its
     share both ways, and the aggregate is all work over the max device time."""
     rank, world, local = dist_env()
+    # 64 member streams: let the device give them more hardware work queues
+    # than the default 8, so independent streams do not wait on one another
+    # (read once, when this process creates its CUDA context, which is below)
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     import torch
     torch.cuda.set_device(local)
     import pmpic_b200 as pm
@@ -721,6 +725,7 @@ def run_ensemble(args):
                                      "(events across all member streams; max over ranks); the batched run is "
                                      "timed after its tuning (row-pass segments per grid size, then six steps "
                                      "trying 2-64 host threads, then the initial state loaded again)"},
+                "cuda_device_max_connections": os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS"),
                 "sequential": {"value": seq_v, "ms": 1e3 * t_seq, "concurrency": 1, "par2grid_segment": 64},
                 "batched": {"value": bat_v, "ms": 1e3 * t_bat, "concurrency": threads,
                             "par2grid_segment_by_grid": sizes, "tuning_ms": ms_tune},
