@@ -383,8 +383,10 @@ def run_b200(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
         pg = dist
-    forms = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
-    headline = forms[-1]
+    # the headline form first, on a device no other context of this process has
+    # allocated and freed memory on yet; the FP64 form after it
+    forms = ["mixed", "fp64"] if args.precision == "both" else [args.precision]
+    headline = forms[0]
     res = {f: run_form(f, args, local, pg, f == headline) for f in forms}
     hr = res[headline]
     err = None

@@ -225,3 +225,53 @@ def test_plume_100_steps_vs_oracle(pm):
         if prec == "fp64":
             np.testing.assert_array_equal(ctx.get("tag"), ref_tag)
         ctx.close()
+
+
+def test_plume_invariants_after_100_steps(pm):
+    """Size-independent properties of the reference's algorithm on the GPU path,
+    both forms, after 100 steps of the 128^3 plume (dt 0.005):
+    * every interior cell holds at least three parcels after mixing (a cell with
+      fewer kept parcels gets a new one, parcel_mixing.F90:160-212);
+    * without splits and removals (this plume has none), every set-up tag
+      survives exactly once through the haloswap re-slots and mixing, and the
+      new parcels carry the zero tag of the unused slots they are appended to
+      (the reference does not set a new parcel's tag);
+    * every position lies in the box, z in [0, Lz];
+    * the total volume equals the set-up's (splitting halves, mixing moves
+      volume between parcels: the compensated total is conserved to rounding);
+    * the step info's counters add up: final count = initial + added + split -
+      removed over the run."""
+    G, dt, steps = 128, 0.005, 100
+    for prec in ("fp64", "mixed"):
+        cap = int(1.1 * 8 * G ** 3)
+        ctx = pm.Context(G, G, G, TWO_PI, TWO_PI, math.pi, dtm=dt, dtmax=dt, max_parcels=cap, precision=prec)
+        ctx.setup_thermal(nx=G, ny=G, nz=G, **THERMAL)
+        n0 = ctx.n
+        v0 = ctx.conserved_sums()[0]
+        added = removed = split = 0
+        for _ in range(steps):
+            ctx.step(1)
+            inf = ctx.info()
+            added += inf.n_added
+            removed += inf.n_removed
+            split += inf.n_split
+        n = ctx.n
+        assert n == n0 + added + split - removed, (prec, n, n0, added, split, removed)
+        x, y, z = ctx.get("x"), ctx.get("y"), ctx.get("z")
+        assert x.min() >= 0 and x.max() < TWO_PI and y.min() >= 0 and y.max() < TWO_PI, prec
+        assert z.min() >= 0 and z.max() <= math.pi, prec
+        cells = ctx.cell_ids()
+        per_cell = np.bincount(cells, minlength=G ** 3)
+        assert per_cell.min() >= 3, (prec, per_cell.min())
+        tag = ctx.get("tag").astype(np.int64)
+        if split == 0 and removed == 0:
+            # every set-up tag once; the new parcels keep their slot's tag, 0 in the
+            # never-used slots they are appended to (the reference does not set it)
+            cnt = np.bincount(tag)
+            assert len(cnt) == n0 and (cnt[1:] == 1).all() and cnt[0] == 1 + added, prec
+        v1 = ctx.conserved_sums()[0]
+        tol = 1e-12 if prec == "fp64" else 1e-5
+        assert abs(v1 - v0) <= tol * v0, (prec, v0, v1)
+        print(f"{prec}: {steps} steps, parcels {n0} -> {n} (added {added}, split {split}, removed {removed}), "
+              f"min parcels per cell {per_cell.min()}, volume {v0!r} -> {v1!r}")
+        ctx.close()
