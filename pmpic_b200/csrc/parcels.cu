@@ -1139,13 +1139,17 @@ struct ResPtrsF {
   float* r[6];
   const float* k[6];
 };
+// A grid point is a corner of a removed or a new parcel's cell only if its
+// cell (i, j, min(k, Nz - 1)) is marked near such a cell: every other point's
+// residuals are zero and stay zero (doubled at a wall or not).
 __global__ void k_residual_update_m(Geom g, ResPtrsF RP, const int32_t* __restrict__ newslot,
-                                    const float* __restrict__ portion) {
+                                    const float* __restrict__ portion, const uint8_t* __restrict__ near) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= g.nphys) return;
   const int i = (int)(e % g.Nx);
   const int j = (int)((e / g.Nx) % g.Ny);
   const int k = (int)(e / ((int64_t)g.Nx * g.Ny));
+  if (!near[cell_encode(g, i, j, k < g.Nz ? k : g.Nz - 1)]) return;
   const int im = i == 0 ? g.Nx - 1 : i - 1, jm = j == 0 ? g.Ny - 1 : j - 1;
   float por[8];
   int np = 0;
@@ -1172,11 +1176,17 @@ __global__ void k_residual_update_m(Geom g, ResPtrsF RP, const int32_t* __restri
 // residual at its corners; the others would only re-round their properties
 // (f v / v) and are left as they are (near, built by k_mix_uncount and
 // k_new_parcels_m).
+// The corners are read from the kept volume grid and the six residual grids
+// themselves (x fastest): few parcels are near an event, so no packed copy is
+// made for them.
+struct RedistGrids {
+  const float* kv;    // kept volume
+  const float* r[6];  // vres, bres, hres, pres, qres, rres
+};
 __global__ void __launch_bounds__(256, 6) k_redistribute_m(Geom g, int64_t norig, const int32_t* __restrict__ keep,
                                                           double* __restrict__ parcels, int64_t cap,
                                                           const int32_t* __restrict__ cell,
-                                                          const uint8_t* __restrict__ near,
-                                                          const float* __restrict__ G8) {
+                                                          const uint8_t* __restrict__ near, RedistGrids RD) {
   const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= norig) return;
   auto F = [&](int pid) { return (float*)(parcels + (size_t)pid * cap); };
@@ -1200,8 +1210,9 @@ __global__ void __launch_bounds__(256, 6) k_redistribute_m(Geom g, int64_t norig
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int x = (u & 1) ? ci1 : ci, y = (u & 2) ? cj1 : cj, z = ck + (u >> 2);
-    const float4* P = (const float4*)(G8 + (((size_t)x * g.Ny + y) * g.nzp + z) * 8);
-    const float4 a0 = P[0], a1 = P[1];  // (vol, vres, b, h) (p, q, r, pad)
+    const size_t gi = ((size_t)z * g.Ny + y) * g.Nx + x;
+    const float4 a0 = make_float4(RD.kv[gi], RD.r[0][gi], RD.r[1][gi], RD.r[2][gi]);  // (vol, vres, bres, hres)
+    const float4 a1 = make_float4(RD.r[3][gi], RD.r[4][gi], RD.r[5][gi], 0.f);        // (pres, qres, rres)
     const float w = ((u & 4) ? delz : 1.f - delz) * ((u & 2) ? dely : 1.f - dely) * ((u & 1) ? delx : 1.f - delx) * v;
     const float wv = __fdividef(w, a0.x);  // the fast quotient (within 2 ulp) of the FP32 form
     nv = nv + wv * a0.y;  // :268-276
@@ -1762,12 +1773,14 @@ int mixing(pmpic_ctx* ctx) {
     k_new_parcels_m<<<592, 256, 0, ctx->stream>>>(g, olist, nnew, zlist, nz0, norig, ctx->cap, ctx->keep, ctx->parcels,
                                                   KF[0], KF[1], KF[2], KF[3], KF[4], KF[5], ctx->newslot, por,
                                                   (float)g.vmin, ctx->cell, ctx->near, ctx->dinfo); ++ctx->nlaunch;
-    k_residual_update_m<<<nblk(g.nphys, 256), 256, 0, ctx->stream>>>(g, RF, ctx->newslot, por); ++ctx->nlaunch;
+    k_residual_update_m<<<nblk(g.nphys, 256), 256, 0, ctx->stream>>>(g, RF, ctx->newslot, por, ctx->near);
+    ++ctx->nlaunch;
     if (norig > 0) {
-      const float* g7[7] = {KF[0], RF.r[0], RF.r[1], RF.r[2], RF.r[3], RF.r[4], RF.r[5]};
-      pack8<float>(ctx, g7, (float*)ctx->gpack);
+      RedistGrids RD;
+      RD.kv = KF[0];
+      for (int q = 0; q < 6; ++q) RD.r[q] = RF.r[q];
       k_redistribute_m<<<nblk(norig, 256), 256, 0, ctx->stream>>>(g, norig, ctx->keep, ctx->parcels, ctx->cap,
-                                                                  ctx->cell, ctx->near, (const float*)ctx->gpack);
+                                                                  ctx->cell, ctx->near, RD);
       ++ctx->nlaunch;
     }
   } else {
