@@ -81,6 +81,9 @@ __global__ void k_bin_count_m(Geom g, int64_t n, const int32_t* __restrict__ cel
 // is used, so their round trips overlap), and such a cell's segment is sorted
 // by slot afterwards (its fill counter is then non-zero).  Whether a cell is
 // one run is a property of the cell, so all its slots take the same path.
+// The 32 slots either side of a window are loaded with the window (one
+// coalesced load each, mostly L1 hits) and the run's extent there is read off
+// two ballots; only a run reaching past them is followed further slot by slot.
 constexpr int SC_ITEMS = 4;
 // the total of counts kept current by other kernels against the parcel count
 // (a mismatch would leave the cell index inconsistent: reported as an error)
@@ -94,18 +97,30 @@ __global__ void __launch_bounds__(256) k_bin_scatter(int64_t n, const int32_t* _
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int64_t t0 = (int64_t)blockIdx.x * 256 * SC_ITEMS + threadIdx.x;
-  int32_t id[SC_ITEMS], base[SC_ITEMS], st[SC_ITEMS];
+  int32_t id[SC_ITEMS], prv[SC_ITEMS], nxt[SC_ITEMS], base[SC_ITEMS], st[SC_ITEMS], cnt[SC_ITEMS];
   unsigned same[SC_ITEMS];
 #pragma unroll
-  for (int k = 0; k < SC_ITEMS; ++k) {
+  for (int k = 0; k < SC_ITEMS; ++k) {  // the window and the 32 slots either side (-2 outside)
     const int64_t t = t0 + 256 * k;
     id[k] = t < n ? cell[t] : -1;
+    prv[k] = t - 32 >= 0 && t - 32 < n ? cell[t - 32] : -2;
+    nxt[k] = t + 32 < n ? cell[t + 32] : -2;
   }
 #pragma unroll
   for (int k = 0; k < SC_ITEMS; ++k) {
     same[k] = __match_any_sync(FULL, id[k]);
+    const bool lead = id[k] >= 0 && lane == __ffs(same[k]) - 1;
+    cnt[k] = lead ? count[id[k]] : 0;
+    st[k] = id[k] >= 0 ? start[id[k]] : 0;
+  }
+#pragma unroll
+  for (int k = 0; k < SC_ITEMS; ++k) {
+    // slots of lane 0's cell just before the window, of lane 31's just after
+    const unsigned bb = __ballot_sync(FULL, prv[k] == __shfl_sync(FULL, id[k], 0));
+    const unsigned ba = __ballot_sync(FULL, nxt[k] == __shfl_sync(FULL, id[k], 31));
+    const int nbefore = __clz(~bb);                        // from slot w0-1 down (32 when all match)
+    const int nafter = ba == FULL ? 32 : __ffs(~ba) - 1;  // from slot w0+32 up
     base[k] = 0;
-    st[k] = 0;
     const int first = __ffs(same[k]) - 1;
     if (id[k] >= 0 && lane == first) {
       // the run containing this window's slots of the cell: contiguous here,
@@ -114,19 +129,24 @@ __global__ void __launch_bounds__(256) k_bin_scatter(int64_t n, const int32_t* _
       const int last = 31 - __clz(same[k]);
       const unsigned m = same[k] >> first;
       const int gsize = __popc(same[k]);
-      const int cnt = count[id[k]];
+      const int c = cnt[k];
       bool run = (m & (m + 1)) == 0;
       int before = 0, after = 0;
-      if (run && gsize < cnt) {
-        if (first == 0)
-          for (int64_t s = w0 - 1; s >= 0 && before < cnt - gsize && cell[s] == id[k]; --s) ++before;
-        if (last == 31)
-          for (int64_t s = w0 + 32; s < n && before + after < cnt - gsize && cell[s] == id[k]; ++s) ++after;
+      if (run && gsize < c) {
+        if (first == 0) {
+          before = min(nbefore, c - gsize);
+          if (before == 32)
+            for (int64_t s = w0 - 33; s >= 0 && before < c - gsize && cell[s] == id[k]; --s) ++before;
+        }
+        if (last == 31) {
+          after = min(nafter, c - gsize - before);
+          if (after == 32)
+            for (int64_t s = w0 + 64; s < n && before + after < c - gsize && cell[s] == id[k]; ++s) ++after;
+        }
       }
-      run = run && before + gsize + after == cnt;
+      run = run && before + gsize + after == c;
       base[k] = run ? before : atomicAdd(&fill[id[k]], gsize);
     }
-    if (id[k] >= 0) st[k] = start[id[k]];
   }
 #pragma unroll
   for (int k = 0; k < SC_ITEMS; ++k) {
@@ -592,26 +612,44 @@ template <int NQ, int MODE, class R = double>
 __global__ void __launch_bounds__(256) k_p2g_combine(Geom g, int nzc, const R* __restrict__ rowpart,
                                                     P2GArgs<NQ, R> a) {
   constexpr int NA = MODE == 0 ? NQ + 1 : NQ;
-  constexpr int TS = NA * NLV + 1;  // odd stride: conflict-free reads by consecutive points
-  constexpr int PX = P2GPx<R>::value;
   constexpr int SEG = NA * NLV;
-  __shared__ R T[2][PX * TS];       // [0]: row y (y-low part), [1]: row y-1 (y-high part)
-  __shared__ R Bz[2][PX * NA];      // the chunk below's top level, same rows
+  constexpr int TS = SEG | 1;  // odd stride: conflict-free reads by consecutive points
+  constexpr int PX = P2GPx<R>::value;
+  __shared__ __align__(16) R T[2][PX * TS];  // [0]: row y (y-low part), [1]: row y-1 (y-high part)
+  __shared__ R Bz[2][PX * NA];               // the chunk below's top level, same rows
   const int px0 = blockIdx.x * PX, py = blockIdx.y, zc = blockIdx.z;
   const int pym = py == 0 ? g.Ny - 1 : py - 1;
   const size_t half = (size_t)nzc * g.Ny * g.Nx * SEG;  // the y-high half follows the y-low one
   const int npx = min(PX, g.Nx - px0);
   const int k0 = zc * ZC, nk = min(ZC, g.Nz - k0);
-  // one warp per (row, point) half-record, lanes along it: coalesced, and no
-  // index division per staged value
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int rp = warp; rp < 2 * PX; rp += blockDim.x >> 5) {
-    const int r = rp / PX, pxl = rp % PX;  // PX is a power of two
-    if (pxl >= npx) continue;
+  // the CTA's records of a row are one contiguous range of npx * SEG values:
+  // copied with 16-byte loads where the range is 16-byte aligned
+  for (int r = 0; r < 2; ++r) {
     const int row = r == 0 ? py : pym;
-    const R* src = rowpart + r * half + (((size_t)zc * g.Ny + row) * g.Nx + px0 + pxl) * SEG;
-    R* dst = &T[r][pxl * TS];
-    for (int o = lane; o < SEG; o += 32) dst[o] = src[o];
+    const R* src = rowpart + r * half + (((size_t)zc * g.Ny + row) * g.Nx + px0) * SEG;
+    R* dst = T[r];
+    const int len = npx * SEG;
+    constexpr int V = 16 / sizeof(R);
+    if (((uintptr_t)src & 15) == 0 && len % V == 0) {
+      for (int e = threadIdx.x; e < len / V; e += blockDim.x) {
+        const float4 u = __ldcs(reinterpret_cast<const float4*>(src) + e);
+        if constexpr (TS == SEG) {  // unpadded: the range as it lies (T[r] is 16-byte aligned)
+          reinterpret_cast<float4*>(dst)[e] = u;
+        } else {
+          const R* uv = reinterpret_cast<const R*>(&u);
+#pragma unroll
+          for (int c = 0; c < V; ++c) {
+            const int f = e * V + c, pxl = f / SEG;
+            dst[pxl * TS + (f - pxl * SEG)] = uv[c];
+          }
+        }
+      }
+    } else {
+      for (int f = threadIdx.x; f < len; f += blockDim.x) {
+        const int pxl = f / SEG;
+        dst[pxl * TS + (f - pxl * SEG)] = src[f];
+      }
+    }
   }
   if (zc > 0) {
     for (int e = threadIdx.x; e < 2 * PX * NA; e += blockDim.x) {
@@ -641,8 +679,14 @@ __global__ void __launch_bounds__(256) k_p2g_combine(Geom g, int nzc, const R* _
     if (MODE == 0) {
       R wv = v[NQ];
       if (wv == R(0)) wv = R(1);  // parcel_interpolation.F90:466
+      if constexpr (sizeof(R) == 8) {
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) a.out[q][o] = v[q] / wv;  // :467
+        for (int q = 0; q < NQ; ++q) a.out[q][o] = v[q] / wv;  // :467
+      } else {  // the FP32 form: one reciprocal for the point's fields
+        const R rw = R(1) / wv;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) a.out[q][o] = v[q] * rw;
+      }
     } else {
       const bool wall = (MODE == 1) && (gl == 0 || gl == g.Nz);
 #pragma unroll
