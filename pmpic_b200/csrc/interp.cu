@@ -695,6 +695,80 @@ __global__ void __launch_bounds__(256) k_p2g_combine(Geom g, int nzc, const R* _
   }
 }
 
+// construct_grids (parcel_mixing.F90:440-624) with the wall doubling
+// (:141-152) for b, h, p, q, r at single grid points: the eight corners of
+// each new parcel's cell, on the mixed form in a mixing call that removes no
+// parcel.  Mixing reads those five grids nowhere else then (the new parcels'
+// box sums :174-186 and their residual portions :202-207); the kept volume
+// grid is made in full.  One warp per (new cell, corner): the lanes take the
+// kept parcels of the point's cells (x, then y, then z low and high, each
+// cell's parcels in slot order) in turn, and a fixed shuffle tree adds their
+// shares, so a point's sums do not depend on timing.  A point shared by two
+// new cells is written twice with the same value.
+struct KeptCorners {
+  const float* f[5];  // b, h, p, q, r
+  float* out[5];      // the B, HG, P, Q, R grids
+  double vmin;
+};
+__global__ void __launch_bounds__(256) k_kept_corners_m(Geom g, const int32_t* __restrict__ olist,
+                                                        const int32_t* __restrict__ nnew,
+                                                        const int32_t* __restrict__ start,
+                                                        const int32_t* __restrict__ sorted,
+                                                        const float* __restrict__ DX, const float* __restrict__ DY,
+                                                        const float* __restrict__ DZ, const float* __restrict__ VOL,
+                                                        KeptCorners a) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int u = threadIdx.x >> 5;  // the corner: x low/high, then y, then z
+  const int64_t e = blockIdx.x;
+  if (e >= *nnew) return;  // the whole block leaves together
+  int ci, cj, ck;
+  cell_decode(g, olist[e], ci, cj, ck);
+  const int px = wrap_index(ci + (u & 1), g.Nx), py = wrap_index(cj + ((u >> 1) & 1), g.Ny), pz = ck + (u >> 2);
+  // the point's cells m = sx + 2 sy + 4 sz: cell (px-1+sx, py-1+sy, pz-1+sz),
+  // of which the point is corner (1-sx, 1-sy, 1-sz); cells below z = 0 or at
+  // z = Nz do not exist
+  int cs[8], len[8];
+  int tot = 0;
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    const int cz = pz - 1 + (m >> 2);
+    cs[m] = 0;
+    len[m] = 0;
+    if (cz >= 0 && cz < g.Nz) {
+      const int32_t id = cell_encode(g, wrap_index(px - 1 + (m & 1), g.Nx), wrap_index(py - 1 + ((m >> 1) & 1), g.Ny), cz);
+      cs[m] = start[id];
+      len[m] = start[id + 1] - cs[m];
+    }
+    tot += len[m];
+  }
+  float acc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+  for (int t = lane; t < tot; t += 32) {
+    int m = 0, off = t;
+    while (off >= len[m]) off -= len[m++];  // t < tot: ends at a cell holding position t
+    const int32_t n = sorted[cs[m] + off];
+    const float vv = VOL[n];
+    if (vv < a.vmin) continue;  // parcel_mixing.F90:488
+    const float delx = DX[n], dely = DY[n], delz = DZ[n];
+    // the corner's weight as the par2grid pass evaluates it
+    const float ez = (m >> 2) ? (1.f - delz) : delz;
+    const float zy = ez * (((m >> 1) & 1) ? (1.f - dely) : dely);
+    const float w = zy * ((m & 1) ? (1.f - delx) : delx) * vv;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) acc[q] = __fmaf_rn(w, a.f[q][n], acc[q]);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int q = 0; q < 5; ++q) acc[q] += __shfl_xor_sync(FULL, acc[q], o);
+  if (lane == 0) {
+    const bool wall = pz == 0 || pz == g.Nz;
+    const size_t gi = ((size_t)pz * g.Ny + py) * g.Nx + px;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) a.out[q][gi] = wall ? acc[q] * 2.f : acc[q];
+  }
+}
+
 // z-fastest cell id -> x-fastest id ((k*Ny + j)*Nx + i); -1 stays -1
 __global__ void k_cell_xfast(Geom g, int64_t n, const int32_t* __restrict__ cell, int32_t* __restrict__ out) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -901,7 +975,9 @@ size_t rowpart_bytes(const Geom& g) {
 // kept grids into VOL, B, HG, P, Q, R (as the reference reuses state%vol,
 // state%b, state%hg, state%p, ...), residual grids into mixres, npercell.
 // With no parcel in the removed class (any_removed false) its sums are all
-// +0.0, which a memset gives without a pass over the parcels.
+// +0.0, which a memset gives without a pass over the parcels.  The mixed form
+// then makes the kept volume grid (and npercell) in full and the five other
+// kept grids only where mixing reads them (launch_kept_corners).
 int launch_mix_grids(pmpic_ctx* ctx, bool any_removed) {
   if (ctx->mixed) {
     const float* f[6] = {nullptr, propf(ctx, PMPIC_PROP_B), propf(ctx, PMPIC_PROP_H),
@@ -909,7 +985,7 @@ int launch_mix_grids(pmpic_ctx* ctx, bool any_removed) {
     float* kept[6] = {(float*)ctx->grid[PMPIC_GRID_VOL], (float*)ctx->grid[PMPIC_GRID_B],
                       (float*)ctx->grid[PMPIC_GRID_HG],  (float*)ctx->grid[PMPIC_GRID_P],
                       (float*)ctx->grid[PMPIC_GRID_Q],   (float*)ctx->grid[PMPIC_GRID_R]};
-    int rc = launch_p2g_m<6, 1>(ctx, f, kept);
+    int rc = any_removed ? launch_p2g_m<6, 1>(ctx, f, kept) : launch_p2g_m<1, 1>(ctx, f, kept);
     if (rc) return rc;
     float* res[6];
     for (int q = 0; q < 6; ++q) res[q] = (float*)ctx->mixres[q];
@@ -927,6 +1003,27 @@ int launch_mix_grids(pmpic_ctx* ctx, bool any_removed) {
   if (any_removed) return launch_p2g<6, 2, false>(ctx, f, ctx->mixres);
   for (int q = 0; q < 6; ++q)
     PMPIC_CUDA(cudaMemsetAsync(ctx->mixres[q], 0, sizeof(double) * ctx->g.nphys, ctx->stream));
+  return 0;
+}
+
+// The kept grids B, HG, P, Q, R at the eight corners of the nnew cells in
+// olist (mixed form, a mixing call without removed parcels; hnew the count,
+// read back).  Requires bin_and_sort of the parcels before mixing.
+int launch_kept_corners(pmpic_ctx* ctx, const int32_t* olist, const int32_t* nnew, int64_t hnew) {
+  if (hnew <= 0) return 0;
+  KeptCorners k;
+  const int pf[5] = {PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
+  const int pg[5] = {PMPIC_GRID_B, PMPIC_GRID_HG, PMPIC_GRID_P, PMPIC_GRID_Q, PMPIC_GRID_R};
+  for (int q = 0; q < 5; ++q) {
+    k.f[q] = propf(ctx, pf[q]);
+    k.out[q] = (float*)ctx->grid[pg[q]];
+  }
+  k.vmin = (double)(float)ctx->g.vmin;
+  k_kept_corners_m<<<(unsigned)hnew, 256, 0, ctx->stream>>>(ctx->g, olist, nnew, ctx->cell_start, ctx->sorted,
+                                                           curoff(ctx, 0), curoff(ctx, 1), curoff(ctx, 2),
+                                                           propf(ctx, PMPIC_PROP_VOL), k);
+  ++ctx->nlaunch;
+  PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
 

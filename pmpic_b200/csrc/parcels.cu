@@ -14,6 +14,7 @@ namespace pmpic {
 
 int scan_excl(pmpic_ctx* ctx, const int32_t* in, int64_t n, int32_t* out);
 int launch_mix_grids(pmpic_ctx* ctx, bool any_removed);
+int launch_kept_corners(pmpic_ctx* ctx, const int32_t* olist, const int32_t* nnew, int64_t hnew);
 
 namespace {
 
@@ -1770,6 +1771,8 @@ int mixing(pmpic_ctx* ctx) {
       RF.k[q] = KF[q];
     }
     float* por = (float*)ctx->newportion;
+    // without removed parcels only the kept volume grid was made in full
+    if (hz0 == 0 && (rc = launch_kept_corners(ctx, olist, nnew, hnew))) return rc;
     k_new_parcels_m<<<592, 256, 0, ctx->stream>>>(g, olist, nnew, zlist, nz0, norig, ctx->cap, ctx->keep, ctx->parcels,
                                                   KF[0], KF[1], KF[2], KF[3], KF[4], KF[5], ctx->newslot, por,
                                                   (float)g.vmin, ctx->cell, ctx->near, ctx->dinfo); ++ctx->nlaunch;

@@ -180,9 +180,12 @@ def test_mixed_rejects_fp64_kernel_ops(pm):
 def test_mixed_mixing_without_events_keeps_parcels(pm):
     """A mixing call that removes no parcel and adds none leaves every residual
     grid at zero; the mixed form then skips the redistribution: the parcels are
-    unchanged bit for bit, the counts report no event, and the kept-class grids
-    (the model's vol, b, hg, p, q, r grids of construct_grids) are still built,
-    within FP32 rounding of the oracle's."""
+    unchanged bit for bit, the counts report no event, and the kept volume grid
+    (the model's vol grid of construct_grids, which the dumps write) is still
+    built, within FP32 rounding of the oracle's.  Without removed parcels the
+    mixed form builds the other kept grids (b, hg, p, q, r) only at the corners
+    of new parcels' cells (covered by the next test): elsewhere they are
+    scratch."""
     from oracle import Oracle
     n = 16
     ic = _vortical(pm, n)
@@ -202,8 +205,52 @@ def test_mixed_mixing_without_events_keeps_parcels(pm):
     o.set_counters([3, 3, 4, 3, 3])
     o.parcel_mixing()
     assert o.info().n_removed == 0 and o.info().n_added == 0
-    for name in ["vol", "b", "hg", "p", "q", "r"]:
-        assert rel(g.grid(name), o.grid(name)) < 1e-5, name
+    assert rel(g.grid("vol"), o.grid("vol")) < 1e-5
+
+
+def test_mixed_new_parcels_without_removals_vs_oracle(pm):
+    """Cells emptied of parcels (inside, at both walls, across the periodic
+    corner), no parcel below vmin: mixing adds a parcel in each under-populated
+    cell.  The mixed form makes the kept volume grid in full and the kept b, h,
+    p, q, r sums only at the corners of the new parcels' cells, from the cells'
+    parcels directly.  Counts, slots and tags equal the oracle's; the new and
+    the redistributed parcels, the volume grid and the kept sums at those
+    corners agree with the FP64 oracle within FP32 rounding."""
+    from oracle import Oracle
+    n = 16
+    ic = _vortical(pm, n)
+    dx, dz = TWO_PI / n, math.pi / n
+    ci = np.floor(ic["x"] / dx).astype(int) % n
+    cj = np.floor(ic["y"] / dx).astype(int) % n
+    ck = np.minimum(np.floor(ic["z"] / dz).astype(int), n - 1)
+    emptied = [(5, 5, 5), (5, 6, 5), (10, 3, 0), (12, 12, n - 1), (0, 0, 8), (n - 1, n - 1, 8)]
+    drop = np.zeros(len(ic["x"]), bool)
+    for c in emptied:
+        drop |= (ci == c[0]) & (cj == c[1]) & (ck == c[2])
+    assert drop.sum() >= len(emptied)
+    ic = {q: v[~drop] for q, v in ic.items()}
+    k = len(ic["x"])
+    g = pm.Context(n, n, n, TWO_PI, TWO_PI, math.pi, max_parcels=2 * k, precision="mixed")
+    g.upload(**ic)
+    g.set_counters([3, 3, 4, 3, 3])
+    g.parcel_mixing()
+    o = Oracle(n, n, n, TWO_PI, TWO_PI, math.pi, max_parcels=2 * k)
+    o.set_parcels(**ic)
+    o.set_counters([3, 3, 4, 3, 3])
+    o.parcel_mixing()
+    ig, io = g.info(), o.info()
+    assert ig.n_removed == io.n_removed == 0
+    assert ig.n_added == io.n_added >= len(emptied) and g.n == o.n
+    np.testing.assert_array_equal(g.get("tag"), o.get("tag"))
+    for q in ["x", "y", "z", "b", "h", "p", "q", "r", "vol"]:
+        assert rel(g.get(q), o.get(q)) < 1e-5, q
+    assert rel(g.grid("vol"), o.grid("vol")) < 1e-5
+    # the kept sums at the corners of the emptied cells (grids are (z, y, x))
+    pts = {(c[2] + a, (c[1] + b) % n, (c[0] + d) % n) for c in emptied for a in (0, 1) for b in (0, 1) for d in (0, 1)}
+    idx = tuple(np.array(sorted(pts)).T)
+    for name in ["b", "hg", "p", "q", "r"]:
+        a, b = g.grid(name)[idx], o.grid(name)[idx]
+        assert np.abs(a - b).max() <= 1e-5 * np.abs(b).max(), name
 
 
 def test_mixed_mixing_redistributes_only_near_events(pm):
