@@ -302,7 +302,7 @@ struct pmpic_ctx {
   double* gspare;            // spare physical grid
   int32_t* sorted;           // cap: slot indices sorted by cell
   double* rowpart;           // par2grid row partials (rowpart_bytes)
-  double* gpack;             // 8 x nphys: gather grids packed z fastest (parcels.cu)
+  double* gpack;             // 6 x nphys: the RK4 gather grids packed z fastest (parcels.cu)
   double* lapcp;             // laplinv's Thomas factor tables (spectral.cu laplinv_tables;
                              // FP32 values on the mixed form)
   int32_t* cell_count;       // ncell + 1

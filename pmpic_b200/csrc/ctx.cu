@@ -248,7 +248,7 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   if (!rc) rc = dalloc(ctx, &ctx->gspare, (size_t)g.nphys);
   if (!rc) rc = dalloc(ctx, &ctx->sorted, cap);
   if (!rc) rc = dalloc(ctx, (char**)&ctx->rowpart, rowpart_bytes(g));
-  if (!rc) rc = dalloc(ctx, &ctx->gpack, 8 * (size_t)g.nphys);  // six RK4 grids or eight mixing fields
+  if (!rc) rc = dalloc(ctx, &ctx->gpack, 6 * (size_t)g.nphys);  // the six RK4 gather grids
   ctx->stage_n = std::min<int64_t>(ctx->cap, (int64_t)1 << 24);
   if (!rc && ctx->mixed) rc = dalloc(ctx, &ctx->stage64, (size_t)ctx->stage_n);
   if (!rc) rc = dalloc(ctx, &ctx->keep, cap);
@@ -265,7 +265,7 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   for (int i = 0; i < 6 && !rc; ++i) rc = dalloc(ctx, &ctx->mixres[i], (size_t)g.nphys);
   if (!rc) rc = dalloc(ctx, &ctx->npercell, (size_t)g.ncell);
   if (!rc) rc = dalloc(ctx, &ctx->newslot, (size_t)g.ncell);
-  if (!rc && ctx->mixed) rc = dalloc(ctx, &ctx->near, (size_t)g.ncell);
+  if (!rc) rc = dalloc(ctx, &ctx->near, (size_t)g.ncell);
   if (!rc) rc = dalloc(ctx, &ctx->newportion, (size_t)g.ncell);
   for (int i = 0; i < PMPIC_NSPEC && !rc; ++i) rc = dalloc(ctx, &ctx->spec[i], (size_t)g.nspec);
   double** sp[] = {&ctx->sa, &ctx->sb, &ctx->sc, &ctx->sd, &ctx->se, &ctx->sf, &ctx->sas, &ctx->sbs};

@@ -148,25 +148,23 @@ struct PkT {
   static constexpr int value = sizeof(R) == 4 ? 64 : 32;
 };
 constexpr int PK_K = 16;  // z extent of a tile
-template <class R, int NF>
+template <class R>
 __global__ void __launch_bounds__(256) k_pack(Geom g, const R* __restrict__ G0, const R* __restrict__ G1,
                                               const R* __restrict__ G2, const R* __restrict__ G3,
                                               const R* __restrict__ G4, const R* __restrict__ G5,
-                                              const R* __restrict__ G6, R* __restrict__ out) {
-  // NF = 6: fields G0..G5; NF = 8: G0..G6 and a zero pad
+                                              R* __restrict__ out) {
+  constexpr int NF = 6;
   constexpr int PK_T = PkT<R>::value;
   constexpr int TS = PK_K * (PK_T + 1) + 1;  // per-field tile stride, odd
   __shared__ R tile[NF * TS];
   const int i0 = blockIdx.x * PK_T, k0 = blockIdx.y * PK_K, j = blockIdx.z;
-  const R* G[7] = {G0, G1, G2, G3, G4, G5, G6};
+  const R* G[NF] = {G0, G1, G2, G3, G4, G5};
   const int ni = min(PK_T, g.Nx - i0), nk = min(PK_K, g.nzp - k0);
 #pragma unroll
   for (int f = 0; f < NF; ++f) {
     for (int e = threadIdx.x; e < PK_K * PK_T; e += blockDim.x) {
       const int kk = e / PK_T, ii = e - kk * PK_T;
-      if (kk < nk && ii < ni)
-        tile[f * TS + kk * (PK_T + 1) + ii] =
-            f < 7 ? G[f][((size_t)(k0 + kk) * g.Ny + j) * g.Nx + i0 + ii] : R(0);
+      if (kk < nk && ii < ni) tile[f * TS + kk * (PK_T + 1) + ii] = G[f][((size_t)(k0 + kk) * g.Ny + j) * g.Nx + i0 + ii];
     }
   }
   __syncthreads();
@@ -182,17 +180,7 @@ static void pack6(pmpic_ctx* ctx, const R* const* grids, R* out) {
   const Geom& g = ctx->g;
   constexpr int PK_T = PkT<R>::value;
   dim3 gr((g.Nx + PK_T - 1) / PK_T, (g.nzp + PK_K - 1) / PK_K, g.Ny);
-  k_pack<R, 6><<<gr, 256, 0, ctx->stream>>>(g, grids[0], grids[1], grids[2], grids[3], grids[4], grids[5], nullptr,
-                                            out);
-  ++ctx->nlaunch;
-}
-template <class R>
-static void pack8(pmpic_ctx* ctx, const R* const* grids, R* out) {  // 7 grids + a pad
-  const Geom& g = ctx->g;
-  constexpr int PK_T = PkT<R>::value;
-  dim3 gr((g.Nx + PK_T - 1) / PK_T, (g.nzp + PK_K - 1) / PK_K, g.Ny);
-  k_pack<R, 8><<<gr, 256, 0, ctx->stream>>>(g, grids[0], grids[1], grids[2], grids[3], grids[4], grids[5], grids[6],
-                                            out);
+  k_pack<R><<<gr, 256, 0, ctx->stream>>>(g, grids[0], grids[1], grids[2], grids[3], grids[4], grids[5], out);
   ++ctx->nlaunch;
 }
 // the six fields at the two levels of xy corner (ci, cj) of a cell of level ck:
@@ -573,6 +561,28 @@ __global__ void k_btot(int64_t n, const double* __restrict__ B, const double* __
 }
 
 // ---- mixing (parcel_mixing.F90:68-431) --------------------------------------------------
+// Residual grids are non-zero only at the corners of cells holding a removed
+// parcel or a new one.  The cells whose corners such a residual can reach: id
+// and its neighbours (periodic in x and y), marked in near (both forms).
+__device__ __forceinline__ void mark_near(const Geom& g, int32_t id, uint8_t* __restrict__ near) {
+  int i, j, k;
+  cell_decode(g, id, i, j, k);
+  for (int dk = -1; dk <= 1; ++dk) {
+    const int kk = k + dk;
+    if (kk < 0 || kk >= g.Nz) continue;
+    for (int dj = -1; dj <= 1; ++dj)
+      for (int di = -1; di <= 1; ++di) near[cell_encode(g, wrap_index(i + di, g.Nx), wrap_index(j + dj, g.Ny), kk)] = 1;
+  }
+}
+// the removed parcels' cells (FP64 path; the mixed form marks them as it uncounts them)
+__global__ void k_mark_removed(Geom g, const int32_t* __restrict__ zlist, const int32_t* __restrict__ nz,
+                               const int32_t* __restrict__ cell, uint8_t* __restrict__ near) {
+  const int n = *nz;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int32_t c = cell[zlist[t]];
+    if (c >= 0 && c < g.ncell) mark_near(g, c, near);
+  }
+}
 __global__ void k_keep(int64_t n, const double* __restrict__ VOL, double vmin, int32_t* __restrict__ keep) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -588,7 +598,8 @@ __global__ void k_new_parcels(Geom g, const int32_t* __restrict__ olist, const i
                               const double* __restrict__ KV, const double* __restrict__ KB,
                               const double* __restrict__ KH, const double* __restrict__ KP,
                               const double* __restrict__ KQ, const double* __restrict__ KR,
-                              int32_t* __restrict__ newslot, double* __restrict__ portion, DevInfo* info) {
+                              int32_t* __restrict__ newslot, double* __restrict__ portion,
+                              uint8_t* __restrict__ near, DevInfo* info) {
   const int na = *nnew, nz0 = *nzero;
   for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < na; a += (int64_t)gridDim.x * blockDim.x) {
     int64_t o = olist[a];
@@ -633,6 +644,7 @@ __global__ void k_new_parcels(Geom g, const int32_t* __restrict__ olist, const i
     int64_t cell = ((int64_t)k * g.Ny + j) * g.Nx + i;
     newslot[cell] = (int32_t)slot;
     portion[cell] = por;
+    mark_near(g, (int32_t)o, near);  // the new parcel's portion comes off its cell's corners
   }
 }
 
@@ -642,13 +654,16 @@ struct ResPtrs {
   double* r[6];
   const double* k[6];
 };
+// A point outside the cells marked near an event keeps its residuals (+0.0,
+// doubled or not), so it is left at once.
 __global__ void k_residual_update(Geom g, ResPtrs RP, const int32_t* __restrict__ newslot,
-                                  const double* __restrict__ portion) {
+                                  const double* __restrict__ portion, const uint8_t* __restrict__ near) {
   int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= g.nphys) return;
   int i = (int)(e % g.Nx);
   int j = (int)((e / g.Nx) % g.Ny);
   int k = (int)(e / ((int64_t)g.Nx * g.Ny));
+  if (!near[cell_encode(g, i, j, k < g.Nz ? k : g.Nz - 1)]) return;
   int im = i == 0 ? g.Nx - 1 : i - 1, jm = j == 0 ? g.Ny - 1 : j - 1;
   double por[8];
   int np = 0;
@@ -673,15 +688,25 @@ __global__ void k_residual_update(Geom g, ResPtrs RP, const int32_t* __restrict_
 }
 
 // residuals onto the kept original parcels (:245-342), with the binning
-// cached at the start of mixing (:80; kept parcels have not moved).  The kept
-// volume grid and the six residual grids are read packed (k_pack, 8 fields per
-// level: vol, vres, bres, hres, pres, qres, rres, pad), the corners visited in
-// the reference's order u = 0..7 (x fastest, then y, then z).
+// cached at the start of mixing (:80; kept parcels have not moved), the
+// corners visited in the reference's order u = 0..7 (x fastest, then y, then
+// z) and read from the kept volume grid and the six residual grids.
+// A parcel whose cell is not marked near an event sees +0.0 residuals at all
+// eight corners; when its eight corner weights are positive (so the kept
+// volume there is too) every term the reference adds is +0.0: nv stays v and
+// each field becomes (f v + 0) / v.  That is computed without the corners,
+// with the same IEEE operations, so the bits are the reference's.  (A corner
+// weight of exactly zero could meet a zero kept volume, 0/0 in the reference:
+// such a parcel takes the full path.)
+struct RedistGridsD {
+  const double* kv;    // kept volume
+  const double* r[6];  // vres, bres, hres, pres, qres, rres
+};
 __global__ void __launch_bounds__(256, 3) k_redistribute(Geom g, int64_t norig, const int32_t* __restrict__ keep,
                                                          double* __restrict__ parcels, int64_t cap,
                                                          const int32_t* __restrict__ cell,
                                                          const double* __restrict__ del,
-                                                         const double* __restrict__ G8) {
+                                                         const uint8_t* __restrict__ near, RedistGridsD RD) {
   int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= norig) return;
   auto A = [&](int pid) -> double* { return parcels + (size_t)pid * cap; };
@@ -695,26 +720,34 @@ __global__ void __launch_bounds__(256, 3) k_redistribute(Geom g, int64_t norig, 
   double s[5];
 #pragma unroll
   for (int q = 0; q < 5; ++q) s[q] = A(pids[q])[m];
-  if (kp != 1 || id < 0) return;
-  const int ck = id % g.Nz, cj = (id / g.Nz) % g.Ny, ci = id / (g.Nz * g.Ny);
-  const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
+  if (kp != 1 || id < 0 || id >= g.ncell) return;
 #pragma unroll
   for (int q = 0; q < 5; ++q) s[q] = s[q] * v;
+  // weight of corner u (:258-265, evaluated left to right as there)
+  auto weight = [&](int u) {
+    return ((u & 4) ? delz : 1 - delz) * ((u & 2) ? dely : 1 - dely) * ((u & 1) ? delx : 1 - delx) * v;
+  };
+  bool far = !near[id];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) far = far && weight(u) > 0.0;
+  if (far) {
+#pragma unroll
+    for (int q = 0; q < 5; ++q) A(pids[q])[m] = __dadd_rn(s[q], 0.0) / v;
+    return;  // vol: v + 0 = v
+  }
+  const int ck = id % g.Nz, cj = (id / g.Nz) % g.Ny, ci = id / (g.Nz * g.Ny);
+  const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
   double nv = v;
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int x = (u & 1) ? ci1 : ci, y = (u & 2) ? cj1 : cj, z = ck + (u >> 2);
-    const double2* P = (const double2*)(G8 + (((size_t)x * g.Ny + y) * g.nzp + z) * 8);
-    const double2 a0 = P[0], a1 = P[1], a2 = P[2], a3 = P[3];  // (vol, vres) (b, h) (p, q) (r, pad)
-    // weight of corner u (:258-265, evaluated left to right as there)
-    const double w = ((u & 4) ? delz : 1 - delz) * ((u & 2) ? dely : 1 - dely) * ((u & 1) ? delx : 1 - delx) * v;
-    const double wv = w / a0.x;  // the w/vol_g factor shared by b, h, p, q, r (:280-335)
-    nv = nv + w * a0.y / a0.x;   // :268-276
-    s[0] = s[0] + wv * a1.x;     // :279-336
-    s[1] = s[1] + wv * a1.y;
-    s[2] = s[2] + wv * a2.x;
-    s[3] = s[3] + wv * a2.y;
-    s[4] = s[4] + wv * a3.x;
+    const size_t gi = ((size_t)z * g.Ny + y) * g.Nx + x;
+    const double kv = RD.kv[gi];
+    const double w = weight(u);
+    const double wv = w / kv;         // the w/vol_g factor shared by b, h, p, q, r (:280-335)
+    nv = nv + w * RD.r[0][gi] / kv;   // :268-276
+#pragma unroll
+    for (int q = 0; q < 5; ++q) s[q] = s[q] + wv * RD.r[q + 1][gi];  // :279-336
   }
   A(PMPIC_PROP_VOL)[m] = nv;
 #pragma unroll
@@ -1068,18 +1101,6 @@ __global__ void k_btot_m(Geom g, int64_t n, const float* __restrict__ B, const f
 }
 
 // mixing (parcel_mixing.F90:68-431) in FP32
-// the cells whose corners a residual at the corners of cell id can reach: id
-// and its neighbours (periodic in x and y), marked in near
-__device__ __forceinline__ void mark_near(const Geom& g, int32_t id, uint8_t* __restrict__ near) {
-  int i, j, k;
-  cell_decode(g, id, i, j, k);
-  for (int dk = -1; dk <= 1; ++dk) {
-    const int kk = k + dk;
-    if (kk < 0 || kk >= g.Nz) continue;
-    for (int dj = -1; dj <= 1; ++dj)
-      for (int di = -1; di <= 1; ++di) near[cell_encode(g, wrap_index(i + di, g.Nx), wrap_index(j + dj, g.Ny), kk)] = 1;
-  }
-}
 __global__ void k_keep_m(int64_t n, const float* __restrict__ VOL, float vmin, int32_t* __restrict__ keep) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -1787,20 +1808,27 @@ int mixing(pmpic_ctx* ctx) {
       ++ctx->nlaunch;
     }
   } else {
+    PMPIC_CUDA(cudaMemsetAsync(ctx->near, 0, (size_t)g.ncell, ctx->stream));
+    if (hz0 > 0) {
+      k_mark_removed<<<148, 256, 0, ctx->stream>>>(g, zlist, nz0, ctx->cell, ctx->near);
+      ++ctx->nlaunch;
+    }
     k_new_parcels<<<592, 256, 0, ctx->stream>>>(g, olist, nnew, zlist, nz0, norig, ctx->cap, ctx->keep, ctx->parcels,
                                                 K[0], K[1], K[2], K[3], K[4], K[5], ctx->newslot, ctx->newportion,
-                                                ctx->dinfo); ++ctx->nlaunch;
+                                                ctx->near, ctx->dinfo); ++ctx->nlaunch;
     ResPtrs RP;
     for (int q = 0; q < 6; ++q) {
       RP.r[q] = ctx->mixres[q];
       RP.k[q] = K[q];
     }
-    k_residual_update<<<nblk(g.nphys, 256), 256, 0, ctx->stream>>>(g, RP, ctx->newslot, ctx->newportion); ++ctx->nlaunch;
+    k_residual_update<<<nblk(g.nphys, 256), 256, 0, ctx->stream>>>(g, RP, ctx->newslot, ctx->newportion, ctx->near);
+    ++ctx->nlaunch;
     if (norig > 0) {
-      const double* g7[7] = {K[0], RP.r[0], RP.r[1], RP.r[2], RP.r[3], RP.r[4], RP.r[5]};
-      pack8<double>(ctx, g7, ctx->gpack);
+      RedistGridsD RD;
+      RD.kv = K[0];
+      for (int q = 0; q < 6; ++q) RD.r[q] = RP.r[q];
       k_redistribute<<<nblk(norig, 256), 256, 0, ctx->stream>>>(g, norig, ctx->keep, ctx->parcels, ctx->cap,
-                                                                ctx->cell, ctx->del, ctx->gpack); ++ctx->nlaunch;
+                                                                ctx->cell, ctx->del, ctx->near, RD); ++ctx->nlaunch;
     }
   }
   const int64_t nremove = hz0, nadd = hnew;

@@ -375,6 +375,66 @@ def test_split_and_mix_steps_vs_oracle(pm):
         assert rel_l2(g.grid(name), o.grid(name)) < 1e-10, name
 
 
+def test_mixing_far_from_events_bit_exact(pm):
+    """Mixing with parcels removed in one corner region and cells emptied in
+    another: a kept parcel more than one cell from every removed or new
+    parcel's cell sees +0.0 residuals at its corners, so the reference's
+    redistribution gives it (f v + 0) / v and leaves its volume.  The FP64 path
+    computes that without reading the grids: those parcels equal the oracle's
+    bit for bit (and the formula, evaluated by numpy); the others agree with
+    the oracle to 1e-12 (its grids sum in another order)."""
+    from oracle import Oracle
+    n = 16
+    ic = _vortical_ic(pm, n)
+    dx, dz = TWO_PI / n, math.pi / n
+    vmin = dx * dx * dz / 216
+    ci = np.floor(ic["x"] / dx).astype(int) % n
+    cj = np.floor(ic["y"] / dx).astype(int) % n
+    ck = np.minimum(np.floor(ic["z"] / dz).astype(int), n - 1)
+    region = (ci < 2) & (cj < 2) & (ck < 2)
+    ic["vol"][np.nonzero(region)[0][::3]] = 0.5 * vmin
+    keep = ~((ci == 8) & (cj == 9) & (ck == 10))  # an emptied cell: a new parcel there
+    ic = {q: v[keep] for q, v in ic.items()}
+    ci, cj, ck = ci[keep], cj[keep], ck[keep]
+    k = len(ic["x"])
+    ic["tag"] = np.arange(k, dtype=np.float64) + 1000.0
+    before = {q: ic[q].copy() for q in ["x", "y", "z", "b", "h", "p", "q", "r", "vol"]}
+    g = pm.Context(n, n, n, TWO_PI, TWO_PI, math.pi, max_parcels=2 * k)
+    o = Oracle(n, n, n, TWO_PI, TWO_PI, math.pi, max_parcels=2 * k)
+    g.upload(**ic)
+    o.set_parcels(**ic)
+    g.set_counters([3, 3, 4, 3, 3])
+    o.set_counters([3, 3, 4, 3, 3])
+    g.parcel_mixing()
+    o.parcel_mixing()
+    ig, io = g.info(), o.info()
+    assert ig.n_removed == io.n_removed > 0 and ig.n_added == io.n_added > 0 and g.n == o.n
+    np.testing.assert_array_equal(g.get("tag"), o.get("tag"))
+    for q in ["b", "h", "p", "q", "r", "vol"]:
+        assert rel(g.get(q), o.get(q)) < 1e-12, q
+
+    def dist(a, c):  # periodic distance in cells
+        return np.minimum((a - c) % n, (c - a) % n)
+    near_new = (dist(ci, 8) <= 1) & (dist(cj, 9) <= 1) & (np.abs(ck - 10) <= 1)
+    near_rem = (np.minimum(dist(ci, 0), dist(ci, 1)) <= 1) & (np.minimum(dist(cj, 0), dist(cj, 1)) <= 1) & (ck <= 2)
+    far = np.nonzero(~near_new & ~near_rem)[0]  # original indices
+    assert len(far) > k // 2
+    # their final slots, by tag (a new parcel keeps its slot's old tag; no far
+    # parcel's slot takes one), checked by the unchanged position
+    tags = g.get("tag")
+    order = np.argsort(tags, kind="stable")
+    pos = np.searchsorted(tags[order], ic["tag"][far])
+    slot = order[pos]
+    assert np.all(tags[slot] == ic["tag"][far])
+    for q in ["x", "y", "z"]:
+        np.testing.assert_array_equal(g.get(q)[slot], before[q][far], err_msg=q)
+    for q in ["b", "h", "p", "q", "r", "vol"]:
+        a, b = g.get(q)[slot], o.get(q)[slot]
+        np.testing.assert_array_equal(a, b, err_msg=q)
+        want = before[q][far] if q == "vol" else (before[q][far] * before["vol"][far] + 0.0) / before["vol"][far]
+        np.testing.assert_array_equal(a, want, err_msg=q)
+
+
 def test_deterministic_steps(pm):
     """No floating-point atomics: two runs give identical bits."""
     n = 32
