@@ -322,8 +322,10 @@ struct pmpic_ctx {
   double* mixres[6];         // residual grids vres..rres
   int32_t* npercell;         // ncell
   int32_t* newslot;          // ncell: slot of the new parcel of a cell or -1
-  uint8_t* near;             // ncell (mixed form, mixing): cell within one of a cell with a
-                             // removed or a new parcel (its corners may hold residuals)
+  uint8_t* near;             // ncell (mixing): cell within one of a cell with a removed or a
+                             // new parcel (its corners may hold residuals)
+  int32_t* whint;            // cap/256 + 1 (mixed form): per RK4 CTA, the cell its first parcel
+                             // moved to at the last stage (where the next stage's window is staged)
   double* newportion;        // ncell: portion of the new parcel of a cell
   // spectral arrays
   double* spec[PMPIC_NSPEC]; // u_s, v_s, w_s

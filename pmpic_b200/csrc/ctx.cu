@@ -122,7 +122,7 @@ void free_all(pmpic_ctx* c) {
                   c->aux,     c->aux2,     c->dir,       c->swapbuf,    c->scan_tmp,   c->npercell,  c->newslot,
                   c->newportion, c->sa,    c->sb,        c->sc,         c->sd,         c->se,        c->sf,
                   c->sas,     c->sbs,      c->sscratch,  c->fftmid,     c->ftw,        c->ftw32,      c->wn32,       c->hsum,       c->stage64,        c->kx,        c->ky,
-                  c->k2,      c->filt,     c->bt,        c->zmode,      c->csum,       c->near,       c->dinfo};
+                  c->k2,      c->filt,     c->bt,        c->zmode,      c->csum,       c->near,       c->whint,      c->dinfo};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int i = 0; i < PMPIC_NGRID; ++i)
@@ -266,6 +266,7 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   if (!rc) rc = dalloc(ctx, &ctx->npercell, (size_t)g.ncell);
   if (!rc) rc = dalloc(ctx, &ctx->newslot, (size_t)g.ncell);
   if (!rc) rc = dalloc(ctx, &ctx->near, (size_t)g.ncell);
+  if (!rc && ctx->mixed) rc = dalloc(ctx, &ctx->whint, (size_t)cap / 256 + 1);
   if (!rc) rc = dalloc(ctx, &ctx->newportion, (size_t)g.ncell);
   for (int i = 0; i < PMPIC_NSPEC && !rc; ++i) rc = dalloc(ctx, &ctx->spec[i], (size_t)g.nspec);
   double** sp[] = {&ctx->sa, &ctx->sb, &ctx->sc, &ctx->sd, &ctx->se, &ctx->sf, &ctx->sas, &ctx->sbs};
@@ -291,6 +292,7 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
     e = cudaMemset(ctx->parcels, 0, sizeof(double) * (size_t)PMPIC_NPROP * cap);
     if (e == cudaSuccess) e = cudaMemset(ctx->dinfo, 0, sizeof(DevInfo) + 64 * sizeof(int32_t));
     for (int i = 0; i < PMPIC_NGRID && e == cudaSuccess; ++i) e = cudaMemset(ctx->grid[i], 0, sizeof(double) * g.nphys);
+    if (e == cudaSuccess && ctx->whint) e = cudaMemset(ctx->whint, 0, sizeof(int32_t) * ((size_t)cap / 256 + 1));
     for (int i = 0; i < PMPIC_NSPEC && e == cudaSuccess; ++i) e = cudaMemset(ctx->spec[i], 0, sizeof(double) * g.nspec);
     if (e != cudaSuccess) rc = cuda_fail(ctx, e, "cudaMemset", __LINE__);
   }

@@ -223,25 +223,118 @@ __device__ __forceinline__ void g2p_packed(const Geom& g, const R* __restrict__ 
 #pragma unroll
   for (int f = 0; f < 6; ++f) d[f] = c0[f] * ex + (c00[f] * ey + (lo[f] * ez + hi[f] * delz) * dely) * delx;
 }
+// The FP32 form of the same, over a corner loader: corner(c, lo, hi) gives the
+// six fields at the two levels of xy corner c = 0: (i, j), 1: (i, j+1),
+// 2: (i+1, j), 3: (i+1, j+1); each product is fused into its sum
+template <class Corner>
+__device__ __forceinline__ void g2p_packed_f(Corner corner, float delx, float dely, float delz, float* d) {
+  const float ez = 1.f - delz, ey = 1.f - dely, ex = 1.f - delx;
+  float lo[6], hi[6], c00[6], c0[6];
+  corner(0, lo, hi);
+#pragma unroll
+  for (int f = 0; f < 6; ++f) c00[f] = __fmaf_rn(hi[f], delz, lo[f] * ez);
+  corner(1, lo, hi);
+#pragma unroll
+  for (int f = 0; f < 6; ++f) c0[f] = __fmaf_rn(__fmaf_rn(hi[f], delz, lo[f] * ez), dely, c00[f] * ey);
+  corner(2, lo, hi);
+#pragma unroll
+  for (int f = 0; f < 6; ++f) c00[f] = __fmaf_rn(hi[f], delz, lo[f] * ez);
+  corner(3, lo, hi);
+#pragma unroll
+  for (int f = 0; f < 6; ++f)
+    d[f] = __fmaf_rn(__fmaf_rn(__fmaf_rn(hi[f], delz, lo[f] * ez), dely, c00[f] * ey), delx, c0[f] * ex);
+}
 template <>
 __device__ __forceinline__ void g2p_packed<float>(const Geom& g, const float* __restrict__ G6, int ci, int cj, int ck,
                                                   float delx, float dely, float delz, float* d) {
   const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
-  const float ez = 1.f - delz, ey = 1.f - dely, ex = 1.f - delx;
-  float lo[6], hi[6], c00[6], c0[6];
-  corner6(g, G6, ci, cj, ck, lo, hi);
+  g2p_packed_f(
+      [&](int c, float* lo, float* hi) { corner6(g, G6, (c & 2) ? ci1 : ci, (c & 1) ? cj1 : cj, ck, lo, hi); }, delx,
+      dely, delz, d);
+}
+
+// ---- staged gather window (mixed form) ---------------------------------------------
+// An RK4 CTA's parcels are consecutive slots, and slots follow cell order (the
+// set-up writes parcels cell by cell and they move little in a stage), so
+// they sit mostly in one column of cells, in a run of levels.  The CTA copies
+// the four corner columns of that run out of the packed grids into shared
+// memory with bulk asynchronous copies (cp.async.bulk, completed on an
+// mbarrier; no multicast) at its start, while its threads load their parcel
+// state; the threads then interpolate from shared memory instead of making a
+// dependent round trip to L2 after their cell ids arrive.  The window is
+// placed by a hint, the cell the CTA's first parcel moved to at the previous
+// stage (written by that stage; L2-resident); a parcel outside the window
+// (or any parcel, if the hint is stale) gathers from the packed grids as
+// before.  The values and their arithmetic are the same either way.
+constexpr int GW_KW = 48;  // levels per staged corner column: 48 * 24 bytes, a multiple of 16
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// bytes (a multiple of 16) from global src to shared dst (both 16-byte aligned)
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+               : "=r"(ok)
+               : "r"(smem_u32(bar)), "r"(parity)
+               : "memory");
+  return ok != 0;
+}
+// the barrier's first phase, with a bound on the tries (false: gave up)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar) {
+  for (int it = 0; it < (1 << 22); ++it)
+    if (mbar_try_wait(bar, 0)) return true;
+  return false;
+}
+// window of corner columns (i0|i0+1, j0|j0+1) around hint cell (i0, j0, k0):
+// column c holds levels s[c] .. s[c] + GW_KW - 1 (s[c] is k0 or k0 - 1, whichever
+// starts the copy on a 16-byte boundary); a parcel in column (i0, j0) with
+// k0 <= ck <= k0 + GW_KW - 3 finds both its levels in every column
+struct GatherWindow {
+  int i0, j0, k0;
+  int s[4];
+};
+__device__ __forceinline__ void window_issue(const Geom& g, const float* G6, int32_t hint, GatherWindow& w,
+                                             float* S, uint64_t* bar) {
+  if (hint < 0 || hint >= g.ncell) hint = 0;
+  int i0, j0, k0;
+  cell_decode(g, hint, i0, j0, k0);
+  const int i1 = i0 + 1 == g.Nx ? 0 : i0 + 1, j1 = j0 + 1 == g.Ny ? 0 : j0 + 1;
+  int64_t src[4];
+  w.i0 = i0;
+  w.j0 = j0;
+  w.k0 = k0;
 #pragma unroll
-  for (int f = 0; f < 6; ++f) c00[f] = __fmaf_rn(hi[f], delz, lo[f] * ez);
-  corner6(g, G6, ci, cj1, ck, lo, hi);
+  for (int c = 0; c < 4; ++c) {
+    const int64_t base = ((int64_t)((c & 2) ? i1 : i0) * g.Ny + ((c & 1) ? j1 : j0)) * g.nzp;
+    const int s0 = k0 - (int)((base + k0) & 1);  // an even point index: 24-byte records on a 16-byte boundary
+    w.s[c] = s0;
+    src[c] = base + s0;
+  }
+  // the window is written before the arrive, which releases it to the waiting threads
+  mbar_expect_tx(bar, 4u * GW_KW * 24u);
+  // (at most GW_KW levels past the grids' end: the pack buffer holds twice their size)
 #pragma unroll
-  for (int f = 0; f < 6; ++f) c0[f] = __fmaf_rn(__fmaf_rn(hi[f], delz, lo[f] * ez), dely, c00[f] * ey);
-  corner6(g, G6, ci1, cj, ck, lo, hi);
-#pragma unroll
-  for (int f = 0; f < 6; ++f) c00[f] = __fmaf_rn(hi[f], delz, lo[f] * ez);
-  corner6(g, G6, ci1, cj1, ck, lo, hi);
-#pragma unroll
-  for (int f = 0; f < 6; ++f)
-    d[f] = __fmaf_rn(__fmaf_rn(__fmaf_rn(hi[f], delz, lo[f] * ez), dely, c00[f] * ey), delx, c0[f] * ex);
+  for (int c = 0; c < 4; ++c) bulk_g2s(S + c * GW_KW * 6, G6 + src[c] * 6, GW_KW * 24u, bar);
+}
+// the six fields at levels lev and lev + 1 of staged corner column c
+__device__ __forceinline__ void corner6_staged(const float* S, int c, int lev, float* lo, float* hi) {
+  const float2* p = (const float2*)(S + (c * GW_KW + lev) * 6);
+  const float2 a = p[0], b = p[1], cc = p[2], d = p[3], e = p[4], f = p[5];
+  lo[0] = a.x; lo[1] = a.y; lo[2] = b.x; lo[3] = b.y; lo[4] = cc.x; lo[5] = cc.y;
+  hi[0] = d.x; hi[1] = d.y; hi[2] = e.x; hi[3] = e.y; hi[4] = f.x; hi[5] = f.y;
 }
 
 // ---- RK4 stage (rk4_integrator.F90:95-319) -----------------------------------------
@@ -790,6 +883,7 @@ struct MPtrs {
   float* fv[3];
   float* d[6];      // dxdt, dydt, dzdt, dpdt, dqdt, drdt
   const float* grid[6];
+  int32_t* whint;   // per CTA: the cell its first parcel moved to at the last stage
 };
 
 // grid2par (parcel_interpolation.F90:299-321) of one FP32 grid at cell (i, j, k), offsets (dx, dy, dz)
@@ -850,8 +944,18 @@ template <bool GU, bool GP>
 __global__ void __launch_bounds__(256, 6) k_rk4_m(Geom g, int64_t n, MPtrs P, int stage, const double* __restrict__ dtp,
                         int8_t* __restrict__ dir, int32_t* __restrict__ count, DevInfo* info,
                         float* __restrict__ stretch, int store_d, int32_t* __restrict__ dircnt) {
+  // the staged gather window, when both gathers are pending (the step's path)
+  __shared__ __align__(16) float gws[(GU && GP) ? 4 * GW_KW * 6 : 4];
+  __shared__ __align__(8) uint64_t gwbar;
+  __shared__ GatherWindow gw;
+  if constexpr (GU && GP) {
+    if (threadIdx.x == 0) mbar_init(&gwbar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) window_issue(g, P.g6, P.whint[blockIdx.x], gw, gws, &gwbar);
+  }
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
+  if (t >= n) return;  // (thread 0 stays: the copies complete before the CTA ends)
+  bool ready = false;
   const float dt = (float)*dtp;  // state%dtm (rk4_integrator.F90:102)
   const float dt6 = dt * (1.f / 6.f), dt2 = dt * 0.5f, dt3 = dt * (1.f / 3.f);
   const float* inv = P.inv;
@@ -878,8 +982,14 @@ __global__ void __launch_bounds__(256, 6) k_rk4_m(Geom g, int64_t n, MPtrs P, in
 #pragma unroll
   for (int v = 0; v < 6; ++v)
     if ((v < 3 && !GU) || (v >= 3 && !GP)) d[v] = P.d[v][t];
-  if (GU && GP) {
-    g2p_packed<float>(g, P.g6, cx[0], cx[1], cx[2], cf[0], cf[1], cf[2], d);
+  if constexpr (GU && GP) {
+    ready = mbar_wait_bounded(&gwbar);
+    if (!ready) atomicCAS(&info->error, 0, PMPIC_ERR_TIMEOUT);
+    if (ready && cx[0] == gw.i0 && cx[1] == gw.j0 && cx[2] >= gw.k0 && cx[2] <= gw.k0 + GW_KW - 3)
+      g2p_packed_f([&](int c, float* lo, float* hi) { corner6_staged(gws, c, cx[2] - gw.s[c], lo, hi); }, cf[0],
+                   cf[1], cf[2], d);
+    else
+      g2p_packed<float>(g, P.g6, cx[0], cx[1], cx[2], cf[0], cf[1], cf[2], d);
   } else if (GU || GP) {
 #pragma unroll
     for (int v = 0; v < 6; ++v) {
@@ -945,6 +1055,12 @@ __global__ void __launch_bounds__(256, 6) k_rk4_m(Geom g, int64_t n, MPtrs P, in
   dir[t] = (int8_t)dr;
   count_mover(t, dr != 0, dircnt);
   count_cell(nid, count);
+  if constexpr (GU && GP) {
+    if (threadIdx.x == 0) {
+      P.whint[blockIdx.x] = nid;  // the next stage's window
+      if (!ready) mbar_wait_bounded(&gwbar);  // no copy in flight when the CTA ends
+    }
+  }
 }
 
 // the haloswap staging of the mixed form: each property as its 8-byte slot or
@@ -1517,6 +1633,7 @@ int rk4_stage(pmpic_ctx* ctx, int stage) {
     P.inv[1] = (float)(1.0 / ctx->g.dy);
     P.inv[2] = (float)(1.0 / ctx->g.dz);
     P.g6 = (const float*)ctx->gpack;
+    P.whint = ctx->whint;
     if (gu && gp) pack6<float>(ctx, P.grid, (float*)ctx->gpack);
     auto kern = gu ? (gp ? k_rk4_m<true, true> : k_rk4_m<true, false>) : (gp ? k_rk4_m<false, true> : k_rk4_m<false, false>);
     PMPIC_CUDA(cudaMemsetAsync(ctx->cell_count, 0, sizeof(int32_t) * (ctx->g.ncell + 1), ctx->stream));
