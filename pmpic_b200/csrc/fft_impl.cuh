@@ -209,32 +209,39 @@ __device__ __forceinline__ void st2(real* __restrict__ p, size_t i, real2 v) { *
 
 // The operator on the values of one spectral element pair of rows ra (xa)
 // and ra + 1 (xb); ca, cb are their spectral columns, lev their level.  For
-// SPEC_VEL x is e (u, v) or a (w) and y is c (u, v) or b (w).
+// SPEC_VEL x is e (u, v) or a (w) and y is c (u, v) or b (w).  The wavenumber
+// tables are laid out like the spectra but kx depends on the x index alone and
+// ky on the row alone, so kx is read from row 0 (x2 = 2 km, the pair's x
+// index) and ky from column 0 of rows ca - x2 and cb - x2: the same values,
+// one small L1-resident row or a per-thread constant instead of a second
+// spectrum-sized read per element.
 template <int OP>
 __device__ __forceinline__ void spec_op(const SpecIn<real>& S, real2 xa, real2 xb, real2 ya, real2 yb, int ca, int cb,
-                                        int lev, real2& A, real2& B) {
+                                        int x2, int lev, real2& A, real2& B) {
+  auto kxp = [&](const real* t) { return ld2(t, x2); };
+  auto kyp = [&](const real* t, int c) { const real v = t[c - x2]; return mk2(v, v); };
   if constexpr (OP == SPEC_VEL) {
     if (S.vmode == 0) {  // f = e - diffy(c), f(:,1,1) = ubar
-      const real2 ta = ld2(S.ky, ca), tb = ld2(S.ky, cb);
+      const real2 ta = kyp(S.ky, ca), tb = kyp(S.ky, cb);
       A = mk2(xa.x - (real(-1) * yb.x) * ta.x, xa.y - (real(-1) * yb.y) * ta.y);
       B = mk2(xb.x - ya.x * tb.x, xb.y - ya.y * tb.y);
       if (ca == 0) A.x = (real)S.zbar[lev];
     } else if (S.vmode == 1) {  // f = diffx(c) - e, f(:,1,1) = vbar
-      const real2 ta = ld2(S.kx, ca), tb = ld2(S.kx, cb);
+      const real2 ta = kxp(S.kx), tb = ta;
       A = mk2((real(-1) * ya.y) * ta.x - xa.x, ya.x * ta.y - xa.y);
       B = mk2((real(-1) * yb.y) * tb.x - xb.x, yb.x * tb.y - xb.y);
       if (ca == 0) A.x = (real)S.zbar[lev];
     } else {  // f = diffy(a) - diffx(b)
-      const real2 ya2 = ld2(S.ky, ca), yb2 = ld2(S.ky, cb), xa2 = ld2(S.kx, ca), xb2 = ld2(S.kx, cb);
+      const real2 ya2 = kyp(S.ky, ca), yb2 = kyp(S.ky, cb), xa2 = kxp(S.kx), xb2 = xa2;
       A = mk2((real(-1) * xb.x) * ya2.x - (real(-1) * ya.y) * xa2.x, (real(-1) * xb.y) * ya2.y - ya.x * xa2.y);
       B = mk2(xa.x * yb2.x - (real(-1) * yb.y) * xb2.x, xa.y * yb2.y - yb.x * xb2.y);
     }
-  } else if constexpr (OP == SPEC_DX) {
-    const real2 ta = ld2(S.tab, ca), tb = ld2(S.tab, cb);
+  } else if constexpr (OP == SPEC_DX) {  // tab = kx
+    const real2 ta = kxp(S.tab), tb = ta;
     A = mk2((real(-1) * xa.y) * ta.x, xa.x * ta.y);
     B = mk2((real(-1) * xb.y) * tb.x, xb.x * tb.y);
-  } else if constexpr (OP == SPEC_DY) {
-    const real2 ta = ld2(S.tab, ca), tb = ld2(S.tab, cb);
+  } else if constexpr (OP == SPEC_DY) {  // tab = ky
+    const real2 ta = kyp(S.tab, ca), tb = kyp(S.tab, cb);
     A = mk2((real(-1) * xb.x) * ta.x, (real(-1) * xb.y) * ta.y);
     B = mk2(xa.x * tb.x, xa.y * tb.y);
   } else if constexpr (OP == SPEC_FILT) {
@@ -262,11 +269,11 @@ __device__ __forceinline__ void spec_pair(const Geom& g, const real* __restrict_
   if constexpr (OP == SPEC_VEL) {
     const real* x = S.vmode == 2 ? S.a : S.e;
     const real* y = S.vmode == 2 ? S.b : S.c;
-    spec_op<OP>(S, ld2(x, ea), ld2(x, eb), ld2(y, ea), ld2(y, eb), ca, cb, lev, A, B);
+    spec_op<OP>(S, ld2(x, ea), ld2(x, eb), ld2(y, ea), ld2(y, eb), ca, cb, 2 * km, lev, A, B);
     if (own) vel_store(S, ea, eb, ca, cb, A, B);
   } else {
     const real2 a = ld2(spec, ea), b = ld2(spec, eb);
-    spec_op<OP>(S, a, b, a, b, ca, cb, lev, A, B);
+    spec_op<OP>(S, a, b, a, b, ca, cb, 2 * km, lev, A, B);
   }
 }
 // the same with the operator chosen at run time (generic-length path)
