@@ -10,13 +10,16 @@ template <class P>
 inline real* RP(P* p) { return reinterpret_cast<real*>(p); }
 
 // ---- elementwise spectral operators --------------------------------------------
+// The wavenumber tables are laid out like a spectral level, but kx depends on
+// the x index ip alone and ky on the row jp alone: kx is read from row 0
+// (kx[ip]) and ky from column 0 (ky[jp * sx]), the same values.
 // diffx (fft_ops.F90:266-295): out(i) = -in(i+1) kx, out(i+1) = in(i) kx
-__device__ __forceinline__ real dx_of(const real* in, int64_t e, int ip, const real* kx, int col) {
-  return (ip & 1) == 0 ? (real(-1) * in[e + 1]) * kx[col] : in[e - 1] * kx[col];
+__device__ __forceinline__ real dx_of(const real* in, int64_t e, int ip, const real* kx) {
+  return (ip & 1) == 0 ? (real(-1) * in[e + 1]) * kx[ip] : in[e - 1] * kx[ip];
 }
 // diffy (fft_ops.F90:366-394)
-__device__ __forceinline__ real dy_of(const real* in, int64_t e, int jp, int sx, const real* ky, int col) {
-  return (jp & 1) == 0 ? (real(-1) * in[e + sx]) * ky[col] : in[e - sx] * ky[col];
+__device__ __forceinline__ real dy_of(const real* in, int64_t e, int jp, int sx, const real* ky) {
+  return (jp & 1) == 0 ? (real(-1) * in[e + sx]) * ky[jp * sx] : in[e - sx] * ky[jp * sx];
 }
 
 struct EwIdx {
@@ -38,12 +41,12 @@ __device__ __forceinline__ bool ew_index(const Geom& g, EwIdx& x) {
 __global__ void k_diffx(Geom g, const real* __restrict__ in, real* __restrict__ out, const real* __restrict__ kx) {
   EwIdx x;
   if (!ew_index(g, x)) return;
-  out[x.e] = dx_of(in, x.e, x.ip, kx, x.col);
+  out[x.e] = dx_of(in, x.e, x.ip, kx);
 }
 __global__ void k_diffy(Geom g, const real* __restrict__ in, real* __restrict__ out, const real* __restrict__ ky) {
   EwIdx x;
   if (!ew_index(g, x)) return;
-  out[x.e] = dy_of(in, x.e, x.jp, g.sx, ky, x.col);
+  out[x.e] = dy_of(in, x.e, x.jp, g.sx, ky);
 }
 __global__ void k_filter(Geom g, const real* __restrict__ in, real* __restrict__ out,
                          const real* __restrict__ filt) {
@@ -61,8 +64,8 @@ __global__ void k_div(Geom g, const real* __restrict__ a, const real* __restrict
   if (!ew_index(g, x)) return;
   const int64_t cs = (int64_t)g.sx * g.sy;
   const int nz = g.nzp;
-  real d = dx_of(a, x.e, x.ip, kx, x.col);
-  real e = dy_of(b, x.e, x.jp, g.sx, ky, x.col);
+  real d = dx_of(a, x.e, x.ip, kx);
+  real e = dy_of(b, x.e, x.jp, g.sx, ky);
   real fz;
   if (x.k == 0) {
     fz = hdzi * (real(4) * c[x.e + cs] - c[x.e + 2 * cs] - real(3) * c[x.e]);
@@ -86,10 +89,11 @@ __global__ void k_filter_sub2(Geom g, const real* __restrict__ f, real* __restri
   EwIdx x;
   if (!ew_index(g, x)) return;
   fo[x.e] = f[x.e] * filt[x.col];
-  const real dxf = (x.ip & 1) == 0 ? (real(-1) * (f[x.e + 1] * filt[x.col + 1])) * kx[x.col]
-                                   : (f[x.e - 1] * filt[x.col - 1]) * kx[x.col];
-  const real dyf = (x.jp & 1) == 0 ? (real(-1) * (f[x.e + g.sx] * filt[x.col + g.sx])) * ky[x.col]
-                                   : (f[x.e - g.sx] * filt[x.col - g.sx]) * ky[x.col];
+  const real kxv = kx[x.ip], kyv = ky[x.jp * g.sx];  // (row 0, column 0: the same values)
+  const real dxf = (x.ip & 1) == 0 ? (real(-1) * (f[x.e + 1] * filt[x.col + 1])) * kxv
+                                   : (f[x.e - 1] * filt[x.col - 1]) * kxv;
+  const real dyf = (x.jp & 1) == 0 ? (real(-1) * (f[x.e + g.sx] * filt[x.col + g.sx])) * kyv
+                                   : (f[x.e - g.sx] * filt[x.col - g.sx]) * kyv;
   a[x.e] = a[x.e] - dxf;
   b[x.e] = b[x.e] - dyf;
 }
