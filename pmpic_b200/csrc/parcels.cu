@@ -110,6 +110,12 @@ struct PredKeepEq {
   int v;
   __device__ bool operator()(int64_t i) const { return keep[i] == v; }
 };
+// the removed class of the mixed form (vol < vmin, parcel_mixing.F90:488), from the volumes
+struct PredVolBelowF {
+  const float* vol;
+  float vmin;
+  __device__ bool operator()(int64_t i) const { return vol[i] < vmin; }
+};
 struct PredDirNZ {
   const int8_t* dir;
   __device__ bool operator()(int64_t i) const { return dir[i] != 0; }
@@ -1329,7 +1335,7 @@ __global__ void __launch_bounds__(256, 6) k_redistribute_m(Geom g, int64_t norig
   if (m >= norig) return;
   auto F = [&](int pid) { return (float*)(parcels + (size_t)pid * cap); };
   const int pids[5] = {PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
-  const int kp = keep[m];
+  const int kp = keep ? keep[m] : 1;  // (no keep flags: no parcel was removed)
   const int32_t id = cell[m];
   if (kp != 1) return;
   if (id < 0 || id >= g.ncell) return;  // reported by the binning
@@ -1854,9 +1860,9 @@ int mixing(pmpic_ctx* ctx) {
   const int64_t norig = ctx->n;
   int rc;
   // keep flags (:488) and the kept / residual grids (construct_grids :440-624)
-  if (norig > 0 && ctx->mixed) {
-    k_keep_m<<<nblk(norig, 256), 256, 0, ctx->stream>>>(norig, propf(ctx, PMPIC_PROP_VOL), (float)g.vmin, ctx->keep); ++ctx->nlaunch;
-  } else if (norig > 0) {
+  // (the mixed form writes the keep flags only once a parcel is known to be removed: without one
+  // every original parcel is kept and nothing reads them)
+  if (norig > 0 && !ctx->mixed) {
     k_keep<<<nblk(norig, 256), 256, 0, ctx->stream>>>(norig, prop(ctx, PMPIC_PROP_VOL), g.vmin, ctx->keep); ++ctx->nlaunch;
   }
   if ((rc = bin_and_sort(ctx))) return rc;
@@ -1864,7 +1870,9 @@ int mixing(pmpic_ctx* ctx) {
   // pass over the parcels only when the class is not empty
   int32_t* zlist = ctx->aux;
   int32_t* nz0 = dcounter(ctx, 3);
-  if ((rc = compact(ctx, PredKeepEq{ctx->keep, 0}, norig, zlist, nz0))) return rc;
+  if (ctx->mixed) rc = compact(ctx, PredVolBelowF{propf(ctx, PMPIC_PROP_VOL), (float)g.vmin}, norig, zlist, nz0);
+  else rc = compact(ctx, PredKeepEq{ctx->keep, 0}, norig, zlist, nz0);
+  if (rc) return rc;
   if (ctx->mixed) {  // the binning counts stay current through mixing
     PMPIC_CUDA(cudaMemsetAsync(ctx->near, 0, (size_t)g.ncell, ctx->stream));
     k_mix_uncount<<<148, 256, 0, ctx->stream>>>(g, zlist, nz0, ctx->cell, ctx->cell_count, ctx->near); ++ctx->nlaunch;
@@ -1872,6 +1880,10 @@ int mixing(pmpic_ctx* ctx) {
   int32_t hz0 = 0;
   PMPIC_CUDA(cudaMemcpyAsync(&hz0, nz0, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
   PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (ctx->mixed && hz0 > 0 && norig > 0) {
+    k_keep_m<<<nblk(norig, 256), 256, 0, ctx->stream>>>(norig, propf(ctx, PMPIC_PROP_VOL), (float)g.vmin, ctx->keep);
+    ++ctx->nlaunch;
+  }
   if ((rc = launch_mix_grids(ctx, hz0 > 0))) return rc;
   // under-populated cells in loop order
   int32_t* olist = ctx->cell_fill;  // ncell entries; free after bin_and_sort
@@ -1920,7 +1932,8 @@ int mixing(pmpic_ctx* ctx) {
       RedistGrids RD;
       RD.kv = KF[0];
       for (int q = 0; q < 6; ++q) RD.r[q] = RF.r[q];
-      k_redistribute_m<<<nblk(norig, 256), 256, 0, ctx->stream>>>(g, norig, ctx->keep, ctx->parcels, ctx->cap,
+      k_redistribute_m<<<nblk(norig, 256), 256, 0, ctx->stream>>>(g, norig, hz0 > 0 ? ctx->keep : nullptr,
+                                                                  ctx->parcels, ctx->cap,
                                                                   ctx->cell, ctx->near, RD);
       ++ctx->nlaunch;
     }
