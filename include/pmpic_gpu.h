@@ -239,8 +239,7 @@ int pmpic_sort_parcels(pmpic_ctx* ctx);
  *  - Calls that overlap on one device share the scratch and race: serialize
  *    them (one stream, or synchronize between calls).
  *  - The first call on a device, made with that device current, looks up the
- *    scratch array's device address (cudaGetSymbolAddress); make that first
- *    call before any stream capture begins. */
+ *    scratch array's device address (cudaGetSymbolAddress). */
 int pmpic_par2grid_static(int32_t nx, int32_t ny, int32_t nz, double lx, double ly, double lz,
                           int64_t n, const double* x, const double* y, const double* z,
                           const double* vol, const double* field, double* out, void* stream);
