@@ -223,8 +223,10 @@ int pmpic_op_vort2vel_grids(pmpic_ctx* ctx);
 int pmpic_sort_parcels(pmpic_ctx* ctx);
 
 /* par2grid without a context and without allocation.  No counterpart in the
- * reference: an addition for callers that cannot allocate device memory at call
- * time.  Same arithmetic and result as pmpic_op_par2grid (binning
+ * reference: an addition for callers that cannot allocate device memory when
+ * they call it, such as a host model whose device memory is all handed to its
+ * own pool allocator, or one that forbids cudaMalloc (which can synchronize the
+ * device) inside its time step.  Same arithmetic and result as pmpic_op_par2grid (binning
  * parcel_interpolation.F90:186-262, par2grid :336-481) of one field with volume
  * weights over an nx x ny x nz box, x in [0,lx), y in [0,ly), z in [0,lz) (the
  * reference's binning rule k < nz rejects z = lz).  nx, ny >= 4 and nz >= 3,
@@ -239,7 +241,8 @@ int pmpic_sort_parcels(pmpic_ctx* ctx);
  *  - Calls that overlap on one device share the scratch and race: serialize
  *    them (one stream, or synchronize between calls).
  *  - The first call on a device, made with that device current, looks up the
- *    scratch array's device address (cudaGetSymbolAddress). */
+ *    scratch array's device address (cudaGetSymbolAddress); make that first
+ *    call before any stream capture begins. */
 int pmpic_par2grid_static(int32_t nx, int32_t ny, int32_t nz, double lx, double ly, double lz,
                           int64_t n, const double* x, const double* y, const double* z,
                           const double* vol, const double* field, double* out, void* stream);
