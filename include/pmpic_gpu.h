@@ -139,9 +139,9 @@ int pmpic_rk4_integrator(pmpic_ctx* ctx);        /* rk4_integrator.F90:95-319 (+
 int pmpic_parcel_splitting(pmpic_ctx* ctx);      /* parcel_splitting.F90:47-168 */
 int pmpic_parcel_mixing(pmpic_ctx* ctx);         /* parcel_mixing.F90:68-431 */
 /* (The kept-class grids of construct_grids go to the vol, b, hg, p, q, r grids as in the
- * reference.  On a PMPIC_MIXED context a call that removes no parcel makes the vol grid in
- * full and the b, hg, p, q, r sums only at the corners of new parcels' cells, the only points
- * mixing reads; elsewhere those five grids are left as scratch.) */
+ * reference.  A call that removes no parcel makes the vol grid in full and the b, hg, p, q, r
+ * sums only at the corners of new parcels' cells, the only points mixing reads; elsewhere
+ * those five grids are left as scratch.) */
 /* nsteps model steps: the integrator group run rksteps (=4) times per step
  * (timestepper.F90:89-106 with global_config:43's group contents). */
 int pmpic_step(pmpic_ctx* ctx, int nsteps);

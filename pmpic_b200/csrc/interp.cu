@@ -705,18 +705,19 @@ __global__ void __launch_bounds__(256) k_p2g_combine(Geom g, int nzc, const R* _
 // cell's parcels in slot order) in turn, and a fixed shuffle tree adds their
 // shares, so a point's sums do not depend on timing.  A point shared by two
 // new cells is written twice with the same value.
+template <class R>
 struct KeptCorners {
-  const float* f[5];  // b, h, p, q, r
-  float* out[5];      // the B, HG, P, Q, R grids
+  const R* f[5];  // b, h, p, q, r
+  R* out[5];      // the B, HG, P, Q, R grids
   double vmin;
 };
-__global__ void __launch_bounds__(256) k_kept_corners_m(Geom g, const int32_t* __restrict__ olist,
-                                                        const int32_t* __restrict__ nnew,
-                                                        const int32_t* __restrict__ start,
-                                                        const int32_t* __restrict__ sorted,
-                                                        const float* __restrict__ DX, const float* __restrict__ DY,
-                                                        const float* __restrict__ DZ, const float* __restrict__ VOL,
-                                                        KeptCorners a) {
+template <class R>
+__global__ void __launch_bounds__(256) k_kept_corners(Geom g, const int32_t* __restrict__ olist,
+                                                      const int32_t* __restrict__ nnew,
+                                                      const int32_t* __restrict__ start,
+                                                      const int32_t* __restrict__ sorted, const R* __restrict__ DX,
+                                                      const R* __restrict__ DY, const R* __restrict__ DZ,
+                                                      const R* __restrict__ VOL, KeptCorners<R> a) {
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int u = threadIdx.x >> 5;  // the corner: x low/high, then y, then z
@@ -742,20 +743,20 @@ __global__ void __launch_bounds__(256) k_kept_corners_m(Geom g, const int32_t* _
     }
     tot += len[m];
   }
-  float acc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+  R acc[5] = {R(0), R(0), R(0), R(0), R(0)};
   for (int t = lane; t < tot; t += 32) {
     int m = 0, off = t;
     while (off >= len[m]) off -= len[m++];  // t < tot: ends at a cell holding position t
     const int32_t n = sorted[cs[m] + off];
-    const float vv = VOL[n];
+    const R vv = VOL[n];
     if (vv < a.vmin) continue;  // parcel_mixing.F90:488
-    const float delx = DX[n], dely = DY[n], delz = DZ[n];
-    // the corner's weight as the par2grid pass evaluates it
-    const float ez = (m >> 2) ? (1.f - delz) : delz;
-    const float zy = ez * (((m >> 1) & 1) ? (1.f - dely) : dely);
-    const float w = zy * ((m & 1) ? (1.f - delx) : delx) * vv;
+    const R delx = DX[n], dely = DY[n], delz = DZ[n];
+    // the corner's weight and products as the par2grid pass evaluates them
+    const R ez = (m >> 2) ? (R(1) - delz) : delz;
+    const R zy = ez * (((m >> 1) & 1) ? (R(1) - dely) : dely);
+    const R w = zy * ((m & 1) ? (R(1) - delx) : delx) * vv;
 #pragma unroll
-    for (int q = 0; q < 5; ++q) acc[q] = __fmaf_rn(w, a.f[q][n], acc[q]);
+    for (int q = 0; q < 5; ++q) acc[q] = madd(w, a.f[q][n], acc[q]);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1)
@@ -765,7 +766,7 @@ __global__ void __launch_bounds__(256) k_kept_corners_m(Geom g, const int32_t* _
     const bool wall = pz == 0 || pz == g.Nz;
     const size_t gi = ((size_t)pz * g.Ny + py) * g.Nx + px;
 #pragma unroll
-    for (int q = 0; q < 5; ++q) a.out[q][gi] = wall ? acc[q] * 2.f : acc[q];
+    for (int q = 0; q < 5; ++q) a.out[q][gi] = wall ? acc[q] * R(2) : acc[q];
   }
 }
 
@@ -975,9 +976,9 @@ size_t rowpart_bytes(const Geom& g) {
 // kept grids into VOL, B, HG, P, Q, R (as the reference reuses state%vol,
 // state%b, state%hg, state%p, ...), residual grids into mixres, npercell.
 // With no parcel in the removed class (any_removed false) its sums are all
-// +0.0, which a memset gives without a pass over the parcels.  The mixed form
-// then makes the kept volume grid (and npercell) in full and the five other
-// kept grids only where mixing reads them (launch_kept_corners).
+// +0.0, which a memset gives without a pass over the parcels, and the kept
+// volume grid (and npercell) is made in full, the five other kept grids only
+// where mixing reads them (launch_kept_corners).
 int launch_mix_grids(pmpic_ctx* ctx, bool any_removed) {
   if (ctx->mixed) {
     const float* f[6] = {nullptr, propf(ctx, PMPIC_PROP_B), propf(ctx, PMPIC_PROP_H),
@@ -998,7 +999,7 @@ int launch_mix_grids(pmpic_ctx* ctx, bool any_removed) {
                         prop(ctx, PMPIC_PROP_P), prop(ctx, PMPIC_PROP_Q), prop(ctx, PMPIC_PROP_R)};
   double* kept[6] = {ctx->grid[PMPIC_GRID_VOL], ctx->grid[PMPIC_GRID_B], ctx->grid[PMPIC_GRID_HG],
                      ctx->grid[PMPIC_GRID_P],   ctx->grid[PMPIC_GRID_Q], ctx->grid[PMPIC_GRID_R]};
-  int rc = launch_p2g<6, 1, false>(ctx, f, kept);
+  int rc = any_removed ? launch_p2g<6, 1, false>(ctx, f, kept) : launch_p2g<1, 1, false>(ctx, f, kept);
   if (rc) return rc;
   if (any_removed) return launch_p2g<6, 2, false>(ctx, f, ctx->mixres);
   for (int q = 0; q < 6; ++q)
@@ -1011,17 +1012,30 @@ int launch_mix_grids(pmpic_ctx* ctx, bool any_removed) {
 // read back).  Requires bin_and_sort of the parcels before mixing.
 int launch_kept_corners(pmpic_ctx* ctx, const int32_t* olist, const int32_t* nnew, int64_t hnew) {
   if (hnew <= 0) return 0;
-  KeptCorners k;
   const int pf[5] = {PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
   const int pg[5] = {PMPIC_GRID_B, PMPIC_GRID_HG, PMPIC_GRID_P, PMPIC_GRID_Q, PMPIC_GRID_R};
-  for (int q = 0; q < 5; ++q) {
-    k.f[q] = propf(ctx, pf[q]);
-    k.out[q] = (float*)ctx->grid[pg[q]];
+  if (ctx->mixed) {
+    KeptCorners<float> k;
+    for (int q = 0; q < 5; ++q) {
+      k.f[q] = propf(ctx, pf[q]);
+      k.out[q] = (float*)ctx->grid[pg[q]];
+    }
+    k.vmin = (double)(float)ctx->g.vmin;
+    k_kept_corners<float><<<(unsigned)hnew, 256, 0, ctx->stream>>>(ctx->g, olist, nnew, ctx->cell_start, ctx->sorted,
+                                                                  curoff(ctx, 0), curoff(ctx, 1), curoff(ctx, 2),
+                                                                  propf(ctx, PMPIC_PROP_VOL), k);
+  } else {
+    KeptCorners<double> k;
+    for (int q = 0; q < 5; ++q) {
+      k.f[q] = prop(ctx, pf[q]);
+      k.out[q] = ctx->grid[pg[q]];
+    }
+    k.vmin = ctx->g.vmin;
+    const double* del = ctx->del;  // the binning made at the start of mixing
+    k_kept_corners<double><<<(unsigned)hnew, 256, 0, ctx->stream>>>(ctx->g, olist, nnew, ctx->cell_start, ctx->sorted,
+                                                                   del, del + ctx->cap, del + 2 * ctx->cap,
+                                                                   prop(ctx, PMPIC_PROP_VOL), k);
   }
-  k.vmin = (double)(float)ctx->g.vmin;
-  k_kept_corners_m<<<(unsigned)hnew, 256, 0, ctx->stream>>>(ctx->g, olist, nnew, ctx->cell_start, ctx->sorted,
-                                                           curoff(ctx, 0), curoff(ctx, 1), curoff(ctx, 2),
-                                                           propf(ctx, PMPIC_PROP_VOL), k);
   ++ctx->nlaunch;
   PMPIC_CUDA(cudaGetLastError());
   return 0;

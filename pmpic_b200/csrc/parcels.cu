@@ -110,10 +110,11 @@ struct PredKeepEq {
   int v;
   __device__ bool operator()(int64_t i) const { return keep[i] == v; }
 };
-// the removed class of the mixed form (vol < vmin, parcel_mixing.F90:488), from the volumes
-struct PredVolBelowF {
-  const float* vol;
-  float vmin;
+// the removed class (vol < vmin, parcel_mixing.F90:488), from the volumes; R the form's type
+template <class R>
+struct PredVolBelow {
+  const R* vol;
+  R vmin;
   __device__ bool operator()(int64_t i) const { return vol[i] < vmin; }
 };
 struct PredDirNZ {
@@ -812,7 +813,7 @@ __global__ void __launch_bounds__(256, 3) k_redistribute(Geom g, int64_t norig, 
   const int pids[5] = {PMPIC_PROP_B, PMPIC_PROP_H, PMPIC_PROP_P, PMPIC_PROP_Q, PMPIC_PROP_R};
   // the state is read before the keep flag is known: one memory round trip
   // less per parcel (removed parcels are few)
-  const int kp = keep[m];
+  const int kp = keep ? keep[m] : 1;  // (no keep flags: no parcel was removed)
   const int32_t id = cell[m];
   const double delx = del[m], dely = del[cap + m], delz = del[2 * cap + m];
   const double v = A(PMPIC_PROP_VOL)[m];
@@ -1860,18 +1861,15 @@ int mixing(pmpic_ctx* ctx) {
   const int64_t norig = ctx->n;
   int rc;
   // keep flags (:488) and the kept / residual grids (construct_grids :440-624)
-  // (the mixed form writes the keep flags only once a parcel is known to be removed: without one
-  // every original parcel is kept and nothing reads them)
-  if (norig > 0 && !ctx->mixed) {
-    k_keep<<<nblk(norig, 256), 256, 0, ctx->stream>>>(norig, prop(ctx, PMPIC_PROP_VOL), g.vmin, ctx->keep); ++ctx->nlaunch;
-  }
+  // (the keep flags are written only once a parcel is known to be removed: without one every
+  // original parcel is kept and nothing reads them)
   if ((rc = bin_and_sort(ctx))) return rc;
   // removed slots Z (ascending), counted first: the removed-class grids need a
   // pass over the parcels only when the class is not empty
   int32_t* zlist = ctx->aux;
   int32_t* nz0 = dcounter(ctx, 3);
-  if (ctx->mixed) rc = compact(ctx, PredVolBelowF{propf(ctx, PMPIC_PROP_VOL), (float)g.vmin}, norig, zlist, nz0);
-  else rc = compact(ctx, PredKeepEq{ctx->keep, 0}, norig, zlist, nz0);
+  if (ctx->mixed) rc = compact(ctx, PredVolBelow<float>{propf(ctx, PMPIC_PROP_VOL), (float)g.vmin}, norig, zlist, nz0);
+  else rc = compact(ctx, PredVolBelow<double>{prop(ctx, PMPIC_PROP_VOL), g.vmin}, norig, zlist, nz0);
   if (rc) return rc;
   if (ctx->mixed) {  // the binning counts stay current through mixing
     PMPIC_CUDA(cudaMemsetAsync(ctx->near, 0, (size_t)g.ncell, ctx->stream));
@@ -1880,8 +1878,11 @@ int mixing(pmpic_ctx* ctx) {
   int32_t hz0 = 0;
   PMPIC_CUDA(cudaMemcpyAsync(&hz0, nz0, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
   PMPIC_CUDA(cudaStreamSynchronize(ctx->stream));
-  if (ctx->mixed && hz0 > 0 && norig > 0) {
-    k_keep_m<<<nblk(norig, 256), 256, 0, ctx->stream>>>(norig, propf(ctx, PMPIC_PROP_VOL), (float)g.vmin, ctx->keep);
+  if (hz0 > 0 && norig > 0) {
+    if (ctx->mixed)
+      k_keep_m<<<nblk(norig, 256), 256, 0, ctx->stream>>>(norig, propf(ctx, PMPIC_PROP_VOL), (float)g.vmin, ctx->keep);
+    else
+      k_keep<<<nblk(norig, 256), 256, 0, ctx->stream>>>(norig, prop(ctx, PMPIC_PROP_VOL), g.vmin, ctx->keep);
     ++ctx->nlaunch;
   }
   if ((rc = launch_mix_grids(ctx, hz0 > 0))) return rc;
@@ -1938,6 +1939,8 @@ int mixing(pmpic_ctx* ctx) {
       ++ctx->nlaunch;
     }
   } else {
+    // without removed parcels only the kept volume grid was made in full
+    if (hz0 == 0 && (rc = launch_kept_corners(ctx, olist, nnew, hnew))) return rc;
     PMPIC_CUDA(cudaMemsetAsync(ctx->near, 0, (size_t)g.ncell, ctx->stream));
     if (hz0 > 0) {
       k_mark_removed<<<148, 256, 0, ctx->stream>>>(g, zlist, nz0, ctx->cell, ctx->near);
@@ -1957,7 +1960,8 @@ int mixing(pmpic_ctx* ctx) {
       RedistGridsD RD;
       RD.kv = K[0];
       for (int q = 0; q < 6; ++q) RD.r[q] = RP.r[q];
-      k_redistribute<<<nblk(norig, 256), 256, 0, ctx->stream>>>(g, norig, ctx->keep, ctx->parcels, ctx->cap,
+      k_redistribute<<<nblk(norig, 256), 256, 0, ctx->stream>>>(g, norig, hz0 > 0 ? ctx->keep : nullptr,
+                                                                ctx->parcels, ctx->cap,
                                                                 ctx->cell, ctx->del, ctx->near, RD); ++ctx->nlaunch;
     }
   }

@@ -435,6 +435,61 @@ def test_mixing_far_from_events_bit_exact(pm):
         np.testing.assert_array_equal(a, want, err_msg=q)
 
 
+def test_mixing_new_parcels_without_removals(pm):
+    """Cells emptied of parcels (inside, at both walls, across the periodic
+    corner) and no parcel below vmin: mixing adds a parcel in each.  Without a
+    removed parcel the kept volume grid is made in full and the kept b, h, p,
+    q, r sums only at the corners of the new parcels' cells, from those cells'
+    parcels directly.  Counts, slots and tags equal the oracle's; parcels, the
+    volume grid and the kept sums at those corners agree to 1e-12 (the sums run
+    in another order); parcels away from the new cells equal it bit for bit."""
+    from oracle import Oracle
+    n = 16
+    ic = _vortical_ic(pm, n)
+    dx, dz = TWO_PI / n, math.pi / n
+    ci = np.floor(ic["x"] / dx).astype(int) % n
+    cj = np.floor(ic["y"] / dx).astype(int) % n
+    ck = np.minimum(np.floor(ic["z"] / dz).astype(int), n - 1)
+    emptied = [(5, 5, 5), (5, 6, 5), (10, 3, 0), (12, 12, n - 1), (0, 0, 8), (n - 1, n - 1, 8)]
+    drop = np.zeros(len(ic["x"]), bool)
+    for c in emptied:
+        drop |= (ci == c[0]) & (cj == c[1]) & (ck == c[2])
+    ic = {q: v[~drop] for q, v in ic.items()}
+    k = len(ic["x"])
+    g = pm.Context(n, n, n, TWO_PI, TWO_PI, math.pi, max_parcels=2 * k)
+    o = Oracle(n, n, n, TWO_PI, TWO_PI, math.pi, max_parcels=2 * k)
+    g.upload(**ic)
+    o.set_parcels(**ic)
+    g.set_counters([3, 3, 4, 3, 3])
+    o.set_counters([3, 3, 4, 3, 3])
+    g.parcel_mixing()
+    o.parcel_mixing()
+    ig, io = g.info(), o.info()
+    assert ig.n_removed == io.n_removed == 0
+    assert ig.n_added == io.n_added >= len(emptied) and g.n == o.n
+    np.testing.assert_array_equal(g.get("tag"), o.get("tag"))
+    for q in ["x", "y", "z"]:
+        np.testing.assert_array_equal(g.get(q), o.get(q), err_msg=q)
+    for q in ["b", "h", "p", "q", "r", "vol"]:
+        assert rel(g.get(q), o.get(q)) < 1e-12, q
+    assert rel(g.grid("vol"), o.grid("vol")) < 1e-12
+    pts = {(c[2] + a, (c[1] + b) % n, (c[0] + d) % n) for c in emptied for a in (0, 1) for b in (0, 1) for d in (0, 1)}
+    idx = tuple(np.array(sorted(pts)).T)
+    for name in ["b", "hg", "p", "q", "r"]:
+        a, b = g.grid(name)[idx], o.grid(name)[idx]
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max(), name
+    # parcels of the original slots more than one cell from every emptied cell
+    def dist(a, c):
+        return np.minimum((a - c) % n, (c - a) % n)
+    ci, cj, ck = ci[~drop], cj[~drop], ck[~drop]
+    far = np.ones(k, bool)
+    for c in emptied:
+        far &= ~((dist(ci, c[0]) <= 1) & (dist(cj, c[1]) <= 1) & (np.abs(ck - c[2]) <= 1))
+    assert far.sum() > k // 2
+    for q in ["b", "h", "p", "q", "r", "vol"]:
+        np.testing.assert_array_equal(g.get(q)[:k][far], o.get(q)[:k][far], err_msg=q)
+
+
 def test_deterministic_steps(pm):
     """No floating-point atomics: two runs give identical bits."""
     n = 32
