@@ -335,8 +335,11 @@ struct pmpic_ctx {
   float* ftw32;              // the same twiddles as float2 (mixed-precision form)
   float* wn32;               // FP32 kx, ky, k2, filter tables and diffz factors
   double* hsum;              // FP64 horizontal sums of p and q per level (mixed form's zero mode)
-  double* stage64;           // mixed form: FP64 staging of host transfers (stage_n values)
+  double* stage64;           // mixed form: FP64 staging of host transfers (stage_n values, two halves)
   int64_t stage_n;
+  cudaStream_t xstream;      // mixed form: the host copies of the staged transfers
+  cudaEvent_t xfull[2];      // a staging half holds its chunk (its producer is done)
+  cudaEvent_t xfree[2];      // a staging half has been read (its consumer is done)
   int ftw_off_x, ftw_off_y;
   pmpic::FftPlan plan_x, plan_y;
   // small per-column data

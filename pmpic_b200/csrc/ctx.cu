@@ -137,6 +137,11 @@ void free_all(pmpic_ctx* c) {
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
   for (int i = 0; i < 8; ++i)
     if (c->marks[i]) cudaEventDestroy(c->marks[i]);
+  for (int i = 0; i < 2; ++i) {
+    if (c->xfull[i]) cudaEventDestroy(c->xfull[i]);
+    if (c->xfree[i]) cudaEventDestroy(c->xfree[i]);
+  }
+  if (c->xstream) cudaStreamDestroy(c->xstream);
   if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -251,6 +256,14 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   if (!rc) rc = dalloc(ctx, &ctx->gpack, 6 * (size_t)g.nphys);  // the six RK4 gather grids
   ctx->stage_n = std::min<int64_t>(ctx->cap, (int64_t)1 << 24);
   if (!rc && ctx->mixed) rc = dalloc(ctx, &ctx->stage64, (size_t)ctx->stage_n);
+  if (!rc && ctx->mixed) {  // the staged transfers' copy stream: copies overlap the conversions
+    e = cudaStreamCreateWithFlags(&ctx->xstream, cudaStreamNonBlocking);
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
+      e = cudaEventCreateWithFlags(&ctx->xfull[i], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->xfree[i], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) rc = cuda_fail(ctx, e, "copy stream", __LINE__);
+  }
   if (!rc) rc = dalloc(ctx, &ctx->keep, cap);
   if (!rc) rc = dalloc(ctx, &ctx->aux, cap);
   if (!rc) rc = dalloc(ctx, &ctx->aux2, 2 * (size_t)ctx->nbmax + cap);
@@ -458,13 +471,23 @@ int pmpic::prop_upload(pmpic_ctx* ctx, int pid, int64_t off, int64_t n, const do
   c.d = cell_size(ctx->g, c.axis);
   c.info = ctx->dinfo;
   char* base = (char*)prop(ctx, pid) + es * off;
-  for (int64_t c0 = 0; c0 < n; c0 += ctx->stage_n) {
-    const int64_t len = std::min<int64_t>(ctx->stage_n, n - c0);
+  // chunks alternate between the staging halves: the copy stream fills one
+  // while the context's stream converts the other
+  const int64_t h = std::max<int64_t>(ctx->stage_n / 2, 1);
+  for (int64_t c0 = 0, i = 0; c0 < n; c0 += h, ++i) {
+    const int64_t len = std::min<int64_t>(h, n - c0);
+    double* buf = ctx->stage64 + (i & 1) * h;
     c.base = propc(ctx, PMPIC_PROP_XO + c.axis) + off + c0;
     c.cell = ctx->cell + off + c0;
-    if (src) PMPIC_CUDA(cudaMemcpyAsync(ctx->stage64, src + c0, sizeof(double) * len, cudaMemcpyHostToDevice, ctx->stream));
-    k_conv_in<<<cblk(len), 256, 0, ctx->stream>>>(ctx->g, len, src ? ctx->stage64 : nullptr, base + es * c0, c);
+    if (src) {
+      PMPIC_CUDA(cudaStreamWaitEvent(ctx->xstream, ctx->xfree[i & 1], 0));  // its last conversion is done
+      PMPIC_CUDA(cudaMemcpyAsync(buf, src + c0, sizeof(double) * len, cudaMemcpyHostToDevice, ctx->xstream));
+      PMPIC_CUDA(cudaEventRecord(ctx->xfull[i & 1], ctx->xstream));
+      PMPIC_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->xfull[i & 1], 0));
+    }
+    k_conv_in<<<cblk(len), 256, 0, ctx->stream>>>(ctx->g, len, src ? buf : nullptr, base + es * c0, c);
     ++ctx->nlaunch;
+    if (src) PMPIC_CUDA(cudaEventRecord(ctx->xfree[i & 1], ctx->stream));
   }
   PMPIC_CUDA(cudaGetLastError());
   return 0;
@@ -482,14 +505,24 @@ int pmpic::prop_download(pmpic_ctx* ctx, int pid, int64_t off, int64_t n, double
   c.axis = axis_of(pid);
   c.d = cell_size(ctx->g, c.axis);
   const char* base = (const char*)prop(ctx, pid) + es * off;
-  for (int64_t c0 = 0; c0 < n; c0 += ctx->stage_n) {
-    const int64_t len = std::min<int64_t>(ctx->stage_n, n - c0);
+  // chunks alternate between the staging halves: the context's stream
+  // converts one while the copy stream empties the other
+  const int64_t h = std::max<int64_t>(ctx->stage_n / 2, 1);
+  for (int64_t c0 = 0, i = 0; c0 < n; c0 += h, ++i) {
+    const int64_t len = std::min<int64_t>(h, n - c0);
+    double* buf = ctx->stage64 + (i & 1) * h;
     c.base = propc(ctx, PMPIC_PROP_XO + c.axis) + off + c0;
     c.cell = ctx->cell + off + c0;
-    k_conv_out<<<cblk(len), 256, 0, ctx->stream>>>(ctx->g, len, base + es * c0, ctx->stage64, c);
+    PMPIC_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->xfree[i & 1], 0));  // its last copy is done
+    k_conv_out<<<cblk(len), 256, 0, ctx->stream>>>(ctx->g, len, base + es * c0, buf, c);
     ++ctx->nlaunch;
-    PMPIC_CUDA(cudaMemcpyAsync(dst + c0, ctx->stage64, sizeof(double) * len, cudaMemcpyDeviceToHost, ctx->stream));
+    PMPIC_CUDA(cudaEventRecord(ctx->xfull[i & 1], ctx->stream));
+    PMPIC_CUDA(cudaStreamWaitEvent(ctx->xstream, ctx->xfull[i & 1], 0));
+    PMPIC_CUDA(cudaMemcpyAsync(dst + c0, buf, sizeof(double) * len, cudaMemcpyDeviceToHost, ctx->xstream));
+    PMPIC_CUDA(cudaEventRecord(ctx->xfree[i & 1], ctx->xstream));
   }
+  // the context's stream waits for the copies, so a caller synchronizing it finds the values on the host
+  for (int i = 0; i < 2; ++i) PMPIC_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->xfree[i], 0));
   PMPIC_CUDA(cudaGetLastError());
   return 0;
 }
