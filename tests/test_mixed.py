@@ -54,6 +54,35 @@ def test_mixed_transfer_round_trip(pm):
     np.testing.assert_array_equal(g.get("tag"), ic["tag"])
 
 
+def test_mixed_transfers_in_several_staged_chunks(pm):
+    """Host transfers of the mixed form go through two device staging halves
+    in chunks of half the staging size (the staging holds min(max_parcels,
+    2^24) values), copied on a separate stream while the context's stream
+    converts.  With max_parcels = n (odd) every property crosses three chunks
+    and both halves: the round trip is what one chunk gives (positions within
+    one FP32 rounding of the offset, fields rounded to FP32, tags exact), and a
+    property set afterwards reads back as set."""
+    rng = np.random.default_rng(17)
+    n = 4097
+    ic = {"x": rng.uniform(0, TWO_PI, n), "y": rng.uniform(0, TWO_PI, n), "z": rng.uniform(0, math.pi, n)}
+    for q in ["p", "q", "r", "b", "h", "stretch"]:
+        ic[q] = rng.standard_normal(n)
+    ic["vol"] = rng.uniform(0.5, 1.5, n) * 1e-3
+    ic["tag"] = np.arange(n, dtype=np.float64) * 3 + 1
+    g = pm.Context(16, 16, 16, TWO_PI, TWO_PI, math.pi, max_parcels=n, precision="mixed")
+    g.upload(**ic)
+    dx, dz = TWO_PI / 16, math.pi / 16
+    out = g.download()
+    for q, d in [("x", dx), ("y", dx), ("z", dz)]:
+        assert np.abs(out[q] - ic[q]).max() <= d * 2.0 ** -23, q
+    for q in ["p", "q", "r", "b", "h", "vol", "stretch"]:
+        np.testing.assert_array_equal(out[q], ic[q].astype(np.float32).astype(np.float64), err_msg=q)
+    np.testing.assert_array_equal(out["tag"], ic["tag"])
+    v = rng.standard_normal(n)
+    g.set("p", v)
+    np.testing.assert_array_equal(g.get("p"), v.astype(np.float32).astype(np.float64))
+
+
 def test_mixed_config0_twenty_steps_vs_oracle(pm):
     """Config 0: 32^3 plume, dt = 0.01, 20 steps."""
     from oracle import Oracle
