@@ -324,8 +324,9 @@ struct pmpic_ctx {
   int32_t* newslot;          // ncell: slot of the new parcel of a cell or -1
   uint8_t* near;             // ncell (mixing): cell within one of a cell with a removed or a
                              // new parcel (its corners may hold residuals)
-  int32_t* whint;            // cap/256 + 1 (mixed form): per RK4 CTA, the cell its first parcel
-                             // moved to at the last stage (where the next stage's window is staged)
+  int32_t* whint;            // cap/256 + 1: per RK4 CTA, where its gather window is staged: the
+                             // cell its first parcel moved to at the last stage (mixed form), or
+                             // the one the last binning found (FP64 path)
   double* newportion;        // ncell: portion of the new parcel of a cell
   // spectral arrays
   double* spec[PMPIC_NSPEC]; // u_s, v_s, w_s

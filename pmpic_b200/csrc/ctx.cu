@@ -279,7 +279,7 @@ int pmpic_create(const pmpic_config* cfg, pmpic_ctx** out) {
   if (!rc) rc = dalloc(ctx, &ctx->npercell, (size_t)g.ncell);
   if (!rc) rc = dalloc(ctx, &ctx->newslot, (size_t)g.ncell);
   if (!rc) rc = dalloc(ctx, &ctx->near, (size_t)g.ncell);
-  if (!rc && ctx->mixed) rc = dalloc(ctx, &ctx->whint, (size_t)cap / 256 + 1);
+  if (!rc) rc = dalloc(ctx, &ctx->whint, (size_t)cap / 256 + 1);
   if (!rc) rc = dalloc(ctx, &ctx->newportion, (size_t)g.ncell);
   for (int i = 0; i < PMPIC_NSPEC && !rc; ++i) rc = dalloc(ctx, &ctx->spec[i], (size_t)g.nspec);
   double** sp[] = {&ctx->sa, &ctx->sb, &ctx->sc, &ctx->sd, &ctx->se, &ctx->sf, &ctx->sas, &ctx->sbs};

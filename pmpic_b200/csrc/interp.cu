@@ -34,9 +34,11 @@ namespace {
 inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
 // ---- binning (cache_parcel_interp_weights, parcel_interpolation.F90:186-262) ----
+// (whint, when given: each block's first cell, the window hint of the FP64 RK4 stage)
 __global__ void k_bin_count(Geom g, int64_t n, const double* __restrict__ X, const double* __restrict__ Y,
                             const double* __restrict__ Z, int32_t* __restrict__ cell, double* __restrict__ del,
-                            int64_t cap, int32_t* __restrict__ count, DevInfo* info) {
+                            int64_t cap, int32_t* __restrict__ count, DevInfo* info,
+                            int32_t* __restrict__ whint = nullptr) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   int ci, cj, ck;
@@ -48,6 +50,7 @@ __global__ void k_bin_count(Geom g, int64_t n, const double* __restrict__ X, con
   }
   int32_t id = (int32_t)(((int64_t)ci * g.Ny + cj) * g.Nz + ck);
   cell[t] = id;
+  if (whint && threadIdx.x == 0) whint[blockIdx.x] = id;
   del[t] = dx;
   del[cap + t] = dy;
   del[2 * cap + t] = dz;
@@ -859,7 +862,7 @@ int bin_and_sort(pmpic_ctx* ctx) {
     } else if (n > 0) {
       k_bin_count<<<nblk(n, 256), 256, 0, ctx->stream>>>(g, n, prop(ctx, PMPIC_PROP_X), prop(ctx, PMPIC_PROP_Y),
                                                          prop(ctx, PMPIC_PROP_Z), ctx->cell, ctx->del, ctx->cap,
-                                                         ctx->cell_count, ctx->dinfo); ++ctx->nlaunch;
+                                                         ctx->cell_count, ctx->dinfo, ctx->whint); ++ctx->nlaunch;
     }
   }
   ctx->count_ready = false;

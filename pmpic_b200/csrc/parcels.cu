@@ -344,6 +344,60 @@ __device__ __forceinline__ void corner6_staged(const float* S, int c, int lev, f
   hi[0] = d.x; hi[1] = d.y; hi[2] = e.x; hi[3] = e.y; hi[4] = f.x; hi[5] = f.y;
 }
 
+// The FP64 path's window: its packed records are 48 bytes (always on a 16-byte
+// boundary), so every column starts at the hint's level k0 and holds the
+// levels k0 .. k0 + len - 1 that its column has (len <= GWD_KW; no copy reads
+// past the grids).  The hint is the cell of the CTA's first parcel as the
+// binning before the stage found it, so it is exact.
+constexpr int GWD_KW = 40;  // levels per staged corner column, FP64
+struct GatherWindowD {
+  int i0, j0, k0, len;
+};
+__device__ __forceinline__ void window_issue_d(const Geom& g, const double* G6, int32_t hint, GatherWindowD& w,
+                                               double* S, uint64_t* bar) {
+  if (hint < 0 || hint >= g.ncell) hint = 0;
+  int i0, j0, k0;
+  cell_decode(g, hint, i0, j0, k0);
+  const int i1 = i0 + 1 == g.Nx ? 0 : i0 + 1, j1 = j0 + 1 == g.Ny ? 0 : j0 + 1;
+  const int len = min(GWD_KW, g.nzp - k0);
+  w.i0 = i0;
+  w.j0 = j0;
+  w.k0 = k0;
+  w.len = len;
+  // the window is written before the arrive, which releases it to the waiting threads
+  mbar_expect_tx(bar, 4u * (uint32_t)len * 48u);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int64_t base = ((int64_t)((c & 2) ? i1 : i0) * g.Ny + ((c & 1) ? j1 : j0)) * g.nzp;
+    bulk_g2s(S + c * GWD_KW * 6, G6 + (base + k0) * 6, (uint32_t)len * 48u, bar);
+  }
+}
+// grid2par of the six fields from a staged window, in the FP64 path's order
+// (the same operations as g2p_packed<double>)
+__device__ __forceinline__ void g2p_staged_d(const double* S, int lev, double delx, double dely, double delz,
+                                             double* d) {
+  const double ez = 1.0 - delz, ey = 1.0 - dely, ex = 1.0 - delx;
+  double lo[6], hi[6], c00[6], c0[6];
+  auto corner = [&](int c) {
+    const double2* p = (const double2*)(S + (c * GWD_KW + lev) * 6);
+    const double2 a = p[0], b = p[1], cc = p[2], dd = p[3], e = p[4], f = p[5];
+    lo[0] = a.x; lo[1] = a.y; lo[2] = b.x; lo[3] = b.y; lo[4] = cc.x; lo[5] = cc.y;
+    hi[0] = dd.x; hi[1] = dd.y; hi[2] = e.x; hi[3] = e.y; hi[4] = f.x; hi[5] = f.y;
+  };
+  corner(0);
+#pragma unroll
+  for (int f = 0; f < 6; ++f) c00[f] = lo[f] * ez + hi[f] * delz;
+  corner(1);
+#pragma unroll
+  for (int f = 0; f < 6; ++f) c0[f] = c00[f] * ey + (lo[f] * ez + hi[f] * delz) * dely;
+  corner(2);
+#pragma unroll
+  for (int f = 0; f < 6; ++f) c00[f] = lo[f] * ez + hi[f] * delz;
+  corner(3);
+#pragma unroll
+  for (int f = 0; f < 6; ++f) d[f] = c0[f] * ex + (c00[f] * ey + (lo[f] * ez + hi[f] * delz) * dely) * delx;
+}
+
 // ---- RK4 stage (rk4_integrator.F90:95-319) -----------------------------------------
 // One pass per stage: the deferred grid2par gathers of vort2vel (u, v, w ->
 // dxdt, dydt, dzdt, vort2vel.F90:325-327) and of vorticity_tendency (dp, dq,
@@ -358,6 +412,7 @@ struct RkPtrs {
   double* d[6];
   const double* grid[6];  // u, v, w, dp, dq, dr
   const double* g6;       // the six packed (k_pack), when both gathers are pending
+  const int32_t* whint;   // per CTA: the cell of its first parcel (the binning's)
 };
 
 __device__ __forceinline__ int classify_dir(const Geom& g, double x, double y) {
@@ -378,8 +433,18 @@ template <bool GU, bool GP>
 __global__ void __launch_bounds__(256, 4) k_rk4(Geom g, int64_t n, RkPtrs P, int stage, const double* __restrict__ dtp,
                       const int32_t* __restrict__ cell, const double* __restrict__ del, int64_t cap,
                       int8_t* __restrict__ dir, int store_d, int32_t* __restrict__ dircnt) {
+  // the staged gather window, when both gathers are pending (the step's path)
+  __shared__ __align__(16) double gws[(GU && GP) ? 4 * GWD_KW * 6 : 2];
+  __shared__ __align__(8) uint64_t gwbar;
+  __shared__ GatherWindowD gw;
+  if constexpr (GU && GP) {
+    if (threadIdx.x == 0) mbar_init(&gwbar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) window_issue_d(g, P.g6, P.whint[blockIdx.x], gw, gws, &gwbar);
+  }
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
+  if (t >= n) return;  // (thread 0 stays: the copies complete before the CTA ends)
+  bool ready = false;
   const double dt = *dtp;  // state%dtm (rk4_integrator.F90:102)
   const double dt6 = dt / 6, dt2 = dt / 2, dt3 = dt / 3;
   // every load of this parcel is issued before the first store, so none of
@@ -401,7 +466,13 @@ __global__ void __launch_bounds__(256, 4) k_rk4(Geom g, int64_t n, RkPtrs P, int
     const int ci1 = ci + 1 == g.Nx ? 0 : ci + 1, cj1 = cj + 1 == g.Ny ? 0 : cj + 1;
     const size_t r00 = ((size_t)ck * g.Ny + cj) * g.Nx, r01 = ((size_t)ck * g.Ny + cj1) * g.Nx;
     const size_t r10 = ((size_t)(ck + 1) * g.Ny + cj) * g.Nx, r11 = ((size_t)(ck + 1) * g.Ny + cj1) * g.Nx;
-    if (GU && GP) g2p_packed<double>(g, P.g6, ci, cj, ck, delx, dely, delz, d);
+    if constexpr (GU && GP) {
+      ready = mbar_wait_bounded(&gwbar);
+      if (ready && ci == gw.i0 && cj == gw.j0 && ck >= gw.k0 && ck <= gw.k0 + gw.len - 2)
+        g2p_staged_d(gws, ck - gw.k0, delx, dely, delz, d);
+      else
+        g2p_packed<double>(g, P.g6, ci, cj, ck, delx, dely, delz, d);
+    }
 #pragma unroll
     for (int v = 0; v < 6; ++v) {
       if ((v < 3 && !GU) || (v >= 3 && !GP) || (GU && GP)) continue;
@@ -452,6 +523,9 @@ __global__ void __launch_bounds__(256, 4) k_rk4(Geom g, int64_t n, RkPtrs P, int
   const int dr = classify_dir(g, snew[0], snew[1]);
   dir[t] = (int8_t)dr;
   count_mover(t, dr != 0, dircnt);
+  if constexpr (GU && GP) {
+    if (threadIdx.x == 0 && !ready) mbar_wait_bounded(&gwbar);  // no copy in flight when the CTA ends
+  }
 }
 
 // ---- parcel haloswap (parcels/haloswap.F90:109-289, one rank) -------------------------
@@ -1678,6 +1752,7 @@ int rk4_stage(pmpic_ctx* ctx, int stage) {
   const bool gu = ctx->pending_uvw, gp = ctx->pending_pqr;
   if ((gu || gp) && !ctx->sorted_valid) return set_error(ctx, PMPIC_ERR_STATE, "deferred gather without binning");
   P.g6 = ctx->gpack;
+  P.whint = ctx->whint;
   if (gu && gp) pack6<double>(ctx, P.grid, ctx->gpack);
   auto kern = gu ? (gp ? k_rk4<true, true> : k_rk4<true, false>) : (gp ? k_rk4<false, true> : k_rk4<false, false>);
   // the next binning stays a separate pass on this path: its six IEEE
